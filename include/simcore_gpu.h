@@ -1,0 +1,168 @@
+/* simcore_gpu.h -- C ABI of the B200 Brownian-dynamics filament step.
+ *
+ * Drop-in replacement for the two halves of simcore's filament timestep:
+ *   - InteractionManager::Interact's pair path (reference
+ *     src/interaction_manager.cpp:63-95; declared at
+ *     include/simcore/interaction_manager.hpp:72): cell-list rebuild on the
+ *     accumulated-displacement rule, segment-segment minimum distance, WCA
+ *     forces and torques, scatter onto bond force/torque accumulators;
+ *   - FilamentSpecies::UpdatePositions -> Filament::UpdatePosition(bool
+ *     midstep) (src/filament_species.cpp:59-85, src/filament.cpp:394-428;
+ *     declared at include/simcore/species_base.hpp:29 and
+ *     include/simcore/filament.hpp:109): bond-to-site forces, bending and
+ *     metric forces, random-force projection, tension solve, midpoint
+ *     position update, bond renormalisation.
+ * sc_step() runs whole Simulation::RunSimulation steps
+ * (src/simulation.cpp:37-62) with the two halves fused on the GPU.
+ *
+ * Conventions: plain C types only; every vector is 3 doubles (z = 0 in 2D);
+ * sites and bonds are numbered filament by filament in the order given to
+ * sc_add_filaments.  Host arrays are caller owned and copied.  No call
+ * exits, throws or aborts: every entry point returns an sc_status, and
+ * sc_last_error() describes the last failure of a context.  A context is
+ * not thread safe; several contexts may live in one process (there is no
+ * static state, unlike the reference's CellList and MinimumDistance). */
+#ifndef SIMCORE_GPU_H
+#define SIMCORE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  SC_OK = 0,
+  SC_ERR_INVALID_ARG = 1,   /* bad descriptor, sizes or call order */
+  SC_ERR_OOM = 2,           /* device allocation failed */
+  SC_ERR_NAN = 3,           /* NaN/Inf in forces or positions */
+  SC_ERR_LIST_OVERFLOW = 4, /* pair list larger than its capacity */
+  SC_ERR_TIMEOUT = 5,       /* a bounded device wait gave up */
+  SC_ERR_CUDA = 6,          /* CUDA runtime error (see sc_last_error) */
+  SC_ERR_UNPHYSICAL = 7,    /* accumulated displacement > 10000, as the
+                               reference's "Unphysical result"
+                               (include/simcore/species.hpp:114-118) */
+  SC_ERR_INSERTION = 8,     /* random insertion could not place a filament */
+  SC_ERR_NO_DEVICE = 9      /* no usable CUDA device */
+} sc_status;
+
+typedef enum {
+  /* Every stage in FP64 with the reference's operation order and no FMA
+   * contraction: bit-identical to the reference's CPU code. */
+  SC_PREC_FP64 = 0,
+  /* Pair geometry and WCA forces in FP32 (Kahan-compensated per-bond sums);
+   * bending, tension solves and positions stay FP64. */
+  SC_PREC_MIXED = 1
+} sc_precision;
+
+typedef struct {
+  int n_dim;                  /* 2 or 3; every dimension periodic */
+  double system_radius;       /* R: box side 2R (system_radius) */
+  double delta;               /* delta: one step advances delta/2 */
+  double wca_eps;             /* wca_eps */
+  double wca_sig;             /* wca_sig; cutoff 2^(1/6) wca_sig */
+  double f_cutoff;            /* f_cutoff: cap on |WCA force| */
+  int stoch_flag;             /* thermal noise on/off */
+  int interaction_flag;       /* pair forces on/off */
+  int like_like_interactions; /* 0: filaments do not interact */
+  uint32_t seed;              /* Philox key word 0 of the noise streams */
+  int precision;              /* sc_precision */
+  int device;                 /* CUDA device ordinal */
+} sc_system_desc;
+
+typedef struct {
+  double length;              /* filament length */
+  double persistence_length;  /* bending stiffness in kT units */
+  double diameter;
+  double min_bond_length;     /* bonds: floor(length/(1.5*min_bond_length)) */
+  double friction_ratio;      /* gamma_perp / gamma_par */
+} sc_filament_params;
+
+typedef struct {
+  int64_t i_step;             /* steps (i_steps) taken */
+  int64_t n_rebuilds;         /* pair-list rebuilds since sc_add_filaments */
+  int64_t n_pairs;            /* current candidate pairs */
+  int64_t pair_capacity;
+  int64_t n_filaments, n_sites, n_bonds;
+  int32_t n_cells_1d;
+  double cell_length;
+  double dr_update;           /* rebuild threshold 0.25 * cell_length^2 */
+  int64_t kernel_launches;    /* kernels launched by this context */
+} sc_counters;
+
+typedef struct sc_ctx sc_ctx;
+
+/* Context life cycle.  sc_create = Simulation::InitSimulation's space and
+ * interaction set-up (src/simulation.cpp:139-173). */
+sc_status sc_create(const sc_system_desc *desc, sc_ctx **out);
+sc_status sc_destroy(sc_ctx *ctx);
+const char *sc_last_error(const sc_ctx *ctx);
+
+/* Loads all filaments at once (FilamentSpecies with its members in place,
+ * src/simulation.cpp:261-405 minus the random insertion): n filaments with
+ * their parameters and site positions (n_sites_total x 3 doubles, each
+ * filament's sites tail to head).  Builds the initial pair list as the
+ * forced update that ends the reference's insertion does. */
+sc_status sc_add_filaments(sc_ctx *ctx, int n, const sc_filament_params *p,
+                           const double *site_xyz, int64_t n_sites_total);
+
+/* Number of bonds the reference gives a filament (src/filament.cpp:142-147). */
+int sc_filament_n_bonds(const sc_filament_params *p);
+
+/* InteractionManager::Interact for the next step: rebuild check, pair
+ * forces and torques into the device bond accumulators. */
+sc_status sc_interact(sc_ctx *ctx);
+/* FilamentSpecies::UpdatePositions: one integrator (half) step of every
+ * filament from the bond accumulators; toggles the midstep flag. */
+sc_status sc_update_positions(sc_ctx *ctx);
+/* n full reference steps (Simulation::RunSimulation bodies), pair and
+ * integrator stages fused.  Bit-identical to n x (sc_interact +
+ * sc_update_positions). */
+sc_status sc_step(sc_ctx *ctx, int n);
+/* Same as sc_step, replaying a captured CUDA graph of n steps. */
+sc_status sc_step_graph(sc_ctx *ctx, int n);
+/* Waits for the context's stream and reports any deferred device error. */
+sc_status sc_synchronize(sc_ctx *ctx);
+
+/* Host copies of state (caller-sized arrays). */
+sc_status sc_get_sites(sc_ctx *ctx, double *xyz);            /* N_s x 3 */
+sc_status sc_set_sites(sc_ctx *ctx, const double *xyz);      /* N_s x 3 */
+sc_status sc_get_prev_sites(sc_ctx *ctx, double *xyz);       /* N_s x 3 */
+sc_status sc_get_random_forces(sc_ctx *ctx, double *f);      /* N_s x 3 */
+sc_status sc_get_bond_forces(sc_ctx *ctx, double *f, double *t); /* N_b x 3 */
+sc_status sc_get_bond_geometry(sc_ctx *ctx, double *pos, double *spos,
+                               double *u, double *len);
+/* Site forces and tensions of the last integrator step; recorded only while
+ * capture is on (sc_set_capture(ctx, 1)), since they are not state. */
+sc_status sc_set_capture(sc_ctx *ctx, int on);
+sc_status sc_get_site_forces(sc_ctx *ctx, double *f);        /* N_s x 3 */
+sc_status sc_get_tensions(sc_ctx *ctx, double *t);           /* N_b */
+sc_status sc_get_filament_state(sc_ctx *ctx, int *normalize_switch,
+                                int *n_normalize);           /* N_f each */
+sc_status sc_get_dr_tot(sc_ctx *ctx, double *dr);            /* N_s */
+/* Current pair list as (obj1, obj2) global bond ids, in the reference's
+ * list order; *n_pairs receives the count, at most cap pairs written. */
+sc_status sc_get_pairs(sc_ctx *ctx, int32_t *pairs, int64_t cap,
+                       int64_t *n_pairs);
+/* Cell (x, y, z) of every bond from its current scaled position
+ * (CellList::FindCellCoords, src/cell_list.cpp:139-157). */
+sc_status sc_get_bond_cells(sc_ctx *ctx, int32_t *xyz);
+sc_status sc_get_counters(sc_ctx *ctx, sc_counters *out);
+/* The cudaStream_t all work of the context is issued on. */
+void *sc_get_stream(sc_ctx *ctx);
+
+/* Seeded random insertion with overlap rejection on the host (the
+ * distributions of Mesh::InitRandomBond and Filament::InsertFilament,
+ * src/mesh.cpp:244-258, src/filament.cpp:225-249,350-383, rejection of
+ * InteractionManager::CheckOverlap, src/interaction_manager.cpp:561-571).
+ * Writes sum(n_bonds[i] + 1) x 3 doubles. */
+int sc_insert_filaments(int n_dim, double system_radius, uint64_t seed,
+                        int n_fil, const int *n_bonds, const double *length,
+                        const double *persistence_length, double diameter,
+                        int max_attempts, double *site_xyz);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

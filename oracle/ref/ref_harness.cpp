@@ -1,0 +1,596 @@
+// ORACLE / TEST INFRASTRUCTURE ONLY -- built into oracle/_ref/libscref.so
+// together with the reference's own, unmodified hot-path sources (object,
+// site, bond, mesh, filament, cell, cell_list, minimum_distance,
+// linear_algebra, rng, space, logger, cpu_time), compiled where they lie.
+//
+// The reference's InteractionManager, FilamentSpecies and Simulation sources
+// cannot be compiled here (they pull in yaml-cpp, the unvendored KMC
+// submodule and FFTW), so this file restates just the parts of them that the
+// Brownian-dynamics step runs, with the reference's own classes doing all the
+// arithmetic:
+//   - Simulation::RunSimulation step body      src/simulation.cpp:37-62
+//   - InteractionManager::InitInteractions     src/interaction_manager.cpp:37-56
+//   - InteractionManager::Interact             src/interaction_manager.cpp:63-95
+//   - CheckUpdateObjects / CheckUpdateInteractions / GetDrMax / ZeroDrTot
+//                                              src/interaction_manager.cpp:262-321
+//   - UpdateInteractions / UpdatePairInteractions
+//                                              src/interaction_manager.cpp:211-231
+//   - ProcessPairInteraction                   src/interaction_manager.cpp:323-397
+//   - CalculatePairInteractions (OpenMP chunks, culling)
+//                                              src/interaction_manager.cpp:448-498
+//   - ApplyPairInteractions                    src/interaction_manager.cpp:500-517
+//   - FilamentSpecies::UpdatePositions         src/filament_species.cpp:59-85
+//   - Species::GetDrMax / ZeroDrTot / ZeroForces  include/simcore/species.hpp:105-127,198-203
+//   - Simulation::InsertSpecies tail           src/simulation.cpp:399-404
+// Insertion itself is replaced by loading a given configuration into each
+// filament (Mesh::GetSite(i)->SetPosition, then UpdateBondPositions and
+// UpdatePrevPositions, src/mesh.cpp:24,324,175), after which every Philox
+// stream is rewound so that dynamics starts at draw 0 in every code.
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+// White-box access to the reference's private per-filament solver state
+// (tensions_, ...) and to CellList's static configuration, in this
+// translation unit only.  Layout is unaffected.
+#define private public
+#define protected public
+#include "simcore/cell_list.hpp"
+#include "simcore/filament.hpp"
+#include "simcore/minimum_distance.hpp"
+#include "simcore/potential_manager.hpp"
+#include "simcore/space.hpp"
+#undef private
+#undef protected
+
+bool early_exit = false;  // defined by the reference in simulation_manager.cpp
+
+extern "C" void scshim_set_global_seed(uint32_t seed);
+extern "C" void scshim_rewind_all(void);
+
+extern "C" {
+typedef struct {
+  int n_dim;              // 2 or 3; every dimension periodic
+  double system_radius;   // R, the cube (square) has side 2R
+  double delta;
+  double wca_eps;
+  double wca_sig;
+  double f_cutoff;
+  int stoch_flag;
+  int interaction_flag;
+  int like_like_interactions;
+  unsigned int seed;      // Philox key word 0 for every filament stream
+  int n_threads;          // OpenMP threads, 0 = library default
+} scref_system;
+
+typedef struct {
+  double length;
+  double persistence_length;
+  double diameter;
+  double min_bond_length;
+  double friction_ratio;
+} scref_filament;
+}
+
+namespace {
+
+struct RefSim {
+  system_parameters params;
+  Space space;
+  space_struct *sp = nullptr;
+  std::vector<filament_parameters> fparams;
+  std::vector<Filament> members;
+  bool midstep = true;  // FilamentSpecies::midstep_ (filament_species.hpp:9)
+
+  CellList clist;
+  PotentialManager potentials;
+  MinimumDistance mindist;
+  std::vector<Interaction> pair_interactions;
+  std::vector<Object *> interactors;
+  double dr_update = 0;
+  int i_update = 0;
+  int n_objs = -1;
+  long n_rebuilds = 0;
+  int i_step = 0;
+  bool overlap = false;
+  double stress[9] = {0};
+  std::unordered_map<const Object *, int> bond_gid;
+  int n_threads = 0;
+  int n_sites_total = 0;
+  int n_bonds_total = 0;
+
+  // ---- restated Species<Filament> helpers (species.hpp) -------------------
+  double GetDrMax() {  // species.hpp:105-120 and interaction_manager.cpp:299-312
+    double max_dr = 0;
+    for (auto &f : members) {
+      double dr = f.GetDrTot();
+      if (dr > max_dr) max_dr = dr;
+    }
+    if (max_dr > 10000) throw std::runtime_error("Unphysical result");
+    return max_dr;
+  }
+  void ZeroDrTot() {
+    for (auto &f : members) f.ZeroDrTot();
+  }
+  void ZeroForces() {
+    for (auto &f : members) f.ZeroForce();
+  }
+  int CountSpecies() {
+    int c = 0;
+    for (auto &f : members) c += f.GetCount();
+    return c;
+  }
+  bool CheckSpeciesInteractorUpdate() {  // species.hpp:556-563
+    bool result = false;
+    for (auto &f : members)
+      if (f.CheckInteractorUpdate()) result = true;
+    return result;
+  }
+
+  // ---- restated InteractionManager pieces ---------------------------------
+  void UpdateInteractors() {
+    interactors.clear();
+    for (auto &f : members) f.GetInteractors(interactors);
+  }
+  void UpdatePairInteractions() {
+    if (!params.interaction_flag) return;
+    pair_interactions.clear();
+    clist.RenewObjectsCells(interactors);
+    clist.MakePairs(pair_interactions);
+  }
+  void UpdateInteractions() {
+    i_update = 0;
+    n_rebuilds++;
+    UpdatePairInteractions();
+    ZeroDrTot();
+  }
+  void ForceUpdate() {
+    UpdateInteractors();
+    UpdateInteractions();
+  }
+  void CheckUpdateObjects() {
+    if (params.static_particle_number) return;
+    bool ix_update = CheckSpeciesInteractorUpdate();
+    int obj_count = CountSpecies();
+    if (obj_count != n_objs || ix_update) {
+      n_objs = obj_count;
+      ForceUpdate();
+    }
+  }
+  void CheckUpdateInteractions() {
+    double dr_max = GetDrMax();
+    if (dr_max > dr_update) UpdateInteractions();
+  }
+  void ProcessPairInteraction(Interaction *ix) {
+    Object *obj1 = ix->obj1;
+    Object *obj2 = ix->obj2;
+    if (obj1->GetOID() == obj2->GetOID()) {
+      fprintf(stderr, "scref: self interaction\n");
+      exit(1);
+    }
+    if (!params.like_like_interactions && obj1->GetSID() == obj2->GetSID()) {
+      ix->no_interaction = true;
+      return;
+    }
+    if (obj1->GetMeshID() > 0 && obj1->GetMeshID() == obj2->GetMeshID()) {
+      if (obj1->HasNeighbor(obj2->GetOID())) {
+        ix->no_interaction = true;
+        return;
+      }
+    }
+    mindist.ObjectObject(*ix);
+    if (ix->dr_mag2 < 0.25 * SQR(obj1->GetDiameter() + obj2->GetDiameter()))
+      overlap = true;
+    if (ix->dr_mag2 > potentials.GetRCut2()) return;
+    potentials.CalcPotential(*ix);
+  }
+  void CalculatePairInteractions() {
+#ifdef _OPENMP
+    int max_threads = omp_get_max_threads();
+    typedef std::vector<Interaction>::iterator it_t;
+    std::vector<std::pair<it_t, it_t>> chunks;
+    chunks.reserve(max_threads);
+    size_t chunk_size = pair_interactions.size() / max_threads;
+    auto cur = pair_interactions.begin();
+    for (int i = 0; i < max_threads - 1; ++i) {
+      auto last = cur;
+      std::advance(cur, chunk_size);
+      chunks.push_back(std::make_pair(last, cur));
+    }
+    chunks.push_back(std::make_pair(cur, pair_interactions.end()));
+#pragma omp parallel for
+    for (int i = 0; i < max_threads; ++i) {
+      for (auto ix = chunks[i].first; ix != chunks[i].second; ++ix) {
+        ProcessPairInteraction(&*ix);
+        cross_product(ix->contact1, ix->force, ix->t1, 3);
+        cross_product(ix->contact2, ix->force, ix->t2, 3);
+      }
+    }
+#else
+    for (auto ix = pair_interactions.begin(); ix != pair_interactions.end();
+         ++ix) {
+      ProcessPairInteraction(&*ix);
+      cross_product(ix->contact1, ix->force, ix->t1, 3);
+      cross_product(ix->contact2, ix->force, ix->t2, 3);
+    }
+#endif
+    if (i_update == 0) {
+      pair_interactions.erase(
+          std::remove_if(pair_interactions.begin(), pair_interactions.end(),
+                         [](Interaction x) { return x.no_interaction; }),
+          pair_interactions.end());
+    }
+  }
+  void ApplyPairInteractions() {
+    int n_dim = params.n_dim;
+    for (auto ix = pair_interactions.begin(); ix != pair_interactions.end();
+         ++ix) {
+      Object *obj1 = ix->obj1;
+      Object *obj2 = ix->obj2;
+      obj1->AddForce(ix->force);
+      obj2->SubForce(ix->force);
+      obj1->AddTorque(ix->t1);
+      obj2->SubTorque(ix->t2);
+      obj1->AddPotential(ix->pote);
+      obj2->AddPotential(ix->pote);
+      for (int i = 0; i < n_dim; ++i)
+        for (int j = 0; j < n_dim; ++j)
+          stress[n_dim * i + j] += ix->stress[n_dim * i + j];
+    }
+  }
+  void Interact() {
+    if (!params.interaction_flag) return;  // no interactions, no boundaries
+    CheckUpdateObjects();
+    CheckUpdateInteractions();
+    CalculatePairInteractions();
+    ApplyPairInteractions();
+    i_update++;
+  }
+  // FilamentSpecies::UpdatePositions (filament_species.cpp:59-85)
+  void UpdatePositions() {
+#ifdef _OPENMP
+    int max_threads = omp_get_max_threads();
+    typedef std::vector<Filament>::iterator it_t;
+    std::vector<std::pair<it_t, it_t>> chunks;
+    chunks.reserve(max_threads);
+    size_t chunk_size = members.size() / max_threads;
+    auto cur = members.begin();
+    for (int i = 0; i < max_threads - 1; ++i) {
+      auto last = cur;
+      std::advance(cur, chunk_size);
+      chunks.push_back(std::make_pair(last, cur));
+    }
+    chunks.push_back(std::make_pair(cur, members.end()));
+    bool ms = midstep;
+#pragma omp parallel for
+    for (int i = 0; i < max_threads; ++i)
+      for (auto it = chunks[i].first; it != chunks[i].second; ++it)
+        it->UpdatePosition(ms);
+#else
+    for (auto &f : members) f.UpdatePosition(midstep);
+#endif
+    midstep = !midstep;
+  }
+  void Step() {  // simulation.cpp:37-62 (outputs, graphics and thermo off)
+    ++i_step;
+    params.i_step = i_step;
+    ZeroForces();
+    Interact();
+    UpdatePositions();
+  }
+};
+
+RefSim *g_active = nullptr;  // the reference keeps static state: one at a time
+
+}  // namespace
+
+extern "C" {
+
+void *scref_create(const scref_system *sys, int n_fil,
+                   const scref_filament *fils, const double *site_xyz,
+                   int n_sites_given) {
+  if (g_active) return nullptr;
+  if (!sys || n_fil <= 0 || !fils || !site_xyz) return nullptr;
+  RefSim *s = new RefSim();
+  s->n_threads = sys->n_threads;
+#ifdef _OPENMP
+  if (sys->n_threads > 0) omp_set_num_threads(sys->n_threads);
+#endif
+  system_parameters &p = s->params;
+  p.n_dim = sys->n_dim;
+  p.n_periodic = sys->n_dim;
+  p.boundary = 0;
+  p.system_radius = sys->system_radius;
+  p.delta = sys->delta;
+  p.wca_eps = sys->wca_eps;
+  p.wca_sig = sys->wca_sig;
+  p.f_cutoff = sys->f_cutoff;
+  p.stoch_flag = sys->stoch_flag != 0;
+  p.interaction_flag = sys->interaction_flag != 0;
+  p.like_like_interactions = sys->like_like_interactions != 0;
+  p.potential = "wca";
+  p.n_steps = 1 << 30;
+
+  // Simulation::InitSimulation: space, static object parameters.
+  s->space.Init(&p);
+  s->sp = s->space.GetStruct();
+  Object::SetParams(&p);
+  Object::SetSpace(s->sp);
+  Object::SetNDim(p.n_dim);
+  Object::SetDelta(p.delta);
+
+  // Fresh static cell-list configuration for this run.
+  CellList::_min_cell_length_ = -1;
+  CellList::_n_dim_ = -1;
+  CellList::_n_periodic_ = -1;
+
+  // Species parameters, one struct per filament (per-filament persistence
+  // lengths need their own filament_parameters).
+  s->fparams.resize(n_fil);
+  for (int i = 0; i < n_fil; ++i) {
+    filament_parameters &fp = s->fparams[i];
+    fp.num = n_fil;
+    fp.length = fils[i].length;
+    fp.persistence_length = fils[i].persistence_length;
+    fp.diameter = fils[i].diameter;
+    fp.min_bond_length = fils[i].min_bond_length;
+    fp.friction_ratio = fils[i].friction_ratio;
+    fp.insertion_type = "random";
+  }
+  // Simulation::InitSpecies: spec length = 1.5*min_bond_length vs diameter.
+  {
+    double spec_length = 1.5 * fils[0].min_bond_length;
+    double spec_d = fils[0].diameter;
+    spec_length = (spec_d > spec_length ? spec_d : spec_length);
+    CellList::SetMinCellLength(spec_length);
+  }
+  // InteractionManager::InitInteractions (no crosslinks: rcutoff 0).
+  CellList::SetMinCellLength(0.0);
+  s->potentials.InitPotentials(&p);
+  CellList::SetMinCellLength(sqrt(s->potentials.GetRCut2()));
+  CellList::Init(p.n_dim, p.n_periodic, p.system_radius);
+  s->clist.BuildCellList();
+  s->dr_update = 0.25 * CellList::GetCellLength() * CellList::GetCellLength();
+  MinimumDistance::Init(s->sp, 2 * s->dr_update);
+
+  // Members: filament i is seeded with i, so its Philox key is (seed, i).
+  scshim_set_global_seed(sys->seed);
+  s->members.reserve(n_fil);
+  int site_cursor = 0;
+  for (int i = 0; i < n_fil; ++i) {
+    s->members.emplace_back((unsigned long)i);
+    Filament &f = s->members.back();
+    f.SetSID(species_id::filament);
+    f.Init(&s->fparams[i]);
+    int ns = f.n_sites_;
+    if (site_cursor + ns > n_sites_given) {
+      delete s;
+      return nullptr;
+    }
+    for (int j = 0; j < ns; ++j) {
+      double r[3] = {0, 0, 0};
+      for (int d = 0; d < p.n_dim; ++d) r[d] = site_xyz[3 * (site_cursor + j) + d];
+      f.GetSite(j)->SetPosition(r);
+    }
+    f.UpdateBondPositions();
+    f.UpdatePrevPositions();
+    f.CalculateAngles();
+    site_cursor += ns;
+  }
+  if (site_cursor != n_sites_given) {
+    delete s;
+    return nullptr;
+  }
+  s->n_sites_total = site_cursor;
+
+  // Simulation::InsertSpecies tail: half-shell neighbours, then a forced
+  // update that bins every bond and zeroes the displacement trackers.
+  s->clist.ResetNeighbors();
+  s->pair_interactions.clear();
+  s->interactors.clear();
+  s->clist.ClearCellObjects();
+  if (p.interaction_flag) s->CheckUpdateObjects();
+  s->n_rebuilds = 0;  // count rebuilds triggered during dynamics only
+
+  int gid = 0;
+  for (auto &f : s->members)
+    for (int b = 0; b < f.n_bonds_; ++b) s->bond_gid[f.GetBond(b)] = gid++;
+  s->n_bonds_total = gid;
+
+  scshim_rewind_all();
+  g_active = s;
+  return s;
+}
+
+void scref_destroy(void *h) {
+  RefSim *s = (RefSim *)h;
+  if (!s) return;
+  s->clist.Clear();
+  delete s;
+  if (g_active == s) g_active = nullptr;
+}
+
+int scref_n_sites(void *h) { return ((RefSim *)h)->n_sites_total; }
+int scref_n_bonds(void *h) { return ((RefSim *)h)->n_bonds_total; }
+int scref_n_cells_1d(void *) { return CellList::_n_cells_1d_; }
+double scref_cell_length(void *) { return CellList::_cell_length_; }
+double scref_dr_update(void *h) { return ((RefSim *)h)->dr_update; }
+long scref_n_rebuilds(void *h) { return ((RefSim *)h)->n_rebuilds; }
+int scref_i_step(void *h) { return ((RefSim *)h)->i_step; }
+
+// Runs n reference steps (i_steps); returns the wall time of the loop in s,
+// or -1 if the reference raised its "Unphysical result" error.
+double scref_step(void *h, int n) {
+  RefSim *s = (RefSim *)h;
+  auto t0 = std::chrono::steady_clock::now();
+  try {
+    for (int i = 0; i < n; ++i) s->Step();
+  } catch (const std::runtime_error &) {
+    return -1.0;
+  }
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void scref_get_sites(void *h, double *xyz) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int j = 0; j < f.n_sites_; ++j, ++c) {
+      const double *r = f.GetSite(j)->GetPosition();
+      for (int d = 0; d < 3; ++d) xyz[3 * c + d] = r[d];
+    }
+}
+
+void scref_get_prev_sites(void *h, double *xyz) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int j = 0; j < f.n_sites_; ++j, ++c) {
+      const double *r = f.GetSite(j)->GetPrevPosition();
+      for (int d = 0; d < 3; ++d) xyz[3 * c + d] = r[d];
+    }
+}
+
+void scref_get_site_forces(void *h, double *fo) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int j = 0; j < f.n_sites_; ++j, ++c) {
+      const double *v = f.GetSite(j)->GetForce();
+      for (int d = 0; d < 3; ++d) fo[3 * c + d] = v[d];
+    }
+}
+
+void scref_get_random_forces(void *h, double *fo) {
+  RefSim *s = (RefSim *)h;
+  int n_dim = s->params.n_dim;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int j = 0; j < f.n_sites_; ++j, ++c) {
+      const double *v = f.GetSite(j)->GetRandomForce();
+      for (int d = 0; d < 3; ++d) fo[3 * c + d] = d < n_dim ? v[d] : 0.0;
+    }
+}
+
+void scref_get_bond_ft(void *h, double *fo, double *to) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int b = 0; b < f.n_bonds_; ++b, ++c) {
+      const double *v = f.GetBond(b)->GetForce();
+      const double *t = f.GetBond(b)->GetTorque();
+      for (int d = 0; d < 3; ++d) {
+        fo[3 * c + d] = v[d];
+        to[3 * c + d] = t[d];
+      }
+    }
+}
+
+void scref_get_tensions(void *h, double *tens) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int b = 0; b < f.n_bonds_; ++b, ++c) tens[c] = f.tensions_[b];
+}
+
+void scref_get_bond_geom(void *h, double *pos, double *spos, double *u,
+                         double *len) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int b = 0; b < f.n_bonds_; ++b, ++c) {
+      Bond *bd = f.GetBond(b);
+      for (int d = 0; d < 3; ++d) {
+        pos[3 * c + d] = bd->GetPosition()[d];
+        spos[3 * c + d] = bd->GetScaledPosition()[d];
+        u[3 * c + d] = bd->GetOrientation()[d];
+      }
+      len[c] = bd->GetLength();
+    }
+}
+
+void scref_get_filament_state(void *h, int *normalize_switch,
+                              int *n_normalize) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members) {
+    normalize_switch[c] = f.normalize_switch_ ? 1 : 0;
+    n_normalize[c] = f.n_normalize_;
+    ++c;
+  }
+}
+
+void scref_get_frictions(void *h, double *gpar, double *gperp, double *spar,
+                         double *sperp) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members) {
+    gpar[c] = f.friction_par_;
+    gperp[c] = f.friction_perp_;
+    spar[c] = f.rand_sigma_par_;
+    sperp[c] = f.rand_sigma_perp_;
+    ++c;
+  }
+}
+
+// Current pair list (after the culling that follows a rebuild) as pairs of
+// global bond indices in list order.  Returns the number of pairs; writes at
+// most cap of them.
+long scref_get_pairs(void *h, int *out, long cap) {
+  RefSim *s = (RefSim *)h;
+  long n = (long)s->pair_interactions.size();
+  for (long i = 0; i < n && i < cap; ++i) {
+    out[2 * i] = s->bond_gid[s->pair_interactions[i].obj1];
+    out[2 * i + 1] = s->bond_gid[s->pair_interactions[i].obj2];
+  }
+  return n;
+}
+
+// Cell coordinates (x, y, z) that CellList::FindCellCoords gives each bond
+// from its current scaled position.
+void scref_get_bond_cells(void *h, int *xyz) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int b = 0; b < f.n_bonds_; ++b, ++c) {
+      int x, y, z;
+      std::tie(x, y, z) = s->clist.FindCellCoords(*f.GetBond(b));
+      xyz[3 * c] = x;
+      xyz[3 * c + 1] = y;
+      xyz[3 * c + 2] = z;
+    }
+}
+
+// Per-site accumulated squared displacement since the last rebuild.
+void scref_get_dr_tot(void *h, double *dr) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members)
+    for (int j = 0; j < f.n_sites_; ++j, ++c) dr[c] = f.GetSite(j)->dr_tot_;
+}
+
+}  // extern "C"

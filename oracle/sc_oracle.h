@@ -1,0 +1,94 @@
+/* ORACLE / TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement, in plain C, of simcore's Brownian-dynamics step for
+ * semiflexible filaments (cell list, segment-segment WCA pair forces with
+ * the reference's stale-force and stale-list behaviour, bond-to-site force
+ * conversion, bending and metric forces, the two Thomas solves, the
+ * midpoint position update and bond renormalisation).  Only tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg may load it, and
+ * only as the checker.  It is pinned bit for bit against the reference's own
+ * code (oracle/_ref, built by oracle/ref/Makefile) through the fixtures in
+ * tests/golden/.
+ *
+ * Every array is site-, bond- or pair-major with 3 doubles per vector (z = 0
+ * in 2D), filaments stored back to back in the order they were given. */
+#ifndef SC_ORACLE_H
+#define SC_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int n_dim;              /* 2 or 3, every dimension periodic */
+  double system_radius;   /* R: cube (square) of side 2R */
+  double delta;
+  double wca_eps;
+  double wca_sig;
+  double f_cutoff;
+  int stoch_flag;
+  int interaction_flag;
+  int like_like_interactions;
+  unsigned int seed;      /* Philox key word 0 */
+  int n_threads;          /* unused: the oracle is single threaded */
+} sco_system;
+
+typedef struct {
+  double length;
+  double persistence_length;
+  double diameter;
+  double min_bond_length;
+  double friction_ratio;
+} sco_filament;
+
+typedef struct sco_sim sco_sim;
+
+/* Number of bonds the reference gives a filament (src/filament.cpp:142-147). */
+int sco_filament_n_bonds(const sco_filament *f);
+
+sco_sim *sco_create(const sco_system *sys, int n_fil, const sco_filament *fils,
+                    const double *site_xyz, int n_sites);
+void sco_destroy(sco_sim *s);
+int sco_n_sites(const sco_sim *s);
+int sco_n_bonds(const sco_sim *s);
+int sco_n_cells_1d(const sco_sim *s);
+double sco_cell_length(const sco_sim *s);
+double sco_dr_update(const sco_sim *s);
+long sco_n_rebuilds(const sco_sim *s);
+int sco_i_step(const sco_sim *s);
+
+/* Runs n steps (i_steps).  Returns 0, or -1 when the reference would throw
+ * "Unphysical result" (accumulated displacement above 10000). */
+int sco_step(sco_sim *s, int n);
+
+void sco_get_sites(const sco_sim *s, double *xyz);
+void sco_get_prev_sites(const sco_sim *s, double *xyz);
+void sco_get_site_forces(const sco_sim *s, double *f);
+void sco_get_random_forces(const sco_sim *s, double *f);
+void sco_get_bond_ft(const sco_sim *s, double *f, double *t);
+void sco_get_tensions(const sco_sim *s, double *t);
+void sco_get_bond_geom(const sco_sim *s, double *pos, double *spos, double *u,
+                       double *len);
+void sco_get_filament_state(const sco_sim *s, int *normalize_switch,
+                            int *n_normalize);
+void sco_get_frictions(const sco_sim *s, double *gpar, double *gperp,
+                       double *spar, double *sperp);
+long sco_get_pairs(const sco_sim *s, int *out, long cap);
+void sco_get_bond_cells(const sco_sim *s, int *xyz);
+void sco_get_dr_tot(const sco_sim *s, double *dr);
+
+/* Overwrite all site positions (and previous positions) with xyz, rebuild
+ * bond geometry, as when a configuration is loaded. */
+void sco_set_sites(sco_sim *s, const double *xyz);
+
+/* Pair forces alone, evaluated from the current bond geometry on the
+ * current pair list with fresh (zero) stale forces: bond forces/torques are
+ * written to f and t.  Used to check single force evaluations. */
+void sco_pair_forces(sco_sim *s, double *f, double *t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,210 @@
+"""ctypes bindings of the CPU checkers (test infrastructure).
+
+Two libraries with one interface:
+  Oracle    -- oracle/libscoracle.so, the plain-C restatement of the path;
+  Reference -- oracle/_ref/libscref.so, the reference's own hot-path sources
+               driven by a harness (built only where the reference tree is
+               present; absent otherwise).
+Both take the same system/filament descriptors and site positions and expose
+the same getters, so a test can run either, or both, on one configuration.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "libscoracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libscref.so")
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [("n_dim", ctypes.c_int), ("system_radius", ctypes.c_double),
+                ("delta", ctypes.c_double), ("wca_eps", ctypes.c_double),
+                ("wca_sig", ctypes.c_double), ("f_cutoff", ctypes.c_double),
+                ("stoch_flag", ctypes.c_int), ("interaction_flag", ctypes.c_int),
+                ("like_like_interactions", ctypes.c_int), ("seed", ctypes.c_uint),
+                ("n_threads", ctypes.c_int)]
+
+
+class FilamentDesc(ctypes.Structure):
+    _fields_ = [("length", ctypes.c_double), ("persistence_length", ctypes.c_double),
+                ("diameter", ctypes.c_double), ("min_bond_length", ctypes.c_double),
+                ("friction_ratio", ctypes.c_double)]
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class _Checker:
+    prefix = None
+    so = None
+
+    def __init__(self, system, filaments, sites, n_threads=1):
+        self.lib = ctypes.CDLL(self.so)
+        p = self.prefix
+        L = self.lib
+        getattr(L, p + "create").restype = ctypes.c_void_p
+        getattr(L, p + "create").argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_int]
+        for name in ("n_sites", "n_bonds", "n_cells_1d", "i_step"):
+            getattr(L, p + name).restype = ctypes.c_int
+            getattr(L, p + name).argtypes = [ctypes.c_void_p]
+        for name in ("cell_length", "dr_update"):
+            getattr(L, p + name).restype = ctypes.c_double
+            getattr(L, p + name).argtypes = [ctypes.c_void_p]
+        getattr(L, p + "n_rebuilds").restype = ctypes.c_long
+        getattr(L, p + "n_rebuilds").argtypes = [ctypes.c_void_p]
+        getattr(L, p + "get_pairs").restype = ctypes.c_long
+        getattr(L, p + "get_pairs").argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long]
+        getattr(L, p + "destroy").argtypes = [ctypes.c_void_p]
+        sysd = SystemDesc(**{k: system[k] for k, _ in SystemDesc._fields_ if k != "n_threads"},
+                          n_threads=n_threads)
+        fils = (FilamentDesc * len(filaments))(*[FilamentDesc(**f) for f in filaments])
+        sites = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        self.h = getattr(L, p + "create")(ctypes.byref(sysd), len(filaments), fils,
+                                          _ptr(sites), sites.shape[0])
+        if not self.h:
+            raise RuntimeError("%screate failed" % p)
+        self.n_sites = getattr(L, p + "n_sites")(self.h)
+        self.n_bonds = getattr(L, p + "n_bonds")(self.h)
+        self.n_fil = len(filaments)
+
+    def _call(self, name, *args):
+        return getattr(self.lib, self.prefix + name)(ctypes.c_void_p(self.h), *args)
+
+    def close(self):
+        if self.h:
+            self._call("destroy")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_cells_1d(self):
+        return self._call("n_cells_1d")
+
+    @property
+    def cell_length(self):
+        return self._call("cell_length")
+
+    @property
+    def dr_update(self):
+        return self._call("dr_update")
+
+    @property
+    def n_rebuilds(self):
+        return self._call("n_rebuilds")
+
+    @property
+    def i_step(self):
+        return self._call("i_step")
+
+    def sites(self):
+        a = np.zeros((self.n_sites, 3))
+        self._call("get_sites", _ptr(a))
+        return a
+
+    def prev_sites(self):
+        a = np.zeros((self.n_sites, 3))
+        self._call("get_prev_sites", _ptr(a))
+        return a
+
+    def site_forces(self):
+        a = np.zeros((self.n_sites, 3))
+        self._call("get_site_forces", _ptr(a))
+        return a
+
+    def random_forces(self):
+        a = np.zeros((self.n_sites, 3))
+        self._call("get_random_forces", _ptr(a))
+        return a
+
+    def bond_forces(self):
+        f = np.zeros((self.n_bonds, 3))
+        t = np.zeros((self.n_bonds, 3))
+        self._call("get_bond_ft", _ptr(f), _ptr(t))
+        return f, t
+
+    def tensions(self):
+        a = np.zeros(self.n_bonds)
+        self._call("get_tensions", _ptr(a))
+        return a
+
+    def bond_geometry(self):
+        pos = np.zeros((self.n_bonds, 3))
+        spos = np.zeros((self.n_bonds, 3))
+        u = np.zeros((self.n_bonds, 3))
+        ln = np.zeros(self.n_bonds)
+        self._call("get_bond_geom", _ptr(pos), _ptr(spos), _ptr(u), _ptr(ln))
+        return pos, spos, u, ln
+
+    def filament_state(self):
+        sw = np.zeros(self.n_fil, dtype=np.int32)
+        nn = np.zeros(self.n_fil, dtype=np.int32)
+        self._call("get_filament_state", _ptr(sw), _ptr(nn))
+        return sw, nn
+
+    def pairs(self):
+        n = self._call("get_pairs", None, ctypes.c_long(0))
+        out = np.zeros((max(n, 1), 2), dtype=np.int32)
+        self._call("get_pairs", _ptr(out), ctypes.c_long(n))
+        return out[:n]
+
+    def bond_cells(self):
+        a = np.zeros((self.n_bonds, 3), dtype=np.int32)
+        self._call("get_bond_cells", _ptr(a))
+        return a
+
+    def dr_tot(self):
+        a = np.zeros(self.n_sites)
+        self._call("get_dr_tot", _ptr(a))
+        return a
+
+
+class Oracle(_Checker):
+    """The plain-C restatement (always available once built)."""
+    prefix = "sco_"
+    so = ORACLE_SO
+
+    def step(self, n=1):
+        self.lib.sco_step.restype = ctypes.c_int
+        rc = self._call("step", ctypes.c_int(n))
+        if rc != 0:
+            raise RuntimeError("oracle step failed (unphysical displacement)")
+
+    def set_sites(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self._call("set_sites", _ptr(xyz))
+
+    def frictions(self):
+        out = [np.zeros(self.n_fil) for _ in range(4)]
+        self._call("get_frictions", *[_ptr(a) for a in out])
+        return out
+
+
+class Reference(_Checker):
+    """The reference's own code (oracle/_ref), where it was built."""
+    prefix = "scref_"
+    so = REF_SO
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_SO)
+
+    def step(self, n=1):
+        self.lib.scref_step.restype = ctypes.c_double
+        t = self._call("step", ctypes.c_int(n))
+        if t < 0:
+            raise RuntimeError("reference step failed (unphysical displacement)")
+        return t
+
+    def frictions(self):
+        out = [np.zeros(self.n_fil) for _ in range(4)]
+        self._call("get_frictions", *[_ptr(a) for a in out])
+        return out
