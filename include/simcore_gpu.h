@@ -140,6 +140,10 @@ sc_status sc_get_site_forces(sc_ctx *ctx, double *f);        /* N_s x 3 */
 sc_status sc_get_tensions(sc_ctx *ctx, double *t);           /* N_b */
 sc_status sc_get_filament_state(sc_ctx *ctx, int *normalize_switch,
                                 int *n_normalize);           /* N_f each */
+/* Accumulated squared displacement per site since the last rebuild
+ * (Object::dr_tot_).  The GPU adds a full step's contribution in that step
+ * itself; the reference adds it at the following step's rebuild check, so
+ * the two agree after every odd number of steps. */
 sc_status sc_get_dr_tot(sc_ctx *ctx, double *dr);            /* N_s */
 /* Current pair list as (obj1, obj2) global bond ids, in the reference's
  * list order; *n_pairs receives the count, at most cap pairs written. */

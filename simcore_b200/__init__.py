@@ -1,0 +1,243 @@
+"""simcore_b200: B200 Brownian-dynamics step for semiflexible filaments.
+
+Python binding of the C ABI in include/simcore_gpu.h (libsimcore_b200.so,
+built in-tree by simcore_b200/build.py).  The library is required: importing
+this package on a machine where it was not built raises, and every compute
+call runs the CUDA kernels -- there is no CPU fallback.
+
+    ctx = Context(system, filaments, sites, precision="fp64")
+    ctx.step(2)              # two reference steps (one midpoint BD step)
+    xyz = ctx.sites()
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsimcore_b200.so")
+
+SC_OK = 0
+STATUS_NAMES = {0: "SC_OK", 1: "SC_ERR_INVALID_ARG", 2: "SC_ERR_OOM", 3: "SC_ERR_NAN",
+                4: "SC_ERR_LIST_OVERFLOW", 5: "SC_ERR_TIMEOUT", 6: "SC_ERR_CUDA",
+                7: "SC_ERR_UNPHYSICAL", 8: "SC_ERR_INSERTION", 9: "SC_ERR_NO_DEVICE"}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+# Every symbol include/simcore_gpu.h declares.
+EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
+            "sc_filament_n_bonds", "sc_interact", "sc_update_positions", "sc_step",
+            "sc_step_graph", "sc_synchronize", "sc_get_sites", "sc_set_sites",
+            "sc_get_prev_sites", "sc_get_random_forces", "sc_get_bond_forces",
+            "sc_get_bond_geometry", "sc_set_capture", "sc_get_site_forces",
+            "sc_get_tensions", "sc_get_filament_state", "sc_get_dr_tot", "sc_get_pairs",
+            "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_insert_filaments"]
+
+
+class ScError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (STATUS_NAMES.get(code, code), msg))
+        self.code = code
+
+
+class SystemDesc(ctypes.Structure):
+    _fields_ = [("n_dim", ctypes.c_int), ("system_radius", ctypes.c_double),
+                ("delta", ctypes.c_double), ("wca_eps", ctypes.c_double),
+                ("wca_sig", ctypes.c_double), ("f_cutoff", ctypes.c_double),
+                ("stoch_flag", ctypes.c_int), ("interaction_flag", ctypes.c_int),
+                ("like_like_interactions", ctypes.c_int), ("seed", ctypes.c_uint32),
+                ("precision", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class FilamentParams(ctypes.Structure):
+    _fields_ = [("length", ctypes.c_double), ("persistence_length", ctypes.c_double),
+                ("diameter", ctypes.c_double), ("min_bond_length", ctypes.c_double),
+                ("friction_ratio", ctypes.c_double)]
+
+
+class Counters(ctypes.Structure):
+    _fields_ = [("i_step", ctypes.c_int64), ("n_rebuilds", ctypes.c_int64),
+                ("n_pairs", ctypes.c_int64), ("pair_capacity", ctypes.c_int64),
+                ("n_filaments", ctypes.c_int64), ("n_sites", ctypes.c_int64),
+                ("n_bonds", ctypes.c_int64), ("n_cells_1d", ctypes.c_int32),
+                ("cell_length", ctypes.c_double), ("dr_update", ctypes.c_double),
+                ("kernel_launches", ctypes.c_int64)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("simcore_b200: %s is not built (run simcore_b200/build.py); "
+                          "there is no CPU fallback" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    lib.sc_last_error.restype = ctypes.c_char_p
+    lib.sc_last_error.argtypes = [vp]
+    lib.sc_get_stream.restype = vp
+    lib.sc_get_stream.argtypes = [vp]
+    for name in EXPORTED:
+        fn = getattr(lib, name)
+        if name not in ("sc_last_error", "sc_get_stream"):
+            fn.restype = ctypes.c_int
+    return lib
+
+
+lib = _load()
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def filament_n_bonds(params):
+    fp = FilamentParams(**params)
+    return lib.sc_filament_n_bonds(ctypes.byref(fp))
+
+
+def insert_filaments(n_dim, system_radius, seed, n_bonds, lengths, persistence_lengths,
+                     diameter=1.0, max_attempts=10000):
+    """Seeded random insertion with overlap rejection (host).  Returns sites."""
+    n_bonds = np.ascontiguousarray(n_bonds, dtype=np.int32)
+    lengths = np.ascontiguousarray(lengths, dtype=np.float64)
+    lps = np.ascontiguousarray(persistence_lengths, dtype=np.float64)
+    xyz = np.zeros((int(np.sum(n_bonds + 1)), 3))
+    rc = lib.sc_insert_filaments(ctypes.c_int(n_dim), ctypes.c_double(system_radius),
+                                 ctypes.c_uint64(seed), ctypes.c_int(len(n_bonds)),
+                                 _p(n_bonds), _p(lengths), _p(lps), ctypes.c_double(diameter),
+                                 ctypes.c_int(max_attempts), _p(xyz))
+    if rc != SC_OK:
+        raise ScError(rc, "random insertion failed")
+    return xyz
+
+
+class Context:
+    """One simulated system on one GPU (an sc_ctx)."""
+
+    def __init__(self, system, filaments, sites, precision="fp64", device=0):
+        desc = SystemDesc(n_dim=system["n_dim"], system_radius=system["system_radius"],
+                          delta=system["delta"], wca_eps=system.get("wca_eps", 1.0),
+                          wca_sig=system.get("wca_sig", 1.0),
+                          f_cutoff=system.get("f_cutoff", 2000.0),
+                          stoch_flag=system.get("stoch_flag", 1),
+                          interaction_flag=system.get("interaction_flag", 1),
+                          like_like_interactions=system.get("like_like_interactions", 1),
+                          seed=system.get("seed", 0), precision=PRECISION[precision],
+                          device=device)
+        h = ctypes.c_void_p()
+        rc = lib.sc_create(ctypes.byref(desc), ctypes.byref(h))
+        if rc != SC_OK:
+            raise ScError(rc, "sc_create failed")
+        self.h = h
+        self.n_dim = system["n_dim"]
+        fils = (FilamentParams * len(filaments))(*[FilamentParams(**f) for f in filaments])
+        sites = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
+        self._check(lib.sc_add_filaments(h, ctypes.c_int(len(filaments)), fils, _p(sites),
+                                         ctypes.c_int64(sites.shape[0])))
+        c = self.counters()
+        self.n_sites, self.n_bonds, self.n_fil = c.n_sites, c.n_bonds, c.n_filaments
+
+    def _check(self, rc):
+        if rc != SC_OK:
+            msg = lib.sc_last_error(self.h)
+            raise ScError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.sc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # stepping
+    def step(self, n=1):
+        self._check(lib.sc_step(self.h, ctypes.c_int(n)))
+
+    def step_graph(self, n=1):
+        self._check(lib.sc_step_graph(self.h, ctypes.c_int(n)))
+
+    def interact(self):
+        self._check(lib.sc_interact(self.h))
+
+    def update_positions(self):
+        self._check(lib.sc_update_positions(self.h))
+
+    def synchronize(self):
+        self._check(lib.sc_synchronize(self.h))
+
+    def set_capture(self, on=True):
+        self._check(lib.sc_set_capture(self.h, ctypes.c_int(1 if on else 0)))
+
+    @property
+    def stream(self):
+        return lib.sc_get_stream(self.h)
+
+    # state
+    def _vec(self, fn, n):
+        a = np.zeros((n, 3))
+        self._check(fn(self.h, _p(a)))
+        return a
+
+    def sites(self):
+        return self._vec(lib.sc_get_sites, self.n_sites)
+
+    def set_sites(self, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        self._check(lib.sc_set_sites(self.h, _p(xyz)))
+
+    def prev_sites(self):
+        return self._vec(lib.sc_get_prev_sites, self.n_sites)
+
+    def random_forces(self):
+        return self._vec(lib.sc_get_random_forces, self.n_sites)
+
+    def site_forces(self):
+        return self._vec(lib.sc_get_site_forces, self.n_sites)
+
+    def bond_forces(self):
+        f = np.zeros((self.n_bonds, 3))
+        t = np.zeros((self.n_bonds, 3))
+        self._check(lib.sc_get_bond_forces(self.h, _p(f), _p(t)))
+        return f, t
+
+    def bond_geometry(self):
+        pos = np.zeros((self.n_bonds, 3))
+        spos = np.zeros((self.n_bonds, 3))
+        u = np.zeros((self.n_bonds, 3))
+        ln = np.zeros(self.n_bonds)
+        self._check(lib.sc_get_bond_geometry(self.h, _p(pos), _p(spos), _p(u), _p(ln)))
+        return pos, spos, u, ln
+
+    def tensions(self):
+        a = np.zeros(self.n_bonds)
+        self._check(lib.sc_get_tensions(self.h, _p(a)))
+        return a
+
+    def filament_state(self):
+        sw = np.zeros(self.n_fil, dtype=np.int32)
+        nn = np.zeros(self.n_fil, dtype=np.int32)
+        self._check(lib.sc_get_filament_state(self.h, _p(sw), _p(nn)))
+        return sw, nn
+
+    def dr_tot(self):
+        a = np.zeros(self.n_sites)
+        self._check(lib.sc_get_dr_tot(self.h, _p(a)))
+        return a
+
+    def pairs(self):
+        n = ctypes.c_int64()
+        self._check(lib.sc_get_pairs(self.h, None, ctypes.c_int64(0), ctypes.byref(n)))
+        out = np.zeros((max(n.value, 1), 2), dtype=np.int32)
+        self._check(lib.sc_get_pairs(self.h, _p(out), ctypes.c_int64(n.value), ctypes.byref(n)))
+        return out[:n.value]
+
+    def bond_cells(self):
+        a = np.zeros((self.n_bonds, 3), dtype=np.int32)
+        self._check(lib.sc_get_bond_cells(self.h, _p(a)))
+        return a
+
+    def counters(self):
+        c = Counters()
+        self._check(lib.sc_get_counters(self.h, ctypes.byref(c)))
+        return c

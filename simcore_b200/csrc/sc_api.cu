@@ -1,0 +1,760 @@
+// C ABI of the B200 filament step (include/simcore_gpu.h): context,
+// device memory, rebuild orchestration and the step loop.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "sc_common.cuh"
+#include "sc_kernels.h"
+#include "simcore_gpu.h"
+
+using sc::DevState;
+using sc::SysConst;
+
+struct sc_ctx {
+  sc_system_desc desc{};
+  int nd = 3;
+  int prec = 0;
+  SysConst k{};
+  DevState d{};
+  cudaStream_t st = nullptr;
+  std::string err;
+  std::vector<void *> allocs;  // every device allocation, freed at destroy
+
+  // host mirrors
+  int nf = 0, ns = 0, nb = 0;
+  std::vector<int> site_off;
+  std::vector<int> bond_fil;
+  bool loaded = false;
+
+  // cell list and pair list storage
+  int *key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
+  int *sorted = nullptr, *pair_count = nullptr, *pair_off = nullptr;
+  int *deg = nullptr, *scan_tmp = nullptr, *cells_xyz = nullptr;
+  long long np = 0, pcap = 0;
+
+  // integrator blocks
+  int nblocks = 0, C = 128;
+
+  // control state
+  long long i_step = 0, n_rebuilds = 0, launches = 0;
+  int midstep = 1;                 // FilamentSpecies::midstep_
+  unsigned long long mcount = 0;   // midsteps that drew noise
+  int rbuf = 0;                    // geometry buffer read by the next pair stage
+  int capture = 0;
+  bool bond_ft_valid = false;      // bF/bT hold the last step's bond forces
+  int bond_ft_src = -1;            // geometry buffer to recompute them from
+
+  // pinned readback slots
+  struct Readback {
+    unsigned long long dr_bits;
+    unsigned status;
+    int total;
+  } *hb = nullptr;
+
+  // CUDA graph of n fused steps (sc_step_graph)
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_n = 0;
+};
+
+namespace {
+
+sc_status fail(sc_ctx *c, sc_status code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                          \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess)                                                \
+      return fail(c, SC_ERR_CUDA, "%s: %s (%s:%d)", #call,                \
+                  cudaGetErrorString(e_), __FILE__, __LINE__);            \
+  } while (0)
+
+#define CKS(expr)                     \
+  do {                                \
+    sc_status s_ = (expr);            \
+    if (s_ != SC_OK) return s_;       \
+  } while (0)
+
+template <class T>
+sc_status dalloc(sc_ctx *c, T **p, size_t n) {
+  void *q = nullptr;
+  size_t bytes = sizeof(T) * (n ? n : 1);
+  cudaError_t e = cudaMalloc(&q, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, SC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", bytes,
+                cudaGetErrorString(e));
+  }
+  c->allocs.push_back(q);
+  *p = (T *)q;
+  return SC_OK;
+}
+
+void dfree(sc_ctx *c, void *p) {
+  if (!p) return;
+  auto it = std::find(c->allocs.begin(), c->allocs.end(), p);
+  if (it != c->allocs.end()) c->allocs.erase(it);
+  cudaFree(p);
+}
+
+// The reference's symmetric 2x2 / 3x3 inverses (src/linear_algebra.cpp:40-64),
+// so that h^-1 has the same bits as the reference's unit_cell_inv.
+void invert_sym_2d(const double *a, double *b) {
+  double inv_det = a[0] * a[3] - a[1] * a[1];
+  inv_det = 1.0 / inv_det;
+  b[0] = a[3] * inv_det;
+  b[3] = a[0] * inv_det;
+  b[2] = b[1] = -a[1] * inv_det;
+}
+
+void invert_sym_3d(const double *a, double *b) {
+  double inv_det = a[0] * (a[4] * a[8] - a[5] * a[7]) -
+                   a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                   a[2] * (a[3] * a[7] - a[4] * a[6]);
+  inv_det = 1.0 / inv_det;
+  b[0] = inv_det * (a[4] * a[8] - a[5] * a[7]);
+  b[4] = inv_det * (a[0] * a[8] - a[2] * a[6]);
+  b[8] = inv_det * (a[0] * a[4] - a[1] * a[3]);
+  b[1] = b[3] = -inv_det * (a[3] * a[8] - a[5] * a[6]);
+  b[2] = b[6] = inv_det * (a[3] * a[7] - a[4] * a[6]);
+  b[5] = b[7] = -inv_det * (a[0] * a[7] - a[1] * a[6]);
+}
+
+// Filament::InitFilamentLength for static lengths (src/filament.cpp:104-147).
+void filament_length(const sc_filament_params &p, double *length, int *n_bonds) {
+  double max_bond_length = 1.5 * p.min_bond_length;
+  double min_length = 5, max_length = 500, L = p.length;
+  if (min_length < 2 * p.min_bond_length) min_length = 2 * p.min_bond_length;
+  if (max_length < min_length) max_length = min_length;
+  if (L > max_length) L = max_length;
+  else if (L < min_length) L = min_length;
+  int nb = (int)std::floor(L / max_bond_length);
+  nb = (nb == 1 ? 2 : nb);
+  *length = L;
+  *n_bonds = nb;
+}
+
+sc_status check_status(sc_ctx *c) {
+  unsigned s = c->hb->status;
+  if (s & sc::ST_NAN) return fail(c, SC_ERR_NAN, "non-finite position or displacement");
+  if (s & sc::ST_BAD_CELL) return fail(c, SC_ERR_NAN, "bond outside the cell grid (non-finite position)");
+  if (s & sc::ST_LIST_OVERFLOW) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow");
+  return SC_OK;
+}
+
+// Reads status and the displacement maximum written by earlier kernels.
+sc_status readback(sc_ctx *c) {
+  CK(cudaMemcpyAsync(&c->hb->dr_bits, c->d.dr_max_bits, sizeof(unsigned long long),
+                     cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned),
+                     cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return check_status(c);
+}
+
+sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
+  if (need <= c->pcap) return SC_OK;
+  long long cap = std::max<long long>(need + need / 2, 1024);
+  if (cap > (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list of %lld pairs too large", need);
+  dfree(c, c->d.pa);
+  dfree(c, c->d.pb);
+  dfree(c, c->d.pf64);
+  dfree(c, c->d.pf32);
+  dfree(c, c->d.e_ent);
+  c->d.pa = c->d.pb = c->d.e_ent = nullptr;
+  c->d.pf64 = nullptr;
+  c->d.pf32 = nullptr;
+  CKS(dalloc(c, &c->d.pa, cap));
+  CKS(dalloc(c, &c->d.pb, cap));
+  if (c->prec == 0) CKS(dalloc(c, &c->d.pf64, 3 * cap));
+  else CKS(dalloc(c, &c->d.pf32, 3 * cap));
+  CKS(dalloc(c, &c->d.e_ent, 2 * cap));
+  c->pcap = cap;
+  c->graph_n = 0;  // device pointers changed: recapture
+  if (c->graph_exec) {
+    cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+  }
+  return SC_OK;
+}
+
+// InteractionManager::UpdateInteractions (src/interaction_manager.cpp:211-231):
+// bin every bond, emit the half-shell pair list in the reference's order,
+// build the per-bond pair index, zero the displacement trackers.
+sc_status rebuild(sc_ctx *c) {
+  const SysConst &k = c->k;
+  if (c->desc.interaction_flag) {
+    c->launches += sc::launch_bin_count(k, c->d, c->key, c->cell_count, c->st);
+    c->launches += sc::launch_exclusive_scan(c->cell_count, c->cell_start, k.n_cells,
+                                             c->scan_tmp, c->st);
+    c->launches += sc::launch_bin_scatter(c->nb, c->key, c->cell_start, c->cell_count,
+                                          c->sorted, c->st);
+    c->launches += sc::launch_cell_sort_count(k, c->d, c->key, c->sorted, c->cell_start,
+                                              c->pair_count, c->st);
+    c->launches += sc::launch_exclusive_scan(c->pair_count, c->pair_off, c->nb,
+                                             c->scan_tmp, c->st);
+    CK(cudaMemcpyAsync(&c->hb->total, c->pair_off + c->nb, sizeof(int),
+                       cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    long long np = c->hb->total;
+    CKS(ensure_pair_capacity(c, np));
+    c->launches += sc::launch_pair_emit(k, c->d, c->key, c->sorted, c->cell_start,
+                                        c->pair_off, (int)c->pcap, c->deg, c->prec,
+                                        c->st);
+    c->launches += sc::launch_exclusive_scan(c->deg, c->d.e_off, c->nb, c->scan_tmp,
+                                             c->st);
+    c->launches += sc::launch_csr(c->d, (int)np, c->deg, c->st);
+    c->np = np;
+  }
+  c->launches += sc::launch_zero_dr(c->d, c->st);
+  CK(cudaGetLastError());
+  return SC_OK;
+}
+
+// Interact's rebuild check (CheckUpdateInteractions + GetDrMax,
+// src/interaction_manager.cpp:284-312, include/simcore/species.hpp:105-120).
+// Only a query after a full step can see a grown displacement, so the device
+// maximum is read back only then.
+sc_status maybe_rebuild(sc_ctx *c) {
+  if (!c->desc.interaction_flag) return SC_OK;
+  if (!c->midstep) return SC_OK;  // previous update was a midstep: unchanged
+  if (c->i_step <= 1) return SC_OK;
+  CKS(readback(c));
+  double dr_max;
+  std::memcpy(&dr_max, &c->hb->dr_bits, sizeof(double));
+  if (dr_max > 10000) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result: dr_max %g", dr_max);
+  if (dr_max > c->k.dr_update) {
+    CKS(rebuild(c));
+    c->n_rebuilds++;
+  }
+  return SC_OK;
+}
+
+sc_status step_once(sc_ctx *c, bool fused) {
+  c->i_step++;
+  CKS(maybe_rebuild(c));
+  const int interaction = c->desc.interaction_flag ? 1 : 0;
+  if (!fused && interaction) {
+    c->launches += sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, c->st);
+  }
+  c->launches += sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep,
+                                      c->mcount, c->rbuf, interaction, c->capture,
+                                      c->prec, fused, c->st);
+  CK(cudaGetLastError());
+  c->bond_ft_valid = !fused;
+  c->bond_ft_src = c->rbuf;
+  if (c->midstep && c->desc.stoch_flag) c->mcount++;
+  c->midstep = !c->midstep;
+  c->rbuf = 1 - c->rbuf;
+  return SC_OK;
+}
+
+template <class T>
+sc_status copy_soa3(sc_ctx *c, T *const *src, int n, double *xyz) {
+  std::vector<double> tmp(3 * (size_t)n);
+  for (int i = 0; i < 3; ++i)
+    CK(cudaMemcpyAsync(tmp.data() + (size_t)i * n, src[i], sizeof(double) * n,
+                       cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < 3; ++i) xyz[3 * (size_t)j + i] = tmp[(size_t)i * n + j];
+  return SC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sc_filament_n_bonds(const sc_filament_params *p) {
+  if (!p) return -1;
+  double L;
+  int nb;
+  filament_length(*p, &L, &nb);
+  return nb;
+}
+
+sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
+  if (!desc || !out) return SC_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (desc->n_dim != 2 && desc->n_dim != 3) return SC_ERR_INVALID_ARG;
+  if (!(desc->system_radius > 0) || !(desc->delta > 0) || !(desc->wca_sig > 0))
+    return SC_ERR_INVALID_ARG;
+  if (desc->precision != SC_PREC_FP64 && desc->precision != SC_PREC_MIXED)
+    return SC_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return SC_ERR_NO_DEVICE;
+  }
+  if (desc->device < 0 || desc->device >= ndev) return SC_ERR_INVALID_ARG;
+  sc_ctx *c = new sc_ctx();
+  c->desc = *desc;
+  c->nd = desc->n_dim;
+  c->prec = desc->precision;
+  if (cudaSetDevice(desc->device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaHostAlloc((void **)&c->hb, sizeof(sc_ctx::Readback), cudaHostAllocDefault) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return SC_ERR_CUDA;
+  }
+  SysConst &k = c->k;
+  std::memset(&k, 0, sizeof(k));
+  k.n_dim = c->nd;
+  // Space::InitUnitCell / CalculateUnitCellQuantities (src/space.cpp:85-138)
+  const double hh = 2.0 * desc->system_radius;
+  for (int a = 0; a < c->nd; ++a)
+    for (int b = 0; b < c->nd; ++b) k.h[a * c->nd + b] = (a == b ? 1 : 0) * hh;
+  k.h[c->nd * c->nd - 1] = hh;
+  if (c->nd == 2) invert_sym_2d(k.h, k.hinv);
+  else invert_sym_3d(k.h, k.hinv);
+  for (int i = 0; i < 9; ++i) k.hf[i] = (float)k.h[i];
+  k.delta = desc->delta;
+  // WCAPotential::Init (include/simcore/wca_potential.hpp:34-48)
+  double rcut = std::pow(2.0, 1.0 / 6.0) * desc->wca_sig;
+  k.rcut2 = rcut * rcut;
+  k.c12 = 4.0 * desc->wca_eps * std::pow(desc->wca_sig, 12.0);
+  k.c6 = 4.0 * desc->wca_eps * std::pow(desc->wca_sig, 6.0);
+  k.fcut = desc->f_cutoff;
+  k.rcut2f = (float)k.rcut2;
+  k.c12f = (float)k.c12;
+  k.c6f = (float)k.c6;
+  k.fcutf = (float)k.fcut;
+  k.seed = desc->seed;
+  k.stoch = desc->stoch_flag ? 1 : 0;
+  k.like_like = desc->like_like_interactions ? 1 : 0;
+  CK(cudaMalloc((void **)&c->d.status, sizeof(unsigned)));
+  c->allocs.push_back(c->d.status);
+  CK(cudaMalloc((void **)&c->d.dr_max_bits, sizeof(unsigned long long)));
+  c->allocs.push_back(c->d.dr_max_bits);
+  CK(cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->st));
+  CK(cudaMemsetAsync(c->d.dr_max_bits, 0, sizeof(unsigned long long), c->st));
+  *out = c;
+  return SC_OK;
+}
+
+sc_status sc_destroy(sc_ctx *c) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  cudaSetDevice(c->desc.device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  for (void *p : c->allocs) cudaFree(p);
+  if (c->hb) cudaFreeHost(c->hb);
+  if (c->st) cudaStreamDestroy(c->st);
+  cudaGetLastError();
+  delete c;
+  return SC_OK;
+}
+
+const char *sc_last_error(const sc_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
+                           const double *site_xyz, int64_t n_sites_total) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  if (c->loaded) return fail(c, SC_ERR_INVALID_ARG, "filaments already added");
+  if (n <= 0 || !p || !site_xyz) return fail(c, SC_ERR_INVALID_ARG, "bad filament arrays");
+  CK(cudaSetDevice(c->desc.device));
+  const double mbl = p[0].min_bond_length, dia = p[0].diameter;
+  std::vector<double> len(n);
+  std::vector<int> nbf(n);
+  long long ns = 0;
+  int max_ns = 0;
+  for (int f = 0; f < n; ++f) {
+    if (!(p[f].length > 0) || !(p[f].diameter > 0) || !(p[f].min_bond_length > 0) ||
+        !(p[f].friction_ratio > 0) || p[f].persistence_length < 0)
+      return fail(c, SC_ERR_INVALID_ARG, "filament %d: bad parameters", f);
+    if (p[f].min_bond_length != mbl || p[f].diameter != dia)
+      return fail(c, SC_ERR_INVALID_ARG,
+                  "filament %d: min_bond_length and diameter are species-wide", f);
+    filament_length(p[f], &len[f], &nbf[f]);
+    ns += nbf[f] + 1;
+    max_ns = std::max(max_ns, nbf[f] + 1);
+  }
+  if (ns != n_sites_total)
+    return fail(c, SC_ERR_INVALID_ARG, "n_sites_total %lld != %lld implied by the lengths",
+                (long long)n_sites_total, ns);
+  if (max_ns > 256)
+    return fail(c, SC_ERR_INVALID_ARG, "filaments longer than 255 bonds are not supported");
+  if (ns > (1ll << 30)) return fail(c, SC_ERR_INVALID_ARG, "too many sites");
+  const int nsi = (int)ns, nbi = nsi - n;
+  c->nf = n;
+  c->ns = nsi;
+  c->nb = nbi;
+  c->C = max_ns <= 128 ? 128 : 256;
+
+  // Per-filament constants: Filament::SetParameters / InitFilamentLength /
+  // SetDiffusion (src/filament.cpp:6-84, 104-170, 320-348).
+  std::vector<int> site_off(n + 1, 0);
+  std::vector<double> fl(n), flinv(n), fk(n), gpar(n), gperp(n), spar(n), sperp(n);
+  for (int f = 0; f < n; ++f) {
+    site_off[f + 1] = site_off[f] + nbf[f] + 1;
+    const int nsf = nbf[f] + 1;
+    fl[f] = len[f] / nbf[f];
+    flinv[f] = 1.0 / fl[f];
+    fk[f] = p[f].persistence_length;
+    double logLD = std::log(len[f] / p[f].diameter);
+    gperp[f] = 4.0 * len[f] / (3.0 * nsf * logLD);
+    gpar[f] = gperp[f] / p[f].friction_ratio;
+    sperp[f] = std::sqrt(24.0 * gperp[f] / c->desc.delta);
+    spar[f] = std::sqrt(24.0 * gpar[f] / c->desc.delta);
+  }
+  c->site_off = site_off;
+  std::vector<int> site_fil(nsi), bond_fil(nbi);
+  for (int f = 0; f < n; ++f) {
+    for (int s = site_off[f]; s < site_off[f + 1]; ++s) site_fil[s] = f;
+    for (int b = site_off[f] - f; b < site_off[f + 1] - f - 1; ++b) bond_fil[b] = f;
+  }
+  c->bond_fil = bond_fil;
+  // Integrator blocks: greedy runs of whole filaments up to C sites.
+  std::vector<int> blk_site0, blk_f0, blk_nf;
+  {
+    int f = 0;
+    while (f < n) {
+      int s0 = site_off[f], f0 = f;
+      while (f < n && site_off[f + 1] - s0 <= c->C) ++f;
+      blk_site0.push_back(s0);
+      blk_f0.push_back(f0);
+      blk_nf.push_back(f - f0);
+    }
+    blk_site0.push_back(nsi);
+  }
+  c->nblocks = (int)blk_f0.size();
+
+  DevState &d = c->d;
+  d.nf = n;
+  d.ns = nsi;
+  d.nb = nbi;
+  auto up = [&](auto **dst, const auto &vec) -> sc_status {
+    using T = typename std::remove_reference<decltype(vec)>::type::value_type;
+    T *q = nullptr;
+    CKS(dalloc(c, &q, vec.size()));
+    CK(cudaMemcpyAsync(q, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice,
+                       c->st));
+    *dst = q;
+    return SC_OK;
+  };
+  int *tmp_i = nullptr;
+  double *tmp_d = nullptr;
+  CKS(up(&tmp_i, site_off)); d.f_site_off = tmp_i;
+  CKS(up(&tmp_d, fl)); d.f_l = tmp_d;
+  CKS(up(&tmp_d, flinv)); d.f_linv = tmp_d;
+  CKS(up(&tmp_d, fk)); d.f_kappa = tmp_d;
+  CKS(up(&tmp_d, gpar)); d.f_gpar = tmp_d;
+  CKS(up(&tmp_d, gperp)); d.f_gperp = tmp_d;
+  CKS(up(&tmp_d, spar)); d.f_spar = tmp_d;
+  CKS(up(&tmp_d, sperp)); d.f_sperp = tmp_d;
+  std::vector<int> sw(n, 1), nn(n, 0);
+  CKS(up(&d.f_switch, sw));
+  CKS(up(&d.f_nnorm, nn));
+  CKS(up(&tmp_i, site_fil)); d.site_fil = tmp_i;
+  CKS(up(&tmp_i, bond_fil)); d.bond_fil = tmp_i;
+  CKS(up(&tmp_i, blk_site0)); d.blk_site0 = tmp_i;
+  CKS(up(&tmp_i, blk_f0)); d.blk_f0 = tmp_i;
+  CKS(up(&tmp_i, blk_nf)); d.blk_nf = tmp_i;
+
+  // Sites: positions (z = 0 in 2D); previous positions = positions as after
+  // Mesh::UpdatePrevPositions; no stored noise yet.
+  std::vector<double> comp(nsi);
+  for (int i = 0; i < 3; ++i) {
+    for (int s = 0; s < nsi; ++s) comp[s] = i < c->nd ? site_xyz[3 * (size_t)s + i] : 0.0;
+    CKS(up(&d.r[i], comp));
+    CKS(up(&d.rp[i], comp));
+    CKS(dalloc(c, &d.fr[i], nsi));
+    CK(cudaMemsetAsync(d.fr[i], 0, sizeof(double) * nsi, c->st));
+    CKS(dalloc(c, &d.dz[i], nsi));
+    CKS(dalloc(c, &d.cap_F[i], nsi));
+    CK(cudaMemsetAsync(d.cap_F[i], 0, sizeof(double) * nsi, c->st));
+    CKS(dalloc(c, &d.bF[i], nbi));
+    CKS(dalloc(c, &d.bT[i], nbi));
+    CK(cudaMemsetAsync(d.bF[i], 0, sizeof(double) * nbi, c->st));
+    CK(cudaMemsetAsync(d.bT[i], 0, sizeof(double) * nbi, c->st));
+  }
+  CKS(dalloc(c, &d.dt, nsi));
+  CKS(dalloc(c, &d.cap_T, nbi));
+  CK(cudaMemsetAsync(d.cap_T, 0, sizeof(double) * nbi, c->st));
+  for (int b = 0; b < 2; ++b) {
+    CKS(dalloc(c, &d.g64[b], nbi));
+    CKS(dalloc(c, &d.g32[b], nbi));
+  }
+
+  // Cell list: SetMinCellLength calls of Simulation::InitSpecies
+  // (src/simulation.cpp:248-251) and InteractionManager::InitInteractions
+  // (src/interaction_manager.cpp:46-48), CellList::Init (src/cell_list.cpp:17-64).
+  SysConst &k = c->k;
+  {
+    double min_len = -1, spec_length = 1.5 * mbl;
+    if (dia > spec_length) spec_length = dia;
+    if (spec_length > min_len) min_len = spec_length;
+    if (0.0 > min_len) min_len = 0.0;
+    if (std::sqrt(k.rcut2) > min_len) min_len = std::sqrt(k.rcut2);
+    int n1d = (int)std::floor(2 * c->desc.system_radius / min_len);
+    if (n1d <= 3) n1d = 3;
+    long long ncell = (long long)n1d * n1d * (c->nd == 3 ? n1d : 1);
+    if (ncell > (1ll << 30))
+      return fail(c, SC_ERR_INVALID_ARG, "cell grid of %lld cells too large", ncell);
+    k.n1d = n1d;
+    k.third = c->nd == 3 ? n1d : 1;
+    k.n_cells = (int)ncell;
+    double cl = (double)2 * c->desc.system_radius / n1d;
+    k.dr_update = 0.25 * cl * cl;
+  }
+  CKS(dalloc(c, &c->key, nbi));
+  CKS(dalloc(c, &c->cell_count, k.n_cells));
+  CK(cudaMemsetAsync(c->cell_count, 0, sizeof(int) * k.n_cells, c->st));
+  CKS(dalloc(c, &c->cell_start, (size_t)k.n_cells + 1));
+  CKS(dalloc(c, &c->sorted, nbi));
+  CKS(dalloc(c, &c->pair_count, nbi));
+  CKS(dalloc(c, &c->pair_off, (size_t)nbi + 1));
+  CKS(dalloc(c, &c->deg, nbi));
+  CK(cudaMemsetAsync(c->deg, 0, sizeof(int) * nbi, c->st));
+  CKS(dalloc(c, &d.e_off, (size_t)nbi + 1));
+  CK(cudaMemsetAsync(d.e_off, 0, sizeof(int) * ((size_t)nbi + 1), c->st));
+  CKS(dalloc(c, &c->scan_tmp,
+             (size_t)std::max(sc::scan_temp_ints(k.n_cells), sc::scan_temp_ints(nbi))));
+  CKS(dalloc(c, &c->cells_xyz, 3 * (size_t)nbi));
+  CKS(ensure_pair_capacity(c, std::max<long long>(4ll * nbi, 1024)));
+
+  sc::prepare_integrate(c->C);
+  sc::launch_init_geometry(c->k, d, 0, c->prec, c->st);
+  if (c->prec != 0) sc::launch_init_geometry(c->k, d, 0, 0, c->st);
+  c->rbuf = 0;
+  // Simulation::InsertSpecies tail: forced update (rebuild + ZeroDrTot).
+  CKS(rebuild(c));
+  CK(cudaStreamSynchronize(c->st));
+  c->loaded = true;
+  c->i_step = 0;
+  c->n_rebuilds = 0;
+  c->midstep = 1;
+  c->mcount = 0;
+  return SC_OK;
+}
+
+sc_status sc_interact(sc_ctx *c) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  // ZeroForces + Interact of the next step.
+  c->i_step++;
+  CKS(maybe_rebuild(c));
+  if (c->desc.interaction_flag) {
+    c->launches += sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, c->st);
+  } else {
+    for (int i = 0; i < 3; ++i) {
+      CK(cudaMemsetAsync(c->d.bF[i], 0, sizeof(double) * c->nb, c->st));
+      CK(cudaMemsetAsync(c->d.bT[i], 0, sizeof(double) * c->nb, c->st));
+    }
+  }
+  CK(cudaGetLastError());
+  c->bond_ft_valid = true;
+  c->bond_ft_src = c->rbuf;
+  return SC_OK;
+}
+
+sc_status sc_update_positions(sc_ctx *c) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  if (!c->bond_ft_valid) return fail(c, SC_ERR_INVALID_ARG, "sc_update_positions needs sc_interact first");
+  c->launches += sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep,
+                                      c->mcount, c->rbuf, 1, c->capture, c->prec,
+                                      false, c->st);
+  CK(cudaGetLastError());
+  if (c->midstep && c->desc.stoch_flag) c->mcount++;
+  c->midstep = !c->midstep;
+  c->rbuf = 1 - c->rbuf;
+  c->bond_ft_valid = false;  // consumed; bF/bT still hold them for getters
+  c->bond_ft_src = -2;
+  return SC_OK;
+}
+
+sc_status sc_step(sc_ctx *c, int n) {
+  if (!c || !c->loaded || n < 0) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  for (int i = 0; i < n; ++i) CKS(step_once(c, true));
+  return SC_OK;
+}
+
+sc_status sc_step_graph(sc_ctx *c, int n) {
+  // Graph replay is added with device-side rebuild decisions; until then the
+  // fused step loop is the same computation.
+  return sc_step(c, n);
+}
+
+sc_status sc_synchronize(sc_ctx *c) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  CKS(readback(c));
+  return SC_OK;
+}
+
+sc_status sc_get_sites(sc_ctx *c, double *xyz) {
+  if (!c || !c->loaded || !xyz) return SC_ERR_INVALID_ARG;
+  return copy_soa3(c, c->d.r, c->ns, xyz);
+}
+
+sc_status sc_get_prev_sites(sc_ctx *c, double *xyz) {
+  if (!c || !c->loaded || !xyz) return SC_ERR_INVALID_ARG;
+  return copy_soa3(c, c->d.rp, c->ns, xyz);
+}
+
+sc_status sc_get_random_forces(sc_ctx *c, double *f) {
+  if (!c || !c->loaded || !f) return SC_ERR_INVALID_ARG;
+  return copy_soa3(c, c->d.fr, c->ns, f);
+}
+
+sc_status sc_set_sites(sc_ctx *c, const double *xyz) {
+  if (!c || !c->loaded || !xyz) return SC_ERR_INVALID_ARG;
+  std::vector<double> tmp(3 * (size_t)c->ns);
+  for (int s = 0; s < c->ns; ++s)
+    for (int i = 0; i < 3; ++i)
+      tmp[(size_t)i * c->ns + s] = i < c->nd ? xyz[3 * (size_t)s + i] : 0.0;
+  for (int i = 0; i < 3; ++i) {
+    CK(cudaMemcpyAsync(c->d.r[i], tmp.data() + (size_t)i * c->ns, sizeof(double) * c->ns,
+                       cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d.rp[i], tmp.data() + (size_t)i * c->ns, sizeof(double) * c->ns,
+                       cudaMemcpyHostToDevice, c->st));
+  }
+  sc::launch_init_geometry(c->k, c->d, c->rbuf, c->prec, c->st);
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
+  if (!c || !c->loaded || !f || !t) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  if (c->bond_ft_src >= 0 && !c->bond_ft_valid && c->desc.interaction_flag) {
+    // The fused step kept no bond accumulators: re-evaluate them from the
+    // geometry that step read (still intact in the other buffer) and the
+    // pair forces it left; this reproduces its sums exactly.
+    c->launches += sc::launch_pairs(c->k, c->d, c->bond_ft_src, c->prec, c->st);
+    CK(cudaGetLastError());
+  }
+  CKS(copy_soa3(c, c->d.bF, c->nb, f));
+  return copy_soa3(c, c->d.bT, c->nb, t);
+}
+
+sc_status sc_get_bond_geometry(sc_ctx *c, double *pos, double *spos, double *u,
+                               double *len) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  // FP64 geometry of the current positions (buffer 0 of the FP64 records is
+  // scratch in mixed precision; in FP64 the read buffer already holds it).
+  int buf = c->prec == 0 ? c->rbuf : 0;
+  if (c->prec != 0) sc::launch_init_geometry(c->k, c->d, 0, 0, c->st);
+  std::vector<sc::BondGeomF64> g(c->nb);
+  CK(cudaMemcpyAsync(g.data(), c->d.g64[buf], sizeof(sc::BondGeomF64) * c->nb,
+                     cudaMemcpyDeviceToHost, c->st));
+  std::vector<double> r(3 * (size_t)c->ns);
+  CK(cudaStreamSynchronize(c->st));
+  CKS(copy_soa3(c, c->d.r, c->ns, r.data()));
+  for (int b = 0; b < c->nb; ++b) {
+    const int f = c->bond_fil[b];
+    const double *r1 = &r[3 * (size_t)(b + f)];
+    if (pos) {
+      double o[3] = {0, 0, 0};
+      for (int i = 0; i < c->nd; ++i) o[i] = r1[3 + i] - r1[i];
+      for (int i = 0; i < 3; ++i) pos[3 * (size_t)b + i] = i < c->nd ? r1[i] + 0.5 * o[i] : 0.0;
+    }
+    for (int i = 0; i < 3; ++i) {
+      if (spos) spos[3 * (size_t)b + i] = g[b].s[i];
+      if (u) u[3 * (size_t)b + i] = g[b].u[i];
+    }
+    if (len) len[b] = g[b].len;
+  }
+  return SC_OK;
+}
+
+sc_status sc_set_capture(sc_ctx *c, int on) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  c->capture = on ? 1 : 0;
+  return SC_OK;
+}
+
+sc_status sc_get_site_forces(sc_ctx *c, double *f) {
+  if (!c || !c->loaded || !f) return SC_ERR_INVALID_ARG;
+  return copy_soa3(c, c->d.cap_F, c->ns, f);
+}
+
+sc_status sc_get_tensions(sc_ctx *c, double *t) {
+  if (!c || !c->loaded || !t) return SC_ERR_INVALID_ARG;
+  CK(cudaMemcpyAsync(t, c->d.cap_T, sizeof(double) * c->nb, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_get_filament_state(sc_ctx *c, int *sw, int *nn) {
+  if (!c || !c->loaded || !sw || !nn) return SC_ERR_INVALID_ARG;
+  CK(cudaMemcpyAsync(sw, c->d.f_switch, sizeof(int) * c->nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(nn, c->d.f_nnorm, sizeof(int) * c->nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_get_dr_tot(sc_ctx *c, double *dr) {
+  if (!c || !c->loaded || !dr) return SC_ERR_INVALID_ARG;
+  CK(cudaMemcpyAsync(dr, c->d.dt, sizeof(double) * c->ns, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_get_pairs(sc_ctx *c, int32_t *pairs, int64_t cap, int64_t *n_pairs) {
+  if (!c || !c->loaded || !n_pairs) return SC_ERR_INVALID_ARG;
+  *n_pairs = c->np;
+  long long m = std::min<long long>(cap, c->np);
+  if (m > 0 && pairs) {
+    std::vector<int> a(m), b(m);
+    CK(cudaMemcpyAsync(a.data(), c->d.pa, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(b.data(), c->d.pb, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (long long i = 0; i < m; ++i) {
+      pairs[2 * i] = a[i];
+      pairs[2 * i + 1] = b[i];
+    }
+  }
+  return SC_OK;
+}
+
+sc_status sc_get_bond_cells(sc_ctx *c, int32_t *xyz) {
+  if (!c || !c->loaded || !xyz) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  c->launches += sc::launch_bond_cells(c->k, c->d, c->cells_xyz, c->st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(xyz, c->cells_xyz, sizeof(int) * 3 * (size_t)c->nb,
+                     cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_get_counters(sc_ctx *c, sc_counters *o) {
+  if (!c || !o) return SC_ERR_INVALID_ARG;
+  std::memset(o, 0, sizeof(*o));
+  o->i_step = c->i_step;
+  o->n_rebuilds = c->n_rebuilds;
+  o->n_pairs = c->np;
+  o->pair_capacity = c->pcap;
+  o->n_filaments = c->nf;
+  o->n_sites = c->ns;
+  o->n_bonds = c->nb;
+  o->n_cells_1d = c->k.n1d;
+  o->cell_length = c->k.n1d ? (double)2 * c->desc.system_radius / c->k.n1d : 0;
+  o->dr_update = c->k.dr_update;
+  o->kernel_launches = c->launches;
+  return SC_OK;
+}
+
+void *sc_get_stream(sc_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// Shared device-side definitions of the B200 filament step.
+//
+// Every kernel translation unit is compiled with --fmad=false: the FP64
+// stages reproduce the reference's scalar, contraction-free arithmetic
+// operation by operation, which makes them bit-identical to it.  FP32 code
+// that wants fused multiply-adds asks for them explicitly (__fmaf_rn).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sc_host_philox.h"
+
+namespace sc {
+
+// The reference's macros (include/simcore/macros.hpp).
+__device__ __forceinline__ int nint(double x) {
+  return x < 0.0 ? (int)(x - 0.5) : (int)(x + 0.5);
+}
+__device__ __forceinline__ double dabs(double x) { return x < 0 ? -x : x; }
+__device__ __forceinline__ double sign_of(double a, double b) {  // SIGN(a, b)
+  return b >= 0.0 ? fabs(a) : -fabs(a);
+}
+__device__ __forceinline__ int signof(double x) { return x >= 0.0 ? 1 : -1; }
+
+// Status bits set by kernels; the host maps them to sc_status codes.
+enum : unsigned {
+  ST_NAN = 1u,            // non-finite position or force
+  ST_LIST_OVERFLOW = 2u,  // pair list did not fit
+  ST_UNPHYSICAL = 4u,     // accumulated displacement above 10000
+  ST_BAD_CELL = 8u        // cell index out of range (non-finite position)
+};
+
+// Bond geometry for the FP64 pair stage: the reference's Bond state after
+// Bond::ReInit (scaled position, unit orientation, length).  64 bytes.
+struct __align__(16) BondGeomF64 {
+  double s[3];
+  double u[3];
+  double len;
+  double pad;
+};
+
+// Bond geometry for the mixed-precision pair stage.  The scaled position is
+// stored as 32-bit fixed point q = round(s * 2^32) (s in [-1/2, 1/2]): the
+// periodic minimum image of a separation is then the wrapping int32
+// difference, exact, with 2^-32 box-length resolution.  32 bytes.
+struct __align__(16) BondGeomF32 {
+  int32_t q[3];
+  float hl;      // half length
+  float u[3];
+  float pad;
+};
+
+// Per-system constants, in __constant__ memory of each kernel unit.
+struct SysConst {
+  int n_dim;
+  int n1d;
+  int third;          // n1d in 3D, 1 in 2D
+  int n_cells;
+  double h[9];
+  double hinv[9];
+  double delta;
+  double rcut2;
+  double c12, c6, fcut;
+  double dr_update;
+  float hf[9];        // h in FP32 (mixed stage)
+  float rcut2f, c12f, c6f, fcutf;
+  uint32_t seed;
+  int stoch;
+  int like_like;
+};
+
+// Launch-invariant device pointers of one context.
+struct DevState {
+  // filaments
+  int nf, ns, nb;
+  const int *f_site_off;   // nf+1
+  const double *f_l, *f_linv, *f_kappa, *f_gpar, *f_gperp, *f_spar, *f_sperp;
+  int *f_switch, *f_nnorm;
+  const int *site_fil;     // ns
+  const int *bond_fil;     // nb
+  // integrator blocks: packed runs of whole filaments
+  const int *blk_site0;    // per block: first site
+  const int *blk_f0;       // per block: first filament
+  const int *blk_nf;       // per block: filament count
+  // sites (SoA, 3 components each)
+  double *r[3], *rp[3], *fr[3], *dz[3];
+  double *dt;
+  // bonds
+  double *bF[3], *bT[3];   // FP64 accumulators (unfused path)
+  BondGeomF64 *g64[2];     // double-buffered geometry
+  BondGeomF32 *g32[2];
+  // pairs
+  int *pa, *pb;
+  double *pf64;            // stale force per pair, 3 per pair
+  float *pf32;
+  int *e_off;              // nb+1 CSR of pair entries per bond
+  int *e_ent;              // entries (pair << 1 | role)
+  // capture (optional)
+  double *cap_F[3];
+  double *cap_T;
+  // status / control
+  unsigned *status;
+  unsigned long long *dr_max_bits;
+};
+
+}  // namespace sc

@@ -1,0 +1,41 @@
+// Host-side launchers of the device kernels (sc_kernels.cu).  Each returns
+// the number of kernels it launched.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "sc_common.cuh"
+
+namespace sc {
+
+void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
+                          int prec, cudaStream_t st);
+int scan_temp_ints(long long n);
+int launch_exclusive_scan(const int *in, int *out, long long n, int *tmp,
+                          cudaStream_t st);
+int launch_bin_count(const SysConst &k, const DevState &d, int *key,
+                     int *cell_count, cudaStream_t st);
+int launch_bond_cells(const SysConst &k, const DevState &d, int *xyz,
+                      cudaStream_t st);
+int launch_bin_scatter(int nb, const int *key, const int *cell_start,
+                       int *cell_count, int *sorted, cudaStream_t st);
+int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
+                           int *sorted, const int *cell_start, int *pair_count,
+                           cudaStream_t st);
+int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
+                     const int *sorted, const int *cell_start,
+                     const int *pair_off, int cap, int *deg, int prec,
+                     cudaStream_t st);
+int launch_csr(const DevState &d, int np, int *deg, cudaStream_t st);
+int launch_zero_dr(const DevState &d, cudaStream_t st);
+int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
+                 cudaStream_t st);
+size_t integrate_smem_bytes(int C);
+void prepare_integrate(int C);
+int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
+                     int midstep, unsigned long long mcount, int rbuf,
+                     int interaction, int capture, int prec, bool fused,
+                     cudaStream_t st);
+
+}  // namespace sc

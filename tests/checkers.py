@@ -59,7 +59,10 @@ class _Checker:
         getattr(L, p + "get_pairs").restype = ctypes.c_long
         getattr(L, p + "get_pairs").argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long]
         getattr(L, p + "destroy").argtypes = [ctypes.c_void_p]
-        sysd = SystemDesc(**{k: system[k] for k, _ in SystemDesc._fields_ if k != "n_threads"},
+        defaults = dict(wca_eps=1.0, wca_sig=1.0, f_cutoff=2000.0, stoch_flag=1,
+                        interaction_flag=1, like_like_interactions=1, seed=0)
+        vals = dict(defaults, **system)
+        sysd = SystemDesc(**{k: vals[k] for k, _ in SystemDesc._fields_ if k != "n_threads"},
                           n_threads=n_threads)
         fils = (FilamentDesc * len(filaments))(*[FilamentDesc(**f) for f in filaments])
         sites = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)

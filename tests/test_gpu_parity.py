@@ -1,0 +1,134 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+The FP64 path is bit-identical to the oracle (which is itself bit-identical
+to the reference's own code, see test_oracle.py): every comparison below is
+exact equality, over single steps and over long runs that include pair-list
+rebuilds and bond renormalisations.
+"""
+import numpy as np
+import pytest
+
+from checkers import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(system, filaments, sites, precision="fp64"):
+    import simcore_b200 as sc
+    return sc.Context(system, filaments, sites, precision=precision)
+
+
+def _workload(name, scale, seed=0, **kw):
+    from simcore_b200 import workloads
+    return workloads.make(name, scale=scale, seed=seed, **kw)
+
+
+def assert_same(a, b, what):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    assert a.shape == b.shape, what
+    bad = ~((a == b) | (np.isnan(a) & np.isnan(b)))
+    if bad.any():
+        idx = np.argwhere(bad)[0]
+        raise AssertionError("%s differs at %s: %r vs %r (%d entries)"
+                             % (what, idx, a[tuple(idx)], b[tuple(idx)], bad.sum()))
+
+
+def compare_state(ctx, o, nd, capture=True):
+    assert_same(ctx.sites()[:, :nd], o.sites()[:, :nd], "sites")
+    assert_same(ctx.prev_sites()[:, :nd], o.prev_sites()[:, :nd], "prev sites")
+    assert_same(ctx.random_forces()[:, :nd], o.random_forces()[:, :nd], "random forces")
+    gf, gt = ctx.bond_forces()
+    of, ot = o.bond_forces()
+    assert_same(gf[:, :nd], of[:, :nd], "bond forces")
+    assert_same(gt, ot, "bond torques")
+    if capture:
+        assert_same(ctx.site_forces()[:, :nd], o.site_forces()[:, :nd], "site forces")
+        assert_same(ctx.tensions(), o.tensions(), "tensions")
+    assert_same(ctx.pairs(), o.pairs(), "pair list")
+    if o.i_step % 2 == 1:
+        # The GPU adds a full step's displacement in that step's epilogue;
+        # the reference adds it at the next (odd) step's rebuild check.  The
+        # two agree whenever that check has happened, i.e. after odd steps.
+        assert_same(ctx.dr_tot(), o.dr_tot(), "dr_tot")
+    sw, nn = ctx.filament_state()
+    osw, onn = o.filament_state()
+    assert_same(sw, osw, "normalize_switch")
+    assert_same(nn, onn, "n_normalize")
+    assert ctx.counters().n_rebuilds == o.n_rebuilds
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_fp64_single_steps_bitwise(fused):
+    system, fils, sites = _workload("A", 0.3, seed=3)
+    ctx = _ctx(system, fils, sites)
+    ctx.set_capture(True)
+    o = Oracle(system, fils, sites)
+    assert_same(ctx.pairs(), o.pairs(), "initial pair list (before culling both drop exclusions)")
+    for _ in range(7):
+        if fused:
+            ctx.step(1)
+        else:
+            ctx.interact()
+            ctx.update_positions()
+        o.step(1)
+        compare_state(ctx, o, 3)
+
+
+def test_fp64_workload_A_run_bitwise():
+    """Full-size workload A (100 x 20 bonds) for 408 steps: identical state,
+    identical rebuild count and pair lists, every 51 steps."""
+    system, fils, sites = _workload("A", 1.0, seed=0)
+    ctx = _ctx(system, fils, sites)
+    ctx.set_capture(True)
+    o = Oracle(system, fils, sites)
+    for _ in range(8):
+        ctx.step(51)
+        o.step(51)
+        compare_state(ctx, o, 3)
+    assert o.n_rebuilds > 5
+
+
+def test_fp64_2d_bitwise():
+    import simcore_b200 as sc
+    n_fil, n_seg, R = 60, 16, 30.0
+    nb = np.full(n_fil, n_seg, dtype=np.int32)
+    sites = sc.insert_filaments(2, R, 7, nb, nb.astype(float), np.full(n_fil, 200.0))
+    system = dict(n_dim=2, system_radius=R, delta=1e-4, stoch_flag=1, interaction_flag=1,
+                  like_like_interactions=1, seed=5)
+    fils = [dict(length=float(n_seg), persistence_length=200.0, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * n_fil
+    ctx = _ctx(system, fils, sites)
+    ctx.set_capture(True)
+    o = Oracle(system, fils, sites)
+    for _ in range(6):
+        ctx.step(41)
+        o.step(41)
+        compare_state(ctx, o, 2)
+
+
+def test_bond_cells_and_pairs_bitwise():
+    system, fils, sites = _workload("B", 0.05, seed=1)
+    ctx = _ctx(system, fils, sites)
+    o = Oracle(system, fils, sites)
+    assert ctx.counters().n_cells_1d == o.n_cells_1d
+    assert_same(ctx.bond_cells(), o.bond_cells(), "bond cells")
+    ctx.step(1)
+    o.step(1)
+    assert_same(ctx.pairs(), o.pairs(), "pair list")
+
+
+def test_mixed_force_error():
+    """Mixed precision (FP32 pair forces) against FP64 on the same state:
+    max |dF| / max |F| <= 1e-5 over all bond forces and torques."""
+    system, fils, sites = _workload("B", 0.1, seed=2)
+    c64 = _ctx(system, fils, sites, "fp64")
+    c32 = _ctx(system, fils, sites, "mixed")
+    c64.interact()
+    c32.interact()
+    f64, t64 = c64.bond_forces()
+    f32, t32 = c32.bond_forces()
+    ef = np.abs(f32 - f64).max() / np.abs(f64).max()
+    et = np.abs(t32 - t64).max() / np.abs(t64).max()
+    assert ef <= 1e-5, ef
+    assert et <= 1e-5, et
