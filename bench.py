@@ -1,0 +1,356 @@
+#!/usr/bin/env python
+"""Throughput of the filament Brownian-dynamics step on B200.
+
+Metric: segment-steps/s = bonds x reference steps / second, one reference
+step (i_step) being one pair-force evaluation plus one integrator half step
+(the reference's step loop, src/simulation.cpp:37-62, advances delta/2).
+
+Workload (default): 20,000 filaments x 10 bonds in a 3D periodic cube of side
+200, persistence length 100, WCA eps = sigma = 1, dt = 1e-4, thermal noise on
+(synthetic, seeded random insertion).  One bench step = one captured-graph
+launch of 20 reference steps (10 midpoint BD steps, pair-list rebuilds
+included as they fall due), timed with CUDA events on the context's stream;
+L2 is flushed (256 MiB write) before every timed launch.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1: one process per GPU under torch.distributed.run, each rank an
+independent replica (weak scaling, no data-path collective); the time is the
+max over ranks.  --impl reference times the reference's own CPU code
+(oracle/_ref, OpenMP over all host cores) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "segment-steps/s, 1 B200: mixed+batched vs FP64 GPU at ≤1e-5 force err"
+UNIT = "segment-steps/s"
+I_STEPS_PER_STEP = 20
+WORKLOAD_DESC = ("B: 20,000 filaments x 10 bonds (200,000 segments, 220,000 sites), 3D periodic "
+                 "cube side 200, lp 100, WCA eps=sigma=1, dt 1e-4, noise on")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="B")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def load_measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device = device_index
+        self.proc = None
+        self.lines = []
+        self.windows = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "20"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self, t0, t1):
+        self.windows.append((t0, t1))
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        # Samples inside the timed windows (one 20 ms sample period of slack).
+        inside = [l for (t, l) in self.lines
+                  if any(a - 0.02 <= t <= b + 0.02 for (a, b) in self.windows)]
+        for line in inside:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def algorithmic_bytes(n_sites, n_bonds, n_pairs, precision):
+    """Bytes one reference step must move (per launch of the step kernel):
+    sites 96 B (r read + write, previous position, projected noise), bonds
+    112 B mixed / 208 B FP64 (geometry written and read, force/torque
+    accumulators), 8 B per candidate pair."""
+    per_bond = 112 if precision == "mixed" else 208
+    return 96 * n_sites + per_bond * n_bonds + 8 * n_pairs
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    import simcore_b200 as sc
+    from simcore_b200 import workloads
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        dist = dist_mod
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+
+    system, fils, sites = workloads.make(args.workload, 1.0, seed=rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed_graph(ctx, k, flush_l2=True):
+        """k bench steps; returns per-step device ms (CUDA events)."""
+        out = []
+        for _ in range(k):
+            if flush_l2:
+                flush.zero_()
+                torch.cuda.synchronize()
+            ctx.step_graph(I_STEPS_PER_STEP)
+            out.append(ctx.graph_time_ms())
+        return out
+
+    results = {}
+    contexts = {}
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(1.5)  # nvidia-smi needs a moment before its first sample
+    for prec in ("fp64", "mixed"):
+        ctx = sc.Context(system, fils, sites, precision=prec, device=local_rank)
+        contexts[prec] = ctx
+        timed_graph(ctx, args.warmup)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        c0 = ctx.counters()
+        t_start = time.perf_counter()
+        ms = timed_graph(ctx, args.steps)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.mark(t_start, time.perf_counter())
+        c1 = ctx.counters()
+        total_ms = float(sum(ms))
+        if dist is not None:
+            t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        results[prec] = dict(total_ms=total_ms, n_bonds=c1.n_bonds, n_sites=c1.n_sites,
+                             n_pairs=c1.n_pairs, rebuilds=c1.n_rebuilds - c0.n_rebuilds,
+                             launches=c1.kernel_launches - c0.kernel_launches)
+
+    if sampler:
+        results["clocks"] = sampler.stop()
+
+    # Roofline of the dominant kernel (the fused step kernel), mixed path:
+    # per-launch CUDA-event durations on the host-driven path.
+    ctx = contexts["mixed"]
+    ctx.set_kernel_timing(True)
+    ctx.step(2 * I_STEPS_PER_STEP)
+    kms, kn = ctx.kernel_timing()
+    ctx.set_kernel_timing(False)
+    avg_kernel_ms = kms / max(kn, 1)
+
+    # End to end through the C ABI with host buffers: upload positions,
+    # run one bench step, read positions back.
+    host_xyz = ctx.sites()
+    e2e_times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.set_sites(host_xyz)
+        ctx.step_graph(I_STEPS_PER_STEP)
+        host_xyz = ctx.sites()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_total = float(sum(e2e_times))
+    if dist is not None:
+        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    for c in contexts.values():
+        c.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    r = results["mixed"]
+    r64 = results["fp64"]
+    n_b = r["n_bonds"]
+    seg_steps = n_b * I_STEPS_PER_STEP * args.steps * world
+    value = seg_steps / (r["total_ms"] * 1e-3)
+    value64 = seg_steps / (r64["total_ms"] * 1e-3)
+    peak, peak_kind = load_measured_peaks()
+    bytes_per_launch = algorithmic_bytes(r["n_sites"], n_b, r["n_pairs"], "mixed")
+    achieved = bytes_per_launch / (avg_kernel_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair forces + f64 integrator",
+        "data": "synthetic (seeded random insertion with overlap rejection)",
+        "config": {"workload": WORKLOAD_DESC, "precision": "mixed",
+                   "i_steps_per_step": I_STEPS_PER_STEP,
+                   "timed_unit": "one CUDA-graph launch of 20 reference steps (WHILE loop of 10 "
+                                 "midpoint BD steps with device-decided pair-list rebuilds)",
+                   "l2": "flushed by a 256 MiB write before every timed step",
+                   "parallelism": "replicas" if world > 1 else "single system",
+                   "pairs": r["n_pairs"], "rebuilds_in_timed_region": r["rebuilds"]},
+        "fp64": {"value": value64, "ms_per_step": r64["total_ms"] / args.steps,
+                 "rebuilds_in_timed_region": r64["rebuilds"]},
+        "mixed_over_fp64": value / value64,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "k_integrate<3,1,fused> (pair stage + integrator)",
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "avg_launch_ms": avg_kernel_ms, "peak_kind": peak_kind + " hbm_gbs"},
+        "e2e": {"value": seg_steps / e2e_total, "unit": UNIT,
+                "h2d_bytes_per_step": 24 * r["n_sites"], "d2h_bytes_per_step": 24 * r["n_sites"]},
+        "gpu_launches": int(r["launches"]),
+        "clocks": results.get("clocks"),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(system, fils, sites, n_b)
+    return line
+
+
+def cpu_baseline(system, fils, sites, n_bonds, target_s=10.0):
+    """The reference's own code (oracle/_ref) on the same workload, OpenMP
+    over all host cores; falls back to the single-threaded C oracle when the
+    reference build is not present.  A bounded sample of steps."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from checkers import Oracle, Reference
+    cores = host_cores()
+    if Reference.available():
+        sim = Reference(system, fils, sites, n_threads=cores)
+        kind = "reference"
+    else:
+        sim = Oracle(system, fils, sites)
+        kind, cores = "port", 1
+    t0 = time.perf_counter()
+    sim.step(2)
+    dt = max(time.perf_counter() - t0, 1e-6)
+    n = int(max(2, min(400, target_s / (dt / 2))))
+    n += n % 2
+    t0 = time.perf_counter()
+    sim.step(n)
+    el = time.perf_counter() - t0
+    sim.close()
+    return {"value": n_bonds * n / el, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": "%d reference steps of the same workload (after 2 warm-up steps)" % n}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from checkers import Reference
+    from simcore_b200 import workloads
+    if not Reference.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libscref.so (the reference's "
+                "own sources) was not built on this machine"}
+    system, fils, sites = workloads.make(args.workload, 1.0, seed=0)
+    cores = host_cores()
+    sim = Reference(system, fils, sites, n_threads=cores)
+    n_b = sim.n_bonds
+    # Size each bench step to a bounded sample: at most 20 reference steps,
+    # fewer if one step is slow, so that warm-up + timed steps stay short.
+    t0 = time.perf_counter()
+    sim.step(2)
+    per = max((time.perf_counter() - t0) / 2, 1e-6)
+    budget_s = 150.0 / max(args.steps + args.warmup, 1)
+    per_step = int(max(2, min(I_STEPS_PER_STEP, budget_s / per)))
+    per_step -= per_step % 2
+    for _ in range(args.warmup):
+        sim.step(per_step)
+    times = []
+    for _ in range(args.steps):
+        times.append(sim.step(per_step))
+    sim.close()
+    total = float(sum(times))
+    value = n_b * per_step * args.steps / total
+    return {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded random insertion with overlap rejection)",
+        "config": {"workload": WORKLOAD_DESC, "i_steps_per_step": per_step,
+                   "implementation": "reference C++ (object, site, bond, mesh, filament, cell, "
+                                     "cell_list, minimum_distance, linear_algebra) -O3 OpenMP"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": "%d reference steps per bench step" % per_step},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        line = run_ours(args, rank, world, local_rank)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -13,7 +13,7 @@
  *     metric forces, random-force projection, tension solve, midpoint
  *     position update, bond renormalisation.
  * sc_step() runs whole Simulation::RunSimulation steps
- * (src/simulation.cpp:37-62) with the two halves fused on the GPU.
+ * (src/simulation.cpp:37-62) back to back on the GPU.
  *
  * Conventions: plain C types only; every vector is 3 doubles (z = 0 in 2D);
  * sites and bonds are numbered filament by filament in the order given to
@@ -116,8 +116,8 @@ sc_status sc_interact(sc_ctx *ctx);
 /* FilamentSpecies::UpdatePositions: one integrator (half) step of every
  * filament from the bond accumulators; toggles the midstep flag. */
 sc_status sc_update_positions(sc_ctx *ctx);
-/* n full reference steps (Simulation::RunSimulation bodies), pair and
- * integrator stages fused.  Bit-identical to n x (sc_interact +
+/* n reference steps (Simulation::RunSimulation bodies), each a pair-force
+ * kernel and an integrator kernel.  Bit-identical to n x (sc_interact +
  * sc_update_positions). */
 sc_status sc_step(sc_ctx *ctx, int n);
 /* Same as sc_step, replaying a captured CUDA graph of n steps. */
@@ -133,6 +133,11 @@ sc_status sc_get_random_forces(sc_ctx *ctx, double *f);      /* N_s x 3 */
 sc_status sc_get_bond_forces(sc_ctx *ctx, double *f, double *t); /* N_b x 3 */
 sc_status sc_get_bond_geometry(sc_ctx *ctx, double *pos, double *spos,
                                double *u, double *len);
+/* Integrator variant of the mixed-precision step: 1 (default) uses FMA
+ * contraction, one reciprocal per shared denominator and rsqrt
+ * normalisation; 0 runs the exact FP64 integrator of SC_PREC_FP64.  No
+ * effect in SC_PREC_FP64, which is always exact. */
+sc_status sc_set_fast_integrator(sc_ctx *ctx, int on);
 /* Site forces and tensions of the last integrator step; recorded only while
  * capture is on (sc_set_capture(ctx, 1)), since they are not state. */
 sc_status sc_set_capture(sc_ctx *ctx, int on);
@@ -155,6 +160,15 @@ sc_status sc_get_bond_cells(sc_ctx *ctx, int32_t *xyz);
 sc_status sc_get_counters(sc_ctx *ctx, sc_counters *out);
 /* The cudaStream_t all work of the context is issued on. */
 void *sc_get_stream(sc_ctx *ctx);
+/* Per-launch CUDA-event timing of the pair-force and integrator kernels
+ * launched by host-driven calls (sc_step, sc_interact, sc_update_positions);
+ * the total and the number of timed launches since timing was (re)switched
+ * on. */
+sc_status sc_set_kernel_timing(sc_ctx *ctx, int on);
+sc_status sc_get_kernel_timing(sc_ctx *ctx, double *total_ms, int64_t *launches);
+/* Device time (CUDA events on the context's stream) of the graph launch of
+ * the last sc_step_graph call, in ms. */
+sc_status sc_get_graph_time(sc_ctx *ctx, double *ms);
 
 /* Seeded random insertion with overlap rejection on the host (the
  * distributions of Mesh::InitRandomBond and Filament::InsertFilament,

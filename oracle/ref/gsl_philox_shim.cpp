@@ -25,7 +25,9 @@
 struct sc_shim_rng {
   uint32_t key0;
   uint32_t key1;
-  uint64_t k;  // next draw index
+  uint64_t k;       // next draw index
+  int noise_sites;  // > 0 once the harness declared this a filament's noise stream
+  int noise_dim;
 };
 
 namespace {
@@ -36,7 +38,7 @@ const gsl_rng_type g_type = {"philox4x32_10"};
 
 uint32_t next_word(const gsl_rng *r) {
   sc_shim_rng *s = const_cast<sc_shim_rng *>(r);
-  return sc_philox_word(s->key0, s->key1, s->k++);
+  return sc_philox_other_word(s->key0, s->key1, s->k++);
 }
 }  // namespace
 
@@ -51,6 +53,8 @@ gsl_rng *gsl_rng_alloc(const gsl_rng_type *) {
   r->key0 = g_seed;
   r->key1 = 0;
   r->k = 0;
+  r->noise_sites = 0;
+  r->noise_dim = 0;
   std::lock_guard<std::mutex> lk(g_mtx);
   if (!g_live) g_live = new std::set<sc_shim_rng *>();
   g_live->insert(r);
@@ -75,6 +79,17 @@ void gsl_rng_free(gsl_rng *r) {
 unsigned long int gsl_rng_get(const gsl_rng *r) { return next_word(r); }
 
 double gsl_rng_uniform_pos(const gsl_rng *r) {
+  sc_shim_rng *s = const_cast<sc_shim_rng *>(r);
+  if (s->noise_sites > 0) {
+    // A filament's noise draws: site-major, dimension-minor per midstep
+    // (src/filament.cpp:527-531), mapped onto the shared noise counters.
+    uint64_t k = s->k++;
+    uint64_t per = (uint64_t)s->noise_sites * (uint64_t)s->noise_dim;
+    uint64_t m = k / per;
+    uint32_t j = (uint32_t)((k / s->noise_dim) % s->noise_sites);
+    int i = (int)(k % s->noise_dim);
+    return sc_philox_noise(s->key0, s->key1, m, j, i);
+  }
   return ((double)next_word(r) + 0.5) * 2.3283064365386963e-10;
 }
 
@@ -123,6 +138,18 @@ void scshim_rewind_all(void) {
   std::lock_guard<std::mutex> lk(g_mtx);
   if (!g_live) return;
   for (sc_shim_rng *r : *g_live) r->k = 0;
+}
+
+// Declares the stream keyed (global seed, key1) a filament noise stream of a
+// filament with n_sites sites in n_dim dimensions.
+void scshim_set_noise_layout(uint32_t key1, int n_sites, int n_dim) {
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (!g_live) return;
+  for (sc_shim_rng *r : *g_live)
+    if (r->key0 == g_seed && r->key1 == key1) {
+      r->noise_sites = n_sites;
+      r->noise_dim = n_dim;
+    }
 }
 
 }  // extern "C"

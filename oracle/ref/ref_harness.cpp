@@ -70,6 +70,7 @@ bool early_exit = false;  // defined by the reference in simulation_manager.cpp
 
 extern "C" void scshim_set_global_seed(uint32_t seed);
 extern "C" void scshim_rewind_all(void);
+extern "C" void scshim_set_noise_layout(uint32_t key1, int n_sites, int n_dim);
 
 extern "C" {
 typedef struct {
@@ -372,7 +373,13 @@ void *scref_create(const scref_system *sys, int n_fil,
   s->potentials.InitPotentials(&p);
   CellList::SetMinCellLength(sqrt(s->potentials.GetRCut2()));
   CellList::Init(p.n_dim, p.n_periodic, p.system_radius);
-  s->clist.BuildCellList();
+  // CellList::BuildCellList (src/cell_list.cpp:66-74) minus its redundant
+  // full-shell neighbour pass, which only serves insertion's overlap checks
+  // (not run here) and is replaced by the half-shell pass of
+  // ResetNeighbors below anyway; the final cell structure is the same.
+  s->clist.AllocateCells();
+  s->clist.LabelCells();
+  s->clist.ClearCellObjects();
   s->dr_update = 0.25 * CellList::GetCellLength() * CellList::GetCellLength();
   MinimumDistance::Init(s->sp, 2 * s->dr_update);
 
@@ -420,6 +427,11 @@ void *scref_create(const scref_system *sys, int n_fil,
     for (int b = 0; b < f.n_bonds_; ++b) s->bond_gid[f.GetBond(b)] = gid++;
   s->n_bonds_total = gid;
 
+  // Filament i draws its noise from stream (seed, i); sites and bonds own
+  // streams of their own keyed by other values.  Only the filament streams
+  // are declared noise streams (key1 = i, n_sites of filament i).
+  for (int i = 0; i < n_fil; ++i)
+    scshim_set_noise_layout((uint32_t)i, s->members[i].n_sites_, p.n_dim);
   scshim_rewind_all();
   g_active = s;
   return s;

@@ -41,7 +41,7 @@ struct sco_sim {
   int *fs_off, *fb_off;
   double *fl, *flp, *fd, *gpar, *gperp, *spar, *sperp, *fdrmesh;
   int *fswitch, *fnnorm, *fmid;
-  uint64_t *fdraw;
+  uint64_t *fdraw; /* noisy midsteps taken, per filament */
   /* sites */
   double *r, *rp, *fr, *F, *tn, *u, *dz, *dt;
   /* bonds */
@@ -587,7 +587,7 @@ static void filament_update(sco_sim *s, int f, int midstep) {
         const double *ut = ST(j);
         double xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
         for (i = 0; i < nd; ++i)
-          xi[i] = sc_philox_uniform(s->seed, (uint32_t)f, s->fdraw[f]++) - 0.5;
+          xi[i] = sc_philox_noise(s->seed, (uint32_t)f, s->fdraw[f], (uint32_t)j, i) - 0.5;
         if (nd == 2) {
           xt[0] = SQR(ut[0]) * xi[0] + ut[0] * ut[1] * xi[1];
           xt[1] = SQR(ut[1]) * xi[1] + ut[0] * ut[1] * xi[0];
@@ -602,6 +602,7 @@ static void filament_update(sco_sim *s, int f, int midstep) {
         for (i = 0; i < nd; ++i)
           SFR(j)[i] = s->sperp[f] * xi[i] + (s->spar[f] - s->sperp[f]) * xt[i];
       }
+      s->fdraw[f]++; /* one noisy midstep of this filament */
       /* GeometricallyProjectRandomForces (:550-599) */
       for (j = 0; j < n - 1; ++j) {
         double tmp[3];

@@ -8,13 +8,17 @@
  *
  * Stream convention (identical in every code that draws thermal noise):
  *   key     = (k0, k1) = (system seed, filament index within the system)
- *   draw k  = k-th uniform of that filament since dynamics started
- *   word    = philox4x32_10(counter = (k >> 2 low32, k >> 34, 0, 0), key)[k & 3]
- *   uniform = (word + 0.5) * 2^-32, strictly inside (0, 1) like
- *             gsl_rng_uniform_pos (reference src/rng.cpp:20).
- * The reference draws, per midstep, one uniform per site and per dimension in
- * site-major order (reference src/filament.cpp:527-531), so site j, dim i of
- * midstep m uses k = (m * n_sites + j) * n_dim + i.
+ *   The reference draws, per midstep, one uniform per site and per dimension
+ *   in site-major order (reference src/filament.cpp:527-531).  The draw for
+ *   site j, dimension i (< 3) of the filament's m-th noisy midstep is
+ *     word    = philox4x32_10(counter = (j, m low32, m >> 32, 0), key)[i]
+ *     uniform = (word + 0.5) * 2^-32, strictly inside (0, 1) like
+ *               gsl_rng_uniform_pos (reference src/rng.cpp:20).
+ *   A filament's k-th draw since dynamics started maps to
+ *   m = k / (n_sites n_dim), j = (k / n_dim) % n_sites, i = k % n_dim.
+ * Any other draw of a stream (the reference's construction and insertion
+ * calls, which happen before the stream is rewound) uses
+ *   word = philox4x32_10(counter = (k >> 2, k >> 34, 0, 0xFFFFFFFF), key)[k & 3].
  */
 #ifndef SC_ORACLE_PHILOX_H
 #define SC_ORACLE_PHILOX_H
@@ -52,22 +56,31 @@ static inline void sc_philox4x32_10(const uint32_t ctr_in[4],
   out[3] = c3;
 }
 
-/* k-th 32-bit word of the stream keyed by (k0, k1). */
-static inline uint32_t sc_philox_word(uint32_t k0, uint32_t k1, uint64_t k) {
+/* Thermal-noise uniform of site j, dimension i, midstep m of stream (k0, k1). */
+static inline double sc_philox_noise(uint32_t k0, uint32_t k1, uint64_t m,
+                                     uint32_t j, int i) {
   uint32_t ctr[4], key[2], out[4];
-  ctr[0] = (uint32_t)(k >> 2);
-  ctr[1] = (uint32_t)(k >> 34);
-  ctr[2] = 0u;
+  ctr[0] = j;
+  ctr[1] = (uint32_t)m;
+  ctr[2] = (uint32_t)(m >> 32);
   ctr[3] = 0u;
   key[0] = k0;
   key[1] = k1;
   sc_philox4x32_10(ctr, key, out);
-  return out[k & 3u];
+  return ((double)out[i] + 0.5) * 2.3283064365386963e-10;
 }
 
-/* Uniform strictly inside (0, 1); exact in double. */
-static inline double sc_philox_uniform(uint32_t k0, uint32_t k1, uint64_t k) {
-  return ((double)sc_philox_word(k0, k1, k) + 0.5) * 2.3283064365386963e-10;
+/* Any other (non-noise) word k of stream (k0, k1). */
+static inline uint32_t sc_philox_other_word(uint32_t k0, uint32_t k1, uint64_t k) {
+  uint32_t ctr[4], key[2], out[4];
+  ctr[0] = (uint32_t)(k >> 2);
+  ctr[1] = (uint32_t)(k >> 34);
+  ctr[2] = 0u;
+  ctr[3] = 0xFFFFFFFFu;
+  key[0] = k0;
+  key[1] = k1;
+  sc_philox4x32_10(ctr, key, out);
+  return out[k & 3u];
 }
 
 #endif

@@ -30,7 +30,9 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_prev_sites", "sc_get_random_forces", "sc_get_bond_forces",
             "sc_get_bond_geometry", "sc_set_capture", "sc_get_site_forces",
             "sc_get_tensions", "sc_get_filament_state", "sc_get_dr_tot", "sc_get_pairs",
-            "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_insert_filaments"]
+            "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_set_kernel_timing",
+            "sc_get_kernel_timing", "sc_get_graph_time", "sc_set_fast_integrator",
+            "sc_insert_filaments"]
 
 
 class ScError(RuntimeError):
@@ -166,6 +168,9 @@ class Context:
     def synchronize(self):
         self._check(lib.sc_synchronize(self.h))
 
+    def set_fast_integrator(self, on=True):
+        self._check(lib.sc_set_fast_integrator(self.h, ctypes.c_int(1 if on else 0)))
+
     def set_capture(self, on=True):
         self._check(lib.sc_set_capture(self.h, ctypes.c_int(1 if on else 0)))
 
@@ -236,6 +241,20 @@ class Context:
         a = np.zeros((self.n_bonds, 3), dtype=np.int32)
         self._check(lib.sc_get_bond_cells(self.h, _p(a)))
         return a
+
+    def set_kernel_timing(self, on=True):
+        self._check(lib.sc_set_kernel_timing(self.h, ctypes.c_int(1 if on else 0)))
+
+    def kernel_timing(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        self._check(lib.sc_get_kernel_timing(self.h, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def graph_time_ms(self):
+        ms = ctypes.c_double()
+        self._check(lib.sc_get_graph_time(self.h, ctypes.byref(ms)))
+        return ms.value
 
     def counters(self):
         c = Counters()

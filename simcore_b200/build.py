@@ -16,7 +16,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsimcore_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["sc_kernels.cu", "sc_api.cu"]
+CU_SOURCES = ["sc_kernels.cu", "sc_kernels_fast.cu", "sc_api.cu"]
+# Units compiled with FMA contraction (everything else keeps --fmad=false).
+FMAD_SOURCES = {"sc_kernels_fast.cu"}
 CPP_SOURCES = ["sc_insert.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -48,7 +50,8 @@ def build(verbose=False, force=False, ptxas_verbose=False):
         o = os.path.join(BUILD_DIR, src + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            cmd = [nvcc] + ARCH + common + ["--fmad=false"] + inc + ["-c", s, "-o", o]
+            fmad = "--fmad=true" if src in FMAD_SOURCES else "--fmad=false"
+            cmd = [nvcc] + ARCH + common + [fmad] + inc + ["-c", s, "-o", o]
             if ptxas_verbose:
                 cmd += ["-Xptxas", "-v"]
             if verbose:

@@ -49,8 +49,8 @@ struct sc_ctx {
   unsigned long long mcount = 0;   // midsteps that drew noise
   int rbuf = 0;                    // geometry buffer read by the next pair stage
   int capture = 0;
-  bool bond_ft_valid = false;      // bF/bT hold the last step's bond forces
-  int bond_ft_src = -1;            // geometry buffer to recompute them from
+  bool fast = true;                // mixed precision: contraction/reciprocal integrator
+  bool pairs_ready = false;        // pair contributions of the next update exist
 
   // pinned readback slots
   struct Readback {
@@ -59,9 +59,19 @@ struct sc_ctx {
     int total;
   } *hb = nullptr;
 
-  // CUDA graph of n fused steps (sc_step_graph)
+  // CUDA graph: a WHILE loop of BD steps (sc_step_graph)
   cudaGraphExec_t graph_exec = nullptr;
-  int graph_n = 0;
+  int graph_rbuf = -1;             // geometry buffer parity the graph was built for
+  int *h_loop = nullptr;           // pinned loop count
+
+  // optional per-launch timing of the step kernel (host-driven path)
+  long long rebuild_kernels = 0;    // kernels in one rebuild sequence
+  bool timing = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double timed_ms = 0.0;
+  long long timed_launches = 0;
+  cudaEvent_t gev0 = nullptr, gev1 = nullptr;  // around each graph launch
+  double graph_ms = 0.0;
 };
 
 namespace {
@@ -167,37 +177,92 @@ sc_status readback(sc_ctx *c) {
   return check_status(c);
 }
 
-sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
-  if (need <= c->pcap) return SC_OK;
-  long long cap = std::max<long long>(need + need / 2, 1024);
-  if (cap > (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list of %lld pairs too large", need);
-  dfree(c, c->d.pa);
-  dfree(c, c->d.pb);
-  dfree(c, c->d.pf64);
-  dfree(c, c->d.pf32);
-  dfree(c, c->d.e_ent);
-  c->d.pa = c->d.pb = c->d.e_ent = nullptr;
-  c->d.pf64 = nullptr;
-  c->d.pf32 = nullptr;
-  CKS(dalloc(c, &c->d.pa, cap));
-  CKS(dalloc(c, &c->d.pb, cap));
-  if (c->prec == 0) CKS(dalloc(c, &c->d.pf64, 3 * cap));
-  else CKS(dalloc(c, &c->d.pf32, 3 * cap));
-  CKS(dalloc(c, &c->d.e_ent, 2 * cap));
-  c->pcap = cap;
-  c->graph_n = 0;  // device pointers changed: recapture
+void drop_graph(sc_ctx *c) {
   if (c->graph_exec) {
     cudaGraphExecDestroy(c->graph_exec);
     c->graph_exec = nullptr;
   }
+  c->graph_rbuf = -1;
+}
+
+// Grows the pair storage to at least `need` pairs, keeping the current list
+// (pairs, their stored forces and the per-bond entries).
+sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
+  if (need <= c->pcap) return SC_OK;
+  long long cap = std::max<long long>(need + need / 2, 1024);
+  if (cap > (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list of %lld pairs too large", need);
+  int *pa = nullptr, *pb = nullptr, *ent = nullptr, *pos1 = nullptr, *pos2 = nullptr;
+  double *pf64 = nullptr, *cf64 = nullptr;
+  float *pf32 = nullptr, *cf32 = nullptr;
+  CKS(dalloc(c, &pa, cap));
+  CKS(dalloc(c, &pb, cap));
+  CKS(dalloc(c, &pos1, cap));
+  CKS(dalloc(c, &pos2, cap));
+  // Stored pair forces padded to 4 values, per-bond slots to 8 values, so
+  // that every write is a 16-byte vector store.
+  if (c->prec == 0) {
+    CKS(dalloc(c, &pf64, 4 * cap));
+    CKS(dalloc(c, &cf64, 16 * cap));
+  } else {
+    CKS(dalloc(c, &pf32, 4 * cap));
+    CKS(dalloc(c, &cf32, 16 * cap));
+  }
+  CKS(dalloc(c, &ent, 2 * cap));
+  long long keep = std::min(c->np, c->pcap);
+  if (keep > 0) {
+    auto cp = [&](void *dst, const void *src, size_t bytes) {
+      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->st);
+    };
+    CK(cp(pa, c->d.pa, sizeof(int) * keep));
+    CK(cp(pb, c->d.pb, sizeof(int) * keep));
+    CK(cp(pos1, c->d.pos1, sizeof(int) * keep));
+    CK(cp(pos2, c->d.pos2, sizeof(int) * keep));
+    if (c->prec == 0) {
+      CK(cp(pf64, c->d.pf64, sizeof(double) * 4 * keep));
+      CK(cp(cf64, c->d.cf64, sizeof(double) * 16 * keep));
+    } else {
+      CK(cp(pf32, c->d.pf32, sizeof(float) * 4 * keep));
+      CK(cp(cf32, c->d.cf32, sizeof(float) * 16 * keep));
+    }
+    CK(cp(ent, c->d.e_ent, sizeof(int) * 2 * keep));
+  } else {
+    if (c->prec == 0) CK(cudaMemsetAsync(cf64, 0, sizeof(double) * 16 * cap, c->st));
+    else CK(cudaMemsetAsync(cf32, 0, sizeof(float) * 16 * cap, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  for (void *q : {(void *)c->d.pa, (void *)c->d.pb, (void *)c->d.pos1, (void *)c->d.pos2,
+                  (void *)c->d.pf64, (void *)c->d.pf32, (void *)c->d.cf64, (void *)c->d.cf32,
+                  (void *)c->d.e_ent})
+    dfree(c, q);
+  c->d.pa = pa;
+  c->d.pb = pb;
+  c->d.pos1 = pos1;
+  c->d.pos2 = pos2;
+  c->d.pf64 = pf64;
+  c->d.pf32 = pf32;
+  c->d.cf64 = cf64;
+  c->d.cf32 = cf32;
+  c->d.e_ent = ent;
+  c->pcap = cap;
+  drop_graph(c);  // device pointers changed
+  return SC_OK;
+}
+
+// Pair count of the current list (device value).
+sc_status sync_pair_count(sc_ctx *c) {
+  CK(cudaMemcpyAsync(&c->hb->total, c->d.n_pairs, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->np = c->hb->total;
   return SC_OK;
 }
 
 // InteractionManager::UpdateInteractions (src/interaction_manager.cpp:211-231):
 // bin every bond, emit the half-shell pair list in the reference's order,
-// build the per-bond pair index, zero the displacement trackers.
-sc_status rebuild(sc_ctx *c) {
+// build the per-bond pair index, zero the displacement trackers.  Device work
+// only (capturable); a list longer than the capacity sets the overflow bit.
+void rebuild_enqueue(sc_ctx *c) {
   const SysConst &k = c->k;
+  const long long before = c->launches;
   if (c->desc.interaction_flag) {
     c->launches += sc::launch_bin_count(k, c->d, c->key, c->cell_count, c->st);
     c->launches += sc::launch_exclusive_scan(c->cell_count, c->cell_start, k.n_cells,
@@ -208,22 +273,42 @@ sc_status rebuild(sc_ctx *c) {
                                               c->pair_count, c->st);
     c->launches += sc::launch_exclusive_scan(c->pair_count, c->pair_off, c->nb,
                                              c->scan_tmp, c->st);
-    CK(cudaMemcpyAsync(&c->hb->total, c->pair_off + c->nb, sizeof(int),
-                       cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    long long np = c->hb->total;
-    CKS(ensure_pair_capacity(c, np));
     c->launches += sc::launch_pair_emit(k, c->d, c->key, c->sorted, c->cell_start,
                                         c->pair_off, (int)c->pcap, c->deg, c->prec,
                                         c->st);
     c->launches += sc::launch_exclusive_scan(c->deg, c->d.e_off, c->nb, c->scan_tmp,
                                              c->st);
-    c->launches += sc::launch_csr(c->d, (int)np, c->deg, c->st);
-    c->np = np;
+    c->launches += sc::launch_csr(c->d, (int)c->pcap, c->deg, c->st);
   }
   c->launches += sc::launch_zero_dr(c->d, c->st);
-  CK(cudaGetLastError());
-  return SC_OK;
+  c->rebuild_kernels = c->launches - before;
+}
+
+// Host-driven rebuild: enqueue, then check the list fitted; if it did not,
+// grow the storage and rebuild again (binning is a pure function of the
+// positions, so the second pass gives the same list).
+sc_status rebuild(sc_ctx *c) {
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    rebuild_enqueue(c);
+    CK(cudaGetLastError());
+    if (!c->desc.interaction_flag) return SC_OK;
+    CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned),
+                       cudaMemcpyDeviceToHost, c->st));
+    CKS(sync_pair_count(c));
+    if (!(c->hb->status & sc::ST_LIST_OVERFLOW)) return SC_OK;
+    // Clear the overflow bit, undo the extra rebuild count, grow, retry.
+    unsigned clear = c->hb->status & ~sc::ST_LIST_OVERFLOW;
+    CK(cudaMemcpyAsync(c->d.status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice, c->st));
+    c->np = 0;  // the overflowed list is incomplete: nothing to keep
+    CKS(ensure_pair_capacity(c, (long long)c->hb->total));
+    long long cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    cnt -= 1;
+    CK(cudaMemcpyAsync(c->d.n_rebuilds, &cnt, sizeof(long long), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return fail(c, SC_ERR_LIST_OVERFLOW, "pair list kept overflowing");
 }
 
 // Interact's rebuild check (CheckUpdateInteractions + GetDrMax,
@@ -238,26 +323,42 @@ sc_status maybe_rebuild(sc_ctx *c) {
   double dr_max;
   std::memcpy(&dr_max, &c->hb->dr_bits, sizeof(double));
   if (dr_max > 10000) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result: dr_max %g", dr_max);
-  if (dr_max > c->k.dr_update) {
-    CKS(rebuild(c));
-    c->n_rebuilds++;
+  if (dr_max > c->k.dr_update) CKS(rebuild(c));
+  return SC_OK;
+}
+
+// Records CUDA events around one launch when kernel timing is on.
+template <class F>
+sc_status timed(sc_ctx *c, F launch) {
+  if (c->timing) CK(cudaEventRecord(c->ev0, c->st));
+  c->launches += launch();
+  if (c->timing) {
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    c->timed_ms += ms;
+    c->timed_launches += 1;
   }
   return SC_OK;
 }
 
-sc_status step_once(sc_ctx *c, bool fused) {
+sc_status step_once(sc_ctx *c) {
   c->i_step++;
   CKS(maybe_rebuild(c));
   const int interaction = c->desc.interaction_flag ? 1 : 0;
-  if (!fused && interaction) {
-    c->launches += sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, c->st);
-  }
-  c->launches += sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep,
-                                      c->mcount, c->rbuf, interaction, c->capture,
-                                      c->prec, fused, c->st);
+  if (interaction)
+    CKS(timed(c, [&] {
+      return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st);
+    }));
+  CKS(timed(c, [&] {
+    return sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep, c->rbuf,
+                                interaction, c->capture, c->prec, c->fast, c->st);
+  }));
+  if (c->midstep && c->desc.stoch_flag)
+    c->launches += sc::launch_advance_mcount(c->d, c->st);
   CK(cudaGetLastError());
-  c->bond_ft_valid = !fused;
-  c->bond_ft_src = c->rbuf;
+  c->pairs_ready = false;
   if (c->midstep && c->desc.stoch_flag) c->mcount++;
   c->midstep = !c->midstep;
   c->rbuf = 1 - c->rbuf;
@@ -343,8 +444,21 @@ sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
   c->allocs.push_back(c->d.status);
   CK(cudaMalloc((void **)&c->d.dr_max_bits, sizeof(unsigned long long)));
   c->allocs.push_back(c->d.dr_max_bits);
+  CK(cudaMalloc((void **)&c->d.mcount, sizeof(unsigned long long)));
+  c->allocs.push_back(c->d.mcount);
+  CK(cudaMalloc((void **)&c->d.n_rebuilds, sizeof(long long)));
+  c->allocs.push_back(c->d.n_rebuilds);
+  CK(cudaMalloc((void **)&c->d.loop_count, sizeof(int)));
+  c->allocs.push_back(c->d.loop_count);
   CK(cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->st));
   CK(cudaMemsetAsync(c->d.dr_max_bits, 0, sizeof(unsigned long long), c->st));
+  CK(cudaMemsetAsync(c->d.mcount, 0, sizeof(unsigned long long), c->st));
+  CK(cudaMemsetAsync(c->d.n_rebuilds, 0, sizeof(long long), c->st));
+  CK(cudaMemsetAsync(c->d.loop_count, 0, sizeof(int), c->st));
+  if (cudaHostAlloc((void **)&c->h_loop, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, SC_ERR_CUDA, "pinned allocation failed");
+  }
   *out = c;
   return SC_OK;
 }
@@ -353,9 +467,14 @@ sc_status sc_destroy(sc_ctx *c) {
   if (!c) return SC_ERR_INVALID_ARG;
   cudaSetDevice(c->desc.device);
   if (c->st) cudaStreamSynchronize(c->st);
-  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  drop_graph(c);
   for (void *p : c->allocs) cudaFree(p);
   if (c->hb) cudaFreeHost(c->hb);
+  if (c->h_loop) cudaFreeHost(c->h_loop);
+  if (c->gev0) cudaEventDestroy(c->gev0);
+  if (c->gev1) cudaEventDestroy(c->gev1);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->st) cudaStreamDestroy(c->st);
   cudaGetLastError();
   delete c;
@@ -401,18 +520,27 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   // Per-filament constants: Filament::SetParameters / InitFilamentLength /
   // SetDiffusion (src/filament.cpp:6-84, 104-170, 320-348).
   std::vector<int> site_off(n + 1, 0);
-  std::vector<double> fl(n), flinv(n), fk(n), gpar(n), gperp(n), spar(n), sperp(n);
+  std::vector<sc::FilConst> fil(n);
   for (int f = 0; f < n; ++f) {
     site_off[f + 1] = site_off[f] + nbf[f] + 1;
     const int nsf = nbf[f] + 1;
-    fl[f] = len[f] / nbf[f];
-    flinv[f] = 1.0 / fl[f];
-    fk[f] = p[f].persistence_length;
+    sc::FilConst &q = fil[f];
+    q.l = len[f] / nbf[f];
+    q.linv = 1.0 / q.l;
+    q.kappa = p[f].persistence_length;
+    q.l2 = q.l * q.l;
     double logLD = std::log(len[f] / p[f].diameter);
-    gperp[f] = 4.0 * len[f] / (3.0 * nsf * logLD);
-    gpar[f] = gperp[f] / p[f].friction_ratio;
-    sperp[f] = std::sqrt(24.0 * gperp[f] / c->desc.delta);
-    spar[f] = std::sqrt(24.0 * gpar[f] / c->desc.delta);
+    double gperp = 4.0 * len[f] / (3.0 * nsf * logLD);
+    double gpar = gperp / p[f].friction_ratio;
+    q.igpar = 1.0 / gpar;
+    q.igperp = 1.0 / gperp;
+    q.two_igperp = 2.0 / gperp;
+    q.m1_igperp = -1.0 / gperp;
+    q.dgam = 1.0 / gpar - 1.0 / gperp;
+    q.sperp = std::sqrt(24.0 * gperp / c->desc.delta);
+    q.spar = std::sqrt(24.0 * gpar / c->desc.delta);
+    q.site0 = site_off[f];
+    q.n = nsf;
   }
   c->site_off = site_off;
   std::vector<int> site_fil(nsi), bond_fil(nbi);
@@ -450,15 +578,11 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
     return SC_OK;
   };
   int *tmp_i = nullptr;
-  double *tmp_d = nullptr;
-  CKS(up(&tmp_i, site_off)); d.f_site_off = tmp_i;
-  CKS(up(&tmp_d, fl)); d.f_l = tmp_d;
-  CKS(up(&tmp_d, flinv)); d.f_linv = tmp_d;
-  CKS(up(&tmp_d, fk)); d.f_kappa = tmp_d;
-  CKS(up(&tmp_d, gpar)); d.f_gpar = tmp_d;
-  CKS(up(&tmp_d, gperp)); d.f_gperp = tmp_d;
-  CKS(up(&tmp_d, spar)); d.f_spar = tmp_d;
-  CKS(up(&tmp_d, sperp)); d.f_sperp = tmp_d;
+  {
+    sc::FilConst *q = nullptr;
+    CKS(up(&q, fil));
+    d.fil = q;
+  }
   std::vector<int> sw(n, 1), nn(n, 0);
   CKS(up(&d.f_switch, sw));
   CKS(up(&d.f_nnorm, nn));
@@ -480,6 +604,7 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
     CKS(dalloc(c, &d.dz[i], nsi));
     CKS(dalloc(c, &d.cap_F[i], nsi));
     CK(cudaMemsetAsync(d.cap_F[i], 0, sizeof(double) * nsi, c->st));
+    CKS(dalloc(c, &d.ub[i], nbi));
     CKS(dalloc(c, &d.bF[i], nbi));
     CKS(dalloc(c, &d.bT[i], nbi));
     CK(cudaMemsetAsync(d.bF[i], 0, sizeof(double) * nbi, c->st));
@@ -521,6 +646,8 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   CKS(dalloc(c, &c->sorted, nbi));
   CKS(dalloc(c, &c->pair_count, nbi));
   CKS(dalloc(c, &c->pair_off, (size_t)nbi + 1));
+  CK(cudaMemsetAsync(c->pair_off, 0, sizeof(int) * ((size_t)nbi + 1), c->st));
+  d.n_pairs = c->pair_off + nbi;
   CKS(dalloc(c, &c->deg, nbi));
   CK(cudaMemsetAsync(c->deg, 0, sizeof(int) * nbi, c->st));
   CKS(dalloc(c, &d.e_off, (size_t)nbi + 1));
@@ -528,7 +655,7 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   CKS(dalloc(c, &c->scan_tmp,
              (size_t)std::max(sc::scan_temp_ints(k.n_cells), sc::scan_temp_ints(nbi))));
   CKS(dalloc(c, &c->cells_xyz, 3 * (size_t)nbi));
-  CKS(ensure_pair_capacity(c, std::max<long long>(4ll * nbi, 1024)));
+  CKS(ensure_pair_capacity(c, std::max<long long>(nbi, 1024)));
 
   sc::prepare_integrate(c->C);
   sc::launch_init_geometry(c->k, d, 0, c->prec, c->st);
@@ -536,10 +663,12 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   c->rbuf = 0;
   // Simulation::InsertSpecies tail: forced update (rebuild + ZeroDrTot).
   CKS(rebuild(c));
+  // Headroom for list growth during captured runs (no resizing inside a graph).
+  CKS(ensure_pair_capacity(c, c->np + c->np / 2 + 1024));
+  CK(cudaMemsetAsync(c->d.n_rebuilds, 0, sizeof(long long), c->st));
   CK(cudaStreamSynchronize(c->st));
   c->loaded = true;
   c->i_step = 0;
-  c->n_rebuilds = 0;
   c->midstep = 1;
   c->mcount = 0;
   return SC_OK;
@@ -551,47 +680,159 @@ sc_status sc_interact(sc_ctx *c) {
   // ZeroForces + Interact of the next step.
   c->i_step++;
   CKS(maybe_rebuild(c));
-  if (c->desc.interaction_flag) {
-    c->launches += sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, c->st);
-  } else {
-    for (int i = 0; i < 3; ++i) {
-      CK(cudaMemsetAsync(c->d.bF[i], 0, sizeof(double) * c->nb, c->st));
-      CK(cudaMemsetAsync(c->d.bT[i], 0, sizeof(double) * c->nb, c->st));
-    }
-  }
+  if (c->desc.interaction_flag)
+    CKS(timed(c, [&] {
+      return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st);
+    }));
   CK(cudaGetLastError());
-  c->bond_ft_valid = true;
-  c->bond_ft_src = c->rbuf;
+  c->pairs_ready = true;
   return SC_OK;
 }
 
 sc_status sc_update_positions(sc_ctx *c) {
   if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
   CK(cudaSetDevice(c->desc.device));
-  if (!c->bond_ft_valid) return fail(c, SC_ERR_INVALID_ARG, "sc_update_positions needs sc_interact first");
-  c->launches += sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep,
-                                      c->mcount, c->rbuf, 1, c->capture, c->prec,
-                                      false, c->st);
+  if (!c->pairs_ready) return fail(c, SC_ERR_INVALID_ARG, "sc_update_positions needs sc_interact first");
+  CKS(timed(c, [&] {
+    return sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep, c->rbuf,
+                                c->desc.interaction_flag ? 1 : 0, c->capture, c->prec,
+                                c->fast, c->st);
+  }));
+  if (c->midstep && c->desc.stoch_flag)
+    c->launches += sc::launch_advance_mcount(c->d, c->st);
   CK(cudaGetLastError());
   if (c->midstep && c->desc.stoch_flag) c->mcount++;
   c->midstep = !c->midstep;
   c->rbuf = 1 - c->rbuf;
-  c->bond_ft_valid = false;  // consumed; bF/bT still hold them for getters
-  c->bond_ft_src = -2;
+  c->pairs_ready = false;
   return SC_OK;
 }
 
 sc_status sc_step(sc_ctx *c, int n) {
   if (!c || !c->loaded || n < 0) return SC_ERR_INVALID_ARG;
   CK(cudaSetDevice(c->desc.device));
-  for (int i = 0; i < n; ++i) CKS(step_once(c, true));
+  for (int i = 0; i < n; ++i) CKS(step_once(c));
+  return SC_OK;
+}
+
+// Captures one graph: WHILE (loop_count > 0) { decide -> IF(rebuild) ->
+// midstep -> full step -> tail }.  Built for the current geometry-buffer
+// parity; every BD step returns the parity to where it started.
+static sc_status build_graph(sc_ctx *c) {
+  drop_graph(c);
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle h_loop;
+  CK(cudaGraphConditionalHandleCreate(&h_loop, g, 0, 0));
+  // head kernel: sets the loop condition
+  CK(cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  sc::launch_loop_head(c->d, h_loop, c->st);
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, nullptr, &deps, &ndeps));
+  std::vector<cudaGraphNode_t> head(deps, deps + ndeps);
+  CK(cudaStreamEndCapture(c->st, &g));
+  // WHILE node
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = h_loop;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  CK(cudaGraphAddNode(&wnode, g, head.data(), head.size(), &wp));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  const int interaction = c->desc.interaction_flag ? 1 : 0;
+  std::vector<cudaGraphNode_t> tail;
+  if (interaction) {
+    cudaGraphConditionalHandle h_if;
+    CK(cudaGraphConditionalHandleCreate(&h_if, body, 0, 0));
+    CK(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    sc::launch_decide(c->k, c->d, h_if, c->st);
+    CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, nullptr, &deps, &ndeps));
+    std::vector<cudaGraphNode_t> dec(deps, deps + ndeps);
+    CK(cudaStreamEndCapture(c->st, &body));
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = h_if;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    CK(cudaGraphAddNode(&inode, body, dec.data(), dec.size(), &ip));
+    cudaGraph_t rb = ip.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(c->st, rb, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    long long launches = c->launches;
+    rebuild_enqueue(c);
+    c->launches = launches;
+    CK(cudaStreamEndCapture(c->st, &rb));
+    tail.push_back(inode);
+  }
+  CK(cudaStreamBeginCaptureToGraph(c->st, body, tail.empty() ? nullptr : tail.data(), nullptr,
+                                   tail.size(), cudaStreamCaptureModeRelaxed));
+  for (int half = 0; half < 2; ++half) {
+    const int rb = half == 0 ? c->rbuf : 1 - c->rbuf;
+    if (interaction) sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st);
+    sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
+                         c->capture, c->prec, c->fast, c->st);
+  }
+  sc::launch_loop_tail(c->d, c->desc.stoch_flag ? 1 : 0, h_loop, c->st);
+  CK(cudaStreamEndCapture(c->st, &body));
+  CK(cudaGetLastError());
+  cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    c->graph_exec = nullptr;
+    return fail(c, SC_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+  }
+  c->graph_rbuf = c->rbuf;
   return SC_OK;
 }
 
 sc_status sc_step_graph(sc_ctx *c, int n) {
-  // Graph replay is added with device-side rebuild decisions; until then the
-  // fused step loop is the same computation.
-  return sc_step(c, n);
+  if (!c || !c->loaded || n < 0) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  // Align to a midstep with the host-driven loop, then run whole BD steps.
+  if (!c->midstep && n > 0) {
+    CKS(step_once(c));
+    --n;
+  }
+  int bd = n / 2;
+  if (bd > 0) {
+    // The list must have room to grow by half before a captured run.
+    CKS(sync_pair_count(c));
+    if (c->np + c->np / 2 > c->pcap) CKS(ensure_pair_capacity(c, c->np + c->np / 2));
+    if (!c->graph_exec || c->graph_rbuf != c->rbuf) CKS(build_graph(c));
+    *c->h_loop = bd;
+    CK(cudaMemcpyAsync(c->d.loop_count, c->h_loop, sizeof(int), cudaMemcpyHostToDevice, c->st));
+    long long nr0 = 0, nr1 = 0;
+    CK(cudaMemcpyAsync(&nr0, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    if (!c->gev0) {
+      CK(cudaEventCreate(&c->gev0));
+      CK(cudaEventCreate(&c->gev1));
+    }
+    CK(cudaEventRecord(c->gev0, c->st));
+    CK(cudaGraphLaunch(c->graph_exec, c->st));
+    CK(cudaEventRecord(c->gev1, c->st));
+    CK(cudaMemcpyAsync(&nr1, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    c->i_step += 2 * (long long)bd;
+    if (c->desc.stoch_flag) c->mcount += bd;
+    c->pairs_ready = false;
+    CKS(readback(c));
+    {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
+      c->graph_ms = ms;
+    }
+    // Kernels the graph ran: loop head, per BD step decide + 2 steps + tail,
+    // per rebuild the captured rebuild sequence.
+    c->launches += 1 + (long long)bd * (c->desc.interaction_flag ? 6 : 3) +
+                   (nr1 - nr0) * c->rebuild_kernels;
+    unsigned st = c->hb->status;
+    if (st & sc::ST_UNPHYSICAL) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result");
+    if (st & sc::ST_LIST_OVERFLOW) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow inside a captured run");
+  }
+  if (n % 2) CKS(step_once(c));
+  return SC_OK;
 }
 
 sc_status sc_synchronize(sc_ctx *c) {
@@ -636,13 +877,17 @@ sc_status sc_set_sites(sc_ctx *c, const double *xyz) {
 sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
   if (!c || !c->loaded || !f || !t) return SC_ERR_INVALID_ARG;
   CK(cudaSetDevice(c->desc.device));
-  if (c->bond_ft_src >= 0 && !c->bond_ft_valid && c->desc.interaction_flag) {
-    // The fused step kept no bond accumulators: re-evaluate them from the
-    // geometry that step read (still intact in the other buffer) and the
-    // pair forces it left; this reproduces its sums exactly.
-    c->launches += sc::launch_pairs(c->k, c->d, c->bond_ft_src, c->prec, c->st);
-    CK(cudaGetLastError());
+  // Bond accumulators of the last pair evaluation (Bond::force_/torque_
+  // after Interact), summed from its per-bond slots.
+  if (c->desc.interaction_flag) {
+    c->launches += sc::launch_bond_sum(c->k, c->d, c->prec, c->st);
+  } else {
+    for (int i = 0; i < 3; ++i) {
+      CK(cudaMemsetAsync(c->d.bF[i], 0, sizeof(double) * c->nb, c->st));
+      CK(cudaMemsetAsync(c->d.bT[i], 0, sizeof(double) * c->nb, c->st));
+    }
   }
+  CK(cudaGetLastError());
   CKS(copy_soa3(c, c->d.bF, c->nb, f));
   return copy_soa3(c, c->d.bT, c->nb, t);
 }
@@ -677,8 +922,16 @@ sc_status sc_get_bond_geometry(sc_ctx *c, double *pos, double *spos, double *u,
   return SC_OK;
 }
 
+sc_status sc_set_fast_integrator(sc_ctx *c, int on) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  if (c->fast != (on != 0)) drop_graph(c);
+  c->fast = on != 0;
+  return SC_OK;
+}
+
 sc_status sc_set_capture(sc_ctx *c, int on) {
   if (!c) return SC_ERR_INVALID_ARG;
+  if (c->capture != (on ? 1 : 0)) drop_graph(c);
   c->capture = on ? 1 : 0;
   return SC_OK;
 }
@@ -712,6 +965,7 @@ sc_status sc_get_dr_tot(sc_ctx *c, double *dr) {
 
 sc_status sc_get_pairs(sc_ctx *c, int32_t *pairs, int64_t cap, int64_t *n_pairs) {
   if (!c || !c->loaded || !n_pairs) return SC_ERR_INVALID_ARG;
+  CKS(sync_pair_count(c));
   *n_pairs = c->np;
   long long m = std::min<long long>(cap, c->np);
   if (m > 0 && pairs) {
@@ -741,6 +995,12 @@ sc_status sc_get_bond_cells(sc_ctx *c, int32_t *xyz) {
 sc_status sc_get_counters(sc_ctx *c, sc_counters *o) {
   if (!c || !o) return SC_ERR_INVALID_ARG;
   std::memset(o, 0, sizeof(*o));
+  if (c->loaded) {
+    long long nr = 0;
+    CK(cudaMemcpyAsync(&nr, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    CKS(sync_pair_count(c));
+    c->n_rebuilds = nr;
+  }
   o->i_step = c->i_step;
   o->n_rebuilds = c->n_rebuilds;
   o->n_pairs = c->np;
@@ -756,5 +1016,30 @@ sc_status sc_get_counters(sc_ctx *c, sc_counters *o) {
 }
 
 void *sc_get_stream(sc_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+sc_status sc_set_kernel_timing(sc_ctx *c, int on) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  if (on && !c->ev0) {
+    CK(cudaEventCreate(&c->ev0));
+    CK(cudaEventCreate(&c->ev1));
+  }
+  c->timing = on != 0;
+  c->timed_ms = 0.0;
+  c->timed_launches = 0;
+  return SC_OK;
+}
+
+sc_status sc_get_graph_time(sc_ctx *c, double *ms) {
+  if (!c || !ms) return SC_ERR_INVALID_ARG;
+  *ms = c->graph_ms;
+  return SC_OK;
+}
+
+sc_status sc_get_kernel_timing(sc_ctx *c, double *total_ms, int64_t *launches) {
+  if (!c || !total_ms || !launches) return SC_ERR_INVALID_ARG;
+  *total_ms = c->timed_ms;
+  *launches = c->timed_launches;
+  return SC_OK;
+}
 
 }  // extern "C"

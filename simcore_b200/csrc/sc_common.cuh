@@ -70,12 +70,24 @@ struct SysConst {
   int like_like;
 };
 
+// Per-filament constants of the integrator.  The reciprocals are the
+// reference's own quotients (1.0 / friction_par_, 2.0 / friction_perp_, ...,
+// src/filament.cpp:783-830, 992-996), evaluated once on the host with the
+// same IEEE operations, so every use sees the bits the reference computes
+// inline.  96 bytes.
+struct FilConst {
+  double l, linv, kappa, l2;                   // bond length, 1/l, lp, l*l
+  double igpar, igperp, two_igperp, m1_igperp; // 1/g_par, 1/g_perp, 2/g_perp, -1/g_perp
+  double dgam;                                 // 1/g_par - 1/g_perp
+  double spar, sperp;                          // sqrt(24 g / delta)
+  int site0, n;                                // first site, number of sites
+};
+
 // Launch-invariant device pointers of one context.
 struct DevState {
   // filaments
   int nf, ns, nb;
-  const int *f_site_off;   // nf+1
-  const double *f_l, *f_linv, *f_kappa, *f_gpar, *f_gperp, *f_spar, *f_sperp;
+  const FilConst *fil;     // nf
   int *f_switch, *f_nnorm;
   const int *site_fil;     // ns
   const int *bond_fil;     // nb
@@ -87,21 +99,29 @@ struct DevState {
   double *r[3], *rp[3], *fr[3], *dz[3];
   double *dt;
   // bonds
+  double *ub[3];           // FP64 orientation of every bond (Bond::orientation_)
   double *bF[3], *bT[3];   // FP64 accumulators (unfused path)
   BondGeomF64 *g64[2];     // double-buffered geometry
   BondGeomF32 *g32[2];
   // pairs
   int *pa, *pb;
-  double *pf64;            // stale force per pair, 3 per pair
+  double *pf64;            // stored force per pair, 4 per pair (x, y, z, pad)
   float *pf32;
   int *e_off;              // nb+1 CSR of pair entries per bond
-  int *e_ent;              // entries (pair << 1 | role)
+  int *e_ent;              // entries (pair << 1 | role), sorted by pair per bond
+  int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
+  double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
+  float *cf32;
   // capture (optional)
   double *cap_F[3];
   double *cap_T;
-  // status / control
+  // status / control (device-resident so captured graphs need no host state)
   unsigned *status;
   unsigned long long *dr_max_bits;
+  unsigned long long *mcount;  // midsteps that drew noise (Philox draw offset)
+  long long *n_rebuilds;       // pair-list rebuilds
+  int *loop_count;             // remaining BD steps of a graph launch
+  const int *n_pairs;          // current pair count (last entry of the pair offsets)
 };
 
 }  // namespace sc

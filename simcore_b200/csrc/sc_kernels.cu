@@ -6,88 +6,20 @@
 //                                 src/cell.cpp)
 //   pair CSR       k_csr_fill, k_csr_sort (per-bond pair entries in list
 //                  order, for the reference's serial scatter order)
-//   pair forces    k_pairs       (InteractionManager::CalculatePairInteractions
-//                                 + ApplyPairInteractions)
+//   pair forces    k_pair_eval   (InteractionManager::CalculatePairInteractions,
+//                                 one thread per pair, signed per-bond slots)
+//                  k_bond_sum    (ApplyPairInteractions into bond accumulators)
 //   integrator     k_integrate   (Filament::UpdatePosition for every
-//                                 filament; FUSED also runs the pair stage)
+//                                 filament; sums each bond's pair slots first)
 //   utilities      exclusive scan, geometry init, displacement reset.
 #include <cuda_runtime.h>
 
 #include "sc_common.cuh"
 #include "sc_kernels.h"
 #include "sc_pair.cuh"
+#include "sc_step.cuh"
 
 namespace sc {
-
-// ---------------------------------------------------------------------------
-// Bond geometry from two sites: Bond::ReInit (src/bond.cpp:22-37) followed by
-// Object::UpdatePeriodic / periodic_boundary_conditions
-// (src/object.cpp:202-210, src/linear_algebra.cpp:100-117).
-template <int ND>
-__device__ __forceinline__ void bond_from_sites(const SysConst &k,
-                                                const double *r1,
-                                                const double *r2, double s[3],
-                                                double u[3], double &len) {
-  double pos[3] = {0, 0, 0};
-  u[0] = u[1] = u[2] = 0.0;
-  s[0] = s[1] = s[2] = 0.0;
-  len = 0;
-#pragma unroll
-  for (int i = 0; i < ND; ++i) {
-    u[i] = r2[i] - r1[i];
-    len += u[i] * u[i];
-  }
-  len = sqrt(len);
-#pragma unroll
-  for (int i = 0; i < ND; ++i) {
-    pos[i] = r1[i] + 0.5 * u[i];
-    u[i] /= len;
-  }
-#pragma unroll
-  for (int i = 0; i < ND; ++i) {
-    s[i] = 0.0;
-#pragma unroll
-    for (int j = 0; j < ND; ++j) s[i] += k.hinv[ND * i + j] * pos[j];
-    s[i] -= nint(s[i]);
-  }
-}
-
-__device__ __forceinline__ int32_t to_fixed(double s) {
-  // s in [-1/2, 1/2]: round(s * 2^32) wraps into int32 (1/2 and -1/2 map to
-  // the same point of the periodic box).
-  long long q = __double2ll_rn(s * 4294967296.0);
-  return (int32_t)(uint32_t)(unsigned long long)q;
-}
-
-template <int ND>
-__device__ __forceinline__ void store_geom(const DevState &d, int buf, int b,
-                                           const double s[3],
-                                           const double u[3], double len,
-                                           int prec) {
-  if (prec == 0) {
-    BondGeomF64 g;
-    g.s[0] = s[0];
-    g.s[1] = s[1];
-    g.s[2] = s[2];
-    g.u[0] = u[0];
-    g.u[1] = u[1];
-    g.u[2] = u[2];
-    g.len = len;
-    g.pad = 0.0;
-    d.g64[buf][b] = g;
-  } else {
-    BondGeomF32 g;
-    g.q[0] = to_fixed(s[0]);
-    g.q[1] = to_fixed(s[1]);
-    g.q[2] = ND == 3 ? to_fixed(s[2]) : 0;
-    g.hl = (float)(0.5 * len);
-    g.u[0] = (float)u[0];
-    g.u[1] = (float)u[1];
-    g.u[2] = (float)u[2];
-    g.pad = 0.f;
-    d.g32[buf][b] = g;
-  }
-}
 
 template <int ND>
 __global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec) {
@@ -102,6 +34,9 @@ __global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec) {
   }
   bond_from_sites<ND>(k, r1, r2, s, u, len);
   store_geom<ND>(d, buf, b, s, u, len, prec);
+  d.ub[0][b] = u[0];
+  d.ub[1][b] = u[1];
+  d.ub[2][b] = u[2];
 }
 
 // ---------------------------------------------------------------------------
@@ -297,13 +232,11 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
       d.pa[p] = a;
       d.pb[p] = b;
       if (prec == 0) {
-        d.pf64[3 * (size_t)p] = 0.0;
-        d.pf64[3 * (size_t)p + 1] = 0.0;
-        d.pf64[3 * (size_t)p + 2] = 0.0;
+        double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)p;
+        st[0] = make_double2(0.0, 0.0);
+        st[1] = make_double2(0.0, 0.0);
       } else {
-        d.pf32[3 * (size_t)p] = 0.f;
-        d.pf32[3 * (size_t)p + 1] = 0.f;
-        d.pf32[3 * (size_t)p + 2] = 0.f;
+        reinterpret_cast<float4 *>(d.pf32)[p] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       atomicAdd(&deg[a], 1);
       atomicAdd(&deg[b], 1);
@@ -322,9 +255,11 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
 
 // Entries (pair << 1 | role) of every bond; role 0 = obj1, 1 = obj2.  The
 // degree array is decremented back to zero.
-__global__ void k_csr_fill(DevState d, int np, int *deg) {
+__global__ void k_csr_fill(DevState d, int cap, int *deg) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= np) return;
+  int np = *d.n_pairs;
+  if (p == 0 && np > cap) atomicOr(d.status, ST_LIST_OVERFLOW);
+  if (p >= np || p >= cap) return;
   int a = d.pa[p], b = d.pb[p];
   int sa = atomicSub(&deg[a], 1) - 1;
   int sb = atomicSub(&deg[b], 1) - 1;
@@ -352,7 +287,10 @@ __global__ void k_csr_sort(DevState d) {
 // InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321).
 __global__ void k_zero_dr(DevState d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *d.dr_max_bits = 0ull;
+  if (i == 0) {
+    *d.dr_max_bits = 0ull;
+    *d.n_rebuilds += 1;
+  }
   if (i >= d.ns) return;
   d.dz[0][i] = d.r[0][i];
   d.dz[1][i] = d.r[1][i];
@@ -439,692 +377,115 @@ __global__ void k_scan_add(int *out, int n, const int *tile_sums) {
 }
 
 // ---------------------------------------------------------------------------
-// Pair stage of one bond: loops over the bond's pairs in list order and sums
-// +F / -F and +t1 / -t2 as ApplyPairInteractions does
-// (src/interaction_manager.cpp:500-517).  A pair whose potential is not
-// evaluated this step keeps its force from the last evaluation since the
-// list was built (the reference's Interaction records are never cleared,
-// src/minimum_distance.cpp:31-34 resets only dr and the contacts).  Only the
-// obj1 side stores a new force; both sides reach the same in-range verdict
-// bit for bit, so no side reads a force the other is writing.
-
-__device__ __forceinline__ void cross3(const double *a, const double *b,
-                                       double *c) {
-  c[0] = a[1] * b[2] - a[2] * b[1];
-  c[1] = a[2] * b[0] - a[0] * b[2];
-  c[2] = a[0] * b[1] - a[1] * b[0];
-}
-
-template <int ND>
-__device__ __forceinline__ void bond_pairs_f64(const SysConst &k,
-                                               const DevState &d, int b,
-                                               int rbuf, double F[3],
-                                               double T[3]) {
-  F[0] = F[1] = F[2] = 0.0;
-  T[0] = T[1] = T[2] = 0.0;
-  const BondGeomF64 *geo = d.g64[rbuf];
-  const BondGeomF64 self = geo[b];
-  const int e1 = d.e_off[b + 1];
-  for (int e = d.e_off[b]; e < e1; ++e) {
-    int ent = d.e_ent[e];
-    int p = ent >> 1, role = ent & 1;
-    int other = role ? d.pa[p] : d.pb[p];
-    const BondGeomF64 o = geo[other];
-    PairGeom<double> g;
-    if (role == 0) sphero_f64<ND>(k, self, o, g);
-    else sphero_f64<ND>(k, o, self, g);
-    double force[3] = {0.0, 0.0, 0.0};
-    double *stale = d.pf64 + 3 * (size_t)p;
-    if (wca_f64<ND>(k, g, force)) {
-      if (role == 0) {
-        stale[0] = force[0];
-        stale[1] = force[1];
-        stale[2] = force[2];
-      }
-    } else {
-      force[0] = stale[0];
-      force[1] = stale[1];
-      force[2] = stale[2];
-    }
-    double t[3];
-    cross3(role ? g.c2 : g.c1, force, t);
-    if (role == 0) {
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += force[i];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) T[i] += t[i];
-    } else {
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] -= force[i];
-#pragma unroll
-      for (int i = 0; i < 3; ++i) T[i] -= t[i];
-    }
-  }
-}
-
-__device__ __forceinline__ void kahan_add(float &sum, float &comp, float x) {
-  float y = x - comp;
-  float t = sum + y;
-  comp = (t - sum) - y;
-  sum = t;
-}
-
-template <int ND>
-__device__ __forceinline__ void bond_pairs_f32(const SysConst &k,
-                                               const DevState &d, int b,
-                                               int rbuf, double F[3],
-                                               double T[3]) {
-  float sF[3] = {0.f, 0.f, 0.f}, cF[3] = {0.f, 0.f, 0.f};
-  float sT[3] = {0.f, 0.f, 0.f}, cT[3] = {0.f, 0.f, 0.f};
-  const BondGeomF32 *geo = d.g32[rbuf];
-  const BondGeomF32 self = geo[b];
-  const int e1 = d.e_off[b + 1];
-  for (int e = d.e_off[b]; e < e1; ++e) {
-    int ent = d.e_ent[e];
-    int p = ent >> 1, role = ent & 1;
-    int other = role ? d.pa[p] : d.pb[p];
-    const BondGeomF32 o = geo[other];
-    PairGeom<float> g;
-    if (role == 0) sphero_f32<ND>(k, self, o, g);
-    else sphero_f32<ND>(k, o, self, g);
-    float force[3] = {0.f, 0.f, 0.f};
-    float *stale = d.pf32 + 3 * (size_t)p;
-    if (wca_f32<ND>(k, g, force)) {
-      if (role == 0) {
-        stale[0] = force[0];
-        stale[1] = force[1];
-        stale[2] = force[2];
-      }
-    } else {
-      force[0] = stale[0];
-      force[1] = stale[1];
-      force[2] = stale[2];
-    }
-    const float *c = role ? g.c2 : g.c1;
-    float t[3] = {c[1] * force[2] - c[2] * force[1],
-                  c[2] * force[0] - c[0] * force[2],
-                  c[0] * force[1] - c[1] * force[0]};
-    float sgn = role ? -1.f : 1.f;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) kahan_add(sF[i], cF[i], sgn * force[i]);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) kahan_add(sT[i], cT[i], sgn * t[i]);
-  }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    F[i] = (double)sF[i] - (double)cF[i];
-    T[i] = (double)sT[i] - (double)cT[i];
-  }
-}
+// Pair stage.  One thread per candidate pair evaluates it once
+// (ProcessPairInteraction + the torque cross products of
+// CalculatePairInteractions, src/interaction_manager.cpp:323-397, 466-471)
+// and writes its signed contributions -- (+F, +t1) for obj1, (-F, -t2) for
+// obj2 -- into the two per-bond slots the pair owns.  Every bond's slots are
+// sorted by pair index, so summing them in slot order repeats the
+// reference's serial scatter ApplyPairInteractions
+// (src/interaction_manager.cpp:500-517) operation for operation; x - y and
+// x + (-y) are the same IEEE operation.
+//
+// A pair whose potential is not evaluated this step keeps the force of its
+// last evaluation since the list was built: the reference never clears an
+// Interaction's force (src/minimum_distance.cpp:31-34 resets only dr and the
+// contacts), and the pair's thread owns that stored force.
 
 template <int ND, int PREC>
-__global__ void k_pairs(SysConst k, DevState d, int rbuf) {
+__device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d, int rbuf,
+                                              int p) {
+  const int a = d.pa[p], b = d.pb[p];
+  const int s1 = d.pos1[p], s2 = d.pos2[p];
+  if (PREC == 0) {
+    const BondGeomF64 A = d.g64[rbuf][a], B = d.g64[rbuf][b];
+    double2 *stale = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)p;
+    const double2 st0 = stale[0], st1 = stale[1];
+    PairGeom<double> g;
+    sphero_f64<ND>(k, A, B, g);
+    double force[3];
+    if (!wca_f64<ND>(k, g, force)) {
+      force[0] = st0.x;
+      force[1] = st0.y;
+      force[2] = st1.x;
+    } else {
+      if (ND == 2) force[2] = st1.x;
+      stale[0] = make_double2(force[0], force[1]);
+      stale[1] = make_double2(force[2], 0.0);
+    }
+    double t1[3], t2[3];
+    cross3(g.c1, force, t1);
+    cross3(g.c2, force, t2);
+    double2 *c1 = reinterpret_cast<double2 *>(d.cf64) + 4 * (size_t)s1;
+    double2 *c2 = reinterpret_cast<double2 *>(d.cf64) + 4 * (size_t)s2;
+    c1[0] = make_double2(force[0], force[1]);
+    c1[1] = make_double2(force[2], t1[0]);
+    c1[2] = make_double2(t1[1], t1[2]);
+    c2[0] = make_double2(-force[0], -force[1]);
+    c2[1] = make_double2(-force[2], -t2[0]);
+    c2[2] = make_double2(-t2[1], -t2[2]);
+  } else {
+    const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
+    float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
+    const float4 st = *stale;
+    PairGeom<float> g;
+    sphero_f32<ND>(k, A, B, g);
+    float force[3];
+    if (!wca_f32<ND>(k, g, force)) {
+      force[0] = st.x;
+      force[1] = st.y;
+      force[2] = st.z;
+    } else {
+      if (ND == 2) force[2] = st.z;
+      *stale = make_float4(force[0], force[1], force[2], 0.f);
+    }
+    float t1[3] = {g.c1[1] * force[2] - g.c1[2] * force[1],
+                   g.c1[2] * force[0] - g.c1[0] * force[2],
+                   g.c1[0] * force[1] - g.c1[1] * force[0]};
+    float t2[3] = {g.c2[1] * force[2] - g.c2[2] * force[1],
+                   g.c2[2] * force[0] - g.c2[0] * force[2],
+                   g.c2[0] * force[1] - g.c2[1] * force[0]};
+    float4 *c1 = reinterpret_cast<float4 *>(d.cf32) + 2 * (size_t)s1;
+    float4 *c2 = reinterpret_cast<float4 *>(d.cf32) + 2 * (size_t)s2;
+    c1[0] = make_float4(force[0], force[1], force[2], t1[0]);
+    c1[1] = make_float4(t1[1], t1[2], 0.f, 0.f);
+    c2[0] = make_float4(-force[0], -force[1], -force[2], -t2[0]);
+    c2[1] = make_float4(-t2[1], -t2[2], 0.f, 0.f);
+  }
+}
+
+// Grid-stride over the current list, so a captured launch stays correct
+// whatever length the list grows to between captures.
+template <int ND, int PREC>
+__global__ void __launch_bounds__(256) k_pair_eval(SysConst k, DevState d, int rbuf) {
+  const int np = *d.n_pairs;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
+    pair_eval_one<ND, PREC>(k, d, rbuf, p);
+}
+
+// Bond force/torque accumulators (Bond::force_ / torque_ after Interact),
+// for sc_interact and the getters.
+template <int ND, int PREC>
+__global__ void k_bond_sum(DevState d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
   double F[3], T[3];
-  if (PREC == 0) bond_pairs_f64<ND>(k, d, b, rbuf, F, T);
-  else bond_pairs_f32<ND>(k, d, b, rbuf, F, T);
+  bond_pair_sum<ND, PREC>(d, b, F, T);
   for (int i = 0; i < 3; ++i) {
     d.bF[i][b] = F[i];
     d.bT[i][b] = T[i];
   }
 }
 
-// ---------------------------------------------------------------------------
-// Integrator.  A block holds a run of whole filaments, one thread per site,
-// filaments back to back.  Per-site work runs in parallel; the sequential
-// recurrences of one filament (Thomas solves, metric determinants,
-// renormalisation) run on its first thread, in the reference's order.
-
-// Thomas algorithm of the reference's tridiagonal_solver
-// (src/linear_algebra.cpp:164-197); n unknowns, in place.
-__device__ __forceinline__ void thomas(double *a, const double *b, double *c,
-                                       double *d, int n) {
-  n--;
-  c[0] /= b[0];
-  d[0] /= b[0];
-  for (int i = 1; i < n; ++i) {
-    c[i] /= b[i] - a[i - 1] * c[i - 1];
-    d[i] = (d[i] - a[i - 1] * d[i - 1]) / (b[i] - a[i - 1] * c[i - 1]);
+// Slot of each (pair, role) entry after the per-bond sort.
+__global__ void k_csr_pos(DevState d) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  for (int e = d.e_off[b]; e < d.e_off[b + 1]; ++e) {
+    int ent = d.e_ent[e];
+    if (ent & 1) d.pos2[ent >> 1] = e;
+    else d.pos1[ent >> 1] = e;
   }
-  d[n] = (d[n] - a[n - 1] * d[n - 1]) / (b[n] - a[n - 1] * c[n - 1]);
-  for (int i = n; i-- > 0;) d[i] -= c[i] * d[i + 1];
-}
-
-template <int ND>
-__device__ __forceinline__ double dotn(const double *a, const double *b) {
-  double m = 0.0;
-#pragma unroll
-  for (int i = 0; i < ND; ++i) m += a[i] * b[i];
-  return m;
-}
-
-template <int ND, int PREC, bool FUSED>
-__global__ void __launch_bounds__(256)
-    k_integrate(SysConst k, DevState d, int midstep, unsigned long long mcount,
-                int rbuf, int interaction, int capture) {
-  extern __shared__ double smem[];
-  const int C = blockDim.x;
-  double *sr = smem;            // positions            3C
-  double *su = sr + 3 * C;      // site orientations    3C
-  double *stn = su + 3 * C;     // tangents             3C
-  double *sfr = stn + 3 * C;    // random forces        3C
-  double *sbF = sfr + 3 * C;    // bond forces / gamma.F 3C
-  double *sbT = sbF + 3 * C;    // bond torques         3C
-  double *scos = sbT + 3 * C;   // cos(theta)           C
-  double *sT = scos + C;        // rhs / tensions       C
-  double *sa = sT + C;          // lower diagonal       C
-  double *sb = sa + C;          // diagonal             C
-  double *sc = sb + C;          // upper diagonal       C
-  double *skeff = sc + C;       // k_eff                C
-  double *sdt = skeff + C;      // det_t                2C
-  double *sdb = sdt + 2 * C;    // det_b                2C
-  int *sflag = (int *)(sdb + 2 * C);
-  __shared__ double s_drmax[32];
-
-#define V(arr, slot, comp) arr[(comp) * C + (slot)]
-
-  const int blk = blockIdx.x;
-  const int t = threadIdx.x;
-  const int s0 = d.blk_site0[blk];
-  const int count = d.blk_site0[blk + 1] - s0;
-  const bool active = t < count;
-  const int g = s0 + t;
-  int f = 0, n = 0, j = -1, base = 0, dbase = 0, lf = 0;
-  if (active) {
-    f = d.site_fil[g];
-    int fs0 = d.f_site_off[f];
-    n = d.f_site_off[f + 1] - fs0;
-    j = g - fs0;
-    base = t - j;
-    lf = f - d.blk_f0[blk];
-    dbase = base + lf;
-  }
-  if (t < C) sflag[t] = 0;
-  const int b = g - f;  // this thread's bond (valid when j < n-1)
-  const bool has_bond = active && j < n - 1;
-  double l = 0, linv = 0, kappa = 0, gpar = 1, gperp = 1, spar = 0, sperp = 0;
-  if (active) {
-    l = d.f_l[f];
-    linv = d.f_linv[f];
-    kappa = d.f_kappa[f];
-    gpar = d.f_gpar[f];
-    gperp = d.f_gperp[f];
-    spar = d.f_spar[f];
-    sperp = d.f_sperp[f];
-  }
-
-  // ---- P0: positions, orientations, bond forces --------------------------
-  double r[3] = {0, 0, 0};
-  if (active) {
-    r[0] = d.r[0][g];
-    r[1] = d.r[1][g];
-    r[2] = d.r[2][g];
-    V(sr, t, 0) = r[0];
-    V(sr, t, 1) = r[1];
-    V(sr, t, 2) = r[2];
-  }
-  double bF[3] = {0, 0, 0}, bT[3] = {0, 0, 0};
-  if (has_bond && interaction) {
-    if (FUSED) {
-      if (PREC == 0) bond_pairs_f64<ND>(k, d, b, rbuf, bF, bT);
-      else bond_pairs_f32<ND>(k, d, b, rbuf, bF, bT);
-    } else {
-      for (int i = 0; i < 3; ++i) {
-        bF[i] = d.bF[i][b];
-        bT[i] = d.bT[i][b];
-      }
-    }
-  }
-  if (has_bond) {
-    for (int i = 0; i < 3; ++i) {
-      V(sbF, t, i) = bF[i];
-      V(sbT, t, i) = bT[i];
-    }
-  }
-  __syncthreads();
-  // Site orientation = orientation of its bond (Mesh::UpdateSiteOrientations,
-  // src/mesh.cpp:168-173), recomputed as Bond::ReInit does.
-  double u[3] = {0, 0, 0};
-  if (has_bond) {
-    double r2[3] = {V(sr, t + 1, 0), V(sr, t + 1, 1), V(sr, t + 1, 2)};
-    double len = 0;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      u[i] = r2[i] - r[i];
-      len += u[i] * u[i];
-    }
-    len = sqrt(len);
-#pragma unroll
-    for (int i = 0; i < ND; ++i) u[i] /= len;
-    for (int i = 0; i < 3; ++i) V(su, t, i) = u[i];
-  }
-  __syncthreads();
-  if (active && j == n - 1) {
-    for (int i = 0; i < 3; ++i) {
-      u[i] = V(su, t - 1, i);
-      V(su, t, i) = u[i];
-    }
-  }
-  __syncthreads();
-
-  // ---- P1: ApplyInteractionForces (src/filament.cpp:992-1048) -------------
-  double F[3] = {0.0, 0.0, 0.0};
-  if (active) {
-    const double mag = 0.5 * 0.0 * l;  // driving_factor 0, from bond centre
-    if (j >= 1) {  // this site is site i+1 of bond i = j-1
-      double up[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
-      double fb[3] = {V(sbF, t - 1, 0), V(sbF, t - 1, 1), V(sbF, t - 1, 2)};
-      double tb[3] = {V(sbT, t - 1, 0), V(sbT, t - 1, 1), V(sbT, t - 1, 2)};
-      double pt[3], sf[3];
-      cross3(up, tb, pt);
-#pragma unroll
-      for (int i = 0; i < ND; ++i) {
-        pt[i] *= linv;
-        sf[i] = 0.5 * fb[i];
-      }
-#pragma unroll
-      for (int i = 0; i < ND; ++i) pt[i] *= -1;
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += sf[i];
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += pt[i];
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += mag * up[i];
-    }
-    if (j <= n - 2) {  // site i of bond i = j
-      double pt[3], sf[3];
-      cross3(u, bT, pt);  // bF/bT hold this thread's bond
-#pragma unroll
-      for (int i = 0; i < ND; ++i) {
-        pt[i] *= linv;
-        sf[i] = 0.5 * bF[i];
-      }
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += sf[i];
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += pt[i];
-#pragma unroll
-      for (int i = 0; i < ND; ++i) F[i] += mag * u[i];
-    }
-  }
-  // CalculateAngles (:430-437), CalculateTangents (:439-443, Site::CalcTangent)
-  double tn[3] = {0, 0, 0};
-  if (active) {
-    if (j < n - 2) {
-      double un[3] = {V(su, t + 1, 0), V(su, t + 1, 1), V(su, t + 1, 2)};
-      scos[t] = dotn<ND>(u, un);
-    }
-    if (j == 0 || j == n - 1) {
-      tn[0] = u[0];
-      tn[1] = u[1];
-      tn[2] = u[2];
-    } else {
-      double mag = 0.0;
-#pragma unroll
-      for (int i = 0; i < ND; ++i) {
-        tn[i] = V(su, t - 1, i) + u[i];
-      }
-#pragma unroll
-      for (int i = 0; i < ND; ++i) mag += tn[i] * tn[i];
-      mag = sqrt(mag);
-#pragma unroll
-      for (int i = 0; i < ND; ++i) tn[i] /= mag;
-    }
-    for (int i = 0; i < 3; ++i) V(stn, t, i) = tn[i];
-  }
-  __syncthreads();
-
-  // ---- P2: random forces, projection, previous positions -----------------
-  double fr[3] = {0, 0, 0}, rp[3] = {0, 0, 0};
-  if (midstep) {
-    if (active) rp[0] = r[0], rp[1] = r[1], rp[2] = r[2];
-    if (k.stoch) {
-      if (active) {  // ConstructUnprojectedRandomForces (:518-548)
-        double xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
-        unsigned long long k0 = (mcount * (unsigned long long)n + j) * ND;
-#pragma unroll
-        for (int i = 0; i < ND; ++i)
-          xi[i] = sc_host_philox_uniform(k.seed, (uint32_t)f, k0 + i) - 0.5;
-        if (ND == 2) {
-          xt[0] = tn[0] * tn[0] * xi[0] + tn[0] * tn[1] * xi[1];
-          xt[1] = tn[1] * tn[1] * xi[1] + tn[0] * tn[1] * xi[0];
-        } else {
-          xt[0] = tn[0] * tn[0] * xi[0] + tn[0] * tn[1] * xi[1] +
-                  tn[0] * tn[2] * xi[2];
-          xt[1] = tn[1] * tn[1] * xi[1] + tn[0] * tn[1] * xi[0] +
-                  tn[1] * tn[2] * xi[2];
-          xt[2] = tn[2] * tn[2] * xi[2] + tn[0] * tn[2] * xi[0] +
-                  tn[1] * tn[2] * xi[1];
-        }
-#pragma unroll
-        for (int i = 0; i < ND; ++i) fr[i] = sperp * xi[i] + (spar - sperp) * xt[i];
-        for (int i = 0; i < 3; ++i) V(sfr, t, i) = fr[i];
-      }
-      __syncthreads();
-      // GeometricallyProjectRandomForces (:550-599)
-      if (has_bond) {
-        double tmp[3];
-#pragma unroll
-        for (int i = 0; i < ND; ++i) tmp[i] = V(sfr, t + 1, i) - fr[i];
-        sT[t] = dotn<ND>(tmp, u);
-        sb[t] = 2;
-        if (j > 0) {
-          sc[t - 1] = -scos[t - 1];
-          sa[t - 1] = -scos[t - 1];
-        }
-      }
-      __syncthreads();
-      if (active && j == 0) thomas(sa + t, sb + t, sc + t, sT + t, n - 1);
-      __syncthreads();
-      if (active) {
-        double fp[3];
-        if (j == 0) {
-#pragma unroll
-          for (int i = 0; i < ND; ++i) fp[i] = fr[i] + sT[t] * u[i];
-        } else if (j == n - 1) {
-#pragma unroll
-          for (int i = 0; i < ND; ++i) fp[i] = fr[i] - sT[t - 1] * V(su, t - 1, i);
-        } else {
-#pragma unroll
-          for (int i = 0; i < ND; ++i)
-            fp[i] = fr[i] + sT[t] * u[i] - sT[t - 1] * V(su, t - 1, i);
-        }
-#pragma unroll
-        for (int i = 0; i < ND; ++i) fr[i] = fp[i];
-      }
-    }
-  } else if (active) {
-    rp[0] = d.rp[0][g];
-    rp[1] = d.rp[1][g];
-    rp[2] = d.rp[2][g];
-    if (k.stoch) {
-      fr[0] = d.fr[0][g];
-      fr[1] = d.fr[1][g];
-      fr[2] = d.fr[2][g];
-    }
-  }
-  // AddRandomForces (:601-606)
-  if (active && k.stoch) {
-#pragma unroll
-    for (int i = 0; i < ND; ++i) F[i] += fr[i];
-  }
-
-  // ---- P3: bending and metric forces (:608-776) ---------------------------
-  if (active && j == 0) {
-    double *dt = sdt + dbase;
-    dt[0] = 1;
-    dt[1] = 2;
-    for (int i = 2; i < n; ++i)
-      dt[i] = 2 * dt[i - 1] - (-scos[t + i - 2]) * (-scos[t + i - 2]) * dt[i - 2];
-  }
-  if (active && j == 1) {
-    double *db = sdb + dbase;  // the filament's det_b[0]
-    db[n] = 1;
-    db[n - 1] = 2;
-    const int tb0 = t - 1;  // slot of the filament's first site
-    for (int i = 2; i < n; ++i)
-      db[n - i] = 2 * db[n - i + 1] -
-                  (-scos[tb0 + n - i - 1]) * (-scos[tb0 + n - i - 1]) * db[n - i + 2];
-  }
-  __syncthreads();
-  if (active && j < n - 2) {
-    const double det_g = sdt[dbase + n - 1];
-    double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] / det_g;
-    skeff[t] = (kappa + l * ginv) / (l * l);
-  }
-  __syncthreads();
-  if (active) {
-    double fs[3] = {0, 0, 0};
-    const int kk = j;
-    if (ND == 2) {
-      if (kk > 1) {
-        double u1[3] = {V(su, t - 2, 0), V(su, t - 2, 1), 0};
-        double u2[3] = {V(su, t - 1, 0), V(su, t - 1, 1), 0};
-        double ke = skeff[t - 2];
-        fs[0] += ke * ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1]);
-        fs[1] += ke * ((1 - u2[1] * u2[1]) * u1[1] - u2[0] * u2[1] * u1[0]);
-      }
-      if (kk > 0 && kk < n - 1) {
-        double u1[3] = {V(su, t - 1, 0), V(su, t - 1, 1), 0};
-        double u2[3] = {u[0], u[1], 0};
-        double ke = skeff[t - 1];
-        fs[0] += ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1] -
-                       ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1]));
-        fs[1] += ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[0] * u1[1] * u2[0] -
-                       ((1 - u2[1] * u2[1]) * u1[1] - u2[0] * u2[1] * u1[0]));
-      }
-      if (kk < n - 2) {
-        double u1[3] = {u[0], u[1], 0};
-        double u2[3] = {V(su, t + 1, 0), V(su, t + 1, 1), 0};
-        double ke = skeff[t];
-        fs[0] -= ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1]);
-        fs[1] -= ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[0] * u1[1] * u2[0]);
-      }
-    } else {
-      if (kk > 1) {
-        double u1[3] = {V(su, t - 2, 0), V(su, t - 2, 1), V(su, t - 2, 2)};
-        double u2[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
-        double ke = skeff[t - 2];
-        fs[0] += ke * ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1] -
-                       u2[0] * u2[2] * u1[2]);
-        fs[1] += ke * ((1 - u2[1] * u2[1]) * u1[1] - u2[1] * u2[0] * u1[0] -
-                       u2[1] * u2[2] * u1[2]);
-        fs[2] += ke * ((1 - u2[2] * u2[2]) * u1[2] - u2[2] * u2[0] * u1[0] -
-                       u2[2] * u2[1] * u1[1]);
-      }
-      if (kk > 0 && kk < n - 1) {
-        double u1[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
-        const double *u2 = u;
-        double ke = skeff[t - 1];
-        fs[0] += ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1] -
-                       u1[0] * u1[2] * u2[2] -
-                       ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1] -
-                        u2[0] * u2[2] * u1[2]));
-        fs[1] += ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[1] * u1[0] * u2[0] -
-                       u1[1] * u1[2] * u2[2] -
-                       ((1 - u2[1] * u2[1]) * u1[1] - u2[1] * u2[0] * u1[0] -
-                        u2[1] * u2[2] * u1[2]));
-        fs[2] += ke * ((1 - u1[2] * u1[2]) * u2[2] - u1[2] * u1[0] * u2[0] -
-                       u1[2] * u1[1] * u2[1] -
-                       ((1 - u2[2] * u2[2]) * u1[2] - u2[2] * u2[0] * u1[0] -
-                        u2[1] * u2[2] * u1[1]));
-      }
-      if (kk < n - 2) {
-        const double *u1 = u;
-        double u2[3] = {V(su, t + 1, 0), V(su, t + 1, 1), V(su, t + 1, 2)};
-        double ke = skeff[t];
-        fs[0] -= ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1] -
-                       u1[0] * u1[2] * u2[2]);
-        fs[1] -= ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[1] * u1[0] * u2[0] -
-                       u1[1] * u1[2] * u2[2]);
-        fs[2] -= ke * ((1 - u1[2] * u1[2]) * u2[2] - u1[2] * u1[0] * u2[0] -
-                       u1[2] * u1[1] * u2[1]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < ND; ++i) F[i] += fs[i];
-  }
-
-  // ---- P4: tensions (:778-838) --------------------------------------------
-  double gam[9];
-  if (active) {
-    int gi = 0;
-#pragma unroll
-    for (int a = 0; a < ND; ++a)
-#pragma unroll
-      for (int c = 0; c < ND; ++c) {
-        gam[gi] = 1.0 / gpar * (tn[a] * tn[c]) +
-                  1.0 / gperp * ((a == c ? 1 : 0) - tn[a] * tn[c]);
-        gi++;
-      }
-    // gamma^-1 F of this site: "temp_a" of row j and "temp_b" of row j-1.
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      double v = gam[ND * i] * F[0] + gam[ND * i + 1] * F[1];
-      if (ND == 3) v += gam[ND * i + 2] * F[2];
-      V(sbF, t, i) = v;
-    }
-  }
-  __syncthreads();
-  if (has_bond) {
-    double fdiff[3];
-#pragma unroll
-    for (int i = 0; i < ND; ++i) fdiff[i] = V(sbF, t + 1, i) - V(sbF, t, i);
-    sT[t] = dotn<ND>(u, fdiff);
-    double tn2[3] = {V(stn, t + 1, 0), V(stn, t + 1, 1), V(stn, t + 1, 2)};
-    double d1 = dotn<ND>(tn, u);
-    double d2 = dotn<ND>(tn2, u);
-    sb[t] = 2.0 / gperp + (1.0 / gpar - 1.0 / gperp) * (d1 * d1 + d2 * d2);
-    if (j > 0) {
-      double u1[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
-      double hu = -1.0 / gperp * dotn<ND>(u, u1) -
-                  (1.0 / gpar - 1.0 / gperp) * (dotn<ND>(tn, u1) * dotn<ND>(tn, u));
-      sc[t - 1] = hu;
-      sa[t - 1] = hu;
-    }
-  }
-  __syncthreads();
-  if (active && j == 0) thomas(sa + t, sb + t, sc + t, sT + t, n - 1);
-  __syncthreads();
-
-  // ---- P5: UpdateSitePositions (:840-927), CheckBondLengths (:934-951) ----
-  if (active) {
-    double fs[3];
-    if (j == 0) {
-#pragma unroll
-      for (int i = 0; i < ND; ++i) fs[i] = sT[t] * u[i];
-    } else if (j == n - 1) {
-#pragma unroll
-      for (int i = 0; i < ND; ++i) fs[i] = -sT[t - 1] * V(su, t - 1, i);
-    } else {
-#pragma unroll
-      for (int i = 0; i < ND; ++i) fs[i] = sT[t] * u[i] - sT[t - 1] * V(su, t - 1, i);
-    }
-#pragma unroll
-    for (int i = 0; i < ND; ++i) F[i] += fs[i];
-    const double dl = (midstep ? 0.5 * k.delta : k.delta);
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      double ft = gam[ND * i] * F[0] + gam[ND * i + 1] * F[1];
-      if (ND == 3) ft += gam[ND * i + 2] * F[2];
-      r[i] = rp[i] + dl * ft;
-    }
-  }
-  __syncthreads();  // everyone is done reading su / sr of the old state
-  if (active) {
-    for (int i = 0; i < 3; ++i) V(sr, t, i) = r[i];
-  }
-  __syncthreads();
-  if (has_bond) {
-    double rd[3], um = 0.0;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      rd[i] = V(sr, t + 1, i) - r[i];
-      um += rd[i] * rd[i];
-    }
-    um = sqrt(um);
-#pragma unroll
-    for (int i = 0; i < ND; ++i) V(su, t, i) = rd[i] / um;
-  }
-  if (active && j >= 1) {
-    double a = 0.0;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      double temp = r[i] - V(sr, t - 1, i);
-      a += temp * temp;
-    }
-    a = sqrt(a);
-    double err = dabs(l - a) / l;
-    if (err > 1e-3) sflag[lf] = 1;
-  }
-  __syncthreads();
-  if (active && j == 0) {
-    int sw = d.f_switch[f], nn = d.f_nnorm[f];
-    if (sflag[lf]) {
-      sw = !sw;
-      nn = 0;
-      if (sw) {
-        for (int jj = 1; jj < n; ++jj)
-#pragma unroll
-          for (int i = 0; i < ND; ++i)
-            V(sr, t + jj, i) = V(sr, t + jj - 1, i) + l * V(su, t + jj - 1, i);
-      } else {
-        for (int jj = n - 1; jj > 0; --jj)
-#pragma unroll
-          for (int i = 0; i < ND; ++i)
-            V(sr, t + jj - 1, i) = V(sr, t + jj, i) - l * V(su, t + jj - 1, i);
-      }
-    }
-    nn++;
-    d.f_switch[f] = sw;
-    d.f_nnorm[f] = nn;
-  }
-  __syncthreads();
-
-  // ---- P6: bond geometry (Mesh::UpdateBondPositions), state write-back ----
-  double my_dr = 0.0;
-  if (active) {
-    for (int i = 0; i < 3; ++i) r[i] = V(sr, t, i);
-    if (has_bond) {
-      double r2[3] = {V(sr, t + 1, 0), V(sr, t + 1, 1), V(sr, t + 1, 2)};
-      double s[3], ub[3], len;
-      bond_from_sites<ND>(k, r, r2, s, ub, len);
-      store_geom<ND>(d, 1 - rbuf, b, s, ub, len, PREC);
-    }
-    d.r[0][g] = r[0];
-    d.r[1][g] = r[1];
-    d.r[2][g] = r[2];
-    if (midstep) {
-      d.rp[0][g] = rp[0];
-      d.rp[1][g] = rp[1];
-      d.rp[2][g] = rp[2];
-      if (k.stoch) {
-        d.fr[0][g] = fr[0];
-        d.fr[1][g] = fr[1];
-        d.fr[2][g] = fr[2];
-      }
-    }
-    bool bad = false;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) bad |= !isfinite(r[i]);
-    if (bad) atomicOr(d.status, ST_NAN);
-    if (capture) {
-      for (int i = 0; i < 3; ++i) d.cap_F[i][g] = F[i];
-      if (has_bond) d.cap_T[b] = sT[t];
-    }
-    // Displacement tracking for the next query (Mesh::UpdateDrTot runs on
-    // the filaments whose last update was a full step; each query adds the
-    // squared displacement twice, src/mesh.cpp:538-541, src/object.cpp:
-    // 282-292).
-    if (!midstep && interaction) {
-      double acc = d.dt[g];
-      for (int twice = 0; twice < 2; ++twice)
-#pragma unroll
-        for (int i = 0; i < ND; ++i) {
-          double dr = r[i] - d.dz[i][g];
-          acc += dr * dr;
-        }
-      d.dt[g] = acc;
-      my_dr = acc;
-    }
-  }
-  if (!midstep && interaction) {
-    // Block max, then one atomic per block on the IEEE bits (non-negative).
-    double v = my_dr;
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    if ((t & 31) == 0) s_drmax[t >> 5] = v;
-    __syncthreads();
-    if (t < 32) {
-      v = (t < (C + 31) / 32) ? s_drmax[t] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-      if (t == 0) {
-        if (!(v <= 1e300)) atomicOr(d.status, ST_NAN);
-        atomicMax(d.dr_max_bits, (unsigned long long)__double_as_longlong(v));
-      }
-    }
-  }
-#undef V
 }
 
 // ---------------------------------------------------------------------------
@@ -1191,14 +552,66 @@ int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
   return 1;
 }
 
-int launch_csr(const DevState &d, int np, int *deg, cudaStream_t st) {
-  int n = 0;
-  if (np > 0) {
-    k_csr_fill<<<cdiv(np, 256), 256, 0, st>>>(d, np, deg);
-    ++n;
-  }
+int launch_csr(const DevState &d, int cap, int *deg, cudaStream_t st) {
+  k_csr_fill<<<cdiv(cap > 0 ? cap : 1, 256), 256, 0, st>>>(d, cap, deg);
   k_csr_sort<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
-  return n + 1;
+  k_csr_pos<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
+  return 3;
+}
+
+// ---------------------------------------------------------------------------
+// Device-side control of captured step graphs.
+
+// Interact's rebuild check on the device (CheckUpdateInteractions + GetDrMax,
+// src/interaction_manager.cpp:284-312, include/simcore/species.hpp:114-118):
+// sets the IF condition of the rebuild body; above 10000 the reference
+// throws, here the status word records it and no rebuild runs.
+__global__ void k_decide(SysConst k, DevState d, cudaGraphConditionalHandle h) {
+  double dr = __longlong_as_double((long long)*d.dr_max_bits);
+  unsigned cond = 0;
+  if (dr > 10000.0 || !(dr == dr)) atomicOr(d.status, ST_UNPHYSICAL);
+  else cond = dr > k.dr_update ? 1u : 0u;
+  cudaGraphSetConditional(h, cond);
+}
+
+__global__ void k_loop_head(DevState d, cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, *d.loop_count > 0 ? 1u : 0u);
+}
+
+// End of one BD step (midstep + full step) of a graph loop: advances the
+// noise counter and decrements the remaining count.  A recorded error stops
+// the loop.
+__global__ void k_loop_tail(DevState d, int stoch, cudaGraphConditionalHandle h) {
+  if (stoch) *d.mcount += 1ull;
+  int left = *d.loop_count - 1;
+  if (*d.status != 0u) left = 0;
+  *d.loop_count = left;
+  cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
+}
+
+__global__ void k_advance_mcount(DevState d) { *d.mcount += 1ull; }
+
+int launch_decide(const SysConst &k, const DevState &d,
+                  cudaGraphConditionalHandle h, cudaStream_t st) {
+  k_decide<<<1, 1, 0, st>>>(k, d, h);
+  return 1;
+}
+
+int launch_loop_head(const DevState &d, cudaGraphConditionalHandle h,
+                     cudaStream_t st) {
+  k_loop_head<<<1, 1, 0, st>>>(d, h);
+  return 1;
+}
+
+int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
+                     cudaStream_t st) {
+  k_loop_tail<<<1, 1, 0, st>>>(d, stoch, h);
+  return 1;
+}
+
+int launch_advance_mcount(const DevState &d, cudaStream_t st) {
+  k_advance_mcount<<<1, 1, 0, st>>>(d);
+  return 1;
 }
 
 int launch_zero_dr(const DevState &d, cudaStream_t st) {
@@ -1207,62 +620,81 @@ int launch_zero_dr(const DevState &d, cudaStream_t st) {
 }
 
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
-                 cudaStream_t st) {
-  int grid = cdiv(d.nb, 128);
+                 int expected, cudaStream_t st) {
+  int grid = cdiv(expected > 0 ? expected : 1, 256);
   if (k.n_dim == 3) {
-    if (prec == 0) k_pairs<3, 0><<<grid, 128, 0, st>>>(k, d, rbuf);
-    else k_pairs<3, 1><<<grid, 128, 0, st>>>(k, d, rbuf);
+    if (prec == 0) k_pair_eval<3, 0><<<grid, 256, 0, st>>>(k, d, rbuf);
+    else k_pair_eval<3, 1><<<grid, 256, 0, st>>>(k, d, rbuf);
   } else {
-    if (prec == 0) k_pairs<2, 0><<<grid, 128, 0, st>>>(k, d, rbuf);
-    else k_pairs<2, 1><<<grid, 128, 0, st>>>(k, d, rbuf);
+    if (prec == 0) k_pair_eval<2, 0><<<grid, 256, 0, st>>>(k, d, rbuf);
+    else k_pair_eval<2, 1><<<grid, 256, 0, st>>>(k, d, rbuf);
+  }
+  return 1;
+}
+
+int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st) {
+  int grid = cdiv(d.nb, 256);
+  if (k.n_dim == 3) {
+    if (prec == 0) k_bond_sum<3, 0><<<grid, 256, 0, st>>>(d);
+    else k_bond_sum<3, 1><<<grid, 256, 0, st>>>(d);
+  } else {
+    if (prec == 0) k_bond_sum<2, 0><<<grid, 256, 0, st>>>(d);
+    else k_bond_sum<2, 1><<<grid, 256, 0, st>>>(d);
   }
   return 1;
 }
 
 size_t integrate_smem_bytes(int C) {
-  return sizeof(double) * 28 * (size_t)C + sizeof(int) * (size_t)C;
+  // (shared by both integrator units)
+  return sizeof(double) * integrate_smem_doubles(C) + sizeof(FilConst) * (size_t)(C / 2) +
+         sizeof(int) * (size_t)(C / 2);
 }
 
-template <int ND, int PREC, bool FUSED>
+template <int ND, int PREC, int MAXC>
 static void set_attr(size_t smem) {
-  cudaFuncSetAttribute(k_integrate<ND, PREC, FUSED>,
+  cudaFuncSetAttribute(k_integrate<ND, PREC, false, MAXC>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 void prepare_integrate(int C) {
   size_t smem = integrate_smem_bytes(C);
-  set_attr<3, 0, false>(smem);
-  set_attr<3, 0, true>(smem);
-  set_attr<3, 1, false>(smem);
-  set_attr<3, 1, true>(smem);
-  set_attr<2, 0, false>(smem);
-  set_attr<2, 0, true>(smem);
-  set_attr<2, 1, false>(smem);
-  set_attr<2, 1, true>(smem);
+  if (C <= 128) {
+    set_attr<3, 0, 128>(smem);
+    set_attr<3, 1, 128>(smem);
+    set_attr<2, 0, 128>(smem);
+    set_attr<2, 1, 128>(smem);
+  } else {
+    set_attr<3, 0, 256>(smem);
+    set_attr<3, 1, 256>(smem);
+    set_attr<2, 0, 256>(smem);
+    set_attr<2, 1, 256>(smem);
+  }
+  prepare_integrate_fast(C);
 }
 
 int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
-                     int midstep, unsigned long long mcount, int rbuf,
-                     int interaction, int capture, int prec, bool fused,
-                     cudaStream_t st) {
+                     int midstep, int rbuf, int interaction, int capture,
+                     int prec, bool fast, cudaStream_t st) {
+  if (fast && prec == 1)
+    return launch_integrate_fast(k, d, nblocks, C, midstep, rbuf, interaction, capture, st);
   size_t smem = integrate_smem_bytes(C);
-#define SC_LAUNCH(ND, P, FU)                                                   \
-  k_integrate<ND, P, FU><<<nblocks, C, smem, st>>>(k, d, midstep, mcount, rbuf, \
-                                                    interaction, capture)
-  if (k.n_dim == 3) {
-    if (prec == 0) {
-      if (fused) SC_LAUNCH(3, 0, true); else SC_LAUNCH(3, 0, false);
+#define SC_INTEGRATE(ND, P, MC)                                              \
+  k_integrate<ND, P, false, MC><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, \
+                                                          interaction, capture)
+  if (C <= 128) {
+    if (k.n_dim == 3) {
+      if (prec == 0) SC_INTEGRATE(3, 0, 128); else SC_INTEGRATE(3, 1, 128);
     } else {
-      if (fused) SC_LAUNCH(3, 1, true); else SC_LAUNCH(3, 1, false);
+      if (prec == 0) SC_INTEGRATE(2, 0, 128); else SC_INTEGRATE(2, 1, 128);
     }
   } else {
-    if (prec == 0) {
-      if (fused) SC_LAUNCH(2, 0, true); else SC_LAUNCH(2, 0, false);
+    if (k.n_dim == 3) {
+      if (prec == 0) SC_INTEGRATE(3, 0, 256); else SC_INTEGRATE(3, 1, 256);
     } else {
-      if (fused) SC_LAUNCH(2, 1, true); else SC_LAUNCH(2, 1, false);
+      if (prec == 0) SC_INTEGRATE(2, 0, 256); else SC_INTEGRATE(2, 1, 256);
     }
   }
-#undef SC_LAUNCH
+#undef SC_INTEGRATE
   return 1;
 }
 

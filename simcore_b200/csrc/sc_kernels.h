@@ -27,15 +27,28 @@ int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      const int *sorted, const int *cell_start,
                      const int *pair_off, int cap, int *deg, int prec,
                      cudaStream_t st);
-int launch_csr(const DevState &d, int np, int *deg, cudaStream_t st);
+int launch_csr(const DevState &d, int cap, int *deg, cudaStream_t st);
+int launch_decide(const SysConst &k, const DevState &d,
+                  cudaGraphConditionalHandle h, cudaStream_t st);
+int launch_loop_head(const DevState &d, cudaGraphConditionalHandle h,
+                     cudaStream_t st);
+int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
+                     cudaStream_t st);
+int launch_advance_mcount(const DevState &d, cudaStream_t st);
 int launch_zero_dr(const DevState &d, cudaStream_t st);
+// Grid sized for `expected` pairs; the kernel strides over the actual count.
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
-                 cudaStream_t st);
+                 int expected, cudaStream_t st);
+int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st);
 size_t integrate_smem_bytes(int C);
 void prepare_integrate(int C);
+// fast: the contraction/reciprocal variant (mixed precision only).
 int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
-                     int midstep, unsigned long long mcount, int rbuf,
-                     int interaction, int capture, int prec, bool fused,
-                     cudaStream_t st);
+                     int midstep, int rbuf, int interaction, int capture,
+                     int prec, bool fast, cudaStream_t st);
+void prepare_integrate_fast(int C);
+int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int C,
+                          int midstep, int rbuf, int interaction, int capture,
+                          cudaStream_t st);
 
 }  // namespace sc

@@ -1,0 +1,50 @@
+// Fast variant of the integrator for the mixed-precision step, compiled with
+// --fmad=true: the algorithm of sc_step.cuh with FMA contraction, one
+// reciprocal per shared denominator and rsqrt normalisation.  FP64
+// throughout; not bit-identical to the reference (differences at the level
+// of FP64 rounding), which the mixed path does not claim.
+#include <cuda_runtime.h>
+
+#include "sc_common.cuh"
+#include "sc_kernels.h"
+#include "sc_pair.cuh"
+#include "sc_step.cuh"
+
+namespace sc {
+
+template <int ND, int MAXC>
+static void set_attr_fast(size_t smem) {
+  cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+void prepare_integrate_fast(int C) {
+  size_t smem = integrate_smem_bytes(C);
+  if (C <= 128) {
+    set_attr_fast<3, 128>(smem);
+    set_attr_fast<2, 128>(smem);
+  } else {
+    set_attr_fast<3, 256>(smem);
+    set_attr_fast<2, 256>(smem);
+  }
+}
+
+int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int C,
+                          int midstep, int rbuf, int interaction, int capture,
+                          cudaStream_t st) {
+  size_t smem = integrate_smem_bytes(C);
+  if (C <= 128) {
+    if (k.n_dim == 3)
+      k_integrate<3, 1, true, 128><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
+    else
+      k_integrate<2, 1, true, 128><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
+  } else {
+    if (k.n_dim == 3)
+      k_integrate<3, 1, true, 256><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
+    else
+      k_integrate<2, 1, true, 256><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
+  }
+  return 1;
+}
+
+}  // namespace sc

@@ -1,0 +1,777 @@
+// Integrator of the filament step and the device helpers it shares with the
+// rest of the pipeline, as a header compiled by two units:
+//   sc_kernels.cu      (--fmad=false): FAST = false, the reference's exact
+//                      arithmetic, bit-identical to it;
+//   sc_kernels_fast.cu (--fmad=true):  FAST = true, the same algorithm with
+//                      contraction, one reciprocal per shared denominator and
+//                      rsqrt normalisation (mixed precision only).
+#pragma once
+
+#include "sc_common.cuh"
+#include "sc_pair.cuh"
+
+namespace sc {
+
+// ---------------------------------------------------------------------------
+// Bond geometry from two sites: Bond::ReInit (src/bond.cpp:22-37) followed by
+// Object::UpdatePeriodic / periodic_boundary_conditions
+// (src/object.cpp:202-210, src/linear_algebra.cpp:100-117).
+template <int ND>
+__device__ __forceinline__ void bond_from_sites(const SysConst &k,
+                                                const double *r1,
+                                                const double *r2, double s[3],
+                                                double u[3], double &len) {
+  double pos[3] = {0, 0, 0};
+  u[0] = u[1] = u[2] = 0.0;
+  s[0] = s[1] = s[2] = 0.0;
+  len = 0;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    u[i] = r2[i] - r1[i];
+    len += u[i] * u[i];
+  }
+  len = sqrt(len);
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    pos[i] = r1[i] + 0.5 * u[i];
+    u[i] /= len;
+  }
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    s[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) s[i] += k.hinv[ND * i + j] * pos[j];
+    s[i] -= nint(s[i]);
+  }
+}
+
+__device__ __forceinline__ int32_t to_fixed(double s) {
+  // s in [-1/2, 1/2]: round(s * 2^32) wraps into int32 (1/2 and -1/2 map to
+  // the same point of the periodic box).
+  long long q = __double2ll_rn(s * 4294967296.0);
+  return (int32_t)(uint32_t)(unsigned long long)q;
+}
+
+template <int ND>
+__device__ __forceinline__ void store_geom(const DevState &d, int buf, int b,
+                                           const double s[3],
+                                           const double u[3], double len,
+                                           int prec) {
+  if (prec == 0) {
+    BondGeomF64 g;
+    g.s[0] = s[0];
+    g.s[1] = s[1];
+    g.s[2] = s[2];
+    g.u[0] = u[0];
+    g.u[1] = u[1];
+    g.u[2] = u[2];
+    g.len = len;
+    g.pad = 0.0;
+    d.g64[buf][b] = g;
+  } else {
+    BondGeomF32 g;
+    g.q[0] = to_fixed(s[0]);
+    g.q[1] = to_fixed(s[1]);
+    g.q[2] = ND == 3 ? to_fixed(s[2]) : 0;
+    g.hl = (float)(0.5 * len);
+    g.u[0] = (float)u[0];
+    g.u[1] = (float)u[1];
+    g.u[2] = (float)u[2];
+    g.pad = 0.f;
+    d.g32[buf][b] = g;
+  }
+}
+
+__device__ __forceinline__ void cross3(const double *a, const double *b,
+                                       double *c) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+__device__ __forceinline__ void kahan_add(float &sum, float &comp, float x) {
+  float y = x - comp;
+  float t = sum + y;
+  comp = (t - sum) - y;
+  sum = t;
+}
+
+// Sum of one bond's pair contributions in slot (= pair) order: FP64 sums as
+// the reference accumulates Object::force_/torque_, FP32 with Kahan
+// compensation.  A slot is 8 values: force (3), torque (3), padding (2).
+template <int ND, int PREC>
+__device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F[3],
+                                              double T[3]) {
+  const int e0 = d.e_off[b], e1 = d.e_off[b + 1];
+  if (PREC == 0) {
+    F[0] = F[1] = F[2] = 0.0;
+    T[0] = T[1] = T[2] = 0.0;
+    const double2 *c = reinterpret_cast<const double2 *>(d.cf64) + 4 * (size_t)e0;
+#pragma unroll 2
+    for (int e = e0; e < e1; ++e, c += 4) {
+      const double2 v0 = c[0], v1 = c[1], v2 = c[2];
+      F[0] += v0.x;
+      F[1] += v0.y;
+      if (ND == 3) F[2] += v1.x;
+      T[0] += v1.y;
+      T[1] += v2.x;
+      T[2] += v2.y;
+    }
+  } else {
+    float sF[3] = {0.f, 0.f, 0.f}, cF[3] = {0.f, 0.f, 0.f};
+    float sT[3] = {0.f, 0.f, 0.f}, cT[3] = {0.f, 0.f, 0.f};
+    const float4 *c = reinterpret_cast<const float4 *>(d.cf32) + 2 * (size_t)e0;
+#pragma unroll 2
+    for (int e = e0; e < e1; ++e, c += 2) {
+      const float4 v0 = c[0], v1 = c[1];
+      kahan_add(sF[0], cF[0], v0.x);
+      kahan_add(sF[1], cF[1], v0.y);
+      if (ND == 3) kahan_add(sF[2], cF[2], v0.z);
+      kahan_add(sT[0], cT[0], v0.w);
+      kahan_add(sT[1], cT[1], v1.x);
+      kahan_add(sT[2], cT[2], v1.y);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      F[i] = (double)sF[i] - (double)cF[i];
+      T[i] = (double)sT[i] - (double)cT[i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Integrator.  A block holds a run of whole filaments, one thread per site,
+// filaments back to back.  Per-site work runs in parallel; the sequential
+// recurrences of one filament (metric determinants, Thomas solves,
+// renormalisation) run on one dedicated lane per filament (lane lf for
+// filament lf of the block, lane C/2 + lf for the backward determinant), so
+// a block's serial work occupies one or two warps instead of every warp.
+
+// Thomas algorithm of the reference's tridiagonal_solver
+// (src/linear_algebra.cpp:164-197); n unknowns, in place.
+__device__ __forceinline__ void thomas(double *a, const double *b, double *c,
+                                       double *d, int n) {
+  n--;
+  c[0] /= b[0];
+  d[0] /= b[0];
+  for (int i = 1; i < n; ++i) {
+    c[i] /= b[i] - a[i - 1] * c[i - 1];
+    d[i] = (d[i] - a[i - 1] * d[i - 1]) / (b[i] - a[i - 1] * c[i - 1]);
+  }
+  d[n] = (d[n] - a[n - 1] * d[n - 1]) / (b[n] - a[n - 1] * c[n - 1]);
+  for (int i = n; i-- > 0;) d[i] -= c[i] * d[i + 1];
+}
+
+// FAST: one reciprocal per row instead of two divisions.
+__device__ __forceinline__ void thomas_fast(double *a, const double *b, double *c,
+                                            double *d, int n) {
+  n--;
+  double r = 1.0 / b[0];
+  c[0] *= r;
+  d[0] *= r;
+  for (int i = 1; i < n; ++i) {
+    r = 1.0 / (b[i] - a[i - 1] * c[i - 1]);
+    c[i] *= r;
+    d[i] = (d[i] - a[i - 1] * d[i - 1]) * r;
+  }
+  d[n] = (d[n] - a[n - 1] * d[n - 1]) / (b[n] - a[n - 1] * c[n - 1]);
+  for (int i = n; i-- > 0;) d[i] -= c[i] * d[i + 1];
+}
+
+template <bool FAST>
+__device__ __forceinline__ void solve_tridiag(double *a, const double *b, double *c,
+                                              double *d, int n) {
+  if (FAST) thomas_fast(a, b, c, d, n);
+  else thomas(a, b, c, d, n);
+}
+
+// v /= |v| over ND components.  Exact: the reference's normalize_vector
+// (src/linear_algebra.cpp:26-35).  FAST: one rsqrt and ND products.
+template <int ND, bool FAST>
+__device__ __forceinline__ double normalize(double *v) {
+  double mag = 0.0;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) mag += v[i] * v[i];
+  if (FAST) {
+    double inv = rsqrt(mag);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) v[i] *= inv;
+    return mag * inv;
+  }
+  mag = sqrt(mag);
+#pragma unroll
+  for (int i = 0; i < ND; ++i) v[i] /= mag;
+  return mag;
+}
+
+template <int ND>
+__device__ __forceinline__ double dotn(const double *a, const double *b) {
+  double m = 0.0;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) m += a[i] * b[i];
+  return m;
+}
+
+// Shared-memory words of one integrator block of C sites.
+__host__ __device__ constexpr size_t integrate_smem_doubles(int C) {
+  return 31 * (size_t)C;
+}
+
+// 8-byte asynchronous global -> shared copy (cp.async), completed by
+// cp_async_wait_all() in the same thread.
+__device__ __forceinline__ void cp_async8(double *smem_dst, const double *gsrc) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc));
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// MAXC: largest block (sites) the instantiation is launched with; blocks
+// per SM requested so that the register budget leaves room for several
+// blocks in flight.
+template <int MAXC>
+struct IntegrateBounds {
+  static constexpr int min_blocks = MAXC <= 128 ? 5 : 2;
+};
+
+template <int ND, int PREC, bool FAST, int MAXC>
+__global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
+    k_integrate(SysConst k, DevState d, int midstep, int rbuf, int interaction,
+                int capture) {
+  extern __shared__ double smem[];
+  const int C = blockDim.x;
+  double *sr = smem;            // positions            3C
+  double *su = sr + 3 * C;      // site orientations    3C
+  double *stn = su + 3 * C;     // tangents             3C
+  double *sfr = stn + 3 * C;    // random forces; bond torques in P0-P1  3C
+  double *sbF = sfr + 3 * C;    // bond forces, then gamma^-1 F          3C
+  double *scos = sbF + 3 * C;   // cos(theta)           C
+  double *sT = scos + C;        // rhs / tensions       C
+  double *sa = sT + C;          // lower diagonal       C
+  double *sb = sa + C;          // diagonal             C
+  double *sc = sb + C;          // upper diagonal       C
+  double *skeff = sc + C;       // k_eff                C
+  double *sdt = skeff + C;      // det_t                2C
+  double *sdb = sdt + 2 * C;    // det_b                2C
+  double *srp = sdb + 2 * C;    // full step: prefetched previous positions 3C
+  double *sfp = srp + 3 * C;    // full step: prefetched projected noise     3C
+  FilConst *sfil = (FilConst *)(sfp + 3 * C);   // C/2 filaments
+  int *sflag = (int *)(sfil + C / 2);           // C/2 renormalisation flags
+  __shared__ double s_drmax[32];
+
+#define V(arr, slot, comp) arr[(comp) * C + (slot)]
+
+  const int blk = blockIdx.x;
+  const int t = threadIdx.x;
+  const unsigned long long mcount = *d.mcount;
+  const int s0 = d.blk_site0[blk];
+  const int count = d.blk_site0[blk + 1] - s0;
+  const int f0 = d.blk_f0[blk];
+  const int nfb = d.blk_nf[blk];
+  if (t < nfb) {
+    sfil[t] = d.fil[f0 + t];
+    sflag[t] = 0;
+  }
+  const bool active = t < count;
+  const int g = s0 + t;
+  int f = 0, lf = 0;
+  if (active) {
+    f = d.site_fil[g];
+    lf = f - f0;
+  }
+  __syncthreads();
+  const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
+  const int n = active ? fc.n : 0;
+  const int j = active ? g - fc.site0 : -1;
+  const int base = t - j;            // slot of the filament's first site
+  const int b = g - f;               // this thread's bond (valid when j < n-1)
+  const bool has_bond = active && j < n - 1;
+
+  // ---- P0: positions, orientations, bond forces --------------------------
+  double r[3] = {0, 0, 0}, u[3] = {0, 0, 0};
+  double bF[3] = {0, 0, 0}, bT[3] = {0, 0, 0};
+  if (active) {
+    r[0] = d.r[0][g];
+    r[1] = d.r[1][g];
+    r[2] = d.r[2][g];
+    if (midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
+      d.rp[0][g] = r[0];
+      d.rp[1][g] = r[1];
+      d.rp[2][g] = r[2];
+    } else {
+      // The full step needs the midstep's positions and projected noise
+      // later; fetch them now, in the background.
+      for (int i = 0; i < ND; ++i) cp_async8(&V(srp, t, i), &d.rp[i][g]);
+      if (k.stoch)
+        for (int i = 0; i < ND; ++i) cp_async8(&V(sfp, t, i), &d.fr[i][g]);
+      cp_async_commit();
+    }
+  }
+  if (has_bond) {
+    // Site orientation = orientation of its bond as Bond::ReInit left it
+    // (Mesh::UpdateSiteOrientations, src/mesh.cpp:168-173).
+    u[0] = d.ub[0][b];
+    u[1] = d.ub[1][b];
+    u[2] = d.ub[2][b];
+    if (interaction) bond_pair_sum<ND, PREC>(d, b, bF, bT);
+    for (int i = 0; i < 3; ++i) {
+      V(su, t, i) = u[i];
+      V(sbF, t, i) = bF[i];
+      V(sfr, t, i) = bT[i];
+    }
+  }
+  __syncthreads();
+  if (active && j == n - 1) {
+    for (int i = 0; i < 3; ++i) u[i] = V(su, t - 1, i);
+  }
+
+  // ---- P1: ApplyInteractionForces (src/filament.cpp:992-1048) -------------
+  double F[3] = {0.0, 0.0, 0.0};
+  if (active) {
+    const double mag = 0.5 * 0.0 * fc.l;  // driving_factor 0, from bond centre
+    if (j >= 1) {  // this site is site i+1 of bond i = j-1
+      double up[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
+      double fb[3] = {V(sbF, t - 1, 0), V(sbF, t - 1, 1), V(sbF, t - 1, 2)};
+      double tb[3] = {V(sfr, t - 1, 0), V(sfr, t - 1, 1), V(sfr, t - 1, 2)};
+      double pt[3], sf[3];
+      cross3(up, tb, pt);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        pt[i] *= fc.linv;
+        sf[i] = 0.5 * fb[i];
+      }
+#pragma unroll
+      for (int i = 0; i < ND; ++i) pt[i] *= -1;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) F[i] += sf[i];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) F[i] += pt[i];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) F[i] += mag * up[i];
+    }
+    if (j <= n - 2) {  // site i of bond i = j (bF/bT hold this bond)
+      double pt[3], sf[3];
+      cross3(u, bT, pt);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        pt[i] *= fc.linv;
+        sf[i] = 0.5 * bF[i];
+      }
+#pragma unroll
+      for (int i = 0; i < ND; ++i) F[i] += sf[i];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) F[i] += pt[i];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) F[i] += mag * u[i];
+    }
+  }
+  // CalculateAngles (:430-437), CalculateTangents (:439-443, Site::CalcTangent)
+  double tn[3] = {0, 0, 0};
+  if (active) {
+    if (j < n - 2) {
+      double un[3] = {V(su, t + 1, 0), V(su, t + 1, 1), V(su, t + 1, 2)};
+      scos[t] = dotn<ND>(u, un);
+    }
+    if (j == 0 || j == n - 1) {
+      tn[0] = u[0];
+      tn[1] = u[1];
+      tn[2] = u[2];
+    } else {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) tn[i] = V(su, t - 1, i) + u[i];
+      normalize<ND, FAST>(tn);
+    }
+    for (int i = 0; i < 3; ++i) V(stn, t, i) = tn[i];
+  }
+  if (active && j == n - 1) {
+    for (int i = 0; i < 3; ++i) V(su, t, i) = u[i];
+  }
+  __syncthreads();
+
+  // ---- P2: random forces, projection, previous positions -----------------
+  double fr[3] = {0, 0, 0};
+  if (midstep) {
+    if (k.stoch) {
+      if (active) {  // ConstructUnprojectedRandomForces (:518-548)
+        uint32_t w[4];
+        sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
+                              k.seed, (uint32_t)f, w);
+        double xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
+#pragma unroll
+        for (int i = 0; i < ND; ++i)
+          xi[i] = ((double)w[i] + 0.5) * 2.3283064365386963e-10 - 0.5;
+        if (ND == 2) {
+          xt[0] = tn[0] * tn[0] * xi[0] + tn[0] * tn[1] * xi[1];
+          xt[1] = tn[1] * tn[1] * xi[1] + tn[0] * tn[1] * xi[0];
+        } else {
+          xt[0] = tn[0] * tn[0] * xi[0] + tn[0] * tn[1] * xi[1] +
+                  tn[0] * tn[2] * xi[2];
+          xt[1] = tn[1] * tn[1] * xi[1] + tn[0] * tn[1] * xi[0] +
+                  tn[1] * tn[2] * xi[2];
+          xt[2] = tn[2] * tn[2] * xi[2] + tn[0] * tn[2] * xi[0] +
+                  tn[1] * tn[2] * xi[1];
+        }
+#pragma unroll
+        for (int i = 0; i < ND; ++i)
+          fr[i] = fc.sperp * xi[i] + (fc.spar - fc.sperp) * xt[i];
+        for (int i = 0; i < 3; ++i) V(sfr, t, i) = fr[i];
+      }
+      __syncthreads();
+      // GeometricallyProjectRandomForces (:550-599)
+      if (has_bond) {
+        double tmp[3];
+#pragma unroll
+        for (int i = 0; i < ND; ++i) tmp[i] = V(sfr, t + 1, i) - fr[i];
+        sT[t] = dotn<ND>(tmp, u);
+        sb[t] = 2;
+        if (j > 0) {
+          sc[t - 1] = -scos[t - 1];
+          sa[t - 1] = -scos[t - 1];
+        }
+      }
+      __syncthreads();
+      if (t < nfb) {
+        const int fb0 = sfil[t].site0 - s0;
+        solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[t].n - 1);
+      }
+      __syncthreads();
+      if (active) {
+        double fp[3];
+        if (j == 0) {
+#pragma unroll
+          for (int i = 0; i < ND; ++i) fp[i] = fr[i] + sT[t] * u[i];
+        } else if (j == n - 1) {
+#pragma unroll
+          for (int i = 0; i < ND; ++i) fp[i] = fr[i] - sT[t - 1] * V(su, t - 1, i);
+        } else {
+#pragma unroll
+          for (int i = 0; i < ND; ++i)
+            fp[i] = fr[i] + sT[t] * u[i] - sT[t - 1] * V(su, t - 1, i);
+        }
+#pragma unroll
+        for (int i = 0; i < ND; ++i) fr[i] = fp[i];
+        d.fr[0][g] = fr[0];  // the projected noise, reused by the full step
+        d.fr[1][g] = fr[1];
+        d.fr[2][g] = fr[2];
+      }
+    }
+  } else if (active) {
+    cp_async_wait_all();
+    if (k.stoch)
+      for (int i = 0; i < ND; ++i) fr[i] = V(sfp, t, i);
+  }
+  // AddRandomForces (:601-606)
+  if (active && k.stoch) {
+#pragma unroll
+    for (int i = 0; i < ND; ++i) F[i] += fr[i];
+  }
+
+  // ---- P3: bending and metric forces (:608-776) ---------------------------
+  if (t < nfb) {  // det_t of filament t, forward
+    const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
+    double *dt = sdt + fb0 + t;
+    const double *cs = scos + fb0;
+    dt[0] = 1;
+    dt[1] = 2;
+    for (int i = 2; i < nn; ++i) dt[i] = 2 * dt[i - 1] - (-cs[i - 2]) * (-cs[i - 2]) * dt[i - 2];
+  } else if (t >= C / 2 && t - C / 2 < nfb) {  // det_b of filament t - C/2, backward
+    const int q = t - C / 2;
+    const int fb0 = sfil[q].site0 - s0, nn = sfil[q].n;
+    double *db = sdb + fb0 + q;
+    const double *cs = scos + fb0;
+    db[nn] = 1;
+    db[nn - 1] = 2;
+    for (int i = 2; i < nn; ++i)
+      db[nn - i] = 2 * db[nn - i + 1] - (-cs[nn - i - 1]) * (-cs[nn - i - 1]) * db[nn - i + 2];
+  }
+  __syncthreads();
+  if (active && j < n - 2) {
+    const int dbase = base + lf;
+    const double det_g = sdt[dbase + n - 1];
+    double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] / det_g;
+    skeff[t] = (fc.kappa + fc.l * ginv) / fc.l2;
+  }
+  __syncthreads();
+  if (active) {
+    double fs[3] = {0, 0, 0};
+    const int kk = j;
+    if (ND == 2) {
+      if (kk > 1) {
+        double u1[3] = {V(su, t - 2, 0), V(su, t - 2, 1), 0};
+        double u2[3] = {V(su, t - 1, 0), V(su, t - 1, 1), 0};
+        double ke = skeff[t - 2];
+        fs[0] += ke * ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1]);
+        fs[1] += ke * ((1 - u2[1] * u2[1]) * u1[1] - u2[0] * u2[1] * u1[0]);
+      }
+      if (kk > 0 && kk < n - 1) {
+        double u1[3] = {V(su, t - 1, 0), V(su, t - 1, 1), 0};
+        double u2[3] = {u[0], u[1], 0};
+        double ke = skeff[t - 1];
+        fs[0] += ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1] -
+                       ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1]));
+        fs[1] += ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[0] * u1[1] * u2[0] -
+                       ((1 - u2[1] * u2[1]) * u1[1] - u2[0] * u2[1] * u1[0]));
+      }
+      if (kk < n - 2) {
+        double u1[3] = {u[0], u[1], 0};
+        double u2[3] = {V(su, t + 1, 0), V(su, t + 1, 1), 0};
+        double ke = skeff[t];
+        fs[0] -= ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1]);
+        fs[1] -= ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[0] * u1[1] * u2[0]);
+      }
+    } else {
+      if (kk > 1) {
+        double u1[3] = {V(su, t - 2, 0), V(su, t - 2, 1), V(su, t - 2, 2)};
+        double u2[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
+        double ke = skeff[t - 2];
+        fs[0] += ke * ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1] -
+                       u2[0] * u2[2] * u1[2]);
+        fs[1] += ke * ((1 - u2[1] * u2[1]) * u1[1] - u2[1] * u2[0] * u1[0] -
+                       u2[1] * u2[2] * u1[2]);
+        fs[2] += ke * ((1 - u2[2] * u2[2]) * u1[2] - u2[2] * u2[0] * u1[0] -
+                       u2[2] * u2[1] * u1[1]);
+      }
+      if (kk > 0 && kk < n - 1) {
+        double u1[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
+        const double *u2 = u;
+        double ke = skeff[t - 1];
+        fs[0] += ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1] -
+                       u1[0] * u1[2] * u2[2] -
+                       ((1 - u2[0] * u2[0]) * u1[0] - u2[0] * u2[1] * u1[1] -
+                        u2[0] * u2[2] * u1[2]));
+        fs[1] += ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[1] * u1[0] * u2[0] -
+                       u1[1] * u1[2] * u2[2] -
+                       ((1 - u2[1] * u2[1]) * u1[1] - u2[1] * u2[0] * u1[0] -
+                        u2[1] * u2[2] * u1[2]));
+        fs[2] += ke * ((1 - u1[2] * u1[2]) * u2[2] - u1[2] * u1[0] * u2[0] -
+                       u1[2] * u1[1] * u2[1] -
+                       ((1 - u2[2] * u2[2]) * u1[2] - u2[2] * u2[0] * u1[0] -
+                        u2[1] * u2[2] * u1[1]));
+      }
+      if (kk < n - 2) {
+        const double *u1 = u;
+        double u2[3] = {V(su, t + 1, 0), V(su, t + 1, 1), V(su, t + 1, 2)};
+        double ke = skeff[t];
+        fs[0] -= ke * ((1 - u1[0] * u1[0]) * u2[0] - u1[0] * u1[1] * u2[1] -
+                       u1[0] * u1[2] * u2[2]);
+        fs[1] -= ke * ((1 - u1[1] * u1[1]) * u2[1] - u1[1] * u1[0] * u2[0] -
+                       u1[1] * u1[2] * u2[2]);
+        fs[2] -= ke * ((1 - u1[2] * u1[2]) * u2[2] - u1[2] * u1[0] * u2[0] -
+                       u1[2] * u1[1] * u2[1]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) F[i] += fs[i];
+  }
+
+  // ---- P4: tensions (:778-838) --------------------------------------------
+  // gamma^-1 = (1/gpar) t t + (1/gperp)(I - t t); the reciprocals are the
+  // reference's own quotients 1.0 / friction, computed once per filament.
+  auto gam = [&](int a, int c) -> double {
+    return fc.igpar * (tn[a] * tn[c]) + fc.igperp * ((a == c ? 1 : 0) - tn[a] * tn[c]);
+  };
+  if (active) {
+    // gamma^-1 F of this site: "temp_a" of row j and "temp_b" of row j-1.
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      double v = gam(i, 0) * F[0] + gam(i, 1) * F[1];
+      if (ND == 3) v += gam(i, 2) * F[2];
+      V(sbF, t, i) = v;
+    }
+  }
+  __syncthreads();
+  if (has_bond) {
+    double fdiff[3];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) fdiff[i] = V(sbF, t + 1, i) - V(sbF, t, i);
+    sT[t] = dotn<ND>(u, fdiff);
+    double tn2[3] = {V(stn, t + 1, 0), V(stn, t + 1, 1), V(stn, t + 1, 2)};
+    double d1 = dotn<ND>(tn, u);
+    double d2 = dotn<ND>(tn2, u);
+    sb[t] = fc.two_igperp + fc.dgam * (d1 * d1 + d2 * d2);
+    if (j > 0) {
+      double u1[3] = {V(su, t - 1, 0), V(su, t - 1, 1), V(su, t - 1, 2)};
+      double hu = fc.m1_igperp * dotn<ND>(u, u1) -
+                  fc.dgam * (dotn<ND>(tn, u1) * dotn<ND>(tn, u));
+      sc[t - 1] = hu;
+      sa[t - 1] = hu;
+    }
+  }
+  __syncthreads();
+  if (t < nfb) {
+    const int fb0 = sfil[t].site0 - s0;
+    solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[t].n - 1);
+  }
+  __syncthreads();
+
+  // ---- P5: UpdateSitePositions (:840-927), CheckBondLengths (:934-951) ----
+  if (active) {
+    double fs[3];
+    if (j == 0) {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) fs[i] = sT[t] * u[i];
+    } else if (j == n - 1) {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) fs[i] = -sT[t - 1] * V(su, t - 1, i);
+    } else {
+#pragma unroll
+      for (int i = 0; i < ND; ++i) fs[i] = sT[t] * u[i] - sT[t - 1] * V(su, t - 1, i);
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) F[i] += fs[i];
+    const double dl = (midstep ? 0.5 * k.delta : k.delta);
+    double rp[3] = {r[0], r[1], r[2]};  // midstep: the previous positions are these
+    if (!midstep)
+      for (int i = 0; i < ND; ++i) rp[i] = V(srp, t, i);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      double ft = gam(i, 0) * F[0] + gam(i, 1) * F[1];
+      if (ND == 3) ft += gam(i, 2) * F[2];
+      r[i] = rp[i] + dl * ft;
+    }
+    for (int i = 0; i < 3; ++i) V(sr, t, i) = r[i];
+  }
+  __syncthreads();
+  double rd[3] = {0, 0, 0}, um = 0.0;
+  if (has_bond) {
+#pragma unroll
+    for (int i = 0; i < ND; ++i) rd[i] = V(sr, t + 1, i) - r[i];
+    um = normalize<ND, FAST>(rd);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) V(su, t, i) = rd[i];
+  }
+  if (active && j >= 1) {
+    double a = 0.0;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      double temp = r[i] - V(sr, t - 1, i);
+      a += temp * temp;
+    }
+    if (FAST) {
+      // |l - |dr|| / l > 1e-3 without the root and the quotient
+      const double lo = fc.l * (1.0 - 1e-3), hi = fc.l * (1.0 + 1e-3);
+      if (a < lo * lo || a > hi * hi) sflag[lf] = 1;
+    } else {
+      a = sqrt(a);
+      double err = dabs(fc.l - a) / fc.l;
+      if (err > 1e-3) sflag[lf] = 1;
+    }
+  }
+  __syncthreads();
+  if (t < nfb) {
+    const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
+    const double l = sfil[t].l;
+    const int fg = f0 + t;
+    int sw = d.f_switch[fg], nnorm = d.f_nnorm[fg];
+    if (sflag[t]) {
+      sw = !sw;
+      nnorm = 0;
+      if (sw) {
+        for (int jj = 1; jj < nn; ++jj)
+#pragma unroll
+          for (int i = 0; i < ND; ++i)
+            V(sr, fb0 + jj, i) = V(sr, fb0 + jj - 1, i) + l * V(su, fb0 + jj - 1, i);
+      } else {
+        for (int jj = nn - 1; jj > 0; --jj)
+#pragma unroll
+          for (int i = 0; i < ND; ++i)
+            V(sr, fb0 + jj - 1, i) = V(sr, fb0 + jj, i) - l * V(su, fb0 + jj - 1, i);
+      }
+    }
+    nnorm++;
+    d.f_switch[fg] = sw;
+    d.f_nnorm[fg] = nnorm;
+  }
+  __syncthreads();
+
+  // ---- P6: bond geometry (Mesh::UpdateBondPositions), state write-back ----
+  double my_dr = 0.0;
+  if (active) {
+    const bool renorm = sflag[lf] != 0;
+    if (renorm)
+      for (int i = 0; i < 3; ++i) r[i] = V(sr, t, i);
+    if (has_bond) {
+      // Bond::ReInit on the final sites.  Without renormalisation it repeats
+      // the orientation just computed (same operands, same operations).
+      double r2[3] = {V(sr, t + 1, 0), V(sr, t + 1, 1), V(sr, t + 1, 2)};
+      double s[3] = {0, 0, 0}, ub[3] = {0, 0, 0}, len, pos[3] = {0, 0, 0}, o[3] = {0, 0, 0};
+      if (renorm) {
+#pragma unroll
+        for (int i = 0; i < ND; ++i) {
+          o[i] = r2[i] - r[i];
+          ub[i] = o[i];
+        }
+        len = normalize<ND, FAST>(ub);
+      } else {
+#pragma unroll
+        for (int i = 0; i < ND; ++i) {
+          o[i] = r2[i] - r[i];
+          ub[i] = rd[i];
+        }
+        len = um;
+      }
+#pragma unroll
+      for (int i = 0; i < ND; ++i) pos[i] = r[i] + 0.5 * o[i];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        s[i] = 0.0;
+#pragma unroll
+        for (int jj = 0; jj < ND; ++jj) s[i] += k.hinv[ND * i + jj] * pos[jj];
+        s[i] -= nint(s[i]);
+      }
+      store_geom<ND>(d, 1 - rbuf, b, s, ub, len, PREC);
+      d.ub[0][b] = ub[0];
+      d.ub[1][b] = ub[1];
+      d.ub[2][b] = ub[2];
+    }
+    d.r[0][g] = r[0];
+    d.r[1][g] = r[1];
+    d.r[2][g] = r[2];
+    bool bad = false;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) bad |= !isfinite(r[i]);
+    if (bad) atomicOr(d.status, ST_NAN);
+    if (capture) {
+      for (int i = 0; i < 3; ++i) d.cap_F[i][g] = F[i];
+      if (has_bond) d.cap_T[b] = sT[t];
+    }
+    // Displacement tracking for the next query (Mesh::UpdateDrTot runs on
+    // the filaments whose last update was a full step; each query adds the
+    // squared displacement twice, src/mesh.cpp:538-541, src/object.cpp:
+    // 282-292).
+    if (!midstep && interaction) {
+      double acc = d.dt[g];
+      for (int twice = 0; twice < 2; ++twice)
+#pragma unroll
+        for (int i = 0; i < ND; ++i) {
+          double dr = r[i] - d.dz[i][g];
+          acc += dr * dr;
+        }
+      d.dt[g] = acc;
+      my_dr = acc;
+    }
+  }
+  if (!midstep && interaction) {
+    // Block max, then one atomic per block on the IEEE bits (non-negative).
+    double v = my_dr;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((t & 31) == 0) s_drmax[t >> 5] = v;
+    __syncthreads();
+    if (t < 32) {
+      v = (t < (C + 31) / 32) ? s_drmax[t] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+      if (t == 0) {
+        if (!(v <= 1e300)) atomicOr(d.status, ST_NAN);
+        atomicMax(d.dr_max_bits, (unsigned long long)__double_as_longlong(v));
+      }
+    }
+  }
+#undef V
+}
+
+
+}  // namespace sc

@@ -132,3 +132,45 @@ def test_mixed_force_error():
     et = np.abs(t32 - t64).max() / np.abs(t64).max()
     assert ef <= 1e-5, ef
     assert et <= 1e-5, et
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_path_matches_host_path(precision):
+    """The captured WHILE-loop graph (device-decided rebuilds) gives the same
+    bits as the host-driven loop, in both precisions."""
+    system, fils, sites = _workload("B", 0.05, seed=6)
+    a = _ctx(system, fils, sites, precision)
+    b = _ctx(system, fils, sites, precision)
+    for n in (40, 41, 20):
+        a.step_graph(n)
+        b.step(n)
+        assert_same(a.sites(), b.sites(), "sites")
+        assert_same(a.pairs(), b.pairs(), "pairs")
+        assert a.counters().n_rebuilds == b.counters().n_rebuilds
+    assert a.counters().n_rebuilds > 0
+
+
+def test_graph_matches_oracle():
+    system, fils, sites = _workload("A", 1.0, seed=4)
+    ctx = _ctx(system, fils, sites)
+    o = Oracle(system, fils, sites)
+    for _ in range(3):
+        ctx.step_graph(101)
+        o.step(101)
+        compare_state(ctx, o, 3, capture=False)
+
+
+def test_fast_integrator_close_to_exact():
+    """The mixed path's contraction/reciprocal integrator against the exact
+    FP64 integrator on identical forces (both mixed precision): positions
+    agree to 1e-12 relative after one full BD step."""
+    system, fils, sites = _workload("B", 0.05, seed=8)
+    a = _ctx(system, fils, sites, "mixed")
+    b = _ctx(system, fils, sites, "mixed")
+    b.set_fast_integrator(False)
+    a.step(2)
+    b.step(2)
+    ra, rb = a.sites(), b.sites()
+    scale = np.abs(rb).max()
+    assert np.abs(ra - rb).max() <= 1e-12 * scale
+    ta, tb = a.tensions(), b.tensions()
