@@ -170,6 +170,43 @@ sc_status sc_get_kernel_timing(sc_ctx *ctx, double *total_ms, int64_t *launches)
  * the last sc_step_graph call, in ms. */
 sc_status sc_get_graph_time(sc_ctx *ctx, double *ms);
 
+/* Pair forces for callers that cannot allocate device memory.
+ *
+ * No counterpart in the reference.  Some callers cannot call cudaMalloc:
+ * an application recording its own CUDA graph (allocation is illegal during
+ * stream capture), or one whose device memory belongs to its own pool.  This
+ * entry point computes, for a configuration in the caller's device buffers,
+ * the bond forces and torques that the first Interact after a pair-list
+ * rebuild produces (fresh pairs, FP64, bit-identical to sc_interact on a
+ * context just loaded with the same sites), without allocating anything: its
+ * scratch is a fixed array inside the library (SC_NOALLOC_SCRATCH_BYTES,
+ * held by every GPU that loads the library until the process exits).
+ *
+ *   species         min_bond_length and diameter (they set the cell size)
+ *   d_site_offsets  device, n_filaments + 1 int32 site offsets (first 0)
+ *   d_site_xyz      device, n_sites x 3 doubles (z = 0 in 2D)
+ *   d_bond_force    device, n_bonds x 3 doubles (output)
+ *   d_bond_torque   device, n_bonds x 3 doubles (output)
+ *   stream          cudaStream_t the work is issued on (0: legacy stream)
+ *
+ * Limits: at most SC_NOALLOC_MAX_BONDS bonds and filaments, a cell grid of
+ * at most SC_NOALLOC_MAX_CELLS cells, at most SC_NOALLOC_MAX_PAIRS
+ * candidate pairs; larger inputs return SC_ERR_INVALID_ARG (sizes, cells)
+ * or SC_ERR_LIST_OVERFLOW (pairs).  The call synchronises the stream.  The
+ * first call on a device looks up the scratch address with
+ * cudaGetSymbolAddress; make that first call before any stream capture.
+ * All calls on a device share the scratch and leave their data in it; calls
+ * whose GPU work overlaps race and must be serialised by the caller. */
+#define SC_NOALLOC_MAX_BONDS 8192
+#define SC_NOALLOC_MAX_CELLS 131072
+#define SC_NOALLOC_MAX_PAIRS 32768
+#define SC_NOALLOC_SCRATCH_BYTES 8816384 /* 8.4 MiB per GPU */
+sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
+                                 const sc_filament_params *species, int n_filaments,
+                                 const int32_t *d_site_offsets, const double *d_site_xyz,
+                                 double *d_bond_force, double *d_bond_torque,
+                                 void *stream);
+
 /* Seeded random insertion with overlap rejection on the host (the
  * distributions of Mesh::InitRandomBond and Filament::InsertFilament,
  * src/mesh.cpp:244-258, src/filament.cpp:225-249,350-383, rejection of

@@ -32,7 +32,7 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_tensions", "sc_get_filament_state", "sc_get_dr_tot", "sc_get_pairs",
             "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_set_kernel_timing",
             "sc_get_kernel_timing", "sc_get_graph_time", "sc_set_fast_integrator",
-            "sc_insert_filaments"]
+            "sc_pair_forces_noalloc", "sc_insert_filaments"]
 
 
 class ScError(RuntimeError):

@@ -1,0 +1,300 @@
+// Pair forces without any device allocation (sc_pair_forces_noalloc).
+//
+// Some callers cannot call cudaMalloc: a host application that records its
+// work into its own CUDA graph (allocation is not allowed while a stream is
+// being captured), or one whose device memory is owned by its own pool or
+// allocator and must not be grown behind its back.  This entry point serves
+// them: it evaluates the WCA bond forces and torques of one configuration
+// held in the caller's device buffers, using only a fixed scratch area that
+// is part of the library image.
+//
+// The scratch is one file-scope __device__ array (g_noalloc_scratch below,
+// SC_NOALLOC_SCRATCH_BYTES = 8.4 MiB).  Every GPU that loads the library holds it until the
+// process exits.  All calls on a device share it and it keeps the last
+// call's contents, so every call clears what must start at zero; calls
+// whose GPU work overlaps (several host threads, or several streams) race
+// on it and must be serialised by the caller.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "sc_common.cuh"
+#include "sc_kernels.h"
+#include "simcore_gpu.h"
+
+namespace {
+
+using sc::DevState;
+using sc::SysConst;
+
+// Limits of the static scratch.
+constexpr int kMaxBonds = SC_NOALLOC_MAX_BONDS;
+constexpr int kMaxFilaments = SC_NOALLOC_MAX_BONDS;
+constexpr int kMaxSites = kMaxBonds + kMaxFilaments;
+constexpr int kMaxCells = SC_NOALLOC_MAX_CELLS;
+constexpr int kMaxPairs = SC_NOALLOC_MAX_PAIRS;
+
+// Byte layout of the scratch area: each region 256-byte aligned.
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Layout {
+  size_t r, key, cell_count, cell_start, sorted, pair_count, pair_off, deg, e_off,
+      scan_tmp, bond_fil, ub, g64, pa, pb, pos1, pos2, pf, cf, e_ent, bF, bT, status,
+      counters, total;
+};
+
+constexpr int kScanTmp = (kMaxCells > kMaxBonds ? kMaxCells : kMaxBonds) / 2048 + 2;
+
+constexpr Layout make_layout() {
+  Layout L{};
+  size_t o = 0;
+  L.r = o;          o = align256(o + sizeof(double) * 3 * kMaxSites);
+  L.key = o;        o = align256(o + sizeof(int) * kMaxBonds);
+  L.cell_count = o; o = align256(o + sizeof(int) * kMaxCells);
+  L.cell_start = o; o = align256(o + sizeof(int) * (kMaxCells + 1));
+  L.sorted = o;     o = align256(o + sizeof(int) * kMaxBonds);
+  L.pair_count = o; o = align256(o + sizeof(int) * kMaxBonds);
+  L.pair_off = o;   o = align256(o + sizeof(int) * (kMaxBonds + 1));
+  L.deg = o;        o = align256(o + sizeof(int) * kMaxBonds);
+  L.e_off = o;      o = align256(o + sizeof(int) * (kMaxBonds + 1));
+  L.scan_tmp = o;   o = align256(o + sizeof(int) * kScanTmp);
+  L.bond_fil = o;   o = align256(o + sizeof(int) * kMaxBonds);
+  L.ub = o;         o = align256(o + sizeof(double) * 3 * kMaxBonds);
+  L.g64 = o;        o = align256(o + sizeof(sc::BondGeomF64) * kMaxBonds);
+  L.pa = o;         o = align256(o + sizeof(int) * kMaxPairs);
+  L.pb = o;         o = align256(o + sizeof(int) * kMaxPairs);
+  L.pos1 = o;       o = align256(o + sizeof(int) * kMaxPairs);
+  L.pos2 = o;       o = align256(o + sizeof(int) * kMaxPairs);
+  L.pf = o;         o = align256(o + sizeof(double) * 4 * kMaxPairs);
+  L.cf = o;         o = align256(o + sizeof(double) * 16 * kMaxPairs);
+  L.e_ent = o;      o = align256(o + sizeof(int) * 2 * kMaxPairs);
+  L.bF = o;         o = align256(o + sizeof(double) * 3 * kMaxBonds);
+  L.bT = o;         o = align256(o + sizeof(double) * 3 * kMaxBonds);
+  L.status = o;     o = align256(o + sizeof(unsigned));
+  L.counters = o;   o = align256(o + sizeof(unsigned long long) * 4);
+  L.total = o;
+  return L;
+}
+
+constexpr Layout kLayout = make_layout();
+static_assert(kLayout.total == SC_NOALLOC_SCRATCH_BYTES,
+              "SC_NOALLOC_SCRATCH_BYTES must state the scratch size");
+
+}  // namespace
+
+// The scratch area itself (device memory of the library image).
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kLayout.total];
+
+namespace {
+
+// Device address of g_noalloc_scratch per device ordinal, looked up once per
+// device (with that device current) and cached.  In host code the symbol
+// name is only a host-side stand-in, never a device address.
+constexpr int kMaxDevices = 64;
+std::mutex g_addr_mtx;
+unsigned char *g_addr[kMaxDevices] = {};
+
+sc_status scratch_address(int dev, unsigned char **out) {
+  if (dev < 0 || dev >= kMaxDevices) return SC_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_addr_mtx);
+  if (!g_addr[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return SC_ERR_CUDA;
+    }
+    g_addr[dev] = (unsigned char *)p;
+  }
+  *out = g_addr[dev];
+  return SC_OK;
+}
+
+// The reference's symmetric inverses (src/linear_algebra.cpp:40-64).
+void inv2(const double *a, double *b) {
+  double inv_det = a[0] * a[3] - a[1] * a[1];
+  inv_det = 1.0 / inv_det;
+  b[0] = a[3] * inv_det;
+  b[3] = a[0] * inv_det;
+  b[2] = b[1] = -a[1] * inv_det;
+}
+
+void inv3(const double *a, double *b) {
+  double inv_det = a[0] * (a[4] * a[8] - a[5] * a[7]) -
+                   a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                   a[2] * (a[3] * a[7] - a[4] * a[6]);
+  inv_det = 1.0 / inv_det;
+  b[0] = inv_det * (a[4] * a[8] - a[5] * a[7]);
+  b[4] = inv_det * (a[0] * a[8] - a[2] * a[6]);
+  b[8] = inv_det * (a[0] * a[4] - a[1] * a[3]);
+  b[1] = b[3] = -inv_det * (a[3] * a[8] - a[5] * a[6]);
+  b[2] = b[6] = inv_det * (a[3] * a[7] - a[4] * a[6]);
+  b[5] = b[7] = -inv_det * (a[0] * a[7] - a[1] * a[6]);
+}
+
+// AoS caller positions -> SoA scratch; bond -> filament map from offsets.
+__global__ void k_noalloc_unpack(int nf, int ns, const int32_t *site_off,
+                                 const double *xyz, int n_dim, DevState d, int *bond_fil) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ns) {
+    for (int c = 0; c < 3; ++c) d.r[c][i] = c < n_dim ? xyz[3 * (size_t)i + c] : 0.0;
+  }
+  if (i < nf) {
+    int s0 = site_off[i], s1 = site_off[i + 1];
+    for (int b = s0 - i; b < s1 - i - 1; ++b) bond_fil[b] = i;
+  }
+}
+
+// Bond accumulators (SoA scratch) -> caller's AoS outputs.
+__global__ void k_noalloc_pack(int nb, DevState d, double *f, double *t) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  for (int c = 0; c < 3; ++c) {
+    f[3 * (size_t)b + c] = d.bF[c][b];
+    t[3 * (size_t)b + c] = d.bT[c][b];
+  }
+}
+
+#define NA_CK(call)                                      \
+  do {                                                   \
+    if ((call) != cudaSuccess) {                         \
+      cudaGetLastError();                                \
+      return SC_ERR_CUDA;                                \
+    }                                                    \
+  } while (0)
+
+}  // namespace
+
+extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
+                                            const sc_filament_params *species,
+                                            int n_filaments, const int32_t *d_site_offsets,
+                                            const double *d_site_xyz, double *d_bond_force,
+                                            double *d_bond_torque, void *stream) {
+  if (!desc || !species || !d_site_offsets || !d_site_xyz || !d_bond_force ||
+      !d_bond_torque)
+    return SC_ERR_INVALID_ARG;
+  if (desc->n_dim != 2 && desc->n_dim != 3) return SC_ERR_INVALID_ARG;
+  if (!(desc->system_radius > 0) || !(desc->wca_sig > 0)) return SC_ERR_INVALID_ARG;
+  if (!(species->min_bond_length > 0) || !(species->diameter > 0)) return SC_ERR_INVALID_ARG;
+  if (n_filaments <= 0 || n_filaments > kMaxFilaments) return SC_ERR_INVALID_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0;
+  NA_CK(cudaGetDevice(&dev));
+  unsigned char *base = nullptr;
+  sc_status s = scratch_address(dev, &base);
+  if (s != SC_OK) return s;
+
+  // Sizes: the last site offset (one 4-byte read of the caller's array).
+  int32_t ns32 = 0;
+  NA_CK(cudaMemcpyAsync(&ns32, d_site_offsets + n_filaments, sizeof(int32_t),
+                        cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaStreamSynchronize(st));
+  const int ns = ns32, nb = ns32 - n_filaments;
+  if (ns <= 0 || nb <= 0 || ns > kMaxSites || nb > kMaxBonds) return SC_ERR_INVALID_ARG;
+
+  // System constants, as sc_create and sc_add_filaments derive them.
+  SysConst k;
+  std::memset(&k, 0, sizeof(k));
+  const int nd = desc->n_dim;
+  k.n_dim = nd;
+  const double hh = 2.0 * desc->system_radius;
+  for (int a = 0; a < nd; ++a)
+    for (int b = 0; b < nd; ++b) k.h[a * nd + b] = (a == b ? 1 : 0) * hh;
+  k.h[nd * nd - 1] = hh;
+  if (nd == 2) inv2(k.h, k.hinv);
+  else inv3(k.h, k.hinv);
+  for (int i = 0; i < 9; ++i) k.hf[i] = (float)k.h[i];
+  k.delta = desc->delta;
+  const double rcut = std::pow(2.0, 1.0 / 6.0) * desc->wca_sig;
+  k.rcut2 = rcut * rcut;
+  k.c12 = 4.0 * desc->wca_eps * std::pow(desc->wca_sig, 12.0);
+  k.c6 = 4.0 * desc->wca_eps * std::pow(desc->wca_sig, 6.0);
+  k.fcut = desc->f_cutoff;
+  k.like_like = desc->like_like_interactions ? 1 : 0;
+  {
+    double min_len = -1, spec_length = 1.5 * species->min_bond_length;
+    if (species->diameter > spec_length) spec_length = species->diameter;
+    if (spec_length > min_len) min_len = spec_length;
+    if (0.0 > min_len) min_len = 0.0;
+    if (std::sqrt(k.rcut2) > min_len) min_len = std::sqrt(k.rcut2);
+    int n1d = (int)std::floor(2 * desc->system_radius / min_len);
+    if (n1d <= 3) n1d = 3;
+    long long ncell = (long long)n1d * n1d * (nd == 3 ? n1d : 1);
+    if (ncell > kMaxCells) return SC_ERR_INVALID_ARG;
+    k.n1d = n1d;
+    k.third = nd == 3 ? n1d : 1;
+    k.n_cells = (int)ncell;
+  }
+
+  // Device views into the scratch area.
+  const Layout &L = kLayout;
+  DevState d;
+  std::memset(&d, 0, sizeof(d));
+  d.nf = n_filaments;
+  d.ns = ns;
+  d.nb = nb;
+  double *r = (double *)(base + L.r);
+  for (int c = 0; c < 3; ++c) d.r[c] = r + (size_t)c * kMaxSites;
+  d.bond_fil = (const int *)(base + L.bond_fil);
+  double *ub = (double *)(base + L.ub);
+  for (int c = 0; c < 3; ++c) d.ub[c] = ub + (size_t)c * kMaxBonds;
+  d.g64[0] = d.g64[1] = (sc::BondGeomF64 *)(base + L.g64);
+  d.pa = (int *)(base + L.pa);
+  d.pb = (int *)(base + L.pb);
+  d.pos1 = (int *)(base + L.pos1);
+  d.pos2 = (int *)(base + L.pos2);
+  d.pf64 = (double *)(base + L.pf);
+  d.cf64 = (double *)(base + L.cf);
+  d.e_off = (int *)(base + L.e_off);
+  d.e_ent = (int *)(base + L.e_ent);
+  double *bF = (double *)(base + L.bF), *bT = (double *)(base + L.bT);
+  for (int c = 0; c < 3; ++c) {
+    d.bF[c] = bF + (size_t)c * kMaxBonds;
+    d.bT[c] = bT + (size_t)c * kMaxBonds;
+  }
+  d.status = (unsigned *)(base + L.status);
+  unsigned long long *ctr = (unsigned long long *)(base + L.counters);
+  d.dr_max_bits = ctr;
+  d.mcount = ctr + 1;
+  d.n_rebuilds = (long long *)(ctr + 2);
+  int *key = (int *)(base + L.key), *cell_count = (int *)(base + L.cell_count);
+  int *cell_start = (int *)(base + L.cell_start), *sorted = (int *)(base + L.sorted);
+  int *pair_count = (int *)(base + L.pair_count), *pair_off = (int *)(base + L.pair_off);
+  int *deg = (int *)(base + L.deg), *scan_tmp = (int *)(base + L.scan_tmp);
+  d.n_pairs = pair_off + nb;
+
+  // What must start at zero: the cell and degree counters (the previous
+  // call may have stopped early), the status word and the counters.
+  NA_CK(cudaMemsetAsync(cell_count, 0, sizeof(int) * (size_t)k.n_cells, st));
+  NA_CK(cudaMemsetAsync(deg, 0, sizeof(int) * (size_t)nb, st));
+  NA_CK(cudaMemsetAsync(d.status, 0, sizeof(unsigned), st));
+  NA_CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 4, st));
+
+  const int grid = (ns > n_filaments ? ns : n_filaments) / 256 + 1;
+  k_noalloc_unpack<<<grid, 256, 0, st>>>(n_filaments, ns, d_site_offsets, d_site_xyz, nd, d,
+                                         (int *)(base + L.bond_fil));
+  sc::launch_init_geometry(k, d, 0, 0, st);
+  // Pair list of a rebuild (InteractionManager::UpdatePairInteractions) and
+  // one evaluation with fresh Interaction records, as the first Interact
+  // after the reference's insertion computes.
+  sc::launch_bin_count(k, d, key, cell_count, st);
+  sc::launch_exclusive_scan(cell_count, cell_start, k.n_cells, scan_tmp, st);
+  sc::launch_bin_scatter(nb, key, cell_start, cell_count, sorted, st);
+  sc::launch_cell_sort_count(k, d, key, sorted, cell_start, pair_count, st);
+  sc::launch_exclusive_scan(pair_count, pair_off, nb, scan_tmp, st);
+  sc::launch_pair_emit(k, d, key, sorted, cell_start, pair_off, kMaxPairs, deg, 0, st);
+  sc::launch_exclusive_scan(deg, d.e_off, nb, scan_tmp, st);
+  sc::launch_csr(d, kMaxPairs, deg, st);
+  sc::launch_pairs(k, d, 0, 0, kMaxPairs, st);
+  sc::launch_bond_sum(k, d, 0, st);
+  k_noalloc_pack<<<nb / 256 + 1, 256, 0, st>>>(nb, d, d_bond_force, d_bond_torque);
+  NA_CK(cudaGetLastError());
+
+  unsigned status = 0;
+  NA_CK(cudaMemcpyAsync(&status, d.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  NA_CK(cudaStreamSynchronize(st));
+  if (status & sc::ST_LIST_OVERFLOW) return SC_ERR_LIST_OVERFLOW;
+  if (status) return SC_ERR_NAN;
+  return SC_OK;
+}
