@@ -128,6 +128,23 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+def replica_seed(rank):
+    """Seed of the replica a rank runs (independent systems, one per GPU)."""
+    return rank
+
+
+def reduce_max(value, dist):
+    """Max over ranks (the device times of all replicas); dist may be None."""
+    if dist is None:
+        return float(value)
+    import torch
+    backend = dist.get_backend()
+    dev = "cuda" if backend == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def algorithmic_bytes(n_sites, n_bonds, n_pairs, precision):
     """Bytes one reference step must move (per launch of the step kernel):
     sites 96 B (r read + write, previous position, projected noise), bonds
@@ -151,7 +168,7 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    system, fils, sites = workloads.make(args.workload, 1.0, seed=rank)
+    system, fils, sites = workloads.make(args.workload, 1.0, seed=replica_seed(rank))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def timed_graph(ctx, k, flush_l2=True):
@@ -185,11 +202,7 @@ def run_ours(args, rank, world, local_rank):
         if sampler:
             sampler.mark(t_start, time.perf_counter())
         c1 = ctx.counters()
-        total_ms = float(sum(ms))
-        if dist is not None:
-            t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
+        total_ms = reduce_max(float(sum(ms)), dist)
         results[prec] = dict(total_ms=total_ms, n_bonds=c1.n_bonds, n_sites=c1.n_sites,
                              n_pairs=c1.n_pairs, rebuilds=c1.n_rebuilds - c0.n_rebuilds,
                              launches=c1.kernel_launches - c0.kernel_launches)
@@ -216,11 +229,7 @@ def run_ours(args, rank, world, local_rank):
         ctx.step_graph(I_STEPS_PER_STEP)
         host_xyz = ctx.sites()
         e2e_times.append(time.perf_counter() - t0)
-    e2e_total = float(sum(e2e_times))
-    if dist is not None:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = reduce_max(float(sum(e2e_times)), dist)
 
     for c in contexts.values():
         c.close()

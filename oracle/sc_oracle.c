@@ -1092,3 +1092,80 @@ void sco_get_bond_cells(const sco_sim *s, int *xyz) {
 void sco_get_dr_tot(const sco_sim *s, double *dr) {
   memcpy(dr, s->dt, sizeof(double) * s->ns);
 }
+
+void sco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  sc_philox4x32_10(ctr, key, out);
+}
+
+int sco_segment_force(const sco_system *sys, const double *a1, const double *a2,
+                      const double *b1, const double *b2, double *force) {
+  /* Two one-bond "filaments" are not allowed (at least two bonds), so build
+   * the pair geometry directly with the oracle's own routines. */
+  sco_sim s;
+  double sa[3], sb[3], ua[3], ub[3], pa[3], pb[3], la = 0, lb = 0, t1[3], t2[3];
+  double f[3] = {0, 0, 0};
+  int i, n = sys->n_dim;
+  memset(&s, 0, sizeof(s));
+  s.n_dim = n;
+  {
+    double hh = 2.0 * sys->system_radius;
+    int a, b;
+    for (a = 0; a < n; ++a)
+      for (b = 0; b < n; ++b) s.h[a * n + b] = (a == b ? 1 : 0) * hh;
+    s.h[n * n - 1] = hh;
+    if (n == 2) invert_sym_2d(s.h, s.hinv);
+    else invert_sym_3d(s.h, s.hinv);
+  }
+  {
+    double rcut = pow(2.0, 1.0 / 6.0) * sys->wca_sig;
+    s.rcut2 = rcut * rcut;
+    s.c12 = 4.0 * sys->wca_eps * pow(sys->wca_sig, 12.0);
+    s.c6 = 4.0 * sys->wca_eps * pow(sys->wca_sig, 6.0);
+    s.fcut = sys->f_cutoff;
+  }
+  for (i = 0; i < 3; ++i) ua[i] = ub[i] = pa[i] = pb[i] = sa[i] = sb[i] = 0;
+  for (i = 0; i < n; ++i) {
+    ua[i] = a2[i] - a1[i];
+    la += ua[i] * ua[i];
+    ub[i] = b2[i] - b1[i];
+    lb += ub[i] * ub[i];
+  }
+  la = sqrt(la);
+  lb = sqrt(lb);
+  for (i = 0; i < n; ++i) {
+    pa[i] = a1[i] + 0.5 * ua[i];
+    pb[i] = b1[i] + 0.5 * ub[i];
+    ua[i] /= la;
+    ub[i] /= lb;
+  }
+  periodic_bc(n, s.hinv, pa, sa);
+  periodic_bc(n, s.hinv, pb, sb);
+  {
+    double dr[3] = {0, 0, 0}, c1[3] = {0, 0, 0}, c2[3] = {0, 0, 0}, d2 = 0;
+    sphero(&s, sa, ua, la, sb, ub, lb, dr, &d2, c1, c2);
+    (void)t1;
+    (void)t2;
+    if (d2 > s.rcut2) {
+      for (i = 0; i < 3; ++i) force[i] = 0;
+      return 0;
+    }
+  }
+  /* reuse the pair path with a private two-bond geometry table */
+  {
+    double bs[6], bu[6], bl[2];
+    for (i = 0; i < 3; ++i) {
+      bs[i] = sa[i];
+      bs[3 + i] = sb[i];
+      bu[i] = ua[i];
+      bu[3 + i] = ub[i];
+    }
+    bl[0] = la;
+    bl[1] = lb;
+    s.bs = bs;
+    s.bu = bu;
+    s.bl = bl;
+    pair_force(&s, 0, 1, f, t1, t2);
+  }
+  for (i = 0; i < 3; ++i) force[i] = f[i];
+  return 1;
+}

@@ -84,9 +84,18 @@ void sco_get_dr_tot(const sco_sim *s, double *dr);
 void sco_set_sites(sco_sim *s, const double *xyz);
 
 /* Pair forces alone, evaluated from the current bond geometry on the
- * current pair list with fresh (zero) stale forces: bond forces/torques are
- * written to f and t.  Used to check single force evaluations. */
+ * current pair list with the pair forces stored so far, without changing
+ * any state: bond forces/torques are written to f and t. */
 void sco_pair_forces(sco_sim *s, double *f, double *t);
+
+/* Philox4x32-10 block (for the known-answer test of the shared stream). */
+void sco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* Pair force of two bonds given by end points (a1, a2) and (b1, b2) in an
+ * otherwise empty box: force on bond a, following Sphero + WCA.  Returns 1
+ * when the pair is within the cutoff. */
+int sco_segment_force(const sco_system *sys, const double *a1, const double *a2,
+                      const double *b1, const double *b2, double *force);
 
 #ifdef __cplusplus
 }

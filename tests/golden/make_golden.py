@@ -1,0 +1,70 @@
+"""Generates the golden fixtures of tests/golden/ from the reference's own
+code (oracle/_ref/libscref.so, built from the reference sources by
+oracle/ref/Makefile).  Run where the reference tree is present:
+
+    python tests/golden/make_golden.py
+
+Each fixture holds a seeded initial configuration (random insertion with
+overlap rejection) and the reference's state after a fixed number of steps.
+tests/test_oracle.py requires the C oracle to reproduce every array bit for
+bit; the GPU tests require the CUDA path to match the oracle the same way.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from checkers import Reference  # noqa: E402
+
+import simcore_b200 as sc  # noqa: E402
+
+CASES = {
+    # 3D, stiff filaments (workload A's physics) in a small dense box
+    "ref3d_stiff": dict(n_dim=3, R=15.0, n_fil=20, n_seg=20, lp=500.0, delta=1e-4, seed=21,
+                        steps=61),
+    # 3D, flexible filaments: frequent renormalisations
+    "ref3d_flexible": dict(n_dim=3, R=12.0, n_fil=30, n_seg=10, lp=5.0, delta=1e-3, seed=22,
+                           steps=41),
+    # 2D
+    "ref2d": dict(n_dim=2, R=25.0, n_fil=40, n_seg=16, lp=200.0, delta=1e-4, seed=23,
+                  steps=61),
+}
+
+
+def make_case(name, c):
+    nb = np.full(c["n_fil"], c["n_seg"], dtype=np.int32)
+    sites = sc.insert_filaments(c["n_dim"], c["R"], c["seed"], nb, nb.astype(float),
+                                np.full(c["n_fil"], c["lp"]))
+    system = dict(n_dim=c["n_dim"], system_radius=c["R"], delta=c["delta"], wca_eps=1.0,
+                  wca_sig=1.0, f_cutoff=2000.0, stoch_flag=1, interaction_flag=1,
+                  like_like_interactions=1, seed=c["seed"])
+    fils = [dict(length=float(c["n_seg"]), persistence_length=c["lp"], diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * c["n_fil"]
+    ref = Reference(system, fils, sites, n_threads=2)
+    ref.step(c["steps"])
+    f, t = ref.bond_forces()
+    sw, nn = ref.filament_state()
+    out = dict(
+        system=np.array([c["n_dim"], c["R"], c["delta"], c["seed"], c["lp"], c["n_seg"],
+                         c["n_fil"], c["steps"]], dtype=np.float64),
+        sites0=sites, sites=ref.sites(), prev_sites=ref.prev_sites(),
+        random_forces=ref.random_forces(), site_forces=ref.site_forces(), bond_force=f,
+        bond_torque=t, tensions=ref.tensions(), pairs=ref.pairs(), dr_tot=ref.dr_tot(),
+        normalize_switch=sw, n_normalize=nn, bond_cells=ref.bond_cells(),
+        n_rebuilds=np.array([ref.n_rebuilds]))
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return out
+
+
+if __name__ == "__main__":
+    if not Reference.available():
+        sys.exit("oracle/_ref/libscref.so is not built (python oracle/build.py)")
+    for name, c in CASES.items():
+        o = make_case(name, c)
+        print(name, "rebuilds", int(o["n_rebuilds"][0]), "renormalised filaments",
+              int((o["n_normalize"] < c["steps"]).sum()), "pairs", len(o["pairs"]))

@@ -1,0 +1,172 @@
+"""CPU oracle: pinned against the reference's own code.
+
+* Philox4x32-10 against the published known-answer vectors (Salmon et al.).
+* The oracle replays the golden fixtures of tests/golden/ -- generated by
+  tests/golden/make_golden.py from the reference's own sources
+  (oracle/_ref) -- bit for bit, including rebuilds and renormalisations.
+* Where the reference build is present, both run side by side on a fresh
+  configuration and must agree bit for bit every step.
+* Analytic known answers: WCA force of two segments at a known distance and
+  its cap; a straight rod without noise or forces does not move.
+"""
+import ctypes
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from checkers import Oracle, Reference, ORACLE_SO, SystemDesc
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+
+
+def _oracle_lib():
+    return ctypes.CDLL(ORACLE_SO)
+
+
+def test_philox_known_answers():
+    lib = _oracle_lib()
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+           ((0xffffffff,) * 4, (0xffffffff,) * 2, (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+           ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for ctr, key, want in kat:
+        c = (ctypes.c_uint32 * 4)(*ctr)
+        k = (ctypes.c_uint32 * 2)(*key)
+        o = (ctypes.c_uint32 * 4)()
+        lib.sco_philox4x32_10(c, k, o)
+        assert tuple(o) == want
+
+
+def _case(path):
+    z = np.load(path)
+    n_dim, R, delta, seed, lp, n_seg, n_fil, steps = z["system"]
+    system = dict(n_dim=int(n_dim), system_radius=R, delta=delta, wca_eps=1.0, wca_sig=1.0,
+                  f_cutoff=2000.0, stoch_flag=1, interaction_flag=1, like_like_interactions=1,
+                  seed=int(seed))
+    fils = [dict(length=float(n_seg), persistence_length=float(lp), diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * int(n_fil)
+    return z, system, fils, int(steps)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_reproduces_reference_fixture(path):
+    z, system, fils, steps = _case(path)
+    nd = system["n_dim"]
+    o = Oracle(system, fils, z["sites0"])
+    o.step(steps)
+    f, t = o.bond_forces()
+    sw, nn = o.filament_state()
+    checks = {
+        "sites": (o.sites()[:, :nd], z["sites"][:, :nd]),
+        "prev_sites": (o.prev_sites()[:, :nd], z["prev_sites"][:, :nd]),
+        "random_forces": (o.random_forces()[:, :nd], z["random_forces"][:, :nd]),
+        "site_forces": (o.site_forces()[:, :nd], z["site_forces"][:, :nd]),
+        "bond_force": (f[:, :nd], z["bond_force"][:, :nd]),
+        "bond_torque": (t, z["bond_torque"]),
+        "tensions": (o.tensions(), z["tensions"]),
+        "pairs": (o.pairs(), z["pairs"]),
+        "dr_tot": (o.dr_tot(), z["dr_tot"]),
+        "normalize_switch": (sw, z["normalize_switch"]),
+        "n_normalize": (nn, z["n_normalize"]),
+        "bond_cells": (o.bond_cells(), z["bond_cells"]),
+    }
+    for name, (a, b) in checks.items():
+        assert a.shape == b.shape, name
+        assert np.array_equal(a, b), name
+    assert o.n_rebuilds == int(z["n_rebuilds"][0])
+    assert o.n_rebuilds > 0
+
+
+def test_fixtures_exercise_rebuilds_and_renormalisation():
+    assert len(GOLDEN) >= 3
+    for path in GOLDEN:
+        z, system, fils, steps = _case(path)
+        assert int(z["n_rebuilds"][0]) >= 1
+        assert (z["n_normalize"] < steps).any()
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build not present")
+@pytest.mark.parametrize("n_dim", [3, 2])
+def test_oracle_and_reference_side_by_side(n_dim):
+    import simcore_b200 as sc
+    n_fil, n_seg, R = (25, 12, 14.0) if n_dim == 3 else (30, 14, 22.0)
+    nb = np.full(n_fil, n_seg, dtype=np.int32)
+    sites = sc.insert_filaments(n_dim, R, 99 + n_dim, nb, nb.astype(float), np.full(n_fil, 50.0))
+    system = dict(n_dim=n_dim, system_radius=R, delta=2e-4, seed=7)
+    fils = [dict(length=float(n_seg), persistence_length=50.0, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * n_fil
+    o = Oracle(system, fils, sites)
+    r = Reference(system, fils, sites, n_threads=2)
+    for _ in range(30):
+        o.step(3)
+        r.step(3)
+        assert np.array_equal(o.sites()[:, :n_dim], r.sites()[:, :n_dim])
+        assert np.array_equal(o.bond_forces()[0][:, :n_dim], r.bond_forces()[0][:, :n_dim])
+        assert np.array_equal(o.tensions(), r.tensions())
+        assert np.array_equal(o.pairs(), r.pairs())
+    assert o.n_rebuilds == r.n_rebuilds
+
+
+def _segment_force(a1, a2, b1, b2):
+    lib = _oracle_lib()
+    sysd = SystemDesc(n_dim=3, system_radius=50.0, delta=1e-4, wca_eps=1.0, wca_sig=1.0,
+                      f_cutoff=2000.0, stoch_flag=0, interaction_flag=1,
+                      like_like_interactions=1, seed=0, n_threads=1)
+    arr = lambda v: (ctypes.c_double * 3)(*v)  # noqa: E731
+    out = (ctypes.c_double * 3)()
+    lib.sco_segment_force.restype = ctypes.c_int
+    inside = lib.sco_segment_force(ctypes.byref(sysd), arr(a1), arr(a2), arr(b1), arr(b2), out)
+    return inside, np.array(out[:])
+
+
+def test_wca_known_answers():
+    rcut = 2 ** (1 / 6)
+    for r in (0.9, 1.0, 1.1):
+        inside, f = _segment_force([0, 0, 0], [1, 0, 0], [0, r, 0], [1, r, 0])
+        assert inside == 1
+        # F = -24 eps (2 sigma^12 / r^13 - sigma^6 / r^7) along y, pushing a away from b
+        fa = -24.0 * (2.0 / r ** 13 - 1.0 / r ** 7)
+        assert abs(f[1] - fa) <= 1e-12 * abs(fa)
+        assert f[0] == 0 and f[2] == 0
+    inside, f = _segment_force([0, 0, 0], [1, 0, 0], [0, 0.5, 0], [1, 0.5, 0])
+    assert f[1] == -2000.0  # capped at f_cutoff
+    inside, f = _segment_force([0, 0, 0], [1, 0, 0], [0, rcut + 0.01, 0], [1, rcut + 0.01, 0])
+    assert inside == 0
+    # periodic image across the box face (side 100)
+    inside, f = _segment_force([-49.8, 0, 0], [-49.8, 1, 0], [49.2, 0, 0], [49.2, 1, 0])
+    assert inside == 1 and f[0] > 0
+
+
+def _straight_rod(interaction):
+    n_seg = 10
+    sites = np.zeros((n_seg + 1, 3))
+    sites[:, 0] = np.arange(n_seg + 1) - 5.0
+    system = dict(n_dim=3, system_radius=20.0, delta=1e-3, stoch_flag=0, seed=0,
+                  interaction_flag=interaction)
+    fils = [dict(length=float(n_seg), persistence_length=100.0, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)]
+    return Oracle(system, fils, sites), sites
+
+
+def test_straight_rod_without_noise_or_interactions_stays_put():
+    o, sites = _straight_rod(0)
+    o.step(20)
+    assert np.allclose(o.sites(), sites, atol=1e-12)
+    assert np.abs(o.tensions()).max() < 1e-9
+
+
+def test_straight_rod_second_neighbour_bonds_repel():
+    """Bonds i and i+2 of one filament are not excluded (only bonds sharing a
+    site are, reference src/bond.cpp:118-121); on a straight rod with unit
+    bonds they are 1 sigma apart, inside the WCA cutoff, so candidate pairs
+    among them push with 24 eps/sigma and the tensions balance the push: the
+    rod does not move."""
+    o, sites = _straight_rod(1)
+    o.step(1)
+    f, _ = o.bond_forces()
+    assert np.allclose(np.abs(f[:, 0][f[:, 0] != 0]), 24.0)
+    assert np.abs(o.tensions()).max() > 1.0
+    o.step(19)
+    assert np.allclose(o.sites(), sites, atol=1e-12)
