@@ -36,6 +36,10 @@ sys.path.insert(0, ROOT)
 METRIC = "segment-steps/s, 1 B200: mixed+batched vs FP64 GPU at ≤1e-5 force err"
 UNIT = "segment-steps/s"
 I_STEPS_PER_STEP = 20
+# DRAM bytes (read + write) of one k_integrate launch of the default workload,
+# mixed precision, from ncu (cold cache): the mean of a midstep launch
+# (21.87 MB) and a full-step launch (39.48 MB), which alternate.
+TRAFFIC_K_INTEGRATE_MIXED = 30.67e6
 WORKLOAD_DESC = ("B: 20,000 filaments x 10 bonds (200,000 segments, 220,000 sites), 3D periodic "
                  "cube side 200, lp 100, WCA eps=sigma=1, dt 1e-4, noise on")
 
@@ -48,6 +52,10 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="B")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="run this many host-driven steps and exit (for ncu)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="precision of --profile-steps")
     return ap.parse_args()
 
 
@@ -146,12 +154,54 @@ def reduce_max(value, dist):
 
 
 def algorithmic_bytes(n_sites, n_bonds, n_pairs, precision):
-    """Bytes one reference step must move (per launch of the step kernel):
-    sites 96 B (r read + write, previous position, projected noise), bonds
-    112 B mixed / 208 B FP64 (geometry written and read, force/torque
-    accumulators), 8 B per candidate pair."""
-    per_bond = 112 if precision == "mixed" else 208
-    return 96 * n_sites + per_bond * n_bonds + 8 * n_pairs
+    """Bytes one reference step (i_step) must move, split by kernel.
+
+    Sites are FP64: r read and written, the previous position and the
+    projected noise read or written (96 B/site), all in the integrator.
+    Bond geometry (centre, u, l) is written by the integrator and read by the
+    pair kernel: 32 B mixed, 56 B FP64.  The per-bond force/torque
+    accumulators are written by the pair kernel and read by the integrator:
+    24 B mixed, 48 B FP64.  Each candidate pair costs 8 B of list read.
+    Returns (integrator bytes, pair-kernel bytes) per launch."""
+    geom, acc = (32, 24) if precision == "mixed" else (56, 48)
+    integrate = 96 * n_sites + (geom + acc) * n_bonds
+    pairs = (geom + acc) * n_bonds + 8 * n_pairs
+    return integrate, pairs
+
+
+def kernel_times(ctx, n):
+    """Average CUDA-event duration (ms) of the pair kernel and of the
+    integrator over n host-driven reference steps on the context's stream
+    (L2 warm, as between the reference steps inside one timed launch)."""
+    tp = ti = 0.0
+    for _ in range(n):
+        ctx.set_kernel_timing(True)
+        ctx.interact()
+        a, _ = ctx.kernel_timing()
+        ctx.set_kernel_timing(True)
+        ctx.update_positions()
+        b, _ = ctx.kernel_timing()
+        tp += a
+        ti += b
+    ctx.set_kernel_timing(False)
+    return tp / n, ti / n
+
+
+def profile_only(args):
+    """--profile-steps N: host-driven reference steps of the bench workload
+    (one pair launch and one integrator launch each) after 4 warm-up steps,
+    nothing timed; the command the ncu captures run."""
+    import simcore_b200 as sc
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make(args.workload, 1.0, seed=0)
+    ctx = sc.Context(system, fils, sites, precision=args.precision, device=0)
+    ctx.step(4)
+    ctx.step(args.profile_steps)
+    ctx.synchronize()
+    c = ctx.counters()
+    ctx.close()
+    print(json.dumps({"profile_steps": args.profile_steps, "precision": args.precision,
+                      "bonds": c.n_bonds, "pairs": c.n_pairs}))
 
 
 def run_ours(args, rank, world, local_rank):
@@ -210,14 +260,10 @@ def run_ours(args, rank, world, local_rank):
     if sampler:
         results["clocks"] = sampler.stop()
 
-    # Roofline of the dominant kernel (the fused step kernel), mixed path:
-    # per-launch CUDA-event durations on the host-driven path.
+    # Roofline: per-launch CUDA-event durations of the two kernels of a
+    # reference step, host-driven, on the context's stream.
+    kt = {p: kernel_times(contexts[p], 2 * I_STEPS_PER_STEP) for p in ("mixed", "fp64")}
     ctx = contexts["mixed"]
-    ctx.set_kernel_timing(True)
-    ctx.step(2 * I_STEPS_PER_STEP)
-    kms, kn = ctx.kernel_timing()
-    ctx.set_kernel_timing(False)
-    avg_kernel_ms = kms / max(kn, 1)
 
     # End to end through the C ABI with host buffers: upload positions,
     # run one bench step, read positions back.
@@ -246,8 +292,18 @@ def run_ours(args, rank, world, local_rank):
     value = seg_steps / (r["total_ms"] * 1e-3)
     value64 = seg_steps / (r64["total_ms"] * 1e-3)
     peak, peak_kind = load_measured_peaks()
-    bytes_per_launch = algorithmic_bytes(r["n_sites"], n_b, r["n_pairs"], "mixed")
-    achieved = bytes_per_launch / (avg_kernel_ms * 1e-3) / 1e9
+
+    def roof(prec):
+        rr = results[prec]
+        b_int, b_pair = algorithmic_bytes(rr["n_sites"], rr["n_bonds"], rr["n_pairs"], prec)
+        t_pair, t_int = kt[prec]
+        return b_int, b_pair, t_pair, t_int
+
+    b_int, b_pair, t_pair, t_int = roof("mixed")
+    achieved = b_int / (t_int * 1e-3) / 1e9
+    step_achieved = (b_int + b_pair) / ((t_int + t_pair) * 1e-3) / 1e9
+    b_int64, b_pair64, t_pair64, t_int64 = roof("fp64")
+    step64 = (b_int64 + b_pair64) / ((t_int64 + t_pair64) * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -265,10 +321,23 @@ def run_ours(args, rank, world, local_rank):
                  "rebuilds_in_timed_region": r64["rebuilds"]},
         "mixed_over_fp64": value / value64,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "kernel": "k_integrate<3,1,fused> (pair stage + integrator)",
-                     "algorithmic_bytes_per_launch": bytes_per_launch,
-                     "avg_launch_ms": avg_kernel_ms, "peak_kind": peak_kind + " hbm_gbs"},
+                     "frac": achieved / peak, "traffic": TRAFFIC_K_INTEGRATE_MIXED,
+                     "kernel": "k_integrate<3,mixed,fast> (dominant: one launch per reference "
+                               "step, all 20,000 filaments)",
+                     "algorithmic_bytes_per_launch": b_int, "avg_launch_ms": t_int,
+                     "peak_kind": peak_kind + " hbm_gbs",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
+                                       "launch of bench.py --profile-steps 8 (cold cache)",
+                     "pair_kernel": {"kernel": "k_pair_eval (mixed)", "avg_launch_ms": t_pair,
+                                     "algorithmic_bytes_per_launch": b_pair,
+                                     "achieved": b_pair / (t_pair * 1e-3) / 1e9},
+                     "reference_step": {"kernels": "k_pair_eval + k_integrate",
+                                        "algorithmic_bytes": b_int + b_pair,
+                                        "ms": t_int + t_pair, "achieved": step_achieved,
+                                        "frac": step_achieved / peak},
+                     "reference_step_fp64": {"algorithmic_bytes": b_int64 + b_pair64,
+                                             "ms": t_int64 + t_pair64, "achieved": step64,
+                                             "frac": step64 / peak}},
         "e2e": {"value": seg_steps / e2e_total, "unit": UNIT,
                 "h2d_bytes_per_step": 24 * r["n_sites"], "d2h_bytes_per_step": 24 * r["n_sites"]},
         "gpu_launches": int(r["launches"]),
@@ -350,6 +419,9 @@ def run_reference(args, rank, world):
 
 def main():
     args = parse_args()
+    if args.profile_steps:
+        profile_only(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

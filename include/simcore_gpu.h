@@ -110,6 +110,25 @@ sc_status sc_add_filaments(sc_ctx *ctx, int n, const sc_filament_params *p,
 /* Number of bonds the reference gives a filament (src/filament.cpp:142-147). */
 int sc_filament_n_bonds(const sc_filament_params *p);
 
+/* Static doubly-bound crosslinks: n harmonic tethers between sites site_a[k]
+ * and site_b[k] (global site indices), force k_spring (|dr| - rest_length)
+ * along the minimum-image separation of the two anchors, k_spring_compress
+ * instead when compressed and k_spring_compress >= 0 (Crosslink::
+ * CalculateTetherForces, src/crosslink.cpp:247-275).  An anchor on site j
+ * sits at the tail of bond j; on a filament's last site, at the head of the
+ * last bond.  Forces and torques go to the anchors' bonds
+ * (Anchor::ApplyAnchorForces, src/anchor.cpp:132-146), recomputed on even
+ * steps and re-applied unchanged on odd steps (CrosslinkSpecies::
+ * UpdatePositions, src/crosslink_species.cpp:218-238).  Active only with
+ * interaction_flag on, as the reference's Interact returns early otherwise.
+ * Once, after sc_add_filaments and before the first step. */
+sc_status sc_add_crosslinks(sc_ctx *ctx, int n, const int32_t *site_a,
+                            const int32_t *site_b, double k_spring,
+                            double k_spring_compress, double rest_length);
+/* Tether force of every link from its last recomputation (n x 3; anchor 0
+ * receives +F, anchor 1 -F). */
+sc_status sc_get_crosslink_forces(sc_ctx *ctx, double *f);
+
 /* InteractionManager::Interact for the next step: rebuild check, pair
  * forces and torques into the device bond accumulators. */
 sc_status sc_interact(sc_ctx *ctx);
@@ -211,11 +230,16 @@ sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
  * distributions of Mesh::InitRandomBond and Filament::InsertFilament,
  * src/mesh.cpp:244-258, src/filament.cpp:225-249,350-383, rejection of
  * InteractionManager::CheckOverlap, src/interaction_manager.cpp:561-571).
- * Writes sum(n_bonds[i] + 1) x 3 doubles. */
+ * insertion_type follows the filament species' insertion_type
+ * (Filament::InsertFirstBond, src/filament.cpp:192-222): SC_INSERT_RANDOM
+ * draws an isotropic first bond and later bonds from the bending
+ * distribution; SC_INSERT_RANDOM_NEMATIC / _POLAR place straight filaments
+ * along -+z / +z (y in 2D).  Writes sum(n_bonds[i] + 1) x 3 doubles. */
+enum { SC_INSERT_RANDOM = 0, SC_INSERT_RANDOM_NEMATIC = 1, SC_INSERT_RANDOM_POLAR = 2 };
 int sc_insert_filaments(int n_dim, double system_radius, uint64_t seed,
                         int n_fil, const int *n_bonds, const double *length,
                         const double *persistence_length, double diameter,
-                        int max_attempts, double *site_xyz);
+                        int insertion_type, int max_attempts, double *site_xyz);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,13 @@ struct sco_sim {
   long np, pcap;
   int *pa, *pb;
   double *pf;
+  /* static crosslinks: anchor 2k+a of link k sits on bond xbond[2k+a], at its
+   * tail (xhead 0, lambda = 0) or head (xhead 1, lambda = bond length) */
+  int nx;
+  int *xbond, *xhead;
+  double xk, xkc, xrest;
+  double *xc; /* 6 per anchor: the anchor's force_ and torque_ */
+  double *xF; /* 3 per link: Crosslink::force_ */
   /* control */
   int i_update;
   long n_rebuilds;
@@ -503,6 +510,84 @@ static double get_dr_max(sco_sim *s) {
   }
   if (max_dr > 10000) return -1.0;
   return max_dr;
+}
+
+/* ---- static crosslinks (config E) ----------------------------------------- */
+
+/* Anchor::UpdateAnchorPositionToBond (src/anchor.cpp:236-249) on a bond
+ * re-initialised from its sites, then Object::UpdatePeriodic: the anchor's
+ * scaled position, bond orientation, bond length and lambda. */
+static void anchor_state(const sco_sim *s, int anchor, double *sp, double *u,
+                         double *len, double *lambda) {
+  const int b = s->xbond[anchor];
+  const int site1 = b + filament_of_bond(s, b);
+  const double *r1 = V3(s->r, site1), *r2 = V3(s->r, site1 + 1);
+  double pos[3] = {0, 0, 0}, ap[3] = {0, 0, 0}, l = 0;
+  int i, n = s->n_dim;
+  for (i = 0; i < n; ++i) {
+    u[i] = r2[i] - r1[i];
+    l += u[i] * u[i];
+  }
+  l = sqrt(l);
+  for (i = 0; i < n; ++i) {
+    pos[i] = r1[i] + 0.5 * u[i];
+    u[i] /= l;
+  }
+  *len = l;
+  *lambda = s->xhead[anchor] ? l : 0.0;
+  for (i = 0; i < n; ++i) ap[i] = pos[i] - (0.5 * l - *lambda) * u[i];
+  periodic_bc(n, s->hinv, ap, sp);
+}
+
+/* Crosslink::CalculateTetherForces (src/crosslink.cpp:247-275) with
+ * MinimumDistance::PointPoint (src/minimum_distance.cpp:71-101), then the
+ * torque of Anchor::ApplyAnchorForces (src/anchor.cpp:132-146). */
+static void tether_forces(sco_sim *s) {
+  int k, i, a, n = s->n_dim;
+  for (k = 0; k < s->nx; ++k) {
+    double sp[2][3] = {{0}}, u[2][3] = {{0}}, len[2], lam[2];
+    double ds[3] = {0, 0, 0}, dr[3] = {0, 0, 0}, dr2 = 0, f[3] = {0, 0, 0};
+    double length, stretch, tf;
+    int j;
+    for (a = 0; a < 2; ++a) anchor_state(s, 2 * k + a, sp[a], u[a], &len[a], &lam[a]);
+    for (i = 0; i < n; ++i) {
+      ds[i] = sp[1][i] - sp[0][i];
+      ds[i] -= NINT(ds[i]);
+    }
+    for (i = 0; i < n; ++i) {
+      dr[i] = 0.0;
+      for (j = 0; j < n; ++j) dr[i] += s->h[n * i + j] * ds[j];
+    }
+    for (i = 0; i < n; ++i) dr2 += dr[i] * dr[i];
+    length = sqrt(dr2);
+    stretch = length - s->xrest;
+    tf = (s->xkc >= 0 && stretch < 0) ? s->xkc * stretch : s->xk * stretch;
+    for (i = 0; i < n; ++i) f[i] = tf * (dr[i] / length);
+    memcpy(s->xF + 3 * k, f, sizeof(f));
+    for (a = 0; a < 2; ++a) {
+      double *c = s->xc + 6 * (size_t)(2 * k + a);
+      double dl[3] = {0, 0, 0};
+      c[0] = c[1] = c[2] = 0.0;
+      for (i = 0; i < n; ++i) c[i] = a == 0 ? c[i] + f[i] : c[i] - f[i];
+      for (i = 0; i < n; ++i) dl[i] = (lam[a] - 0.5 * len[a]) * u[a][i];
+      cross3(dl, c, c + 3);
+    }
+  }
+}
+
+/* CrosslinkSpecies::UpdatePositions (src/crosslink_species.cpp:218-238):
+ * even i_steps recompute the tether forces, every i_step applies the stored
+ * anchor forces and torques in link order (ApplyCrosslinkTetherForces
+ * :260-266, Anchor::ApplyAnchorForces). */
+static void crosslink_update(sco_sim *s) {
+  int k, i;
+  if (s->i_step % 2 == 0) tether_forces(s);
+  for (k = 0; k < 2 * s->nx; ++k) {
+    const double *c = s->xc + 6 * (size_t)k;
+    const int b = s->xbond[k];
+    for (i = 0; i < s->n_dim; ++i) V3(s->bF, b)[i] += c[i];
+    for (i = 0; i < 3; ++i) V3(s->bT, b)[i] += c[3 + i];
+  }
 }
 
 /* CalculatePairInteractions + ApplyPairInteractions
@@ -997,6 +1082,7 @@ void sco_destroy(sco_sim *s) {
   free(s->r); free(s->rp); free(s->fr); free(s->F); free(s->tn); free(s->u);
   free(s->dz); free(s->dt); free(s->bp); free(s->bs); free(s->bu); free(s->bl);
   free(s->bF); free(s->bT); free(s->tens);
+  free(s->xbond); free(s->xhead); free(s->xc); free(s->xF);
   free(s->pa); free(s->pb); free(s->pf);
   free(s->w_cos); free(s->w_gl); free(s->w_gd); free(s->w_gu); free(s->w_dt);
   free(s->w_db); free(s->w_ginv); free(s->w_keff); free(s->w_hd); free(s->w_hu);
@@ -1022,7 +1108,9 @@ int sco_step(sco_sim *s, int nsteps) {
     memset(s->bF, 0, sizeof(double) * 3 * s->nb);
     memset(s->bT, 0, sizeof(double) * 3 * s->nb);
     if (s->interaction) {
-      double dr_max = get_dr_max(s);
+      double dr_max;
+      if (s->nx) crosslink_update(s); /* src/interaction_manager.cpp:70 */
+      dr_max = get_dr_max(s);
       if (dr_max < 0) return -1;
       if (dr_max > s->dr_update) update_interactions(s);
       pair_interactions(s, s->bF, s->bT, 1);
@@ -1032,6 +1120,39 @@ int sco_step(sco_sim *s, int nsteps) {
     s->species_midstep = !s->species_midstep;
   }
   return 0;
+}
+
+int sco_add_crosslinks(sco_sim *s, int n, const int *site_a, const int *site_b,
+                       double k_spring, double k_spring_compress, double rest_length) {
+  int k, a;
+  if (s->nx || n <= 0) return -1;
+  s->xbond = (int *)xcalloc(2 * (size_t)n, sizeof(int));
+  s->xhead = (int *)xcalloc(2 * (size_t)n, sizeof(int));
+  s->xc = (double *)xcalloc(12 * (size_t)n, sizeof(double));
+  s->xF = (double *)xcalloc(3 * (size_t)n, sizeof(double));
+  for (k = 0; k < n; ++k)
+    for (a = 0; a < 2; ++a) {
+      const int site = a == 0 ? site_a[k] : site_b[k];
+      int f = 0;
+      if (site < 0 || site >= s->ns) return -1;
+      while (s->fs_off[f + 1] <= site) ++f;
+      if (site - s->fs_off[f] < s->fb_off[f + 1] - s->fb_off[f]) {
+        s->xbond[2 * k + a] = site - f; /* bond j of site j: its tail */
+        s->xhead[2 * k + a] = 0;
+      } else {
+        s->xbond[2 * k + a] = site - f - 1; /* last site: head of the last bond */
+        s->xhead[2 * k + a] = 1;
+      }
+    }
+  s->nx = n;
+  s->xk = k_spring;
+  s->xkc = k_spring_compress;
+  s->xrest = rest_length;
+  return 0;
+}
+
+void sco_get_crosslink_forces(const sco_sim *s, double *f) {
+  memcpy(f, s->xF, sizeof(double) * 3 * (size_t)s->nx);
 }
 
 void sco_pair_forces(sco_sim *s, double *f, double *t) {

@@ -83,6 +83,15 @@ void sco_get_dr_tot(const sco_sim *s, double *dr);
  * bond geometry, as when a configuration is loaded. */
 void sco_set_sites(sco_sim *s, const double *xyz);
 
+/* Static doubly-bound crosslinks (harmonic tethers) between site_a[k] and
+ * site_b[k] (global site indices): an anchor on site j < last sits at the
+ * tail of bond j, an anchor on a filament's last site at the head of its last
+ * bond.  Once per simulation, before the first step.  Returns 0 or -1. */
+int sco_add_crosslinks(sco_sim *s, int n, const int *site_a, const int *site_b,
+                       double k_spring, double k_spring_compress, double rest_length);
+/* Tether force of each link from its last recomputation (anchor 0 gets +F). */
+void sco_get_crosslink_forces(const sco_sim *s, double *f);
+
 /* Pair forces alone, evaluated from the current bond geometry on the
  * current pair list with the pair forces stored so far, without changing
  * any state: bond forces/torques are written to f and t. */

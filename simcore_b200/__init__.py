@@ -32,7 +32,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_tensions", "sc_get_filament_state", "sc_get_dr_tot", "sc_get_pairs",
             "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_set_kernel_timing",
             "sc_get_kernel_timing", "sc_get_graph_time", "sc_set_fast_integrator",
-            "sc_pair_forces_noalloc", "sc_insert_filaments"]
+            "sc_pair_forces_noalloc", "sc_insert_filaments", "sc_add_crosslinks",
+            "sc_get_crosslink_forces"]
 
 
 class ScError(RuntimeError):
@@ -94,8 +95,11 @@ def filament_n_bonds(params):
     return lib.sc_filament_n_bonds(ctypes.byref(fp))
 
 
+INSERTION = {"random": 0, "random_nematic": 1, "random_polar": 2}
+
+
 def insert_filaments(n_dim, system_radius, seed, n_bonds, lengths, persistence_lengths,
-                     diameter=1.0, max_attempts=10000):
+                     diameter=1.0, max_attempts=10000, insertion="random"):
     """Seeded random insertion with overlap rejection (host).  Returns sites."""
     n_bonds = np.ascontiguousarray(n_bonds, dtype=np.int32)
     lengths = np.ascontiguousarray(lengths, dtype=np.float64)
@@ -104,6 +108,7 @@ def insert_filaments(n_dim, system_radius, seed, n_bonds, lengths, persistence_l
     rc = lib.sc_insert_filaments(ctypes.c_int(n_dim), ctypes.c_double(system_radius),
                                  ctypes.c_uint64(seed), ctypes.c_int(len(n_bonds)),
                                  _p(n_bonds), _p(lengths), _p(lps), ctypes.c_double(diameter),
+                                 ctypes.c_int(INSERTION[insertion]),
                                  ctypes.c_int(max_attempts), _p(xyz))
     if rc != SC_OK:
         raise ScError(rc, "random insertion failed")
@@ -158,6 +163,24 @@ class Context:
 
     def step_graph(self, n=1):
         self._check(lib.sc_step_graph(self.h, ctypes.c_int(n)))
+
+    def add_crosslinks(self, site_a, site_b, k_spring=10.0, k_spring_compress=-1.0,
+                       rest_length=0.0):
+        """Static doubly-bound tethers between global site indices."""
+        a = np.ascontiguousarray(site_a, dtype=np.int32)
+        b = np.ascontiguousarray(site_b, dtype=np.int32)
+        if a.shape != b.shape:
+            raise ValueError("site_a and site_b differ in length")
+        self.n_links = int(a.size)
+        self._check(lib.sc_add_crosslinks(self.h, ctypes.c_int(a.size), _p(a), _p(b),
+                                          ctypes.c_double(k_spring),
+                                          ctypes.c_double(k_spring_compress),
+                                          ctypes.c_double(rest_length)))
+
+    def crosslink_forces(self):
+        f = np.zeros((getattr(self, "n_links", 0), 3))
+        self._check(lib.sc_get_crosslink_forces(self.h, _p(f)))
+        return f
 
     def interact(self):
         self._check(lib.sc_interact(self.h))

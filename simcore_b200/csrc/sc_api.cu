@@ -343,8 +343,16 @@ sc_status timed(sc_ctx *c, F launch) {
   return SC_OK;
 }
 
+// Crosslinks of Interact (src/interaction_manager.cpp:70): on even steps the
+// tethers are recomputed; odd steps re-use the stored anchor contributions.
+void tether_if_due(sc_ctx *c) {
+  if (c->desc.interaction_flag && c->d.nx && c->i_step % 2 == 0)
+    c->launches += sc::launch_tether(c->k, c->d, c->st);
+}
+
 sc_status step_once(sc_ctx *c) {
   c->i_step++;
+  tether_if_due(c);
   CKS(maybe_rebuild(c));
   const int interaction = c->desc.interaction_flag ? 1 : 0;
   if (interaction)
@@ -679,6 +687,7 @@ sc_status sc_interact(sc_ctx *c) {
   CK(cudaSetDevice(c->desc.device));
   // ZeroForces + Interact of the next step.
   c->i_step++;
+  tether_if_due(c);
   CKS(maybe_rebuild(c));
   if (c->desc.interaction_flag)
     CKS(timed(c, [&] {
@@ -771,6 +780,8 @@ static sc_status build_graph(sc_ctx *c) {
                                    tail.size(), cudaStreamCaptureModeRelaxed));
   for (int half = 0; half < 2; ++half) {
     const int rb = half == 0 ? c->rbuf : 1 - c->rbuf;
+    // The second half is the even (full) step: crosslink tethers first.
+    if (half == 1 && interaction) sc::launch_tether(c->k, c->d, c->st);
     if (interaction) sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st);
     sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
                          c->capture, c->prec, c->fast, c->st);
@@ -825,7 +836,7 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
     }
     // Kernels the graph ran: loop head, per BD step decide + 2 steps + tail,
     // per rebuild the captured rebuild sequence.
-    c->launches += 1 + (long long)bd * (c->desc.interaction_flag ? 6 : 3) +
+    c->launches += 1 + (long long)bd * (c->desc.interaction_flag ? (c->d.nx ? 7 : 6) : 3) +
                    (nr1 - nr0) * c->rebuild_kernels;
     unsigned st = c->hb->status;
     if (st & sc::ST_UNPHYSICAL) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result");
@@ -890,6 +901,74 @@ sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
   CK(cudaGetLastError());
   CKS(copy_soa3(c, c->d.bF, c->nb, f));
   return copy_soa3(c, c->d.bT, c->nb, t);
+}
+
+sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32_t *site_b,
+                            double k_spring, double k_spring_compress, double rest_length) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  if (c->d.nx) return fail(c, SC_ERR_INVALID_ARG, "crosslinks already added");
+  if (c->i_step != 0) return fail(c, SC_ERR_INVALID_ARG, "crosslinks must be added before the first step");
+  if (n <= 0 || !site_a || !site_b) return fail(c, SC_ERR_INVALID_ARG, "bad crosslink arrays");
+  if (!(k_spring >= 0) || !(rest_length >= 0))
+    return fail(c, SC_ERR_INVALID_ARG, "bad spring constants");
+  CK(cudaSetDevice(c->desc.device));
+  // Anchor on site j of a filament: tail of bond j; on the last site: head of
+  // the last bond (lambda = bond length, as an end-paused anchor).
+  std::vector<int> anchor(2 * (size_t)n);
+  for (int x = 0; x < n; ++x)
+    for (int a = 0; a < 2; ++a) {
+      const int site = a == 0 ? site_a[x] : site_b[x];
+      if (site < 0 || site >= c->ns)
+        return fail(c, SC_ERR_INVALID_ARG, "crosslink %d: site %d out of range", x, site);
+      const int f = (int)(std::upper_bound(c->site_off.begin(), c->site_off.end(), site) -
+                          c->site_off.begin()) - 1;
+      const bool last = site == c->site_off[f + 1] - 1;
+      const int bond = last ? site - f - 1 : site - f;
+      anchor[2 * (size_t)x + a] = bond << 1 | (last ? 1 : 0);
+    }
+  // Per-bond anchor lists, ascending anchor id (link order, anchor 0 first).
+  std::vector<int> off(c->nb + 1, 0), ent(2 * (size_t)n);
+  for (int e = 0; e < 2 * n; ++e) off[(anchor[e] >> 1) + 1]++;
+  for (int b = 0; b < c->nb; ++b) off[b + 1] += off[b];
+  {
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int e = 0; e < 2 * n; ++e) ent[fill[anchor[e] >> 1]++] = e;
+  }
+  auto up = [&](int **dst, const std::vector<int> &v) -> sc_status {
+    int *q = nullptr;
+    CKS(dalloc(c, &q, v.size()));
+    CK(cudaMemcpyAsync(q, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, c->st));
+    *dst = q;
+    return SC_OK;
+  };
+  int *q = nullptr;
+  CKS(up(&q, anchor)); c->d.xl_anchor = q;
+  CKS(up(&q, off)); c->d.xb_off = q;
+  CKS(up(&q, ent)); c->d.xb_ent = q;
+  CKS(dalloc(c, &c->d.xl_c, 16 * (size_t)n));
+  CK(cudaMemsetAsync(c->d.xl_c, 0, sizeof(double) * 16 * (size_t)n, c->st));
+  CKS(dalloc(c, &c->d.xl_F, 4 * (size_t)n));
+  CK(cudaMemsetAsync(c->d.xl_F, 0, sizeof(double) * 4 * (size_t)n, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->k.xk = k_spring;
+  c->k.xkc = k_spring_compress;
+  c->k.xrest = rest_length;
+  c->d.nx = n;
+  drop_graph(c);  // kernel parameters changed
+  return SC_OK;
+}
+
+sc_status sc_get_crosslink_forces(sc_ctx *c, double *f) {
+  if (!c || !c->loaded || !f) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  if (c->d.nx == 0) return SC_OK;
+  std::vector<double> tmp(4 * (size_t)c->d.nx);
+  CK(cudaMemcpyAsync(tmp.data(), c->d.xl_F, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int x = 0; x < c->d.nx; ++x)
+    for (int i = 0; i < 3; ++i) f[3 * (size_t)x + i] = tmp[4 * (size_t)x + i];
+  return SC_OK;
 }
 
 sc_status sc_get_bond_geometry(sc_ctx *c, double *pos, double *spos, double *u,

@@ -68,6 +68,7 @@ struct SysConst {
   uint32_t seed;
   int stoch;
   int like_like;
+  double xk, xkc, xrest;  // crosslink tether: k_spring, k_spring_compress, rest_length
 };
 
 // Per-filament constants of the integrator.  The reciprocals are the
@@ -112,6 +113,13 @@ struct DevState {
   int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
   double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
   float *cf32;
+  // static crosslinks (harmonic tethers between two bonds)
+  int nx;                  // links
+  const int *xl_anchor;    // 2 per link: bond << 1 | head (anchor at the bond's head)
+  double *xl_c;            // 8 per anchor: force (3), torque (3), pad (2)
+  double *xl_F;            // 4 per link: tether force (Crosslink::force_), pad
+  const int *xb_off;       // nb+1 CSR of anchors per bond
+  const int *xb_ent;       // anchor ids (2 link + a), ascending per bond
   // capture (optional)
   double *cap_F[3];
   double *cap_T;

@@ -126,10 +126,11 @@ extern "C" int sc_insert_filaments(int n_dim, double system_radius,
                                    uint64_t seed, int n_fil,
                                    const int *n_bonds, const double *length,
                                    const double *persistence_length,
-                                   double diameter, int max_attempts,
-                                   double *site_xyz) {
+                                   double diameter, int insertion_type,
+                                   int max_attempts, double *site_xyz) {
   if ((n_dim != 2 && n_dim != 3) || n_fil <= 0 || !n_bonds || !length ||
-      !persistence_length || !site_xyz || system_radius <= diameter)
+      !persistence_length || !site_xyz || system_radius <= diameter ||
+      insertion_type < SC_INSERT_RANDOM || insertion_type > SC_INSERT_RANDOM_POLAR)
     return SC_ERR_INVALID_ARG;
   const double L = 2.0 * system_radius;
   double max_bond = 0;
@@ -153,23 +154,32 @@ extern "C" int sc_insert_filaments(int n_dim, double system_radius,
       cen.assign(3 * nb, 0.0);
       axis.assign(3 * nb, 0.0);
       double u[3] = {0, 0, 0}, p[3] = {0, 0, 0};
-      // RNG::RandomUnitVector (src/rng.cpp:34-49)
-      double w = 1.0;
-      if (n_dim == 3) {
-        double z = 2.0 * rng.uniform() - 1.0;
-        w = std::sqrt(1 - z * z);
-        u[2] = z;
+      if (insertion_type == SC_INSERT_RANDOM) {
+        // RNG::RandomUnitVector (src/rng.cpp:34-49)
+        double w = 1.0;
+        if (n_dim == 3) {
+          double z = 2.0 * rng.uniform() - 1.0;
+          w = std::sqrt(1 - z * z);
+          u[2] = z;
+        }
+        double t = 2.0 * M_PI * rng.uniform();
+        u[0] = w * std::cos(t);
+        u[1] = w * std::sin(t);
+      } else {
+        // Filament::InsertFirstBond, random_nematic / random_polar
+        // (src/filament.cpp:195-202): along +-z (+-y in 2D), straight.
+        u[n_dim - 1] = insertion_type == SC_INSERT_RANDOM_POLAR
+                           ? 1.0
+                           : (rng.uniform() > 0.5 ? 1.0 : -1.0);
       }
-      double t = 2.0 * M_PI * rng.uniform();
-      u[0] = w * std::cos(t);
-      u[1] = w * std::sin(t);
       // RNG::RandomCoordinate, box/none (src/rng.cpp:50-66)
       for (int i = 0; i < n_dim; ++i)
         p[i] = (2.0 * rng.uniform() - 1.0) * (system_radius - diameter);
       for (int i = 0; i < n_dim; ++i) p[i] -= 0.5 * u[i] * length[f];
       for (int i = 0; i < 3; ++i) pos[i] = p[i];
       for (int b = 0; b < nb; ++b) {
-        if (b > 0) {  // Filament::GenerateProbableOrientation
+        if (b > 0 && insertion_type == SC_INSERT_RANDOM) {
+          // Filament::GenerateProbableOrientation
           double k = lp / l, theta;
           if (lp == 0) {
             theta = rng.uniform() * M_PI;

@@ -477,6 +477,94 @@ __global__ void k_bond_sum(DevState d) {
   }
 }
 
+// Crosslink tethers, recomputed on even steps (CrosslinkSpecies::
+// UpdateBoundCrosslinks, src/crosslink_species.cpp:218-258), one thread per
+// link.  Each anchor is placed on its bond re-initialised from the current
+// sites (Bond::ReInit, src/bond.cpp:22-37, then Anchor::
+// UpdateAnchorPositionToBond, src/anchor.cpp:236-249, and
+// periodic_boundary_conditions); the tether follows Crosslink::
+// CalculateTetherForces (src/crosslink.cpp:247-275) with MinimumDistance::
+// PointPoint (src/minimum_distance.cpp:71-101); each anchor's force and its
+// torque (lambda - l/2) u x f are stored as Anchor::ApplyAnchorForces
+// (src/anchor.cpp:132-146) computes them, for re-use on the odd step.
+template <int ND>
+__global__ void k_tether(SysConst k, DevState d) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= d.nx) return;
+  double sp[2][3], ua[2][3], len[2], lam[2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    const int code = d.xl_anchor[2 * x + a];
+    const int b = code >> 1;
+    const int s1 = b + d.bond_fil[b];
+    double r1[3], r2[3], pos[3] = {0, 0, 0}, ap[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      r1[i] = d.r[i][s1];
+      r2[i] = d.r[i][s1 + 1];
+    }
+    double l = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) ua[a][i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      ua[a][i] = r2[i] - r1[i];
+      l += ua[a][i] * ua[a][i];
+    }
+    l = sqrt(l);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      pos[i] = r1[i] + 0.5 * ua[a][i];
+      ua[a][i] /= l;
+    }
+    len[a] = l;
+    lam[a] = (code & 1) ? l : 0.0;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) ap[i] = pos[i] - (0.5 * l - lam[a]) * ua[a][i];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      double v = 0.0;
+#pragma unroll
+      for (int j = 0; j < ND; ++j) v += k.hinv[ND * i + j] * ap[j];
+      sp[a][i] = v - nint(v);
+    }
+  }
+  double dr[3] = {0, 0, 0}, dr2 = 0.0, f[3] = {0, 0, 0};
+  double ds[3] = {0, 0, 0};
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    ds[i] = sp[1][i] - sp[0][i];
+    ds[i] -= nint(ds[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    double v = 0.0;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) v += k.h[ND * i + j] * ds[j];
+    dr[i] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < ND; ++i) dr2 += dr[i] * dr[i];
+  const double length = sqrt(dr2);
+  const double stretch = length - k.xrest;
+  const double tf = (k.xkc >= 0 && stretch < 0) ? k.xkc * stretch : k.xk * stretch;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) f[i] = tf * (dr[i] / length);
+  reinterpret_cast<double4 *>(d.xl_F)[x] = make_double4(f[0], f[1], f[2], 0.0);
+#pragma unroll
+  for (int a = 0; a < 2; ++a) {
+    double c[3] = {0.0, 0.0, 0.0}, dl[3] = {0.0, 0.0, 0.0}, t[3];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) c[i] = a == 0 ? c[i] + f[i] : c[i] - f[i];
+#pragma unroll
+    for (int i = 0; i < ND; ++i) dl[i] = (lam[a] - 0.5 * len[a]) * ua[a][i];
+    cross3(dl, c, t);
+    double4 *o = reinterpret_cast<double4 *>(d.xl_c) + 2 * (size_t)(2 * x + a);
+    o[0] = make_double4(c[0], c[1], c[2], t[0]);
+    o[1] = make_double4(t[1], t[2], 0.0, 0.0);
+  }
+}
+
 // Slot of each (pair, role) entry after the per-bond sort.
 __global__ void k_csr_pos(DevState d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -629,6 +717,13 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
     if (prec == 0) k_pair_eval<2, 0><<<grid, 256, 0, st>>>(k, d, rbuf);
     else k_pair_eval<2, 1><<<grid, 256, 0, st>>>(k, d, rbuf);
   }
+  return 1;
+}
+
+int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st) {
+  if (d.nx == 0) return 0;
+  if (k.n_dim == 3) k_tether<3><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
+  else k_tether<2><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
   return 1;
 }
 

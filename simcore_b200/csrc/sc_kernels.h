@@ -39,6 +39,8 @@ int launch_zero_dr(const DevState &d, cudaStream_t st);
 // Grid sized for `expected` pairs; the kernel strides over the actual count.
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
                  int expected, cudaStream_t st);
+// Crosslink tethers of an even step into the per-anchor contributions.
+int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st);
 int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st);
 size_t integrate_smem_bytes(int C);
 void prepare_integrate(int C);

@@ -96,16 +96,39 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float x) {
   sum = t;
 }
 
-// Sum of one bond's pair contributions in slot (= pair) order: FP64 sums as
-// the reference accumulates Object::force_/torque_, FP32 with Kahan
-// compensation.  A slot is 8 values: force (3), torque (3), padding (2).
+// Sum of one bond's crosslink anchor contributions in link order, as
+// CrosslinkSpecies::ApplyCrosslinkTetherForces adds them to Bond::force_ /
+// torque_ before the pair path (src/crosslink_species.cpp:260-266,
+// src/anchor.cpp:132-146): ND force components, 3 torque components.
+template <int ND>
+__device__ __forceinline__ void bond_xlink_sum(const DevState &d, int b, double F[3],
+                                               double T[3]) {
+  const int e0 = d.xb_off[b], e1 = d.xb_off[b + 1];
+  for (int e = e0; e < e1; ++e) {
+    const double2 *c = reinterpret_cast<const double2 *>(d.xl_c) + 4 * (size_t)d.xb_ent[e];
+    const double2 v0 = c[0], v1 = c[1], v2 = c[2];
+    F[0] += v0.x;
+    F[1] += v0.y;
+    if (ND == 3) F[2] += v1.x;
+    T[0] += v1.y;
+    T[1] += v2.x;
+    T[2] += v2.y;
+  }
+}
+
+// Bond::force_ / torque_ after Interact: crosslink anchors first, then the
+// bond's pair contributions in slot (= pair) order.  FP64 sums as the
+// reference accumulates them; FP32 pair sums with Kahan compensation, added
+// to the FP64 crosslink sum.  A pair slot is 8 values: force (3), torque (3),
+// padding (2).
 template <int ND, int PREC>
 __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F[3],
                                               double T[3]) {
   const int e0 = d.e_off[b], e1 = d.e_off[b + 1];
+  F[0] = F[1] = F[2] = 0.0;
+  T[0] = T[1] = T[2] = 0.0;
+  if (d.nx) bond_xlink_sum<ND>(d, b, F, T);
   if (PREC == 0) {
-    F[0] = F[1] = F[2] = 0.0;
-    T[0] = T[1] = T[2] = 0.0;
     const double2 *c = reinterpret_cast<const double2 *>(d.cf64) + 4 * (size_t)e0;
 #pragma unroll 2
     for (int e = e0; e < e1; ++e, c += 4) {
@@ -133,8 +156,8 @@ __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F
     }
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
-      F[i] = (double)sF[i] - (double)cF[i];
-      T[i] = (double)sT[i] - (double)cT[i];
+      F[i] += (double)sF[i] - (double)cF[i];
+      T[i] += (double)sT[i] - (double)cT[i];
     }
   }
 }
@@ -404,7 +427,12 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
 #pragma unroll
         for (int i = 0; i < ND; ++i)
           xi[i] = ((double)w[i] + 0.5) * 2.3283064365386963e-10 - 0.5;
-        if (ND == 2) {
+        if (FAST) {
+          // (t t^T) xi = (t . xi) t
+          const double txi = dotn<ND>(tn, xi);
+#pragma unroll
+          for (int i = 0; i < ND; ++i) xt[i] = txi * tn[i];
+        } else if (ND == 2) {
           xt[0] = tn[0] * tn[0] * xi[0] + tn[0] * tn[1] * xi[1];
           xt[1] = tn[1] * tn[1] * xi[1] + tn[0] * tn[1] * xi[0];
         } else {
@@ -496,7 +524,32 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
     skeff[t] = (fc.kappa + fc.l * ginv) / fc.l2;
   }
   __syncthreads();
-  if (active) {
+  if (active && FAST) {
+    // (I - u2 u2^T) u1 = u1 - (u1 . u2) u2 with the cosines of
+    // CalculateAngles: the reference's three stencil terms in vector form.
+    double fs[3] = {0, 0, 0};
+    const int kk = j;
+    if (kk > 1) {
+      const double ke = skeff[t - 2], c = scos[t - 2];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) fs[i] += ke * (V(su, t - 2, i) - c * V(su, t - 1, i));
+    }
+    if (kk > 0 && kk < n - 1) {
+      const double ke = skeff[t - 1], c = scos[t - 1];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        const double um = V(su, t - 1, i);
+        fs[i] += ke * ((u[i] - c * um) - (um - c * u[i]));
+      }
+    }
+    if (kk < n - 2) {
+      const double ke = skeff[t], c = scos[t];
+#pragma unroll
+      for (int i = 0; i < ND; ++i) fs[i] -= ke * (V(su, t + 1, i) - c * u[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) F[i] += fs[i];
+  } else if (active) {
     double fs[3] = {0, 0, 0};
     const int kk = j;
     if (ND == 2) {
@@ -574,12 +627,22 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
   auto gam = [&](int a, int c) -> double {
     return fc.igpar * (tn[a] * tn[c]) + fc.igperp * ((a == c ? 1 : 0) - tn[a] * tn[c]);
   };
+  // FAST: gamma^-1 F = F / g_perp + (1/g_par - 1/g_perp) (t . F) t
+  auto gamF = [&](int i, const double *Fv, double tF) -> double {
+    return fc.igperp * Fv[i] + fc.dgam * tF * tn[i];
+  };
   if (active) {
     // gamma^-1 F of this site: "temp_a" of row j and "temp_b" of row j-1.
+    const double tF = FAST ? dotn<ND>(tn, F) : 0.0;
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
-      double v = gam(i, 0) * F[0] + gam(i, 1) * F[1];
-      if (ND == 3) v += gam(i, 2) * F[2];
+      double v;
+      if (FAST) {
+        v = gamF(i, F, tF);
+      } else {
+        v = gam(i, 0) * F[0] + gam(i, 1) * F[1];
+        if (ND == 3) v += gam(i, 2) * F[2];
+      }
       V(sbF, t, i) = v;
     }
   }
@@ -627,10 +690,16 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
     double rp[3] = {r[0], r[1], r[2]};  // midstep: the previous positions are these
     if (!midstep)
       for (int i = 0; i < ND; ++i) rp[i] = V(srp, t, i);
+    const double tF = FAST ? dotn<ND>(tn, F) : 0.0;
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
-      double ft = gam(i, 0) * F[0] + gam(i, 1) * F[1];
-      if (ND == 3) ft += gam(i, 2) * F[2];
+      double ft;
+      if (FAST) {
+        ft = gamF(i, F, tF);
+      } else {
+        ft = gam(i, 0) * F[0] + gam(i, 1) * F[1];
+        if (ND == 3) ft += gam(i, 2) * F[2];
+      }
       r[i] = rp[i] + dl * ft;
     }
     for (int i = 0; i < 3; ++i) V(sr, t, i) = r[i];

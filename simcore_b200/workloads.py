@@ -10,7 +10,10 @@ rejection (sc_insert_filaments); no dataset is involved.
   A  100 x 20 bonds, lp 500, side 50, dt 1e-4          (CPU parity case)
   B  20,000 x 10 bonds, lp 100, side 200, dt 1e-4       (dense suspension)
   C  50,000 x log-uniform[5,200] bonds, lp U[10,1000], side 300, dt 5e-5
-  E  10,000 x 50 bonds, lp 1000, side 150, dt 1e-4      (network geometry)
+  E  10,000 x 50 bonds, lp 1000, side 150, dt 1e-4      (network geometry;
+     volume fraction 0.116 is above the isotropic-nematic point of 50:1 rods,
+     so the filaments are inserted straight along -+z, random_nematic)
+     plus 100,000 static tethers, k 10, rest length 1 (crosslinks())
 
 scale < 1 shrinks the filament count and the box volume together (same
 density) for parity tests at small sizes.
@@ -19,7 +22,7 @@ import math
 
 import numpy as np
 
-from . import insert_filaments
+from . import filament_n_bonds, insert_filaments
 
 MIN_BOND_LENGTH = 0.666
 DIAMETER = 1.0
@@ -30,8 +33,41 @@ WORKLOADS = {
     "B": dict(n_dim=3, side=200.0, n_fil=20000, n_seg=10, lp=100.0, delta=1e-4, n_steps=2000),
     "C": dict(n_dim=3, side=300.0, n_fil=50000, n_seg=("loguniform", 5, 200),
               lp=("uniform", 10.0, 1000.0), delta=5e-5, n_steps=1000),
-    "E": dict(n_dim=3, side=150.0, n_fil=10000, n_seg=50, lp=1000.0, delta=1e-4, n_steps=1000),
+    "E": dict(n_dim=3, side=150.0, n_fil=10000, n_seg=50, lp=1000.0, delta=1e-4, n_steps=1000,
+              insertion="random_nematic"),
 }
+
+
+CROSSLINKS = {"E": dict(n_links=100000, k_spring=10.0, rest_length=1.0, reach=2.0)}
+
+
+def crosslinks(name, sites, filaments, side, scale=1.0, seed=0):
+    """Static tethers of workload `name`: site pairs drawn uniformly from all
+    pairs closer than `reach` (minimum image) that are not the same or
+    adjacent sites of one filament.  Returns (site_a, site_b, k_spring,
+    rest_length), or None for a workload without crosslinks."""
+    if name not in CROSSLINKS:
+        return None
+    from scipy.spatial import cKDTree
+    c = CROSSLINKS[name]
+    n_dim = 3 if np.any(sites[:, 2] != 0) else 2
+    pts = np.mod(sites[:, :n_dim], side)
+    pts[pts >= side] = 0.0
+    tree = cKDTree(pts, boxsize=side)
+    pairs = tree.query_pairs(c["reach"], output_type="ndarray")
+    n_sites = np.array([filament_n_bonds(f) + 1 for f in filaments])
+    fil = np.repeat(np.arange(len(filaments)), n_sites)
+    same = (fil[pairs[:, 0]] == fil[pairs[:, 1]]) & (np.abs(pairs[:, 0] - pairs[:, 1]) <= 1)
+    pairs = pairs[~same]
+    d = sites[pairs[:, 0], :n_dim] - sites[pairs[:, 1], :n_dim]
+    d -= side * np.round(d / side)
+    pairs = pairs[np.einsum("ij,ij->i", d, d) < c["reach"] ** 2]  # strictly closer
+    pairs = pairs[np.lexsort((pairs[:, 1], pairs[:, 0]))]
+    n = min(len(pairs), max(1, int(round(c["n_links"] * scale))))
+    rng = np.random.default_rng(seed + 777)
+    pick = pairs[rng.choice(len(pairs), size=n, replace=False)]
+    return (pick[:, 0].astype(np.int32), pick[:, 1].astype(np.int32), c["k_spring"],
+            c["rest_length"])
 
 
 def describe(name):
@@ -39,18 +75,23 @@ def describe(name):
     return dict(w)
 
 
-def make(name, scale=1.0, seed=0, precision_seed=None, stoch=True, interaction=True):
-    """Returns (system, filaments, sites) for workload `name`."""
+def make(name, scale=1.0, seed=0, precision_seed=None, stoch=True, interaction=True,
+         n_seg=None, side=None):
+    """Returns (system, filaments, sites) for workload `name`.  For small test
+    systems that full-length filaments would not fit: n_seg replaces the
+    bonds per filament, side the box side (lower density)."""
     w = WORKLOADS[name]
     n_fil = max(2, int(round(w["n_fil"] * scale)))
-    side = w["side"] * (scale ** (1.0 / w["n_dim"]))
+    if side is None:
+        side = w["side"] * (scale ** (1.0 / w["n_dim"]))
     rng = np.random.default_rng(seed + 12345)
-    if isinstance(w["n_seg"], tuple):
-        _, lo, hi = w["n_seg"]
+    seg = w["n_seg"] if n_seg is None else int(n_seg)
+    if isinstance(seg, tuple):
+        _, lo, hi = seg
         n_seg = np.clip(np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), n_fil))),
                         lo, hi).astype(np.int32)
     else:
-        n_seg = np.full(n_fil, w["n_seg"], dtype=np.int32)
+        n_seg = np.full(n_fil, seg, dtype=np.int32)
     if isinstance(w["lp"], tuple):
         _, lo, hi = w["lp"]
         lp = rng.uniform(lo, hi, n_fil)
@@ -58,7 +99,7 @@ def make(name, scale=1.0, seed=0, precision_seed=None, stoch=True, interaction=T
         lp = np.full(n_fil, w["lp"])
     lengths = n_seg.astype(np.float64)  # bond length 1
     sites = insert_filaments(w["n_dim"], 0.5 * side, seed, n_seg, lengths, lp,
-                             diameter=DIAMETER)
+                             diameter=DIAMETER, insertion=w.get("insertion", "random"))
     system = dict(n_dim=w["n_dim"], system_radius=0.5 * side, delta=w["delta"],
                   wca_eps=1.0, wca_sig=1.0, f_cutoff=2000.0,
                   stoch_flag=1 if stoch else 0, interaction_flag=1 if interaction else 0,

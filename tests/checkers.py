@@ -185,6 +185,23 @@ class Oracle(_Checker):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         self._call("set_sites", _ptr(xyz))
 
+    def add_crosslinks(self, site_a, site_b, k_spring=10.0, k_spring_compress=-1.0,
+                       rest_length=0.0):
+        a = np.ascontiguousarray(site_a, dtype=np.int32)
+        b = np.ascontiguousarray(site_b, dtype=np.int32)
+        self.n_links = int(a.size)
+        self.lib.sco_add_crosslinks.restype = ctypes.c_int
+        rc = self._call("add_crosslinks", ctypes.c_int(a.size), _ptr(a), _ptr(b),
+                        ctypes.c_double(k_spring), ctypes.c_double(k_spring_compress),
+                        ctypes.c_double(rest_length))
+        if rc != 0:
+            raise RuntimeError("oracle rejected the crosslinks")
+
+    def crosslink_forces(self):
+        f = np.zeros((getattr(self, "n_links", 0), 3))
+        self._call("get_crosslink_forces", _ptr(f))
+        return f
+
     def frictions(self):
         out = [np.zeros(self.n_fil) for _ in range(4)]
         self._call("get_frictions", *[_ptr(a) for a in out])

@@ -174,3 +174,78 @@ def test_fast_integrator_close_to_exact():
     scale = np.abs(rb).max()
     assert np.abs(ra - rb).max() <= 1e-12 * scale
     ta, tb = a.tensions(), b.tensions()
+
+
+def _workload_E(scale, seed=0):
+    """Workload E's density, stiffness and tethers, with 10-bond filaments so
+    that a small box holds them."""
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("E", scale=scale, seed=seed, n_seg=10)
+    a, b, k, rest = workloads.crosslinks("E", sites, fils, 2 * system["system_radius"],
+                                         scale=scale, seed=seed)
+    return system, fils, sites, (a, b, k, rest)
+
+
+def test_crosslinks_fp64_bitwise():
+    """Workload E at 1/100 scale (100 x 10 bonds, up to 1,000 tethers): the
+    tether kernel, the per-bond anchor sums and the stale odd-step forces are
+    bit-identical to the oracle, host-driven and through the captured graph."""
+    system, fils, sites, (a, b, k, rest) = _workload_E(0.01, seed=4)
+    ctx = _ctx(system, fils, sites)
+    ctx.set_capture(True)
+    o = Oracle(system, fils, sites)
+    ctx.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+    o.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+    for _ in range(4):
+        ctx.step(1)
+        o.step(1)
+        compare_state(ctx, o, 3)
+        assert_same(ctx.crosslink_forces(), o.crosslink_forces(), "tether forces")
+    assert np.abs(o.crosslink_forces()).max() > 0
+    ctx.set_capture(False)
+    for n in (41, 60):
+        ctx.step_graph(n)
+        o.step(n)
+        compare_state(ctx, o, 3, capture=False)
+        assert_same(ctx.crosslink_forces(), o.crosslink_forces(), "tether forces")
+
+
+def test_crosslinks_mixed_close():
+    """Mixed precision with tethers, one step after identical starts: bond
+    forces (FP64 tethers plus FP32 pair sums) and tether forces within 1e-5
+    (relative to the largest) of the FP64 path."""
+    system, fils, sites, (a, b, k, rest) = _workload_E(0.01, seed=5)
+    c64 = _ctx(system, fils, sites, "fp64")
+    c32 = _ctx(system, fils, sites, "mixed")
+    for c in (c64, c32):
+        c.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+        c.step(1)
+        c.interact()
+    f64, t64 = c64.bond_forces()
+    f32, t32 = c32.bond_forces()
+    assert np.abs(f32 - f64).max() / np.abs(f64).max() <= 1e-5
+    assert np.abs(t32 - t64).max() / np.abs(t64).max() <= 1e-5
+    x32, x64 = c32.crosslink_forces(), c64.crosslink_forces()
+    assert np.abs(x32 - x64).max() <= 1e-5 * np.abs(x64).max()
+
+
+def test_fp64_uneven_lengths_bitwise():
+    """Workload C's length and stiffness spread (5 to 200 bonds, log-uniform;
+    lp uniform in [10, 1000]) on 100 filaments: 256-site integrator blocks
+    holding filaments of mixed lengths, bit-identical to the oracle over
+    host-driven and captured steps with rebuilds."""
+    system, fils, sites = _workload("C", 0.002, seed=3, side=150.0)
+    assert max(f["length"] for f in fils) > 128
+    ctx = _ctx(system, fils, sites)
+    ctx.set_capture(True)
+    o = Oracle(system, fils, sites)
+    for _ in range(3):
+        ctx.step(1)
+        o.step(1)
+        compare_state(ctx, o, 3)
+    ctx.set_capture(False)
+    for n in (101, 100):
+        ctx.step_graph(n)
+        o.step(n)
+        compare_state(ctx, o, 3, capture=False)
+    assert o.n_rebuilds > 0

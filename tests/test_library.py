@@ -109,3 +109,19 @@ def test_replicas_reduce_max_over_gloo_ranks():
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert [g[1] for g in got] == [11.0, 11.0]
     assert got[0][2] != got[1][2]  # each replica its own seed
+
+
+def test_workload_E_crosslinks():
+    """Tethers of workload E: distinct site pairs within reach (minimum
+    image), never the same or adjacent sites of one filament."""
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("E", scale=0.01, seed=1, n_seg=10)
+    side = 2 * system["system_radius"]
+    a, b, k, rest = workloads.crosslinks("E", sites, fils, side, scale=0.01, seed=1)
+    assert 100 < len(a) <= 1000 and k == 10.0 and rest == 1.0
+    d = sites[a] - sites[b]
+    d -= side * np.round(d / side)
+    assert np.all(np.sqrt((d ** 2).sum(1)) < 2.0)
+    fil = np.repeat(np.arange(len(fils)), 11)
+    assert not np.any((fil[a] == fil[b]) & (np.abs(a - b) <= 1))
+    assert len(set(zip(a.tolist(), b.tolist()))) == len(a)

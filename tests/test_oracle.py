@@ -170,3 +170,61 @@ def test_straight_rod_second_neighbour_bonds_repel():
     assert np.abs(o.tensions()).max() > 1.0
     o.step(19)
     assert np.allclose(o.sites(), sites, atol=1e-12)
+
+
+def _two_rods(n_dim, gap):
+    """Two straight 5-bond rods along x, `gap` apart in y, no noise."""
+    sites = np.zeros((12, 3))
+    sites[:6, 0] = np.arange(6) - 2.5
+    sites[6:, 0] = np.arange(6) - 2.5
+    sites[6:, 1] = gap
+    system = dict(n_dim=n_dim, system_radius=10.0, delta=1e-4, stoch_flag=0, seed=0,
+                  interaction_flag=1)
+    fils = [dict(length=5.0, persistence_length=100.0, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * 2
+    return system, fils, sites
+
+
+@pytest.mark.parametrize("n_dim", [2, 3])
+def test_crosslink_tether_known_answer(n_dim):
+    """Two tethers (k 10, rest 1) between rods 1.5 apart (beyond the WCA
+    cutoff): tail-to-tail on bond 0 of each rod and head-to-head on the last
+    bonds.  Step 1 (odd) applies the zero forces stored so far; step 2 (even)
+    computes F = k (|dr| - rest) = 5 along +y on anchor 0, -F on anchor 1, and
+    torques (lambda - l/2) u x F = -/+2.5 z at the tails, +/-2.5 z at the
+    heads (src/crosslink.cpp:247-275, src/anchor.cpp:132-146)."""
+    system, fils, sites = _two_rods(n_dim, 1.5)
+    o = Oracle(system, fils, sites)
+    o.add_crosslinks([0, 5], [6, 11], k_spring=10.0, rest_length=1.0)
+    o.step(1)
+    f, t = o.bond_forces()
+    assert np.all(f == 0) and np.all(t == 0)
+    assert np.all(o.crosslink_forces() == 0)
+    o.step(1)
+    xf = o.crosslink_forces()
+    assert np.allclose(xf, [[0, 5, 0], [0, 5, 0]], atol=1e-12)
+    f, t = o.bond_forces()
+    assert np.allclose(f[0], [0, 5, 0]) and np.allclose(f[5], [0, -5, 0])
+    assert np.allclose(f[4], [0, 5, 0]) and np.allclose(f[9], [0, -5, 0])
+    assert np.allclose(t[0], [0, 0, -2.5]) and np.allclose(t[5], [0, 0, 2.5])
+    assert np.allclose(t[4], [0, 0, 2.5]) and np.allclose(t[9], [0, 0, -2.5])
+    assert np.all(f[[1, 2, 3, 6, 7, 8]] == 0)
+    # Step 3 (odd) re-applies the step-2 forces unchanged although the rods
+    # have moved.
+    before = o.sites()
+    o.step(1)
+    assert not np.array_equal(o.sites(), before)
+    f3, t3 = o.bond_forces()
+    assert np.array_equal(f3, f) and np.array_equal(t3, t)
+    # The tether pulls the rods together.
+    assert o.sites()[6:, 1].mean() < 1.5 and o.sites()[:6, 1].mean() > 0.0
+
+
+def test_crosslink_compression_constant():
+    """k_spring_compress >= 0 replaces k_spring when the tether is shorter
+    than its rest length."""
+    system, fils, sites = _two_rods(3, 1.5)
+    o = Oracle(system, fils, sites)
+    o.add_crosslinks([0], [6], k_spring=10.0, k_spring_compress=4.0, rest_length=2.0)
+    o.step(2)
+    assert np.allclose(o.crosslink_forces(), [[0, -2.0, 0]], atol=1e-12)
