@@ -234,6 +234,7 @@ def run_ours(args, rank, world, local_rank):
 
     results = {}
     contexts = {}
+    layouts = {}
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if sampler:
         sampler.start()
@@ -241,6 +242,7 @@ def run_ours(args, rank, world, local_rank):
     for prec in ("fp64", "mixed"):
         ctx = sc.Context(system, fils, sites, precision=prec, device=local_rank)
         contexts[prec] = ctx
+        layouts[prec] = ctx.autotune()  # integrator layout for this shape
         timed_graph(ctx, args.warmup)
         if dist is not None:
             dist.barrier()
@@ -316,7 +318,9 @@ def run_ours(args, rank, world, local_rank):
                                  "midpoint BD steps with device-decided pair-list rebuilds)",
                    "l2": "flushed by a 256 MiB write before every timed step",
                    "parallelism": "replicas" if world > 1 else "single system",
-                   "pairs": r["n_pairs"], "rebuilds_in_timed_region": r["rebuilds"]},
+                   "pairs": r["n_pairs"], "rebuilds_in_timed_region": r["rebuilds"],
+                   "integrator_layout": {p: {"warp_max_sites": w, "block_sites": b}
+                                         for p, (w, b) in layouts.items()}},
         "fp64": {"value": value64, "ms_per_step": r64["total_ms"] / args.steps,
                  "rebuilds_in_timed_region": r64["rebuilds"]},
         "mixed_over_fp64": value / value64,

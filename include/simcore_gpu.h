@@ -157,6 +157,21 @@ sc_status sc_get_bond_geometry(sc_ctx *ctx, double *pos, double *spos,
  * normalisation; 0 runs the exact FP64 integrator of SC_PREC_FP64.  No
  * effect in SC_PREC_FP64, which is always exact. */
 sc_status sc_set_fast_integrator(sc_ctx *ctx, int on);
+/* Integrator layout, a tuning knob (every layout gives the same results):
+ * filaments of at most warp_max_sites sites (<= 32) run on the
+ * warp-synchronous kernel, one warp per group of whole filaments; longer
+ * ones on the block kernel, block_sites sites per block (a multiple of 32 up
+ * to 256, at least the longest such filament; 0 picks 128 or 256).
+ * warp_max_sites 0 puts every filament on the block kernel. */
+sc_status sc_set_integrator_layout(sc_ctx *ctx, int warp_max_sites, int block_sites);
+/* Autotuner for the layout above: times every candidate on the context's
+ * own state (saved and restored, so the simulation is unchanged), applies
+ * the fastest and reports it.  With cache_path (may be NULL) the choice is
+ * read from, or appended to, that text file under a key of device, precision,
+ * filament count and site range, so a later context of the same shape skips
+ * the timing. */
+sc_status sc_autotune(sc_ctx *ctx, const char *cache_path, int *warp_max_sites,
+                      int *block_sites);
 /* Site forces and tensions of the last integrator step; recorded only while
  * capture is on (sc_set_capture(ctx, 1)), since they are not state. */
 sc_status sc_set_capture(sc_ctx *ctx, int on);

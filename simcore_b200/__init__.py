@@ -33,7 +33,7 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_set_kernel_timing",
             "sc_get_kernel_timing", "sc_get_graph_time", "sc_set_fast_integrator",
             "sc_pair_forces_noalloc", "sc_insert_filaments", "sc_add_crosslinks",
-            "sc_get_crosslink_forces"]
+            "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune"]
 
 
 class ScError(RuntimeError):
@@ -193,6 +193,22 @@ class Context:
 
     def set_fast_integrator(self, on=True):
         self._check(lib.sc_set_fast_integrator(self.h, ctypes.c_int(1 if on else 0)))
+
+    def set_integrator_layout(self, warp_max_sites=32, block_sites=0):
+        """Filaments of at most warp_max_sites sites on the warp-synchronous
+        integrator (0: none), the rest on blocks of block_sites sites."""
+        self._check(lib.sc_set_integrator_layout(self.h, ctypes.c_int(warp_max_sites),
+                                                 ctypes.c_int(block_sites)))
+
+    def autotune(self, cache_path=None):
+        """Times the integrator layouts on this context's state (restored
+        afterwards), applies the fastest; returns (warp_max_sites,
+        block_sites).  cache_path: optional text cache keyed by shape."""
+        w = ctypes.c_int()
+        b = ctypes.c_int()
+        path = cache_path.encode() if cache_path else None
+        self._check(lib.sc_autotune(self.h, path, ctypes.byref(w), ctypes.byref(b)))
+        return w.value, b.value
 
     def set_capture(self, on=True):
         self._check(lib.sc_set_capture(self.h, ctypes.c_int(1 if on else 0)))

@@ -42,6 +42,8 @@ struct sc_ctx {
 
   // integrator blocks
   int nblocks = 0, C = 128;
+  int warp_sites = 32;             // longest filament for the warp-synchronous kernel
+  int block_sites = 0;             // sites per block of the block kernel (0: 128 or 256)
 
   // control state
   long long i_step = 0, n_rebuilds = 0, launches = 0;
@@ -327,6 +329,65 @@ sc_status maybe_rebuild(sc_ctx *c) {
   return SC_OK;
 }
 
+// Integrator work units over the filaments in order: runs of whole
+// filaments of at most warp_sites sites each go to the warp-synchronous
+// kernel (one lane per site, at most 32 sites per group); longer filaments go
+// to the block kernel (runs of whole filaments up to C sites per block).
+sc_status layout_integrator(sc_ctx *c) {
+  const std::vector<int> &off = c->site_off;
+  const int n = c->nf;
+  std::vector<int> blk_site0, blk_f0, blk_nf, blk_ns, wg_site0, wg_f0, wg_ns;
+  int max_long = 0;
+  auto short_fil = [&](int f) { return off[f + 1] - off[f] <= c->warp_sites; };
+  for (int f = 0; f < n; ++f)
+    if (!short_fil(f)) max_long = std::max(max_long, off[f + 1] - off[f]);
+  c->C = c->block_sites > 0 ? c->block_sites : (max_long <= 128 ? 128 : 256);
+  if (max_long > c->C)
+    return fail(c, SC_ERR_INVALID_ARG, "a %d-site filament does not fit %d-site blocks", max_long,
+                c->C);
+  int f = 0;
+  while (f < n) {
+    const int s0 = off[f], f0 = f;
+    if (short_fil(f)) {
+      while (f < n && short_fil(f) && off[f + 1] - s0 <= 32) ++f;
+      wg_site0.push_back(s0);
+      wg_f0.push_back(f0);
+      wg_ns.push_back(off[f] - s0);
+    } else {
+      while (f < n && !short_fil(f) && off[f + 1] - s0 <= c->C) ++f;
+      blk_site0.push_back(s0);
+      blk_f0.push_back(f0);
+      blk_nf.push_back(f - f0);
+      blk_ns.push_back(off[f] - s0);
+    }
+  }
+  for (const int *q : {c->d.blk_site0, c->d.blk_f0, c->d.blk_nf, c->d.blk_ns, c->d.wg_site0,
+                       c->d.wg_f0, c->d.wg_ns})
+    dfree(c, const_cast<int *>(q));
+  auto up = [&](const int **dst, const std::vector<int> &v) -> sc_status {
+    int *q = nullptr;
+    CKS(dalloc(c, &q, v.size()));
+    if (!v.empty())
+      CK(cudaMemcpyAsync(q, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, c->st));
+    *dst = q;
+    return SC_OK;
+  };
+  DevState &d = c->d;
+  CKS(up(&d.blk_site0, blk_site0));
+  CKS(up(&d.blk_f0, blk_f0));
+  CKS(up(&d.blk_nf, blk_nf));
+  CKS(up(&d.blk_ns, blk_ns));
+  CKS(up(&d.wg_site0, wg_site0));
+  CKS(up(&d.wg_f0, wg_f0));
+  CKS(up(&d.wg_ns, wg_ns));
+  CK(cudaStreamSynchronize(c->st));
+  c->nblocks = (int)blk_f0.size();
+  d.n_wg = (int)wg_f0.size();
+  sc::prepare_integrate(c->C);
+  drop_graph(c);
+  return SC_OK;
+}
+
 // Records CUDA events around one launch when kernel timing is on.
 template <class F>
 sc_status timed(sc_ctx *c, F launch) {
@@ -523,7 +584,6 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   c->nf = n;
   c->ns = nsi;
   c->nb = nbi;
-  c->C = max_ns <= 128 ? 128 : 256;
 
   // Per-filament constants: Filament::SetParameters / InitFilamentLength /
   // SetDiffusion (src/filament.cpp:6-84, 104-170, 320-348).
@@ -551,27 +611,15 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
     q.n = nsf;
   }
   c->site_off = site_off;
-  std::vector<int> site_fil(nsi), bond_fil(nbi);
+  std::vector<int> site_fil(nsi), site_jn(nsi), bond_fil(nbi);
   for (int f = 0; f < n; ++f) {
-    for (int s = site_off[f]; s < site_off[f + 1]; ++s) site_fil[s] = f;
+    for (int s = site_off[f]; s < site_off[f + 1]; ++s) {
+      site_fil[s] = f;
+      site_jn[s] = (s - site_off[f]) | (site_off[f + 1] - site_off[f]) << 16;
+    }
     for (int b = site_off[f] - f; b < site_off[f + 1] - f - 1; ++b) bond_fil[b] = f;
   }
   c->bond_fil = bond_fil;
-  // Integrator blocks: greedy runs of whole filaments up to C sites.
-  std::vector<int> blk_site0, blk_f0, blk_nf;
-  {
-    int f = 0;
-    while (f < n) {
-      int s0 = site_off[f], f0 = f;
-      while (f < n && site_off[f + 1] - s0 <= c->C) ++f;
-      blk_site0.push_back(s0);
-      blk_f0.push_back(f0);
-      blk_nf.push_back(f - f0);
-    }
-    blk_site0.push_back(nsi);
-  }
-  c->nblocks = (int)blk_f0.size();
-
   DevState &d = c->d;
   d.nf = n;
   d.ns = nsi;
@@ -595,10 +643,10 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   CKS(up(&d.f_switch, sw));
   CKS(up(&d.f_nnorm, nn));
   CKS(up(&tmp_i, site_fil)); d.site_fil = tmp_i;
+  CKS(up(&tmp_i, site_jn)); d.site_jn = tmp_i;
   CKS(up(&tmp_i, bond_fil)); d.bond_fil = tmp_i;
-  CKS(up(&tmp_i, blk_site0)); d.blk_site0 = tmp_i;
-  CKS(up(&tmp_i, blk_f0)); d.blk_f0 = tmp_i;
-  CKS(up(&tmp_i, blk_nf)); d.blk_nf = tmp_i;
+  c->warp_sites = 32;
+  CKS(layout_integrator(c));
 
   // Sites: positions (z = 0 in 2D); previous positions = positions as after
   // Mesh::UpdatePrevPositions; no stored noise yet.
@@ -665,7 +713,6 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   CKS(dalloc(c, &c->cells_xyz, 3 * (size_t)nbi));
   CKS(ensure_pair_capacity(c, std::max<long long>(nbi, 1024)));
 
-  sc::prepare_integrate(c->C);
   sc::launch_init_geometry(c->k, d, 0, c->prec, c->st);
   if (c->prec != 0) sc::launch_init_geometry(c->k, d, 0, 0, c->st);
   c->rbuf = 0;
@@ -901,6 +948,165 @@ sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
   CK(cudaGetLastError());
   CKS(copy_soa3(c, c->d.bF, c->nb, f));
   return copy_soa3(c, c->d.bT, c->nb, t);
+}
+
+sc_status sc_set_integrator_layout(sc_ctx *c, int warp_max_sites, int block_sites) {
+  if (!c || !c->loaded || warp_max_sites < 0 || warp_max_sites > 32) return SC_ERR_INVALID_ARG;
+  if (block_sites != 0 && (block_sites < 32 || block_sites > 256 || block_sites % 32))
+    return fail(c, SC_ERR_INVALID_ARG, "block_sites must be 0 or a multiple of 32 in [32, 256]");
+  CK(cudaSetDevice(c->desc.device));
+  const int ow = c->warp_sites, ob = c->block_sites;
+  c->warp_sites = warp_max_sites;
+  c->block_sites = block_sites;
+  sc_status st = layout_integrator(c);
+  if (st != SC_OK) {
+    c->warp_sites = ow;
+    c->block_sites = ob;
+    layout_integrator(c);
+  }
+  return st;
+}
+
+// Integrator autotuner.  Candidate layouts (warp kernel or not, block size)
+// are timed on the context's own state: the arrays the integrator writes are
+// saved first and restored afterwards, so the simulation is unchanged.  The
+// fastest layout is applied and, with a cache file, recorded per shape (device,
+// precision, filament count and site range) so later contexts skip the timing.
+sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
+                      int *block_sites_out) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, c->desc.device));
+  int min_n = 1 << 30, max_n = 0;
+  for (int f = 0; f < c->nf; ++f) {
+    const int nn = c->site_off[f + 1] - c->site_off[f];
+    min_n = std::min(min_n, nn);
+    max_n = std::max(max_n, nn);
+  }
+  char key[512];
+  std::snprintf(key, sizeof(key), "v1|%s|sm%d|nd%d|prec%d|fast%d|nf%d|ns%d|n%d-%d", prop.name,
+                prop.multiProcessorCount, c->nd, c->prec, (c->prec == 1 && c->fast) ? 1 : 0, c->nf,
+                c->ns, min_n, max_n);
+  auto finish = [&](int w, int b) -> sc_status {
+    if (warp_sites_out) *warp_sites_out = w;
+    if (block_sites_out) *block_sites_out = b;
+    return SC_OK;
+  };
+  if (cache_path) {
+    if (FILE *fp = std::fopen(cache_path, "r")) {
+      char line[768];
+      int w = -1, b = -1;
+      while (std::fgets(line, sizeof(line), fp)) {
+        char *tab = std::strchr(line, '\t');
+        if (!tab) continue;
+        *tab = 0;
+        int ww, bb;
+        if (std::strcmp(line, key) == 0 && std::sscanf(tab + 1, "%d %d", &ww, &bb) == 2) {
+          w = ww;
+          b = bb;
+        }
+      }
+      std::fclose(fp);
+      if (w >= 0) {
+        CKS(sc_set_integrator_layout(c, w, b));
+        return finish(w, b);
+      }
+    }
+  }
+  // Candidates: every block size that holds the longest block-kernel
+  // filament, with and without the warp kernel for filaments of <= 32 sites.
+  std::vector<std::pair<int, int>> cand;
+  for (int w : {32, 0}) {
+    if (w == 32 && min_n > 32) continue;
+    const int longest = w == 32 ? (max_n > 32 ? max_n : 0) : max_n;
+    if (longest == 0) {
+      cand.push_back({w, 0});
+      continue;
+    }
+    for (int bsz : {64, 96, 128, 192, 256})
+      if (bsz >= longest) cand.push_back({w, bsz});
+  }
+  // Save what the integrator writes.
+  const int wbuf = 1 - c->rbuf;
+  std::vector<std::pair<void *, size_t>> regions;
+  for (int i = 0; i < 3; ++i) {
+    regions.push_back({c->d.r[i], sizeof(double) * c->ns});
+    regions.push_back({c->d.rp[i], sizeof(double) * c->ns});
+    regions.push_back({c->d.fr[i], sizeof(double) * c->ns});
+    regions.push_back({c->d.ub[i], sizeof(double) * c->nb});
+  }
+  regions.push_back({c->d.dt, sizeof(double) * c->ns});
+  regions.push_back({c->d.f_switch, sizeof(int) * c->nf});
+  regions.push_back({c->d.f_nnorm, sizeof(int) * c->nf});
+  if (c->prec == 0) regions.push_back({c->d.g64[wbuf], sizeof(sc::BondGeomF64) * c->nb});
+  else regions.push_back({c->d.g32[wbuf], sizeof(sc::BondGeomF32) * c->nb});
+  regions.push_back({c->d.dr_max_bits, sizeof(unsigned long long)});
+  regions.push_back({c->d.status, sizeof(unsigned)});
+  size_t total = 0;
+  for (auto &r : regions) total += (r.second + 255) & ~(size_t)255;
+  char *save = nullptr;
+  CKS(dalloc(c, &save, total));
+  auto copy_all = [&](bool to_save) -> sc_status {
+    size_t off = 0;
+    for (auto &r : regions) {
+      void *dst = to_save ? (void *)(save + off) : r.first;
+      const void *src = to_save ? (const void *)r.first : (const void *)(save + off);
+      CK(cudaMemcpyAsync(dst, src, r.second, cudaMemcpyDeviceToDevice, c->st));
+      off += (r.second + 255) & ~(size_t)255;
+    }
+    return SC_OK;
+  };
+  CKS(copy_all(true));
+  const int ow = c->warp_sites, ob = c->block_sites;
+  const int interaction = c->desc.interaction_flag ? 1 : 0;
+  float best = 1e30f;
+  std::pair<int, int> best_lay{ow, ob};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  sc_status st = SC_OK;
+  for (auto lay : cand) {
+    c->warp_sites = lay.first;
+    c->block_sites = lay.second;
+    st = layout_integrator(c);
+    if (st != SC_OK) break;
+    for (int it = 0; it < 2; ++it)
+      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1 - it, c->rbuf, interaction, 0,
+                           c->prec, c->fast, c->st);
+    cudaEventRecord(e0, c->st);
+    for (int it = 0; it < 8; ++it)
+      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1 - (it & 1), c->rbuf, interaction, 0,
+                           c->prec, c->fast, c->st);
+    cudaEventRecord(e1, c->st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      st = fail(c, SC_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      best_lay = lay;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CKS(copy_all(false));
+  CK(cudaStreamSynchronize(c->st));
+  dfree(c, save);
+  CKS(st);
+  c->warp_sites = best_lay.first;
+  c->block_sites = best_lay.second;
+  CKS(layout_integrator(c));
+  if (cache_path) {
+    if (FILE *fp = std::fopen(cache_path, "a")) {
+      std::fprintf(fp, "%s\t%d %d %.2f\n", key, best_lay.first, best_lay.second,
+                   1000.0 * best / 8);
+      std::fclose(fp);
+    }
+  }
+  return finish(best_lay.first, best_lay.second);
 }
 
 sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32_t *site_b,

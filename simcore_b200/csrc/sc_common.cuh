@@ -91,11 +91,19 @@ struct DevState {
   const FilConst *fil;     // nf
   int *f_switch, *f_nnorm;
   const int *site_fil;     // ns
+  const int *site_jn;      // ns: site index in its filament | filament sites << 16
   const int *bond_fil;     // nb
-  // integrator blocks: packed runs of whole filaments
+  // integrator blocks (filaments longer than a warp): runs of whole filaments
   const int *blk_site0;    // per block: first site
   const int *blk_f0;       // per block: first filament
   const int *blk_nf;       // per block: filament count
+  const int *blk_ns;       // per block: site count
+  // integrator warp groups (filaments of at most 32 sites): runs of whole
+  // filaments, one lane per site
+  int n_wg;
+  const int *wg_site0;     // per group: first site
+  const int *wg_f0;        // per group: first filament
+  const int *wg_ns;        // per group: site count
   // sites (SoA, 3 components each)
   double *r[3], *rp[3], *fr[3], *dz[3];
   double *dt;

@@ -18,6 +18,7 @@
 #include "sc_kernels.h"
 #include "sc_pair.cuh"
 #include "sc_step.cuh"
+#include "sc_step_warp.cuh"
 
 namespace sc {
 
@@ -772,6 +773,21 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
                      int prec, bool fast, cudaStream_t st) {
   if (fast && prec == 1)
     return launch_integrate_fast(k, d, nblocks, C, midstep, rbuf, interaction, capture, st);
+  int launched = 0;
+  if (d.n_wg > 0) {
+    const int grid = cdiv(d.n_wg, kIntWarps);
+#define SC_INTEGRATE_WARP(ND, P)                                              \
+  k_integrate_warp<ND, P, false><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf, \
+                                                                  interaction, capture)
+    if (k.n_dim == 3) {
+      if (prec == 0) SC_INTEGRATE_WARP(3, 0); else SC_INTEGRATE_WARP(3, 1);
+    } else {
+      if (prec == 0) SC_INTEGRATE_WARP(2, 0); else SC_INTEGRATE_WARP(2, 1);
+    }
+#undef SC_INTEGRATE_WARP
+    ++launched;
+  }
+  if (nblocks == 0) return launched;
   size_t smem = integrate_smem_bytes(C);
 #define SC_INTEGRATE(ND, P, MC)                                              \
   k_integrate<ND, P, false, MC><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, \
@@ -790,7 +806,7 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
     }
   }
 #undef SC_INTEGRATE
-  return 1;
+  return launched + 1;
 }
 
 }  // namespace sc

@@ -9,6 +9,7 @@
 #include "sc_kernels.h"
 #include "sc_pair.cuh"
 #include "sc_step.cuh"
+#include "sc_step_warp.cuh"
 
 namespace sc {
 
@@ -32,6 +33,18 @@ void prepare_integrate_fast(int C) {
 int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int C,
                           int midstep, int rbuf, int interaction, int capture,
                           cudaStream_t st) {
+  int launched = 0;
+  if (d.n_wg > 0) {
+    const int grid = (d.n_wg + kIntWarps - 1) / kIntWarps;
+    if (k.n_dim == 3)
+      k_integrate_warp<3, 1, true><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf,
+                                                                    interaction, capture);
+    else
+      k_integrate_warp<2, 1, true><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf,
+                                                                    interaction, capture);
+    ++launched;
+  }
+  if (nblocks == 0) return launched;
   size_t smem = integrate_smem_bytes(C);
   if (C <= 128) {
     if (k.n_dim == 3)
@@ -44,7 +57,7 @@ int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int
     else
       k_integrate<2, 1, true, 256><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
   }
-  return 1;
+  return launched + 1;
 }
 
 }  // namespace sc

@@ -118,8 +118,8 @@ __device__ __forceinline__ void bond_xlink_sum(const DevState &d, int b, double 
 
 // Bond::force_ / torque_ after Interact: crosslink anchors first, then the
 // bond's pair contributions in slot (= pair) order.  FP64 sums as the
-// reference accumulates them; FP32 pair sums with Kahan compensation, added
-// to the FP64 crosslink sum.  A pair slot is 8 values: force (3), torque (3),
+// reference accumulates them; in mixed precision FP32 sums with Kahan
+// compensation, added to the FP64 crosslink sum.  A pair slot is 8 values: force (3), torque (3),
 // padding (2).
 template <int ND, int PREC>
 __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F[3],
@@ -171,34 +171,70 @@ __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F
 // a block's serial work occupies one or two warps instead of every warp.
 
 // Thomas algorithm of the reference's tridiagonal_solver
-// (src/linear_algebra.cpp:164-197); n unknowns, in place.
+// (src/linear_algebra.cpp:164-197); n unknowns, in place.  The previous
+// row's c and d stay in registers (same values, same operations as reading
+// them back).
 __device__ __forceinline__ void thomas(double *a, const double *b, double *c,
                                        double *d, int n) {
   n--;
-  c[0] /= b[0];
-  d[0] /= b[0];
+  double cp = c[0] / b[0];
+  double dp = d[0] / b[0];
+  c[0] = cp;
+  d[0] = dp;
   for (int i = 1; i < n; ++i) {
-    c[i] /= b[i] - a[i - 1] * c[i - 1];
-    d[i] = (d[i] - a[i - 1] * d[i - 1]) / (b[i] - a[i - 1] * c[i - 1]);
+    const double am = a[i - 1], bi = b[i];
+    const double cn = c[i] / (bi - am * cp);
+    const double dn = (d[i] - am * dp) / (bi - am * cp);
+    c[i] = cn;
+    d[i] = dn;
+    cp = cn;
+    dp = dn;
   }
-  d[n] = (d[n] - a[n - 1] * d[n - 1]) / (b[n] - a[n - 1] * c[n - 1]);
-  for (int i = n; i-- > 0;) d[i] -= c[i] * d[i + 1];
+  dp = (d[n] - a[n - 1] * dp) / (b[n] - a[n - 1] * cp);
+  d[n] = dp;
+  for (int i = n; i-- > 0;) {
+    dp = d[i] - c[i] * dp;
+    d[i] = dp;
+  }
 }
 
-// FAST: one reciprocal per row instead of two divisions.
+// 1/x for the fast integrator: Newton-Raphson iteration y <- y (2 - x y),
+// written as e = 1 - x y, y <- y + y e, twice from the FP32 reciprocal of x
+// (relative error 2^-23 -> 2^-46 -> FP64 rounding).  For |x| within the FP32
+// normal range, which the diagonals, determinants and lengths it serves are.
+__device__ __forceinline__ double recip_nr(double x) {
+  double y = (double)__frcp_rn((float)x);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+
+// FAST: one Newton reciprocal per row instead of two divisions.
 __device__ __forceinline__ void thomas_fast(double *a, const double *b, double *c,
                                             double *d, int n) {
   n--;
-  double r = 1.0 / b[0];
-  c[0] *= r;
-  d[0] *= r;
+  double r = recip_nr(b[0]);
+  double cp = c[0] * r;
+  double dp = d[0] * r;
+  c[0] = cp;
+  d[0] = dp;
   for (int i = 1; i < n; ++i) {
-    r = 1.0 / (b[i] - a[i - 1] * c[i - 1]);
-    c[i] *= r;
-    d[i] = (d[i] - a[i - 1] * d[i - 1]) * r;
+    const double am = a[i - 1];
+    r = recip_nr(b[i] - am * cp);
+    const double cn = c[i] * r;
+    const double dn = (d[i] - am * dp) * r;
+    c[i] = cn;
+    d[i] = dn;
+    cp = cn;
+    dp = dn;
   }
-  d[n] = (d[n] - a[n - 1] * d[n - 1]) / (b[n] - a[n - 1] * c[n - 1]);
-  for (int i = n; i-- > 0;) d[i] -= c[i] * d[i + 1];
+  dp = (d[n] - a[n - 1] * dp) * recip_nr(b[n] - a[n - 1] * cp);
+  d[n] = dp;
+  for (int i = n; i-- > 0;) {
+    dp = d[i] - c[i] * dp;
+    d[i] = dp;
+  }
 }
 
 template <bool FAST>
@@ -292,7 +328,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
   const int t = threadIdx.x;
   const unsigned long long mcount = *d.mcount;
   const int s0 = d.blk_site0[blk];
-  const int count = d.blk_site0[blk + 1] - s0;
+  const int count = d.blk_ns[blk];
   const int f0 = d.blk_f0[blk];
   const int nfb = d.blk_nf[blk];
   if (t < nfb) {
@@ -520,8 +556,13 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
   if (active && j < n - 2) {
     const int dbase = base + lf;
     const double det_g = sdt[dbase + n - 1];
-    double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] / det_g;
-    skeff[t] = (fc.kappa + fc.l * ginv) / fc.l2;
+    if (FAST) {
+      const double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] * recip_nr(det_g);
+      skeff[t] = (fc.kappa + fc.l * ginv) * recip_nr(fc.l2);
+    } else {
+      double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] / det_g;
+      skeff[t] = (fc.kappa + fc.l * ginv) / fc.l2;
+    }
   }
   __syncthreads();
   if (active && FAST) {

@@ -249,3 +249,53 @@ def test_fp64_uneven_lengths_bitwise():
         o.step(n)
         compare_state(ctx, o, 3, capture=False)
     assert o.n_rebuilds > 0
+
+
+@pytest.mark.parametrize("precision,fast", [("fp64", False), ("mixed", False), ("mixed", True)])
+def test_warp_and_block_integrators_agree(precision, fast):
+    """The warp-synchronous integrator (filaments of at most 32 sites) and the
+    block integrator give the same bits where both are exact, and agree to
+    1e-12 in the fast mixed variant (contraction choices differ)."""
+    system, fils, sites = _workload("B", 0.05, seed=9)
+    a = _ctx(system, fils, sites, precision)
+    b = _ctx(system, fils, sites, precision)
+    b.set_integrator_layout(0, 64)
+    for c in (a, b):
+        c.set_fast_integrator(fast)
+        c.set_capture(True)
+    for n in (1, 2, 3):
+        a.step(n)
+        b.step(n)
+    for c in (a, b):
+        c.set_capture(False)
+    a.step_graph(40)
+    b.step_graph(40)
+    if precision == "fp64" or not fast:
+        assert_same(a.sites(), b.sites(), "sites")
+        assert_same(a.pairs(), b.pairs(), "pairs")
+    else:
+        ra, rb = a.sites(), b.sites()
+        assert np.abs(ra - rb).max() <= 1e-12 * np.abs(rb).max()
+
+
+def test_autotune_leaves_state_and_caches(tmp_path):
+    """The autotuner times layouts on the live state and restores it: an
+    autotuned FP64 context stays bit-identical to an untuned one (every
+    layout is exact).  Its choice is cached per shape and read back."""
+    system, fils, sites = _workload("B", 0.05, seed=10)
+    a = _ctx(system, fils, sites)
+    b = _ctx(system, fils, sites)
+    a.step(3)
+    b.step(3)
+    cache = str(tmp_path / "tune.txt")
+    lay = a.autotune(cache)
+    assert lay[0] in (0, 32)
+    for n in (1, 40):
+        a.step_graph(n)
+        b.step_graph(n)
+        assert_same(a.sites(), b.sites(), "sites")
+    lines = open(cache).read().strip().splitlines()
+    assert len(lines) == 1
+    c = _ctx(system, fils, sites)
+    assert c.autotune(cache) == lay
+    assert len(open(cache).read().strip().splitlines()) == 1
