@@ -262,6 +262,21 @@ def run_ours(args, rank, world, local_rank):
     if sampler:
         results["clocks"] = sampler.stop()
 
+    # Mixed-precision force error on this workload: fresh contexts of both
+    # precisions on the initial positions evaluate the pair forces once; the
+    # mixed bond forces and torques are compared with the FP64 ones
+    # (max |dF| / max |F|).
+    errs = {}
+    for p_ in ("fp64", "mixed"):
+        cc = sc.Context(system, fils, sites, precision=p_, device=local_rank)
+        cc.interact()
+        errs[p_] = cc.bond_forces()
+        cc.close()
+    force_err = float(np.abs(errs["mixed"][0] - errs["fp64"][0]).max() /
+                      np.abs(errs["fp64"][0]).max())
+    torque_err = float(np.abs(errs["mixed"][1] - errs["fp64"][1]).max() /
+                       np.abs(errs["fp64"][1]).max())
+
     # Roofline: per-launch CUDA-event durations of the two kernels of a
     # reference step, host-driven, on the context's stream.
     kt = {p: kernel_times(contexts[p], 2 * I_STEPS_PER_STEP) for p in ("mixed", "fp64")}
@@ -324,6 +339,9 @@ def run_ours(args, rank, world, local_rank):
         "fp64": {"value": value64, "ms_per_step": r64["total_ms"] / args.steps,
                  "rebuilds_in_timed_region": r64["rebuilds"]},
         "mixed_over_fp64": value / value64,
+        "mixed_error": {"max_rel_bond_force": force_err, "max_rel_bond_torque": torque_err,
+                        "vs": "FP64 GPU path (bit-identical to the reference) on the same "
+                              "positions, one pair evaluation", "bound": 1e-5},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": TRAFFIC_K_INTEGRATE_MIXED,
                      "kernel": "k_integrate<3,mixed,fast> (dominant: one launch per reference "
