@@ -81,14 +81,15 @@ typedef struct {
 
 typedef struct {
   int64_t i_step;             /* steps (i_steps) taken */
-  int64_t n_rebuilds;         /* pair-list rebuilds since sc_add_filaments */
+  int64_t n_rebuilds;         /* rebuild passes (any system) since loading */
   int64_t n_pairs;            /* current candidate pairs */
   int64_t pair_capacity;
   int64_t n_filaments, n_sites, n_bonds;
   int32_t n_cells_1d;
-  double cell_length;
-  double dr_update;           /* rebuild threshold 0.25 * cell_length^2 */
+  double cell_length;         /* of system 0 */
+  double dr_update;           /* rebuild threshold 0.25 * cell_length^2 (system 0) */
   int64_t kernel_launches;    /* kernels launched by this context */
+  int32_t n_replicas;         /* independent systems in the context */
 } sc_counters;
 
 typedef struct sc_ctx sc_ctx;
@@ -109,6 +110,23 @@ sc_status sc_add_filaments(sc_ctx *ctx, int n, const sc_filament_params *p,
 
 /* Number of bonds the reference gives a filament (src/filament.cpp:142-147). */
 int sc_filament_n_bonds(const sc_filament_params *p);
+
+/* Batched independent systems (replicas) in one context, instead of
+ * sc_add_filaments: system r is a periodic box of radius system_radius[r]
+ * whose noise key is seed[r] (the desc's radius and seed are not used), with
+ * the next n_filaments[r] of the n filaments (parameters p, sites site_xyz,
+ * systems back to back).  Every system behaves exactly as a context of its
+ * own would: its own cell grid, pair list and rebuilds, decided by its own
+ * displacements; every stage of a step runs for all systems in one launch.
+ * Pair lists are kept in per-system segments with room for half again their
+ * initial length; a list that outgrows its segment is SC_ERR_LIST_OVERFLOW. */
+sc_status sc_add_replicas(sc_ctx *ctx, int n_replicas, const double *system_radius,
+                          const uint32_t *seed, const int32_t *n_filaments, int n,
+                          const sc_filament_params *p, const double *site_xyz,
+                          int64_t n_sites_total);
+/* Per-system rebuild counts and current pair counts (n_replicas entries
+ * each; either pointer may be NULL). */
+sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);
 
 /* Static doubly-bound crosslinks: n harmonic tethers between sites site_a[k]
  * and site_b[k] (global site indices), force k_spring (|dr| - rest_length)
@@ -234,7 +252,7 @@ sc_status sc_get_graph_time(sc_ctx *ctx, double *ms);
 #define SC_NOALLOC_MAX_BONDS 8192
 #define SC_NOALLOC_MAX_CELLS 131072
 #define SC_NOALLOC_MAX_PAIRS 32768
-#define SC_NOALLOC_SCRATCH_BYTES 8816384 /* 8.4 MiB per GPU */
+#define SC_NOALLOC_SCRATCH_BYTES 8882432 /* 8.5 MiB per GPU */
 sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
                                  const sc_filament_params *species, int n_filaments,
                                  const int32_t *d_site_offsets, const double *d_site_xyz,

@@ -33,7 +33,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_bond_cells", "sc_get_counters", "sc_get_stream", "sc_set_kernel_timing",
             "sc_get_kernel_timing", "sc_get_graph_time", "sc_set_fast_integrator",
             "sc_pair_forces_noalloc", "sc_insert_filaments", "sc_add_crosslinks",
-            "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune"]
+            "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune",
+            "sc_add_replicas", "sc_get_replica_counters"]
 
 
 class ScError(RuntimeError):
@@ -63,7 +64,7 @@ class Counters(ctypes.Structure):
                 ("n_filaments", ctypes.c_int64), ("n_sites", ctypes.c_int64),
                 ("n_bonds", ctypes.c_int64), ("n_cells_1d", ctypes.c_int32),
                 ("cell_length", ctypes.c_double), ("dr_update", ctypes.c_double),
-                ("kernel_launches", ctypes.c_int64)]
+                ("kernel_launches", ctypes.c_int64), ("n_replicas", ctypes.c_int32)]
 
 
 def _load():
@@ -118,7 +119,10 @@ def insert_filaments(n_dim, system_radius, seed, n_bonds, lengths, persistence_l
 class Context:
     """One simulated system on one GPU (an sc_ctx)."""
 
-    def __init__(self, system, filaments, sites, precision="fp64", device=0):
+    def __init__(self, system, filaments, sites, precision="fp64", device=0, replicas=None):
+        """replicas: None for one system, or a list of dicts (system_radius,
+        seed, n_filaments) of independent systems whose filaments and sites
+        follow one another in `filaments` and `sites`."""
         desc = SystemDesc(n_dim=system["n_dim"], system_radius=system["system_radius"],
                           delta=system["delta"], wca_eps=system.get("wca_eps", 1.0),
                           wca_sig=system.get("wca_sig", 1.0),
@@ -136,8 +140,17 @@ class Context:
         self.n_dim = system["n_dim"]
         fils = (FilamentParams * len(filaments))(*[FilamentParams(**f) for f in filaments])
         sites = np.ascontiguousarray(sites, dtype=np.float64).reshape(-1, 3)
-        self._check(lib.sc_add_filaments(h, ctypes.c_int(len(filaments)), fils, _p(sites),
-                                         ctypes.c_int64(sites.shape[0])))
+        if replicas is None:
+            self._check(lib.sc_add_filaments(h, ctypes.c_int(len(filaments)), fils, _p(sites),
+                                             ctypes.c_int64(sites.shape[0])))
+        else:
+            radius = np.array([r["system_radius"] for r in replicas], dtype=np.float64)
+            seeds = np.array([r["seed"] for r in replicas], dtype=np.uint32)
+            nfil = np.array([r["n_filaments"] for r in replicas], dtype=np.int32)
+            self._check(lib.sc_add_replicas(h, ctypes.c_int(len(replicas)), _p(radius),
+                                            _p(seeds), _p(nfil), ctypes.c_int(len(filaments)),
+                                            fils, _p(sites), ctypes.c_int64(sites.shape[0])))
+        self.n_replicas = 1 if replicas is None else len(replicas)
         c = self.counters()
         self.n_sites, self.n_bonds, self.n_fil = c.n_sites, c.n_bonds, c.n_filaments
 
@@ -294,6 +307,13 @@ class Context:
         ms = ctypes.c_double()
         self._check(lib.sc_get_graph_time(self.h, ctypes.byref(ms)))
         return ms.value
+
+    def replica_counters(self):
+        """(rebuilds, pairs) per system."""
+        nr = np.zeros(self.n_replicas, dtype=np.int64)
+        npr = np.zeros(self.n_replicas, dtype=np.int64)
+        self._check(lib.sc_get_replica_counters(self.h, _p(nr), _p(npr)))
+        return nr, npr
 
     def counters(self):
         c = Counters()

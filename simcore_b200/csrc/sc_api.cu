@@ -32,13 +32,18 @@ struct sc_ctx {
   int nf = 0, ns = 0, nb = 0;
   std::vector<int> site_off;
   std::vector<int> bond_fil;
+  std::vector<int> fil_rep;        // system of each filament
   bool loaded = false;
+
+  // systems (replicas): host copy of the device table
+  std::vector<sc::ReplicaConst> reps;
+  std::vector<int> np_rep;         // pairs per system (last read back)
 
   // cell list and pair list storage
   int *key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
   int *sorted = nullptr, *pair_count = nullptr, *pair_off = nullptr;
-  int *deg = nullptr, *scan_tmp = nullptr, *cells_xyz = nullptr;
-  long long np = 0, pcap = 0;
+  int *deg = nullptr, *deg_off = nullptr, *scan_tmp = nullptr, *cells_xyz = nullptr;
+  long long np = 0, pcap = 0;      // pairs and slots of all systems
 
   // integrator blocks
   int nblocks = 0, C = 128;
@@ -60,6 +65,9 @@ struct sc_ctx {
     unsigned status;
     int total;
   } *hb = nullptr;
+  unsigned long long *h_dr = nullptr;  // per system displacement maxima
+  int *h_np = nullptr;                 // per system pair counts
+  int *h_due = nullptr;                // per system rebuild flags
 
   // CUDA graph: a WHILE loop of BD steps (sc_step_graph)
   cudaGraphExec_t graph_exec = nullptr;
@@ -169,10 +177,11 @@ sc_status check_status(sc_ctx *c) {
   return SC_OK;
 }
 
-// Reads status and the displacement maximum written by earlier kernels.
+// Reads the status word and every system's displacement maximum.
 sc_status readback(sc_ctx *c) {
-  CK(cudaMemcpyAsync(&c->hb->dr_bits, c->d.dr_max_bits, sizeof(unsigned long long),
-                     cudaMemcpyDeviceToHost, c->st));
+  if (c->d.nrep > 0)
+    CK(cudaMemcpyAsync(c->h_dr, c->d.dr_max_bits, sizeof(unsigned long long) * c->d.nrep,
+                       cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned),
                      cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -187,12 +196,73 @@ void drop_graph(sc_ctx *c) {
   c->graph_rbuf = -1;
 }
 
-// Grows the pair storage to at least `need` pairs, keeping the current list
-// (pairs, their stored forces and the per-bond entries).
+// Copies the system table to the device (segments or layout changed).
+sc_status upload_reps(sc_ctx *c) {
+  const int nrep = (int)c->reps.size();
+  if (!c->d.rep) {
+    sc::ReplicaConst *q = nullptr;
+    CKS(dalloc(c, &q, nrep));
+    c->d.rep = q;
+  }
+  CK(cudaMemcpyAsync(const_cast<sc::ReplicaConst *>(c->d.rep), c->reps.data(),
+                     sizeof(sc::ReplicaConst) * nrep, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->d.pcap_total = (int)c->pcap;
+  drop_graph(c);  // kernel parameters changed
+  return SC_OK;
+}
+
+void free_pair_storage(sc_ctx *c) {
+  for (void *q : {(void *)c->d.pa, (void *)c->d.pb, (void *)c->d.pos1, (void *)c->d.pos2,
+                  (void *)c->d.pf64, (void *)c->d.pf32, (void *)c->d.cf64, (void *)c->d.cf32,
+                  (void *)c->d.e_ent})
+    dfree(c, q);
+}
+
+// Pair storage for segments of the given capacities, one per system, back
+// to back; previous contents are discarded.  Stored pair forces are padded
+// to 4 values and per-bond slots to 8, so every write is a 16-byte store.
+sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
+  long long total = 0;
+  for (long long x : caps) total += x;
+  if (total >= (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair lists of %lld slots too large", total);
+  free_pair_storage(c);
+  DevState &d = c->d;
+  CKS(dalloc(c, &d.pa, total));
+  CKS(dalloc(c, &d.pb, total));
+  CKS(dalloc(c, &d.pos1, total));
+  CKS(dalloc(c, &d.pos2, total));
+  if (c->prec == 0) {
+    CKS(dalloc(c, &d.pf64, 4 * total));
+    CKS(dalloc(c, &d.cf64, 16 * total));
+    CK(cudaMemsetAsync(d.cf64, 0, sizeof(double) * 16 * total, c->st));
+  } else {
+    CKS(dalloc(c, &d.pf32, 4 * total));
+    CKS(dalloc(c, &d.cf32, 16 * total));
+    CK(cudaMemsetAsync(d.cf32, 0, sizeof(float) * 16 * total, c->st));
+  }
+  CKS(dalloc(c, &d.e_ent, 2 * total));
+  long long p0 = 0;
+  for (size_t r = 0; r < caps.size(); ++r) {
+    c->reps[r].p0 = (int)p0;
+    c->reps[r].pcap = (int)caps[r];
+    p0 += caps[r];
+  }
+  c->pcap = total;
+  return upload_reps(c);
+}
+
+// One system only: grows its segment to at least `need` pairs, keeping the
+// current list (pairs, their stored forces and the per-bond entries).
 sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
   if (need <= c->pcap) return SC_OK;
+  if (c->reps.size() != 1)
+    return fail(c, SC_ERR_LIST_OVERFLOW, "a system's pair list outgrew its segment");
   long long cap = std::max<long long>(need + need / 2, 1024);
-  if (cap > (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list of %lld pairs too large", need);
+  if (cap >= (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list of %lld pairs too large", need);
+  DevState old = c->d;
+  const long long keep = std::min<long long>(c->np, c->pcap);
+  DevState &d = c->d;
   int *pa = nullptr, *pb = nullptr, *ent = nullptr, *pos1 = nullptr, *pos2 = nullptr;
   double *pf64 = nullptr, *cf64 = nullptr;
   float *pf32 = nullptr, *cf32 = nullptr;
@@ -200,96 +270,97 @@ sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
   CKS(dalloc(c, &pb, cap));
   CKS(dalloc(c, &pos1, cap));
   CKS(dalloc(c, &pos2, cap));
-  // Stored pair forces padded to 4 values, per-bond slots to 8 values, so
-  // that every write is a 16-byte vector store.
   if (c->prec == 0) {
     CKS(dalloc(c, &pf64, 4 * cap));
     CKS(dalloc(c, &cf64, 16 * cap));
+    CK(cudaMemsetAsync(cf64, 0, sizeof(double) * 16 * cap, c->st));
   } else {
     CKS(dalloc(c, &pf32, 4 * cap));
     CKS(dalloc(c, &cf32, 16 * cap));
+    CK(cudaMemsetAsync(cf32, 0, sizeof(float) * 16 * cap, c->st));
   }
   CKS(dalloc(c, &ent, 2 * cap));
-  long long keep = std::min(c->np, c->pcap);
   if (keep > 0) {
     auto cp = [&](void *dst, const void *src, size_t bytes) {
       return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->st);
     };
-    CK(cp(pa, c->d.pa, sizeof(int) * keep));
-    CK(cp(pb, c->d.pb, sizeof(int) * keep));
-    CK(cp(pos1, c->d.pos1, sizeof(int) * keep));
-    CK(cp(pos2, c->d.pos2, sizeof(int) * keep));
+    CK(cp(pa, old.pa, sizeof(int) * keep));
+    CK(cp(pb, old.pb, sizeof(int) * keep));
+    CK(cp(pos1, old.pos1, sizeof(int) * keep));
+    CK(cp(pos2, old.pos2, sizeof(int) * keep));
     if (c->prec == 0) {
-      CK(cp(pf64, c->d.pf64, sizeof(double) * 4 * keep));
-      CK(cp(cf64, c->d.cf64, sizeof(double) * 16 * keep));
+      CK(cp(pf64, old.pf64, sizeof(double) * 4 * keep));
+      CK(cp(cf64, old.cf64, sizeof(double) * 16 * keep));
     } else {
-      CK(cp(pf32, c->d.pf32, sizeof(float) * 4 * keep));
-      CK(cp(cf32, c->d.cf32, sizeof(float) * 16 * keep));
+      CK(cp(pf32, old.pf32, sizeof(float) * 4 * keep));
+      CK(cp(cf32, old.cf32, sizeof(float) * 16 * keep));
     }
-    CK(cp(ent, c->d.e_ent, sizeof(int) * 2 * keep));
-  } else {
-    if (c->prec == 0) CK(cudaMemsetAsync(cf64, 0, sizeof(double) * 16 * cap, c->st));
-    else CK(cudaMemsetAsync(cf32, 0, sizeof(float) * 16 * cap, c->st));
+    CK(cp(ent, old.e_ent, sizeof(int) * 2 * keep));
   }
   CK(cudaStreamSynchronize(c->st));
-  for (void *q : {(void *)c->d.pa, (void *)c->d.pb, (void *)c->d.pos1, (void *)c->d.pos2,
-                  (void *)c->d.pf64, (void *)c->d.pf32, (void *)c->d.cf64, (void *)c->d.cf32,
-                  (void *)c->d.e_ent})
-    dfree(c, q);
-  c->d.pa = pa;
-  c->d.pb = pb;
-  c->d.pos1 = pos1;
-  c->d.pos2 = pos2;
-  c->d.pf64 = pf64;
-  c->d.pf32 = pf32;
-  c->d.cf64 = cf64;
-  c->d.cf32 = cf32;
-  c->d.e_ent = ent;
+  free_pair_storage(c);
+  d.pa = pa;
+  d.pb = pb;
+  d.pos1 = pos1;
+  d.pos2 = pos2;
+  d.pf64 = pf64;
+  d.pf32 = pf32;
+  d.cf64 = cf64;
+  d.cf32 = cf32;
+  d.e_ent = ent;
+  c->reps[0].p0 = 0;
+  c->reps[0].pcap = (int)cap;
   c->pcap = cap;
-  drop_graph(c);  // device pointers changed
-  return SC_OK;
+  return upload_reps(c);
 }
 
-// Pair count of the current list (device value).
+// Pair counts of every system (device values); c->np is their total.
 sc_status sync_pair_count(sc_ctx *c) {
-  CK(cudaMemcpyAsync(&c->hb->total, c->d.n_pairs, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  const int nrep = c->d.nrep;
+  CK(cudaMemcpyAsync(c->h_np, c->d.np_rep, sizeof(int) * nrep, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  c->np = c->hb->total;
+  c->np = 0;
+  for (int r = 0; r < nrep; ++r) {
+    c->np_rep[r] = c->h_np[r];
+    c->np += std::min(c->h_np[r], c->reps[r].pcap);
+  }
   return SC_OK;
 }
 
-// InteractionManager::UpdateInteractions (src/interaction_manager.cpp:211-231):
-// bin every bond, emit the half-shell pair list in the reference's order,
-// build the per-bond pair index, zero the displacement trackers.  Device work
-// only (capturable); a list longer than the capacity sets the overflow bit.
+// InteractionManager::UpdateInteractions (src/interaction_manager.cpp:211-231)
+// for the systems flagged in d.due: bin their bonds, emit their half-shell
+// pair lists in the reference's order into their segments, build their
+// per-bond pair entries, zero their displacement trackers.  Device work only
+// (capturable); a list longer than its segment sets the overflow bit.
 void rebuild_enqueue(sc_ctx *c) {
   const SysConst &k = c->k;
   const long long before = c->launches;
+  const DevState &d = c->d;
   if (c->desc.interaction_flag) {
-    c->launches += sc::launch_bin_count(k, c->d, c->key, c->cell_count, c->st);
+    c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
     c->launches += sc::launch_exclusive_scan(c->cell_count, c->cell_start, k.n_cells,
                                              c->scan_tmp, c->st);
-    c->launches += sc::launch_bin_scatter(c->nb, c->key, c->cell_start, c->cell_count,
-                                          c->sorted, c->st);
-    c->launches += sc::launch_cell_sort_count(k, c->d, c->key, c->sorted, c->cell_start,
+    c->launches += sc::launch_bin_scatter(d, c->key, c->cell_start, c->cell_count, c->sorted,
+                                          c->st);
+    c->launches += sc::launch_cell_sort_count(k, d, c->key, c->sorted, c->cell_start,
                                               c->pair_count, c->st);
     c->launches += sc::launch_exclusive_scan(c->pair_count, c->pair_off, c->nb,
                                              c->scan_tmp, c->st);
-    c->launches += sc::launch_pair_emit(k, c->d, c->key, c->sorted, c->cell_start,
-                                        c->pair_off, (int)c->pcap, c->deg, c->prec,
-                                        c->st);
-    c->launches += sc::launch_exclusive_scan(c->deg, c->d.e_off, c->nb, c->scan_tmp,
-                                             c->st);
-    c->launches += sc::launch_csr(c->d, (int)c->pcap, c->deg, c->st);
+    c->launches += sc::launch_pair_emit(k, d, c->key, c->sorted, c->cell_start,
+                                        c->pair_off, c->deg, c->prec, c->st);
+    c->launches += sc::launch_exclusive_scan(c->deg, c->deg_off, c->nb, c->scan_tmp, c->st);
+    c->launches += sc::launch_csr(d, c->deg, c->deg_off, c->st);
   }
-  c->launches += sc::launch_zero_dr(c->d, c->st);
+  c->launches += sc::launch_zero_dr(d, c->st);
   c->rebuild_kernels = c->launches - before;
 }
 
-// Host-driven rebuild: enqueue, then check the list fitted; if it did not,
-// grow the storage and rebuild again (binning is a pure function of the
-// positions, so the second pass gives the same list).
-sc_status rebuild(sc_ctx *c) {
+// Host-driven rebuild of the systems flagged in d.due, then a check that
+// every list fitted.  One system grows its segment and rebuilds again
+// (binning is a pure function of the positions, so the second pass gives the
+// same list); with several systems an overflow is reported, unless
+// allow_overflow (the initial pass, whose caller sizes the segments).
+sc_status rebuild(sc_ctx *c, bool allow_overflow = false) {
   for (int attempt = 0; attempt < 3; ++attempt) {
     rebuild_enqueue(c);
     CK(cudaGetLastError());
@@ -298,35 +369,59 @@ sc_status rebuild(sc_ctx *c) {
                        cudaMemcpyDeviceToHost, c->st));
     CKS(sync_pair_count(c));
     if (!(c->hb->status & sc::ST_LIST_OVERFLOW)) return SC_OK;
-    // Clear the overflow bit, undo the extra rebuild count, grow, retry.
     unsigned clear = c->hb->status & ~sc::ST_LIST_OVERFLOW;
     CK(cudaMemcpyAsync(c->d.status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice, c->st));
-    c->np = 0;  // the overflowed list is incomplete: nothing to keep
-    CKS(ensure_pair_capacity(c, (long long)c->hb->total));
-    long long cnt = 0;
-    CK(cudaMemcpyAsync(&cnt, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    cnt -= 1;
-    CK(cudaMemcpyAsync(c->d.n_rebuilds, &cnt, sizeof(long long), cudaMemcpyHostToDevice, c->st));
+    if (allow_overflow) return SC_OK;
+    if (c->reps.size() != 1)
+      return fail(c, SC_ERR_LIST_OVERFLOW, "a system's pair list outgrew its segment");
+    // Undo the extra rebuild count, grow, retry.
+    const int want = c->np_rep[0];
+    c->np = 0;  // the overflowed list is incomplete: nothing to keep
+    CKS(ensure_pair_capacity(c, (long long)want));
+    long long cnt[2] = {0, 0};
+    CK(cudaMemcpyAsync(&cnt[0], c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&cnt[1], c->d.rep_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    cnt[0] -= 1;
+    cnt[1] -= 1;
+    CK(cudaMemcpyAsync(c->d.n_rebuilds, &cnt[0], sizeof(long long), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d.rep_rebuilds, &cnt[1], sizeof(long long), cudaMemcpyHostToDevice, c->st));
     CK(cudaStreamSynchronize(c->st));
   }
   return fail(c, SC_ERR_LIST_OVERFLOW, "pair list kept overflowing");
 }
 
+// Flags every system and rebuilds (the forced update after insertion).
+sc_status rebuild_all(sc_ctx *c) {
+  const int nrep = c->d.nrep;
+  for (int r = 0; r < nrep; ++r) c->h_due[r] = 1;
+  CK(cudaMemcpyAsync(c->d.due, c->h_due, sizeof(int) * nrep, cudaMemcpyHostToDevice, c->st));
+  return rebuild(c, true);
+}
+
 // Interact's rebuild check (CheckUpdateInteractions + GetDrMax,
-// src/interaction_manager.cpp:284-312, include/simcore/species.hpp:105-120).
-// Only a query after a full step can see a grown displacement, so the device
-// maximum is read back only then.
+// src/interaction_manager.cpp:284-312, include/simcore/species.hpp:105-120),
+// per system.  Only a query after a full step can see a grown displacement,
+// so the device maxima are read back only then.
 sc_status maybe_rebuild(sc_ctx *c) {
   if (!c->desc.interaction_flag) return SC_OK;
   if (!c->midstep) return SC_OK;  // previous update was a midstep: unchanged
   if (c->i_step <= 1) return SC_OK;
   CKS(readback(c));
-  double dr_max;
-  std::memcpy(&dr_max, &c->hb->dr_bits, sizeof(double));
-  if (dr_max > 10000) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result: dr_max %g", dr_max);
-  if (dr_max > c->k.dr_update) CKS(rebuild(c));
-  return SC_OK;
+  const int nrep = c->d.nrep;
+  bool any = false;
+  for (int r = 0; r < nrep; ++r) {
+    double dr_max;
+    std::memcpy(&dr_max, &c->h_dr[r], sizeof(double));
+    if (dr_max > 10000)
+      return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result: dr_max %g (system %d)", dr_max, r);
+    c->h_due[r] = dr_max > c->reps[r].dr_update ? 1 : 0;
+    any = any || c->h_due[r];
+  }
+  if (!any) return SC_OK;
+  CK(cudaMemcpyAsync(c->d.due, c->h_due, sizeof(int) * nrep, cudaMemcpyHostToDevice, c->st));
+  return rebuild(c);
 }
 
 // Integrator work units over the filaments in order: runs of whole
@@ -345,16 +440,19 @@ sc_status layout_integrator(sc_ctx *c) {
   if (max_long > c->C)
     return fail(c, SC_ERR_INVALID_ARG, "a %d-site filament does not fit %d-site blocks", max_long,
                 c->C);
+  // A work unit never mixes systems (its displacement maximum is one
+  // system's).
+  auto same = [&](int f, int f0) { return c->fil_rep.empty() || c->fil_rep[f] == c->fil_rep[f0]; };
   int f = 0;
   while (f < n) {
     const int s0 = off[f], f0 = f;
     if (short_fil(f)) {
-      while (f < n && short_fil(f) && off[f + 1] - s0 <= 32) ++f;
+      while (f < n && short_fil(f) && same(f, f0) && off[f + 1] - s0 <= 32) ++f;
       wg_site0.push_back(s0);
       wg_f0.push_back(f0);
       wg_ns.push_back(off[f] - s0);
     } else {
-      while (f < n && !short_fil(f) && off[f + 1] - s0 <= c->C) ++f;
+      while (f < n && !short_fil(f) && same(f, f0) && off[f + 1] - s0 <= c->C) ++f;
       blk_site0.push_back(s0);
       blk_f0.push_back(f0);
       blk_nf.push_back(f - f0);
@@ -487,14 +585,6 @@ sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
   SysConst &k = c->k;
   std::memset(&k, 0, sizeof(k));
   k.n_dim = c->nd;
-  // Space::InitUnitCell / CalculateUnitCellQuantities (src/space.cpp:85-138)
-  const double hh = 2.0 * desc->system_radius;
-  for (int a = 0; a < c->nd; ++a)
-    for (int b = 0; b < c->nd; ++b) k.h[a * c->nd + b] = (a == b ? 1 : 0) * hh;
-  k.h[c->nd * c->nd - 1] = hh;
-  if (c->nd == 2) invert_sym_2d(k.h, k.hinv);
-  else invert_sym_3d(k.h, k.hinv);
-  for (int i = 0; i < 9; ++i) k.hf[i] = (float)k.h[i];
   k.delta = desc->delta;
   // WCAPotential::Init (include/simcore/wca_potential.hpp:34-48)
   double rcut = std::pow(2.0, 1.0 / 6.0) * desc->wca_sig;
@@ -506,13 +596,10 @@ sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
   k.c12f = (float)k.c12;
   k.c6f = (float)k.c6;
   k.fcutf = (float)k.fcut;
-  k.seed = desc->seed;
   k.stoch = desc->stoch_flag ? 1 : 0;
   k.like_like = desc->like_like_interactions ? 1 : 0;
   CK(cudaMalloc((void **)&c->d.status, sizeof(unsigned)));
   c->allocs.push_back(c->d.status);
-  CK(cudaMalloc((void **)&c->d.dr_max_bits, sizeof(unsigned long long)));
-  c->allocs.push_back(c->d.dr_max_bits);
   CK(cudaMalloc((void **)&c->d.mcount, sizeof(unsigned long long)));
   c->allocs.push_back(c->d.mcount);
   CK(cudaMalloc((void **)&c->d.n_rebuilds, sizeof(long long)));
@@ -520,7 +607,6 @@ sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
   CK(cudaMalloc((void **)&c->d.loop_count, sizeof(int)));
   c->allocs.push_back(c->d.loop_count);
   CK(cudaMemsetAsync(c->d.status, 0, sizeof(unsigned), c->st));
-  CK(cudaMemsetAsync(c->d.dr_max_bits, 0, sizeof(unsigned long long), c->st));
   CK(cudaMemsetAsync(c->d.mcount, 0, sizeof(unsigned long long), c->st));
   CK(cudaMemsetAsync(c->d.n_rebuilds, 0, sizeof(long long), c->st));
   CK(cudaMemsetAsync(c->d.loop_count, 0, sizeof(int), c->st));
@@ -540,6 +626,8 @@ sc_status sc_destroy(sc_ctx *c) {
   for (void *p : c->allocs) cudaFree(p);
   if (c->hb) cudaFreeHost(c->hb);
   if (c->h_loop) cudaFreeHost(c->h_loop);
+  for (void *h : {(void *)c->h_dr, (void *)c->h_np, (void *)c->h_due})
+    if (h) cudaFreeHost(h);
   if (c->gev0) cudaEventDestroy(c->gev0);
   if (c->gev1) cudaEventDestroy(c->gev1);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -552,11 +640,28 @@ sc_status sc_destroy(sc_ctx *c) {
 
 const char *sc_last_error(const sc_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
-sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
-                           const double *site_xyz, int64_t n_sites_total) {
+// Loads nrep independent systems: system r has radius[r], noise key seed[r]
+// and nfil[r] filaments, which come next in p and site_xyz.  A single-system
+// context is the case nrep = 1.
+static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const uint32_t *seed,
+                             const int32_t *nfil, int n, const sc_filament_params *p,
+                             const double *site_xyz, int64_t n_sites_total) {
   if (!c) return SC_ERR_INVALID_ARG;
   if (c->loaded) return fail(c, SC_ERR_INVALID_ARG, "filaments already added");
   if (n <= 0 || !p || !site_xyz) return fail(c, SC_ERR_INVALID_ARG, "bad filament arrays");
+  if (nrep <= 0 || !radius || !seed || !nfil)
+    return fail(c, SC_ERR_INVALID_ARG, "bad system arrays");
+  {
+    long long tot = 0;
+    for (int r = 0; r < nrep; ++r) {
+      if (nfil[r] <= 0) return fail(c, SC_ERR_INVALID_ARG, "system %d has no filaments", r);
+      if (!(radius[r] > 0)) return fail(c, SC_ERR_INVALID_ARG, "system %d: bad radius", r);
+      tot += nfil[r];
+    }
+    if (tot != n)
+      return fail(c, SC_ERR_INVALID_ARG, "filament counts of the systems sum to %lld, not %d",
+                  tot, n);
+  }
   CK(cudaSetDevice(c->desc.device));
   const double mbl = p[0].min_bond_length, dia = p[0].diameter;
   std::vector<double> len(n);
@@ -611,6 +716,16 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
     q.n = nsf;
   }
   c->site_off = site_off;
+  std::vector<int> fil_rep(n);
+  {
+    int f = 0;
+    for (int r = 0; r < nrep; ++r)
+      for (int i = 0; i < nfil[r]; ++i, ++f) {
+        fil[f].rep = r;
+        fil[f].f_local = i;
+        fil_rep[f] = r;
+      }
+  }
   std::vector<int> site_fil(nsi), site_jn(nsi), bond_fil(nbi);
   for (int f = 0; f < n; ++f) {
     for (int s = site_off[f]; s < site_off[f + 1]; ++s) {
@@ -645,8 +760,15 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
   CKS(up(&tmp_i, site_fil)); d.site_fil = tmp_i;
   CKS(up(&tmp_i, site_jn)); d.site_jn = tmp_i;
   CKS(up(&tmp_i, bond_fil)); d.bond_fil = tmp_i;
+  d.bond_rep = nullptr;  // one system: every bond in system 0
+  if (nrep > 1) {
+    std::vector<int> bond_rep(nbi);
+    for (int b = 0; b < nbi; ++b) bond_rep[b] = fil_rep[bond_fil[b]];
+    CKS(up(&tmp_i, bond_rep));
+    d.bond_rep = tmp_i;
+  }
+  c->fil_rep = fil_rep;
   c->warp_sites = 32;
-  CKS(layout_integrator(c));
 
   // Sites: positions (z = 0 in 2D); previous positions = positions as after
   // Mesh::UpdatePrevPositions; no stored noise yet.
@@ -674,59 +796,134 @@ sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
     CKS(dalloc(c, &d.g32[b], nbi));
   }
 
-  // Cell list: SetMinCellLength calls of Simulation::InitSpecies
-  // (src/simulation.cpp:248-251) and InteractionManager::InitInteractions
-  // (src/interaction_manager.cpp:46-48), CellList::Init (src/cell_list.cpp:17-64).
+  // Systems: Space::InitUnitCell / CalculateUnitCellQuantities
+  // (src/space.cpp:85-138); cell lists: SetMinCellLength calls of
+  // Simulation::InitSpecies (src/simulation.cpp:248-251) and
+  // InteractionManager::InitInteractions (src/interaction_manager.cpp:46-48),
+  // CellList::Init (src/cell_list.cpp:17-64).
   SysConst &k = c->k;
+  c->reps.assign(nrep, sc::ReplicaConst{});
+  long long cells = 0;
   {
-    double min_len = -1, spec_length = 1.5 * mbl;
-    if (dia > spec_length) spec_length = dia;
-    if (spec_length > min_len) min_len = spec_length;
-    if (0.0 > min_len) min_len = 0.0;
-    if (std::sqrt(k.rcut2) > min_len) min_len = std::sqrt(k.rcut2);
-    int n1d = (int)std::floor(2 * c->desc.system_radius / min_len);
-    if (n1d <= 3) n1d = 3;
-    long long ncell = (long long)n1d * n1d * (c->nd == 3 ? n1d : 1);
-    if (ncell > (1ll << 30))
-      return fail(c, SC_ERR_INVALID_ARG, "cell grid of %lld cells too large", ncell);
-    k.n1d = n1d;
-    k.third = c->nd == 3 ? n1d : 1;
-    k.n_cells = (int)ncell;
-    double cl = (double)2 * c->desc.system_radius / n1d;
-    k.dr_update = 0.25 * cl * cl;
+    int f = 0;
+    for (int r = 0; r < nrep; ++r) {
+      sc::ReplicaConst &R = c->reps[r];
+      std::memset(&R, 0, sizeof(R));
+      const double hh = 2.0 * radius[r];
+      for (int a = 0; a < c->nd; ++a)
+        for (int b = 0; b < c->nd; ++b) R.h[a * c->nd + b] = (a == b ? 1 : 0) * hh;
+      R.h[c->nd * c->nd - 1] = hh;
+      if (c->nd == 2) invert_sym_2d(R.h, R.hinv);
+      else invert_sym_3d(R.h, R.hinv);
+      for (int i = 0; i < 9; ++i) R.hf[i] = (float)R.h[i];
+      double min_len = -1, spec_length = 1.5 * mbl;
+      if (dia > spec_length) spec_length = dia;
+      if (spec_length > min_len) min_len = spec_length;
+      if (0.0 > min_len) min_len = 0.0;
+      if (std::sqrt(k.rcut2) > min_len) min_len = std::sqrt(k.rcut2);
+      int n1d = (int)std::floor(2 * radius[r] / min_len);
+      if (n1d <= 3) n1d = 3;
+      const long long ncell = (long long)n1d * n1d * (c->nd == 3 ? n1d : 1);
+      R.n1d = n1d;
+      R.third = c->nd == 3 ? n1d : 1;
+      R.n_cells = (int)std::min<long long>(ncell, 1ll << 30);
+      R.cell0 = (int)std::min<long long>(cells, 1ll << 30);
+      cells += ncell;
+      const double cl = (double)2 * radius[r] / n1d;
+      R.dr_update = 0.25 * cl * cl;
+      R.seed = seed[r];
+      R.f0 = f;
+      R.nf = nfil[r];
+      R.s0 = site_off[f];
+      R.ns = site_off[f + nfil[r]] - site_off[f];
+      R.b0 = R.s0 - f;
+      R.nb = R.ns - nfil[r];
+      f += nfil[r];
+    }
   }
+  if (cells > (1ll << 30))
+    return fail(c, SC_ERR_INVALID_ARG, "cell grids of %lld cells too large", cells);
+  k.n_cells = (int)cells;
+  d.nrep = nrep;
+  CKS(upload_reps(c));  // every kernel below reads the system table
+  CKS(layout_integrator(c));
+  auto dzero = [&](auto **dst, size_t count) -> sc_status {
+    CKS(dalloc(c, dst, count));
+    CK(cudaMemsetAsync(*dst, 0, sizeof(**dst) * (count ? count : 1), c->st));
+    return SC_OK;
+  };
+  CKS(dzero(&d.dr_max_bits, nrep));
+  CKS(dzero(&d.due, nrep));
+  CKS(dzero(&d.np_rep, nrep));
+  CKS(dzero(&d.rep_rebuilds, nrep));
+  for (void **h : {(void **)&c->h_dr, (void **)&c->h_np, (void **)&c->h_due})
+    if (cudaHostAlloc(h, sizeof(unsigned long long) * nrep, cudaHostAllocDefault) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return fail(c, SC_ERR_OOM, "pinned allocation failed");
+    }
+  c->np_rep.assign(nrep, 0);
   CKS(dalloc(c, &c->key, nbi));
-  CKS(dalloc(c, &c->cell_count, k.n_cells));
-  CK(cudaMemsetAsync(c->cell_count, 0, sizeof(int) * k.n_cells, c->st));
+  CKS(dzero(&c->cell_count, (size_t)k.n_cells));
   CKS(dalloc(c, &c->cell_start, (size_t)k.n_cells + 1));
   CKS(dalloc(c, &c->sorted, nbi));
   CKS(dalloc(c, &c->pair_count, nbi));
-  CKS(dalloc(c, &c->pair_off, (size_t)nbi + 1));
-  CK(cudaMemsetAsync(c->pair_off, 0, sizeof(int) * ((size_t)nbi + 1), c->st));
-  d.n_pairs = c->pair_off + nbi;
-  CKS(dalloc(c, &c->deg, nbi));
-  CK(cudaMemsetAsync(c->deg, 0, sizeof(int) * nbi, c->st));
-  CKS(dalloc(c, &d.e_off, (size_t)nbi + 1));
-  CK(cudaMemsetAsync(d.e_off, 0, sizeof(int) * ((size_t)nbi + 1), c->st));
+  CKS(dzero(&c->pair_off, (size_t)nbi + 1));
+  CKS(dzero(&c->deg, nbi));
+  CKS(dzero(&c->deg_off, (size_t)nbi + 1));
+  CKS(dzero(&d.e_off, nbi));
+  CKS(dzero(&d.e_cnt, nbi));
   CKS(dalloc(c, &c->scan_tmp,
              (size_t)std::max(sc::scan_temp_ints(k.n_cells), sc::scan_temp_ints(nbi))));
   CKS(dalloc(c, &c->cells_xyz, 3 * (size_t)nbi));
-  CKS(ensure_pair_capacity(c, std::max<long long>(nbi, 1024)));
 
   sc::launch_init_geometry(c->k, d, 0, c->prec, c->st);
   if (c->prec != 0) sc::launch_init_geometry(c->k, d, 0, 0, c->st);
   c->rbuf = 0;
-  // Simulation::InsertSpecies tail: forced update (rebuild + ZeroDrTot).
-  CKS(rebuild(c));
-  // Headroom for list growth during captured runs (no resizing inside a graph).
-  CKS(ensure_pair_capacity(c, c->np + c->np / 2 + 1024));
+  // Simulation::InsertSpecies tail: forced update (rebuild + ZeroDrTot) of
+  // every system, into pair segments sized until every list fits with
+  // headroom for growth during captured runs (no resizing inside a graph).
+  std::vector<long long> want(nrep);
+  for (int r = 0; r < nrep; ++r) want[r] = std::max<long long>(c->reps[r].nb, 1024);
+  for (int attempt = 0;; ++attempt) {
+    CKS(layout_pairs(c, want));
+    CKS(rebuild_all(c));
+    bool ok = true;
+    for (int r = 0; r < nrep; ++r) {
+      const long long need = (long long)c->np_rep[r] + c->np_rep[r] / 2 + 1024;
+      if (need > want[r]) {
+        want[r] = need;
+        ok = false;
+      }
+    }
+    if (ok) break;
+    if (attempt == 3) return fail(c, SC_ERR_LIST_OVERFLOW, "pair lists kept overflowing");
+  }
   CK(cudaMemsetAsync(c->d.n_rebuilds, 0, sizeof(long long), c->st));
+  CK(cudaMemsetAsync(c->d.rep_rebuilds, 0, sizeof(long long) * nrep, c->st));
   CK(cudaStreamSynchronize(c->st));
   c->loaded = true;
   c->i_step = 0;
   c->midstep = 1;
   c->mcount = 0;
   return SC_OK;
+}
+
+sc_status sc_add_filaments(sc_ctx *c, int n, const sc_filament_params *p,
+                           const double *site_xyz, int64_t n_sites_total) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  const double radius = c->desc.system_radius;
+  const uint32_t seed = c->desc.seed;
+  const int32_t nf = n;
+  return add_systems(c, 1, &radius, &seed, &nf, n, p, site_xyz, n_sites_total);
+}
+
+sc_status sc_add_replicas(sc_ctx *c, int n_replicas, const double *system_radius,
+                          const uint32_t *seed, const int32_t *n_filaments, int n,
+                          const sc_filament_params *p, const double *site_xyz,
+                          int64_t n_sites_total) {
+  return add_systems(c, n_replicas, system_radius, seed, n_filaments, n, p, site_xyz,
+                     n_sites_total);
 }
 
 sc_status sc_interact(sc_ctx *c) {
@@ -858,7 +1055,8 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
   if (bd > 0) {
     // The list must have room to grow by half before a captured run.
     CKS(sync_pair_count(c));
-    if (c->np + c->np / 2 > c->pcap) CKS(ensure_pair_capacity(c, c->np + c->np / 2));
+    if (c->reps.size() == 1 && c->np + c->np / 2 > c->pcap)
+      CKS(ensure_pair_capacity(c, c->np + c->np / 2));
     if (!c->graph_exec || c->graph_rbuf != c->rbuf) CKS(build_graph(c));
     *c->h_loop = bd;
     CK(cudaMemcpyAsync(c->d.loop_count, c->h_loop, sizeof(int), cudaMemcpyHostToDevice, c->st));
@@ -1041,7 +1239,7 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   regions.push_back({c->d.f_nnorm, sizeof(int) * c->nf});
   if (c->prec == 0) regions.push_back({c->d.g64[wbuf], sizeof(sc::BondGeomF64) * c->nb});
   else regions.push_back({c->d.g32[wbuf], sizeof(sc::BondGeomF32) * c->nb});
-  regions.push_back({c->d.dr_max_bits, sizeof(unsigned long long)});
+  regions.push_back({c->d.dr_max_bits, sizeof(unsigned long long) * c->d.nrep});
   regions.push_back({c->d.status, sizeof(unsigned)});
   size_t total = 0;
   for (auto &r : regions) total += (r.second + 255) & ~(size_t)255;
@@ -1131,6 +1329,11 @@ sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32
       const bool last = site == c->site_off[f + 1] - 1;
       const int bond = last ? site - f - 1 : site - f;
       anchor[2 * (size_t)x + a] = bond << 1 | (last ? 1 : 0);
+      if (a == 1 && c->fil_rep[f] != c->fil_rep[(int)(std::upper_bound(c->site_off.begin(),
+                                                                        c->site_off.end(),
+                                                                        site_a[x]) -
+                                                       c->site_off.begin()) - 1])
+        return fail(c, SC_ERR_INVALID_ARG, "crosslink %d joins two systems", x);
     }
   // Per-bond anchor lists, ascending anchor id (link order, anchor 0 first).
   std::vector<int> off(c->nb + 1, 0), ent(2 * (size_t)n);
@@ -1252,17 +1455,37 @@ sc_status sc_get_pairs(sc_ctx *c, int32_t *pairs, int64_t cap, int64_t *n_pairs)
   if (!c || !c->loaded || !n_pairs) return SC_ERR_INVALID_ARG;
   CKS(sync_pair_count(c));
   *n_pairs = c->np;
-  long long m = std::min<long long>(cap, c->np);
-  if (m > 0 && pairs) {
+  long long out = 0;
+  for (size_t r = 0; r < c->reps.size() && pairs && out < cap; ++r) {
+    const long long m = std::min<long long>(std::min(c->np_rep[r], c->reps[r].pcap), cap - out);
+    if (m <= 0) continue;
     std::vector<int> a(m), b(m);
-    CK(cudaMemcpyAsync(a.data(), c->d.pa, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(b.data(), c->d.pb, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
+    const int p0 = c->reps[r].p0;
+    CK(cudaMemcpyAsync(a.data(), c->d.pa + p0, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(b.data(), c->d.pb + p0, sizeof(int) * m, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    for (long long i = 0; i < m; ++i) {
-      pairs[2 * i] = a[i];
-      pairs[2 * i + 1] = b[i];
+    for (long long i = 0; i < m; ++i, ++out) {
+      pairs[2 * out] = a[i];
+      pairs[2 * out + 1] = b[i];
     }
   }
+  return SC_OK;
+}
+
+sc_status sc_get_replica_counters(sc_ctx *c, int64_t *n_rebuilds, int64_t *n_pairs) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  const int nrep = c->d.nrep;
+  CKS(sync_pair_count(c));
+  if (n_rebuilds) {
+    std::vector<long long> v(nrep);
+    CK(cudaMemcpyAsync(v.data(), c->d.rep_rebuilds, sizeof(long long) * nrep,
+                       cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int r = 0; r < nrep; ++r) n_rebuilds[r] = v[r];
+  }
+  if (n_pairs)
+    for (int r = 0; r < nrep; ++r) n_pairs[r] = std::min(c->np_rep[r], c->reps[r].pcap);
   return SC_OK;
 }
 
@@ -1293,9 +1516,12 @@ sc_status sc_get_counters(sc_ctx *c, sc_counters *o) {
   o->n_filaments = c->nf;
   o->n_sites = c->ns;
   o->n_bonds = c->nb;
-  o->n_cells_1d = c->k.n1d;
-  o->cell_length = c->k.n1d ? (double)2 * c->desc.system_radius / c->k.n1d : 0;
-  o->dr_update = c->k.dr_update;
+  if (!c->reps.empty()) {  // system 0's cell grid
+    o->n_cells_1d = c->reps[0].n1d;
+    o->cell_length = c->reps[0].h[0] / c->reps[0].n1d;
+    o->dr_update = c->reps[0].dr_update;
+  }
+  o->n_replicas = (int32_t)c->reps.size();
   o->kernel_launches = c->launches;
   return SC_OK;
 }

@@ -51,41 +51,62 @@ struct __align__(16) BondGeomF32 {
   float pad;
 };
 
-// Per-system constants, in __constant__ memory of each kernel unit.
+// Constants shared by every system of a context (kernel parameter).
 struct SysConst {
   int n_dim;
-  int n1d;
-  int third;          // n1d in 3D, 1 in 2D
-  int n_cells;
-  double h[9];
-  double hinv[9];
+  int n_cells;        // cells of all systems together
   double delta;
   double rcut2;
   double c12, c6, fcut;
-  double dr_update;
-  float hf[9];        // h in FP32 (mixed stage)
   float rcut2f, c12f, c6f, fcutf;
-  uint32_t seed;
   int stoch;
   int like_like;
   double xk, xkc, xrest;  // crosslink tether: k_spring, k_spring_compress, rest_length
+};
+
+// One independent periodic system (a replica) of a context: its box, cell
+// grid, rebuild threshold and noise key, and where its sites, bonds, cells
+// and pairs lie in the context's arrays.  A single-system context has one.
+struct ReplicaConst {
+  double h[9];        // unit cell (box side 2R on the diagonal), n_dim stride
+  double hinv[9];     // its inverse, as the reference computes it
+  float hf[9];        // h in FP32 (mixed pair stage)
+  int n1d;            // cells per dimension
+  int third;          // n1d in 3D, 1 in 2D
+  int n_cells;        // n1d^n_dim
+  int cell0;          // first cell in the context's cell arrays
+  double dr_update;   // rebuild threshold 0.25 cell_length^2
+  uint32_t seed;      // Philox key word 0 of this system's noise
+  int f0, nf;         // filaments
+  int s0, ns;         // sites
+  int b0, nb;         // bonds
+  int p0, pcap;       // pair segment [p0, p0 + pcap), slots [2 p0, 2 (p0 + pcap))
 };
 
 // Per-filament constants of the integrator.  The reciprocals are the
 // reference's own quotients (1.0 / friction_par_, 2.0 / friction_perp_, ...,
 // src/filament.cpp:783-830, 992-996), evaluated once on the host with the
 // same IEEE operations, so every use sees the bits the reference computes
-// inline.  96 bytes.
+// inline.  112 bytes.
 struct FilConst {
   double l, linv, kappa, l2;                   // bond length, 1/l, lp, l*l
   double igpar, igperp, two_igperp, m1_igperp; // 1/g_par, 1/g_perp, 2/g_perp, -1/g_perp
   double dgam;                                 // 1/g_par - 1/g_perp
   double spar, sperp;                          // sqrt(24 g / delta)
   int site0, n;                                // first site, number of sites
+  int rep, f_local;                            // system, index within it (noise key)
+  int pad0, pad1;
 };
 
 // Launch-invariant device pointers of one context.
 struct DevState {
+  // systems (replicas)
+  int nrep;
+  const ReplicaConst *rep;  // nrep
+  const int *bond_rep;      // nb: system of every bond (null: all in system 0)
+  int *due;                 // nrep: pair list rebuilt in the current rebuild pass
+  int *np_rep;              // nrep: pairs in each system's segment
+  long long *rep_rebuilds;  // nrep: rebuilds per system
   // filaments
   int nf, ns, nb;
   const FilConst *fil;     // nf
@@ -116,7 +137,8 @@ struct DevState {
   int *pa, *pb;
   double *pf64;            // stored force per pair, 4 per pair (x, y, z, pad)
   float *pf32;
-  int *e_off;              // nb+1 CSR of pair entries per bond
+  int *e_off;              // nb: first slot of each bond's pair entries
+  int *e_cnt;              // nb: its number of entries
   int *e_ent;              // entries (pair << 1 | role), sorted by pair per bond
   int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
   double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
@@ -133,11 +155,15 @@ struct DevState {
   double *cap_T;
   // status / control (device-resident so captured graphs need no host state)
   unsigned *status;
-  unsigned long long *dr_max_bits;
+  unsigned long long *dr_max_bits;  // nrep: displacement maximum per system
   unsigned long long *mcount;  // midsteps that drew noise (Philox draw offset)
-  long long *n_rebuilds;       // pair-list rebuilds
+  long long *n_rebuilds;       // rebuild passes (any system)
   int *loop_count;             // remaining BD steps of a graph launch
-  const int *n_pairs;          // current pair count (last entry of the pair offsets)
+  int pcap_total;              // pair slots of all segments
 };
+
+__device__ __forceinline__ int rep_of_bond(const DevState &d, int b) {
+  return d.bond_rep ? d.bond_rep[b] : 0;
+}
 
 }  // namespace sc

@@ -33,7 +33,7 @@ __global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec) {
     r1[i] = d.r[i][site];
     r2[i] = d.r[i][site + 1];
   }
-  bond_from_sites<ND>(k, r1, r2, s, u, len);
+  bond_from_sites<ND>(d.rep[rep_of_bond(d, b)].hinv, r1, r2, s, u, len);
   store_geom<ND>(d, buf, b, s, u, len, prec);
   d.ub[0][b] = u[0];
   d.ub[1][b] = u[1];
@@ -44,10 +44,11 @@ __global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec) {
 // Cell list.
 
 // CellList::FindCellCoords (src/cell_list.cpp:139-157) on the bond's scaled
-// position, recomputed exactly from its sites.
+// position, recomputed exactly from its sites; the cell index within the
+// bond's system.
 template <int ND>
-__device__ __forceinline__ int bond_cell(const SysConst &k, const DevState &d,
-                                         int b, int *xyz) {
+__device__ __forceinline__ int bond_cell(const DevState &d, const ReplicaConst &R, int b,
+                                         int *xyz) {
   int f = d.bond_fil[b];
   int site = b + f;
   double r1[3], r2[3], s[3], u[3], len;
@@ -55,15 +56,15 @@ __device__ __forceinline__ int bond_cell(const SysConst &k, const DevState &d,
     r1[i] = d.r[i][site];
     r2[i] = d.r[i][site + 1];
   }
-  bond_from_sites<ND>(k, r1, r2, s, u, len);
+  bond_from_sites<ND>(R.hinv, r1, r2, s, u, len);
   int c[3] = {0, 0, 0};
   bool bad = false;
 #pragma unroll
   for (int i = 0; i < ND; ++i) {
     double x = s[i] + 0.5;
-    double fl = floor(k.n1d * x);
-    int cc = (fl >= 0.0 && fl <= (double)k.n1d) ? (int)fl : -1;
-    if (cc == k.n1d) cc -= 1;
+    double fl = floor(R.n1d * x);
+    int cc = (fl >= 0.0 && fl <= (double)R.n1d) ? (int)fl : -1;
+    if (cc == R.n1d) cc -= 1;
     if (cc < 0) {
       bad = true;
       cc = 0;
@@ -74,25 +75,33 @@ __device__ __forceinline__ int bond_cell(const SysConst &k, const DevState &d,
   xyz[0] = c[0];
   xyz[1] = c[1];
   xyz[2] = c[2];
-  return (c[0] * k.n1d + c[1]) * k.third + c[2];
+  return (c[0] * R.n1d + c[1]) * R.third + c[2];
 }
 
 template <int ND>
 __global__ void k_bond_cells(SysConst k, DevState d, int *xyz) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
-  bond_cell<ND>(k, d, b, xyz + 3 * (size_t)b);
+  bond_cell<ND>(d, d.rep[rep_of_bond(d, b)], b, xyz + 3 * (size_t)b);
 }
 
+// Bonds of the systems whose list is rebuilt in this pass: global cell key
+// and cell counts.
 template <int ND>
 __global__ void k_bin_count(SysConst k, DevState d, int *key, int *cell_count) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = b < d.nb;
   int c = -1;
   if (active) {
-    int xyz[3];
-    c = bond_cell<ND>(k, d, b, xyz);
-    key[b] = c;
+    const int r = rep_of_bond(d, b);
+    if (d.due[r]) {
+      const ReplicaConst &R = d.rep[r];
+      int xyz[3];
+      c = R.cell0 + bond_cell<ND>(d, R, b, xyz);
+      key[b] = c;
+    } else {
+      active = false;
+    }
   }
   // Warp-aggregated increment: one atomic per distinct cell in the warp.
   unsigned mask = __ballot_sync(0xffffffffu, active);
@@ -105,20 +114,21 @@ __global__ void k_bin_count(SysConst k, DevState d, int *key, int *cell_count) {
 
 // Places each bond into its cell's range; decrements the counts back to
 // zero so the count array is ready for the next rebuild without clearing.
-__global__ void k_bin_scatter(int nb, const int *key, const int *cell_start,
+__global__ void k_bin_scatter(DevState d, const int *key, const int *cell_start,
                               int *cell_count, int *sorted) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb) return;
+  if (b >= d.nb || !d.due[rep_of_bond(d, b)]) return;
   int c = key[b];
   int slot = atomicSub(&cell_count[c], 1) - 1;
   sorted[cell_start[c] + slot] = b;
 }
 
 // Half-shell neighbour cells of (x, y, z) in the order of
-// CellList::AssignCellNeighbors(false) (src/cell_list.cpp:206-262).
-__device__ __forceinline__ int half_shell(const SysConst &k, int x, int y,
-                                          int z, int *out) {
-  int n1d = k.n1d, cnt = 0;
+// CellList::AssignCellNeighbors(false) (src/cell_list.cpp:206-262), as
+// indices within the system.
+__device__ __forceinline__ int half_shell(const SysConst &k, const ReplicaConst &R, int x,
+                                          int y, int z, int *out) {
+  int n1d = R.n1d, cnt = 0;
   int z_end = (k.n_dim == 3 ? z + 2 : z + 1);
   for (int zp = z; zp < z_end; ++zp) {
     int nz = zp;
@@ -132,7 +142,7 @@ __device__ __forceinline__ int half_shell(const SysConst &k, int x, int y,
         if (nx < 0) nx = n1d - 1;
         else if (nx == n1d) nx = 0;
         if (nx == x && ny == y && nz == z) continue;
-        out[cnt++] = (nx * n1d + ny) * k.third + nz;
+        out[cnt++] = (nx * n1d + ny) * R.third + nz;
       }
     }
   }
@@ -153,21 +163,21 @@ __device__ __forceinline__ bool pair_excluded(const SysConst &k,
   return false;
 }
 
-__device__ __forceinline__ void cell_coords(const SysConst &k, int c, int &x,
-                                            int &y, int &z) {
-  z = c % k.third;
-  int t = c / k.third;
-  y = t % k.n1d;
-  x = t / k.n1d;
+__device__ __forceinline__ void cell_coords(const ReplicaConst &R, int c, int &x, int &y,
+                                            int &z) {
+  z = c % R.third;
+  int t = c / R.third;
+  y = t % R.n1d;
+  x = t / R.n1d;
 }
 
 // One thread per cell head (first entry of a cell in the sorted order):
 // restores insertion order inside the cell (bond order, as Cell::AddObj
-// appends in interactor order).
-__global__ void k_cell_sort(int nb, const int *key, int *sorted,
-                            const int *cell_start) {
+// appends in interactor order).  The sorted order holds the bonds of the
+// systems rebuilt in this pass, cell_start[n_cells] of them.
+__global__ void k_cell_sort(SysConst k, const int *key, int *sorted, const int *cell_start) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nb) return;
+  if (q >= cell_start[k.n_cells]) return;
   int c = key[sorted[q]];
   if (cell_start[c] != q) return;
   int m = cell_start[c + 1] - q;
@@ -182,27 +192,33 @@ __global__ void k_cell_sort(int nb, const int *key, int *sorted,
   }
 }
 
-// One thread per cell head: number of kept pairs the cell contributes.
+// One thread per cell head: number of kept pairs the cell contributes (zero
+// for every other entry, so that the scan over all bonds sees only heads).
 __global__ void k_cell_count(SysConst k, DevState d, int nb, const int *key,
                              const int *sorted, const int *cell_start,
                              int *pair_count) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nb) return;
+  if (q >= cell_start[k.n_cells]) {
+    pair_count[q] = 0;
+    return;
+  }
   int c = key[sorted[q]];
   if (cell_start[c] != q) {
     pair_count[q] = 0;
     return;
   }
+  const ReplicaConst &R = d.rep[rep_of_bond(d, sorted[q])];
   int m = cell_start[c + 1] - q;
   const int *it = sorted + q;
   long long cnt = 0;
   for (int i = 0; i < m - 1; ++i)
     for (int j = i + 1; j < m; ++j) cnt += !pair_excluded(k, d, it[i], it[j]);
   int x, y, z, nbr[13];
-  cell_coords(k, c, x, y, z);
-  int nn = half_shell(k, x, y, z, nbr);
+  cell_coords(R, c - R.cell0, x, y, z);
+  int nn = half_shell(k, R, x, y, z, nbr);
   for (int kk = 0; kk < nn; ++kk) {
-    int cn = nbr[kk];
+    int cn = R.cell0 + nbr[kk];
     int s0 = cell_start[cn], s1 = cell_start[cn + 1];
     for (int i = 0; i < m; ++i)
       for (int j = s0; j < s1; ++j) cnt += !pair_excluded(k, d, it[i], sorted[j]);
@@ -210,34 +226,37 @@ __global__ void k_cell_count(SysConst k, DevState d, int nb, const int *key,
   pair_count[q] = cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
 }
 
-// Writes each cell's pairs at its offset in the reference's list order
-// (Cell::MakePairs, src/cell.cpp:14-22): pairs inside the cell, then with
-// each half-shell neighbour; clears each new pair's stored force and counts
-// per-bond pair entries for the CSR.
+// Writes each cell's pairs at its offset in its system's pair segment, in the
+// reference's list order (Cell::MakePairs, src/cell.cpp:14-22): pairs inside
+// the cell, then with each half-shell neighbour; clears each new pair's
+// stored force and counts per-bond pair entries for the CSR.
 __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
                             const int *sorted, const int *cell_start,
-                            const int *pair_off, int cap, int *deg, int prec) {
+                            const int *pair_off, int *deg, int prec) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nb) return;
+  if (q >= cell_start[k.n_cells]) return;
   int c = key[sorted[q]];
   if (cell_start[c] != q) return;
+  const ReplicaConst &R = d.rep[rep_of_bond(d, sorted[q])];
   int m = cell_start[c + 1] - q;
   const int *it = sorted + q;
-  int p = pair_off[q];
+  // Offset within the system: its pairs start at its first cell's head.
+  int p = pair_off[q] - pair_off[cell_start[R.cell0]];
   int x, y, z, nbr[13];
-  cell_coords(k, c, x, y, z);
-  int nn = half_shell(k, x, y, z, nbr);
+  cell_coords(R, c - R.cell0, x, y, z);
+  int nn = half_shell(k, R, x, y, z, nbr);
   auto emit = [&](int a, int b) {
     if (pair_excluded(k, d, a, b)) return;
-    if (p < cap) {
-      d.pa[p] = a;
-      d.pb[p] = b;
+    if (p < R.pcap) {
+      const int g = R.p0 + p;
+      d.pa[g] = a;
+      d.pb[g] = b;
       if (prec == 0) {
-        double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)p;
+        double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)g;
         st[0] = make_double2(0.0, 0.0);
         st[1] = make_double2(0.0, 0.0);
       } else {
-        reinterpret_cast<float4 *>(d.pf32)[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        reinterpret_cast<float4 *>(d.pf32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       atomicAdd(&deg[a], 1);
       atomicAdd(&deg[b], 1);
@@ -247,20 +266,63 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
   for (int i = 0; i < m - 1; ++i)
     for (int j = i + 1; j < m; ++j) emit(it[i], it[j]);
   for (int kk = 0; kk < nn; ++kk) {
-    int cn = nbr[kk];
+    int cn = R.cell0 + nbr[kk];
     int s0 = cell_start[cn], s1 = cell_start[cn + 1];
     for (int i = 0; i < m; ++i)
       for (int j = s0; j < s1; ++j) emit(it[i], sorted[j]);
   }
 }
 
-// Entries (pair << 1 | role) of every bond; role 0 = obj1, 1 = obj2.  The
-// degree array is decremented back to zero.
-__global__ void k_csr_fill(DevState d, int cap, int *deg) {
+// Pairs of each rebuilt system: the span of its cells' offsets.  A list
+// longer than its segment sets the overflow bit (the count is kept so the
+// host can size the segment).
+__global__ void k_rep_pairs(SysConst k, DevState d, const int *cell_start, const int *pair_off) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= d.nrep || !d.due[r]) return;
+  const ReplicaConst &R = d.rep[r];
+  const int np = pair_off[cell_start[R.cell0 + R.n_cells]] - pair_off[cell_start[R.cell0]];
+  d.np_rep[r] = np;
+  if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+}
+
+// Per-bond entry ranges of the rebuilt systems, inside their slot segments,
+// from the exclusive scan of the degrees over all bonds.
+__global__ void k_csr_offsets(DevState d, const int *deg_off, const int *deg) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  const int r = rep_of_bond(d, b);
+  if (!d.due[r]) return;
+  const ReplicaConst &R = d.rep[r];
+  d.e_off[b] = 2 * R.p0 + (deg_off[b] - deg_off[R.b0]);
+  d.e_cnt[b] = deg[b];
+}
+
+// System of pair slot p (the segment that holds it).
+__device__ __forceinline__ int rep_of_pair(const DevState &d, int p) {
+  int lo = 0, hi = d.nrep - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (d.rep[mid].p0 <= p) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Slot p holds a current pair of its system.
+__device__ __forceinline__ bool pair_live(const DevState &d, int p, int &r) {
+  r = rep_of_pair(d, p);
+  const ReplicaConst &R = d.rep[r];
+  const int local = p - R.p0;
+  return local < R.pcap && local < d.np_rep[r];
+}
+
+// Entries (pair << 1 | role) of every bond of the rebuilt systems; role 0 =
+// obj1, 1 = obj2.  The degree array is decremented back to zero.
+__global__ void k_csr_fill(DevState d, int *deg) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
-  int np = *d.n_pairs;
-  if (p == 0 && np > cap) atomicOr(d.status, ST_LIST_OVERFLOW);
-  if (p >= np || p >= cap) return;
+  if (p >= d.pcap_total) return;
+  int r;
+  if (!pair_live(d, p, r) || !d.due[r]) return;
   int a = d.pa[p], b = d.pb[p];
   int sa = atomicSub(&deg[a], 1) - 1;
   int sb = atomicSub(&deg[b], 1) - 1;
@@ -272,8 +334,8 @@ __global__ void k_csr_fill(DevState d, int cap, int *deg) {
 // reference's serial ApplyPairInteractions adds them to the bond.
 __global__ void k_csr_sort(DevState d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= d.nb) return;
-  int e0 = d.e_off[b], e1 = d.e_off[b + 1];
+  if (b >= d.nb || !d.due[rep_of_bond(d, b)]) return;
+  int e0 = d.e_off[b], e1 = e0 + d.e_cnt[b];
   int *e = d.e_ent;
   for (int i = e0 + 1; i < e1; ++i) {
     int v = e[i], j = i - 1;
@@ -285,14 +347,17 @@ __global__ void k_csr_sort(DevState d) {
   }
 }
 
-// InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321).
+// InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321) for
+// the systems rebuilt in this pass.
 __global__ void k_zero_dr(DevState d) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) {
-    *d.dr_max_bits = 0ull;
-    *d.n_rebuilds += 1;
+  if (i == 0) *d.n_rebuilds += 1;
+  if (i < d.nrep && d.due[i]) {
+    d.dr_max_bits[i] = 0ull;
+    d.rep_rebuilds[i] += 1;
   }
   if (i >= d.ns) return;
+  if (!d.due[d.fil[d.site_fil[i]].rep]) return;
   d.dz[0][i] = d.r[0][i];
   d.dz[1][i] = d.r[1][i];
   d.dz[2][i] = d.r[2][i];
@@ -394,8 +459,8 @@ __global__ void k_scan_add(int *out, int n, const int *tile_sums) {
 // contacts), and the pair's thread owns that stored force.
 
 template <int ND, int PREC>
-__device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d, int rbuf,
-                                              int p) {
+__device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
+                                              const ReplicaConst &R, int rbuf, int p) {
   const int a = d.pa[p], b = d.pb[p];
   const int s1 = d.pos1[p], s2 = d.pos2[p];
   if (PREC == 0) {
@@ -403,7 +468,7 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     double2 *stale = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)p;
     const double2 st0 = stale[0], st1 = stale[1];
     PairGeom<double> g;
-    sphero_f64<ND>(k, A, B, g);
+    sphero_f64<ND>(R.h, A, B, g);
     double force[3];
     if (!wca_f64<ND>(k, g, force)) {
       force[0] = st0.x;
@@ -430,7 +495,7 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
     PairGeom<float> g;
-    sphero_f32<ND>(k, A, B, g);
+    sphero_f32<ND>(R.hf, A, B, g);
     float force[3];
     if (!wca_f32<ND>(k, g, force)) {
       force[0] = st.x;
@@ -455,13 +520,24 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
   }
 }
 
-// Grid-stride over the current list, so a captured launch stays correct
-// whatever length the list grows to between captures.
+// Grid-stride over the pair slots, so a captured launch stays correct
+// whatever length the lists grow to between captures.  A single system's
+// list is the prefix of its segment; with several systems every slot checks
+// that it holds a current pair of its system.
 template <int ND, int PREC>
 __global__ void __launch_bounds__(256) k_pair_eval(SysConst k, DevState d, int rbuf) {
-  const int np = *d.n_pairs;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
-    pair_eval_one<ND, PREC>(k, d, rbuf, p);
+  if (d.nrep == 1) {
+    const ReplicaConst &R = d.rep[0];
+    const int np = min(d.np_rep[0], R.pcap);
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
+      pair_eval_one<ND, PREC>(k, d, R, rbuf, p);
+    return;
+  }
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
+       p += gridDim.x * blockDim.x) {
+    int r;
+    if (pair_live(d, p, r)) pair_eval_one<ND, PREC>(k, d, d.rep[r], rbuf, p);
+  }
 }
 
 // Bond force/torque accumulators (Bond::force_ / torque_ after Interact),
@@ -492,6 +568,8 @@ template <int ND>
 __global__ void k_tether(SysConst k, DevState d) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= d.nx) return;
+  // Both anchors lie in one system (checked when the links are added).
+  const ReplicaConst &Rx = d.rep[rep_of_bond(d, d.xl_anchor[2 * x] >> 1)];
   double sp[2][3], ua[2][3], len[2], lam[2];
 #pragma unroll
   for (int a = 0; a < 2; ++a) {
@@ -526,7 +604,7 @@ __global__ void k_tether(SysConst k, DevState d) {
     for (int i = 0; i < ND; ++i) {
       double v = 0.0;
 #pragma unroll
-      for (int j = 0; j < ND; ++j) v += k.hinv[ND * i + j] * ap[j];
+      for (int j = 0; j < ND; ++j) v += Rx.hinv[ND * i + j] * ap[j];
       sp[a][i] = v - nint(v);
     }
   }
@@ -541,7 +619,7 @@ __global__ void k_tether(SysConst k, DevState d) {
   for (int i = 0; i < ND; ++i) {
     double v = 0.0;
 #pragma unroll
-    for (int j = 0; j < ND; ++j) v += k.h[ND * i + j] * ds[j];
+    for (int j = 0; j < ND; ++j) v += Rx.h[ND * i + j] * ds[j];
     dr[i] = v;
   }
 #pragma unroll
@@ -570,7 +648,8 @@ __global__ void k_tether(SysConst k, DevState d) {
 __global__ void k_csr_pos(DevState d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
-  for (int e = d.e_off[b]; e < d.e_off[b + 1]; ++e) {
+  if (!d.due[rep_of_bond(d, b)]) return;
+  for (int e = d.e_off[b]; e < d.e_off[b] + d.e_cnt[b]; ++e) {
     int ent = d.e_ent[e];
     if (ent & 1) d.pos2[ent >> 1] = e;
     else d.pos1[ent >> 1] = e;
@@ -617,16 +696,16 @@ int launch_bond_cells(const SysConst &k, const DevState &d, int *xyz,
   return 1;
 }
 
-int launch_bin_scatter(int nb, const int *key, const int *cell_start,
+int launch_bin_scatter(const DevState &d, const int *key, const int *cell_start,
                        int *cell_count, int *sorted, cudaStream_t st) {
-  k_bin_scatter<<<cdiv(nb, 256), 256, 0, st>>>(nb, key, cell_start, cell_count, sorted);
+  k_bin_scatter<<<cdiv(d.nb, 256), 256, 0, st>>>(d, key, cell_start, cell_count, sorted);
   return 1;
 }
 
 int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
                            int *sorted, const int *cell_start, int *pair_count,
                            cudaStream_t st) {
-  k_cell_sort<<<cdiv(d.nb, 128), 128, 0, st>>>(d.nb, key, sorted, cell_start);
+  k_cell_sort<<<cdiv(d.nb, 128), 128, 0, st>>>(k, key, sorted, cell_start);
   k_cell_count<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted,
                                                 cell_start, pair_count);
   return 2;
@@ -634,18 +713,20 @@ int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
 
 int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      const int *sorted, const int *cell_start,
-                     const int *pair_off, int cap, int *deg, int prec,
+                     const int *pair_off, int *deg, int prec,
                      cudaStream_t st) {
   k_pair_emit<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted, cell_start,
-                                               pair_off, cap, deg, prec);
-  return 1;
+                                               pair_off, deg, prec);
+  k_rep_pairs<<<cdiv(d.nrep, 128), 128, 0, st>>>(k, d, cell_start, pair_off);
+  return 2;
 }
 
-int launch_csr(const DevState &d, int cap, int *deg, cudaStream_t st) {
-  k_csr_fill<<<cdiv(cap > 0 ? cap : 1, 256), 256, 0, st>>>(d, cap, deg);
+int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st) {
+  k_csr_offsets<<<cdiv(d.nb, 256), 256, 0, st>>>(d, deg_off, deg);
+  k_csr_fill<<<cdiv(d.pcap_total > 0 ? d.pcap_total : 1, 256), 256, 0, st>>>(d, deg);
   k_csr_sort<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
   k_csr_pos<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
-  return 3;
+  return 4;
 }
 
 // ---------------------------------------------------------------------------
@@ -656,11 +737,19 @@ int launch_csr(const DevState &d, int cap, int *deg, cudaStream_t st) {
 // sets the IF condition of the rebuild body; above 10000 the reference
 // throws, here the status word records it and no rebuild runs.
 __global__ void k_decide(SysConst k, DevState d, cudaGraphConditionalHandle h) {
-  double dr = __longlong_as_double((long long)*d.dr_max_bits);
-  unsigned cond = 0;
-  if (dr > 10000.0 || !(dr == dr)) atomicOr(d.status, ST_UNPHYSICAL);
-  else cond = dr > k.dr_update ? 1u : 0u;
-  cudaGraphSetConditional(h, cond);
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < d.nrep; r += blockDim.x) {
+    const double dr = __longlong_as_double((long long)d.dr_max_bits[r]);
+    int due = 0;
+    if (dr > 10000.0 || !(dr == dr)) atomicOr(d.status, ST_UNPHYSICAL);
+    else due = dr > d.rep[r].dr_update ? 1 : 0;
+    d.due[r] = due;
+    if (due) any = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
 }
 
 __global__ void k_loop_head(DevState d, cudaGraphConditionalHandle h) {
@@ -682,7 +771,7 @@ __global__ void k_advance_mcount(DevState d) { *d.mcount += 1ull; }
 
 int launch_decide(const SysConst &k, const DevState &d,
                   cudaGraphConditionalHandle h, cudaStream_t st) {
-  k_decide<<<1, 1, 0, st>>>(k, d, h);
+  k_decide<<<1, 256, 0, st>>>(k, d, h);
   return 1;
 }
 
@@ -704,12 +793,14 @@ int launch_advance_mcount(const DevState &d, cudaStream_t st) {
 }
 
 int launch_zero_dr(const DevState &d, cudaStream_t st) {
-  k_zero_dr<<<cdiv(d.ns > 0 ? d.ns : 1, 256), 256, 0, st>>>(d);
+  const int n = d.ns > d.nrep ? d.ns : d.nrep;
+  k_zero_dr<<<cdiv(n > 0 ? n : 1, 256), 256, 0, st>>>(d);
   return 1;
 }
 
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
                  int expected, cudaStream_t st) {
+  if (d.nrep > 1) expected = d.pcap_total;
   int grid = cdiv(expected > 0 ? expected : 1, 256);
   if (k.n_dim == 3) {
     if (prec == 0) k_pair_eval<3, 0><<<grid, 256, 0, st>>>(k, d, rbuf);

@@ -18,16 +18,20 @@ int launch_bin_count(const SysConst &k, const DevState &d, int *key,
                      int *cell_count, cudaStream_t st);
 int launch_bond_cells(const SysConst &k, const DevState &d, int *xyz,
                       cudaStream_t st);
-int launch_bin_scatter(int nb, const int *key, const int *cell_start,
+// The rebuild pass covers the systems flagged in d.due; bonds of other
+// systems are skipped and keep their lists.
+int launch_bin_scatter(const DevState &d, const int *key, const int *cell_start,
                        int *cell_count, int *sorted, cudaStream_t st);
 int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
                            int *sorted, const int *cell_start, int *pair_count,
                            cudaStream_t st);
+// Emits the pairs into the systems' segments and records each system's count.
 int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      const int *sorted, const int *cell_start,
-                     const int *pair_off, int cap, int *deg, int prec,
+                     const int *pair_off, int *deg, int prec,
                      cudaStream_t st);
-int launch_csr(const DevState &d, int cap, int *deg, cudaStream_t st);
+// Per-bond entry lists; deg_off is the exclusive scan of deg over all bonds.
+int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st);
 int launch_decide(const SysConst &k, const DevState &d,
                   cudaGraphConditionalHandle h, cudaStream_t st);
 int launch_loop_head(const DevState &d, cudaGraphConditionalHandle h,
@@ -36,7 +40,8 @@ int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
                      cudaStream_t st);
 int launch_advance_mcount(const DevState &d, cudaStream_t st);
 int launch_zero_dr(const DevState &d, cudaStream_t st);
-// Grid sized for `expected` pairs; the kernel strides over the actual count.
+// Grid sized for `expected` pairs (one system) or every slot (several); the
+// kernel strides over the actual pairs.
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
                  int expected, cudaStream_t st);
 // Crosslink tethers of an even step into the per-anchor contributions.

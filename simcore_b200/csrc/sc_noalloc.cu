@@ -9,7 +9,7 @@
 // is part of the library image.
 //
 // The scratch is one file-scope __device__ array (g_noalloc_scratch below,
-// SC_NOALLOC_SCRATCH_BYTES = 8.4 MiB).  Every GPU that loads the library holds it until the
+// SC_NOALLOC_SCRATCH_BYTES = 8.5 MiB).  Every GPU that loads the library holds it until the
 // process exits.  All calls on a device share it and it keeps the last
 // call's contents, so every call clears what must start at zero; calls
 // whose GPU work overlaps (several host threads, or several streams) race
@@ -40,9 +40,9 @@ constexpr int kMaxPairs = SC_NOALLOC_MAX_PAIRS;
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
-  size_t r, key, cell_count, cell_start, sorted, pair_count, pair_off, deg, e_off,
-      scan_tmp, bond_fil, ub, g64, pa, pb, pos1, pos2, pf, cf, e_ent, bF, bT, status,
-      counters, total;
+  size_t r, key, cell_count, cell_start, sorted, pair_count, pair_off, deg, deg_off, e_off,
+      e_cnt, scan_tmp, bond_fil, ub, g64, pa, pb, pos1, pos2, pf, cf, e_ent, bF, bT, status,
+      counters, rep, sys, total;
 };
 
 constexpr int kScanTmp = (kMaxCells > kMaxBonds ? kMaxCells : kMaxBonds) / 2048 + 2;
@@ -58,7 +58,9 @@ constexpr Layout make_layout() {
   L.pair_count = o; o = align256(o + sizeof(int) * kMaxBonds);
   L.pair_off = o;   o = align256(o + sizeof(int) * (kMaxBonds + 1));
   L.deg = o;        o = align256(o + sizeof(int) * kMaxBonds);
-  L.e_off = o;      o = align256(o + sizeof(int) * (kMaxBonds + 1));
+  L.deg_off = o;    o = align256(o + sizeof(int) * (kMaxBonds + 1));
+  L.e_off = o;      o = align256(o + sizeof(int) * kMaxBonds);
+  L.e_cnt = o;      o = align256(o + sizeof(int) * kMaxBonds);
   L.scan_tmp = o;   o = align256(o + sizeof(int) * kScanTmp);
   L.bond_fil = o;   o = align256(o + sizeof(int) * kMaxBonds);
   L.ub = o;         o = align256(o + sizeof(double) * 3 * kMaxBonds);
@@ -74,6 +76,8 @@ constexpr Layout make_layout() {
   L.bT = o;         o = align256(o + sizeof(double) * 3 * kMaxBonds);
   L.status = o;     o = align256(o + sizeof(unsigned));
   L.counters = o;   o = align256(o + sizeof(unsigned long long) * 4);
+  L.rep = o;        o = align256(o + sizeof(sc::ReplicaConst));
+  L.sys = o;        o = align256(o + sizeof(int) * 4);
   L.total = o;
   return L;
 }
@@ -198,13 +202,15 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   std::memset(&k, 0, sizeof(k));
   const int nd = desc->n_dim;
   k.n_dim = nd;
+  sc::ReplicaConst R;
+  std::memset(&R, 0, sizeof(R));
   const double hh = 2.0 * desc->system_radius;
   for (int a = 0; a < nd; ++a)
-    for (int b = 0; b < nd; ++b) k.h[a * nd + b] = (a == b ? 1 : 0) * hh;
-  k.h[nd * nd - 1] = hh;
-  if (nd == 2) inv2(k.h, k.hinv);
-  else inv3(k.h, k.hinv);
-  for (int i = 0; i < 9; ++i) k.hf[i] = (float)k.h[i];
+    for (int b = 0; b < nd; ++b) R.h[a * nd + b] = (a == b ? 1 : 0) * hh;
+  R.h[nd * nd - 1] = hh;
+  if (nd == 2) inv2(R.h, R.hinv);
+  else inv3(R.h, R.hinv);
+  for (int i = 0; i < 9; ++i) R.hf[i] = (float)R.h[i];
   k.delta = desc->delta;
   const double rcut = std::pow(2.0, 1.0 / 6.0) * desc->wca_sig;
   k.rcut2 = rcut * rcut;
@@ -222,10 +228,16 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
     if (n1d <= 3) n1d = 3;
     long long ncell = (long long)n1d * n1d * (nd == 3 ? n1d : 1);
     if (ncell > kMaxCells) return SC_ERR_INVALID_ARG;
-    k.n1d = n1d;
-    k.third = nd == 3 ? n1d : 1;
+    R.n1d = n1d;
+    R.third = nd == 3 ? n1d : 1;
+    R.n_cells = (int)ncell;
     k.n_cells = (int)ncell;
   }
+  R.seed = desc->seed;
+  R.nf = n_filaments;
+  R.ns = ns;
+  R.nb = nb;
+  R.pcap = kMaxPairs;
 
   // Device views into the scratch area.
   const Layout &L = kLayout;
@@ -247,7 +259,15 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   d.pf64 = (double *)(base + L.pf);
   d.cf64 = (double *)(base + L.cf);
   d.e_off = (int *)(base + L.e_off);
+  d.e_cnt = (int *)(base + L.e_cnt);
   d.e_ent = (int *)(base + L.e_ent);
+  d.nrep = 1;
+  d.rep = (const sc::ReplicaConst *)(base + L.rep);
+  d.bond_rep = nullptr;
+  int *sys = (int *)(base + L.sys);
+  d.due = sys;
+  d.np_rep = sys + 1;
+  d.pcap_total = kMaxPairs;
   double *bF = (double *)(base + L.bF), *bT = (double *)(base + L.bT);
   for (int c = 0; c < 3; ++c) {
     d.bF[c] = bF + (size_t)c * kMaxBonds;
@@ -258,11 +278,12 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   d.dr_max_bits = ctr;
   d.mcount = ctr + 1;
   d.n_rebuilds = (long long *)(ctr + 2);
+  d.rep_rebuilds = (long long *)(ctr + 3);
   int *key = (int *)(base + L.key), *cell_count = (int *)(base + L.cell_count);
   int *cell_start = (int *)(base + L.cell_start), *sorted = (int *)(base + L.sorted);
   int *pair_count = (int *)(base + L.pair_count), *pair_off = (int *)(base + L.pair_off);
   int *deg = (int *)(base + L.deg), *scan_tmp = (int *)(base + L.scan_tmp);
-  d.n_pairs = pair_off + nb;
+  int *deg_off = (int *)(base + L.deg_off);
 
   // What must start at zero: the cell and degree counters (the previous
   // call may have stopped early), the status word and the counters.
@@ -270,6 +291,11 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   NA_CK(cudaMemsetAsync(deg, 0, sizeof(int) * (size_t)nb, st));
   NA_CK(cudaMemsetAsync(d.status, 0, sizeof(unsigned), st));
   NA_CK(cudaMemsetAsync(ctr, 0, sizeof(unsigned long long) * 4, st));
+  // The system table and its rebuild flag (a pageable copy: staged before
+  // the call returns).
+  const int sys_init[4] = {1, 0, 0, 0};
+  NA_CK(cudaMemcpyAsync(base + L.rep, &R, sizeof(R), cudaMemcpyHostToDevice, st));
+  NA_CK(cudaMemcpyAsync(sys, sys_init, sizeof(sys_init), cudaMemcpyHostToDevice, st));
 
   const int grid = (ns > n_filaments ? ns : n_filaments) / 256 + 1;
   k_noalloc_unpack<<<grid, 256, 0, st>>>(n_filaments, ns, d_site_offsets, d_site_xyz, nd, d,
@@ -280,12 +306,12 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   // after the reference's insertion computes.
   sc::launch_bin_count(k, d, key, cell_count, st);
   sc::launch_exclusive_scan(cell_count, cell_start, k.n_cells, scan_tmp, st);
-  sc::launch_bin_scatter(nb, key, cell_start, cell_count, sorted, st);
+  sc::launch_bin_scatter(d, key, cell_start, cell_count, sorted, st);
   sc::launch_cell_sort_count(k, d, key, sorted, cell_start, pair_count, st);
   sc::launch_exclusive_scan(pair_count, pair_off, nb, scan_tmp, st);
-  sc::launch_pair_emit(k, d, key, sorted, cell_start, pair_off, kMaxPairs, deg, 0, st);
-  sc::launch_exclusive_scan(deg, d.e_off, nb, scan_tmp, st);
-  sc::launch_csr(d, kMaxPairs, deg, st);
+  sc::launch_pair_emit(k, d, key, sorted, cell_start, pair_off, deg, 0, st);
+  sc::launch_exclusive_scan(deg, deg_off, nb, scan_tmp, st);
+  sc::launch_csr(d, deg, deg_off, st);
   sc::launch_pairs(k, d, 0, 0, kMaxPairs, st);
   sc::launch_bond_sum(k, d, 0, st);
   k_noalloc_pack<<<nb / 256 + 1, 256, 0, st>>>(nb, d, d_bond_force, d_bond_torque);

@@ -27,7 +27,7 @@ struct PairGeom {
 };
 
 template <int ND>
-__device__ __forceinline__ void sphero_f64(const SysConst &k,
+__device__ __forceinline__ void sphero_f64(const double *h,
                                            const BondGeomF64 &A,
                                            const BondGeomF64 &B,
                                            PairGeom<double> &g) {
@@ -43,7 +43,7 @@ __device__ __forceinline__ void sphero_f64(const SysConst &k,
   for (int i = 0; i < ND; ++i) {
     dr[i] = 0.0;
 #pragma unroll
-    for (int j = 0; j < ND; ++j) dr[i] += k.h[ND * i + j] * ds[j];
+    for (int j = 0; j < ND; ++j) dr[i] += h[ND * i + j] * ds[j];
   }
   double dr_dot_u_1 = 0.0, dr_dot_u_2 = 0.0, u_1_dot_u_2 = 0.0;
 #pragma unroll
@@ -167,7 +167,7 @@ __device__ __forceinline__ float fsign_of(float a, float b) {
 }
 
 template <int ND>
-__device__ __forceinline__ void sphero_f32(const SysConst &k,
+__device__ __forceinline__ void sphero_f32(const float *hf,
                                            const BondGeomF32 &A,
                                            const BondGeomF32 &B,
                                            PairGeom<float> &g) {
@@ -182,7 +182,7 @@ __device__ __forceinline__ void sphero_f32(const SysConst &k,
   for (int i = 0; i < ND; ++i) {
     float acc = 0.0f;
 #pragma unroll
-    for (int j = 0; j < ND; ++j) acc = __fmaf_rn(k.hf[ND * i + j], ds[j], acc);
+    for (int j = 0; j < ND; ++j) acc = __fmaf_rn(hf[ND * i + j], ds[j], acc);
     dr[i] = acc;
   }
   float a1 = 0.f, a2 = 0.f, c = 0.f;

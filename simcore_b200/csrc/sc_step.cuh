@@ -17,7 +17,7 @@ namespace sc {
 // Object::UpdatePeriodic / periodic_boundary_conditions
 // (src/object.cpp:202-210, src/linear_algebra.cpp:100-117).
 template <int ND>
-__device__ __forceinline__ void bond_from_sites(const SysConst &k,
+__device__ __forceinline__ void bond_from_sites(const double *hinv,
                                                 const double *r1,
                                                 const double *r2, double s[3],
                                                 double u[3], double &len) {
@@ -40,7 +40,7 @@ __device__ __forceinline__ void bond_from_sites(const SysConst &k,
   for (int i = 0; i < ND; ++i) {
     s[i] = 0.0;
 #pragma unroll
-    for (int j = 0; j < ND; ++j) s[i] += k.hinv[ND * i + j] * pos[j];
+    for (int j = 0; j < ND; ++j) s[i] += hinv[ND * i + j] * pos[j];
     s[i] -= nint(s[i]);
   }
 }
@@ -124,7 +124,7 @@ __device__ __forceinline__ void bond_xlink_sum(const DevState &d, int b, double 
 template <int ND, int PREC>
 __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F[3],
                                               double T[3]) {
-  const int e0 = d.e_off[b], e1 = d.e_off[b + 1];
+  const int e0 = d.e_off[b], e1 = e0 + d.e_cnt[b];
   F[0] = F[1] = F[2] = 0.0;
   T[0] = T[1] = T[2] = 0.0;
   if (d.nx) bond_xlink_sum<ND>(d, b, F, T);
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
       if (active) {  // ConstructUnprojectedRandomForces (:518-548)
         uint32_t w[4];
         sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
-                              k.seed, (uint32_t)f, w);
+                              d.rep[fc.rep].seed, (uint32_t)fc.f_local, w);
         double xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
 #pragma unroll
         for (int i = 0; i < ND; ++i)
@@ -830,7 +830,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
       for (int i = 0; i < ND; ++i) {
         s[i] = 0.0;
 #pragma unroll
-        for (int jj = 0; jj < ND; ++jj) s[i] += k.hinv[ND * i + jj] * pos[jj];
+        for (int jj = 0; jj < ND; ++jj) s[i] += d.rep[fc.rep].hinv[ND * i + jj] * pos[jj];
         s[i] -= nint(s[i]);
       }
       store_geom<ND>(d, 1 - rbuf, b, s, ub, len, PREC);
@@ -876,7 +876,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
       for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
       if (t == 0) {
         if (!(v <= 1e300)) atomicOr(d.status, ST_NAN);
-        atomicMax(d.dr_max_bits, (unsigned long long)__double_as_longlong(v));
+        atomicMax(&d.dr_max_bits[sfil[0].rep], (unsigned long long)__double_as_longlong(v));
       }
     }
   }

@@ -85,8 +85,8 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
   double xi[3] = {0, 0, 0};
   if (midstep && k.stoch) {  // uniforms of ConstructUnprojectedRandomForces
     uint32_t wv[4];
-    sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u, k.seed,
-                          (uint32_t)f, wv);
+    sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
+                          d.rep[fc.rep].seed, (uint32_t)fc.f_local, wv);
 #pragma unroll
     for (int i = 0; i < ND; ++i) xi[i] = ((double)wv[i] + 0.5) * 2.3283064365386963e-10 - 0.5;
   }
@@ -529,7 +529,7 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
       for (int i = 0; i < ND; ++i) {
         s[i] = 0.0;
 #pragma unroll
-        for (int jj = 0; jj < ND; ++jj) s[i] += k.hinv[ND * i + jj] * pos[jj];
+        for (int jj = 0; jj < ND; ++jj) s[i] += d.rep[fc.rep].hinv[ND * i + jj] * pos[jj];
         s[i] -= nint(s[i]);
       }
       store_geom<ND>(d, 1 - rbuf, b, s, ub, len, PREC);
@@ -571,7 +571,8 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
       // Non-negative doubles order as their bit patterns; most warps see a
       // larger maximum already and skip the atomic.
       const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
-      if (bits > *(volatile unsigned long long *)d.dr_max_bits) atomicMax(d.dr_max_bits, bits);
+      unsigned long long *slot = &d.dr_max_bits[fc.rep];
+      if (bits > *(volatile unsigned long long *)slot) atomicMax(slot, bits);
     }
   }
 }

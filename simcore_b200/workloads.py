@@ -10,6 +10,8 @@ rejection (sc_insert_filaments); no dataset is involved.
   A  100 x 20 bonds, lp 500, side 50, dt 1e-4          (CPU parity case)
   B  20,000 x 10 bonds, lp 100, side 200, dt 1e-4       (dense suspension)
   C  50,000 x log-uniform[5,200] bonds, lp U[10,1000], side 300, dt 5e-5
+  D  256 independent 2D systems (make_replicas): N_r ~ U{200..2000}
+     filaments x 16 bonds, side sqrt(N_r (16 + pi/4) / 0.1), lp 200, dt 1e-4
   E  10,000 x 50 bonds, lp 1000, side 150, dt 1e-4      (network geometry;
      volume fraction 0.116 is above the isotropic-nematic point of 50:1 rods,
      so the filaments are inserted straight along -+z, random_nematic)
@@ -68,6 +70,58 @@ def crosslinks(name, sites, filaments, side, scale=1.0, seed=0):
     pick = pairs[rng.choice(len(pairs), size=n, replace=False)]
     return (pick[:, 0].astype(np.int32), pick[:, 1].astype(np.int32), c["k_spring"],
             c["rest_length"])
+
+
+REPLICAS = {"D": dict(n_dim=2, n_replicas=256, n_fil=(200, 2000), n_seg=16, lp=200.0,
+                      area_fraction=0.1, delta=1e-4, n_steps=500)}
+
+
+def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
+                  interaction=True):
+    """Independent systems of workload `name`: returns (system, filaments,
+    sites, replicas) for Context(..., replicas=replicas).  System r has
+    N_r = round(U{lo..hi} * fil_scale) filaments (at least 2) in a periodic
+    square of area N_r (n_seg + pi/4) / area_fraction (the reference's 2D
+    filament area, src/filament.cpp:385-388), noise seed seed * 1000 + r."""
+    w = REPLICAS[name]
+    nrep = w["n_replicas"] if n_replicas is None else int(n_replicas)
+    rng = np.random.default_rng(seed + 4242)
+    lo, hi = w["n_fil"]
+    counts = np.maximum(2, np.round(rng.integers(lo, hi + 1, nrep) * fil_scale)).astype(int)
+    fil_area = w["n_seg"] + math.pi / 4
+    filaments, blocks, replicas = [], [], []
+    for r in range(nrep):
+        n = int(counts[r])
+        side = math.sqrt(n * fil_area / w["area_fraction"])
+        n_seg = np.full(n, w["n_seg"], dtype=np.int32)
+        lengths = n_seg.astype(np.float64)
+        lp = np.full(n, w["lp"])
+        rseed = seed * 1000 + r
+        blocks.append(insert_filaments(w["n_dim"], 0.5 * side, rseed, n_seg, lengths, lp,
+                                       diameter=DIAMETER))
+        filaments += [dict(length=float(lengths[i]), persistence_length=float(lp[i]),
+                           diameter=DIAMETER, min_bond_length=MIN_BOND_LENGTH,
+                           friction_ratio=FRICTION_RATIO) for i in range(n)]
+        replicas.append(dict(system_radius=0.5 * side, seed=rseed, n_filaments=n))
+    system = dict(n_dim=w["n_dim"], system_radius=replicas[0]["system_radius"],
+                  delta=w["delta"], wca_eps=1.0, wca_sig=1.0, f_cutoff=2000.0,
+                  stoch_flag=1 if stoch else 0, interaction_flag=1 if interaction else 0,
+                  like_like_interactions=1, seed=replicas[0]["seed"])
+    return system, filaments, np.concatenate(blocks), replicas
+
+
+def split_replicas(system, filaments, sites, replicas):
+    """Per-system (system, filaments, sites) triples of a replica batch, each
+    as a stand-alone configuration."""
+    out, f0, s0 = [], 0, 0
+    for rep in replicas:
+        fils = filaments[f0:f0 + rep["n_filaments"]]
+        ns = sum(filament_n_bonds(f) + 1 for f in fils)
+        out.append((dict(system, system_radius=rep["system_radius"], seed=rep["seed"]), fils,
+                    sites[s0:s0 + ns]))
+        f0 += rep["n_filaments"]
+        s0 += ns
+    return out
 
 
 def describe(name):

@@ -299,3 +299,72 @@ def test_autotune_leaves_state_and_caches(tmp_path):
     c = _ctx(system, fils, sites)
     assert c.autotune(cache) == lay
     assert len(open(cache).read().strip().splitlines()) == 1
+
+
+def _replica_batch(n_replicas, fil_scale, seed):
+    from simcore_b200 import workloads
+    return workloads.make_replicas("D", n_replicas=n_replicas, fil_scale=fil_scale, seed=seed)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_replicas_bitwise_per_system(graph):
+    """Workload D's batching: five independent 2D systems of different sizes
+    in one context.  Each system is bit-identical to its own oracle run --
+    sites, bond forces, pair list and rebuild count -- although the systems
+    rebuild at different steps and every stage runs for all of them in one
+    launch."""
+    from simcore_b200 import workloads
+    system, fils, sites, reps = _replica_batch(5, 0.03, seed=2)
+    ctx = _ctx_replicas(system, fils, sites, reps)
+    parts = workloads.split_replicas(system, fils, sites, reps)
+    oracles = [Oracle(*p) for p in parts]
+    independent = False
+    for n in (3, 40, 81):
+        if graph:
+            ctx.step_graph(n)
+        else:
+            ctx.step(n)
+        for o in oracles:
+            o.step(n)
+        xyz = ctx.sites()
+        f, t = ctx.bond_forces()
+        pairs = ctx.pairs()
+        nreb, npairs = ctx.replica_counters()
+        s0 = b0 = p0 = 0
+        for r, o in enumerate(oracles):
+            ns, nb = o.n_sites, o.n_bonds
+            assert_same(xyz[s0:s0 + ns, :2], o.sites()[:, :2], "system %d sites" % r)
+            of, ot = o.bond_forces()
+            assert_same(f[b0:b0 + nb, :2], of[:, :2], "system %d bond forces" % r)
+            assert_same(t[b0:b0 + nb], ot, "system %d bond torques" % r)
+            op = o.pairs()
+            assert npairs[r] == len(op)
+            assert_same(pairs[p0:p0 + len(op)] - b0, op, "system %d pairs" % r)
+            assert nreb[r] == o.n_rebuilds, (r, nreb[r], o.n_rebuilds)
+            s0 += ns
+            b0 += nb
+            p0 += len(op)
+        independent = independent or len(set(int(x) for x in nreb)) > 1
+    assert independent  # at some point the systems had rebuilt different numbers of times
+
+
+def test_replicas_mixed_match_single_contexts():
+    """Mixed precision: a system advanced inside the batch gives the same bits
+    as the same system in a context of its own."""
+    from simcore_b200 import workloads
+    system, fils, sites, reps = _replica_batch(3, 0.03, seed=3)
+    ctx = _ctx_replicas(system, fils, sites, reps, "mixed")
+    ctx.step_graph(60)
+    xyz = ctx.sites()
+    s0 = 0
+    for part in workloads.split_replicas(system, fils, sites, reps):
+        single = _ctx(*part, precision="mixed")
+        single.step_graph(60)
+        got = single.sites()
+        assert_same(xyz[s0:s0 + len(got)], got, "system sites")
+        s0 += len(got)
+
+
+def _ctx_replicas(system, filaments, sites, replicas, precision="fp64"):
+    import simcore_b200 as sc
+    return sc.Context(system, filaments, sites, precision=precision, replicas=replicas)
