@@ -231,13 +231,20 @@ class Context:
         return lib.sc_get_stream(self.h)
 
     # state
-    def _vec(self, fn, n):
-        a = np.zeros((n, 3))
+    def _vec(self, fn, n, out=None):
+        if out is None:
+            a = np.zeros((n, 3))
+        else:
+            a = out
+            if a.shape != (n, 3) or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous float64 array of shape (%d, 3)" % n)
         self._check(fn(self.h, _p(a)))
         return a
 
-    def sites(self):
-        return self._vec(lib.sc_get_sites, self.n_sites)
+    def sites(self, out=None):
+        """Site positions (N_s x 3).  out: an array to fill instead (a pinned
+        host buffer makes the copy run at full link speed)."""
+        return self._vec(lib.sc_get_sites, self.n_sites, out)
 
     def set_sites(self, xyz):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)

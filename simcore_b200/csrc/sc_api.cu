@@ -43,6 +43,7 @@ struct sc_ctx {
   int *key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
   int *sorted = nullptr, *pair_count = nullptr, *pair_off = nullptr;
   int *deg = nullptr, *deg_off = nullptr, *scan_tmp = nullptr, *cells_xyz = nullptr;
+  double *stage = nullptr;         // interleaved host-transfer staging, 3 * max(ns, nb)
   long long np = 0, pcap = 0;      // pairs and slots of all systems
 
   // integrator blocks
@@ -534,13 +535,12 @@ sc_status step_once(sc_ctx *c) {
 
 template <class T>
 sc_status copy_soa3(sc_ctx *c, T *const *src, int n, double *xyz) {
-  std::vector<double> tmp(3 * (size_t)n);
-  for (int i = 0; i < 3; ++i)
-    CK(cudaMemcpyAsync(tmp.data() + (size_t)i * n, src[i], sizeof(double) * n,
-                       cudaMemcpyDeviceToHost, c->st));
+  // Interleave on the device, then one copy into the caller's buffer (at
+  // full link speed when that buffer is pinned).
+  c->launches += sc::launch_soa_to_aos(n, src[0], src[1], src[2], c->stage, c->st);
+  CK(cudaMemcpyAsync(xyz, c->stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost,
+                     c->st));
   CK(cudaStreamSynchronize(c->st));
-  for (int j = 0; j < n; ++j)
-    for (int i = 0; i < 3; ++i) xyz[3 * (size_t)j + i] = tmp[(size_t)i * n + j];
   return SC_OK;
 }
 
@@ -876,6 +876,7 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
   CKS(dalloc(c, &c->scan_tmp,
              (size_t)std::max(sc::scan_temp_ints(k.n_cells), sc::scan_temp_ints(nbi))));
   CKS(dalloc(c, &c->cells_xyz, 3 * (size_t)nbi));
+  CKS(dalloc(c, &c->stage, 3 * (size_t)std::max(nsi, nbi)));
 
   sc::launch_init_geometry(c->k, d, 0, c->prec, c->st);
   if (c->prec != 0) sc::launch_init_geometry(c->k, d, 0, 0, c->st);
@@ -1115,17 +1116,14 @@ sc_status sc_get_random_forces(sc_ctx *c, double *f) {
 
 sc_status sc_set_sites(sc_ctx *c, const double *xyz) {
   if (!c || !c->loaded || !xyz) return SC_ERR_INVALID_ARG;
-  std::vector<double> tmp(3 * (size_t)c->ns);
-  for (int s = 0; s < c->ns; ++s)
-    for (int i = 0; i < 3; ++i)
-      tmp[(size_t)i * c->ns + s] = i < c->nd ? xyz[3 * (size_t)s + i] : 0.0;
-  for (int i = 0; i < 3; ++i) {
-    CK(cudaMemcpyAsync(c->d.r[i], tmp.data() + (size_t)i * c->ns, sizeof(double) * c->ns,
-                       cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d.rp[i], tmp.data() + (size_t)i * c->ns, sizeof(double) * c->ns,
-                       cudaMemcpyHostToDevice, c->st));
-  }
+  CK(cudaSetDevice(c->desc.device));
+  // One copy of the caller's x, y, z triples, split into the component
+  // arrays of positions and previous positions on the device.
+  CK(cudaMemcpyAsync(c->stage, xyz, sizeof(double) * 3 * (size_t)c->ns, cudaMemcpyHostToDevice,
+                     c->st));
+  c->launches += sc::launch_aos_to_soa(c->ns, c->nd, c->stage, c->d, c->st);
   sc::launch_init_geometry(c->k, c->d, c->rbuf, c->prec, c->st);
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
   return SC_OK;
 }

@@ -656,6 +656,27 @@ __global__ void k_csr_pos(DevState d) {
   }
 }
 
+// Host transfers: x, y, z triples <-> component arrays.
+__global__ void k_aos_to_soa(int n, int nd, const double *aos, DevState d) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double v = c < nd ? aos[3 * (size_t)i + c] : 0.0;
+    d.r[c][i] = v;
+    d.rp[c][i] = v;
+  }
+}
+
+template <class T>
+__global__ void k_soa_to_aos(int n, const T *x, const T *y, const T *z, double *aos) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  aos[3 * (size_t)i] = (double)x[i];
+  aos[3 * (size_t)i + 1] = (double)y[i];
+  aos[3 * (size_t)i + 2] = (double)z[i];
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers.
 
@@ -669,6 +690,21 @@ void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
 }
 
 int scan_temp_ints(long long n) { return cdiv(n, SCAN_TILE) + 1; }
+
+int launch_aos_to_soa(int n, int nd, const double *aos, const DevState &d, cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_aos_to_soa<<<cdiv(n, 256), 256, 0, st>>>(n, nd, aos, d);
+  return 1;
+}
+
+template <class T>
+int launch_soa_to_aos(int n, const T *x, const T *y, const T *z, double *aos, cudaStream_t st) {
+  if (n <= 0) return 0;
+  k_soa_to_aos<T><<<cdiv(n, 256), 256, 0, st>>>(n, x, y, z, aos);
+  return 1;
+}
+template int launch_soa_to_aos<double>(int, const double *, const double *, const double *,
+                                       double *, cudaStream_t);
 
 // Exclusive scan in[0..n) -> out[0..n], out[n] = total.  tmp holds
 // scan_temp_ints(n) ints.  Returns launches issued.

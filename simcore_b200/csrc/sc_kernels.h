@@ -12,6 +12,11 @@ namespace sc {
 void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
                           int prec, cudaStream_t st);
 int scan_temp_ints(long long n);
+// Interleaved x, y, z triples into positions and previous positions.
+int launch_aos_to_soa(int n, int nd, const double *aos, const DevState &d, cudaStream_t st);
+// Component arrays into interleaved triples.
+template <class T>
+int launch_soa_to_aos(int n, const T *x, const T *y, const T *z, double *aos, cudaStream_t st);
 int launch_exclusive_scan(const int *in, int *out, long long n, int *tmp,
                           cudaStream_t st);
 int launch_bin_count(const SysConst &k, const DevState &d, int *key,
