@@ -26,6 +26,7 @@
 #define SIMCORE_GPU_H
 
 #include <stddef.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -124,6 +125,19 @@ sc_status sc_add_replicas(sc_ctx *ctx, int n_replicas, const double *system_radi
                           const uint32_t *seed, const int32_t *n_filaments, int n,
                           const sc_filament_params *p, const double *site_xyz,
                           int64_t n_sites_total);
+/* Checkpoint of the whole simulation state: positions, previous positions,
+ * projected noise, displacement trackers, renormalisation state, each
+ * system's pair list with its stored pair forces and per-bond entries,
+ * crosslink contributions and the step, midstep and noise counters.  With
+ * buf NULL only *size (the bytes needed) is set.  sc_restore loads one into a
+ * context holding the same systems (same filaments loaded); the restored
+ * context continues bit for bit as the checkpointed one would
+ * (the reference's checkpoint cadence, Simulation n_checkpoint). */
+sc_status sc_checkpoint(sc_ctx *ctx, void *buf, size_t cap, size_t *size);
+sc_status sc_restore(sc_ctx *ctx, const void *buf, size_t size);
+/* Noise key (Philox key word 0) of system `replica`, or of every system for
+ * -1; the draws continue from the current noise counter. */
+sc_status sc_set_noise_key(sc_ctx *ctx, int replica, uint32_t seed);
 /* Per-system rebuild counts and current pair counts (n_replicas entries
  * each; either pointer may be NULL). */
 sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);

@@ -34,7 +34,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_kernel_timing", "sc_get_graph_time", "sc_set_fast_integrator",
             "sc_pair_forces_noalloc", "sc_insert_filaments", "sc_add_crosslinks",
             "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune",
-            "sc_add_replicas", "sc_get_replica_counters"]
+            "sc_add_replicas", "sc_get_replica_counters", "sc_checkpoint", "sc_restore",
+            "sc_set_noise_key"]
 
 
 class ScError(RuntimeError):
@@ -314,6 +315,21 @@ class Context:
         ms = ctypes.c_double()
         self._check(lib.sc_get_graph_time(self.h, ctypes.byref(ms)))
         return ms.value
+
+    def checkpoint(self):
+        """The whole simulation state as bytes (sc_checkpoint)."""
+        size = ctypes.c_size_t()
+        self._check(lib.sc_checkpoint(self.h, None, ctypes.c_size_t(0), ctypes.byref(size)))
+        buf = ctypes.create_string_buffer(size.value)
+        self._check(lib.sc_checkpoint(self.h, buf, size, ctypes.byref(size)))
+        return buf.raw
+
+    def restore(self, data):
+        """Loads a checkpoint of a context holding the same systems."""
+        self._check(lib.sc_restore(self.h, ctypes.c_char_p(data), ctypes.c_size_t(len(data))))
+
+    def set_noise_key(self, seed, replica=-1):
+        self._check(lib.sc_set_noise_key(self.h, ctypes.c_int(replica), ctypes.c_uint32(seed)))
 
     def replica_counters(self):
         """(rebuilds, pairs) per system."""

@@ -233,6 +233,9 @@ sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
   CKS(dalloc(c, &d.pb, total));
   CKS(dalloc(c, &d.pos1, total));
   CKS(dalloc(c, &d.pos2, total));
+  // Slot indices name a valid slot until a rebuild or a restore fills them.
+  CK(cudaMemsetAsync(d.pos1, 0, sizeof(int) * total, c->st));
+  CK(cudaMemsetAsync(d.pos2, 0, sizeof(int) * total, c->st));
   if (c->prec == 0) {
     CKS(dalloc(c, &d.pf64, 4 * total));
     CKS(dalloc(c, &d.cf64, 16 * total));
@@ -879,7 +882,7 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
   CKS(dalloc(c, &c->stage, 3 * (size_t)std::max(nsi, nbi)));
 
   sc::launch_init_geometry(c->k, d, 0, c->prec, c->st);
-  if (c->prec != 0) sc::launch_init_geometry(c->k, d, 0, 0, c->st);
+  if (c->prec != 0) sc::launch_init_geometry(c->k, d, 0, 0, c->st, false);
   c->rbuf = 0;
   // Simulation::InsertSpecies tail: forced update (rebuild + ZeroDrTot) of
   // every system, into pair segments sized until every list fits with
@@ -1305,6 +1308,176 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   return finish(best_lay.first, best_lay.second);
 }
 
+// ---------------------------------------------------------------------------
+// Checkpoint / restore: every piece of state a later step reads, so that a
+// restored context continues bit for bit.
+
+namespace {
+struct CkptHeader {
+  char magic[8];       // "SCB200CK"
+  int32_t version, nd, prec, nrep, nf, ns, nb, nx;
+  int32_t midstep, rbuf, stoch, pad;
+  int64_t i_step;
+  uint64_t mcount;
+  int64_t n_rebuilds;
+};
+
+// Device regions of a checkpoint, in file order.  Pair-list regions use the
+// current segment capacities (recorded per system first).
+struct Region {
+  void *ptr;
+  size_t bytes;
+};
+
+std::vector<Region> state_regions(sc_ctx *c) {
+  std::vector<Region> v;
+  const DevState &d = c->d;
+  const size_t ns = c->ns, nb = c->nb, nf = c->nf, nrep = c->d.nrep;
+  for (int i = 0; i < 3; ++i) v.push_back({d.r[i], sizeof(double) * ns});
+  for (int i = 0; i < 3; ++i) v.push_back({d.rp[i], sizeof(double) * ns});
+  for (int i = 0; i < 3; ++i) v.push_back({d.fr[i], sizeof(double) * ns});
+  for (int i = 0; i < 3; ++i) v.push_back({d.dz[i], sizeof(double) * ns});
+  v.push_back({d.dt, sizeof(double) * ns});
+  v.push_back({d.f_switch, sizeof(int) * nf});
+  v.push_back({d.f_nnorm, sizeof(int) * nf});
+  v.push_back({d.dr_max_bits, sizeof(unsigned long long) * nrep});
+  v.push_back({d.np_rep, sizeof(int) * nrep});
+  v.push_back({d.rep_rebuilds, sizeof(long long) * nrep});
+  v.push_back({d.e_off, sizeof(int) * nb});
+  v.push_back({d.e_cnt, sizeof(int) * nb});
+  // Bond orientations and the geometry the next pair stage reads, as the
+  // integrator wrote them (the fast integrator's bits differ from a
+  // re-derivation).
+  for (int i = 0; i < 3; ++i) v.push_back({d.ub[i], sizeof(double) * nb});
+  if (c->prec == 0) v.push_back({d.g64[c->rbuf], sizeof(sc::BondGeomF64) * nb});
+  else v.push_back({d.g32[c->rbuf], sizeof(sc::BondGeomF32) * nb});
+  const size_t P = (size_t)c->pcap;
+  v.push_back({d.pa, sizeof(int) * P});
+  v.push_back({d.pb, sizeof(int) * P});
+  v.push_back({d.pos1, sizeof(int) * P});  // where each pair writes its two
+  v.push_back({d.pos2, sizeof(int) * P});  // contributions
+  v.push_back({d.e_ent, sizeof(int) * 2 * P});
+  if (c->prec == 0) {
+    v.push_back({d.pf64, sizeof(double) * 4 * P});
+    v.push_back({d.cf64, sizeof(double) * 16 * P});
+  } else {
+    v.push_back({d.pf32, sizeof(float) * 4 * P});
+    v.push_back({d.cf32, sizeof(float) * 16 * P});
+  }
+  if (d.nx) {
+    v.push_back({d.xl_c, sizeof(double) * 16 * (size_t)d.nx});
+    v.push_back({d.xl_F, sizeof(double) * 4 * (size_t)d.nx});
+  }
+  return v;
+}
+}  // namespace
+
+sc_status sc_checkpoint(sc_ctx *c, void *buf, size_t cap, size_t *size) {
+  if (!c || !c->loaded || !size) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  const int nrep = c->d.nrep;
+  auto regions = state_regions(c);
+  size_t need = sizeof(CkptHeader) + sizeof(int32_t) * nrep;
+  for (auto &r : regions) need += r.bytes;
+  *size = need;
+  if (!buf) return SC_OK;
+  if (cap < need) return fail(c, SC_ERR_INVALID_ARG, "checkpoint needs %zu bytes", need);
+  CKS(readback(c));
+  long long nr = 0;
+  CK(cudaMemcpyAsync(&nr, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  CkptHeader h;
+  std::memset(&h, 0, sizeof(h));
+  std::memcpy(h.magic, "SCB200CK", 8);
+  h.version = 1;
+  h.nd = c->nd;
+  h.prec = c->prec;
+  h.nrep = nrep;
+  h.nf = c->nf;
+  h.ns = c->ns;
+  h.nb = c->nb;
+  h.nx = c->d.nx;
+  h.midstep = c->midstep;
+  h.rbuf = c->rbuf;
+  h.stoch = c->desc.stoch_flag;
+  h.i_step = c->i_step;
+  h.mcount = c->mcount;
+  h.n_rebuilds = nr;
+  char *out = (char *)buf;
+  std::memcpy(out, &h, sizeof(h));
+  out += sizeof(h);
+  for (int r = 0; r < nrep; ++r) {
+    const int32_t pc = c->reps[r].pcap;
+    std::memcpy(out, &pc, sizeof(pc));
+    out += sizeof(pc);
+  }
+  for (auto &r : regions) {
+    CK(cudaMemcpyAsync(out, r.ptr, r.bytes, cudaMemcpyDeviceToHost, c->st));
+    out += r.bytes;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_restore(sc_ctx *c, const void *buf, size_t size) {
+  if (!c || !c->loaded || !buf) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  CkptHeader h;
+  if (size < sizeof(h)) return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
+  std::memcpy(&h, buf, sizeof(h));
+  if (std::memcmp(h.magic, "SCB200CK", 8) != 0 || h.version != 1)
+    return fail(c, SC_ERR_INVALID_ARG, "not a checkpoint of this library");
+  if (h.nd != c->nd || h.prec != c->prec || h.nrep != c->d.nrep || h.nf != c->nf ||
+      h.ns != c->ns || h.nb != c->nb || h.nx != c->d.nx)
+    return fail(c, SC_ERR_INVALID_ARG, "checkpoint of a different system shape");
+  const char *in = (const char *)buf + sizeof(h);
+  const int nrep = h.nrep;
+  c->rbuf = h.rbuf;  // selects the geometry buffer the checkpoint fills
+  if (size < sizeof(h) + sizeof(int32_t) * nrep)
+    return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
+  std::vector<long long> caps(nrep);
+  for (int r = 0; r < nrep; ++r) {
+    int32_t pc;
+    std::memcpy(&pc, in, sizeof(pc));
+    in += sizeof(pc);
+    caps[r] = pc;
+  }
+  CKS(layout_pairs(c, caps));  // the checkpoint's segments
+  auto regions = state_regions(c);
+  size_t need = sizeof(h) + sizeof(int32_t) * nrep;
+  for (auto &r : regions) need += r.bytes;
+  if (size < need) return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
+  for (auto &r : regions) {
+    CK(cudaMemcpyAsync(r.ptr, in, r.bytes, cudaMemcpyHostToDevice, c->st));
+    in += r.bytes;
+  }
+  const long long nr = h.n_rebuilds;
+  CK(cudaMemcpyAsync(c->d.n_rebuilds, &nr, sizeof(long long), cudaMemcpyHostToDevice, c->st));
+  const unsigned long long mc = h.mcount;
+  CK(cudaMemcpyAsync(c->d.mcount, &mc, sizeof(mc), cudaMemcpyHostToDevice, c->st));
+  const unsigned zero = 0;
+  CK(cudaMemcpyAsync(c->d.status, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->st));
+  c->i_step = h.i_step;
+  c->mcount = h.mcount;
+  c->midstep = h.midstep;
+  c->pairs_ready = false;
+  // The FP64 record of mixed precision serves only the geometry getter.
+  if (c->prec != 0) sc::launch_init_geometry(c->k, c->d, 0, 0, c->st, false);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  CKS(sync_pair_count(c));
+  drop_graph(c);
+  return SC_OK;
+}
+
+sc_status sc_set_noise_key(sc_ctx *c, int replica, uint32_t seed) {
+  if (!c || !c->loaded || replica < -1 || replica >= c->d.nrep) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  for (int r = 0; r < c->d.nrep; ++r)
+    if (replica < 0 || r == replica) c->reps[r].seed = seed;
+  return upload_reps(c);
+}
+
 sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32_t *site_b,
                             double k_spring, double k_spring_compress, double rest_length) {
   if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
@@ -1384,7 +1557,7 @@ sc_status sc_get_bond_geometry(sc_ctx *c, double *pos, double *spos, double *u,
   // FP64 geometry of the current positions (buffer 0 of the FP64 records is
   // scratch in mixed precision; in FP64 the read buffer already holds it).
   int buf = c->prec == 0 ? c->rbuf : 0;
-  if (c->prec != 0) sc::launch_init_geometry(c->k, c->d, 0, 0, c->st);
+  if (c->prec != 0) sc::launch_init_geometry(c->k, c->d, 0, 0, c->st, false);
   std::vector<sc::BondGeomF64> g(c->nb);
   CK(cudaMemcpyAsync(g.data(), c->d.g64[buf], sizeof(sc::BondGeomF64) * c->nb,
                      cudaMemcpyDeviceToHost, c->st));

@@ -23,7 +23,7 @@
 namespace sc {
 
 template <int ND>
-__global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec) {
+__global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec, int write_ub) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
   int f = d.bond_fil[b];
@@ -35,9 +35,11 @@ __global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec) {
   }
   bond_from_sites<ND>(d.rep[rep_of_bond(d, b)].hinv, r1, r2, s, u, len);
   store_geom<ND>(d, buf, b, s, u, len, prec);
-  d.ub[0][b] = u[0];
-  d.ub[1][b] = u[1];
-  d.ub[2][b] = u[2];
+  if (write_ub) {
+    d.ub[0][b] = u[0];
+    d.ub[1][b] = u[1];
+    d.ub[2][b] = u[2];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -683,10 +685,11 @@ __global__ void k_soa_to_aos(int n, const T *x, const T *y, const T *z, double *
 static inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 
 void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
-                          int prec, cudaStream_t st) {
+                          int prec, cudaStream_t st, bool write_ub) {
   if (d.nb == 0) return;
-  if (k.n_dim == 3) k_init_geometry<3><<<cdiv(d.nb, 256), 256, 0, st>>>(k, d, buf, prec);
-  else k_init_geometry<2><<<cdiv(d.nb, 256), 256, 0, st>>>(k, d, buf, prec);
+  const int w = write_ub ? 1 : 0;
+  if (k.n_dim == 3) k_init_geometry<3><<<cdiv(d.nb, 256), 256, 0, st>>>(k, d, buf, prec, w);
+  else k_init_geometry<2><<<cdiv(d.nb, 256), 256, 0, st>>>(k, d, buf, prec, w);
 }
 
 int scan_temp_ints(long long n) { return cdiv(n, SCAN_TILE) + 1; }

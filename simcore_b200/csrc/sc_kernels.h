@@ -9,8 +9,11 @@
 
 namespace sc {
 
+// Bond geometry of the current sites (Bond::ReInit) into record buffer buf;
+// write_ub also sets the FP64 bond orientations (loading positions), which
+// the FP64 scratch record of mixed precision must leave alone.
 void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
-                          int prec, cudaStream_t st);
+                          int prec, cudaStream_t st, bool write_ub = true);
 int scan_temp_ints(long long n);
 // Interleaved x, y, z triples into positions and previous positions.
 int launch_aos_to_soa(int n, int nd, const double *aos, const DevState &d, cudaStream_t st);

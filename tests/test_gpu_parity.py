@@ -368,3 +368,96 @@ def test_replicas_mixed_match_single_contexts():
 def _ctx_replicas(system, filaments, sites, replicas, precision="fp64"):
     import simcore_b200 as sc
     return sc.Context(system, filaments, sites, precision=precision, replicas=replicas)
+
+
+def test_checkpoint_restore_continues_bitwise():
+    """A checkpoint taken mid-run (after a midstep, with tethers whose stale
+    odd-step forces are part of the state) restores into a fresh context of
+    the same systems, which then continues bit for bit as the original."""
+    system, fils, sites, (a, b, k, rest) = _workload_E(0.01, seed=6)
+    for prec in ("fp64", "mixed"):
+        ctx = _ctx(system, fils, sites, prec)
+        ctx.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+        ctx.step(3)
+        ctx.step_graph(48)
+        blob = ctx.checkpoint()
+        ctx.step_graph(61)
+        other = _ctx(system, fils, sites, prec)
+        other.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+        other.restore(blob)
+        other.step_graph(61)
+        assert_same(other.sites(), ctx.sites(), "sites")
+        assert_same(other.prev_sites(), ctx.prev_sites(), "prev sites")
+        assert_same(other.pairs(), ctx.pairs(), "pairs")
+        assert_same(other.bond_forces()[0], ctx.bond_forces()[0], "bond forces")
+        assert_same(other.crosslink_forces(), ctx.crosslink_forces(), "tether forces")
+        assert_same(other.dr_tot(), ctx.dr_tot(), "dr_tot")
+        assert other.counters().i_step == ctx.counters().i_step
+        assert other.counters().n_rebuilds == ctx.counters().n_rebuilds
+
+
+def test_checkpoint_of_replicas_and_shape_check():
+    """Replica batches checkpoint and restore per system; a checkpoint does
+    not load into a context of another shape."""
+    import simcore_b200 as sc
+    system, fils, sites, reps = _replica_batch(3, 0.03, seed=4)
+    ctx = _ctx_replicas(system, fils, sites, reps)
+    ctx.step_graph(41)
+    blob = ctx.checkpoint()
+    ctx.step_graph(40)
+    other = _ctx_replicas(system, fils, sites, reps)
+    other.restore(blob)
+    other.step_graph(40)
+    assert_same(other.sites(), ctx.sites(), "sites")
+    assert (other.replica_counters()[0] == ctx.replica_counters()[0]).all()
+    s2, f2, x2 = _workload("A", 0.1, seed=1)
+    wrong = _ctx(s2, f2, x2)
+    with pytest.raises(sc.ScError):
+        wrong.restore(blob)
+
+
+def test_noise_key():
+    """sc_set_noise_key before the first step gives the stream of a context
+    created with that seed."""
+    system, fils, sites = _workload("B", 0.02, seed=12)
+    a = _ctx(dict(system, seed=5), fils, sites)
+    a.set_noise_key(77)
+    b = _ctx(dict(system, seed=77), fils, sites)
+    a.step_graph(20)
+    b.step_graph(20)
+    assert_same(a.sites(), b.sites(), "sites")
+
+
+def test_non_finite_positions_are_reported():
+    """A NaN position fails the next step with SC_ERR_NAN (device status
+    word), without faulting: binning clamps the cell and flags it."""
+    import simcore_b200 as sc
+    system, fils, sites = _workload("B", 0.02, seed=13)
+    ctx = _ctx(system, fils, sites, "mixed")
+    bad = sites.copy()
+    bad[5, 0] = np.nan
+    ctx.set_sites(bad)
+    with pytest.raises(sc.ScError) as e:
+        ctx.step(4)
+        ctx.synchronize()
+    assert e.value.code == 3
+
+
+def test_getters_leave_the_trajectory_alone():
+    """Reading state (geometry, forces, pairs, cells, checkpoint) between
+    steps changes nothing in the mixed path, whose bond orientations come
+    from the fast integrator."""
+    system, fils, sites = _workload("B", 0.03, seed=14)
+    a = _ctx(system, fils, sites, "mixed")
+    b = _ctx(system, fils, sites, "mixed")
+    for n in (7, 30):
+        a.step_graph(n)
+        b.step_graph(n)
+        a.bond_geometry()
+        a.bond_forces()
+        a.pairs()
+        a.bond_cells()
+        a.checkpoint()
+    a.step_graph(21)
+    b.step_graph(21)
+    assert_same(a.sites(), b.sites(), "sites")
