@@ -138,6 +138,21 @@ sc_status sc_restore(sc_ctx *ctx, const void *buf, size_t size);
 /* Noise key (Philox key word 0) of system `replica`, or of every system for
  * -1; the draws continue from the current noise counter. */
 sc_status sc_set_noise_key(sc_ctx *ctx, int replica, uint32_t seed);
+/* Reference-format output: the filament species' spec and posit files
+ * (<run_name>_filament_<species_name>.spec / .posit; with several systems
+ * <run_name>_rNNN_... per system), with the reference's headers (n_steps,
+ * cadence, delta) and frames (spec: per filament diameter, length, bond
+ * length, site count, site positions, bending stiffness, polymerisation
+ * state; posit: average position, its scaled image, average orientation,
+ * diameter, length).  A cadence of 0 skips that file.  sc_output_write
+ * writes the frames due at the current step (i_step % cadence == 0), as
+ * OutputManager::WriteOutputs does after every step: the state is
+ * snapshotted on the device, copied on a separate stream while the run
+ * continues, and written to the file at the next call or at close. */
+sc_status sc_output_open(sc_ctx *ctx, const char *run_name, const char *species_name,
+                         int n_steps, int n_posit, int n_spec);
+sc_status sc_output_write(sc_ctx *ctx);
+sc_status sc_output_close(sc_ctx *ctx);
 /* Per-system rebuild counts and current pair counts (n_replicas entries
  * each; either pointer may be NULL). */
 sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);

@@ -35,7 +35,7 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_pair_forces_noalloc", "sc_insert_filaments", "sc_add_crosslinks",
             "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune",
             "sc_add_replicas", "sc_get_replica_counters", "sc_checkpoint", "sc_restore",
-            "sc_set_noise_key"]
+            "sc_set_noise_key", "sc_output_open", "sc_output_write", "sc_output_close"]
 
 
 class ScError(RuntimeError):
@@ -330,6 +330,19 @@ class Context:
 
     def set_noise_key(self, seed, replica=-1):
         self._check(lib.sc_set_noise_key(self.h, ctypes.c_int(replica), ctypes.c_uint32(seed)))
+
+    def output_open(self, run_name, n_steps, n_posit=0, n_spec=0, species_name="filament"):
+        """Reference-format spec/posit files (<run>_filament_<species>.spec /
+        .posit); write frames with output_write() after every step."""
+        self._check(lib.sc_output_open(self.h, run_name.encode(), species_name.encode(),
+                                       ctypes.c_int(n_steps), ctypes.c_int(n_posit),
+                                       ctypes.c_int(n_spec)))
+
+    def output_write(self):
+        self._check(lib.sc_output_write(self.h))
+
+    def output_close(self):
+        self._check(lib.sc_output_close(self.h))
 
     def replica_counters(self):
         """(rebuilds, pairs) per system."""

@@ -33,6 +33,21 @@ struct sc_ctx {
   std::vector<int> site_off;
   std::vector<int> bond_fil;
   std::vector<int> fil_rep;        // system of each filament
+  // per filament, for output files: diameter, length, bond length, lp
+  std::vector<double> fil_diam, fil_len, fil_bl, fil_lp;
+
+  // reference-format output (sc_output_*): one spec and one posit file per
+  // system, frames snapshotted on the device and copied on out_st
+  struct Output {
+    bool open = false;
+    int n_steps = 0, n_posit = 0, n_spec = 0;
+    std::vector<FILE *> spec, posit;   // per system (null when not written)
+    cudaStream_t out_st = nullptr;
+    cudaEvent_t taken = nullptr, copied = nullptr;
+    double *d_snap = nullptr;          // positions (3 ns) then averages (9 nf)
+    double *h_snap = nullptr;          // pinned copy
+    bool pending_spec = false, pending_posit = false;
+  } out;
   bool loaded = false;
 
   // systems (replicas): host copy of the device table
@@ -547,6 +562,47 @@ sc_status copy_soa3(sc_ctx *c, T *const *src, int n, double *xyz) {
   return SC_OK;
 }
 
+template <class T>
+void put(FILE *f, const T &v) {
+  std::fwrite(&v, sizeof(T), 1, f);
+}
+
+// Writes the frame whose copy has completed.
+sc_status output_flush(sc_ctx *c) {
+  sc_ctx::Output &o = c->out;
+  if (!o.pending_spec && !o.pending_posit) return SC_OK;
+  CK(cudaEventSynchronize(o.copied));
+  const double *pos = o.h_snap;
+  const double *avg = o.h_snap + 3 * (size_t)c->ns;
+  for (size_t r = 0; r < c->reps.size(); ++r) {
+    const sc::ReplicaConst &R = c->reps[r];
+    if (o.pending_spec && o.spec[r]) {
+      FILE *f = o.spec[r];
+      put(f, (int32_t)R.nf);
+      for (int fi = R.f0; fi < R.f0 + R.nf; ++fi) {
+        const int n = c->site_off[fi + 1] - c->site_off[fi];
+        put(f, c->fil_diam[fi]);
+        put(f, c->fil_len[fi]);
+        put(f, c->fil_bl[fi]);
+        put(f, (int32_t)n);
+        std::fwrite(pos + 3 * (size_t)c->site_off[fi], sizeof(double), 3 * (size_t)n, f);
+        put(f, c->fil_lp[fi]);          // bending_stiffness_ = persistence length
+        put(f, (unsigned char)0);       // poly_state::grow
+      }
+    }
+    if (o.pending_posit && o.posit[r]) {
+      FILE *f = o.posit[r];
+      put(f, (int32_t)R.nf);
+      for (int fi = R.f0; fi < R.f0 + R.nf; ++fi) {
+        std::fwrite(avg + 9 * (size_t)fi, sizeof(double), 9, f);  // pos, scaled pos, u
+        put(f, c->fil_diam[fi]);
+        put(f, c->fil_len[fi]);
+      }
+    }
+  }
+  o.pending_spec = o.pending_posit = false;
+  return SC_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -625,6 +681,7 @@ sc_status sc_destroy(sc_ctx *c) {
   if (!c) return SC_ERR_INVALID_ARG;
   cudaSetDevice(c->desc.device);
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->out.open) sc_output_close(c);
   drop_graph(c);
   for (void *p : c->allocs) cudaFree(p);
   if (c->hb) cudaFreeHost(c->hb);
@@ -679,6 +736,10 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
       return fail(c, SC_ERR_INVALID_ARG,
                   "filament %d: min_bond_length and diameter are species-wide", f);
     filament_length(p[f], &len[f], &nbf[f]);
+    c->fil_diam.push_back(p[f].diameter);
+    c->fil_len.push_back(len[f]);
+    c->fil_bl.push_back(len[f] / nbf[f]);
+    c->fil_lp.push_back(p[f].persistence_length);
     ns += nbf[f] + 1;
     max_ns = std::max(max_ns, nbf[f] + 1);
   }
@@ -1476,6 +1537,114 @@ sc_status sc_set_noise_key(sc_ctx *c, int replica, uint32_t seed) {
   for (int r = 0; r < c->d.nrep; ++r)
     if (replica < 0 || r == replica) c->reps[r].seed = seed;
   return upload_reps(c);
+}
+
+// ---------------------------------------------------------------------------
+// Reference-format output files: the filament species' spec and posit files
+// (SpeciesBase::InitSpecFile / InitPositFile, src/species_base.cpp:13-70;
+// Species::WriteSpecs / WritePosits, include/simcore/species.hpp:221-233;
+// Mesh::WriteSpec, src/mesh.cpp:482-492; Filament::WriteSpec / WritePosit,
+// src/filament.cpp:1314-1361), at the cadence of OutputManager::WriteOutputs
+// (include/simcore/output_manager.hpp:112-127).
+
+
+sc_status sc_output_open(sc_ctx *c, const char *run_name, const char *species_name, int n_steps,
+                         int n_posit, int n_spec) {
+  if (!c || !c->loaded || !run_name || !species_name || n_steps < 0 || n_posit < 0 ||
+      n_spec < 0)
+    return SC_ERR_INVALID_ARG;
+  if (c->out.open) return fail(c, SC_ERR_INVALID_ARG, "output already open");
+  CK(cudaSetDevice(c->desc.device));
+  sc_ctx::Output &o = c->out;
+  o.n_steps = n_steps;
+  o.n_posit = n_posit;
+  o.n_spec = n_spec;
+  const size_t nrep = c->reps.size();
+  o.spec.assign(nrep, nullptr);
+  o.posit.assign(nrep, nullptr);
+  for (size_t r = 0; r < nrep; ++r) {
+    std::string run = run_name;
+    if (nrep > 1) {
+      char sfx[16];
+      std::snprintf(sfx, sizeof(sfx), "_r%03zu", r);
+      run += sfx;
+    }
+    const std::string base = run + "_filament_" + species_name;
+    for (int kind = 0; kind < 2; ++kind) {
+      const int cadence = kind == 0 ? n_spec : n_posit;
+      if (cadence <= 0) continue;
+      const std::string name = base + (kind == 0 ? ".spec" : ".posit");
+      FILE *f = std::fopen(name.c_str(), "wb");
+      if (!f) return fail(c, SC_ERR_INVALID_ARG, "cannot open %s", name.c_str());
+      put(f, (int32_t)n_steps);
+      put(f, (int32_t)cadence);
+      put(f, c->desc.delta);
+      (kind == 0 ? o.spec : o.posit)[r] = f;
+    }
+  }
+  const size_t doubles = 3 * (size_t)c->ns + 9 * (size_t)c->nf;
+  CKS(dalloc(c, &o.d_snap, doubles));
+  if (cudaHostAlloc((void **)&o.h_snap, sizeof(double) * doubles, cudaHostAllocDefault) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return fail(c, SC_ERR_OOM, "pinned allocation failed");
+  }
+  CK(cudaStreamCreateWithFlags(&o.out_st, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&o.taken, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&o.copied, cudaEventDisableTiming));
+  o.open = true;
+  return SC_OK;
+}
+
+sc_status sc_output_write(sc_ctx *c) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  sc_ctx::Output &o = c->out;
+  if (!o.open) return fail(c, SC_ERR_INVALID_ARG, "output not open");
+  CK(cudaSetDevice(c->desc.device));
+  const bool spec = o.n_spec > 0 && c->i_step % o.n_spec == 0;
+  const bool posit = o.n_posit > 0 && c->i_step % o.n_posit == 0;
+  if (!spec && !posit) return SC_OK;
+  CKS(output_flush(c));  // the previous frame, whose copy overlapped the steps since
+  // Snapshot on the simulation stream, copy on the output stream.
+  if (spec)
+    c->launches += sc::launch_soa_to_aos(c->ns, c->d.r[0], c->d.r[1], c->d.r[2], o.d_snap, c->st);
+  if (posit)
+    c->launches += sc::launch_filament_averages(c->k, c->d, o.d_snap + 3 * (size_t)c->ns, c->st);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(o.taken, c->st));
+  CK(cudaStreamWaitEvent(o.out_st, o.taken, 0));
+  if (spec)
+    CK(cudaMemcpyAsync(o.h_snap, o.d_snap, sizeof(double) * 3 * (size_t)c->ns,
+                       cudaMemcpyDeviceToHost, o.out_st));
+  if (posit)
+    CK(cudaMemcpyAsync(o.h_snap + 3 * (size_t)c->ns, o.d_snap + 3 * (size_t)c->ns,
+                       sizeof(double) * 9 * (size_t)c->nf, cudaMemcpyDeviceToHost, o.out_st));
+  CK(cudaEventRecord(o.copied, o.out_st));
+  o.pending_spec = spec;
+  o.pending_posit = posit;
+  return SC_OK;
+}
+
+sc_status sc_output_close(sc_ctx *c) {
+  if (!c) return SC_ERR_INVALID_ARG;
+  sc_ctx::Output &o = c->out;
+  if (!o.open) return SC_OK;
+  cudaSetDevice(c->desc.device);
+  sc_status st = output_flush(c);
+  for (FILE *f : o.spec)
+    if (f) std::fclose(f);
+  for (FILE *f : o.posit)
+    if (f) std::fclose(f);
+  o.spec.clear();
+  o.posit.clear();
+  if (o.out_st) cudaStreamSynchronize(o.out_st);
+  if (o.h_snap) cudaFreeHost(o.h_snap);
+  if (o.d_snap) dfree(c, o.d_snap);
+  if (o.taken) cudaEventDestroy(o.taken);
+  if (o.copied) cudaEventDestroy(o.copied);
+  if (o.out_st) cudaStreamDestroy(o.out_st);
+  o = sc_ctx::Output{};
+  return st;
 }
 
 sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32_t *site_b,

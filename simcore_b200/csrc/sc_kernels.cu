@@ -679,6 +679,50 @@ __global__ void k_soa_to_aos(int n, const T *x, const T *y, const T *z, double *
   aos[3 * (size_t)i + 2] = (double)z[i];
 }
 
+// Per filament: average site position, its scaled (periodic) image and the
+// normalised average site orientation, 9 doubles, in the reference's
+// summation order (Mesh::GetAvgPosition / GetAvgOrientation,
+// src/mesh.cpp:581-608, then Object::UpdatePeriodic).  Site orientations are
+// their bonds' (the last site's is the last bond's).
+template <int ND>
+__global__ void k_filament_averages(SysConst k, DevState d, double *out) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const FilConst &fc = d.fil[f];
+  double ap[3] = {0.0, 0.0, 0.0}, au[3] = {0.0, 0.0, 0.0};
+  const int b0 = fc.site0 - f;
+  for (int j = 0; j < fc.n; ++j) {
+    const int b = b0 + (j < fc.n - 1 ? j : fc.n - 2);
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      ap[i] += d.r[i][fc.site0 + j];
+      au[i] += d.ub[i][b];
+    }
+  }
+  double mag = 0.0;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) mag += au[i] * au[i];
+  mag = sqrt(mag);
+#pragma unroll
+  for (int i = 0; i < ND; ++i) au[i] /= mag;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) ap[i] /= fc.n;
+  const ReplicaConst &R = d.rep[fc.rep];
+  double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+#pragma unroll
+    for (int j = 0; j < ND; ++j) s[i] += R.hinv[ND * i + j] * ap[j];
+    s[i] -= nint(s[i]);
+  }
+  double *o = out + 9 * (size_t)f;
+  for (int i = 0; i < 3; ++i) {
+    o[i] = ap[i];
+    o[3 + i] = s[i];
+    o[6 + i] = au[i];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers.
 
@@ -693,6 +737,13 @@ void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
 }
 
 int scan_temp_ints(long long n) { return cdiv(n, SCAN_TILE) + 1; }
+
+int launch_filament_averages(const SysConst &k, const DevState &d, double *out, cudaStream_t st) {
+  if (d.nf <= 0) return 0;
+  if (k.n_dim == 3) k_filament_averages<3><<<cdiv(d.nf, 128), 128, 0, st>>>(k, d, out);
+  else k_filament_averages<2><<<cdiv(d.nf, 128), 128, 0, st>>>(k, d, out);
+  return 1;
+}
 
 int launch_aos_to_soa(int n, int nd, const double *aos, const DevState &d, cudaStream_t st) {
   if (n <= 0) return 0;

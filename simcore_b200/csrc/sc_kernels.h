@@ -15,6 +15,9 @@ namespace sc {
 void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
                           int prec, cudaStream_t st, bool write_ub = true);
 int scan_temp_ints(long long n);
+// Per filament average position, its scaled image and average orientation
+// (9 doubles each).
+int launch_filament_averages(const SysConst &k, const DevState &d, double *out, cudaStream_t st);
 // Interleaved x, y, z triples into positions and previous positions.
 int launch_aos_to_soa(int n, int nd, const double *aos, const DevState &d, cudaStream_t st);
 // Component arrays into interleaved triples.

@@ -461,3 +461,55 @@ def test_getters_leave_the_trajectory_alone():
     a.step_graph(21)
     b.step_graph(21)
     assert_same(a.sites(), b.sites(), "sites")
+
+
+def test_reference_format_output(tmp_path):
+    """Spec and posit files in the reference's format, at its cadence: every
+    spec frame holds the sites of that step bit for bit; every posit frame the
+    average position (reference summation order), its periodic image and the
+    normalised average orientation."""
+    import simcore_b200 as sc
+    from ref_formats import read_posit, read_spec
+    system, fils, sites = _workload("B", 0.01, seed=15)
+    ctx = _ctx(system, fils, sites)
+    run = str(tmp_path / "gpurun")
+    ctx.output_open(run, n_steps=60, n_posit=10, n_spec=20)
+    expect_sites, expect_u = [], []
+    for i in range(61):
+        if i:
+            ctx.step(1)
+        ctx.output_write()
+        if i % 20 == 0:
+            expect_sites.append(ctx.sites())
+        if i % 10 == 0:
+            expect_u.append((ctx.sites(), ctx.bond_geometry()[2]))
+    ctx.output_close()
+    head, frames = read_spec(run + "_filament_filament.spec")
+    assert head == (60, 20, system["delta"]) and len(frames) == 4
+    ns = np.array([sc.filament_n_bonds(f) + 1 for f in fils])
+    off = np.concatenate([[0], np.cumsum(ns)])
+    for fr, xyz in zip(frames, expect_sites):
+        assert len(fr) == len(fils)
+        for k, rec in enumerate(fr):
+            assert_same(rec["sites"], xyz[off[k]:off[k + 1]], "spec sites")
+            assert rec["bending_stiffness"] == fils[k]["persistence_length"] and rec["poly"] == 0
+    head, pframes = read_posit(run + "_filament_filament.posit")
+    assert head == (60, 10, system["delta"]) and len(pframes) == 7
+    R = system["system_radius"]
+    for rec, (xyz, u) in zip(pframes, expect_u):
+        for k in range(len(fils)):
+            p = np.zeros(3)
+            for s in xyz[off[k]:off[k + 1]]:
+                p = p + s
+            p = p / ns[k]
+            assert_same(rec[k, 0:3], p, "posit average position")
+            bu = u[off[k] - k:off[k + 1] - k - 1]
+            a = np.zeros(3)
+            for v in list(bu) + [bu[-1]]:
+                a = a + v
+            a = a / np.sqrt((a * a).sum())
+            assert np.abs(rec[k, 6:9] - a).max() < 1e-14
+            s_img = p / (2 * R)
+            s_img -= np.where(s_img < 0, np.ceil(s_img - 0.5), np.floor(s_img + 0.5))
+            assert np.abs(rec[k, 3:6] - s_img).max() < 1e-14
+            assert rec[k, 9] == fils[k]["diameter"] and rec[k, 10] == fils[k]["length"]
