@@ -153,6 +153,22 @@ sc_status sc_output_open(sc_ctx *ctx, const char *run_name, const char *species_
                          int n_steps, int n_posit, int n_spec);
 sc_status sc_output_write(sc_ctx *ctx);
 sc_status sc_output_close(sc_ctx *ctx);
+/* Filament analyses on the device, per system.  sc_analysis_sample adds one
+ * sample of FilamentSpecies::RunMse2eAnalysis (|head - tail|^2 and its square
+ * over the filaments) and RunThetaAnalysis (per joint index i, the histogram
+ * of cos(theta_i) = u_i . u_{i+1} in n_bins bins, bin = floor((1 + cos)
+ * (n_bins / 2)) clamped to the range; src/filament_species.cpp:569-610).
+ * sc_analysis_results gives, per system, the mean-square end-to-end distance
+ * and its standard error as FinalizeMse2eAnalysis computes them, the sample
+ * count, the joint count per filament of the histograms (max_joints) and the
+ * histograms (n_replicas x max_joints x n_bins).  sc_global_order gives the
+ * polar order vector (3) and nematic order tensor (9) per system
+ * (RunGlobalOrderAnalysis with Filament::GetPolarOrder/GetNematicOrder).
+ * Bond orientations are the current ones. */
+sc_status sc_analysis_sample(sc_ctx *ctx, int n_bins);
+sc_status sc_analysis_results(sc_ctx *ctx, double *mse2e, double *mse2e_err, int64_t *n_samples,
+                              int32_t *max_joints, int64_t *theta_hist);
+sc_status sc_global_order(sc_ctx *ctx, double *polar, double *nematic);
 /* Per-system rebuild counts and current pair counts (n_replicas entries
  * each; either pointer may be NULL). */
 sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);

@@ -35,7 +35,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_pair_forces_noalloc", "sc_insert_filaments", "sc_add_crosslinks",
             "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune",
             "sc_add_replicas", "sc_get_replica_counters", "sc_checkpoint", "sc_restore",
-            "sc_set_noise_key", "sc_output_open", "sc_output_write", "sc_output_close"]
+            "sc_set_noise_key", "sc_output_open", "sc_output_write", "sc_output_close",
+            "sc_analysis_sample", "sc_analysis_results", "sc_global_order"]
 
 
 class ScError(RuntimeError):
@@ -343,6 +344,30 @@ class Context:
 
     def output_close(self):
         self._check(lib.sc_output_close(self.h))
+
+    def analysis_sample(self, n_bins=100):
+        self._check(lib.sc_analysis_sample(self.h, ctypes.c_int(n_bins)))
+
+    def analysis_results(self, n_bins=100):
+        """(mse2e, mse2e_err, n_samples, theta_hist[nrep, max_joints, n_bins])."""
+        R = self.n_replicas
+        m = np.zeros(R)
+        e = np.zeros(R)
+        ns = ctypes.c_int64()
+        mj = ctypes.c_int32()
+        self._check(lib.sc_analysis_results(self.h, None, None, ctypes.byref(ns),
+                                            ctypes.byref(mj), None))
+        hist = np.zeros((R, max(mj.value, 1), n_bins), dtype=np.int64)
+        self._check(lib.sc_analysis_results(self.h, _p(m), _p(e), ctypes.byref(ns),
+                                            ctypes.byref(mj), _p(hist)))
+        return m, e, ns.value, hist
+
+    def global_order(self):
+        R = self.n_replicas
+        p = np.zeros((R, 3))
+        q = np.zeros((R, 9))
+        self._check(lib.sc_global_order(self.h, _p(p), _p(q)))
+        return p, q
 
     def replica_counters(self):
         """(rebuilds, pairs) per system."""

@@ -36,6 +36,15 @@ struct sc_ctx {
   // per filament, for output files: diameter, length, bond length, lp
   std::vector<double> fil_diam, fil_len, fil_bl, fil_lp;
 
+  // analyses (sc_analysis_*): device accumulators
+  struct Analysis {
+    int n_bins = 0, max_joints = 0;
+    long long n_samples = 0;
+    double *acc = nullptr;     // 2 per system
+    int *hist = nullptr;       // nrep x max_joints x n_bins
+    double *order = nullptr;   // 12 per system
+  } an;
+
   // reference-format output (sc_output_*): one spec and one posit file per
   // system, frames snapshotted on the device and copied on out_st
   struct Output {
@@ -1645,6 +1654,78 @@ sc_status sc_output_close(sc_ctx *c) {
   if (o.out_st) cudaStreamDestroy(o.out_st);
   o = sc_ctx::Output{};
   return st;
+}
+
+// ---------------------------------------------------------------------------
+// Filament analyses on the device (FilamentSpecies::RunAnalysis family).
+
+sc_status sc_analysis_sample(sc_ctx *c, int n_bins) {
+  if (!c || !c->loaded || n_bins < 1) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  sc_ctx::Analysis &a = c->an;
+  if (a.n_bins && a.n_bins != n_bins)
+    return fail(c, SC_ERR_INVALID_ARG, "histogram bins changed between samples");
+  if (!a.acc) {
+    int maxn = 0;
+    for (int f = 0; f < c->nf; ++f) maxn = std::max(maxn, c->site_off[f + 1] - c->site_off[f]);
+    a.n_bins = n_bins;
+    a.max_joints = std::max(1, maxn - 2);
+    const size_t nrep = c->reps.size();
+    CKS(dalloc(c, &a.acc, 2 * nrep));
+    CK(cudaMemsetAsync(a.acc, 0, sizeof(double) * 2 * nrep, c->st));
+    CKS(dalloc(c, &a.hist, nrep * a.max_joints * (size_t)n_bins));
+    CK(cudaMemsetAsync(a.hist, 0, sizeof(int) * nrep * a.max_joints * (size_t)n_bins, c->st));
+  }
+  c->launches += sc::launch_analysis_sample(c->k, c->d, a.n_bins, a.max_joints, a.acc, a.hist, c->st);
+  CK(cudaGetLastError());
+  a.n_samples++;
+  return SC_OK;
+}
+
+sc_status sc_analysis_results(sc_ctx *c, double *mse2e, double *mse2e_err, int64_t *n_samples,
+                              int32_t *max_joints, int64_t *theta_hist) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  sc_ctx::Analysis &a = c->an;
+  const int nrep = (int)c->reps.size();
+  if (n_samples) *n_samples = a.n_samples;
+  if (max_joints) *max_joints = a.max_joints;
+  if (!a.acc || a.n_samples == 0) return SC_OK;
+  std::vector<double> acc(2 * (size_t)nrep);
+  CK(cudaMemcpyAsync(acc.data(), a.acc, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost, c->st));
+  std::vector<int> hist((size_t)nrep * a.max_joints * a.n_bins);
+  CK(cudaMemcpyAsync(hist.data(), a.hist, sizeof(int) * hist.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  // FilamentSpecies::FinalizeMse2eAnalysis (src/filament_species.cpp:686-698).
+  for (int r = 0; r < nrep; ++r) {
+    const double num = c->reps[r].nf, ns = (double)a.n_samples;
+    const double m = acc[2 * r] / (ns * num), m2 = acc[2 * r + 1] / (ns * num);
+    if (mse2e) mse2e[r] = m;
+    if (mse2e_err) mse2e_err[r] = std::sqrt((m2 - m * m) / (num * ns));
+  }
+  if (theta_hist)
+    for (size_t i = 0; i < hist.size(); ++i) theta_hist[i] = hist[i];
+  return SC_OK;
+}
+
+sc_status sc_global_order(sc_ctx *c, double *polar, double *nematic) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  sc_ctx::Analysis &a = c->an;
+  const int nrep = (int)c->reps.size();
+  if (!a.order) CKS(dalloc(c, &a.order, 12 * (size_t)nrep));
+  c->launches += sc::launch_global_order(c->k, c->d, a.order, c->st);
+  CK(cudaGetLastError());
+  std::vector<double> o(12 * (size_t)nrep);
+  CK(cudaMemcpyAsync(o.data(), a.order, sizeof(double) * o.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int r = 0; r < nrep; ++r) {
+    for (int i = 0; i < 3; ++i)
+      if (polar) polar[3 * (size_t)r + i] = o[12 * (size_t)r + i];
+    for (int i = 0; i < 9; ++i)
+      if (nematic) nematic[9 * (size_t)r + i] = o[12 * (size_t)r + 3 + i];
+  }
+  return SC_OK;
 }
 
 sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32_t *site_b,

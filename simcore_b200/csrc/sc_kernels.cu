@@ -724,6 +724,102 @@ __global__ void k_filament_averages(SysConst k, DevState d, double *out) {
 }
 
 // ---------------------------------------------------------------------------
+// Filament analyses, one block per system, deterministic reduction order.
+
+// Block sum of v (blockDim.x == 256) into thread 0.
+__device__ __forceinline__ double block_sum256(double v, double *tmp) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) tmp[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < 8; ++w) t += tmp[w];
+  __syncthreads();
+  return t;
+}
+
+// FilamentSpecies::RunMse2eAnalysis (src/filament_species.cpp:569-592):
+// |head - tail|^2 and its square, summed over a system's filaments into
+// acc[2 r]; and RunThetaAnalysis (:594-610): the histogram of each joint's
+// cos(theta) = u_i . u_{i+1} into hist[(r max_joints + i) n_bins + bin].
+template <int ND>
+__global__ void __launch_bounds__(256) k_analysis_sample(DevState d, int n_bins, int max_joints,
+                                                         double *acc, int *hist) {
+  __shared__ double tmp[8];
+  const int r = blockIdx.x;
+  const ReplicaConst &R = d.rep[r];
+  double m = 0.0, m2 = 0.0;
+  for (int f = R.f0 + threadIdx.x; f < R.f0 + R.nf; f += blockDim.x) {
+    const FilConst &fc = d.fil[f];
+    const int tail = fc.site0, head = fc.site0 + fc.n - 1;
+    double e = 0.0;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      const double t = d.r[i][head] - d.r[i][tail];
+      e += t * t;
+    }
+    m += e;
+    m2 += e * e;
+    const int b0 = fc.site0 - f;
+    for (int j = 0; j < fc.n - 2 && j < max_joints; ++j) {
+      double c = 0.0;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) c += d.ub[i][b0 + j] * d.ub[i][b0 + j + 1];
+      int bin = (int)floor((1 + c) * (n_bins / 2));
+      if (bin >= n_bins) bin = n_bins - 1;
+      if (bin < 0) bin = 0;
+      atomicAdd(&hist[((size_t)r * max_joints + j) * n_bins + bin], 1);
+    }
+  }
+  m = block_sum256(m, tmp);
+  m2 = block_sum256(m2, tmp);
+  if (threadIdx.x == 0) {
+    acc[2 * r] += m;
+    acc[2 * r + 1] += m2;
+  }
+}
+
+// FilamentSpecies::RunGlobalOrderAnalysis (src/filament_species.cpp:486-535)
+// with Filament::GetPolarOrder / GetNematicOrder (src/filament.cpp:488-516):
+// per system, the mean over filaments of the mean bond orientation (3) and
+// of the bond nematic tensor 2 u u - I (9, n_dim stride 3).
+template <int ND>
+__global__ void __launch_bounds__(256) k_global_order(DevState d, double *out) {
+  __shared__ double tmp[8];
+  const int r = blockIdx.x;
+  const ReplicaConst &R = d.rep[r];
+  double acc[12];
+#pragma unroll
+  for (int q = 0; q < 12; ++q) acc[q] = 0.0;
+  for (int f = R.f0 + threadIdx.x; f < R.f0 + R.nf; f += blockDim.x) {
+    const FilConst &fc = d.fil[f];
+    const int b0 = fc.site0 - f, nbf = fc.n - 1;
+    double p[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < nbf; ++j) {
+      double u[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        u[i] = d.ub[i][b0 + j];
+        p[i] += u[i];
+      }
+#pragma unroll
+      for (int i = 0; i < ND; ++i)
+#pragma unroll
+        for (int k2 = 0; k2 < ND; ++k2)
+          acc[3 + 3 * i + k2] += (i == k2 ? 2 * u[i] * u[k2] - 1 : 2 * u[i] * u[k2]) / nbf;
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i) acc[i] += p[i] / nbf;
+  }
+  double *o = out + 12 * (size_t)r;
+  for (int q = 0; q < 12; ++q) {
+    const double t = block_sum256(acc[q], tmp);
+    if (threadIdx.x == 0) o[q] = t / R.nf;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers.
 
 static inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
@@ -737,6 +833,19 @@ void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
 }
 
 int scan_temp_ints(long long n) { return cdiv(n, SCAN_TILE) + 1; }
+
+int launch_analysis_sample(const SysConst &k, const DevState &d, int n_bins, int max_joints,
+                           double *acc, int *hist, cudaStream_t st) {
+  if (k.n_dim == 3) k_analysis_sample<3><<<d.nrep, 256, 0, st>>>(d, n_bins, max_joints, acc, hist);
+  else k_analysis_sample<2><<<d.nrep, 256, 0, st>>>(d, n_bins, max_joints, acc, hist);
+  return 1;
+}
+
+int launch_global_order(const SysConst &k, const DevState &d, double *out, cudaStream_t st) {
+  if (k.n_dim == 3) k_global_order<3><<<d.nrep, 256, 0, st>>>(d, out);
+  else k_global_order<2><<<d.nrep, 256, 0, st>>>(d, out);
+  return 1;
+}
 
 int launch_filament_averages(const SysConst &k, const DevState &d, double *out, cudaStream_t st) {
   if (d.nf <= 0) return 0;

@@ -15,6 +15,11 @@ namespace sc {
 void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
                           int prec, cudaStream_t st, bool write_ub = true);
 int scan_temp_ints(long long n);
+// Analyses per system: end-to-end sums and joint-angle histograms
+// (accumulated), polar and nematic order (12 doubles per system).
+int launch_analysis_sample(const SysConst &k, const DevState &d, int n_bins, int max_joints,
+                           double *acc, int *hist, cudaStream_t st);
+int launch_global_order(const SysConst &k, const DevState &d, double *out, cudaStream_t st);
 // Per filament average position, its scaled image and average orientation
 // (9 doubles each).
 int launch_filament_averages(const SysConst &k, const DevState &d, double *out, cudaStream_t st);

@@ -513,3 +513,55 @@ def test_reference_format_output(tmp_path):
             s_img -= np.where(s_img < 0, np.ceil(s_img - 0.5), np.floor(s_img + 0.5))
             assert np.abs(rec[k, 3:6] - s_img).max() < 1e-14
             assert rec[k, 9] == fils[k]["diameter"] and rec[k, 10] == fils[k]["length"]
+
+
+def test_device_analyses_match_host():
+    """On-device analyses of three independent 2D systems against the same
+    quantities computed on the host from the sites and bond orientations:
+    mean-square end-to-end distance and its standard error over samples,
+    joint-angle histograms (exact counts), polar and nematic order."""
+    import simcore_b200 as sc
+    system, fils, sites, reps = _replica_batch(3, 0.03, seed=5)
+    ctx = _ctx_replicas(system, fils, sites, reps)
+    nb_bins = 50
+    ns = np.array([sc.filament_n_bonds(f) + 1 for f in fils])
+    off = np.concatenate([[0], np.cumsum(ns)])
+    rep_of = np.repeat(np.arange(len(reps)), [r["n_filaments"] for r in reps])
+    R = len(reps)
+    m1, m2 = np.zeros(R), np.zeros(R)
+    hist = np.zeros((R, ns.max() - 2, nb_bins), dtype=np.int64)
+    for sample in range(5):
+        ctx.step_graph(10)
+        ctx.analysis_sample(nb_bins)
+        xyz = ctx.sites()
+        u = ctx.bond_geometry()[2]
+        for f in range(len(fils)):
+            p = xyz[off[f]:off[f + 1]]
+            t = p[-1] - p[0]
+            e = t[0] * t[0] + t[1] * t[1]
+            m1[rep_of[f]] += e
+            m2[rep_of[f]] += e * e
+            bu = u[off[f] - f:off[f + 1] - f - 1]
+            for j in range(len(bu) - 1):
+                c = bu[j, 0] * bu[j + 1, 0] + bu[j, 1] * bu[j + 1, 1]
+                b = min(max(int(np.floor((1 + c) * (nb_bins // 2))), 0), nb_bins - 1)
+                hist[rep_of[f], j, b] += 1
+    mse, err, n, h = ctx.analysis_results(nb_bins)
+    assert n == 5
+    num = np.array([r["n_filaments"] for r in reps], dtype=float)
+    want = m1 / (5 * num)
+    want_err = np.sqrt((m2 / (5 * num) - want * want) / (num * 5))
+    assert np.allclose(mse, want, rtol=1e-12) and np.allclose(err, want_err, rtol=1e-9)
+    assert (h == hist).all()
+    polar, nem = ctx.global_order()
+    u = ctx.bond_geometry()[2]
+    for r in range(R):
+        fs = np.where(rep_of == r)[0]
+        pv = np.zeros(3)
+        q = np.zeros((3, 3))
+        for f in fs:
+            bu = u[off[f] - f:off[f + 1] - f - 1][:, :2]
+            pv[:2] += bu.mean(0)
+            q[:2, :2] += (2 * np.einsum("bi,bj->ij", bu, bu) - len(bu) * np.eye(2)) / len(bu)
+        assert np.allclose(polar[r], pv / len(fs), atol=1e-12)
+        assert np.allclose(nem[r].reshape(3, 3), q / len(fs), atol=1e-12)
