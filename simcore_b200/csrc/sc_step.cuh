@@ -273,7 +273,7 @@ __device__ __forceinline__ double dotn(const double *a, const double *b) {
 
 // Shared-memory words of one integrator block of C sites.
 __host__ __device__ constexpr size_t integrate_smem_doubles(int C) {
-  return 31 * (size_t)C;
+  return 27 * (size_t)C;
 }
 
 // 8-byte asynchronous global -> shared copy (cp.async), completed by
@@ -292,13 +292,14 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // MAXC: largest block (sites) the instantiation is launched with; blocks
 // per SM requested so that the register budget leaves room for several
 // blocks in flight.
-template <int MAXC>
+template <int MAXC, bool FAST>
 struct IntegrateBounds {
-  static constexpr int min_blocks = MAXC <= 128 ? 5 : 2;
+  // The exact variant spills below 96 registers; the fast one fits 80.
+  static constexpr int min_blocks = MAXC <= 128 ? (FAST ? 6 : 5) : 2;
 };
 
 template <int ND, int PREC, bool FAST, int MAXC>
-__global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
+__global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     k_integrate(SysConst k, DevState d, int midstep, int rbuf, int interaction,
                 int capture) {
   extern __shared__ double smem[];
@@ -314,9 +315,12 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC>::min_blocks)
   double *sb = sa + C;          // diagonal             C
   double *sc = sb + C;          // upper diagonal       C
   double *skeff = sc + C;       // k_eff                C
-  double *sdt = skeff + C;      // det_t                2C
-  double *sdb = sdt + 2 * C;    // det_b                2C
-  double *srp = sdb + 2 * C;    // full step: prefetched previous positions 3C
+  // The metric determinants live only in the bending stage, after the
+  // random-force solve has been read and before the tension system is
+  // written: they share the Thomas arrays (sT, sa, sb, sc).
+  double *sdt = sT;             // det_t                2C
+  double *sdb = sT + 2 * C;     // det_b                2C
+  double *srp = skeff + C;      // full step: prefetched previous positions 3C
   double *sfp = srp + 3 * C;    // full step: prefetched projected noise     3C
   FilConst *sfil = (FilConst *)(sfp + 3 * C);   // C/2 filaments
   int *sflag = (int *)(sfil + C / 2);           // C/2 renormalisation flags
