@@ -1574,7 +1574,7 @@ sc_status sc_output_open(sc_ctx *c, const char *run_name, const char *species_na
   for (size_t r = 0; r < nrep; ++r) {
     std::string run = run_name;
     if (nrep > 1) {
-      char sfx[16];
+      char sfx[32];
       std::snprintf(sfx, sizeof(sfx), "_r%03zu", r);
       run += sfx;
     }
