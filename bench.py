@@ -40,8 +40,20 @@ I_STEPS_PER_STEP = 20
 # mixed precision, from ncu (cold cache): the mean of a midstep launch
 # (21.87 MB) and a full-step launch (39.48 MB), which alternate.
 TRAFFIC_K_INTEGRATE_MIXED = 30.67e6
-WORKLOAD_DESC = ("B: 20,000 filaments x 10 bonds (200,000 segments, 220,000 sites), 3D periodic "
-                 "cube side 200, lp 100, WCA eps=sigma=1, dt 1e-4, noise on")
+WORKLOAD_DESCS = {
+    "A": "A: 100 filaments x 20 bonds (2,000 segments, 2,100 sites), 3D periodic cube side 50, "
+         "lp 500, WCA eps=sigma=1, dt 1e-4, noise on",
+    "B": "B: 20,000 filaments x 10 bonds (200,000 segments, 220,000 sites), 3D periodic cube side "
+         "200, lp 100, WCA eps=sigma=1, dt 1e-4, noise on",
+    "C": "C: 50,000 filaments x log-uniform[5,200] bonds (2.64M segments), lp uniform[10,1000], "
+         "3D periodic cube side 300, WCA eps=sigma=1, dt 5e-5, noise on",
+    "D": "D: 256 independent 2D periodic systems of uniform[200,2000] filaments x 16 bonds "
+         "(4.5M segments), area fraction 0.1, lp 200, WCA eps=sigma=1, dt 1e-4, noise on, "
+         "one context",
+    "E": "E: 10,000 filaments x 50 bonds (500,000 segments), 3D periodic cube side 150, lp 1000, "
+         "100,000 static tethers k=10 rest 1, WCA eps=sigma=1, dt 1e-4, noise on",
+}
+WORKLOAD_DESC = WORKLOAD_DESCS["B"]
 
 
 def parse_args():
@@ -50,7 +62,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="B")
+    ap.add_argument("--workload", default="B", choices=sorted(WORKLOAD_DESCS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="run this many host-driven steps and exit (for ncu)")
@@ -187,14 +199,68 @@ def kernel_times(ctx, n):
     return tp / n, ti / n
 
 
+def load_workload(name, seed):
+    """(system, filaments, sites, replicas, crosslinks) of a workload."""
+    from simcore_b200 import workloads
+    if name == "D":
+        system, fils, sites, reps = workloads.make_replicas("D", seed=seed)
+        return system, fils, sites, reps, None
+    system, fils, sites = workloads.make(name, 1.0, seed=seed)
+    xl = workloads.crosslinks(name, sites, fils, 2 * system["system_radius"], seed=seed)
+    return system, fils, sites, None, xl
+
+
+def new_context(sc, wl, prec, device):
+    system, fils, sites, reps, xl = wl
+    ctx = sc.Context(system, fils, sites, precision=prec, device=device, replicas=reps)
+    if xl is not None:
+        a, b, k, rest = xl
+        ctx.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+    return ctx
+
+
+def cpu_runs(wl, cores):
+    """CPU simulations of a workload for the baseline: the reference's own
+    code (oracle/_ref, OpenMP on `cores` threads) where it covers the
+    workload; tethered networks run on the C oracle, the reference's tether
+    code being unbuildable here.  Independent systems run one after another
+    (the reference keeps static state: one simulation per process at a time),
+    a leading subset of them.  Returns (kind, cores, [(make, bonds)], note),
+    make() creating one simulation."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from checkers import Oracle, Reference
+    import simcore_b200 as sc
+    from simcore_b200 import workloads
+    system, fils, sites, reps, xl = wl
+    bonds = lambda fs: sum(sc.filament_n_bonds(f) for f in fs)
+    if xl is not None:
+        def make_tethered():
+            sim = Oracle(system, fils, sites)
+            sim.add_crosslinks(xl[0], xl[1], k_spring=xl[2], rest_length=xl[3])
+            return sim
+        return "port", 1, [(make_tethered, bonds(fils))], \
+            "C oracle with the restated tethers (1 thread)"
+    use_ref = Reference.available()
+    kind, cores = ("reference", cores) if use_ref else ("port", 1)
+    make = (lambda *a: Reference(*a, n_threads=cores)) if use_ref else Oracle
+    if reps is None:
+        return kind, cores, [(lambda: make(system, fils, sites), bonds(fils))], ""
+    runs, total = [], 0
+    for part in workloads.split_replicas(system, fils, sites, reps):
+        runs.append(((lambda p=part: make(*p)), bonds(part[1])))
+        total += runs[-1][1]
+        if total >= 100000:
+            break
+    return kind, cores, runs, "the first %d of %d systems, one after another" % (len(runs), len(reps))
+
+
 def profile_only(args):
     """--profile-steps N: host-driven reference steps of the bench workload
     (one pair launch and one integrator launch each) after 4 warm-up steps,
     nothing timed; the command the ncu captures run."""
     import simcore_b200 as sc
     from simcore_b200 import workloads
-    system, fils, sites = workloads.make(args.workload, 1.0, seed=0)
-    ctx = sc.Context(system, fils, sites, precision=args.precision, device=0)
+    ctx = new_context(sc, load_workload(args.workload, 0), args.precision, 0)
     ctx.step(4)
     ctx.step(args.profile_steps)
     ctx.synchronize()
@@ -218,7 +284,8 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    system, fils, sites = workloads.make(args.workload, 1.0, seed=replica_seed(rank))
+    wl = load_workload(args.workload, replica_seed(rank))
+    system, fils, sites = wl[:3]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def timed_graph(ctx, k, flush_l2=True):
@@ -240,7 +307,7 @@ def run_ours(args, rank, world, local_rank):
         sampler.start()
         time.sleep(1.5)  # nvidia-smi needs a moment before its first sample
     for prec in ("fp64", "mixed"):
-        ctx = sc.Context(system, fils, sites, precision=prec, device=local_rank)
+        ctx = new_context(sc, wl, prec, local_rank)
         contexts[prec] = ctx
         layouts[prec] = ctx.autotune()  # integrator layout for this shape
         timed_graph(ctx, args.warmup)
@@ -268,7 +335,7 @@ def run_ours(args, rank, world, local_rank):
     # (max |dF| / max |F|).
     errs = {}
     for p_ in ("fp64", "mixed"):
-        cc = sc.Context(system, fils, sites, precision=p_, device=local_rank)
+        cc = new_context(sc, wl, p_, local_rank)
         cc.interact()
         errs[p_] = cc.bond_forces()
         cc.close()
@@ -337,7 +404,7 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair forces + f64 integrator",
         "data": "synthetic (seeded random insertion with overlap rejection)",
-        "config": {"workload": WORKLOAD_DESC, "precision": "mixed",
+        "config": {"workload": WORKLOAD_DESCS[args.workload], "precision": "mixed",
                    "i_steps_per_step": I_STEPS_PER_STEP,
                    "timed_unit": "one CUDA-graph launch of 20 reference steps (WHILE loop of 10 "
                                  "midpoint BD steps with device-decided pair-list rebuilds)",
@@ -378,34 +445,32 @@ def run_ours(args, rank, world, local_rank):
         "clocks": results.get("clocks"),
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(system, fils, sites, n_b)
+        line["cpu_baseline"] = cpu_baseline(wl)
     return line
 
 
-def cpu_baseline(system, fils, sites, n_bonds, target_s=10.0):
-    """The reference's own code (oracle/_ref) on the same workload, OpenMP
-    over all host cores; falls back to the single-threaded C oracle when the
-    reference build is not present.  A bounded sample of steps."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from checkers import Oracle, Reference
-    cores = host_cores()
-    if Reference.available():
-        sim = Reference(system, fils, sites, n_threads=cores)
-        kind = "reference"
-    else:
-        sim = Oracle(system, fils, sites)
-        kind, cores = "port", 1
-    t0 = time.perf_counter()
-    sim.step(2)
-    dt = max(time.perf_counter() - t0, 1e-6)
-    n = int(max(2, min(400, target_s / (dt / 2))))
-    n += n % 2
-    t0 = time.perf_counter()
-    sim.step(n)
-    el = time.perf_counter() - t0
-    sim.close()
-    return {"value": n_bonds * n / el, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": "%d reference steps of the same workload (after 2 warm-up steps)" % n}
+def cpu_baseline(wl, target_s=10.0):
+    """The reference's CPU code on the same workload (cpu_runs), a bounded
+    sample of steps sized to about target_s seconds in all."""
+    kind, cores, runs, note = cpu_runs(wl, host_cores())
+    seg, el, n_used = 0, 0.0, 0
+    for make, nb in runs:
+        sim = make()
+        t0 = time.perf_counter()
+        sim.step(2)
+        dt = max(time.perf_counter() - t0, 1e-6)
+        n = int(max(2, min(400, target_s / len(runs) / (dt / 2))))
+        n += n % 2
+        t0 = time.perf_counter()
+        sim.step(n)
+        el += time.perf_counter() - t0
+        seg += nb * n
+        n_used = max(n_used, n)
+        sim.close()
+    sample = "up to %d reference steps of the same workload (after 2 warm-up steps)" % n_used
+    if note:
+        sample += "; " + note
+    return {"value": seg / el, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
 
 def run_reference(args, rank, world):
@@ -413,40 +478,48 @@ def run_reference(args, rank, world):
         return None
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from checkers import Reference
-    from simcore_b200 import workloads
     if not Reference.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libscref.so (the reference's "
                 "own sources) was not built on this machine"}
-    system, fils, sites = workloads.make(args.workload, 1.0, seed=0)
-    cores = host_cores()
-    sim = Reference(system, fils, sites, n_threads=cores)
-    n_b = sim.n_bonds
+    kind, cores, runs, note = cpu_runs(load_workload(args.workload, 0), host_cores())
     # Size each bench step to a bounded sample: at most 20 reference steps,
     # fewer if one step is slow, so that warm-up + timed steps stay short.
+    sim = runs[0][0]()
     t0 = time.perf_counter()
     sim.step(2)
-    per = max((time.perf_counter() - t0) / 2, 1e-6)
+    per = max((time.perf_counter() - t0) / 2, 1e-6) * sum(nb for _, nb in runs) / runs[0][1]
+    sim.close()
     budget_s = 150.0 / max(args.steps + args.warmup, 1)
     per_step = int(max(2, min(I_STEPS_PER_STEP, budget_s / per)))
     per_step -= per_step % 2
-    for _ in range(args.warmup):
-        sim.step(per_step)
-    times = []
-    for _ in range(args.steps):
-        times.append(sim.step(per_step))
-    sim.close()
+    # Bench step k is the k-th chunk of per_step steps of every system.
+    times = [0.0] * args.steps
+    seg = 0
+    for make, nb in runs:
+        sim = make()
+        for _ in range(args.warmup):
+            sim.step(per_step)
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            sim.step(per_step)
+            times[k] += time.perf_counter() - t0
+            seg += nb * per_step
+        sim.close()
     total = float(sum(times))
-    value = n_b * per_step * args.steps / total
+    value = seg / total
+    sample = "%d reference steps per bench step" % per_step + ("; " + note if note else "")
     return {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded random insertion with overlap rejection)",
-        "config": {"workload": WORKLOAD_DESC, "i_steps_per_step": per_step,
-                   "implementation": "reference C++ (object, site, bond, mesh, filament, cell, "
-                                     "cell_list, minimum_distance, linear_algebra) -O3 OpenMP"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": "%d reference steps per bench step" % per_step},
+        "config": {"workload": WORKLOAD_DESCS[args.workload], "i_steps_per_step": per_step,
+                   "implementation": ("reference C++ (object, site, bond, mesh, filament, cell, "
+                                      "cell_list, minimum_distance, linear_algebra) -O3 OpenMP"
+                                      if kind == "reference" else
+                                      "C restatement of the reference (tethers included)")},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 

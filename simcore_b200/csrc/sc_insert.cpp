@@ -12,6 +12,7 @@
 // diameter to an already accepted bond).  Randomness is Philox4x32-10 keyed
 // by (seed, 0xC0FFEE), so a configuration is a pure function of its seed.
 // Both the GPU path and the CPU reference load the same configuration.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -143,9 +144,19 @@ extern "C" int sc_insert_filaments(int n_dim, double system_radius,
   std::vector<double> bc, bu;  // accepted bond centres and axes
   std::vector<double> bh;      // half lengths
   Stream rng{(uint32_t)seed ^ (uint32_t)(seed >> 32), 0xC0FFEEu, 0};
-  size_t site_cursor = 0;
+  // Longest filaments first (a stable order, so equal lengths keep theirs):
+  // they find room while the box is empty; each filament's sites still go
+  // to its own place in site_xyz.
+  std::vector<size_t> site_at(n_fil + 1, 0);
+  for (int f = 0; f < n_fil; ++f) site_at[f + 1] = site_at[f] + n_bonds[f] + 1;
+  std::vector<int> order(n_fil);
+  for (int f = 0; f < n_fil; ++f) order[f] = f;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return length[a] > length[b]; });
   std::vector<double> pos, cen, axis;
-  for (int f = 0; f < n_fil; ++f) {
+  for (int oi = 0; oi < n_fil; ++oi) {
+    const int f = order[oi];
+    const size_t site_cursor = site_at[f];
     const int nb = n_bonds[f];
     const double l = length[f] / nb, lp = persistence_length[f];
     bool placed = false;
@@ -249,7 +260,6 @@ extern "C" int sc_insert_filaments(int n_dim, double system_radius,
       }
       std::memcpy(site_xyz + 3 * site_cursor, pos.data(),
                   sizeof(double) * 3 * (nb + 1));
-      site_cursor += nb + 1;
       placed = true;
     }
     if (!placed) return SC_ERR_INSERTION;

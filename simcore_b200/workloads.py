@@ -10,6 +10,8 @@ rejection (sc_insert_filaments); no dataset is involved.
   A  100 x 20 bonds, lp 500, side 50, dt 1e-4          (CPU parity case)
   B  20,000 x 10 bonds, lp 100, side 200, dt 1e-4       (dense suspension)
   C  50,000 x log-uniform[5,200] bonds, lp U[10,1000], side 300, dt 5e-5
+     (its 100-200-bond filaments have an excluded volume several times the
+     box: isotropic insertion cannot place them, so random_nematic)
   D  256 independent 2D systems (make_replicas): N_r ~ U{200..2000}
      filaments x 16 bonds, side sqrt(N_r (16 + pi/4) / 0.1), lp 200, dt 1e-4
   E  10,000 x 50 bonds, lp 1000, side 150, dt 1e-4      (network geometry;
@@ -34,7 +36,8 @@ WORKLOADS = {
     "A": dict(n_dim=3, side=50.0, n_fil=100, n_seg=20, lp=500.0, delta=1e-4, n_steps=1000),
     "B": dict(n_dim=3, side=200.0, n_fil=20000, n_seg=10, lp=100.0, delta=1e-4, n_steps=2000),
     "C": dict(n_dim=3, side=300.0, n_fil=50000, n_seg=("loguniform", 5, 200),
-              lp=("uniform", 10.0, 1000.0), delta=5e-5, n_steps=1000),
+              lp=("uniform", 10.0, 1000.0), delta=5e-5, n_steps=1000,
+              insertion="random_nematic"),
     "E": dict(n_dim=3, side=150.0, n_fil=10000, n_seg=50, lp=1000.0, delta=1e-4, n_steps=1000,
               insertion="random_nematic"),
 }
