@@ -36,10 +36,11 @@ sys.path.insert(0, ROOT)
 METRIC = "segment-steps/s, 1 B200: mixed+batched vs FP64 GPU at ≤1e-5 force err"
 UNIT = "segment-steps/s"
 I_STEPS_PER_STEP = 20
-# DRAM bytes (read + write) of one k_integrate launch of the default workload,
-# mixed precision, from ncu (cold cache): the mean of a midstep launch
-# (21.87 MB) and a full-step launch (39.48 MB), which alternate.
-TRAFFIC_K_INTEGRATE_MIXED = 30.67e6
+# DRAM bytes (read + write) of one k_integrate launch, mixed precision, from
+# ncu (cold cache), per workload captured: for B the mean of a midstep launch
+# (21.87 MB) and a full-step launch (39.48 MB), which alternate.  Workloads
+# without a capture report null.
+TRAFFIC_K_INTEGRATE_MIXED = {"B": 30.67e6}
 WORKLOAD_DESCS = {
     "A": "A: 100 filaments x 20 bonds (2,000 segments, 2,100 sites), 3D periodic cube side 50, "
          "lp 500, WCA eps=sigma=1, dt 1e-4, noise on",
@@ -336,7 +337,7 @@ def run_ours(args, rank, world, local_rank):
         c1 = ctx.counters()
         total_ms = reduce_max(float(sum(ms)), dist)
         results[prec] = dict(total_ms=total_ms, n_bonds=c1.n_bonds, n_sites=c1.n_sites,
-                             n_pairs=c1.n_pairs, rebuilds=c1.n_rebuilds - c0.n_rebuilds,
+                             n_fil=c1.n_filaments, n_dim=wl[0]["n_dim"], n_pairs=c1.n_pairs, rebuilds=c1.n_rebuilds - c0.n_rebuilds,
                              launches=c1.kernel_launches - c0.kernel_launches)
 
     if sampler:
@@ -433,9 +434,10 @@ def run_ours(args, rank, world, local_rank):
                         "vs": "FP64 GPU path (bit-identical to the reference) on the same "
                               "positions, one pair evaluation", "bound": 1e-5},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": TRAFFIC_K_INTEGRATE_MIXED,
-                     "kernel": "k_integrate<3,mixed,fast> (dominant: one launch per reference "
-                               "step, all 20,000 filaments)",
+                     "frac": achieved / peak,
+                     "traffic": TRAFFIC_K_INTEGRATE_MIXED.get(args.workload),
+                     "kernel": "k_integrate<%d,mixed,fast> (dominant: one launch per reference "
+                               "step, all %d filaments)" % (r["n_dim"], r["n_fil"]),
                      "algorithmic_bytes_per_launch": b_int, "avg_launch_ms": t_int,
                      "peak_kind": peak_kind + " hbm_gbs",
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "

@@ -91,6 +91,7 @@ typedef struct {
   double dr_update;           /* rebuild threshold 0.25 * cell_length^2 (system 0) */
   int64_t kernel_launches;    /* kernels launched by this context */
   int32_t n_replicas;         /* independent systems in the context */
+  int64_t n_list_regrowths;   /* pair lists grown after a rebuild outgrew them */
 } sc_counters;
 
 typedef struct sc_ctx sc_ctx;

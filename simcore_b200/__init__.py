@@ -66,7 +66,8 @@ class Counters(ctypes.Structure):
                 ("n_filaments", ctypes.c_int64), ("n_sites", ctypes.c_int64),
                 ("n_bonds", ctypes.c_int64), ("n_cells_1d", ctypes.c_int32),
                 ("cell_length", ctypes.c_double), ("dr_update", ctypes.c_double),
-                ("kernel_launches", ctypes.c_int64), ("n_replicas", ctypes.c_int32)]
+                ("kernel_launches", ctypes.c_int64), ("n_replicas", ctypes.c_int32),
+                ("n_list_regrowths", ctypes.c_int64)]
 
 
 def _load():

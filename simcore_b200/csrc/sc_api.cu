@@ -107,6 +107,7 @@ struct sc_ctx {
   long long timed_launches = 0;
   cudaEvent_t gev0 = nullptr, gev1 = nullptr;  // around each graph launch
   double graph_ms = 0.0;
+  long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
 };
 
 namespace {
@@ -388,6 +389,8 @@ void rebuild_enqueue(sc_ctx *c) {
 // (binning is a pure function of the positions, so the second pass gives the
 // same list); with several systems an overflow is reported, unless
 // allow_overflow (the initial pass, whose caller sizes the segments).
+sc_status grow_after_overflow(sc_ctx *c);
+
 sc_status rebuild(sc_ctx *c, bool allow_overflow = false) {
   for (int attempt = 0; attempt < 3; ++attempt) {
     rebuild_enqueue(c);
@@ -403,21 +406,29 @@ sc_status rebuild(sc_ctx *c, bool allow_overflow = false) {
     if (allow_overflow) return SC_OK;
     if (c->reps.size() != 1)
       return fail(c, SC_ERR_LIST_OVERFLOW, "a system's pair list outgrew its segment");
-    // Undo the extra rebuild count, grow, retry.
-    const int want = c->np_rep[0];
-    c->np = 0;  // the overflowed list is incomplete: nothing to keep
-    CKS(ensure_pair_capacity(c, (long long)want));
-    long long cnt[2] = {0, 0};
-    CK(cudaMemcpyAsync(&cnt[0], c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(&cnt[1], c->d.rep_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    cnt[0] -= 1;
-    cnt[1] -= 1;
-    CK(cudaMemcpyAsync(c->d.n_rebuilds, &cnt[0], sizeof(long long), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(c->d.rep_rebuilds, &cnt[1], sizeof(long long), cudaMemcpyHostToDevice, c->st));
-    CK(cudaStreamSynchronize(c->st));
+    CKS(grow_after_overflow(c));
   }
   return fail(c, SC_ERR_LIST_OVERFLOW, "pair list kept overflowing");
+}
+
+// A rebuild of the single system overflowed its list (the overflow bit
+// already cleared): grow the list to the full count and take that pass back
+// out of the rebuild counters, since the pass is redone.
+sc_status grow_after_overflow(sc_ctx *c) {
+  const int want = c->np_rep[0];
+  c->np = 0;  // the overflowed list is incomplete: nothing to keep
+  CKS(ensure_pair_capacity(c, (long long)want));
+  long long cnt[2] = {0, 0};
+  CK(cudaMemcpyAsync(&cnt[0], c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(&cnt[1], c->d.rep_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  cnt[0] -= 1;
+  cnt[1] -= 1;
+  CK(cudaMemcpyAsync(c->d.n_rebuilds, &cnt[0], sizeof(long long), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(c->d.rep_rebuilds, &cnt[1], sizeof(long long), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->n_regrowths++;
+  return SC_OK;
 }
 
 // Flags every system and rebuilds (the forced update after insertion).
@@ -1131,35 +1142,68 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
     CKS(sync_pair_count(c));
     if (c->reps.size() == 1 && c->np + c->np / 2 > c->pcap)
       CKS(ensure_pair_capacity(c, c->np + c->np / 2));
-    if (!c->graph_exec || c->graph_rbuf != c->rbuf) CKS(build_graph(c));
-    *c->h_loop = bd;
-    CK(cudaMemcpyAsync(c->d.loop_count, c->h_loop, sizeof(int), cudaMemcpyHostToDevice, c->st));
-    long long nr0 = 0, nr1 = 0;
-    CK(cudaMemcpyAsync(&nr0, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
     if (!c->gev0) {
       CK(cudaEventCreate(&c->gev0));
       CK(cudaEventCreate(&c->gev1));
     }
-    CK(cudaEventRecord(c->gev0, c->st));
-    CK(cudaGraphLaunch(c->graph_exec, c->st));
-    CK(cudaEventRecord(c->gev1, c->st));
-    CK(cudaMemcpyAsync(&nr1, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-    c->i_step += 2 * (long long)bd;
-    if (c->desc.stoch_flag) c->mcount += bd;
-    c->pairs_ready = false;
-    CKS(readback(c));
-    {
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
-      c->graph_ms = ms;
+    c->graph_ms = 0.0;
+    // A rebuild whose list outgrows its segment stops the run at that BD
+    // step, with nothing past the rebuild done; the list then grows, the
+    // rebuild is redone host-side and the run resumes with that step.
+    for (int attempt = 0; bd > 0; ++attempt) {
+      if (attempt == 8) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list kept overflowing inside captured runs");
+      if (!c->graph_exec || c->graph_rbuf != c->rbuf) CKS(build_graph(c));
+      *c->h_loop = bd;
+      CK(cudaMemcpyAsync(c->d.loop_count, c->h_loop, sizeof(int), cudaMemcpyHostToDevice, c->st));
+      long long nr0 = 0, nr1 = 0;
+      CK(cudaMemcpyAsync(&nr0, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaEventRecord(c->gev0, c->st));
+      CK(cudaGraphLaunch(c->graph_exec, c->st));
+      CK(cudaEventRecord(c->gev1, c->st));
+      CK(cudaMemcpyAsync(&nr1, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaMemcpyAsync(c->h_loop, c->d.loop_count, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+      c->pairs_ready = false;
+      CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                         c->st));
+      CK(cudaStreamSynchronize(c->st));
+      const unsigned st = c->hb->status;
+      const bool overflow = (st & sc::ST_LIST_OVERFLOW) != 0u;
+      // BD steps completed: all of them, or those before the stopped one.
+      const int done = overflow ? bd - *c->h_loop : bd;
+      c->i_step += 2 * (long long)done;
+      if (c->desc.stoch_flag) c->mcount += done;
+      {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
+        c->graph_ms += ms;
+      }
+      // Kernels the graph ran: loop head, per BD step decide + 2 steps +
+      // tail (the stopped step's too), per rebuild the captured sequence.
+      c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) *
+                             (c->desc.interaction_flag ? (c->d.nx ? 7 : 6) : 3) +
+                     (nr1 - nr0) * c->rebuild_kernels;
+      bd -= done;
+      if (!overflow) {
+        CKS(readback(c));
+        break;
+      }
+      if (st & ~sc::ST_LIST_OVERFLOW) {
+        CKS(readback(c));  // reports the other error
+        return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow inside a captured run");
+      }
+      if (c->reps.size() != 1)
+        return fail(c, SC_ERR_LIST_OVERFLOW, "a system's pair list outgrew its segment inside a captured run");
+      const unsigned clear = 0u;
+      CK(cudaMemcpyAsync(c->d.status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice, c->st));
+      CKS(sync_pair_count(c));
+      CKS(grow_after_overflow(c));
+      // The stopped step's due flag is still set: redo its rebuild, with
+      // headroom for the rest of the run.
+      CKS(rebuild(c));
+      if (c->np + c->np / 2 > c->pcap) CKS(ensure_pair_capacity(c, c->np + c->np / 2));
     }
-    // Kernels the graph ran: loop head, per BD step decide + 2 steps + tail,
-    // per rebuild the captured rebuild sequence.
-    c->launches += 1 + (long long)bd * (c->desc.interaction_flag ? (c->d.nx ? 7 : 6) : 3) +
-                   (nr1 - nr0) * c->rebuild_kernels;
     unsigned st = c->hb->status;
     if (st & sc::ST_UNPHYSICAL) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result");
-    if (st & sc::ST_LIST_OVERFLOW) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow inside a captured run");
   }
   if (n % 2) CKS(step_once(c));
   return SC_OK;
@@ -1943,6 +1987,7 @@ sc_status sc_get_counters(sc_ctx *c, sc_counters *o) {
     o->dr_update = c->reps[0].dr_update;
   }
   o->n_replicas = (int32_t)c->reps.size();
+  o->n_list_regrowths = c->n_regrowths;
   o->kernel_launches = c->launches;
   return SC_OK;
 }

@@ -570,6 +570,7 @@ template <int ND>
 __global__ void k_tether(SysConst k, DevState d) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= d.nx) return;
+  if (*d.status & ST_LIST_OVERFLOW) return;  // the step stopped at its rebuild
   // Both anchors lie in one system (checked when the links are added).
   const ReplicaConst &Rx = d.rep[rep_of_bond(d, d.xl_anchor[2 * x] >> 1)];
   double sp[2][3], ua[2][3], len[2], lam[2];
@@ -957,11 +958,18 @@ __global__ void k_loop_head(DevState d, cudaGraphConditionalHandle h) {
 
 // End of one BD step (midstep + full step) of a graph loop: advances the
 // noise counter and decrements the remaining count.  A recorded error stops
-// the loop.
+// the loop.  A step whose rebuild overflowed its list did nothing past the
+// rebuild: it stays counted as remaining, so the host can grow the list,
+// redo the rebuild and resume with it.
 __global__ void k_loop_tail(DevState d, int stoch, cudaGraphConditionalHandle h) {
+  const unsigned status = *d.status;
+  if (status & ST_LIST_OVERFLOW) {
+    cudaGraphSetConditional(h, 0u);
+    return;
+  }
   if (stoch) *d.mcount += 1ull;
   int left = *d.loop_count - 1;
-  if (*d.status != 0u) left = 0;
+  if (status != 0u) left = 0;
   *d.loop_count = left;
   cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
 }

@@ -330,6 +330,10 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
 
   const int blk = blockIdx.x;
   const int t = threadIdx.x;
+  // A rebuild of this step whose list outgrew its segment stops the step
+  // before its first store (uniform over the grid: nothing in this kernel
+  // sets that bit), so the host can grow the list and redo the step.
+  const bool overflowed = (*d.status & ST_LIST_OVERFLOW) != 0u;
   const unsigned long long mcount = *d.mcount;
   const int s0 = d.blk_site0[blk];
   const int count = d.blk_ns[blk];
@@ -347,6 +351,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     lf = f - f0;
   }
   __syncthreads();
+  if (overflowed) return;
   const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
   const int n = active ? fc.n : 0;
   const int j = active ? g - fc.site0 : -1;

@@ -62,6 +62,9 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
   const int bq = has_bond ? b : (b > 0 ? b - 1 : 0);  // a valid bond for loads
   const FilConst &fc = d.fil[f];
   const unsigned long long mcount = *d.mcount;
+  // An overflowed rebuild of this step stops it before the first store
+  // (read here, tested after the loads are issued).
+  const bool overflowed = (*d.status & ST_LIST_OVERFLOW) != 0u;
 
   // ---- every global read of the step, issued together ---------------------
   double r[3] = {0, 0, 0}, u[3] = {0, 0, 0};
@@ -90,6 +93,7 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
 #pragma unroll
     for (int i = 0; i < ND; ++i) xi[i] = ((double)wv[i] + 0.5) * 2.3283064365386963e-10 - 0.5;
   }
+  if (overflowed) return;  // the whole warp: the bit is uniform
   if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
 #pragma unroll
     for (int i = 0; i < 3; ++i) d.rp[i][g] = r[i];

@@ -150,6 +150,31 @@ def test_graph_path_matches_host_path(precision):
     assert a.counters().n_rebuilds > 0
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_captured_run_grows_an_overflowing_pair_list(precision):
+    """Stiff filaments (persistence length 1000 at dt 1e-4, 50 bonds) buckle
+    under the reference's explicit bending, and their candidate pairs grow
+    about fivefold in 400 steps: past the half-again headroom a captured run
+    starts with.  The run stops at the overflowing rebuild, grows the list,
+    redoes the rebuild and resumes -- bit for bit the host-driven run, with
+    the same rebuild count."""
+    system, fils, sites = _workload("E", 0.1, seed=3)
+    a = _ctx(system, fils, sites, precision)
+    b = _ctx(system, fils, sites, precision)
+    n0 = a.counters().n_pairs
+    a.step_graph(400)
+    b.step(400)
+    ca, cb = a.counters(), b.counters()
+    assert ca.n_list_regrowths > 0
+    assert ca.n_pairs > 2 * n0
+    assert ca.i_step == cb.i_step == 400
+    assert ca.n_rebuilds == cb.n_rebuilds
+    assert_same(a.sites(), b.sites(), "sites")
+    assert_same(a.pairs(), b.pairs(), "pairs")
+    a.close()
+    b.close()
+
+
 def test_graph_matches_oracle():
     system, fils, sites = _workload("A", 1.0, seed=4)
     ctx = _ctx(system, fils, sites)

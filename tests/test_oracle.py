@@ -228,3 +228,38 @@ def test_crosslink_compression_constant():
     o.add_crosslinks([0], [6], k_spring=10.0, k_spring_compress=4.0, rest_length=2.0)
     o.step(2)
     assert np.allclose(o.crosslink_forces(), [[0, -2.0, 0]], atol=1e-12)
+
+
+def _mean_bond_cosine(xyz, n_sites):
+    off = np.concatenate([[0], np.cumsum(n_sites)])
+    cos = []
+    for f in range(len(n_sites)):
+        u = np.diff(xyz[off[f]:off[f + 1]], axis=0)
+        u /= np.linalg.norm(u, axis=1)[:, None]
+        cos.append((u[1:] * u[:-1]).sum(1))
+    return float(np.concatenate(cos).mean())
+
+
+@pytest.mark.parametrize("lp,dt,stable", [(500.0, 1e-4, True), (1000.0, 1e-4, False),
+                                          (1000.0, 5e-5, True)])
+def test_explicit_bending_stability_limit(lp, dt, stable):
+    """The reference's bending forces are explicit, so with 1-sigma bonds its
+    midpoint step is stable only below a persistence length set by dt:
+    20 filaments of 50 bonds, no pair forces, 400 steps.  At workload E's
+    lp 1000 and dt 1e-4 the filaments buckle (mean bond cosine about 0.72
+    against the worm-like-chain 0.999); at lp 500, or at dt 5e-5, they stay
+    within 1e-3 of it."""
+    import simcore_b200 as sc
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("E", 0.002, seed=1)
+    fils = [dict(f, persistence_length=lp) for f in fils]
+    o = Oracle(dict(system, interaction_flag=0, delta=dt), fils, sites)
+    o.step(400)
+    n_sites = np.array([sc.filament_n_bonds(f) + 1 for f in fils])
+    c = _mean_bond_cosine(o.sites(), n_sites)
+    o.close()
+    wlc = 1.0 / np.tanh(lp) - 1.0 / lp
+    if stable:
+        assert abs(c - wlc) < 1e-3, (c, wlc)
+    else:
+        assert c < 0.9, (c, wlc)
