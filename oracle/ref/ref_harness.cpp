@@ -118,6 +118,8 @@ struct RefSim {
   int i_step = 0;
   bool overlap = false;
   double stress[9] = {0};
+  int n_thermo = 0;
+  std::vector<double> thermo_rec;  // i_step, pressure tensor (9), pressure, volume
   std::unordered_map<const Object *, int> bond_gid;
   int n_threads = 0;
   int n_sites_total = 0;
@@ -295,12 +297,36 @@ struct RefSim {
 #endif
     midstep = !midstep;
   }
-  void Step() {  // simulation.cpp:37-62 (outputs, graphics and thermo off)
+  // InteractionManager::CalculatePressure (src/interaction_manager.cpp:535-559)
+  // into a record, with the Space's own volume and the interactor count the
+  // restated CheckUpdateObjects keeps.
+  void CalculatePressure() {
+    int n_dim = params.n_dim;
+    double pressure_tensor[9] = {0};
+    double inv_V = 1.0 / sp->volume;
+    for (int i = 0; i < n_dim; ++i) {
+      for (int j = 0; j < n_dim; ++j) {
+        if (i == j) pressure_tensor[n_dim * i + j] += n_objs * inv_V;
+        pressure_tensor[n_dim * i + j] += stress[n_dim * i + j] * inv_V / n_thermo;
+      }
+    }
+    double pressure = 0;
+    for (int i = 0; i < n_dim; ++i) pressure += pressure_tensor[n_dim * i + i];
+    pressure /= n_dim;
+    std::fill(stress, stress + 9, 0);
+    thermo_rec.push_back((double)i_step);
+    for (int i = 0; i < 9; ++i) thermo_rec.push_back(pressure_tensor[i]);
+    thermo_rec.push_back(pressure);
+    thermo_rec.push_back(sp->volume);
+  }
+  void Step() {  // simulation.cpp:37-62 (outputs and graphics off)
     ++i_step;
     params.i_step = i_step;
     ZeroForces();
     Interact();
     UpdatePositions();
+    // Simulation::Statistics (src/simulation.cpp:108-114)
+    if (n_thermo > 0 && i_step % n_thermo == 0 && i_step > 0) CalculatePressure();
   }
 };
 
@@ -595,6 +621,45 @@ void scref_get_bond_cells(void *h, int *xyz) {
       xyz[3 * c + 1] = y;
       xyz[3 * c + 2] = z;
     }
+}
+
+// Thermo records every n_thermo steps from now on (0: none).
+void scref_set_thermo(void *h, int n_thermo) {
+  RefSim *s = (RefSim *)h;
+  s->n_thermo = n_thermo;
+  s->thermo_rec.clear();
+}
+
+// The records since the last call (at most max): i_step, pressure tensor
+// (9), pressure and volume each.  Returns how many were written.
+long scref_thermo_records(void *h, long max, long *i_step, double *tensor, double *pressure,
+                          double *volume) {
+  RefSim *s = (RefSim *)h;
+  long n = (long)s->thermo_rec.size() / 12;
+  if (n > max) n = max;
+  for (long k = 0; k < n; ++k) {
+    const double *q = s->thermo_rec.data() + 12 * k;
+    i_step[k] = (long)q[0];
+    for (int i = 0; i < 9; ++i) tensor[9 * k + i] = q[1 + i];
+    pressure[k] = q[10];
+    volume[k] = q[11];
+  }
+  s->thermo_rec.clear();
+  return n;
+}
+
+// InteractionManager::stress_ as accumulated since the last pressure.
+void scref_get_stress(void *h, double *out) {
+  RefSim *s = (RefSim *)h;
+  for (int i = 0; i < 9; ++i) out[i] = s->stress[i];
+}
+
+// Object::GetPotentialEnergy of every filament (its bonds' pair potentials,
+// added by Filament::ApplyInteractionForces during the last step).
+void scref_get_potential_energy(void *h, double *pote) {
+  RefSim *s = (RefSim *)h;
+  int c = 0;
+  for (auto &f : s->members) pote[c++] = f.GetPotentialEnergy();
 }
 
 // Per-site accumulated squared displacement since the last rebuild.

@@ -50,6 +50,16 @@ struct sco_sim {
   long np, pcap;
   int *pa, *pb;
   double *pf;
+  /* per pair, beside the force: the dr its stress used and its potential
+   * (Interaction::dr / stress / pote, kept like the force until re-evaluated) */
+  double *pdr, *ppote;
+  /* thermo: InteractionManager::stress_ and the pressure records
+   * (src/interaction_manager.cpp:500-517, 535-559) */
+  double stress[9];
+  double *bpote; /* per bond: Object::p_energy_ after ApplyPairInteractions */
+  int n_thermo;
+  long n_rec, rec_cap;
+  double *rec; /* per record: i_step, pressure tensor (9), pressure, volume */
   /* static crosslinks: anchor 2k+a of link k sits on bond xbond[2k+a], at its
    * tail (xhead 0, lambda = 0) or head (xhead 1, lambda = bond length) */
   int nx;
@@ -301,10 +311,12 @@ static void sphero(const sco_sim *s, const double *s_1, const double *u_1,
  * MaxForcePotential::CalcPotential (include/simcore/max_force_potential.hpp:11-40).
  * force[] holds the pair's force from its last in-range evaluation since the
  * list was built (the reference never clears it) and is overwritten only when
- * a potential is evaluated.  t1 = contact1 x force, t2 = contact2 x force
- * (src/interaction_manager.cpp:469-470). */
+ * a potential is evaluated, and so are the dr its stress was computed from
+ * (rdr; the contact difference in the max-force case) and its potential
+ * (rpote; 0 in the max-force case).  t1 = contact1 x force,
+ * t2 = contact2 x force (src/interaction_manager.cpp:469-470). */
 static void pair_force(const sco_sim *s, int b1, int b2, double *force,
-                       double *t1, double *t2) {
+                       double *t1, double *t2, double *rdr, double *rpote) {
   double dr[3] = {0, 0, 0}, c1[3] = {0, 0, 0}, c2[3] = {0, 0, 0}, dr_mag2 = 0;
   int n = s->n_dim, i;
   sphero(s, V3(s->bs, b1), V3(s->bu, b1), s->bl[b1], V3(s->bs, b2),
@@ -319,6 +331,8 @@ static void pair_force(const sco_sim *s, int b1, int b2, double *force,
       if (!(rmag < 1e-12)) {
         rinv = 1.0 / (rmag);
         for (i = 0; i < n; ++i) force[i] = s->fcut * dr[i] * rinv;
+        for (i = 0; i < n; ++i) rdr[i] = dr[i];
+        *rpote = 0;
       }
     } else {
       double rmag = sqrt(dr_mag2);
@@ -328,6 +342,8 @@ static void pair_force(const sco_sim *s, int b1, int b2, double *force,
       double ffac = -(12.0 * s->c12 * r6 - 6.0 * s->c6) * r6 * rinv;
       if (ABS(ffac) > s->fcut) ffac = SIGNOF(ffac) * s->fcut;
       for (i = 0; i < n; ++i) force[i] = ffac * dr[i] * rinv;
+      for (i = 0; i < n; ++i) rdr[i] = dr[i];
+      *rpote = r6 * (s->c12 * r6 - s->c6) + s->eps;
     }
   }
   cross3(c1, force, t1);
@@ -423,10 +439,14 @@ static void push_pair(sco_sim *s, int a, int b) {
     s->pa = (int *)realloc(s->pa, sizeof(int) * s->pcap);
     s->pb = (int *)realloc(s->pb, sizeof(int) * s->pcap);
     s->pf = (double *)realloc(s->pf, sizeof(double) * 3 * s->pcap);
+    s->pdr = (double *)realloc(s->pdr, sizeof(double) * 3 * s->pcap);
+    s->ppote = (double *)realloc(s->ppote, sizeof(double) * s->pcap);
   }
   s->pa[s->np] = a;
   s->pb[s->np] = b;
   s->pf[3 * s->np] = s->pf[3 * s->np + 1] = s->pf[3 * s->np + 2] = 0.0;
+  s->pdr[3 * s->np] = s->pdr[3 * s->np + 1] = s->pdr[3 * s->np + 2] = 0.0;
+  s->ppote[s->np] = 0.0;
   s->np++;
 }
 
@@ -596,11 +616,16 @@ static void pair_interactions(sco_sim *s, double *bF, double *bT, int commit) {
   long p;
   int i;
   for (p = 0; p < s->np; ++p) {
-    int a = s->pa[p], b = s->pb[p];
-    double force[3], t1[3], t2[3];
+    int a = s->pa[p], b = s->pb[p], n = s->n_dim, j;
+    double force[3], t1[3], t2[3], rdr[3], rpote = s->ppote[p];
     memcpy(force, s->pf + 3 * p, sizeof(force));
-    pair_force(s, a, b, force, t1, t2);
-    if (commit) memcpy(s->pf + 3 * p, force, sizeof(force));
+    memcpy(rdr, s->pdr + 3 * p, sizeof(rdr));
+    pair_force(s, a, b, force, t1, t2, rdr, &rpote);
+    if (commit) {
+      memcpy(s->pf + 3 * p, force, sizeof(force));
+      memcpy(s->pdr + 3 * p, rdr, sizeof(rdr));
+      s->ppote[p] = rpote;
+    }
     for (i = 0; i < s->n_dim; ++i) {
       V3(bF, a)[i] += force[i];
       V3(bF, b)[i] -= force[i];
@@ -608,6 +633,14 @@ static void pair_interactions(sco_sim *s, double *bF, double *bT, int commit) {
     for (i = 0; i < 3; ++i) {
       V3(bT, a)[i] += t1[i];
       V3(bT, b)[i] -= t2[i];
+    }
+    if (commit) {
+      /* obj1/obj2->AddPotential(pote); stress_ += ix->stress, where
+       * ix->stress[n i + j] = -dr[i] * force[j] (wca_potential.hpp:26-28) */
+      s->bpote[a] += rpote;
+      s->bpote[b] += rpote;
+      for (i = 0; i < n; ++i)
+        for (j = 0; j < n; ++j) s->stress[n * i + j] += -rdr[i] * force[j];
     }
   }
 }
@@ -1025,7 +1058,7 @@ sco_sim *sco_create(const sco_system *sys, int n_fil, const sco_filament *fils,
   ALLOCD(s->dz, 3 * n_sites); ALLOCD(s->dt, n_sites);
   ALLOCD(s->bp, 3 * s->nb); ALLOCD(s->bs, 3 * s->nb); ALLOCD(s->bu, 3 * s->nb);
   ALLOCD(s->bl, s->nb); ALLOCD(s->bF, 3 * s->nb); ALLOCD(s->bT, 3 * s->nb);
-  ALLOCD(s->tens, s->nb);
+  ALLOCD(s->tens, s->nb); ALLOCD(s->bpote, s->nb);
   ALLOCD(s->w_cos, max_ns); ALLOCD(s->w_gl, max_ns); ALLOCD(s->w_gd, max_ns);
   ALLOCD(s->w_gu, max_ns); ALLOCD(s->w_dt, max_ns + 1); ALLOCD(s->w_db, max_ns + 1);
   ALLOCD(s->w_ginv, max_ns); ALLOCD(s->w_keff, max_ns); ALLOCD(s->w_hd, max_ns);
@@ -1083,7 +1116,8 @@ void sco_destroy(sco_sim *s) {
   free(s->dz); free(s->dt); free(s->bp); free(s->bs); free(s->bu); free(s->bl);
   free(s->bF); free(s->bT); free(s->tens);
   free(s->xbond); free(s->xhead); free(s->xc); free(s->xF);
-  free(s->pa); free(s->pb); free(s->pf);
+  free(s->pa); free(s->pb); free(s->pf); free(s->pdr); free(s->ppote);
+  free(s->bpote); free(s->rec);
   free(s->w_cos); free(s->w_gl); free(s->w_gd); free(s->w_gu); free(s->w_dt);
   free(s->w_db); free(s->w_ginv); free(s->w_keff); free(s->w_hd); free(s->w_hu);
   free(s->w_hl); free(s->w_gam);
@@ -1098,6 +1132,38 @@ double sco_dr_update(const sco_sim *s) { return s->dr_update; }
 long sco_n_rebuilds(const sco_sim *s) { return s->n_rebuilds; }
 int sco_i_step(const sco_sim *s) { return s->i_step; }
 
+/* InteractionManager::CalculatePressure (src/interaction_manager.cpp:535-559)
+ * for the periodic box of Space::CalculateVolume (src/space.cpp:252-264,
+ * boundary 0): n_objs = the bond count (Mesh::GetCount, src/mesh.cpp:399).
+ * Appends the record OutputManager::WriteThermo writes. */
+static void calculate_pressure(sco_sim *s) {
+  const int n = s->n_dim;
+  const double side = 2 * s->R;
+  const double volume = n == 2 ? side * side : side * side * side;
+  const double inv_V = 1.0 / volume;
+  double P[9] = {0}, pressure = 0;
+  int i, j;
+  for (i = 0; i < n; ++i)
+    for (j = 0; j < n; ++j) {
+      if (i == j) P[n * i + j] += s->nb * inv_V;
+      P[n * i + j] += s->stress[n * i + j] * inv_V / s->n_thermo;
+    }
+  for (i = 0; i < n; ++i) pressure += P[n * i + i];
+  pressure /= n;
+  memset(s->stress, 0, sizeof(s->stress));
+  if (s->n_rec == s->rec_cap) {
+    s->rec_cap = s->rec_cap ? 2 * s->rec_cap : 64;
+    s->rec = (double *)realloc(s->rec, sizeof(double) * 12 * (size_t)s->rec_cap);
+  }
+  {
+    double *q = s->rec + 12 * s->n_rec++;
+    q[0] = (double)s->i_step;
+    memcpy(q + 1, P, sizeof(P));
+    q[10] = pressure;
+    q[11] = volume;
+  }
+}
+
 /* Simulation::RunSimulation body (src/simulation.cpp:37-62): ZeroForces,
  * Interact, Integrate.  Interact follows src/interaction_manager.cpp:63-95. */
 int sco_step(sco_sim *s, int nsteps) {
@@ -1107,6 +1173,7 @@ int sco_step(sco_sim *s, int nsteps) {
     memset(s->F, 0, sizeof(double) * 3 * s->ns);
     memset(s->bF, 0, sizeof(double) * 3 * s->nb);
     memset(s->bT, 0, sizeof(double) * 3 * s->nb);
+    memset(s->bpote, 0, sizeof(double) * s->nb);
     if (s->interaction) {
       double dr_max;
       if (s->nx) crosslink_update(s); /* src/interaction_manager.cpp:70 */
@@ -1118,8 +1185,47 @@ int sco_step(sco_sim *s, int nsteps) {
     }
     for (f = 0; f < s->nf; ++f) filament_update(s, f, s->species_midstep);
     s->species_midstep = !s->species_midstep;
+    /* Simulation::Statistics (src/simulation.cpp:108-114) */
+    if (s->n_thermo > 0 && s->i_step % s->n_thermo == 0) calculate_pressure(s);
   }
   return 0;
+}
+
+void sco_set_thermo(sco_sim *s, int n_thermo) {
+  s->n_thermo = n_thermo;
+  s->n_rec = 0;
+}
+
+/* Pressure records since the last call (at most max): i_step, pressure
+ * tensor (9, n_dim x n_dim packed), pressure and volume each. */
+long sco_thermo_records(sco_sim *s, long max, long *i_step, double *tensor, double *pressure,
+                        double *volume) {
+  long k, n = s->n_rec < max ? s->n_rec : max;
+  for (k = 0; k < n; ++k) {
+    const double *q = s->rec + 12 * k;
+    i_step[k] = (long)q[0];
+    memcpy(tensor + 9 * k, q + 1, 9 * sizeof(double));
+    pressure[k] = q[10];
+    volume[k] = q[11];
+  }
+  s->n_rec = 0;
+  return n;
+}
+
+void sco_get_stress(const sco_sim *s, double *stress) {
+  memcpy(stress, s->stress, sizeof(s->stress));
+}
+
+/* Object::GetPotentialEnergy of each filament after the last step: the sum,
+ * in bond order, of its bonds' potentials (Filament::ApplyInteractionForces,
+ * src/filament.cpp:1007), each the sum of its pairs' in list order. */
+void sco_get_potential_energy(const sco_sim *s, double *pote) {
+  int f, i;
+  for (f = 0; f < s->nf; ++f) {
+    double e = 0;
+    for (i = s->fb_off[f]; i < s->fb_off[f + 1]; ++i) e += s->bpote[i];
+    pote[f] = e;
+  }
 }
 
 int sco_add_crosslinks(sco_sim *s, int n, const int *site_a, const int *site_b,
@@ -1285,7 +1391,8 @@ int sco_segment_force(const sco_system *sys, const double *a1, const double *a2,
     s.bs = bs;
     s.bu = bu;
     s.bl = bl;
-    pair_force(&s, 0, 1, f, t1, t2);
+    double rdr[3] = {0, 0, 0}, rpote = 0;
+    pair_force(&s, 0, 1, f, t1, t2, rdr, &rpote);
   }
   for (i = 0; i < 3; ++i) force[i] = f[i];
   return 1;

@@ -97,6 +97,16 @@ void sco_get_crosslink_forces(const sco_sim *s, double *f);
  * any state: bond forces/torques are written to f and t. */
 void sco_pair_forces(sco_sim *s, double *f, double *t);
 
+/* Thermo: the pair virial accumulated every step and, every n_thermo steps
+ * (i_step % n_thermo == 0), the pressure tensor and pressure of
+ * InteractionManager::CalculatePressure; 0 stops the records.  Per-filament
+ * potential energy of the last step. */
+void sco_set_thermo(sco_sim *s, int n_thermo);
+long sco_thermo_records(sco_sim *s, long max, long *i_step, double *tensor, double *pressure,
+                        double *volume);
+void sco_get_stress(const sco_sim *s, double *stress);
+void sco_get_potential_energy(const sco_sim *s, double *pote);
+
 /* Philox4x32-10 block (for the known-answer test of the shared stream). */
 void sco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

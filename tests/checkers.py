@@ -169,6 +169,31 @@ class _Checker:
         self._call("get_dr_tot", _ptr(a))
         return a
 
+    def set_thermo(self, n_thermo):
+        self._call("set_thermo", ctypes.c_int(n_thermo))
+
+    def thermo_records(self, max_records=100000):
+        """(i_step, pressure tensor (k, 9), pressure, volume) of the records
+        taken since the last call."""
+        getattr(self.lib, self.prefix + "thermo_records").restype = ctypes.c_long
+        st = np.zeros(max_records, dtype=np.int64)
+        P = np.zeros((max_records, 9))
+        p = np.zeros(max_records)
+        V = np.zeros(max_records)
+        n = self._call("thermo_records", ctypes.c_long(max_records), _ptr(st), _ptr(P), _ptr(p),
+                       _ptr(V))
+        return st[:n], P[:n], p[:n], V[:n]
+
+    def stress(self):
+        a = np.zeros(9)
+        self._call("get_stress", _ptr(a))
+        return a
+
+    def potential_energy(self):
+        a = np.zeros(self.n_fil)
+        self._call("get_potential_energy", _ptr(a))
+        return a
+
 
 class Oracle(_Checker):
     """The plain-C restatement (always available once built)."""

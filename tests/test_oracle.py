@@ -263,3 +263,67 @@ def test_explicit_bending_stability_limit(lp, dt, stable):
         assert abs(c - wlc) < 1e-3, (c, wlc)
     else:
         assert c < 0.9, (c, wlc)
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build not present")
+@pytest.mark.parametrize("n_dim", [3, 2])
+def test_thermo_and_potentials_match_reference(n_dim):
+    """The pair virial the reference sums every step (ApplyPairInteractions),
+    its pressure records every n_thermo steps (CalculatePressure, with the
+    Space's volume and the interactor count) and every filament's potential
+    energy: oracle and the reference's own code bit for bit, over runs with
+    rebuilds."""
+    import simcore_b200 as sc
+    n_fil, n_seg, R = (25, 12, 14.0) if n_dim == 3 else (30, 14, 22.0)
+    nb = np.full(n_fil, n_seg, dtype=np.int32)
+    sites = sc.insert_filaments(n_dim, R, 99 + n_dim, nb, nb.astype(float), np.full(n_fil, 50.0))
+    system = dict(n_dim=n_dim, system_radius=R, delta=2e-4, seed=7)
+    fils = [dict(length=float(n_seg), persistence_length=50.0, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * n_fil
+    o = Oracle(system, fils, sites)
+    r = Reference(system, fils, sites, n_threads=2)
+    o.set_thermo(6)
+    r.set_thermo(6)
+    n_rec = 0
+    for _ in range(10):
+        o.step(9)
+        r.step(9)
+        a, b = o.thermo_records(), r.thermo_records()
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+        n_rec += len(a[0])
+        assert np.array_equal(o.stress(), r.stress())
+        assert np.array_equal(o.potential_energy(), r.potential_energy())
+    assert n_rec == 90 // 6 and o.n_rebuilds > 1
+    assert (o.potential_energy() > 0).any()
+    o.close()
+    r.close()
+
+
+def test_ideal_pressure_without_contacts():
+    """Two two-bond rods (bond length 3, so a rod's only bond pair is
+    adjacent and excluded) far apart, no noise: no pair is in range, so the
+    pressure tensor is the ideal n_bonds / V on the diagonal and the
+    potentials are zero."""
+    import simcore_b200 as sc
+    R = 20.0
+    fils = [dict(length=6.0, persistence_length=100.0, diameter=1.0, min_bond_length=2.0,
+                 friction_ratio=2.0)] * 2
+    assert sc.filament_n_bonds(fils[0]) == 2
+    sites = np.zeros((6, 3))
+    sites[:3, 0] = [-3.0, 0.0, 3.0]
+    sites[3:, 0] = [-3.0, 0.0, 3.0]
+    sites[3:, 1] = 10.0
+    system = dict(n_dim=3, system_radius=R, delta=1e-4, seed=1, stoch_flag=0)
+    o = Oracle(system, fils, sites)
+    o.set_thermo(2)
+    o.step(4)
+    st, P, p, V = o.thermo_records()
+    assert list(st) == [2, 4]
+    ideal = 4 * (1.0 / (2 * R) ** 3)
+    assert np.array_equal(V, np.full(2, (2 * R) ** 3))
+    assert np.array_equal(P[:, [0, 4, 8]], np.full((2, 3), ideal))
+    assert not P[:, [1, 2, 3, 5, 6, 7]].any()
+    assert np.array_equal(p, np.full(2, (ideal + ideal + ideal) / 3))
+    assert not o.potential_energy().any()
+    o.close()
