@@ -170,6 +170,30 @@ sc_status sc_analysis_sample(sc_ctx *ctx, int n_bins);
 sc_status sc_analysis_results(sc_ctx *ctx, double *mse2e, double *mse2e_err, int64_t *n_samples,
                               int32_t *max_joints, int64_t *theta_hist);
 sc_status sc_global_order(sc_ctx *ctx, double *polar, double *nematic);
+/* Thermo (InteractionManager::CalculatePressure, src/interaction_manager.cpp:
+ * 500-517, 535-559, called by Simulation::Statistics every n_thermo steps).
+ * sc_set_thermo(ctx, n) makes every step add its pairs' virial -dr x F (each
+ * pair's values from its last evaluation, like its force) to a per-system
+ * sum, and every step with i_step % n == 0 record the pressure tensor
+ * n_bonds/V I + sum/(V n) and the pressure (its trace / n_dim) and reset the
+ * sum; the sums start when it is called (call it before the first step for
+ * the reference's values) and run inside captured runs too.  n = 0 stops
+ * them.  The sums are summed in a fixed order other than the reference's
+ * serial one (agreement to rounding; the same bits on every run).
+ * sc_thermo_open writes <run_name>.thermo (<run_name>_rNNN.thermo per
+ * system) as OutputManager::InitThermo/WriteThermo do: header n_steps,
+ * n_thermo, delta, n_dim; per record unit cell (9), pressure tensor (9),
+ * pressure, volume.  sc_get_thermo returns and removes up to max_records
+ * records: i_step (per record), tensor (9 per record and system, n_dim x
+ * n_dim packed), pressure and volume (per record and system); any pointer
+ * but n_records may be NULL.  sc_get_potential_energy gives every
+ * filament's potential energy of the last pair stage (Object::
+ * GetPotentialEnergy: its bonds' pair potentials), with thermo on. */
+sc_status sc_set_thermo(sc_ctx *ctx, int n_thermo);
+sc_status sc_thermo_open(sc_ctx *ctx, const char *run_name, int n_steps);
+sc_status sc_get_thermo(sc_ctx *ctx, int max_records, int *n_records, int64_t *i_step,
+                        double *tensor, double *pressure, double *volume);
+sc_status sc_get_potential_energy(sc_ctx *ctx, double *pote);
 /* Per-system rebuild counts and current pair counts (n_replicas entries
  * each; either pointer may be NULL). */
 sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);

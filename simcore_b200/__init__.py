@@ -36,7 +36,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_get_crosslink_forces", "sc_set_integrator_layout", "sc_autotune",
             "sc_add_replicas", "sc_get_replica_counters", "sc_checkpoint", "sc_restore",
             "sc_set_noise_key", "sc_output_open", "sc_output_write", "sc_output_close",
-            "sc_analysis_sample", "sc_analysis_results", "sc_global_order"]
+            "sc_analysis_sample", "sc_analysis_results", "sc_global_order",
+            "sc_set_thermo", "sc_thermo_open", "sc_get_thermo", "sc_get_potential_energy"]
 
 
 class ScError(RuntimeError):
@@ -369,6 +370,38 @@ class Context:
         q = np.zeros((R, 9))
         self._check(lib.sc_global_order(self.h, _p(p), _p(q)))
         return p, q
+
+    def set_thermo(self, n_thermo):
+        """Pair virial sums every step and a pressure record every n_thermo
+        steps (0: off)."""
+        self._check(lib.sc_set_thermo(self.h, int(n_thermo)))
+
+    def thermo_open(self, run_name, n_steps):
+        """Writes the records from now on to <run_name>.thermo."""
+        self._check(lib.sc_thermo_open(self.h, run_name.encode(), int(n_steps)))
+
+    def thermo_records(self, max_records=100000):
+        """(i_step (k), pressure tensor (k, systems, 9), pressure (k, systems),
+        volume (k, systems)) of the records since the last call; a single
+        system's arrays drop the systems axis."""
+        R = self.n_replicas
+        st = np.zeros(max_records, dtype=np.int64)
+        P = np.zeros((max_records, R, 9))
+        p = np.zeros((max_records, R))
+        V = np.zeros((max_records, R))
+        n = ctypes.c_int(0)
+        self._check(lib.sc_get_thermo(self.h, int(max_records), ctypes.byref(n), _p(st), _p(P),
+                                      _p(p), _p(V)))
+        k = n.value
+        if R == 1:
+            return st[:k], P[:k, 0], p[:k, 0], V[:k, 0]
+        return st[:k], P[:k], p[:k], V[:k]
+
+    def potential_energy(self):
+        """Potential energy of every filament of the last pair stage."""
+        out = np.zeros(self.n_fil)
+        self._check(lib.sc_get_potential_energy(self.h, _p(out)))
+        return out
 
     def replica_counters(self):
         """(rebuilds, pairs) per system."""

@@ -108,6 +108,13 @@ struct sc_ctx {
   cudaEvent_t gev0 = nullptr, gev1 = nullptr;  // around each graph launch
   double graph_ms = 0.0;
   long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
+
+  // thermo (sc_set_thermo): records are produced on the device every th_n
+  // steps and pulled into th_host (and the open .thermo files)
+  long long th_i0 = 0;            // i_step when the records started
+  long long th_pulled = 0;        // records copied to the host
+  std::vector<double> th_host;    // pulled, not yet returned: per record nrep x 12
+  std::vector<FILE *> th_files;   // per system, while a .thermo file is open
 };
 
 namespace {
@@ -214,6 +221,8 @@ sc_status readback(sc_ctx *c) {
   return check_status(c);
 }
 
+constexpr int kThermoMaxBlocks = 296;  // two per SM
+
 void drop_graph(sc_ctx *c) {
   if (c->graph_exec) {
     cudaGraphExecDestroy(c->graph_exec);
@@ -234,6 +243,10 @@ sc_status upload_reps(sc_ctx *c) {
                      sizeof(sc::ReplicaConst) * nrep, cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   c->d.pcap_total = (int)c->pcap;
+  // Thermo blocks per system: one per 2,048 slots of the largest segment.
+  int maxcap = 0;
+  for (const auto &R : c->reps) maxcap = std::max(maxcap, R.pcap);
+  c->d.th_gx = std::max(1, std::min(kThermoMaxBlocks, (maxcap + 2047) / 2048));
   drop_graph(c);  // kernel parameters changed
   return SC_OK;
 }
@@ -241,8 +254,23 @@ sc_status upload_reps(sc_ctx *c) {
 void free_pair_storage(sc_ctx *c) {
   for (void *q : {(void *)c->d.pa, (void *)c->d.pb, (void *)c->d.pos1, (void *)c->d.pos2,
                   (void *)c->d.pf64, (void *)c->d.pf32, (void *)c->d.cf64, (void *)c->d.cf32,
-                  (void *)c->d.e_ent})
+                  (void *)c->d.e_ent, (void *)c->d.pv64, (void *)c->d.pv32})
     dfree(c, q);
+  c->d.pv64 = nullptr;
+  c->d.pv32 = nullptr;
+}
+
+// Per-pair virial records for `total` slots, zeroed (a pair not evaluated
+// since the list was built has stress and potential 0).
+sc_status alloc_pair_records(sc_ctx *c, long long total) {
+  if (c->prec == 0) {
+    CKS(dalloc(c, &c->d.pv64, 4 * total));
+    CK(cudaMemsetAsync(c->d.pv64, 0, sizeof(double) * 4 * (total ? total : 1), c->st));
+  } else {
+    CKS(dalloc(c, &c->d.pv32, 4 * total));
+    CK(cudaMemsetAsync(c->d.pv32, 0, sizeof(float) * 4 * (total ? total : 1), c->st));
+  }
+  return SC_OK;
 }
 
 // Pair storage for segments of the given capacities, one per system, back
@@ -271,6 +299,7 @@ sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
     CK(cudaMemsetAsync(d.cf32, 0, sizeof(float) * 16 * total, c->st));
   }
   CKS(dalloc(c, &d.e_ent, 2 * total));
+  if (c->k.thermo) CKS(alloc_pair_records(c, total));
   long long p0 = 0;
   for (size_t r = 0; r < caps.size(); ++r) {
     c->reps[r].p0 = (int)p0;
@@ -309,6 +338,17 @@ sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
     CK(cudaMemsetAsync(cf32, 0, sizeof(float) * 16 * cap, c->st));
   }
   CKS(dalloc(c, &ent, 2 * cap));
+  double *pv64 = nullptr;
+  float *pv32 = nullptr;
+  if (c->k.thermo) {
+    if (c->prec == 0) {
+      CKS(dalloc(c, &pv64, 4 * cap));
+      CK(cudaMemsetAsync(pv64, 0, sizeof(double) * 4 * cap, c->st));
+    } else {
+      CKS(dalloc(c, &pv32, 4 * cap));
+      CK(cudaMemsetAsync(pv32, 0, sizeof(float) * 4 * cap, c->st));
+    }
+  }
   if (keep > 0) {
     auto cp = [&](void *dst, const void *src, size_t bytes) {
       return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->st);
@@ -325,9 +365,13 @@ sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
       CK(cp(cf32, old.cf32, sizeof(float) * 16 * keep));
     }
     CK(cp(ent, old.e_ent, sizeof(int) * 2 * keep));
+    if (pv64 && old.pv64) CK(cp(pv64, old.pv64, sizeof(double) * 4 * keep));
+    if (pv32 && old.pv32) CK(cp(pv32, old.pv32, sizeof(float) * 4 * keep));
   }
   CK(cudaStreamSynchronize(c->st));
   free_pair_storage(c);
+  d.pv64 = pv64;
+  d.pv32 = pv32;
   d.pa = pa;
   d.pb = pb;
   d.pos1 = pos1;
@@ -548,15 +592,84 @@ void tether_if_due(sc_ctx *c) {
     c->launches += sc::launch_tether(c->k, c->d, c->st);
 }
 
+// ---- thermo ----------------------------------------------------------------
+
+// Records the device has produced by step i (one every th_n steps since th_i0).
+long long thermo_total(const sc_ctx *c, long long i) {
+  const long long n = c->d.th_n;
+  return n > 0 ? i / n - c->th_i0 / n : 0;
+}
+
+// One record of every system as OutputManager::WriteThermo writes it
+// (include/simcore/output_manager.hpp:169-183): unit cell (9), pressure
+// tensor (9), pressure, volume.
+void thermo_write(sc_ctx *c, const double *rec) {
+  for (size_t r = 0; r < c->th_files.size(); ++r) {
+    FILE *f = c->th_files[r];
+    if (!f) continue;
+    const double *q = rec + 12 * r;
+    std::fwrite(c->reps[r].h, sizeof(double), 9, f);
+    std::fwrite(q + 1, sizeof(double), 11, f);
+  }
+}
+
+// Copies the records produced so far from the device ring to th_host (and
+// the open files).
+sc_status thermo_pull(sc_ctx *c) {
+  if (c->d.th_n <= 0 || !c->d.th_rec) return SC_OK;
+  const long long tot = thermo_total(c, c->i_step);
+  if (tot <= c->th_pulled) return SC_OK;
+  const size_t per = 12 * (size_t)c->d.nrep;
+  std::vector<double> ring(per * (size_t)c->d.th_cap);
+  CK(cudaMemcpyAsync(ring.data(), c->d.th_rec, sizeof(double) * ring.size(),
+                     cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (long long k = c->th_pulled; k < tot; ++k) {
+    const double *rec = ring.data() + per * (size_t)(k % c->d.th_cap);
+    c->th_host.insert(c->th_host.end(), rec, rec + per);
+    thermo_write(c, rec);
+  }
+  c->th_pulled = tot;
+  return SC_OK;
+}
+
+// Room in the device ring for the records of the next n steps: pulls the
+// pending ones, and grows the ring when n steps alone would overrun it.
+sc_status thermo_reserve(sc_ctx *c, long long n) {
+  if (!c->k.thermo) return SC_OK;
+  const long long after = thermo_total(c, c->i_step + n);
+  if (after - c->th_pulled <= c->d.th_cap) return SC_OK;
+  CKS(thermo_pull(c));
+  const long long need = after - c->th_pulled;
+  if (need <= c->d.th_cap) return SC_OK;
+  // Everything produced is pulled: the ring holds nothing live.
+  const long long cap = need + need / 2;
+  if (cap > (1ll << 24)) return fail(c, SC_ERR_INVALID_ARG, "%lld thermo records in one run", need);
+  double *ring = nullptr;
+  CKS(dalloc(c, &ring, 12 * (size_t)c->d.nrep * cap));
+  dfree(c, c->d.th_rec);
+  c->d.th_rec = ring;
+  c->d.th_cap = (int)cap;
+  drop_graph(c);
+  return SC_OK;
+}
+
+// The pair stage of one step, then the step's thermo accumulation.
+sc_status pair_stage(sc_ctx *c) {
+  CKS(timed(c, [&] {
+    return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st);
+  }));
+  if (c->k.thermo) c->launches += sc::launch_thermo(c->k, c->d, c->prec, c->st);
+  return SC_OK;
+}
+
 sc_status step_once(sc_ctx *c) {
+  CKS(thermo_reserve(c, 1));
   c->i_step++;
   tether_if_due(c);
   CKS(maybe_rebuild(c));
   const int interaction = c->desc.interaction_flag ? 1 : 0;
-  if (interaction)
-    CKS(timed(c, [&] {
-      return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st);
-    }));
+  if (interaction) CKS(pair_stage(c));
   CKS(timed(c, [&] {
     return sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep, c->rbuf,
                                 interaction, c->capture, c->prec, c->fast, c->st);
@@ -675,6 +788,8 @@ sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
   k.c12f = (float)k.c12;
   k.c6f = (float)k.c6;
   k.fcutf = (float)k.fcut;
+  k.eps = desc->wca_eps;
+  k.epsf = (float)desc->wca_eps;
   k.stoch = desc->stoch_flag ? 1 : 0;
   k.like_like = desc->like_like_interactions ? 1 : 0;
   CK(cudaMalloc((void **)&c->d.status, sizeof(unsigned)));
@@ -702,6 +817,12 @@ sc_status sc_destroy(sc_ctx *c) {
   cudaSetDevice(c->desc.device);
   if (c->st) cudaStreamSynchronize(c->st);
   if (c->out.open) sc_output_close(c);
+  if (!c->th_files.empty()) {
+    thermo_pull(c);
+    for (FILE *f : c->th_files)
+      if (f) std::fclose(f);
+    c->th_files.clear();
+  }
   drop_graph(c);
   for (void *p : c->allocs) cudaFree(p);
   if (c->hb) cudaFreeHost(c->hb);
@@ -1015,13 +1136,11 @@ sc_status sc_interact(sc_ctx *c) {
   if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
   CK(cudaSetDevice(c->desc.device));
   // ZeroForces + Interact of the next step.
+  CKS(thermo_reserve(c, 1));
   c->i_step++;
   tether_if_due(c);
   CKS(maybe_rebuild(c));
-  if (c->desc.interaction_flag)
-    CKS(timed(c, [&] {
-      return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st);
-    }));
+  if (c->desc.interaction_flag) CKS(pair_stage(c));
   CK(cudaGetLastError());
   c->pairs_ready = true;
   return SC_OK;
@@ -1112,6 +1231,7 @@ static sc_status build_graph(sc_ctx *c) {
     // The second half is the even (full) step: crosslink tethers first.
     if (half == 1 && interaction) sc::launch_tether(c->k, c->d, c->st);
     if (interaction) sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st);
+    if (interaction && c->k.thermo) sc::launch_thermo(c->k, c->d, c->prec, c->st);
     sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
                          c->capture, c->prec, c->fast, c->st);
   }
@@ -1138,6 +1258,7 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
   }
   int bd = n / 2;
   if (bd > 0) {
+    CKS(thermo_reserve(c, 2 * (long long)bd));
     // The list must have room to grow by half before a captured run.
     CKS(sync_pair_count(c));
     if (c->reps.size() == 1 && c->np + c->np / 2 > c->pcap)
@@ -1180,7 +1301,9 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       // Kernels the graph ran: loop head, per BD step decide + 2 steps +
       // tail (the stopped step's too), per rebuild the captured sequence.
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) *
-                             (c->desc.interaction_flag ? (c->d.nx ? 7 : 6) : 3) +
+                             (c->desc.interaction_flag
+                                  ? (c->d.nx ? 7 : 6) + (c->k.thermo ? 2 : 0)
+                                  : 3) +
                      (nr1 - nr0) * c->rebuild_kernels;
       bd -= done;
       if (!overflow) {
@@ -1482,6 +1605,12 @@ std::vector<Region> state_regions(sc_ctx *c) {
     v.push_back({d.xl_c, sizeof(double) * 16 * (size_t)d.nx});
     v.push_back({d.xl_F, sizeof(double) * 4 * (size_t)d.nx});
   }
+  if (c->k.thermo) {  // pair virial records and the running virial sums
+    if (c->prec == 0) v.push_back({d.pv64, sizeof(double) * 4 * P});
+    else v.push_back({d.pv32, sizeof(float) * 4 * P});
+    v.push_back({d.th_acc, sizeof(double) * 9 * nrep});
+    v.push_back({d.th_istep, sizeof(long long) * nrep});
+  }
   return v;
 }
 }  // namespace
@@ -1575,6 +1704,13 @@ sc_status sc_restore(sc_ctx *c, const void *buf, size_t size) {
   c->mcount = h.mcount;
   c->midstep = h.midstep;
   c->pairs_ready = false;
+  if (c->k.thermo) {  // records restart from the restored step
+    CK(cudaMemsetAsync(c->d.th_nrec, 0, sizeof(long long) * c->d.nrep, c->st));
+    CK(cudaMemsetAsync(c->d.th_ticket, 0, sizeof(unsigned) * c->d.nrep, c->st));
+    c->th_i0 = c->i_step;
+    c->th_pulled = 0;
+    c->th_host.clear();
+  }
   // The FP64 record of mixed precision serves only the geometry getter.
   if (c->prec != 0) sc::launch_init_geometry(c->k, c->d, 0, 0, c->st, false);
   CK(cudaGetLastError());
@@ -1934,6 +2070,109 @@ sc_status sc_get_pairs(sc_ctx *c, int32_t *pairs, int64_t cap, int64_t *n_pairs)
       pairs[2 * out + 1] = b[i];
     }
   }
+  return SC_OK;
+}
+
+// ---- thermo ----------------------------------------------------------------
+
+sc_status sc_set_thermo(sc_ctx *c, int n_thermo) {
+  if (!c || !c->loaded || n_thermo < 0) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  DevState &d = c->d;
+  const int nrep = d.nrep;
+  if (c->k.thermo) CKS(thermo_pull(c));
+  if (n_thermo == 0) {
+    for (FILE *f : c->th_files)
+      if (f) std::fclose(f);
+    c->th_files.clear();
+    c->k.thermo = 0;
+    d.th_n = 0;
+    drop_graph(c);
+    return SC_OK;
+  }
+  if (!c->desc.interaction_flag)
+    return fail(c, SC_ERR_INVALID_ARG, "thermo needs pair interactions");
+  if (!d.th_part) {
+    CKS(dalloc(c, &d.th_part, (size_t)nrep * kThermoMaxBlocks * 9));
+    CKS(dalloc(c, &d.th_ticket, nrep));
+    CKS(dalloc(c, &d.th_acc, 9 * (size_t)nrep));
+    CKS(dalloc(c, &d.th_istep, nrep));
+    CKS(dalloc(c, &d.th_nrec, nrep));
+    d.th_cap = 256;
+    CKS(dalloc(c, &d.th_rec, 12 * (size_t)nrep * d.th_cap));
+  }
+  if (!(c->prec == 0 ? (void *)d.pv64 : (void *)d.pv32)) CKS(alloc_pair_records(c, c->pcap));
+  std::vector<long long> ist(nrep, c->i_step);
+  CK(cudaMemsetAsync(d.th_ticket, 0, sizeof(unsigned) * nrep, c->st));
+  CK(cudaMemsetAsync(d.th_acc, 0, sizeof(double) * 9 * nrep, c->st));
+  CK(cudaMemsetAsync(d.th_nrec, 0, sizeof(long long) * nrep, c->st));
+  CK(cudaMemcpyAsync(d.th_istep, ist.data(), sizeof(long long) * nrep, cudaMemcpyHostToDevice,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->th_i0 = c->i_step;
+  c->th_pulled = 0;
+  d.th_n = n_thermo;
+  c->k.thermo = 1;
+  drop_graph(c);
+  return SC_OK;
+}
+
+sc_status sc_thermo_open(sc_ctx *c, const char *run_name, int n_steps) {
+  if (!c || !c->loaded || !run_name || n_steps < 0) return SC_ERR_INVALID_ARG;
+  if (!c->k.thermo) return fail(c, SC_ERR_INVALID_ARG, "thermo is off");
+  if (!c->th_files.empty()) return fail(c, SC_ERR_INVALID_ARG, "thermo file already open");
+  CK(cudaSetDevice(c->desc.device));
+  CKS(thermo_pull(c));  // records taken before the file opened stay out of it
+  const size_t nrep = c->reps.size();
+  c->th_files.assign(nrep, nullptr);
+  for (size_t r = 0; r < nrep; ++r) {
+    std::string name = run_name;
+    if (nrep > 1) {
+      char sfx[32];
+      std::snprintf(sfx, sizeof(sfx), "_r%03zu", r);
+      name += sfx;
+    }
+    name += ".thermo";
+    FILE *f = std::fopen(name.c_str(), "wb");
+    if (!f) return fail(c, SC_ERR_INVALID_ARG, "cannot open %s", name.c_str());
+    // OutputManager::InitThermo (include/simcore/output_manager.hpp:156-168)
+    put(f, (int32_t)n_steps);
+    put(f, (int32_t)c->d.th_n);
+    put(f, c->desc.delta);
+    put(f, (int32_t)c->nd);
+    c->th_files[r] = f;
+  }
+  return SC_OK;
+}
+
+sc_status sc_get_thermo(sc_ctx *c, int max_records, int *n_records, int64_t *i_step,
+                        double *tensor, double *pressure, double *volume) {
+  if (!c || !c->loaded || max_records < 0 || !n_records) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  CKS(thermo_pull(c));
+  const size_t nrep = c->reps.size(), per = 12 * nrep;
+  const size_t n = std::min(c->th_host.size() / per, (size_t)max_records);
+  for (size_t k = 0; k < n; ++k)
+    for (size_t r = 0; r < nrep; ++r) {
+      const double *q = c->th_host.data() + per * k + 12 * r;
+      if (i_step && r == 0) i_step[k] = (int64_t)q[0];
+      if (tensor) std::memcpy(tensor + 9 * (k * nrep + r), q + 1, sizeof(double) * 9);
+      if (pressure) pressure[k * nrep + r] = q[10];
+      if (volume) volume[k * nrep + r] = q[11];
+    }
+  c->th_host.erase(c->th_host.begin(), c->th_host.begin() + per * n);
+  *n_records = (int)n;
+  return SC_OK;
+}
+
+sc_status sc_get_potential_energy(sc_ctx *c, double *pote) {
+  if (!c || !c->loaded || !pote) return SC_ERR_INVALID_ARG;
+  if (!c->k.thermo) return fail(c, SC_ERR_INVALID_ARG, "potential energies need thermo on");
+  CK(cudaSetDevice(c->desc.device));
+  c->launches += sc::launch_potential(c->d, c->prec, c->stage, c->st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(pote, c->stage, sizeof(double) * c->nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
   return SC_OK;
 }
 

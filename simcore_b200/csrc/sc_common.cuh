@@ -62,6 +62,9 @@ struct SysConst {
   int stoch;
   int like_like;
   double xk, xkc, xrest;  // crosslink tether: k_spring, k_spring_compress, rest_length
+  double eps;             // WCA epsilon (the potential's shift)
+  float epsf;
+  int thermo;             // pair virial and potential records kept
 };
 
 // One independent periodic system (a replica) of a context: its box, cell
@@ -143,6 +146,17 @@ struct DevState {
   int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
   double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
   float *cf32;
+  // thermo (kept while SysConst::thermo is set): per pair the dr its stress
+  // was computed from and its potential, stored with the force
+  double *pv64;            // 4 per pair: dr (3), pote
+  float *pv32;
+  double *th_part;         // per system, th_gx partial virials of 9
+  unsigned *th_ticket;     // per system: blocks done in the current launch
+  double *th_acc;          // per system: accumulated virial (9)
+  long long *th_istep;     // per system: steps accumulated (the reference's i_step)
+  long long *th_nrec;      // per system: records written
+  double *th_rec;          // ring of th_cap records per system: i_step, tensor (9), pressure, volume
+  int th_cap, th_gx, th_n;
   // static crosslinks (harmonic tethers between two bonds)
   int nx;                  // links
   const int *xl_anchor;    // 2 per link: bond << 1 | head (anchor at the bond's head)

@@ -257,8 +257,14 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
         double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)g;
         st[0] = make_double2(0.0, 0.0);
         st[1] = make_double2(0.0, 0.0);
+        if (d.pv64) {  // a new Interaction's stress and potential are 0
+          double2 *v = reinterpret_cast<double2 *>(d.pv64) + 2 * (size_t)g;
+          v[0] = make_double2(0.0, 0.0);
+          v[1] = make_double2(0.0, 0.0);
+        }
       } else {
         reinterpret_cast<float4 *>(d.pf32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (d.pv32) reinterpret_cast<float4 *>(d.pv32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       atomicAdd(&deg[a], 1);
       atomicAdd(&deg[b], 1);
@@ -471,8 +477,8 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     const double2 st0 = stale[0], st1 = stale[1];
     PairGeom<double> g;
     sphero_f64<ND>(R.h, A, B, g);
-    double force[3];
-    if (!wca_f64<ND>(k, g, force)) {
+    double force[3], rec[4];
+    if (!wca_f64<ND>(k, g, force, k.thermo ? rec : nullptr)) {
       force[0] = st0.x;
       force[1] = st0.y;
       force[2] = st1.x;
@@ -480,6 +486,11 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
       if (ND == 2) force[2] = st1.x;
       stale[0] = make_double2(force[0], force[1]);
       stale[1] = make_double2(force[2], 0.0);
+      if (k.thermo) {
+        double2 *v = reinterpret_cast<double2 *>(d.pv64) + 2 * (size_t)p;
+        v[0] = make_double2(rec[0], rec[1]);
+        v[1] = make_double2(rec[2], rec[3]);
+      }
     }
     double t1[3], t2[3];
     cross3(g.c1, force, t1);
@@ -498,14 +509,16 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     const float4 st = *stale;
     PairGeom<float> g;
     sphero_f32<ND>(R.hf, A, B, g);
-    float force[3];
-    if (!wca_f32<ND>(k, g, force)) {
+    float force[3], rec[4];
+    if (!wca_f32<ND>(k, g, force, k.thermo ? rec : nullptr)) {
       force[0] = st.x;
       force[1] = st.y;
       force[2] = st.z;
     } else {
       if (ND == 2) force[2] = st.z;
       *stale = make_float4(force[0], force[1], force[2], 0.f);
+      if (k.thermo)
+        reinterpret_cast<float4 *>(d.pv32)[p] = make_float4(rec[0], rec[1], rec[2], rec[3]);
     }
     float t1[3] = {g.c1[1] * force[2] - g.c1[2] * force[1],
                    g.c1[2] * force[0] - g.c1[0] * force[2],
@@ -1016,6 +1029,154 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
     if (prec == 0) k_pair_eval<2, 0><<<grid, 256, 0, st>>>(k, d, rbuf);
     else k_pair_eval<2, 1><<<grid, 256, 0, st>>>(k, d, rbuf);
   }
+  return 1;
+}
+
+// ---------------------------------------------------------------------------
+// Thermo.  One launch per step after the pair stage, while thermo is on.
+// Every live pair's stress -dr x F from its record (the values of its last
+// evaluation, like its force: src/minimum_distance.cpp:31-34 resets neither)
+// is summed per system -- ApplyPairInteractions' stress_ += ix->stress
+// (src/interaction_manager.cpp:511-516) -- and, every th_n steps,
+// CalculatePressure (src/interaction_manager.cpp:535-559) turns the sum into
+// the pressure tensor and pressure of the periodic box (volume (2R)^d,
+// src/space.cpp:252-264; n_objs = the system's bond count, src/mesh.cpp:399)
+// and resets it.  Grid (th_gx, systems): each block sums a fixed stride of
+// its system's pairs and reduces in a fixed order; the last block of a
+// system (ticket counter, no waiting) adds the block sums in block order.
+// The sum order differs from the reference's serial one, so the result
+// agrees to rounding, and is the same on every run.
+template <int ND, int PREC>
+__global__ void __launch_bounds__(256) k_thermo(SysConst k, DevState d) {
+  if (*d.status & ST_LIST_OVERFLOW) return;  // the step stopped at its rebuild
+  const int r = blockIdx.y;
+  const ReplicaConst &R = d.rep[r];
+  const int np = min(d.np_rep[r], R.pcap);
+  double s[ND * ND];
+#pragma unroll
+  for (int c = 0; c < ND * ND; ++c) s[c] = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+    const size_t p = (size_t)R.p0 + q;
+    double F[3], dr[3];
+    if (PREC == 0) {
+      const double2 *f = reinterpret_cast<const double2 *>(d.pf64) + 2 * p;
+      const double2 *v = reinterpret_cast<const double2 *>(d.pv64) + 2 * p;
+      const double2 f0 = f[0], f1 = f[1], v0 = v[0], v1 = v[1];
+      F[0] = f0.x;
+      F[1] = f0.y;
+      F[2] = f1.x;
+      dr[0] = v0.x;
+      dr[1] = v0.y;
+      dr[2] = v1.x;
+    } else {
+      const float4 f = reinterpret_cast<const float4 *>(d.pf32)[p];
+      const float4 v = reinterpret_cast<const float4 *>(d.pv32)[p];
+      F[0] = f.x;
+      F[1] = f.y;
+      F[2] = f.z;
+      dr[0] = v.x;
+      dr[1] = v.y;
+      dr[2] = v.z;
+    }
+#pragma unroll
+    for (int i = 0; i < ND; ++i)
+#pragma unroll
+      for (int j = 0; j < ND; ++j) s[ND * i + j] += -dr[i] * F[j];
+  }
+  __shared__ double red[8][ND * ND];
+  __shared__ int last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < ND * ND; ++c) {
+    double v = s[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][c] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double *part = d.th_part + ((size_t)r * gridDim.x + blockIdx.x) * 9;
+    for (int c = 0; c < ND * ND; ++c) {
+      double v = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[w][c];
+      part[c] = v;
+    }
+    __threadfence();
+    last = atomicAdd(&d.th_ticket[r], 1u) == gridDim.x - 1 ? 1 : 0;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  const volatile double *part = d.th_part + (size_t)r * gridDim.x * 9;
+  double *acc = d.th_acc + 9 * (size_t)r;
+  for (int c = 0; c < ND * ND; ++c) {
+    double v = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) v += part[(size_t)b * 9 + c];
+    acc[c] += v;
+  }
+  d.th_ticket[r] = 0u;
+  const long long istep = ++d.th_istep[r];
+  if (d.th_n <= 0 || istep % d.th_n != 0) return;
+  const double side = R.h[0];
+  const double volume = ND == 2 ? side * side : side * side * side;
+  const double inv_V = 1.0 / volume;
+  double P[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < ND; ++i)
+    for (int j = 0; j < ND; ++j) {
+      if (i == j) P[ND * i + j] += R.nb * inv_V;
+      P[ND * i + j] += acc[ND * i + j] * inv_V / d.th_n;
+    }
+  double pressure = 0;
+  for (int i = 0; i < ND; ++i) pressure += P[ND * i + i];
+  pressure /= ND;
+  for (int c = 0; c < 9; ++c) acc[c] = 0.0;
+  const long long n = d.th_nrec[r]++;
+  double *rec = d.th_rec + ((size_t)(n % d.th_cap) * d.nrep + r) * 12;
+  rec[0] = (double)istep;
+  for (int c = 0; c < 9; ++c) rec[1 + c] = P[c];
+  rec[10] = pressure;
+  rec[11] = volume;
+}
+
+// Object::GetPotentialEnergy of every filament after the last pair stage:
+// Filament::ApplyInteractionForces adds its bonds' potentials in bond order
+// (src/filament.cpp:1007), each bond's the potentials of its pairs in list
+// order (obj1/obj2->AddPotential, src/interaction_manager.cpp:509-510) --
+// the order of its entries, which are sorted by pair.
+template <int PREC>
+__global__ void k_potential(DevState d, double *out) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const FilConst fc = d.fil[f];
+  const int b0 = fc.site0 - f;
+  double e = 0.0;
+  for (int i = 0; i < fc.n - 1; ++i) {
+    const int b = b0 + i;
+    double bp = 0.0;
+    for (int q = d.e_off[b], q1 = q + d.e_cnt[b]; q < q1; ++q) {
+      const size_t p = (size_t)(d.e_ent[q] >> 1);
+      bp += PREC == 0 ? d.pv64[4 * p + 3] : (double)d.pv32[4 * p + 3];
+    }
+    e += bp;
+  }
+  out[f] = e;
+}
+
+int launch_thermo(const SysConst &k, const DevState &d, int prec, cudaStream_t st) {
+  const dim3 grid(d.th_gx, d.nrep);
+  if (k.n_dim == 3) {
+    if (prec == 0) k_thermo<3, 0><<<grid, 256, 0, st>>>(k, d);
+    else k_thermo<3, 1><<<grid, 256, 0, st>>>(k, d);
+  } else {
+    if (prec == 0) k_thermo<2, 0><<<grid, 256, 0, st>>>(k, d);
+    else k_thermo<2, 1><<<grid, 256, 0, st>>>(k, d);
+  }
+  return 1;
+}
+
+int launch_potential(const DevState &d, int prec, double *out, cudaStream_t st) {
+  if (prec == 0) k_potential<0><<<cdiv(d.nf, 128), 128, 0, st>>>(d, out);
+  else k_potential<1><<<cdiv(d.nf, 128), 128, 0, st>>>(d, out);
   return 1;
 }
 

@@ -62,6 +62,11 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
                  int expected, cudaStream_t st);
 // Crosslink tethers of an even step into the per-anchor contributions.
 int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st);
+// Thermo: one step's pair virial per system, the pressure record every
+// th_n steps (grid th_gx x systems).
+int launch_thermo(const SysConst &k, const DevState &d, int prec, cudaStream_t st);
+// Potential energy of every filament from the pair records.
+int launch_potential(const DevState &d, int prec, double *out, cudaStream_t st);
 int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st);
 size_t integrate_smem_bytes(int C);
 void prepare_integrate(int C);

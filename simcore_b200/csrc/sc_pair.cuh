@@ -128,10 +128,14 @@ __device__ __forceinline__ void sphero_f64(const double *h,
 // Evaluates the pair's potential if it is in range.  Returns true and
 // writes force when a potential set the force; returns false when the
 // reference leaves the pair's previous force in place (out of range, or
-// the max-force fallback finds no direction).
+// the max-force fallback finds no direction).  When rec is given, a true
+// return also writes the dr the pair's stress uses (the contact difference
+// in the max-force case) and the potential (0 there) into rec[0..3]
+// (Interaction::dr, pote; include/simcore/wca_potential.hpp:26-31,
+// include/simcore/max_force_potential.hpp:15-39).
 template <int ND>
 __device__ __forceinline__ bool wca_f64(const SysConst &k, PairGeom<double> &g,
-                                        double force[3]) {
+                                        double force[3], double *rec = nullptr) {
   if (g.dr_mag2 > k.rcut2) return false;
   if (g.dr_mag2 < 1e-12) {
     double dr[3] = {g.dr[0], g.dr[1], g.dr[2]};
@@ -147,6 +151,10 @@ __device__ __forceinline__ bool wca_f64(const SysConst &k, PairGeom<double> &g,
     double rinv = 1.0 / (rmag);
 #pragma unroll
     for (int i = 0; i < ND; ++i) force[i] = k.fcut * dr[i] * rinv;
+    if (rec) {
+      for (int i = 0; i < 3; ++i) rec[i] = i < ND ? dr[i] : 0.0;
+      rec[3] = 0.0;
+    }
     return true;
   }
   double rmag = sqrt(g.dr_mag2);
@@ -157,6 +165,10 @@ __device__ __forceinline__ bool wca_f64(const SysConst &k, PairGeom<double> &g,
   if (dabs(ffac) > k.fcut) ffac = signof(ffac) * k.fcut;
 #pragma unroll
   for (int i = 0; i < ND; ++i) force[i] = ffac * g.dr[i] * rinv;
+  if (rec) {
+    for (int i = 0; i < 3; ++i) rec[i] = i < ND ? g.dr[i] : 0.0;
+    rec[3] = r6 * (k.c12 * r6 - k.c6) + k.eps;
+  }
   return true;
 }
 
@@ -260,7 +272,7 @@ __device__ __forceinline__ void sphero_f32(const float *hf,
 
 template <int ND>
 __device__ __forceinline__ bool wca_f32(const SysConst &k, PairGeom<float> &g,
-                                        float force[3]) {
+                                        float force[3], float *rec = nullptr) {
   if (g.dr_mag2 > k.rcut2f) return false;
   if (g.dr_mag2 < 1e-12f) {
     float dr[3] = {g.dr[0], g.dr[1], g.dr[2]};
@@ -276,6 +288,10 @@ __device__ __forceinline__ bool wca_f32(const SysConst &k, PairGeom<float> &g,
     float s = k.fcutf / rmag;
 #pragma unroll
     for (int i = 0; i < ND; ++i) force[i] = s * dr[i];
+    if (rec) {
+      for (int i = 0; i < 3; ++i) rec[i] = i < ND ? dr[i] : 0.f;
+      rec[3] = 0.f;
+    }
     return true;
   }
   float rinv = rsqrtf(g.dr_mag2);
@@ -286,6 +302,10 @@ __device__ __forceinline__ bool wca_f32(const SysConst &k, PairGeom<float> &g,
   float s = ffac * rinv;
 #pragma unroll
   for (int i = 0; i < ND; ++i) force[i] = s * g.dr[i];
+  if (rec) {
+    for (int i = 0; i < 3; ++i) rec[i] = i < ND ? g.dr[i] : 0.f;
+    rec[3] = __fmaf_rn(k.c12f, r6, -k.c6f) * r6 + k.epsf;
+  }
   return true;
 }
 
