@@ -65,6 +65,7 @@ struct sc_ctx {
 
   // cell list and pair list storage
   int *key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
+  unsigned *cell_occ = nullptr;  // one bit per cell: occupied in the last rebuild
   int *sorted = nullptr, *pair_count = nullptr, *pair_off = nullptr;
   int *deg = nullptr, *deg_off = nullptr, *scan_tmp = nullptr, *cells_xyz = nullptr;
   double *stage = nullptr;         // interleaved host-transfer staging, 3 * max(ns, nb)
@@ -412,15 +413,15 @@ void rebuild_enqueue(sc_ctx *c) {
   if (c->desc.interaction_flag) {
     c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
     c->launches += sc::launch_exclusive_scan(c->cell_count, c->cell_start, k.n_cells,
-                                             c->scan_tmp, c->st);
+                                             c->scan_tmp, c->st, c->cell_occ);
     c->launches += sc::launch_bin_scatter(d, c->key, c->cell_start, c->cell_count, c->sorted,
                                           c->st);
     c->launches += sc::launch_cell_sort_count(k, d, c->key, c->sorted, c->cell_start,
-                                              c->pair_count, c->st);
+                                              c->pair_count, c->st, c->cell_occ);
     c->launches += sc::launch_exclusive_scan(c->pair_count, c->pair_off, c->nb,
                                              c->scan_tmp, c->st);
     c->launches += sc::launch_pair_emit(k, d, c->key, c->sorted, c->cell_start,
-                                        c->pair_off, c->deg, c->prec, c->st);
+                                        c->pair_off, c->deg, c->prec, c->st, c->cell_occ);
     c->launches += sc::launch_exclusive_scan(c->deg, c->deg_off, c->nb, c->scan_tmp, c->st);
     c->launches += sc::launch_csr(d, c->deg, c->deg_off, c->st);
   }
@@ -1071,6 +1072,7 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
   CKS(dalloc(c, &c->key, nbi));
   CKS(dzero(&c->cell_count, (size_t)k.n_cells));
   CKS(dalloc(c, &c->cell_start, (size_t)k.n_cells + 1));
+  CKS(dalloc(c, &c->cell_occ, (size_t)k.n_cells / 32 + 1));
   CKS(dalloc(c, &c->sorted, nbi));
   CKS(dalloc(c, &c->pair_count, nbi));
   CKS(dzero(&c->pair_off, (size_t)nbi + 1));

@@ -1,11 +1,12 @@
 // Device kernels of the B200 filament step.  Compiled with --fmad=false
 // (see sc_common.cuh).
 //
-//   cell list      k_bin_count, k_bin_scatter, k_cell_sort, k_cell_count,
+//   cell list      k_bin_count, k_bin_scatter, k_cell_sort_count,
 //                  k_pair_emit   (CellList + Cell, src/cell_list.cpp,
 //                                 src/cell.cpp)
-//   pair CSR       k_csr_fill, k_csr_sort (per-bond pair entries in list
-//                  order, for the reference's serial scatter order)
+//   pair CSR       k_csr_offsets, k_csr_fill, k_csr_sort_pos (per-bond pair
+//                  entries in list order, for the reference's serial
+//                  scatter order)
 //   pair forces    k_pair_eval   (InteractionManager::CalculatePairInteractions,
 //                                 one thread per pair, signed per-bond slots)
 //                  k_bond_sum    (ApplyPairInteractions into bond accumulators)
@@ -125,32 +126,6 @@ __global__ void k_bin_scatter(DevState d, const int *key, const int *cell_start,
   sorted[cell_start[c] + slot] = b;
 }
 
-// Half-shell neighbour cells of (x, y, z) in the order of
-// CellList::AssignCellNeighbors(false) (src/cell_list.cpp:206-262), as
-// indices within the system.
-__device__ __forceinline__ int half_shell(const SysConst &k, const ReplicaConst &R, int x,
-                                          int y, int z, int *out) {
-  int n1d = R.n1d, cnt = 0;
-  int z_end = (k.n_dim == 3 ? z + 2 : z + 1);
-  for (int zp = z; zp < z_end; ++zp) {
-    int nz = zp;
-    if (nz == n1d) nz = 0;
-    for (int yp = (zp > z ? y - 1 : y); yp < y + 2; ++yp) {
-      int ny = yp;
-      if (ny < 0) ny = n1d - 1;
-      else if (ny == n1d) ny = 0;
-      for (int xp = (yp > y || zp > z ? x - 1 : x + 1); xp < x + 2; ++xp) {
-        int nx = xp;
-        if (nx < 0) nx = n1d - 1;
-        else if (nx == n1d) nx = 0;
-        if (nx == x && ny == y && nz == z) continue;
-        out[cnt++] = (nx * n1d + ny) * R.third + nz;
-      }
-    }
-  }
-  return cnt;
-}
-
 // Pairs that ProcessPairInteraction marks no_interaction and the first
 // evaluation after a rebuild culls (src/interaction_manager.cpp:341-367,
 // 485-497): all pairs without like-like interactions, and bonds of one
@@ -165,6 +140,37 @@ __device__ __forceinline__ bool pair_excluded(const SysConst &k,
   return false;
 }
 
+// Half-shell neighbour cells of (x, y, z) in the order of
+// CellList::AssignCellNeighbors(false) (src/cell_list.cpp:206-262), as
+// indices within the system, without compaction: entry kk (a compile-time
+// index) is the kk-th candidate of its loops -- (x+1, y, z); (x-1..x+1,
+// y+1, z); then, in 3D, (x-1..x+1, y-1..y+1, z+1), x fastest -- with
+// periodic wrap, and bit kk of the returned mask says it is kept (it is not
+// the cell itself, which wrap can give on small grids).  Visiting the set
+// bits in order visits the reference's neighbour list in its order, with
+// every index in registers.
+__device__ __forceinline__ unsigned half_shell_fixed(const SysConst &k, const ReplicaConst &R,
+                                                     int x, int y, int z, int out[13]) {
+  const int n1d = R.n1d;
+  unsigned mask = 0;
+#pragma unroll
+  for (int kk = 0; kk < 13; ++kk) {
+    const int dz = kk < 4 ? 0 : 1;
+    const int dy = kk == 0 ? 0 : (kk < 4 ? 1 : (kk - 4) / 3 - 1);
+    const int dx = kk == 0 ? 1 : (kk < 4 ? kk - 2 : (kk - 4) % 3 - 1);
+    int nx = x + dx, ny = y + dy, nz = z + dz;
+    if (nx < 0) nx = n1d - 1;
+    else if (nx == n1d) nx = 0;
+    if (ny < 0) ny = n1d - 1;
+    else if (ny == n1d) ny = 0;
+    if (nz == n1d) nz = 0;
+    out[kk] = (nx * n1d + ny) * R.third + nz;
+    const bool keep = (kk < 4 || k.n_dim == 3) && !(nx == x && ny == y && nz == z);
+    mask |= keep ? (1u << kk) : 0u;
+  }
+  return mask;
+}
+
 __device__ __forceinline__ void cell_coords(const ReplicaConst &R, int c, int &x, int &y,
                                             int &z) {
   z = c % R.third;
@@ -173,16 +179,39 @@ __device__ __forceinline__ void cell_coords(const ReplicaConst &R, int c, int &x
   x = t / R.n1d;
 }
 
+// Whether cell c holds a bond, from the occupancy bits the cell scan wrote
+// (a small array that stays in cache, unlike the cell offsets); without
+// them, every cell is looked up.
+__device__ __forceinline__ bool cell_occupied(const unsigned *occ, int c) {
+  return !occ || ((occ[c >> 5] >> (c & 31)) & 1u);
+}
+
 // One thread per cell head (first entry of a cell in the sorted order):
-// restores insertion order inside the cell (bond order, as Cell::AddObj
-// appends in interactor order).  The sorted order holds the bonds of the
-// systems rebuilt in this pass, cell_start[n_cells] of them.
-__global__ void k_cell_sort(SysConst k, const int *key, int *sorted, const int *cell_start) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= cell_start[k.n_cells]) return;
-  int c = key[sorted[q]];
-  if (cell_start[c] != q) return;
-  int m = cell_start[c + 1] - q;
+// restores insertion order inside its cell (bond order, as Cell::AddObj
+// appends in interactor order), then counts the pairs the cell contributes
+// (zero for every other entry, so that the scan over all bonds sees only
+// heads).  The sorted order holds the bonds of the systems rebuilt in this
+// pass, cell_start[n_cells] of them.  A pair is dropped only between
+// adjacent bonds of one filament, or always without like-like interactions
+// (pair_excluded), so a half-shell neighbour cell contributes m * m_nbr
+// pairs less one for each of the cell's bonds whose filament neighbour
+// (b - 1 or b + 1) lies in it -- told by that bond's cell key.  No thread
+// reads another cell's members, which their heads are sorting meanwhile.
+__global__ void k_cell_sort_count(SysConst k, DevState d, int nb, const int *key, int *sorted,
+                                  const int *cell_start, int *pair_count, const unsigned *occ) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nb) return;
+  if (q >= cell_start[k.n_cells]) {
+    pair_count[q] = 0;
+    return;
+  }
+  // Any entry of a cell names a member of it, also while its head sorts.
+  const int c = key[sorted[q]];
+  if (cell_start[c] != q) {
+    pair_count[q] = 0;
+    return;
+  }
+  const int m = cell_start[c + 1] - q;
   int *it = sorted + q;
   for (int i = 1; i < m; ++i) {  // insertion sort (cells are small)
     int v = it[i], j = i - 1;
@@ -192,40 +221,52 @@ __global__ void k_cell_sort(SysConst k, const int *key, int *sorted, const int *
     }
     it[j + 1] = v;
   }
-}
-
-// One thread per cell head: number of kept pairs the cell contributes (zero
-// for every other entry, so that the scan over all bonds sees only heads).
-__global__ void k_cell_count(SysConst k, DevState d, int nb, const int *key,
-                             const int *sorted, const int *cell_start,
-                             int *pair_count) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nb) return;
-  if (q >= cell_start[k.n_cells]) {
+  if (!k.like_like) {
     pair_count[q] = 0;
     return;
   }
-  int c = key[sorted[q]];
-  if (cell_start[c] != q) {
-    pair_count[q] = 0;
-    return;
-  }
-  const ReplicaConst &R = d.rep[rep_of_bond(d, sorted[q])];
-  int m = cell_start[c + 1] - q;
-  const int *it = sorted + q;
-  long long cnt = 0;
-  for (int i = 0; i < m - 1; ++i)
-    for (int j = i + 1; j < m; ++j) cnt += !pair_excluded(k, d, it[i], it[j]);
+  const ReplicaConst &R = d.rep[rep_of_bond(d, it[0])];
   int x, y, z, nbr[13];
   cell_coords(R, c - R.cell0, x, y, z);
-  int nn = half_shell(k, R, x, y, z, nbr);
-  for (int kk = 0; kk < nn; ++kk) {
-    int cn = R.cell0 + nbr[kk];
-    int s0 = cell_start[cn], s1 = cell_start[cn + 1];
-    for (int i = 0; i < m; ++i)
-      for (int j = s0; j < s1; ++j) cnt += !pair_excluded(k, d, it[i], sorted[j]);
+  const unsigned keep = half_shell_fixed(k, R, x, y, z, nbr);
+  long long cnt = (long long)m * (m - 1) / 2;
+#pragma unroll
+  for (int kk = 0; kk < 13; ++kk) {  // all ranges loaded together
+    nbr[kk] += R.cell0;
+    if ((keep >> kk) & 1u) {
+      if (cell_occupied(occ, nbr[kk]))
+        cnt += (long long)m * (cell_start[nbr[kk] + 1] - cell_start[nbr[kk]]);
+    } else {
+      nbr[kk] = -1;  // matches no cell key
+    }
+  }
+  for (int i = 0; i < m; ++i) {
+    const int a = it[i], fa = d.bond_fil[a];
+    if (a + 1 < nb && d.bond_fil[a + 1] == fa) {
+      const int ka = key[a + 1];
+      if (ka == c) --cnt;  // each adjacent pair inside the cell, once
+#pragma unroll
+      for (int kk = 0; kk < 13; ++kk) cnt -= ka == nbr[kk];
+    }
+    if (a > 0 && d.bond_fil[a - 1] == fa) {
+      const int ka = key[a - 1];
+#pragma unroll
+      for (int kk = 0; kk < 13; ++kk) cnt -= ka == nbr[kk];
+    }
   }
   pair_count[q] = cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
+}
+
+// Pairs of rebuilt system r: the span of its cells' offsets.  A list longer
+// than its segment sets the overflow bit (the count is kept so the host can
+// size the segment).
+__device__ __forceinline__ void rep_pairs(const DevState &d, int r, const int *cell_start,
+                                          const int *pair_off) {
+  if (!d.due[r]) return;
+  const ReplicaConst &R = d.rep[r];
+  const int np = pair_off[cell_start[R.cell0 + R.n_cells]] - pair_off[cell_start[R.cell0]];
+  d.np_rep[r] = np;
+  if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
 }
 
 // Writes each cell's pairs at its offset in its system's pair segment, in the
@@ -234,8 +275,9 @@ __global__ void k_cell_count(SysConst k, DevState d, int nb, const int *key,
 // stored force and counts per-bond pair entries for the CSR.
 __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
                             const int *sorted, const int *cell_start,
-                            const int *pair_off, int *deg, int prec) {
+                            const int *pair_off, int *deg, int prec, const unsigned *occ) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < d.nrep) rep_pairs(d, q, cell_start, pair_off);
   if (q >= cell_start[k.n_cells]) return;
   int c = key[sorted[q]];
   if (cell_start[c] != q) return;
@@ -246,7 +288,7 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
   int p = pair_off[q] - pair_off[cell_start[R.cell0]];
   int x, y, z, nbr[13];
   cell_coords(R, c - R.cell0, x, y, z);
-  int nn = half_shell(k, R, x, y, z, nbr);
+  const unsigned keep = half_shell_fixed(k, R, x, y, z, nbr);
   auto emit = [&](int a, int b) {
     if (pair_excluded(k, d, a, b)) return;
     if (p < R.pcap) {
@@ -273,24 +315,20 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
   };
   for (int i = 0; i < m - 1; ++i)
     for (int j = i + 1; j < m; ++j) emit(it[i], it[j]);
-  for (int kk = 0; kk < nn; ++kk) {
-    int cn = R.cell0 + nbr[kk];
-    int s0 = cell_start[cn], s1 = cell_start[cn + 1];
-    for (int i = 0; i < m; ++i)
-      for (int j = s0; j < s1; ++j) emit(it[i], sorted[j]);
+  int s0[13], s1[13];
+#pragma unroll
+  for (int kk = 0; kk < 13; ++kk) {  // all ranges loaded together
+    s0[kk] = s1[kk] = 0;
+    const int cn = R.cell0 + nbr[kk];
+    if (((keep >> kk) & 1u) && cell_occupied(occ, cn)) {
+      s0[kk] = cell_start[cn];
+      s1[kk] = cell_start[cn + 1];
+    }
   }
-}
-
-// Pairs of each rebuilt system: the span of its cells' offsets.  A list
-// longer than its segment sets the overflow bit (the count is kept so the
-// host can size the segment).
-__global__ void k_rep_pairs(SysConst k, DevState d, const int *cell_start, const int *pair_off) {
-  int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= d.nrep || !d.due[r]) return;
-  const ReplicaConst &R = d.rep[r];
-  const int np = pair_off[cell_start[R.cell0 + R.n_cells]] - pair_off[cell_start[R.cell0]];
-  d.np_rep[r] = np;
-  if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+#pragma unroll
+  for (int kk = 0; kk < 13; ++kk)
+    for (int i = 0; i < m; ++i)
+      for (int j = s0[kk]; j < s1[kk]; ++j) emit(it[i], sorted[j]);
 }
 
 // Per-bond entry ranges of the rebuilt systems, inside their slot segments,
@@ -339,8 +377,9 @@ __global__ void k_csr_fill(DevState d, int *deg) {
 }
 
 // Sorts each bond's entries by pair index = the order in which the
-// reference's serial ApplyPairInteractions adds them to the bond.
-__global__ void k_csr_sort(DevState d) {
+// reference's serial ApplyPairInteractions adds them to the bond, then
+// records the slot of each (pair, role) entry.
+__global__ void k_csr_sort_pos(DevState d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb || !d.due[rep_of_bond(d, b)]) return;
   int e0 = d.e_off[b], e1 = e0 + d.e_cnt[b];
@@ -352,6 +391,11 @@ __global__ void k_csr_sort(DevState d) {
       --j;
     }
     e[j + 1] = v;
+  }
+  for (int i = e0; i < e1; ++i) {
+    const int ent = e[i];
+    if (ent & 1) d.pos2[ent >> 1] = i;
+    else d.pos1[ent >> 1] = i;
   }
 }
 
@@ -405,49 +449,101 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *tmp, int &total)
   return excl;
 }
 
-__global__ void k_scan_tiles(const int *in, int *out, int n, int *tile_sums) {
-  __shared__ int tmp[SCAN_BLOCK / 32];
-  int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-  int v[SCAN_ITEMS], sum = 0;
+// Sum of each tile of SCAN_TILE elements.
+template <bool VEC>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const int *in, int n, int *tile_sums) {
+  __shared__ int red[SCAN_BLOCK / 32];
+  const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  int sum = 0;
+  if (VEC && base + SCAN_ITEMS <= n) {
+    const int4 a = reinterpret_cast<const int4 *>(in + base)[0];
+    const int4 b = reinterpret_cast<const int4 *>(in + base)[1];
+    sum = a.x + a.y + a.z + a.w + b.x + b.y + b.z + b.w;
+  } else {
 #pragma unroll
-  for (int i = 0; i < SCAN_ITEMS; ++i) {
-    v[i] = (base + i < n) ? in[base + i] : 0;
-    sum += v[i];
+    for (int i = 0; i < SCAN_ITEMS; ++i) sum += (base + i < n) ? in[base + i] : 0;
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < SCAN_BLOCK / 32; ++w) t += red[w];
+    tile_sums[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of each tile, offset by the sum of the tiles before it,
+// which every block adds up for itself (no block waits on another); the
+// last tile's block writes the total to out[n].  With occ, also one bit per
+// element: set where the element is non-zero (the occupied cells).
+template <bool VEC>
+__global__ void __launch_bounds__(SCAN_BLOCK) k_scan_down(const int *in, int *out, int n,
+                                                         const int *tile_sums, unsigned *occ) {
+  __shared__ int tmp[SCAN_BLOCK / 32];
+  __shared__ int red[SCAN_BLOCK / 32];
+  // Sum of the earlier tiles: independent loads, then a block reduction.
+  int p0 = 0, p1 = 0, p2 = 0, p3 = 0;
+  const int nt = (int)blockIdx.x;
+  int t = threadIdx.x;
+  for (; t + 3 * SCAN_BLOCK < nt; t += 4 * SCAN_BLOCK) {
+    p0 += tile_sums[t];
+    p1 += tile_sums[t + SCAN_BLOCK];
+    p2 += tile_sums[t + 2 * SCAN_BLOCK];
+    p3 += tile_sums[t + 3 * SCAN_BLOCK];
+  }
+  for (; t < nt; t += SCAN_BLOCK) p0 += tile_sums[t];
+  int pre = (p0 + p1) + (p2 + p3);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = pre;
+  const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  int v[SCAN_ITEMS], sum = 0;
+  const bool full = base + SCAN_ITEMS <= n;
+  if (VEC && full) {
+    const int4 a = reinterpret_cast<const int4 *>(in + base)[0];
+    const int4 b = reinterpret_cast<const int4 *>(in + base)[1];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) v[i] = (base + i < n) ? in[base + i] : 0;
+  }
+#pragma unroll
+  for (int i = 0; i < SCAN_ITEMS; ++i) sum += v[i];
   int total;
-  int run = block_exclusive_scan(sum, tmp, total);
+  int run = block_exclusive_scan(sum, tmp, total);  // synchronises: red[] is complete
+  int offset = 0;
+#pragma unroll
+  for (int w = 0; w < SCAN_BLOCK / 32; ++w) offset += red[w];
+  run += offset;
+  int r[SCAN_ITEMS];
 #pragma unroll
   for (int i = 0; i < SCAN_ITEMS; ++i) {
-    if (base + i < n) out[base + i] = run;
+    r[i] = run;
     run += v[i];
   }
-  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
-}
-
-// Single block: exclusive scan of the tile sums in place; total -> *out_total.
-__global__ void k_scan_sums(int *sums, int n, int *out_total) {
-  __shared__ int tmp[SCAN_BLOCK / 32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < n; base += SCAN_BLOCK) {
-    int i = base + threadIdx.x;
-    int v = i < n ? sums[i] : 0;
-    int total;
-    int e = block_exclusive_scan(v, tmp, total);
-    if (i < n) sums[i] = e + carry;
-    __syncthreads();
-    if (threadIdx.x == 0) carry += total;
-    __syncthreads();
+  if (VEC && full) {
+    reinterpret_cast<int4 *>(out + base)[0] = make_int4(r[0], r[1], r[2], r[3]);
+    reinterpret_cast<int4 *>(out + base)[1] = make_int4(r[4], r[5], r[6], r[7]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i)
+      if (base + i < n) out[base + i] = r[i];
   }
-  if (threadIdx.x == 0) *out_total = carry;
-}
-
-__global__ void k_scan_add(int *out, int n, const int *tile_sums) {
-  int base = blockIdx.x * SCAN_TILE;
-  int add = tile_sums[blockIdx.x];
-  for (int i = threadIdx.x; i < SCAN_TILE; i += SCAN_BLOCK)
-    if (base + i < n) out[base + i] += add;
+  if (occ) {  // four threads' 8 elements make one 32-bit word
+    unsigned m = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) m |= (v[i] != 0 ? 1u : 0u) << i;
+    const int sh = (threadIdx.x & 3) * 8;
+    unsigned w = m << sh;
+    w |= __shfl_down_sync(0xffffffffu, w, 2);
+    w |= __shfl_down_sync(0xffffffffu, w, 1);
+    const int word = (blockIdx.x * SCAN_TILE) / 32 + (threadIdx.x >> 2);
+    if ((threadIdx.x & 3) == 0 && word * 32 < n) occ[word] = w;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = offset + total;
 }
 
 // ---------------------------------------------------------------------------
@@ -657,18 +753,6 @@ __global__ void k_tether(SysConst k, DevState d) {
     double4 *o = reinterpret_cast<double4 *>(d.xl_c) + 2 * (size_t)(2 * x + a);
     o[0] = make_double4(c[0], c[1], c[2], t[0]);
     o[1] = make_double4(t[1], t[2], 0.0, 0.0);
-  }
-}
-
-// Slot of each (pair, role) entry after the per-bond sort.
-__global__ void k_csr_pos(DevState d) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= d.nb) return;
-  if (!d.due[rep_of_bond(d, b)]) return;
-  for (int e = d.e_off[b]; e < d.e_off[b] + d.e_cnt[b]; ++e) {
-    int ent = d.e_ent[e];
-    if (ent & 1) d.pos2[ent >> 1] = e;
-    else d.pos1[ent >> 1] = e;
   }
 }
 
@@ -885,14 +969,19 @@ template int launch_soa_to_aos<double>(int, const double *, const double *, cons
 
 // Exclusive scan in[0..n) -> out[0..n], out[n] = total.  tmp holds
 // scan_temp_ints(n) ints.  Returns launches issued.
-int launch_exclusive_scan(const int *in, int *out, long long n, int *tmp,
-                          cudaStream_t st) {
+int launch_exclusive_scan(const int *in, int *out, long long n, int *tmp, cudaStream_t st,
+                          unsigned *occ) {
   int tiles = cdiv(n, SCAN_TILE);
   if (tiles == 0) tiles = 1;
-  k_scan_tiles<<<tiles, SCAN_BLOCK, 0, st>>>(in, out, (int)n, tmp);
-  k_scan_sums<<<1, SCAN_BLOCK, 0, st>>>(tmp, tiles, out + n);
-  k_scan_add<<<tiles, SCAN_BLOCK, 0, st>>>(out, (int)n, tmp);
-  return 3;
+  const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15u) == 0;
+  if (vec) {
+    k_scan_reduce<true><<<tiles, SCAN_BLOCK, 0, st>>>(in, (int)n, tmp);
+    k_scan_down<true><<<tiles, SCAN_BLOCK, 0, st>>>(in, out, (int)n, tmp, occ);
+  } else {
+    k_scan_reduce<false><<<tiles, SCAN_BLOCK, 0, st>>>(in, (int)n, tmp);
+    k_scan_down<false><<<tiles, SCAN_BLOCK, 0, st>>>(in, out, (int)n, tmp, occ);
+  }
+  return 2;
 }
 
 int launch_bin_count(const SysConst &k, const DevState &d, int *key,
@@ -917,29 +1006,26 @@ int launch_bin_scatter(const DevState &d, const int *key, const int *cell_start,
 
 int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
                            int *sorted, const int *cell_start, int *pair_count,
-                           cudaStream_t st) {
-  k_cell_sort<<<cdiv(d.nb, 128), 128, 0, st>>>(k, key, sorted, cell_start);
-  k_cell_count<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted,
-                                                cell_start, pair_count);
-  return 2;
+                           cudaStream_t st, const unsigned *occ) {
+  k_cell_sort_count<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted, cell_start,
+                                                     pair_count, occ);
+  return 1;
 }
 
 int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      const int *sorted, const int *cell_start,
                      const int *pair_off, int *deg, int prec,
-                     cudaStream_t st) {
+                     cudaStream_t st, const unsigned *occ) {
   k_pair_emit<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted, cell_start,
-                                               pair_off, deg, prec);
-  k_rep_pairs<<<cdiv(d.nrep, 128), 128, 0, st>>>(k, d, cell_start, pair_off);
-  return 2;
+                                               pair_off, deg, prec, occ);
+  return 1;
 }
 
 int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st) {
   k_csr_offsets<<<cdiv(d.nb, 256), 256, 0, st>>>(d, deg_off, deg);
   k_csr_fill<<<cdiv(d.pcap_total > 0 ? d.pcap_total : 1, 256), 256, 0, st>>>(d, deg);
-  k_csr_sort<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
-  k_csr_pos<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
-  return 4;
+  k_csr_sort_pos<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
+  return 3;
 }
 
 // ---------------------------------------------------------------------------

@@ -28,8 +28,9 @@ int launch_aos_to_soa(int n, int nd, const double *aos, const DevState &d, cudaS
 // Component arrays into interleaved triples.
 template <class T>
 int launch_soa_to_aos(int n, const T *x, const T *y, const T *z, double *aos, cudaStream_t st);
+// With occ, also one bit per element (set where it is non-zero), 32 to a word.
 int launch_exclusive_scan(const int *in, int *out, long long n, int *tmp,
-                          cudaStream_t st);
+                          cudaStream_t st, unsigned *occ = nullptr);
 int launch_bin_count(const SysConst &k, const DevState &d, int *key,
                      int *cell_count, cudaStream_t st);
 int launch_bond_cells(const SysConst &k, const DevState &d, int *xyz,
@@ -38,14 +39,15 @@ int launch_bond_cells(const SysConst &k, const DevState &d, int *xyz,
 // systems are skipped and keep their lists.
 int launch_bin_scatter(const DevState &d, const int *key, const int *cell_start,
                        int *cell_count, int *sorted, cudaStream_t st);
+// occ: the cell scan's occupancy bits (null: look every neighbour cell up).
 int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
                            int *sorted, const int *cell_start, int *pair_count,
-                           cudaStream_t st);
+                           cudaStream_t st, const unsigned *occ = nullptr);
 // Emits the pairs into the systems' segments and records each system's count.
 int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      const int *sorted, const int *cell_start,
                      const int *pair_off, int *deg, int prec,
-                     cudaStream_t st);
+                     cudaStream_t st, const unsigned *occ = nullptr);
 // Per-bond entry lists; deg_off is the exclusive scan of deg over all bonds.
 int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st);
 int launch_decide(const SysConst &k, const DevState &d,
