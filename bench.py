@@ -37,10 +37,10 @@ METRIC = "segment-steps/s, 1 B200: mixed+batched vs FP64 GPU at ≤1e-5 force er
 UNIT = "segment-steps/s"
 I_STEPS_PER_STEP = 20
 # DRAM bytes (read + write) of one k_integrate launch, mixed precision, from
-# ncu (cold cache), per workload captured: for B the mean of a midstep launch
-# (21.87 MB) and a full-step launch (39.48 MB), which alternate.  Workloads
-# without a capture report null.
-TRAFFIC_K_INTEGRATE_MIXED = {"B": 30.67e6}
+# ncu (cold cache), per workload captured: for B (96-site blocks) the mean of
+# a midstep launch (23.05 MB) and a full-step launch (40.69 MB), which
+# alternate.  Workloads without a capture report null.
+TRAFFIC_K_INTEGRATE_MIXED = {"B": 31.87e6}
 WORKLOAD_DESCS = {
     "A": "A: 100 filaments x 20 bonds (2,000 segments, 2,100 sites), 3D periodic cube side 50, "
          "lp 500, WCA eps=sigma=1, dt 1e-4, noise on",
@@ -69,6 +69,9 @@ def parse_args():
                     help="run this many host-driven steps and exit (for ncu)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of --profile-steps")
+    ap.add_argument("--profile-layout", default=None,
+                    help="integrator layout W,C for --profile-steps (warp-kernel sites, block "
+                         "sites), e.g. the one the timed run's autotuner chose")
     return ap.parse_args()
 
 
@@ -275,13 +278,17 @@ def profile_only(args):
     import simcore_b200 as sc
     from simcore_b200 import workloads
     ctx = new_context(sc, load_workload(args.workload, 0), args.precision, 0)
+    layout = None
+    if args.profile_layout:
+        layout = [int(v) for v in args.profile_layout.split(",")]
+        ctx.set_integrator_layout(*layout)
     ctx.step(4)
     ctx.step(args.profile_steps)
     ctx.synchronize()
     c = ctx.counters()
     ctx.close()
     print(json.dumps({"profile_steps": args.profile_steps, "precision": args.precision,
-                      "bonds": c.n_bonds, "pairs": c.n_pairs}))
+                      "layout": layout, "bonds": c.n_bonds, "pairs": c.n_pairs}))
 
 
 def run_ours(args, rank, world, local_rank):
@@ -441,7 +448,8 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": b_int, "avg_launch_ms": t_int,
                      "peak_kind": peak_kind + " hbm_gbs",
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
-                                       "launch of bench.py --profile-steps 8 (cold cache)",
+                                       "launch of bench.py --profile-steps 8 --profile-layout "
+                                       "0,96 (cold cache)",
                      "pair_kernel": {"kernel": "k_pair_eval (mixed)", "avg_launch_ms": t_pair,
                                      "algorithmic_bytes_per_launch": b_pair,
                                      "achieved": b_pair / (t_pair * 1e-3) / 1e9},
