@@ -353,17 +353,21 @@ def run_ours(args, rank, world, local_rank):
     # Mixed-precision force error on this workload: fresh contexts of both
     # precisions on the initial positions evaluate the pair forces once; the
     # mixed bond forces and torques are compared with the FP64 ones
-    # (max |dF| / max |F|).
+    # (max |dF| / max |F|), also with nearly parallel pairs evaluated from
+    # the FP64 sites (sc_set_exact_near_parallel; off in the timed runs).
     errs = {}
-    for p_ in ("fp64", "mixed"):
-        cc = new_context(sc, wl, p_, local_rank)
+    for p_ in ("fp64", "mixed", "mixed_npx"):
+        cc = new_context(sc, wl, "fp64" if p_ == "fp64" else "mixed", local_rank)
+        if p_ == "mixed_npx":
+            cc.set_exact_near_parallel(True)
         cc.interact()
         errs[p_] = cc.bond_forces()
         cc.close()
-    force_err = float(np.abs(errs["mixed"][0] - errs["fp64"][0]).max() /
-                      np.abs(errs["fp64"][0]).max())
-    torque_err = float(np.abs(errs["mixed"][1] - errs["fp64"][1]).max() /
-                       np.abs(errs["fp64"][1]).max())
+
+    def rel_err(p_, i):
+        return float(np.abs(errs[p_][i] - errs["fp64"][i]).max() / np.abs(errs["fp64"][i]).max())
+
+    force_err, torque_err = rel_err("mixed", 0), rel_err("mixed", 1)
 
     # Roofline: per-launch CUDA-event durations of the two kernels of a
     # reference step, host-driven, on the context's stream.
@@ -438,6 +442,8 @@ def run_ours(args, rank, world, local_rank):
                  "rebuilds_in_timed_region": r64["rebuilds"]},
         "mixed_over_fp64": value / value64,
         "mixed_error": {"max_rel_bond_force": force_err, "max_rel_bond_torque": torque_err,
+                        "exact_near_parallel": {"max_rel_bond_force": rel_err("mixed_npx", 0),
+                                                "max_rel_bond_torque": rel_err("mixed_npx", 1)},
                         "vs": "FP64 GPU path (bit-identical to the reference) on the same "
                               "positions, one pair evaluation", "bound": 1e-5},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -194,6 +194,14 @@ sc_status sc_thermo_open(sc_ctx *ctx, const char *run_name, int n_steps);
 sc_status sc_get_thermo(sc_ctx *ctx, int max_records, int *n_records, int64_t *i_step,
                         double *tensor, double *pressure, double *volume);
 sc_status sc_get_potential_energy(sc_ctx *ctx, double *pote);
+/* Mixed precision only: evaluate nearly parallel pairs (FP32 |u1 x u2|^2
+ * between 0 and 1e-5, within 0.18 degrees) from the FP64 sites, as the FP64
+ * path does, in a second kernel after each pair stage.  FP32 orientations
+ * cannot resolve the closest points of such pairs: their torques (and
+ * forces) can be off by far more than 1e-5.  Off by default: the second
+ * kernel costs about 10% of the step on workload B.  No counterpart in the
+ * reference, whose pair stage is FP64 throughout. */
+sc_status sc_set_exact_near_parallel(sc_ctx *ctx, int on);
 /* Per-system rebuild counts and current pair counts (n_replicas entries
  * each; either pointer may be NULL). */
 sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);

@@ -109,6 +109,7 @@ struct sc_ctx {
   cudaEvent_t gev0 = nullptr, gev1 = nullptr;  // around each graph launch
   double graph_ms = 0.0;
   long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
+  bool npx = false;           // mixed: near-parallel pairs evaluated from FP64 sites
 
   // thermo (sc_set_thermo): records are produced on the device every th_n
   // steps and pulled into th_host (and the open .thermo files)
@@ -255,10 +256,27 @@ sc_status upload_reps(sc_ctx *c) {
 void free_pair_storage(sc_ctx *c) {
   for (void *q : {(void *)c->d.pa, (void *)c->d.pb, (void *)c->d.pos1, (void *)c->d.pos2,
                   (void *)c->d.pf64, (void *)c->d.pf32, (void *)c->d.cf64, (void *)c->d.cf32,
-                  (void *)c->d.e_ent, (void *)c->d.pv64, (void *)c->d.pv32})
+                  (void *)c->d.e_ent, (void *)c->d.pv64, (void *)c->d.pv32,
+                  (void *)c->d.fix_list})
     dfree(c, q);
   c->d.pv64 = nullptr;
   c->d.pv32 = nullptr;
+  c->d.fix_list = nullptr;
+}
+
+// The list of near-parallel pairs (one slot per pair) of the exact
+// near-parallel mode and its counters, zeroed once; k_pair_fixup leaves
+// them zero after every pair stage.
+sc_status alloc_fixup(sc_ctx *c, long long total) {
+  if (!c->npx) return SC_OK;
+  CKS(dalloc(c, &c->d.fix_list, total));
+  if (!c->d.fix_count) {
+    CKS(dalloc(c, &c->d.fix_count, 1));
+    CKS(dalloc(c, &c->d.fix_done, 1));
+    CK(cudaMemsetAsync(c->d.fix_count, 0, sizeof(int), c->st));
+    CK(cudaMemsetAsync(c->d.fix_done, 0, sizeof(unsigned), c->st));
+  }
+  return SC_OK;
 }
 
 // Per-pair virial records for `total` slots, zeroed (a pair not evaluated
@@ -301,6 +319,7 @@ sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
   }
   CKS(dalloc(c, &d.e_ent, 2 * total));
   if (c->k.thermo) CKS(alloc_pair_records(c, total));
+  CKS(alloc_fixup(c, total));
   long long p0 = 0;
   for (size_t r = 0; r < caps.size(); ++r) {
     c->reps[r].p0 = (int)p0;
@@ -373,6 +392,7 @@ sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
   free_pair_storage(c);
   d.pv64 = pv64;
   d.pv32 = pv32;
+  CKS(alloc_fixup(c, cap));
   d.pa = pa;
   d.pb = pb;
   d.pos1 = pos1;
@@ -658,7 +678,7 @@ sc_status thermo_reserve(sc_ctx *c, long long n) {
 // The pair stage of one step, then the step's thermo accumulation.
 sc_status pair_stage(sc_ctx *c) {
   CKS(timed(c, [&] {
-    return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st);
+    return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st, c->npx);
   }));
   if (c->k.thermo) c->launches += sc::launch_thermo(c->k, c->d, c->prec, c->st);
   return SC_OK;
@@ -1232,7 +1252,8 @@ static sc_status build_graph(sc_ctx *c) {
     const int rb = half == 0 ? c->rbuf : 1 - c->rbuf;
     // The second half is the even (full) step: crosslink tethers first.
     if (half == 1 && interaction) sc::launch_tether(c->k, c->d, c->st);
-    if (interaction) sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st);
+    if (interaction)
+      sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
     if (interaction && c->k.thermo) sc::launch_thermo(c->k, c->d, c->prec, c->st);
     sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
                          c->capture, c->prec, c->fast, c->st);
@@ -1304,7 +1325,8 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       // tail (the stopped step's too), per rebuild the captured sequence.
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) *
                              (c->desc.interaction_flag
-                                  ? (c->d.nx ? 7 : 6) + (c->k.thermo ? 2 : 0)
+                                  ? (c->d.nx ? 7 : 6) + (c->k.thermo ? 2 : 0) +
+                                        (c->npx && c->prec ? 2 : 0)
                                   : 3) +
                      (nr1 - nr0) * c->rebuild_kernels;
       bd -= done;
@@ -2175,6 +2197,17 @@ sc_status sc_get_potential_energy(sc_ctx *c, double *pote) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(pote, c->stage, sizeof(double) * c->nf, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_set_exact_near_parallel(sc_ctx *c, int on) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  if (c->prec == 0 || c->npx == (on != 0)) return SC_OK;
+  CK(cudaSetDevice(c->desc.device));
+  c->npx = on != 0;
+  if (c->npx && !c->d.fix_list) CKS(alloc_fixup(c, c->pcap));
+  CK(cudaStreamSynchronize(c->st));
+  drop_graph(c);
   return SC_OK;
 }
 

@@ -562,7 +562,76 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_down(const int *in, int *ou
 // Interaction's force (src/minimum_distance.cpp:31-34 resets only dr and the
 // contacts), and the pair's thread owns that stored force.
 
-template <int ND, int PREC>
+// A bond's FP64 geometry recomputed from its sites, with the operations of
+// Bond::ReInit (src/bond.cpp:22-37) -- what the FP64 path's geometry holds.
+template <int ND>
+__device__ __forceinline__ void bond_geom_from_sites(const DevState &d, const ReplicaConst &R,
+                                                     int b, BondGeomF64 &G) {
+  const int site = b + d.bond_fil[b];
+  double r1[3], r2[3];
+  for (int i = 0; i < 3; ++i) {
+    r1[i] = d.r[i][site];
+    r2[i] = d.r[i][site + 1];
+  }
+  bond_from_sites<ND>(R.hinv, r1, r2, G.s, G.u, G.len);
+  G.pad = 0.0;
+}
+
+// Nearly parallel segments in the mixed pair stage: |u1 x u2|^2 in FP32
+// (accurate where 1 - (u1 . u2)^2 is rounding alone) above 0 and below
+// 1e-5, i.e. within 0.18 degrees.  For them the closest points depend on
+// orientation bits FP32 does not hold, so they are evaluated in FP64, from
+// the sites (pair_eval_fp64_sites).  Exactly parallel FP32 orientations take the parallel branch
+// in both precisions (their FP64 1 - c^2 is below the reference's 1e-12).
+template <int ND>
+__device__ __forceinline__ bool near_parallel(const BondGeomF32 &A, const BondGeomF32 &B) {
+  float s2;
+  const float cz = __fmaf_rn(A.u[0], B.u[1], -A.u[1] * B.u[0]);
+  if (ND == 3) {
+    const float cx = __fmaf_rn(A.u[1], B.u[2], -A.u[2] * B.u[1]);
+    const float cy = __fmaf_rn(A.u[2], B.u[0], -A.u[0] * B.u[2]);
+    s2 = __fmaf_rn(cx, cx, __fmaf_rn(cy, cy, cz * cz));
+  } else {
+    s2 = cz * cz;
+  }
+  return s2 > 0.f && s2 < 1e-5f;
+}
+
+// A nearly parallel pair of the mixed pair stage, evaluated as the FP64 path
+// evaluates it -- from both bonds' FP64 sites, which both paths share -- and
+// written as the pair stage writes every pair (its two slots, its stored
+// force, its virial record).
+template <int ND>
+__device__ __forceinline__ void pair_eval_fp64_sites(const SysConst &k, const DevState &d,
+                                                  const ReplicaConst &R, int p) {
+  const int a = d.pa[p], b = d.pb[p];
+  BondGeomF64 A64, B64;
+  bond_geom_from_sites<ND>(d, R, a, A64);
+  bond_geom_from_sites<ND>(d, R, b, B64);
+  PairGeom<double> g;
+  sphero_f64<ND>(R.h, A64, B64, g);
+  float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
+  const float4 st = *stale;
+  double f[3] = {st.x, st.y, st.z}, rec[4];
+  if (wca_f64<ND>(k, g, f, k.thermo ? rec : nullptr)) {
+    if (ND == 2) f[2] = st.z;
+    *stale = make_float4((float)f[0], (float)f[1], (float)f[2], 0.f);
+    if (k.thermo)
+      reinterpret_cast<float4 *>(d.pv32)[p] =
+          make_float4((float)rec[0], (float)rec[1], (float)rec[2], (float)rec[3]);
+  }
+  double t1[3], t2[3];
+  cross3(g.c1, f, t1);
+  cross3(g.c2, f, t2);
+  float4 *c1 = reinterpret_cast<float4 *>(d.cf32) + 2 * (size_t)d.pos1[p];
+  float4 *c2 = reinterpret_cast<float4 *>(d.cf32) + 2 * (size_t)d.pos2[p];
+  c1[0] = make_float4((float)f[0], (float)f[1], (float)f[2], (float)t1[0]);
+  c1[1] = make_float4((float)t1[1], (float)t1[2], 0.f, 0.f);
+  c2[0] = make_float4(-(float)f[0], -(float)f[1], -(float)f[2], -(float)t2[0]);
+  c2[1] = make_float4(-(float)t2[1], -(float)t2[2], 0.f, 0.f);
+}
+
+template <int ND, int PREC, bool NPX>
 __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
                                               const ReplicaConst &R, int rbuf, int p) {
   const int a = d.pa[p], b = d.pb[p];
@@ -603,25 +672,35 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
-    PairGeom<float> g;
-    sphero_f32<ND>(R.hf, A, B, g);
-    float force[3], rec[4];
-    if (!wca_f32<ND>(k, g, force, k.thermo ? rec : nullptr)) {
-      force[0] = st.x;
-      force[1] = st.y;
-      force[2] = st.z;
-    } else {
-      if (ND == 2) force[2] = st.z;
+    if (NPX && near_parallel<ND>(A, B)) {  // left to k_pair_fixup
+      d.fix_list[atomicAdd(d.fix_count, 1)] = p;
+      return;
+    }
+    float force[3], rec[4], t1[3], t2[3];
+    bool set;
+    {
+      PairGeom<float> g;
+      sphero_f32<ND>(R.hf, A, B, g);
+      set = wca_f32<ND>(k, g, force, k.thermo ? rec : nullptr);
+      if (!set) {
+        force[0] = st.x;
+        force[1] = st.y;
+        force[2] = st.z;
+      } else if (ND == 2) {
+        force[2] = st.z;
+      }
+      t1[0] = g.c1[1] * force[2] - g.c1[2] * force[1];
+      t1[1] = g.c1[2] * force[0] - g.c1[0] * force[2];
+      t1[2] = g.c1[0] * force[1] - g.c1[1] * force[0];
+      t2[0] = g.c2[1] * force[2] - g.c2[2] * force[1];
+      t2[1] = g.c2[2] * force[0] - g.c2[0] * force[2];
+      t2[2] = g.c2[0] * force[1] - g.c2[1] * force[0];
+    }
+    if (set) {
       *stale = make_float4(force[0], force[1], force[2], 0.f);
       if (k.thermo)
         reinterpret_cast<float4 *>(d.pv32)[p] = make_float4(rec[0], rec[1], rec[2], rec[3]);
     }
-    float t1[3] = {g.c1[1] * force[2] - g.c1[2] * force[1],
-                   g.c1[2] * force[0] - g.c1[0] * force[2],
-                   g.c1[0] * force[1] - g.c1[1] * force[0]};
-    float t2[3] = {g.c2[1] * force[2] - g.c2[2] * force[1],
-                   g.c2[2] * force[0] - g.c2[0] * force[2],
-                   g.c2[0] * force[1] - g.c2[1] * force[0]};
     float4 *c1 = reinterpret_cast<float4 *>(d.cf32) + 2 * (size_t)s1;
     float4 *c2 = reinterpret_cast<float4 *>(d.cf32) + 2 * (size_t)s2;
     c1[0] = make_float4(force[0], force[1], force[2], t1[0]);
@@ -631,23 +710,45 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
   }
 }
 
+// The nearly parallel pairs the NPX mixed pair stage left, evaluated from the
+// FP64 sites (pair_eval_fp64_sites).  The last block out resets the list
+// (ticket counter, no waiting) for the next pair stage.
+template <int ND>
+__global__ void __launch_bounds__(128) k_pair_fixup(SysConst k, DevState d) {
+  const int n = *d.fix_count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int p = d.fix_list[i];
+    const int r = d.nrep == 1 ? 0 : rep_of_pair(d, p);
+    pair_eval_fp64_sites<ND>(k, d, d.rep[r], p);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(d.fix_done, 1u) == gridDim.x - 1) {
+      *d.fix_count = 0;
+      *d.fix_done = 0u;
+    }
+  }
+}
+
 // Grid-stride over the pair slots, so a captured launch stays correct
 // whatever length the lists grow to between captures.  A single system's
 // list is the prefix of its segment; with several systems every slot checks
 // that it holds a current pair of its system.
-template <int ND, int PREC>
+// NPX (mixed only): nearly parallel pairs go to k_pair_fixup.
+template <int ND, int PREC, bool NPX>
 __global__ void __launch_bounds__(256) k_pair_eval(SysConst k, DevState d, int rbuf) {
   if (d.nrep == 1) {
     const ReplicaConst &R = d.rep[0];
     const int np = min(d.np_rep[0], R.pcap);
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
-      pair_eval_one<ND, PREC>(k, d, R, rbuf, p);
+      pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p);
     return;
   }
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
        p += gridDim.x * blockDim.x) {
     int r;
-    if (pair_live(d, p, r)) pair_eval_one<ND, PREC>(k, d, d.rep[r], rbuf, p);
+    if (pair_live(d, p, r)) pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p);
   }
 }
 
@@ -1105,17 +1206,23 @@ int launch_zero_dr(const DevState &d, cudaStream_t st) {
 }
 
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
-                 int expected, cudaStream_t st) {
+                 int expected, cudaStream_t st, bool npx) {
   if (d.nrep > 1) expected = d.pcap_total;
   int grid = cdiv(expected > 0 ? expected : 1, 256);
+  npx = npx && prec != 0;
   if (k.n_dim == 3) {
-    if (prec == 0) k_pair_eval<3, 0><<<grid, 256, 0, st>>>(k, d, rbuf);
-    else k_pair_eval<3, 1><<<grid, 256, 0, st>>>(k, d, rbuf);
+    if (prec == 0) k_pair_eval<3, 0, false><<<grid, 256, 0, st>>>(k, d, rbuf);
+    else if (!npx) k_pair_eval<3, 1, false><<<grid, 256, 0, st>>>(k, d, rbuf);
+    else k_pair_eval<3, 1, true><<<grid, 256, 0, st>>>(k, d, rbuf);
   } else {
-    if (prec == 0) k_pair_eval<2, 0><<<grid, 256, 0, st>>>(k, d, rbuf);
-    else k_pair_eval<2, 1><<<grid, 256, 0, st>>>(k, d, rbuf);
+    if (prec == 0) k_pair_eval<2, 0, false><<<grid, 256, 0, st>>>(k, d, rbuf);
+    else if (!npx) k_pair_eval<2, 1, false><<<grid, 256, 0, st>>>(k, d, rbuf);
+    else k_pair_eval<2, 1, true><<<grid, 256, 0, st>>>(k, d, rbuf);
   }
-  return 1;
+  if (!npx) return 1;
+  if (k.n_dim == 3) k_pair_fixup<3><<<16, 128, 0, st>>>(k, d);
+  else k_pair_fixup<2><<<16, 128, 0, st>>>(k, d);
+  return 2;
 }
 
 // ---------------------------------------------------------------------------

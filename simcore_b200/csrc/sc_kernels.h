@@ -60,8 +60,10 @@ int launch_advance_mcount(const DevState &d, cudaStream_t st);
 int launch_zero_dr(const DevState &d, cudaStream_t st);
 // Grid sized for `expected` pairs (one system) or every slot (several); the
 // kernel strides over the actual pairs.
+// npx (mixed only): nearly parallel pairs are evaluated from the FP64
+// sites by a second kernel.
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
-                 int expected, cudaStream_t st);
+                 int expected, cudaStream_t st, bool npx = false);
 // Crosslink tethers of an even step into the per-anchor contributions.
 int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st);
 // Thermo: one step's pair virial per system, the pressure record every

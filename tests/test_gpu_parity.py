@@ -134,6 +134,52 @@ def test_mixed_force_error():
     assert et <= 1e-5, et
 
 
+@pytest.mark.parametrize("angle", [0.0, 3e-5, 1.7e-4, 2e-3, 5e-3])
+def test_mixed_near_parallel_pairs(angle):
+    """Two straight rods side by side 1.05 apart (inside the WCA range),
+    overlapping, at a small angle.  Within about 0.2 degrees of parallel,
+    FP32's 1 - c^2 is rounding alone and the closest points it finds can be
+    far off; with exact near-parallel pairs on, the mixed pair stage
+    evaluates those pairs from the FP64 sites (exactly parallel rods and
+    wider angles stay in FP32).  Forces and torques then match the FP64 path
+    to 1e-5 of the largest at every angle."""
+    R = 20.0
+    j = np.arange(11.0)
+    sites = np.zeros((22, 3))
+    sites[:11, 0] = j - 5.0
+    sites[11:, 0] = -4.7 + j * np.cos(angle)
+    sites[11:, 2] = 1.05 + j * np.sin(angle)
+    system = dict(n_dim=3, system_radius=R, delta=1e-4, seed=1, stoch_flag=0)
+    fils = [dict(length=10.0, persistence_length=100.0, diameter=1.0, min_bond_length=0.666,
+                 friction_ratio=2.0)] * 2
+    c64 = _ctx(system, fils, sites, "fp64")
+    c32 = _ctx(system, fils, sites, "mixed")
+    c32.set_exact_near_parallel(True)
+    assert len(c64.pairs()) > 0
+    for c in (c64, c32):
+        c.interact()
+    f64, t64 = c64.bond_forces()
+    f32, t32 = c32.bond_forces()
+    assert np.abs(f64).max() > 1.0
+    assert np.abs(f32 - f64).max() <= 1e-5 * np.abs(f64).max()
+    assert np.abs(t32 - t64).max() <= 1e-5 * max(np.abs(t64).max(), np.abs(f64).max())
+
+
+def test_exact_near_parallel_graph_matches_host():
+    """With exact near-parallel pairs on, the captured graph (which captures
+    the second kernel too) gives the host-driven loop's bits, on a batch of
+    independent 2D systems."""
+    system, fils, sites, reps = _replica_batch(3, 0.05, seed=4)
+    a = _ctx_replicas(system, fils, sites, reps, "mixed")
+    b = _ctx_replicas(system, fils, sites, reps, "mixed")
+    for c in (a, b):
+        c.set_exact_near_parallel(True)
+    a.step_graph(40)
+    b.step(40)
+    assert_same(a.sites(), b.sites(), "sites")
+    assert a.counters().n_rebuilds == b.counters().n_rebuilds
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_graph_path_matches_host_path(precision):
     """The captured WHILE-loop graph (device-decided rebuilds) gives the same
