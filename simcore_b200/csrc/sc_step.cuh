@@ -345,16 +345,17 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   }
   const bool active = t < count;
   const int g = s0 + t;
-  int f = 0, lf = 0;
+  // The site's place in its filament comes from site_jn, so every load of
+  // P0 is issued here, alongside the staging of the filament constants,
+  // rather than after the barrier.
+  int f = 0, lf = 0, jn = 0;
   if (active) {
     f = d.site_fil[g];
+    jn = d.site_jn[g];
     lf = f - f0;
   }
-  __syncthreads();
-  if (overflowed) return;
-  const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
-  const int n = active ? fc.n : 0;
-  const int j = active ? g - fc.site0 : -1;
+  const int n = active ? jn >> 16 : 0;
+  const int j = active ? jn & 0xffff : -1;
   const int base = t - j;            // slot of the filament's first site
   const int b = g - f;               // this thread's bond (valid when j < n-1)
   const bool has_bond = active && j < n - 1;
@@ -366,11 +367,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     r[0] = d.r[0][g];
     r[1] = d.r[1][g];
     r[2] = d.r[2][g];
-    if (midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
-      d.rp[0][g] = r[0];
-      d.rp[1][g] = r[1];
-      d.rp[2][g] = r[2];
-    } else {
+    if (!midstep) {
       // The full step needs the midstep's positions and projected noise
       // later; fetch them now, in the background.
       for (int i = 0; i < ND; ++i) cp_async8(&V(srp, t, i), &d.rp[i][g]);
@@ -386,6 +383,16 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     u[1] = d.ub[1][b];
     u[2] = d.ub[2][b];
     if (interaction) bond_pair_sum<ND, PREC>(d, b, bF, bT);
+  }
+  __syncthreads();
+  if (overflowed) return;
+  const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
+  if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
+    d.rp[0][g] = r[0];
+    d.rp[1][g] = r[1];
+    d.rp[2][g] = r[2];
+  }
+  if (has_bond) {
     for (int i = 0; i < 3; ++i) {
       V(su, t, i) = u[i];
       V(sbF, t, i) = bF[i];
