@@ -292,6 +292,65 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // MAXC: largest block (sites) the instantiation is launched with; blocks
 // per SM requested so that the register budget leaves room for several
 // blocks in flight.
+// Block-wide parallel cyclic reduction (Hockney, J. ACM 12:95-113, 1965;
+// Hockney & Jesshope, "Parallel Computers 2", 1988, sec. 5.4) of every
+// filament's tridiagonal system of the block at once, for the fast
+// integrator's blocks of long filaments: the rows laid out as solve_tridiag
+// takes them (row i of a filament at slot first + i: lower coefficient in
+// a[slot - 1], diagonal b, upper c, right-hand side d).  Each row thread
+// eliminates the unknowns s rows away on both sides (s = 1, 2, 4, ... below
+// max_rows), exchanging rows through the same arrays; a coupling that
+// reaches past its filament's rows is zero at every step, so it is skipped.
+// Every thread of the block calls it (max_rows is uniform); the solution
+// ends in d.  O(log n) steps instead of the O(n) sequential elimination,
+// with other rounding (the exact integrator keeps the reference's Thomas).
+__device__ __forceinline__ void pcr_block(double *a, double *b, double *c, double *d, bool row,
+                                          int t, int first, int last, int max_rows) {
+  double lo = 0.0, dg = 1.0, up = 0.0, rhs = 0.0;
+  if (row) {
+    lo = t > first ? a[t - 1] : 0.0;
+    dg = b[t];
+    up = t < last ? c[t] : 0.0;
+    rhs = d[t];
+  }
+  for (int s = 1; s < max_rows; s <<= 1) {
+    __syncthreads();  // every read of the previous values is done
+    if (row) {
+      a[t] = lo;
+      b[t] = dg;
+      c[t] = up;
+      d[t] = rhs;
+    }
+    __syncthreads();
+    if (row) {
+      const bool has_m = t - s >= first, has_p = t + s <= last;
+      double al = 0.0, ga = 0.0, ndg = dg, nrhs = rhs, nlo = 0.0, nup = 0.0;
+      if (has_m) {
+        al = -lo * recip_nr(b[t - s]);
+        ndg = fma(al, c[t - s], ndg);
+        nrhs = fma(al, d[t - s], nrhs);
+        nlo = al * a[t - s];
+      }
+      if (has_p) {
+        ga = -up * recip_nr(b[t + s]);
+        ndg = fma(ga, a[t + s], ndg);
+        nrhs = fma(ga, d[t + s], nrhs);
+        nup = ga * c[t + s];
+      }
+      lo = nlo;
+      up = nup;
+      dg = ndg;
+      rhs = nrhs;
+    }
+  }
+  __syncthreads();
+  if (row) d[t] = rhs * recip_nr(dg);
+}
+
+// Rows of the longest system (bonds of the longest filament) above which the
+// fast 256-site integrator solves by pcr_block instead of Thomas lanes.
+constexpr int kPcrMinRows = 32;
+
 template <int MAXC, bool FAST>
 struct IntegrateBounds {
   // The exact variant spills below 96 registers; the fast one fits 80.
@@ -387,6 +446,12 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   __syncthreads();
   if (overflowed) return;
   const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
+  // Fast 256-site blocks with a long filament solve by parallel cyclic
+  // reduction (uniform over the block).
+  int max_rows = 0;
+  if (FAST && MAXC > 128)
+    for (int q = 0; q < nfb; ++q) max_rows = max(max_rows, sfil[q].n - 1);
+  const bool pcr = FAST && MAXC > 128 && max_rows > kPcrMinRows;
   if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
     d.rp[0][g] = r[0];
     d.rp[1][g] = r[1];
@@ -514,7 +579,9 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
         }
       }
       __syncthreads();
-      if (t < nfb) {
+      if (pcr) {
+        pcr_block(sa, sb, sc, sT, has_bond, t, base, base + n - 2, max_rows);
+      } else if (t < nfb) {
         const int fb0 = sfil[t].site0 - s0;
         solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[t].n - 1);
       }
@@ -722,7 +789,9 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     }
   }
   __syncthreads();
-  if (t < nfb) {
+  if (pcr) {
+    pcr_block(sa, sb, sc, sT, has_bond, t, base, base + n - 2, max_rows);
+  } else if (t < nfb) {
     const int fb0 = sfil[t].site0 - s0;
     solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[t].n - 1);
   }

@@ -231,6 +231,29 @@ def test_graph_matches_oracle():
         compare_state(ctx, o, 3, capture=False)
 
 
+def test_fast_integrator_long_filaments_close_to_exact():
+    """Workload C's length spread (5 to 200 bonds): the fast integrator solves
+    the 256-site blocks that hold a filament of more than 32 bonds by
+    parallel cyclic reduction.  Against the exact integrator (the
+    reference's sequential Thomas) on identical forces, positions agree to
+    1e-12 relative after one BD step; the captured run gives the host-driven
+    loop's bits."""
+    system, fils, sites = _workload("C", 0.002, seed=3, side=150.0)
+    assert max(f["length"] for f in fils) > 128
+    a = _ctx(system, fils, sites, "mixed")
+    b = _ctx(system, fils, sites, "mixed")
+    b.set_fast_integrator(False)
+    a.step(2)
+    b.step(2)
+    ra, rb = a.sites(), b.sites()
+    assert np.abs(ra - rb).max() <= 1e-12 * np.abs(rb).max()
+    c = _ctx(system, fils, sites, "mixed")
+    d = _ctx(system, fils, sites, "mixed")
+    c.step_graph(40)
+    d.step(40)
+    assert_same(c.sites(), d.sites(), "sites")
+
+
 def test_fast_integrator_close_to_exact():
     """The mixed path's contraction/reciprocal integrator against the exact
     FP64 integrator on identical forces (both mixed precision): positions
