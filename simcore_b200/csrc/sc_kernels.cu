@@ -9,7 +9,10 @@
 //                  scatter order)
 //   pair forces    k_pair_eval   (InteractionManager::CalculatePairInteractions,
 //                                 one thread per pair, signed per-bond slots)
+//                  k_pair_fixup  (mixed, opt-in: nearly parallel pairs in FP64)
 //                  k_bond_sum    (ApplyPairInteractions into bond accumulators)
+//   thermo         k_thermo, k_potential (pair virial and pressure records,
+//                                 per-filament potential energy)
 //   integrator     k_integrate   (Filament::UpdatePosition for every
 //                                 filament; sums each bond's pair slots first)
 //   utilities      exclusive scan, geometry init, displacement reset.
