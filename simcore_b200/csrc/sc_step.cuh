@@ -618,6 +618,9 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   }
 
   // ---- P3: bending and metric forces (:608-776) ---------------------------
+  // The determinants below are written over the projection's solution in
+  // sT, which every thread has just read: all reads first.
+  if (midstep && k.stoch) __syncthreads();
   if (t < nfb) {  // det_t of filament t, forward
     const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
     double *dt = sdt + fb0 + t;
