@@ -444,7 +444,10 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     if (interaction) bond_pair_sum<ND, PREC>(d, b, bF, bT);
   }
   __syncthreads();
-  if (overflowed) return;
+  if (overflowed) {
+    cp_async_wait_all();  // no copy into this block's shared memory outlives it
+    return;
+  }
   const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
   // Fast 256-site blocks with a long filament solve by parallel cyclic
   // reduction (uniform over the block).
