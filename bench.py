@@ -69,6 +69,8 @@ def parse_args():
                     help="run this many host-driven steps and exit (for ncu)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of --profile-steps")
+    ap.add_argument("--profile-fused", action="store_true",
+                    help="--profile-steps with the pair evaluation fused into the integrator")
     ap.add_argument("--profile-layout", default=None,
                     help="integrator layout W,C for --profile-steps (warp-kernel sites, block "
                          "sites), e.g. the one the timed run's autotuner chose")
@@ -185,10 +187,33 @@ def algorithmic_bytes(n_sites, n_bonds, n_pairs, precision):
     return integrate, pairs
 
 
+def fused_bytes(n_sites, n_bonds, n_pairs):
+    """Bytes of one launch of the mixed integrator with the pair evaluation
+    fused in: the sites' 96 B, the bond geometry this step reads (32 B) and
+    the one it writes for the next (32 B), and 8 B of list per candidate pair.
+    The pair stage's per-bond accumulators are neither written nor read."""
+    return 96 * n_sites + 64 * n_bonds + 8 * n_pairs
+
+
+def step_kernel_time(ctx, n):
+    """Average CUDA-event duration (ms) of the kernels sc_step launches for a
+    reference step, over n host-driven steps (L2 warm): for the fast mixed
+    step that is the integrator with the pairs fused in, alone."""
+    t = 0.0
+    for _ in range(n):
+        ctx.set_kernel_timing(True)
+        ctx.step(1)
+        a, _ = ctx.kernel_timing()
+        t += a
+    ctx.set_kernel_timing(False)
+    return t / n
+
+
 def kernel_times(ctx, n):
     """Average CUDA-event duration (ms) of the pair kernel and of the
-    integrator over n host-driven reference steps on the context's stream
-    (L2 warm, as between the reference steps inside one timed launch)."""
+    integrator over n host-driven reference steps of the split interface
+    (sc_interact, then sc_update_positions) on the context's stream (L2
+    warm, as between the reference steps inside one timed launch)."""
     tp = ti = 0.0
     for _ in range(n):
         ctx.set_kernel_timing(True)
@@ -273,7 +298,8 @@ def cpu_runs(wl, cores):
 
 def profile_only(args):
     """--profile-steps N: host-driven reference steps of the bench workload
-    (one pair launch and one integrator launch each) after 4 warm-up steps,
+    (a pair launch and an integrator launch each; with --profile-fused, mixed,
+    one integrator launch with the pairs fused in) after 4 warm-up steps,
     nothing timed; the command the ncu captures run."""
     import simcore_b200 as sc
     from simcore_b200 import workloads
@@ -282,6 +308,8 @@ def profile_only(args):
     if args.profile_layout:
         layout = [int(v) for v in args.profile_layout.split(",")]
         ctx.set_integrator_layout(*layout)
+    if args.profile_fused:
+        ctx.set_fused_pairs(True)
     ctx.step(4)
     ctx.step(args.profile_steps)
     ctx.synchronize()
@@ -370,9 +398,14 @@ def run_ours(args, rank, world, local_rank):
     force_err, torque_err = rel_err("mixed", 0), rel_err("mixed", 1)
 
     # Roofline: per-launch CUDA-event durations of the two kernels of a
-    # reference step, host-driven, on the context's stream.
+    # reference step, host-driven, on the context's stream; beside them the
+    # integrator with the pairs fused in (sc_set_fused_pairs, off in the
+    # timed runs).
     kt = {p: kernel_times(contexts[p], 2 * I_STEPS_PER_STEP) for p in ("mixed", "fp64")}
     ctx = contexts["mixed"]
+    ctx.set_fused_pairs(True)
+    t_fused = step_kernel_time(ctx, 2 * I_STEPS_PER_STEP)
+    ctx.set_fused_pairs(False)
 
     # End to end through the C ABI with host buffers: every bench step
     # uploads the positions from pinned host memory, runs the 20 reference
@@ -419,6 +452,7 @@ def run_ours(args, rank, world, local_rank):
         return b_int, b_pair, t_pair, t_int
 
     b_int, b_pair, t_pair, t_int = roof("mixed")
+    b_fused = fused_bytes(r["n_sites"], r["n_bonds"], r["n_pairs"])
     achieved = b_int / (t_int * 1e-3) / 1e9
     step_achieved = (b_int + b_pair) / ((t_int + t_pair) * 1e-3) / 1e9
     b_int64, b_pair64, t_pair64, t_int64 = roof("fp64")
@@ -463,6 +497,11 @@ def run_ours(args, rank, world, local_rank):
                                         "algorithmic_bytes": b_int + b_pair,
                                         "ms": t_int + t_pair, "achieved": step_achieved,
                                         "frac": step_achieved / peak},
+                     "fused_pairs_option": {
+                         "kernel": "k_integrate<%d,mixed,fast,fused pairs> (sc_set_fused_pairs; "
+                                   "off in the timed runs)" % r["n_dim"],
+                         "avg_launch_ms": t_fused, "algorithmic_bytes_per_launch": b_fused,
+                         "achieved": b_fused / (t_fused * 1e-3) / 1e9},
                      "reference_step_fp64": {"algorithmic_bytes": b_int64 + b_pair64,
                                              "ms": t_int64 + t_pair64, "achieved": step64,
                                              "frac": step64 / peak}},

@@ -202,6 +202,15 @@ sc_status sc_get_potential_energy(sc_ctx *ctx, double *pote);
  * kernel costs about 10% of the step on workload B.  No counterpart in the
  * reference, whose pair stage is FP64 throughout. */
 sc_status sc_set_exact_near_parallel(sc_ctx *ctx, int on);
+/* Fast mixed precision only (not with thermo or the option above): sc_step
+ * and sc_step_graph evaluate each bond's pairs inside the integrator and
+ * launch no pair stage.  The results are bit-identical to the separate pair
+ * stage, and sc_get_bond_forces still returns the last step's evaluation.
+ * Off by default: every bond walks its own pairs one after another, and on
+ * workload B the fused integrator (58.5 us) is slower than the pair stage
+ * and the integrator together (54.9 us).  No counterpart in the
+ * reference. */
+sc_status sc_set_fused_pairs(sc_ctx *ctx, int on);
 /* Per-system rebuild counts and current pair counts (n_replicas entries
  * each; either pointer may be NULL). */
 sc_status sc_get_replica_counters(sc_ctx *ctx, int64_t *n_rebuilds, int64_t *n_pairs);

@@ -108,8 +108,13 @@ struct sc_ctx {
   long long timed_launches = 0;
   cudaEvent_t gev0 = nullptr, gev1 = nullptr;  // around each graph launch
   double graph_ms = 0.0;
+  bool graph_fused = false;  // the captured steps evaluate their pairs in the integrator
   long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
   bool npx = false;           // mixed: near-parallel pairs evaluated from FP64 sites
+  // The last step fused its pair evaluation into the integrator, so the
+  // per-bond slots do not hold it yet (materialize_slots writes them).
+  bool slots_stale = false;
+  bool fuse_pairs = false;  // sc_set_fused_pairs
 
   // thermo (sc_set_thermo): records are produced on the device every th_n
   // steps and pulled into th_host (and the open .thermo files)
@@ -675,11 +680,23 @@ sc_status thermo_reserve(sc_ctx *c, long long n) {
   return SC_OK;
 }
 
+// With sc_set_fused_pairs, the fast mixed step evaluates the pairs inside the
+// integrator (each bond its own pairs, bit for bit the pair stage's forces)
+// and launches no pair stage.  Not with thermo (whose records the pair stage
+// writes), nor with the FP64 evaluation of nearly parallel pairs; the split
+// interface (sc_interact, then sc_update_positions) keeps the separate pair
+// stage.
+bool fused_pairs(const sc_ctx *c) {
+  return c->fuse_pairs && c->desc.interaction_flag && c->prec == 1 && c->fast &&
+         !c->k.thermo && !c->npx;
+}
+
 // The pair stage of one step, then the step's thermo accumulation.
 sc_status pair_stage(sc_ctx *c) {
   CKS(timed(c, [&] {
     return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st, c->npx);
   }));
+  c->slots_stale = false;
   if (c->k.thermo) c->launches += sc::launch_thermo(c->k, c->d, c->prec, c->st);
   return SC_OK;
 }
@@ -690,18 +707,34 @@ sc_status step_once(sc_ctx *c) {
   tether_if_due(c);
   CKS(maybe_rebuild(c));
   const int interaction = c->desc.interaction_flag ? 1 : 0;
-  if (interaction) CKS(pair_stage(c));
+  const bool fuse = fused_pairs(c);
+  if (interaction && !fuse) CKS(pair_stage(c));
   CKS(timed(c, [&] {
     return sc::launch_integrate(c->k, c->d, c->nblocks, c->C, c->midstep, c->rbuf,
-                                interaction, c->capture, c->prec, c->fast, c->st);
+                                interaction, c->capture, c->prec, c->fast, c->st, fuse);
   }));
   if (c->midstep && c->desc.stoch_flag)
     c->launches += sc::launch_advance_mcount(c->d, c->st);
   CK(cudaGetLastError());
   c->pairs_ready = false;
+  if (fuse) c->slots_stale = true;
   if (c->midstep && c->desc.stoch_flag) c->mcount++;
   c->midstep = !c->midstep;
   c->rbuf = 1 - c->rbuf;
+  return SC_OK;
+}
+
+// The slots of the last fused step, written by the pair stage run again on
+// that step's geometry: the buffer the step read (1 - rbuf), which nothing
+// writes before the next step (sc_set_sites fills the other one).  With the
+// same pair list, geometry and stored forces, every pair in range gets the
+// bits the step computed and every other pair re-reads its unchanged stored
+// force, so the slots are those a separate pair stage would have left.
+sc_status materialize_slots(sc_ctx *c) {
+  if (!c->slots_stale) return SC_OK;
+  c->launches += sc::launch_pairs(c->k, c->d, 1 - c->rbuf, c->prec, (int)c->np, c->st, false);
+  CK(cudaGetLastError());
+  c->slots_stale = false;
   return SC_OK;
 }
 
@@ -1116,6 +1149,7 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
   for (int attempt = 0;; ++attempt) {
     CKS(layout_pairs(c, want));
     CKS(rebuild_all(c));
+    c->slots_stale = false;
     bool ok = true;
     for (int r = 0; r < nrep; ++r) {
       const long long need = (long long)c->np_rep[r] + c->np_rep[r] / 2 + 1024;
@@ -1248,15 +1282,17 @@ static sc_status build_graph(sc_ctx *c) {
   }
   CK(cudaStreamBeginCaptureToGraph(c->st, body, tail.empty() ? nullptr : tail.data(), nullptr,
                                    tail.size(), cudaStreamCaptureModeRelaxed));
+  const bool fuse = fused_pairs(c);
+  c->graph_fused = fuse;
   for (int half = 0; half < 2; ++half) {
     const int rb = half == 0 ? c->rbuf : 1 - c->rbuf;
     // The second half is the even (full) step: crosslink tethers first.
     if (half == 1 && interaction) sc::launch_tether(c->k, c->d, c->st);
-    if (interaction)
+    if (interaction && !fuse)
       sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
     if (interaction && c->k.thermo) sc::launch_thermo(c->k, c->d, c->prec, c->st);
     sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
-                         c->capture, c->prec, c->fast, c->st);
+                         c->capture, c->prec, c->fast, c->st, fuse);
   }
   sc::launch_loop_tail(c->d, c->desc.stoch_flag ? 1 : 0, h_loop, c->st);
   CK(cudaStreamEndCapture(c->st, &body));
@@ -1314,6 +1350,7 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       const bool overflow = (st & sc::ST_LIST_OVERFLOW) != 0u;
       // BD steps completed: all of them, or those before the stopped one.
       const int done = overflow ? bd - *c->h_loop : bd;
+      if (c->graph_fused && done > 0) c->slots_stale = true;
       c->i_step += 2 * (long long)done;
       if (c->desc.stoch_flag) c->mcount += done;
       {
@@ -1321,13 +1358,18 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
         CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
         c->graph_ms += ms;
       }
-      // Kernels the graph ran: loop head, per BD step decide + 2 steps +
-      // tail (the stopped step's too), per rebuild the captured sequence.
-      c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) *
-                             (c->desc.interaction_flag
-                                  ? (c->d.nx ? 7 : 6) + (c->k.thermo ? 2 : 0) +
-                                        (c->npx && c->prec ? 2 : 0)
-                                  : 3) +
+      // Kernels the graph ran: loop head, per BD step decide + tether + 2
+      // steps + tail (the stopped step's too), per rebuild the captured
+      // sequence.  A step is its pair stage (unless fused), thermo, the
+      // near-parallel fix-up and one or two integrator kernels.
+      const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
+      const long long per_bd =
+          c->desc.interaction_flag
+              ? 2 + (c->d.nx ? 1 : 0) +
+                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0) +
+                         (c->npx && c->prec ? 1 : 0))
+              : 1 + 2 * int_l;
+      c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
                      (nr1 - nr0) * c->rebuild_kernels;
       bd -= done;
       if (!overflow) {
@@ -1398,6 +1440,7 @@ sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
   // Bond accumulators of the last pair evaluation (Bond::force_/torque_
   // after Interact), summed from its per-bond slots.
   if (c->desc.interaction_flag) {
+    CKS(materialize_slots(c));
     c->launches += sc::launch_bond_sum(c->k, c->d, c->prec, c->st);
   } else {
     for (int i = 0; i < 3; ++i) {
@@ -1445,9 +1488,10 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
     max_n = std::max(max_n, nn);
   }
   char key[512];
-  std::snprintf(key, sizeof(key), "v1|%s|sm%d|nd%d|prec%d|fast%d|nf%d|ns%d|n%d-%d", prop.name,
-                prop.multiProcessorCount, c->nd, c->prec, (c->prec == 1 && c->fast) ? 1 : 0, c->nf,
-                c->ns, min_n, max_n);
+  const bool fuse = fused_pairs(c);
+  std::snprintf(key, sizeof(key), "v2|%s|sm%d|nd%d|prec%d|fast%d|fuse%d|nf%d|ns%d|n%d-%d",
+                prop.name, prop.multiProcessorCount, c->nd, c->prec,
+                (c->prec == 1 && c->fast) ? 1 : 0, fuse ? 1 : 0, c->nf, c->ns, min_n, max_n);
   auto finish = [&](int w, int b) -> sc_status {
     if (warp_sites_out) *warp_sites_out = w;
     if (block_sites_out) *block_sites_out = b;
@@ -1503,6 +1547,7 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   else regions.push_back({c->d.g32[wbuf], sizeof(sc::BondGeomF32) * c->nb});
   regions.push_back({c->d.dr_max_bits, sizeof(unsigned long long) * c->d.nrep});
   regions.push_back({c->d.status, sizeof(unsigned)});
+  if (fuse) regions.push_back({c->d.pf32, sizeof(float) * 4 * c->d.pcap_total});
   size_t total = 0;
   for (auto &r : regions) total += (r.second + 255) & ~(size_t)255;
   char *save = nullptr;
@@ -1533,11 +1578,11 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
     if (st != SC_OK) break;
     for (int it = 0; it < 2; ++it)
       sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1 - it, c->rbuf, interaction, 0,
-                           c->prec, c->fast, c->st);
+                           c->prec, c->fast, c->st, fuse);
     cudaEventRecord(e0, c->st);
     for (int it = 0; it < 8; ++it)
       sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1 - (it & 1), c->rbuf, interaction, 0,
-                           c->prec, c->fast, c->st);
+                           c->prec, c->fast, c->st, fuse);
     cudaEventRecord(e1, c->st);
     if (cudaEventSynchronize(e1) != cudaSuccess) {
       st = fail(c, SC_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1649,6 +1694,7 @@ sc_status sc_checkpoint(sc_ctx *c, void *buf, size_t cap, size_t *size) {
   *size = need;
   if (!buf) return SC_OK;
   if (cap < need) return fail(c, SC_ERR_INVALID_ARG, "checkpoint needs %zu bytes", need);
+  CKS(materialize_slots(c));
   CKS(readback(c));
   long long nr = 0;
   CK(cudaMemcpyAsync(&nr, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
@@ -1728,6 +1774,7 @@ sc_status sc_restore(sc_ctx *c, const void *buf, size_t size) {
   c->mcount = h.mcount;
   c->midstep = h.midstep;
   c->pairs_ready = false;
+  c->slots_stale = false;  // the checkpoint's slots hold its last evaluation
   if (c->k.thermo) {  // records restart from the restored step
     CK(cudaMemsetAsync(c->d.th_nrec, 0, sizeof(long long) * c->d.nrep, c->st));
     CK(cudaMemsetAsync(c->d.th_ticket, 0, sizeof(unsigned) * c->d.nrep, c->st));
@@ -2207,6 +2254,16 @@ sc_status sc_set_exact_near_parallel(sc_ctx *c, int on) {
   c->npx = on != 0;
   if (c->npx && !c->d.fix_list) CKS(alloc_fixup(c, c->pcap));
   CK(cudaStreamSynchronize(c->st));
+  drop_graph(c);
+  return SC_OK;
+}
+
+sc_status sc_set_fused_pairs(sc_ctx *c, int on) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  if (c->fuse_pairs == (on != 0)) return SC_OK;
+  CK(cudaSetDevice(c->desc.device));
+  CK(cudaStreamSynchronize(c->st));
+  c->fuse_pairs = on != 0;
   drop_graph(c);
   return SC_OK;
 }

@@ -680,25 +680,8 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
       return;
     }
     float force[3], rec[4], t1[3], t2[3];
-    bool set;
-    {
-      PairGeom<float> g;
-      sphero_f32<ND>(R.hf, A, B, g);
-      set = wca_f32<ND>(k, g, force, k.thermo ? rec : nullptr);
-      if (!set) {
-        force[0] = st.x;
-        force[1] = st.y;
-        force[2] = st.z;
-      } else if (ND == 2) {
-        force[2] = st.z;
-      }
-      t1[0] = g.c1[1] * force[2] - g.c1[2] * force[1];
-      t1[1] = g.c1[2] * force[0] - g.c1[0] * force[2];
-      t1[2] = g.c1[0] * force[1] - g.c1[1] * force[0];
-      t2[0] = g.c2[1] * force[2] - g.c2[2] * force[1];
-      t2[1] = g.c2[2] * force[0] - g.c2[0] * force[2];
-      t2[2] = g.c2[0] * force[1] - g.c2[1] * force[0];
-    }
+    const bool set = pair_force_f32<ND>(k, R.hf, A, B, st, force, t1, t2,
+                                        k.thermo ? rec : nullptr);
     if (set) {
       *stale = make_float4(force[0], force[1], force[2], 0.f);
       if (k.thermo)
@@ -1425,9 +1408,10 @@ void prepare_integrate(int C) {
 
 int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
                      int midstep, int rbuf, int interaction, int capture,
-                     int prec, bool fast, cudaStream_t st) {
+                     int prec, bool fast, cudaStream_t st, bool fuse) {
   if (fast && prec == 1)
-    return launch_integrate_fast(k, d, nblocks, C, midstep, rbuf, interaction, capture, st);
+    return launch_integrate_fast(k, d, nblocks, C, midstep, rbuf, interaction, capture, st,
+                                 fuse && interaction);
   int launched = 0;
   if (d.n_wg > 0) {
     const int grid = cdiv(d.n_wg, kIntWarps);

@@ -75,12 +75,14 @@ int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t
 size_t integrate_smem_bytes(int C);
 void prepare_integrate(int C);
 // fast: the contraction/reciprocal variant (mixed precision only).
+// fuse (fast mixed only): the integrator evaluates the pairs itself, in place
+// of the pair stage (launch_pairs is then not launched for the step).
 int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
                      int midstep, int rbuf, int interaction, int capture,
-                     int prec, bool fast, cudaStream_t st);
+                     int prec, bool fast, cudaStream_t st, bool fuse = false);
 void prepare_integrate_fast(int C);
 int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int C,
                           int midstep, int rbuf, int interaction, int capture,
-                          cudaStream_t st);
+                          cudaStream_t st, bool fuse);
 
 }  // namespace sc

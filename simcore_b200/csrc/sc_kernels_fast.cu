@@ -15,7 +15,9 @@ namespace sc {
 
 template <int ND, int MAXC>
 static void set_attr_fast(size_t smem) {
-  cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC>,
+  cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
@@ -30,34 +32,35 @@ void prepare_integrate_fast(int C) {
   }
 }
 
-int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int C,
-                          int midstep, int rbuf, int interaction, int capture,
-                          cudaStream_t st) {
+template <int ND, bool FUSE>
+static int launch_fast(const SysConst &k, const DevState &d, int nblocks, int C, int midstep,
+                       int rbuf, int interaction, int capture, cudaStream_t st) {
   int launched = 0;
   if (d.n_wg > 0) {
     const int grid = (d.n_wg + kIntWarps - 1) / kIntWarps;
-    if (k.n_dim == 3)
-      k_integrate_warp<3, 1, true><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf,
-                                                                    interaction, capture);
-    else
-      k_integrate_warp<2, 1, true><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf,
-                                                                    interaction, capture);
+    k_integrate_warp<ND, 1, true, FUSE><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf,
+                                                                        interaction, capture);
     ++launched;
   }
   if (nblocks == 0) return launched;
-  size_t smem = integrate_smem_bytes(C);
-  if (C <= 128) {
-    if (k.n_dim == 3)
-      k_integrate<3, 1, true, 128><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
-    else
-      k_integrate<2, 1, true, 128><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
-  } else {
-    if (k.n_dim == 3)
-      k_integrate<3, 1, true, 256><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
-    else
-      k_integrate<2, 1, true, 256><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, interaction, capture);
-  }
+  const size_t smem = integrate_smem_bytes(C);
+  if (C <= 128)
+    k_integrate<ND, 1, true, 128, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
+                                                                  interaction, capture);
+  else
+    k_integrate<ND, 1, true, 256, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
+                                                                  interaction, capture);
   return launched + 1;
+}
+
+int launch_integrate_fast(const SysConst &k, const DevState &d, int nblocks, int C,
+                          int midstep, int rbuf, int interaction, int capture,
+                          cudaStream_t st, bool fuse) {
+  if (k.n_dim == 3)
+    return fuse ? launch_fast<3, true>(k, d, nblocks, C, midstep, rbuf, interaction, capture, st)
+                : launch_fast<3, false>(k, d, nblocks, C, midstep, rbuf, interaction, capture, st);
+  return fuse ? launch_fast<2, true>(k, d, nblocks, C, midstep, rbuf, interaction, capture, st)
+              : launch_fast<2, false>(k, d, nblocks, C, midstep, rbuf, interaction, capture, st);
 }
 
 }  // namespace sc

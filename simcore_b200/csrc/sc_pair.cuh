@@ -261,10 +261,12 @@ __device__ __forceinline__ void sphero_f32(const float *hf,
     }
   }
   g.dr_mag2 = r2;
+  // Explicit roundings here and below: no unit's contraction setting can
+  // fuse these products into a later sum, so every unit computes one bits.
 #pragma unroll
   for (int i = 0; i < ND; ++i) {
-    g.c1[i] = lambda * A.u[i];
-    g.c2[i] = mu * B.u[i];
+    g.c1[i] = __fmul_rn(lambda, A.u[i]);
+    g.c2[i] = __fmul_rn(mu, B.u[i]);
   }
 #pragma unroll
   for (int i = ND; i < 3; ++i) g.dr[i] = g.c1[i] = g.c2[i] = 0.0f;
@@ -287,7 +289,7 @@ __device__ __forceinline__ bool wca_f32(const SysConst &k, PairGeom<float> &g,
     if (rmag < 1e-12f) return false;
     float s = k.fcutf / rmag;
 #pragma unroll
-    for (int i = 0; i < ND; ++i) force[i] = s * dr[i];
+    for (int i = 0; i < ND; ++i) force[i] = __fmul_rn(s, dr[i]);
     if (rec) {
       for (int i = 0; i < 3; ++i) rec[i] = i < ND ? dr[i] : 0.f;
       rec[3] = 0.f;
@@ -301,12 +303,43 @@ __device__ __forceinline__ bool wca_f32(const SysConst &k, PairGeom<float> &g,
   if (fabsf(ffac) > k.fcutf) ffac = (ffac >= 0.0f ? k.fcutf : -k.fcutf);
   float s = ffac * rinv;
 #pragma unroll
-  for (int i = 0; i < ND; ++i) force[i] = s * g.dr[i];
+  for (int i = 0; i < ND; ++i) force[i] = __fmul_rn(s, g.dr[i]);
   if (rec) {
     for (int i = 0; i < 3; ++i) rec[i] = i < ND ? g.dr[i] : 0.f;
-    rec[3] = __fmaf_rn(k.c12f, r6, -k.c6f) * r6 + k.epsf;
+    rec[3] = __fadd_rn(__fmul_rn(__fmaf_rn(k.c12f, r6, -k.c6f), r6), k.epsf);
   }
   return true;
+}
+
+// One pair of the mixed-precision pair stage: ProcessPairInteraction and the
+// two torque cross products of InteractionManager::CalculatePairInteractions
+// (src/interaction_manager.cpp:448-481).  Out of range, the force is the
+// pair's stored one (st); in 2D the stored z component stays.  Returns
+// whether the force was computed (and is to be stored).  The pair stage and
+// the fused integrator both call this, and its products are explicitly
+// rounded, so the two give the same bits.
+template <int ND>
+__device__ __forceinline__ bool pair_force_f32(const SysConst &k, const float *hf,
+                                               const BondGeomF32 &A, const BondGeomF32 &B,
+                                               const float4 &st, float force[3], float t1[3],
+                                               float t2[3], float *rec = nullptr) {
+  PairGeom<float> g;
+  sphero_f32<ND>(hf, A, B, g);
+  const bool set = wca_f32<ND>(k, g, force, rec);
+  if (!set) {
+    force[0] = st.x;
+    force[1] = st.y;
+    force[2] = st.z;
+  } else if (ND == 2) {
+    force[2] = st.z;
+  }
+  t1[0] = __fsub_rn(__fmul_rn(g.c1[1], force[2]), __fmul_rn(g.c1[2], force[1]));
+  t1[1] = __fsub_rn(__fmul_rn(g.c1[2], force[0]), __fmul_rn(g.c1[0], force[2]));
+  t1[2] = __fsub_rn(__fmul_rn(g.c1[0], force[1]), __fmul_rn(g.c1[1], force[0]));
+  t2[0] = __fsub_rn(__fmul_rn(g.c2[1], force[2]), __fmul_rn(g.c2[2], force[1]));
+  t2[1] = __fsub_rn(__fmul_rn(g.c2[2], force[0]), __fmul_rn(g.c2[0], force[2]));
+  t2[2] = __fsub_rn(__fmul_rn(g.c2[0], force[1]), __fmul_rn(g.c2[1], force[0]));
+  return set;
 }
 
 }  // namespace sc

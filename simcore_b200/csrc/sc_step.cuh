@@ -162,6 +162,60 @@ __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F
   }
 }
 
+// Bond::force_ / torque_ of the mixed step with the pair stage fused in.
+// The bond evaluates each of its pairs itself (pair_force_f32 on both bonds'
+// FP32 geometry of this step), in entry (= slot) order, and adds its side of
+// the force and torque exactly as bond_pair_sum adds the slots the pair stage
+// would have written: the same values in the same order, so the same bits.
+// Both bonds of a pair evaluate it.  The first (role 0) stores the force, and
+// only when it was computed; the second reads the stored force only when it
+// was not, so no bond reads a value that another is writing for this step.
+template <int ND>
+__device__ __forceinline__ void bond_pair_eval_sum(const SysConst &k, const DevState &d,
+                                                   const float *hf, int rbuf, int b,
+                                                   double F[3], double T[3]) {
+  const int e0 = d.e_off[b], e1 = e0 + d.e_cnt[b];
+  F[0] = F[1] = F[2] = 0.0;
+  T[0] = T[1] = T[2] = 0.0;
+  if (d.nx) bond_xlink_sum<ND>(d, b, F, T);
+  float sF[3] = {0.f, 0.f, 0.f}, cF[3] = {0.f, 0.f, 0.f};
+  float sT[3] = {0.f, 0.f, 0.f}, cT[3] = {0.f, 0.f, 0.f};
+  for (int e = e0; e < e1; ++e) {
+    const int ent = d.e_ent[e], p = ent >> 1;
+    const BondGeomF32 A = d.g32[rbuf][d.pa[p]], B = d.g32[rbuf][d.pb[p]];
+    float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
+    float f[3], t1[3], t2[3], v[6];
+    const bool set = pair_force_f32<ND>(k, hf, A, B, *stale, f, t1, t2);
+    if (ent & 1) {
+      v[0] = -f[0];
+      v[1] = -f[1];
+      v[2] = -f[2];
+      v[3] = -t2[0];
+      v[4] = -t2[1];
+      v[5] = -t2[2];
+    } else {
+      if (set) *stale = make_float4(f[0], f[1], f[2], 0.f);
+      v[0] = f[0];
+      v[1] = f[1];
+      v[2] = f[2];
+      v[3] = t1[0];
+      v[4] = t1[1];
+      v[5] = t1[2];
+    }
+    kahan_add(sF[0], cF[0], v[0]);
+    kahan_add(sF[1], cF[1], v[1]);
+    if (ND == 3) kahan_add(sF[2], cF[2], v[2]);
+    kahan_add(sT[0], cT[0], v[3]);
+    kahan_add(sT[1], cT[1], v[4]);
+    kahan_add(sT[2], cT[2], v[5]);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    F[i] += (double)sF[i] - (double)cF[i];
+    T[i] += (double)sT[i] - (double)cT[i];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Integrator.  A block holds a run of whole filaments, one thread per site,
 // filaments back to back.  Per-site work runs in parallel; the sequential
@@ -357,7 +411,9 @@ struct IntegrateBounds {
   static constexpr int min_blocks = MAXC <= 128 ? (FAST ? 6 : 5) : 2;
 };
 
-template <int ND, int PREC, bool FAST, int MAXC>
+// FUSE (fast mixed step only): each bond evaluates its own pairs
+// (bond_pair_eval_sum) instead of summing the pair stage's slots.
+template <int ND, int PREC, bool FAST, int MAXC, bool FUSE = false>
 __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     k_integrate(SysConst k, DevState d, int midstep, int rbuf, int interaction,
                 int capture) {
@@ -441,7 +497,17 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     u[0] = d.ub[0][b];
     u[1] = d.ub[1][b];
     u[2] = d.ub[2][b];
-    if (interaction) bond_pair_sum<ND, PREC>(d, b, bF, bT);
+    if (interaction) {
+      // (The fused evaluation follows the pair list only when the rebuild
+      // of this step completed it.)
+      if (FUSE) {
+        if (!overflowed)
+          bond_pair_eval_sum<ND>(k, d, d.rep[d.nrep == 1 ? 0 : d.fil[f].rep].hf, rbuf, b,
+                                 bF, bT);
+      } else {
+        bond_pair_sum<ND, PREC>(d, b, bF, bT);
+      }
+    }
   }
   __syncthreads();
   if (overflowed) {

@@ -26,7 +26,9 @@ __device__ __forceinline__ double shfl_next(double v, int dist) {
   return __shfl_down_sync(0xffffffffu, v, dist);
 }
 
-template <int ND, int PREC, bool FAST>
+// FUSE (fast mixed step only): each bond evaluates its own pairs
+// (bond_pair_eval_sum) instead of summing the pair stage's slots.
+template <int ND, int PREC, bool FAST, bool FUSE = false>
 __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
     k_integrate_warp(SysConst k, DevState d, int midstep, int rbuf, int interaction,
                      int capture) {
@@ -83,7 +85,15 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
     if (interaction) dtot = d.dt[g];
   }
   double bF[3] = {0, 0, 0}, bT[3] = {0, 0, 0};
-  if (has_bond && interaction) bond_pair_sum<ND, PREC>(d, b, bF, bT);
+  if (has_bond && interaction) {
+    // (The fused evaluation follows the pair list only when the rebuild of
+    // this step completed it.)
+    if (FUSE) {
+      if (!overflowed) bond_pair_eval_sum<ND>(k, d, d.rep[fc.rep].hf, rbuf, b, bF, bT);
+    } else {
+      bond_pair_sum<ND, PREC>(d, b, bF, bT);
+    }
+  }
   if (!has_bond) u[0] = u[1] = u[2] = 0.0;
   double xi[3] = {0, 0, 0};
   if (midstep && k.stoch) {  // uniforms of ConstructUnprojectedRandomForces
