@@ -566,7 +566,7 @@ def test_reference_format_output(tmp_path):
     from ref_formats import read_posit, read_spec
     system, fils, sites = _workload("B", 0.01, seed=15)
     ctx = _ctx(system, fils, sites)
-    run = str(tmp_path / "gpurun")
+    run = str(tmp_path / "specrun")
     ctx.output_open(run, n_steps=60, n_posit=10, n_spec=20)
     expect_sites, expect_u = [], []
     for i in range(61):
