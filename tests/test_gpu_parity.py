@@ -537,6 +537,32 @@ def test_non_finite_positions_are_reported():
     assert e.value.code == 3
 
 
+def test_invalid_inputs_are_rejected():
+    """Inputs the library cannot take fail with an error status and a
+    message, before any device work: no filaments, inconsistent site counts,
+    bad parameters, filaments past the 255-bond limit, negative step
+    counts."""
+    import simcore_b200 as sc
+    system, fils, sites = _workload("A", 0.05, seed=1)
+    with pytest.raises(sc.ScError):
+        _ctx(system, [], np.zeros((0, 3)))
+    with pytest.raises(sc.ScError, match="n_sites_total"):
+        _ctx(system, fils, sites[:-1])
+    bad = [dict(f) for f in fils]
+    bad[0]["length"] = 0.0
+    with pytest.raises(sc.ScError, match="bad parameters"):
+        _ctx(system, bad, sites)
+    long_fil = dict(fils[0], length=300.0)
+    n = sc.filament_n_bonds(long_fil) + 1
+    assert n > 256
+    with pytest.raises(sc.ScError, match="255 bonds"):
+        _ctx(system, [long_fil], np.zeros((n, 3)))
+    ctx = _ctx(system, fils, sites)
+    with pytest.raises(sc.ScError):
+        ctx.step(-1)
+    ctx.step(2)  # the context is still usable
+
+
 def test_getters_leave_the_trajectory_alone():
     """Reading state (geometry, forces, pairs, cells, checkpoint) between
     steps changes nothing in the mixed path, whose bond orientations come
