@@ -197,8 +197,9 @@ def fused_bytes(n_sites, n_bonds, n_pairs):
 
 def step_kernel_time(ctx, n):
     """Average CUDA-event duration (ms) of the kernels sc_step launches for a
-    reference step, over n host-driven steps (L2 warm): for the fast mixed
-    step that is the integrator with the pairs fused in, alone."""
+    reference step, over n host-driven steps (L2 warm): with
+    sc_set_fused_pairs on (fast mixed step), the integrator with the pairs
+    fused in, alone."""
     t = 0.0
     for _ in range(n):
         ctx.set_kernel_timing(True)
