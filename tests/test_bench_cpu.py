@@ -1,0 +1,46 @@
+"""The benchmark's CPU-side contract: the reference arm (the reference's own
+CPU code on the host cores) prints one JSON line in the shape the GPU arm
+prints, and the roofline byte counts follow their stated formulas."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from checkers import Reference
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build not present")
+def test_reference_arm_prints_one_contract_line():
+    out = subprocess.run(
+        [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+         "--workload", "A", "--steps", "1", "--warmup", "3"],
+        cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["unit"] == "segment-steps/s" and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1
+    assert d["config"]["workload"].startswith("A:")
+    cb = d["cpu_baseline"]
+    assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["sample"]
+    assert cb["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}
+
+
+def test_algorithmic_bytes():
+    sys.path.insert(0, ROOT)
+    import bench
+    ns, nb, npairs = 220000, 200000, 124288
+    b_int, b_pair = bench.algorithmic_bytes(ns, nb, npairs, "mixed")
+    assert b_int == 96 * ns + 56 * nb
+    assert b_pair == 56 * nb + 8 * npairs
+    b_int, b_pair = bench.algorithmic_bytes(ns, nb, npairs, "fp64")
+    assert b_int == 96 * ns + 104 * nb
+    assert bench.fused_bytes(ns, nb, npairs) == 96 * ns + 64 * nb + 8 * npairs
