@@ -60,7 +60,9 @@ WORKLOAD_DESC = WORKLOAD_DESCS["B"]
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    # 200 launches of 20 reference steps: about 0.3 s per precision on B,
+    # long enough for a few dozen clock samples of the timed region.
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="B", choices=sorted(WORKLOAD_DESCS))
