@@ -1528,7 +1528,7 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
       cand.push_back({w, 0});
       continue;
     }
-    for (int bsz : {64, 96, 128, 192, 256})
+    for (int bsz : {64, 96, 128, 160, 192, 256})
       if (bsz >= longest) cand.push_back({w, bsz});
   }
   // Save what the integrator writes.

@@ -1397,6 +1397,11 @@ void prepare_integrate(int C) {
     set_attr<3, 1, 128>(smem);
     set_attr<2, 0, 128>(smem);
     set_attr<2, 1, 128>(smem);
+  } else if (C <= 192) {
+    set_attr<3, 0, 192>(smem);
+    set_attr<3, 1, 192>(smem);
+    set_attr<2, 0, 192>(smem);
+    set_attr<2, 1, 192>(smem);
   } else {
     set_attr<3, 0, 256>(smem);
     set_attr<3, 1, 256>(smem);
@@ -1436,6 +1441,12 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
       if (prec == 0) SC_INTEGRATE(3, 0, 128); else SC_INTEGRATE(3, 1, 128);
     } else {
       if (prec == 0) SC_INTEGRATE(2, 0, 128); else SC_INTEGRATE(2, 1, 128);
+    }
+  } else if (C <= 192) {
+    if (k.n_dim == 3) {
+      if (prec == 0) SC_INTEGRATE(3, 0, 192); else SC_INTEGRATE(3, 1, 192);
+    } else {
+      if (prec == 0) SC_INTEGRATE(2, 0, 192); else SC_INTEGRATE(2, 1, 192);
     }
   } else {
     if (k.n_dim == 3) {

@@ -26,6 +26,9 @@ void prepare_integrate_fast(int C) {
   if (C <= 128) {
     set_attr_fast<3, 128>(smem);
     set_attr_fast<2, 128>(smem);
+  } else if (C <= 192) {
+    set_attr_fast<3, 192>(smem);
+    set_attr_fast<2, 192>(smem);
   } else {
     set_attr_fast<3, 256>(smem);
     set_attr_fast<2, 256>(smem);
@@ -46,6 +49,9 @@ static int launch_fast(const SysConst &k, const DevState &d, int nblocks, int C,
   const size_t smem = integrate_smem_bytes(C);
   if (C <= 128)
     k_integrate<ND, 1, true, 128, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
+                                                                  interaction, capture);
+  else if (C <= 192)
+    k_integrate<ND, 1, true, 192, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
                                                                   interaction, capture);
   else
     k_integrate<ND, 1, true, 256, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,

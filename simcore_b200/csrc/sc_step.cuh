@@ -407,8 +407,11 @@ constexpr int kPcrMinRows = 32;
 
 template <int MAXC, bool FAST>
 struct IntegrateBounds {
-  // The exact variant spills below 96 registers; the fast one fits 80.
-  static constexpr int min_blocks = MAXC <= 128 ? (FAST ? 6 : 5) : 2;
+  // The exact variant spills below 96 registers; the fast one fits 80, which
+  // also holds 4 blocks of 192 sites per SM (2 waves of 17-filament blocks
+  // for 20,000 11-site filaments on 148 SMs).
+  static constexpr int min_blocks =
+      MAXC <= 128 ? (FAST ? 6 : 5) : MAXC <= 192 ? (FAST ? 4 : 3) : 2;
 };
 
 // FUSE (fast mixed step only): each bond evaluates its own pairs
