@@ -71,6 +71,9 @@ def parse_args():
                     help="run this many host-driven steps and exit (for ncu)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="precision of --profile-steps")
+    ap.add_argument("--layout-sweep", action="store_true",
+                    help="time every integrator layout of the workload (one JSON line each) "
+                         "and exit")
     ap.add_argument("--profile-fused", action="store_true",
                     help="--profile-steps with the pair evaluation fused into the integrator")
     ap.add_argument("--profile-layout", default=None,
@@ -596,10 +599,50 @@ def run_reference(args, rank, world):
     }
 
 
+def layout_sweep(args):
+    """--layout-sweep: for both precisions and every integrator layout that
+    holds the workload (warp kernel on or off, blocks of 64-256 sites), the
+    CUDA-event time of the pair and integrator kernels of a host-driven
+    reference step (L2 warm) and of a captured 20-step launch (L2 flushed
+    first); one JSON line per layout.  Layouts are what sc_autotune chooses
+    among; this prints all of their times."""
+    import torch
+    import simcore_b200 as sc
+    wl = load_workload(args.workload, 0)
+    n_sites = [sc.filament_n_bonds(f) + 1 for f in wl[1]]
+    longest, shortest = max(n_sites), min(n_sites)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for prec in ("mixed", "fp64"):
+        ctx = new_context(sc, wl, prec, 0)
+        for w in (32, 0):
+            if w == 32 and shortest > 32:
+                continue
+            rest = longest if (w == 0 or longest > 32) else 0
+            for bsz in ((0,) if rest == 0 else (64, 96, 128, 160, 192, 256)):
+                if rest and bsz < rest:
+                    continue
+                ctx.set_integrator_layout(w, bsz)
+                t_pair, t_int = kernel_times(ctx, 2 * I_STEPS_PER_STEP)
+                ms = []
+                for i in range(3 + args.steps):
+                    flush.zero_()
+                    torch.cuda.synchronize()
+                    ctx.step_graph(I_STEPS_PER_STEP)
+                    if i >= 3:
+                        ms.append(ctx.graph_time_ms())
+                print(json.dumps({"precision": prec, "warp_max_sites": w, "block_sites": bsz,
+                                  "pair_ms": t_pair, "integrate_ms": t_int,
+                                  "graph_ms_per_20_steps": statistics.mean(ms)}), flush=True)
+        ctx.close()
+
+
 def main():
     args = parse_args()
     if args.profile_steps:
         profile_only(args)
+        return
+    if args.layout_sweep:
+        layout_sweep(args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
