@@ -5,7 +5,8 @@ oracle/ref/Makefile).  Run where the reference tree is present:
     python tests/golden/make_golden.py
 
 Each fixture holds a seeded initial configuration (random insertion with
-overlap rejection) and the reference's state after a fixed number of steps.
+overlap rejection) and the reference's state after a fixed number of steps;
+the thermo_* fixtures hold its pressure records and potential energies.
 tests/test_oracle.py requires the C oracle to reproduce every array bit for
 bit; the GPU tests require the CUDA path to match the oracle the same way.
 """
@@ -61,10 +62,52 @@ def make_case(name, c):
     return out
 
 
+# Pressure records (InteractionManager::CalculatePressure every n_thermo
+# steps) and per-filament potential energies, from runs with rebuilds.
+THERMO_CASES = {
+    "thermo_3d": dict(n_dim=3, R=14.0, n_fil=25, n_seg=12, lp=50.0, delta=2e-4, seed=7,
+                      insert_seed=102, steps=90, n_thermo=6),
+    "thermo_2d": dict(n_dim=2, R=22.0, n_fil=30, n_seg=14, lp=50.0, delta=2e-4, seed=7,
+                      insert_seed=101, steps=90, n_thermo=6),
+}
+
+
+def make_thermo_case(name, c):
+    nb = np.full(c["n_fil"], c["n_seg"], dtype=np.int32)
+    sites = sc.insert_filaments(c["n_dim"], c["R"], c["insert_seed"], nb, nb.astype(float),
+                                np.full(c["n_fil"], c["lp"]))
+    system = dict(n_dim=c["n_dim"], system_radius=c["R"], delta=c["delta"], seed=c["seed"])
+    fils = [dict(length=float(c["n_seg"]), persistence_length=c["lp"], diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * c["n_fil"]
+    ref = Reference(system, fils, sites, n_threads=2)
+    ref.set_thermo(c["n_thermo"])
+    ref.step(c["steps"])
+    st, P, p, V = ref.thermo_records()
+    out = dict(
+        system=np.array([c["n_dim"], c["R"], c["delta"], c["seed"], c["lp"], c["n_seg"],
+                         c["n_fil"], c["steps"]], dtype=np.float64),
+        n_thermo=np.array([c["n_thermo"]]), sites0=sites, sites=ref.sites(),
+        thermo_step=st, thermo_tensor=P, thermo_pressure=p, thermo_volume=V,
+        stress=ref.stress(), potential_energy=ref.potential_energy(),
+        n_rebuilds=np.array([ref.n_rebuilds]))
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return out
+
+
 if __name__ == "__main__":
+    # Arguments: the names of the cases to (re)generate; none = all.
     if not Reference.available():
         sys.exit("oracle/_ref/libscref.so is not built (python oracle/build.py)")
+    want = set(sys.argv[1:])
     for name, c in CASES.items():
+        if want and name not in want:
+            continue
         o = make_case(name, c)
         print(name, "rebuilds", int(o["n_rebuilds"][0]), "renormalised filaments",
               int((o["n_normalize"] < c["steps"]).sum()), "pairs", len(o["pairs"]))
+    for name, c in THERMO_CASES.items():
+        if want and name not in want:
+            continue
+        o = make_thermo_case(name, c)
+        print(name, "rebuilds", int(o["n_rebuilds"][0]), "records", len(o["thermo_step"]))

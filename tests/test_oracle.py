@@ -3,7 +3,8 @@
 * Philox4x32-10 against the published known-answer vectors (Salmon et al.).
 * The oracle replays the golden fixtures of tests/golden/ -- generated by
   tests/golden/make_golden.py from the reference's own sources
-  (oracle/_ref) -- bit for bit, including rebuilds and renormalisations.
+  (oracle/_ref) -- bit for bit, including rebuilds and renormalisations,
+  and the pressure records and potential energies of the thermo_* ones.
 * Where the reference build is present, both run side by side on a fresh
   configuration and must agree bit for bit every step.
 * Analytic known answers: WCA force of two segments at a known distance and
@@ -18,7 +19,9 @@ import pytest
 
 from checkers import Oracle, Reference, ORACLE_SO, SystemDesc
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+_ALL_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = [p for p in _ALL_GOLDEN if not os.path.basename(p).startswith("thermo_")]
+THERMO_GOLDEN = [p for p in _ALL_GOLDEN if os.path.basename(p).startswith("thermo_")]
 
 
 def _oracle_lib():
@@ -77,6 +80,29 @@ def test_oracle_reproduces_reference_fixture(path):
         assert np.array_equal(a, b), name
     assert o.n_rebuilds == int(z["n_rebuilds"][0])
     assert o.n_rebuilds > 0
+
+
+@pytest.mark.parametrize("path", THERMO_GOLDEN, ids=[os.path.basename(p) for p in THERMO_GOLDEN])
+def test_oracle_reproduces_reference_thermo_fixture(path):
+    """Pressure records every n_thermo steps, the running virial sum and every
+    filament's potential energy, from the reference's own code over a run
+    with rebuilds: the oracle gives the same bits."""
+    z, system, fils, steps = _case(path)
+    o = Oracle(system, fils, z["sites0"])
+    o.set_thermo(int(z["n_thermo"][0]))
+    o.step(steps)
+    st, P, p, V = o.thermo_records()
+    assert len(st) == steps // int(z["n_thermo"][0]) == len(z["thermo_step"])
+    assert np.array_equal(st, z["thermo_step"])
+    assert np.array_equal(P, z["thermo_tensor"])
+    assert np.array_equal(p, z["thermo_pressure"])
+    assert np.array_equal(V, z["thermo_volume"])
+    assert np.array_equal(o.stress(), z["stress"])
+    assert np.array_equal(o.potential_energy(), z["potential_energy"])
+    assert np.array_equal(o.sites(), z["sites"])
+    assert o.n_rebuilds == int(z["n_rebuilds"][0]) > 1
+    assert (z["potential_energy"] > 0).any()
+    o.close()
 
 
 def test_fixtures_exercise_rebuilds_and_renormalisation():
