@@ -662,6 +662,33 @@ void scref_get_potential_energy(void *h, double *pote) {
   for (auto &f : s->members) pote[c++] = f.GetPotentialEnergy();
 }
 
+// One spec frame of the filament species appended to the file at path: the
+// member count, then each filament's own Filament::WriteSpec
+// (Species::WriteSpecs, include/simcore/species.hpp:229-235, restated;
+// src/filament.cpp:1314-1319, src/mesh.cpp:482-492).  Returns 0 on success.
+int scref_write_spec_frame(void *h, const char *path) {
+  RefSim *s = (RefSim *)h;
+  std::fstream out(path, std::ios::out | std::ios::binary | std::ios::app);
+  if (!out.is_open()) return -1;
+  int size = (int)s->members.size();
+  out.write(reinterpret_cast<char *>(&size), sizeof(int));
+  for (auto &m : s->members) m.WriteSpec(out);
+  return out.good() ? 0 : -1;
+}
+
+// One posit frame likewise: the member count and each filament's own
+// Filament::WritePosit (Species::WritePosits, include/simcore/species.hpp:
+// 221-227, restated; src/filament.cpp:1347-1361).
+int scref_write_posit_frame(void *h, const char *path) {
+  RefSim *s = (RefSim *)h;
+  std::fstream out(path, std::ios::out | std::ios::binary | std::ios::app);
+  if (!out.is_open()) return -1;
+  int size = (int)s->members.size();
+  out.write(reinterpret_cast<char *>(&size), sizeof(int));
+  for (auto &m : s->members) m.WritePosit(out);
+  return out.good() ? 0 : -1;
+}
+
 // Per-site accumulated squared displacement since the last rebuild.
 void scref_get_dr_tot(void *h, double *dr) {
   RefSim *s = (RefSim *)h;

@@ -253,3 +253,13 @@ class Reference(_Checker):
         out = [np.zeros(self.n_fil) for _ in range(4)]
         self._call("get_frictions", *[_ptr(a) for a in out])
         return out
+
+    def write_spec_frame(self, path):
+        """Appends one spec frame, written by the reference's own writers."""
+        if self._call("write_spec_frame", ctypes.c_char_p(path.encode())) != 0:
+            raise RuntimeError("spec frame not written")
+
+    def write_posit_frame(self, path):
+        """Appends one posit frame, written by the reference's own writers."""
+        if self._call("write_posit_frame", ctypes.c_char_p(path.encode())) != 0:
+            raise RuntimeError("posit frame not written")

@@ -6,7 +6,8 @@ oracle/ref/Makefile).  Run where the reference tree is present:
 
 Each fixture holds a seeded initial configuration (random insertion with
 overlap rejection) and the reference's state after a fixed number of steps;
-the thermo_* fixtures hold its pressure records and potential energies.
+the thermo_* fixtures hold its pressure records and potential energies, the
+format_* ones a spec and a posit frame as its own writers write them.
 tests/test_oracle.py requires the C oracle to reproduce every array bit for
 bit; the GPU tests require the CUDA path to match the oracle the same way.
 """
@@ -95,6 +96,39 @@ def make_thermo_case(name, c):
     return out
 
 
+# One spec frame and one posit frame written by the reference's own
+# Filament::WriteSpec / WritePosit after a run (the bytes as written).
+FORMAT_CASES = {
+    "format_3d": dict(n_dim=3, R=15.0, n_fil=12, n_seg=20, lp=500.0, delta=1e-4, seed=31,
+                      steps=21),
+}
+
+
+def make_format_case(name, c):
+    import tempfile
+    nb = np.full(c["n_fil"], c["n_seg"], dtype=np.int32)
+    sites = sc.insert_filaments(c["n_dim"], c["R"], c["seed"], nb, nb.astype(float),
+                                np.full(c["n_fil"], c["lp"]))
+    system = dict(n_dim=c["n_dim"], system_radius=c["R"], delta=c["delta"], seed=c["seed"])
+    fils = [dict(length=float(c["n_seg"]), persistence_length=c["lp"], diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * c["n_fil"]
+    ref = Reference(system, fils, sites, n_threads=2)
+    ref.step(c["steps"])
+    with tempfile.TemporaryDirectory() as tmp:
+        spec, posit = os.path.join(tmp, "f.spec"), os.path.join(tmp, "f.posit")
+        ref.write_spec_frame(spec)
+        ref.write_posit_frame(posit)
+        spec_b = np.frombuffer(open(spec, "rb").read(), dtype=np.uint8)
+        posit_b = np.frombuffer(open(posit, "rb").read(), dtype=np.uint8)
+    out = dict(
+        system=np.array([c["n_dim"], c["R"], c["delta"], c["seed"], c["lp"], c["n_seg"],
+                         c["n_fil"], c["steps"]], dtype=np.float64),
+        sites0=sites, sites=ref.sites(), spec_frame=spec_b, posit_frame=posit_b)
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return out
+
+
 if __name__ == "__main__":
     # Arguments: the names of the cases to (re)generate; none = all.
     if not Reference.available():
@@ -111,3 +145,8 @@ if __name__ == "__main__":
             continue
         o = make_thermo_case(name, c)
         print(name, "rebuilds", int(o["n_rebuilds"][0]), "records", len(o["thermo_step"]))
+    for name, c in FORMAT_CASES.items():
+        if want and name not in want:
+            continue
+        o = make_format_case(name, c)
+        print(name, "spec bytes", len(o["spec_frame"]), "posit bytes", len(o["posit_frame"]))

@@ -20,7 +20,7 @@ import pytest
 from checkers import Oracle, Reference, ORACLE_SO, SystemDesc
 
 _ALL_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
-GOLDEN = [p for p in _ALL_GOLDEN if not os.path.basename(p).startswith("thermo_")]
+GOLDEN = [p for p in _ALL_GOLDEN if os.path.basename(p).startswith("ref")]
 THERMO_GOLDEN = [p for p in _ALL_GOLDEN if os.path.basename(p).startswith("thermo_")]
 
 
