@@ -689,6 +689,24 @@ int scref_write_posit_frame(void *h, const char *path) {
   return out.good() ? 0 : -1;
 }
 
+// The global order of FilamentSpecies::RunGlobalOrderAnalysis
+// (src/filament_species.cpp:487-517, restated) on freshly zeroed
+// accumulators, as its first sample: every filament's own
+// Filament::GetPolarOrder / GetNematicOrder (src/filament.cpp:488-516) added,
+// then both divided by the member count.
+void scref_global_order(void *h, double *polar, double *nematic) {
+  RefSim *s = (RefSim *)h;
+  std::fill(polar, polar + 3, 0.0);
+  std::fill(nematic, nematic + 9, 0.0);
+  for (auto &m : s->members) {
+    m.GetPolarOrder(polar);
+    m.GetNematicOrder(nematic);
+  }
+  const int n_members = (int)s->members.size();
+  for (int i = 0; i < 3; ++i) polar[i] /= n_members;
+  for (int i = 0; i < 9; ++i) nematic[i] /= n_members;
+}
+
 // Per-site accumulated squared displacement since the last rebuild.
 void scref_get_dr_tot(void *h, double *dr) {
   RefSim *s = (RefSim *)h;

@@ -263,3 +263,10 @@ class Reference(_Checker):
         """Appends one posit frame, written by the reference's own writers."""
         if self._call("write_posit_frame", ctypes.c_char_p(path.encode())) != 0:
             raise RuntimeError("posit frame not written")
+
+    def global_order(self):
+        """Polar order vector (3) and nematic tensor (3 x 3) of the current
+        state, as the reference's first global-order sample."""
+        polar, nem = np.zeros(3), np.zeros(9)
+        self._call("global_order", _ptr(polar), _ptr(nem))
+        return polar, nem.reshape(3, 3)

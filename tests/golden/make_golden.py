@@ -97,10 +97,13 @@ def make_thermo_case(name, c):
 
 
 # One spec frame and one posit frame written by the reference's own
-# Filament::WriteSpec / WritePosit after a run (the bytes as written).
+# Filament::WriteSpec / WritePosit after a run (the bytes as written), and
+# the global order of that state (Filament::GetPolarOrder / GetNematicOrder).
 FORMAT_CASES = {
     "format_3d": dict(n_dim=3, R=15.0, n_fil=12, n_seg=20, lp=500.0, delta=1e-4, seed=31,
                       steps=21),
+    "format_2d": dict(n_dim=2, R=20.0, n_fil=16, n_seg=16, lp=20.0, delta=1e-4, seed=32,
+                      steps=41),
 }
 
 
@@ -120,10 +123,12 @@ def make_format_case(name, c):
         ref.write_posit_frame(posit)
         spec_b = np.frombuffer(open(spec, "rb").read(), dtype=np.uint8)
         posit_b = np.frombuffer(open(posit, "rb").read(), dtype=np.uint8)
+    polar, nematic = ref.global_order()
     out = dict(
         system=np.array([c["n_dim"], c["R"], c["delta"], c["seed"], c["lp"], c["n_seg"],
                          c["n_fil"], c["steps"]], dtype=np.float64),
-        sites0=sites, sites=ref.sites(), spec_frame=spec_b, posit_frame=posit_b)
+        sites0=sites, sites=ref.sites(), spec_frame=spec_b, posit_frame=posit_b,
+        polar_order=polar, nematic_order=nematic)
     ref.close()
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     return out

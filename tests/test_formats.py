@@ -3,7 +3,9 @@ library's spec and posit files) against frames written by the reference's
 own Filament::WriteSpec and Filament::WritePosit (tests/golden/format_*.npz,
 made by tests/golden/make_golden.py): they decode to the oracle's state after
 the same steps, so a file the library writes that decodes to its state holds
-the reference's bytes."""
+the reference's bytes.  Likewise the host formula of the global order that
+the GPU analysis test checks the device against, against the reference's own
+Filament::GetPolarOrder / GetNematicOrder on that state."""
 import glob
 import os
 import struct
@@ -69,3 +71,29 @@ def test_reference_written_frames_read_back(path, tmp_path):
         s_img -= np.where(s_img < 0, np.ceil(s_img - 0.5), np.floor(s_img + 0.5))
         assert np.abs(rec[3:6] - s_img).max() < 1e-14
         assert rec[9] == fils[k]["diameter"] and rec[10] == fils[k]["length"]
+
+
+@pytest.mark.parametrize("path", FORMAT_GOLDEN, ids=[os.path.basename(p) for p in FORMAT_GOLDEN])
+def test_global_order_formula_matches_reference(path):
+    """The mean over filaments of the mean bond orientation and of the bond
+    tensor (2 u u^T - I), n_dim x n_dim in a 3 x 3 array, from the bond
+    orientations of the final sites: the reference's values to 1e-12."""
+    import simcore_b200 as sc
+    z, system, fils, steps = _case(path)
+    nd = system["n_dim"]
+    xyz = z["sites"]
+    nb = np.array([sc.filament_n_bonds(f) for f in fils])
+    off = np.concatenate([[0], np.cumsum(nb + 1)])
+    pv = np.zeros(3)
+    q = np.zeros((3, 3))
+    for k in range(len(fils)):
+        s = xyz[off[k]:off[k + 1], :nd]
+        d = s[1:] - s[:-1]
+        u = d / np.sqrt((d * d).sum(axis=1))[:, None]
+        pv[:nd] += u.mean(0)
+        q[:nd, :nd] += (2 * np.einsum("bi,bj->ij", u, u) - len(u) * np.eye(nd)) / len(u)
+    pv /= len(fils)
+    q /= len(fils)
+    assert np.abs(pv - z["polar_order"]).max() < 1e-12
+    assert np.abs(q - z["nematic_order"]).max() < 1e-12
+    assert np.abs(z["nematic_order"]).max() > 0.05  # not a trivial state
