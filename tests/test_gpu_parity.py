@@ -345,15 +345,18 @@ def test_fp64_uneven_lengths_bitwise():
     assert o.n_rebuilds > 0
 
 
+@pytest.mark.parametrize("block", [64, 160, 192])
 @pytest.mark.parametrize("precision,fast", [("fp64", False), ("mixed", False), ("mixed", True)])
-def test_warp_and_block_integrators_agree(precision, fast):
+def test_warp_and_block_integrators_agree(precision, fast, block):
     """The warp-synchronous integrator (filaments of at most 32 sites) and the
     block integrator give the same bits where both are exact, and agree to
-    1e-12 in the fast mixed variant (contraction choices differ)."""
+    1e-12 in the fast mixed variant (contraction choices differ); blocks of
+    64 sites run the kernel compiled for up to 128, blocks of 160 and 192 the
+    one compiled for up to 192."""
     system, fils, sites = _workload("B", 0.05, seed=9)
     a = _ctx(system, fils, sites, precision)
     b = _ctx(system, fils, sites, precision)
-    b.set_integrator_layout(0, 64)
+    b.set_integrator_layout(0, block)
     for c in (a, b):
         c.set_fast_integrator(fast)
         c.set_capture(True)
