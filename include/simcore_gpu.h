@@ -331,7 +331,9 @@ sc_status sc_get_graph_time(sc_ctx *ctx, double *ms);
  * Limits: at most SC_NOALLOC_MAX_BONDS bonds and filaments, a cell grid of
  * at most SC_NOALLOC_MAX_CELLS cells, at most SC_NOALLOC_MAX_PAIRS
  * candidate pairs; larger inputs return SC_ERR_INVALID_ARG (sizes, cells)
- * or SC_ERR_LIST_OVERFLOW (pairs).  The call synchronises the stream.  The
+ * or SC_ERR_LIST_OVERFLOW (pairs).  Site offsets that do not rise from 0 by
+ * at least 2 sites a filament return SC_ERR_INVALID_ARG (checked on the
+ * device, where they are; nothing is written outside the scratch).  The call synchronises the stream.  The
  * first call on a device looks up the scratch address with
  * cudaGetSymbolAddress; make that first call before any stream capture.
  * All calls on a device share the scratch and leave their data in it; calls

@@ -28,7 +28,8 @@ enum : unsigned {
   ST_NAN = 1u,            // non-finite position or force
   ST_LIST_OVERFLOW = 2u,  // pair list did not fit
   ST_UNPHYSICAL = 4u,     // accumulated displacement above 10000
-  ST_BAD_CELL = 8u        // cell index out of range (non-finite position)
+  ST_BAD_CELL = 8u,       // cell index out of range (non-finite position)
+  ST_BAD_INPUT = 16u      // caller's device data out of range (site offsets)
 };
 
 // Bond geometry for the FP64 pair stage: the reference's Bond state after

@@ -138,6 +138,10 @@ void inv3(const double *a, double *b) {
 }
 
 // AoS caller positions -> SoA scratch; bond -> filament map from offsets.
+// The offsets must rise from 0 by at least 2 sites a filament (the last one,
+// ns, is checked on the host); then filament i's bonds s0 - i .. s1 - i - 2
+// lie in [0, nb).  Offsets that break this set ST_BAD_INPUT, and every write
+// stays inside the bond range whatever they hold.
 __global__ void k_noalloc_unpack(int nf, int ns, const int32_t *site_off,
                                  const double *xyz, int n_dim, DevState d, int *bond_fil) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -145,8 +149,10 @@ __global__ void k_noalloc_unpack(int nf, int ns, const int32_t *site_off,
     for (int c = 0; c < 3; ++c) d.r[c][i] = c < n_dim ? xyz[3 * (size_t)i + c] : 0.0;
   }
   if (i < nf) {
-    int s0 = site_off[i], s1 = site_off[i + 1];
-    for (int b = s0 - i; b < s1 - i - 1; ++b) bond_fil[b] = i;
+    const int s0 = site_off[i], s1 = site_off[i + 1];
+    if ((i == 0 && s0 != 0) || s0 < 0 || s1 > ns || s1 - s0 < 2) atomicOr(d.status, sc::ST_BAD_INPUT);
+    const int b0 = max(s0 - i, 0), b1 = min(s1 - i - 1, d.nb);
+    for (int b = b0; b < b1; ++b) bond_fil[b] = i;
   }
 }
 
@@ -320,6 +326,7 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   unsigned status = 0;
   NA_CK(cudaMemcpyAsync(&status, d.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   NA_CK(cudaStreamSynchronize(st));
+  if (status & sc::ST_BAD_INPUT) return SC_ERR_INVALID_ARG;
   if (status & sc::ST_LIST_OVERFLOW) return SC_ERR_LIST_OVERFLOW;
   if (status) return SC_ERR_NAN;
   return SC_OK;
