@@ -513,6 +513,60 @@ def test_checkpoint_of_replicas_and_shape_check():
         wrong.restore(blob)
 
 
+def _payload_hash(b):
+    """The checkpoint's payload hash: 64-bit FNV-1a over 8-byte words, then
+    the tail bytes."""
+    import numpy as np
+    h = 1469598103934665603
+    n8 = len(b) // 8 * 8
+    for w in np.frombuffer(b[:n8], dtype="<u8"):
+        h = ((h ^ int(w)) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    for x in b[n8:]:
+        h = ((h ^ x) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def test_restore_rejects_corrupted_checkpoints():
+    """A restore checks the blob before it changes the context: a changed
+    byte fails the payload hash, and a blob whose hash matches but whose pair
+    count exceeds its segment fails the index checks.  The context keeps its
+    state through both and continues as before."""
+    import struct
+    import simcore_b200 as sc
+    system, fils, sites = _workload("A", 0.1, seed=21)
+    a = _ctx(system, fils, sites)
+    a.step(5)
+    blob = bytearray(a.checkpoint())
+    hdr = 96
+    assert struct.unpack_from("<q", blob, 80)[0] == len(blob) - hdr  # payload bytes
+    assert struct.unpack_from("<Q", blob, 88)[0] == _payload_hash(bytes(blob[hdr:]))
+    bad = bytearray(blob)
+    bad[len(bad) // 2] ^= 0x40
+    with pytest.raises(sc.ScError, match="hash"):
+        a.restore(bytes(bad))
+    # One system: the pair count follows the capacity (int32), 13 site arrays
+    # of doubles, two filament int arrays and the displacement maxima.
+    ns, nf = a.n_sites, a.n_fil
+    cap = struct.unpack_from("<i", blob, hdr)[0]
+    off_np = hdr + 4 + 13 * 8 * ns + 8 * nf + 8
+    assert 0 < struct.unpack_from("<i", blob, off_np)[0] <= cap
+    bad = bytearray(blob)
+    struct.pack_into("<i", bad, off_np, cap + 1)
+    struct.pack_into("<Q", bad, 88, _payload_hash(bytes(bad[hdr:])))
+    with pytest.raises(sc.ScError, match="pairs"):
+        a.restore(bytes(bad))
+    b = _ctx(system, fils, sites)
+    b.step(5)
+    a.step(7)
+    b.step(7)
+    assert_same(a.sites(), b.sites(), "sites after the refused restores")
+    a.restore(bytes(blob))
+    a.step(7)
+    b2 = _ctx(system, fils, sites)
+    b2.step(12)
+    assert_same(a.sites(), b2.sites(), "sites after a good restore")
+
+
 def test_noise_key():
     """sc_set_noise_key before the first step gives the stream of a context
     created with that seed."""
