@@ -30,13 +30,23 @@ def _reference_forces(system, fils, sites):
     return f, t
 
 
-def _call_noalloc(system, fils, sites):
-    import torch
-
+def _site_offsets(fils):
     import simcore_b200 as sc
     n_bonds = [sc.filament_n_bonds(f) for f in fils]
     offsets = np.zeros(len(fils) + 1, dtype=np.int32)
     offsets[1:] = np.cumsum(np.asarray(n_bonds) + 1)
+    return offsets
+
+
+def _call_noalloc(system, fils, sites, offsets=None, expect=0):
+    """Calls the entry point on test-owned device buffers; returns the bond
+    forces and torques when it is expected to succeed (expect = 0)."""
+    import torch
+
+    import simcore_b200 as sc
+    n_bonds = [sc.filament_n_bonds(f) for f in fils]
+    if offsets is None:
+        offsets = _site_offsets(fils)
     nb = int(sum(n_bonds))
     d_off = torch.from_numpy(offsets).cuda()
     d_xyz = torch.from_numpy(np.ascontiguousarray(sites, dtype=np.float64)).cuda()
@@ -53,7 +63,7 @@ def _call_noalloc(system, fils, sites):
         ctypes.c_void_p(d_off.data_ptr()), ctypes.c_void_p(d_xyz.data_ptr()),
         ctypes.c_void_p(d_f.data_ptr()), ctypes.c_void_p(d_t.data_ptr()),
         ctypes.c_void_p(stream))
-    assert rc == sc.SC_OK, sc.STATUS_NAMES.get(rc, rc)
+    assert rc == expect, sc.STATUS_NAMES.get(rc, rc)
     return d_f.cpu().numpy(), d_t.cpu().numpy()
 
 
@@ -86,3 +96,24 @@ def test_noalloc_rejects_sizes_beyond_the_limit():
         ctypes.c_void_p(o.data_ptr()), ctypes.c_void_p(d.data_ptr()),
         ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(0))
     assert rc == 1  # SC_ERR_INVALID_ARG
+
+
+def test_noalloc_rejects_bad_site_offsets():
+    """The site offsets are device data that the host does not read: the
+    unpack kernel checks them (rising from 0 by at least 2 sites a filament)
+    and the call returns SC_ERR_INVALID_ARG, writing nothing outside its
+    scratch.  A correct call afterwards gives the regular forces."""
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("A", 0.1, seed=13)
+    good = _site_offsets(fils)
+    swapped = good.copy()
+    swapped[1], swapped[2] = good[2], good[1]  # filament 1 runs backwards
+    short = good.copy()
+    short[1] = 1                                # a filament of one site
+    for bad in (swapped, short):
+        assert bad[0] == 0 and bad[-1] == good[-1]  # only the device check can see it
+        _call_noalloc(system, fils, sites, offsets=bad, expect=1)  # SC_ERR_INVALID_ARG
+    f_ref, t_ref = _reference_forces(system, fils, sites)
+    f, t = _call_noalloc(system, fils, sites)
+    assert np.array_equal(f, f_ref)
+    assert np.array_equal(t, t_ref)
