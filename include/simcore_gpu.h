@@ -312,8 +312,10 @@ sc_status sc_get_graph_time(sc_ctx *ctx, double *ms);
 /* Pair forces for callers that cannot allocate device memory.
  *
  * No counterpart in the reference.  Some callers cannot call cudaMalloc:
- * an application recording its own CUDA graph (allocation is illegal during
- * stream capture), or one whose device memory belongs to its own pool.  This
+ * an application whose device memory belongs to its own pool or caching
+ * allocator, which must not be grown or fragmented behind its back, or one
+ * that runs under a fixed device-memory budget reserved at start-up (a
+ * solver embedded in a larger code, a real-time controller).  This
  * entry point computes, for a configuration in the caller's device buffers,
  * the bond forces and torques that the first Interact after a pair-list
  * rebuild produces (fresh pairs, FP64, bit-identical to sc_interact on a
@@ -329,15 +331,19 @@ sc_status sc_get_graph_time(sc_ctx *ctx, double *ms);
  *   stream          cudaStream_t the work is issued on (0: legacy stream)
  *
  * Limits: at most SC_NOALLOC_MAX_BONDS bonds and filaments, a cell grid of
- * at most SC_NOALLOC_MAX_CELLS cells, at most SC_NOALLOC_MAX_PAIRS
- * candidate pairs; larger inputs return SC_ERR_INVALID_ARG (sizes, cells)
- * or SC_ERR_LIST_OVERFLOW (pairs).  Site offsets that do not rise from 0 by
- * at least 2 sites a filament return SC_ERR_INVALID_ARG (checked on the
- * device, where they are; nothing is written outside the scratch).  The call synchronises the stream.  The
- * first call on a device looks up the scratch address with
- * cudaGetSymbolAddress; make that first call before any stream capture.
- * All calls on a device share the scratch and leave their data in it; calls
- * whose GPU work overlaps race and must be serialised by the caller. */
+ * at most SC_NOALLOC_MAX_CELLS cells (at most 50 cells a side in 3D, 362 in
+ * 2D, with the cell length of the species), at most SC_NOALLOC_MAX_PAIRS
+ * candidate pairs; larger inputs, or a radius that is not finite, return
+ * SC_ERR_INVALID_ARG (sizes, cells) or SC_ERR_LIST_OVERFLOW (pairs).  Site
+ * offsets that do not rise from 0 by at least 2 sites a filament return
+ * SC_ERR_INVALID_ARG (checked on the device, where they are; nothing is
+ * written outside the scratch).  The call reads the last site offset back
+ * and synchronises the stream, so it must be made outside stream capture.
+ * The first call on a device (and the first after a cudaDeviceReset, which
+ * makes a new context) looks up the scratch address with
+ * cudaGetSymbolAddress.  All calls on a device share the scratch and leave
+ * their data in it; calls whose GPU work overlaps race and must be
+ * serialised by the caller. */
 #define SC_NOALLOC_MAX_BONDS 8192
 #define SC_NOALLOC_MAX_CELLS 131072
 #define SC_NOALLOC_MAX_PAIRS 32768

@@ -12,7 +12,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE_TREE = "/root/reference"
+# Where the reference's source tree is read from (its src/ and include/);
+# SIMCORE_REFERENCE_TREE overrides the default location.
+REFERENCE_TREE = os.environ.get("SIMCORE_REFERENCE_TREE", "/root/reference")
 
 
 def _cc():

@@ -258,73 +258,124 @@ sc_status upload_reps(sc_ctx *c) {
   return SC_OK;
 }
 
-void free_pair_storage(sc_ctx *c) {
-  for (void *q : {(void *)c->d.pa, (void *)c->d.pb, (void *)c->d.pos1, (void *)c->d.pos2,
-                  (void *)c->d.pf64, (void *)c->d.pf32, (void *)c->d.cf64, (void *)c->d.cf32,
-                  (void *)c->d.e_ent, (void *)c->d.pv64, (void *)c->d.pv32,
-                  (void *)c->d.fix_list})
-    dfree(c, q);
-  c->d.pv64 = nullptr;
-  c->d.pv32 = nullptr;
-  c->d.fix_list = nullptr;
+// The pair-list arrays of a context (DevState's pair members).
+struct PairStore {
+  int *pa = nullptr, *pb = nullptr, *pos1 = nullptr, *pos2 = nullptr, *e_ent = nullptr;
+  double *pf64 = nullptr, *cf64 = nullptr, *pv64 = nullptr;
+  float *pf32 = nullptr, *cf32 = nullptr, *pv32 = nullptr;
+  int *fix_list = nullptr;
+};
+
+void free_store(sc_ctx *c, PairStore &q) {
+  for (void *p : {(void *)q.pa, (void *)q.pb, (void *)q.pos1, (void *)q.pos2, (void *)q.pf64,
+                  (void *)q.pf32, (void *)q.cf64, (void *)q.cf32, (void *)q.e_ent,
+                  (void *)q.pv64, (void *)q.pv32, (void *)q.fix_list})
+    dfree(c, p);
+  q = PairStore{};
 }
 
-// The list of near-parallel pairs (one slot per pair) of the exact
-// near-parallel mode and its counters, zeroed once; k_pair_fixup leaves
-// them zero after every pair stage.
-sc_status alloc_fixup(sc_ctx *c, long long total) {
-  if (!c->npx) return SC_OK;
-  CKS(dalloc(c, &c->d.fix_list, total));
-  if (!c->d.fix_count) {
-    CKS(dalloc(c, &c->d.fix_count, 1));
-    CKS(dalloc(c, &c->d.fix_done, 1));
-    CK(cudaMemsetAsync(c->d.fix_count, 0, sizeof(int), c->st));
-    CK(cudaMemsetAsync(c->d.fix_done, 0, sizeof(unsigned), c->st));
-  }
-  return SC_OK;
+PairStore current_store(const sc_ctx *c) {
+  const DevState &d = c->d;
+  PairStore q;
+  q.pa = d.pa;
+  q.pb = d.pb;
+  q.pos1 = d.pos1;
+  q.pos2 = d.pos2;
+  q.e_ent = d.e_ent;
+  q.pf64 = d.pf64;
+  q.cf64 = d.cf64;
+  q.pv64 = d.pv64;
+  q.pf32 = d.pf32;
+  q.cf32 = d.cf32;
+  q.pv32 = d.pv32;
+  q.fix_list = d.fix_list;
+  return q;
 }
 
-// Per-pair virial records for `total` slots, zeroed (a pair not evaluated
-// since the list was built has stress and potential 0).
-sc_status alloc_pair_records(sc_ctx *c, long long total) {
-  if (c->prec == 0) {
-    CKS(dalloc(c, &c->d.pv64, 4 * total));
-    CK(cudaMemsetAsync(c->d.pv64, 0, sizeof(double) * 4 * (total ? total : 1), c->st));
-  } else {
-    CKS(dalloc(c, &c->d.pv32, 4 * total));
-    CK(cudaMemsetAsync(c->d.pv32, 0, sizeof(float) * 4 * (total ? total : 1), c->st));
-  }
+// Frees the context's pair arrays and puts q's in their place.
+void install_store(sc_ctx *c, const PairStore &q) {
+  PairStore old = current_store(c);
+  free_store(c, old);
+  DevState &d = c->d;
+  d.pa = q.pa;
+  d.pb = q.pb;
+  d.pos1 = q.pos1;
+  d.pos2 = q.pos2;
+  d.e_ent = q.e_ent;
+  d.pf64 = q.pf64;
+  d.cf64 = q.cf64;
+  d.pv64 = q.pv64;
+  d.pf32 = q.pf32;
+  d.cf32 = q.cf32;
+  d.pv32 = q.pv32;
+  d.fix_list = q.fix_list;
+}
+
+// New pair arrays for `total` slots, with the context's precision and
+// options: slot indices and slots zeroed (a slot index names a valid slot
+// until a rebuild or a restore fills it), virial records zeroed (a pair not
+// evaluated since the list was built has stress and potential 0).  Either
+// every array is allocated, or none is (the context is left as it was).
+sc_status alloc_store(sc_ctx *c, long long total, PairStore &q) {
+  q = PairStore{};
+  const size_t n = (size_t)(total > 0 ? total : 1);
+  auto all = [&]() -> sc_status {
+    CKS(dalloc(c, &q.pa, n));
+    CKS(dalloc(c, &q.pb, n));
+    CKS(dalloc(c, &q.pos1, n));
+    CKS(dalloc(c, &q.pos2, n));
+    CKS(dalloc(c, &q.e_ent, 2 * n));
+    CK(cudaMemsetAsync(q.pos1, 0, sizeof(int) * n, c->st));
+    CK(cudaMemsetAsync(q.pos2, 0, sizeof(int) * n, c->st));
+    if (c->prec == 0) {
+      CKS(dalloc(c, &q.pf64, 4 * n));
+      CKS(dalloc(c, &q.cf64, 16 * n));
+      CK(cudaMemsetAsync(q.cf64, 0, sizeof(double) * 16 * n, c->st));
+      if (c->k.thermo) {
+        CKS(dalloc(c, &q.pv64, 4 * n));
+        CK(cudaMemsetAsync(q.pv64, 0, sizeof(double) * 4 * n, c->st));
+      }
+    } else {
+      CKS(dalloc(c, &q.pf32, 4 * n));
+      CKS(dalloc(c, &q.cf32, 16 * n));
+      CK(cudaMemsetAsync(q.cf32, 0, sizeof(float) * 16 * n, c->st));
+      if (c->k.thermo) {
+        CKS(dalloc(c, &q.pv32, 4 * n));
+        CK(cudaMemsetAsync(q.pv32, 0, sizeof(float) * 4 * n, c->st));
+      }
+      if (c->npx) CKS(dalloc(c, &q.fix_list, n));
+    }
+    return SC_OK;
+  };
+  const sc_status s = all();
+  if (s != SC_OK) free_store(c, q);
+  return s;
+}
+
+// The counters of the near-parallel list (k_pair_eval's last block leaves
+// them zero after every pair stage), zeroed once.
+sc_status alloc_fixup_counters(sc_ctx *c) {
+  if (c->d.fix_count) return SC_OK;
+  CKS(dalloc(c, &c->d.fix_count, 1));
+  CKS(dalloc(c, &c->d.fix_done, 1));
+  CK(cudaMemsetAsync(c->d.fix_count, 0, sizeof(int), c->st));
+  CK(cudaMemsetAsync(c->d.fix_done, 0, sizeof(unsigned), c->st));
   return SC_OK;
 }
 
 // Pair storage for segments of the given capacities, one per system, back
 // to back; previous contents are discarded.  Stored pair forces are padded
 // to 4 values and per-bond slots to 8, so every write is a 16-byte store.
+// The new arrays are allocated before the old ones are freed: a failed
+// allocation leaves the context's storage and segments as they were.
 sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
   long long total = 0;
   for (long long x : caps) total += x;
   if (total >= (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair lists of %lld slots too large", total);
-  free_pair_storage(c);
-  DevState &d = c->d;
-  CKS(dalloc(c, &d.pa, total));
-  CKS(dalloc(c, &d.pb, total));
-  CKS(dalloc(c, &d.pos1, total));
-  CKS(dalloc(c, &d.pos2, total));
-  // Slot indices name a valid slot until a rebuild or a restore fills them.
-  CK(cudaMemsetAsync(d.pos1, 0, sizeof(int) * total, c->st));
-  CK(cudaMemsetAsync(d.pos2, 0, sizeof(int) * total, c->st));
-  if (c->prec == 0) {
-    CKS(dalloc(c, &d.pf64, 4 * total));
-    CKS(dalloc(c, &d.cf64, 16 * total));
-    CK(cudaMemsetAsync(d.cf64, 0, sizeof(double) * 16 * total, c->st));
-  } else {
-    CKS(dalloc(c, &d.pf32, 4 * total));
-    CKS(dalloc(c, &d.cf32, 16 * total));
-    CK(cudaMemsetAsync(d.cf32, 0, sizeof(float) * 16 * total, c->st));
-  }
-  CKS(dalloc(c, &d.e_ent, 2 * total));
-  if (c->k.thermo) CKS(alloc_pair_records(c, total));
-  CKS(alloc_fixup(c, total));
+  if (c->prec != 0 && c->npx) CKS(alloc_fixup_counters(c));
+  PairStore q;
+  CKS(alloc_store(c, total, q));
+  install_store(c, q);
   long long p0 = 0;
   for (size_t r = 0; r < caps.size(); ++r) {
     c->reps[r].p0 = (int)p0;
@@ -336,77 +387,39 @@ sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
 }
 
 // One system only: grows its segment to at least `need` pairs, keeping the
-// current list (pairs, their stored forces and the per-bond entries).
+// current list (pairs, their stored forces and the per-bond entries).  A
+// failed allocation leaves the current list in place.
 sc_status ensure_pair_capacity(sc_ctx *c, long long need) {
   if (need <= c->pcap) return SC_OK;
   if (c->reps.size() != 1)
     return fail(c, SC_ERR_LIST_OVERFLOW, "a system's pair list outgrew its segment");
   long long cap = std::max<long long>(need + need / 2, 1024);
   if (cap >= (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list of %lld pairs too large", need);
-  DevState old = c->d;
+  const DevState &old = c->d;
   const long long keep = std::min<long long>(c->np, c->pcap);
-  DevState &d = c->d;
-  int *pa = nullptr, *pb = nullptr, *ent = nullptr, *pos1 = nullptr, *pos2 = nullptr;
-  double *pf64 = nullptr, *cf64 = nullptr;
-  float *pf32 = nullptr, *cf32 = nullptr;
-  CKS(dalloc(c, &pa, cap));
-  CKS(dalloc(c, &pb, cap));
-  CKS(dalloc(c, &pos1, cap));
-  CKS(dalloc(c, &pos2, cap));
-  if (c->prec == 0) {
-    CKS(dalloc(c, &pf64, 4 * cap));
-    CKS(dalloc(c, &cf64, 16 * cap));
-    CK(cudaMemsetAsync(cf64, 0, sizeof(double) * 16 * cap, c->st));
-  } else {
-    CKS(dalloc(c, &pf32, 4 * cap));
-    CKS(dalloc(c, &cf32, 16 * cap));
-    CK(cudaMemsetAsync(cf32, 0, sizeof(float) * 16 * cap, c->st));
-  }
-  CKS(dalloc(c, &ent, 2 * cap));
-  double *pv64 = nullptr;
-  float *pv32 = nullptr;
-  if (c->k.thermo) {
-    if (c->prec == 0) {
-      CKS(dalloc(c, &pv64, 4 * cap));
-      CK(cudaMemsetAsync(pv64, 0, sizeof(double) * 4 * cap, c->st));
-    } else {
-      CKS(dalloc(c, &pv32, 4 * cap));
-      CK(cudaMemsetAsync(pv32, 0, sizeof(float) * 4 * cap, c->st));
-    }
-  }
+  PairStore q;
+  CKS(alloc_store(c, cap, q));
   if (keep > 0) {
     auto cp = [&](void *dst, const void *src, size_t bytes) {
       return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c->st);
     };
-    CK(cp(pa, old.pa, sizeof(int) * keep));
-    CK(cp(pb, old.pb, sizeof(int) * keep));
-    CK(cp(pos1, old.pos1, sizeof(int) * keep));
-    CK(cp(pos2, old.pos2, sizeof(int) * keep));
+    CK(cp(q.pa, old.pa, sizeof(int) * keep));
+    CK(cp(q.pb, old.pb, sizeof(int) * keep));
+    CK(cp(q.pos1, old.pos1, sizeof(int) * keep));
+    CK(cp(q.pos2, old.pos2, sizeof(int) * keep));
     if (c->prec == 0) {
-      CK(cp(pf64, old.pf64, sizeof(double) * 4 * keep));
-      CK(cp(cf64, old.cf64, sizeof(double) * 16 * keep));
+      CK(cp(q.pf64, old.pf64, sizeof(double) * 4 * keep));
+      CK(cp(q.cf64, old.cf64, sizeof(double) * 16 * keep));
     } else {
-      CK(cp(pf32, old.pf32, sizeof(float) * 4 * keep));
-      CK(cp(cf32, old.cf32, sizeof(float) * 16 * keep));
+      CK(cp(q.pf32, old.pf32, sizeof(float) * 4 * keep));
+      CK(cp(q.cf32, old.cf32, sizeof(float) * 16 * keep));
     }
-    CK(cp(ent, old.e_ent, sizeof(int) * 2 * keep));
-    if (pv64 && old.pv64) CK(cp(pv64, old.pv64, sizeof(double) * 4 * keep));
-    if (pv32 && old.pv32) CK(cp(pv32, old.pv32, sizeof(float) * 4 * keep));
+    CK(cp(q.e_ent, old.e_ent, sizeof(int) * 2 * keep));
+    if (q.pv64 && old.pv64) CK(cp(q.pv64, old.pv64, sizeof(double) * 4 * keep));
+    if (q.pv32 && old.pv32) CK(cp(q.pv32, old.pv32, sizeof(float) * 4 * keep));
   }
   CK(cudaStreamSynchronize(c->st));
-  free_pair_storage(c);
-  d.pv64 = pv64;
-  d.pv32 = pv32;
-  CKS(alloc_fixup(c, cap));
-  d.pa = pa;
-  d.pb = pb;
-  d.pos1 = pos1;
-  d.pos2 = pos2;
-  d.pf64 = pf64;
-  d.pf32 = pf32;
-  d.cf64 = cf64;
-  d.cf32 = cf32;
-  d.e_ent = ent;
+  install_store(c, q);
   c->reps[0].p0 = 0;
   c->reps[0].pcap = (int)cap;
   c->pcap = cap;
@@ -910,7 +923,8 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
     long long tot = 0;
     for (int r = 0; r < nrep; ++r) {
       if (nfil[r] <= 0) return fail(c, SC_ERR_INVALID_ARG, "system %d has no filaments", r);
-      if (!(radius[r] > 0)) return fail(c, SC_ERR_INVALID_ARG, "system %d: bad radius", r);
+      if (!(radius[r] > 0) || !std::isfinite(radius[r]))
+        return fail(c, SC_ERR_INVALID_ARG, "system %d: bad radius", r);
       tot += nfil[r];
     }
     if (tot != n)
@@ -925,7 +939,9 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
   int max_ns = 0;
   for (int f = 0; f < n; ++f) {
     if (!(p[f].length > 0) || !(p[f].diameter > 0) || !(p[f].min_bond_length > 0) ||
-        !(p[f].friction_ratio > 0) || p[f].persistence_length < 0)
+        !(p[f].friction_ratio > 0) || !(p[f].persistence_length >= 0) ||
+        !std::isfinite(p[f].diameter) || !std::isfinite(p[f].min_bond_length) ||
+        !std::isfinite(p[f].friction_ratio) || !std::isfinite(p[f].persistence_length))
       return fail(c, SC_ERR_INVALID_ARG, "filament %d: bad parameters", f);
     if (p[f].min_bond_length != mbl || p[f].diameter != dia)
       return fail(c, SC_ERR_INVALID_ARG,
@@ -1080,7 +1096,13 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
       if (spec_length > min_len) min_len = spec_length;
       if (0.0 > min_len) min_len = 0.0;
       if (std::sqrt(k.rcut2) > min_len) min_len = std::sqrt(k.rcut2);
-      int n1d = (int)std::floor(2 * radius[r] / min_len);
+      // Cells a side, bounded while still a double so that no integer below
+      // can overflow: at most 1024 in 3D, 32768 in 2D (2^30 cells).
+      const double per_side = 2 * radius[r] / min_len;
+      if (!std::isfinite(per_side) || !(per_side < (c->nd == 3 ? 1025.0 : 32769.0)))
+        return fail(c, SC_ERR_INVALID_ARG,
+                    "system %d: a cell grid of %g cells a side is too large", r, per_side);
+      int n1d = (int)std::floor(per_side);
       if (n1d <= 3) n1d = 3;
       const long long ncell = (long long)n1d * n1d * (c->nd == 3 ? n1d : 1);
       R.n1d = n1d;
@@ -1833,8 +1855,10 @@ sc_status sc_restore(sc_ctx *c, const void *buf, size_t size) {
     if ((size_t)h.payload_bytes < need) return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
     CKS(check_pair_indices(c, caps, sized, in));
   }
-  c->rbuf = h.rbuf;  // selects the geometry buffer the checkpoint fills
-  CKS(layout_pairs(c, caps));  // the checkpoint's segments
+  // The checkpoint's segments; a failed allocation leaves the context as it
+  // was.  Then rbuf selects the geometry buffer the checkpoint fills.
+  CKS(layout_pairs(c, caps));
+  c->rbuf = h.rbuf;
   auto regions = state_regions(c);
   for (auto &r : regions) {
     CK(cudaMemcpyAsync(r.ptr, in, r.bytes, cudaMemcpyHostToDevice, c->st));
@@ -2248,7 +2272,18 @@ sc_status sc_set_thermo(sc_ctx *c, int n_thermo) {
     d.th_cap = 256;
     CKS(dalloc(c, &d.th_rec, 12 * (size_t)nrep * d.th_cap));
   }
-  if (!(c->prec == 0 ? (void *)d.pv64 : (void *)d.pv32)) CKS(alloc_pair_records(c, c->pcap));
+  if (!(c->prec == 0 ? (void *)d.pv64 : (void *)d.pv32)) {
+    // Per-pair virial records, zeroed (a pair not evaluated since the list
+    // was built has stress and potential 0).
+    const size_t n = (size_t)(c->pcap > 0 ? c->pcap : 1);
+    if (c->prec == 0) {
+      CKS(dalloc(c, &d.pv64, 4 * n));
+      CK(cudaMemsetAsync(d.pv64, 0, sizeof(double) * 4 * n, c->st));
+    } else {
+      CKS(dalloc(c, &d.pv32, 4 * n));
+      CK(cudaMemsetAsync(d.pv32, 0, sizeof(float) * 4 * n, c->st));
+    }
+  }
   std::vector<long long> ist(nrep, c->i_step);
   CK(cudaMemsetAsync(d.th_ticket, 0, sizeof(unsigned) * nrep, c->st));
   CK(cudaMemsetAsync(d.th_acc, 0, sizeof(double) * 9 * nrep, c->st));
@@ -2327,8 +2362,11 @@ sc_status sc_set_exact_near_parallel(sc_ctx *c, int on) {
   if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
   if (c->prec == 0 || c->npx == (on != 0)) return SC_OK;
   CK(cudaSetDevice(c->desc.device));
+  if (on) {
+    CKS(alloc_fixup_counters(c));
+    if (!c->d.fix_list) CKS(dalloc(c, &c->d.fix_list, (size_t)(c->pcap > 0 ? c->pcap : 1)));
+  }
   c->npx = on != 0;
-  if (c->npx && !c->d.fix_list) CKS(alloc_fixup(c, c->pcap));
   CK(cudaStreamSynchronize(c->st));
   drop_graph(c);
   return SC_OK;

@@ -1,19 +1,22 @@
 // Pair forces without any device allocation (sc_pair_forces_noalloc).
 //
-// Some callers cannot call cudaMalloc: a host application that records its
-// work into its own CUDA graph (allocation is not allowed while a stream is
-// being captured), or one whose device memory is owned by its own pool or
-// allocator and must not be grown behind its back.  This entry point serves
-// them: it evaluates the WCA bond forces and torques of one configuration
-// held in the caller's device buffers, using only a fixed scratch area that
-// is part of the library image.
+// Some callers cannot call cudaMalloc: a host application whose device
+// memory is owned by its own pool or caching allocator, which must not be
+// grown or fragmented behind its back, or one that runs under a fixed
+// device-memory budget reserved at start-up (a solver embedded in a larger
+// simulation code, a real-time controller).  This entry point serves them:
+// it evaluates the WCA bond forces and torques of one configuration held in
+// the caller's device buffers, using only a fixed scratch area that is part
+// of the library image.  It reads one size back and synchronises the
+// stream, so it is called outside stream capture.
 //
 // The scratch is one file-scope __device__ array (g_noalloc_scratch below,
-// SC_NOALLOC_SCRATCH_BYTES = 8.5 MiB).  Every GPU that loads the library holds it until the
-// process exits.  All calls on a device share it and it keeps the last
-// call's contents, so every call clears what must start at zero; calls
-// whose GPU work overlaps (several host threads, or several streams) race
-// on it and must be serialised by the caller.
+// SC_NOALLOC_SCRATCH_BYTES = 8.5 MiB).  Every GPU that loads the library
+// holds it until the process exits.  All calls on a device share it and it
+// keeps the last call's contents, so every call clears what must start at
+// zero; calls whose GPU work overlaps (several host threads, or several
+// streams) race on it and must be serialised by the caller.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -93,25 +96,68 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kLayout.total];
 
 namespace {
 
-// Device address of g_noalloc_scratch per device ordinal, looked up once per
-// device (with that device current) and cached.  In host code the symbol
-// name is only a host-side stand-in, never a device address.
+// Device address of g_noalloc_scratch, looked up with cudaGetSymbolAddress
+// once per device and CUDA context (with that device current) and cached.
+// In host code the symbol name is only a host-side stand-in, never a device
+// address.  The cache is keyed on the context's unique id (cuCtxGetId, never
+// reused within a process), so a context created after cudaDeviceReset, or
+// another context made current on the same device, gets its own lookup.  The
+// first call on a device (and after a reset) does the lookup, which may load
+// the library's device code: make that call before any stream capture.
 constexpr int kMaxDevices = 64;
 std::mutex g_addr_mtx;
-unsigned char *g_addr[kMaxDevices] = {};
+struct ScratchAddr {
+  unsigned long long ctx_id;  // 0: not looked up
+  unsigned char *ptr;
+};
+ScratchAddr g_addr[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current context; false when there is
+// none yet (the runtime makes its primary context current on first use).
+bool current_context_id(unsigned long long *id) {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {  // (under g_addr_mtx)
+    looked_up = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_current = (CtxGetCurrentFn)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = (CtxGetIdFn)f;
+    cudaGetLastError();
+  }
+  if (!get_current || !get_id) return false;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return get_id(ctx, id) == CUDA_SUCCESS && *id != 0;
+}
 
 sc_status scratch_address(int dev, unsigned char **out) {
   if (dev < 0 || dev >= kMaxDevices) return SC_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lk(g_addr_mtx);
-  if (!g_addr[dev]) {
+  unsigned long long id = 0;
+  const bool have_id = current_context_id(&id);
+  ScratchAddr &a = g_addr[dev];
+  if (!have_id || a.ctx_id != id || !a.ptr) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
       cudaGetLastError();
       return SC_ERR_CUDA;
     }
-    g_addr[dev] = (unsigned char *)p;
+    // The lookup made the device's primary context current if none was.
+    unsigned long long after = 0;
+    a.ptr = (unsigned char *)p;
+    a.ctx_id = current_context_id(&after) ? after : 0;
   }
-  *out = g_addr[dev];
+  *out = a.ptr;
   return SC_OK;
 }
 
@@ -185,8 +231,12 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
       !d_bond_torque)
     return SC_ERR_INVALID_ARG;
   if (desc->n_dim != 2 && desc->n_dim != 3) return SC_ERR_INVALID_ARG;
-  if (!(desc->system_radius > 0) || !(desc->wca_sig > 0)) return SC_ERR_INVALID_ARG;
-  if (!(species->min_bond_length > 0) || !(species->diameter > 0)) return SC_ERR_INVALID_ARG;
+  if (!(desc->system_radius > 0) || !std::isfinite(desc->system_radius) ||
+      !(desc->wca_sig > 0) || !std::isfinite(desc->wca_sig))
+    return SC_ERR_INVALID_ARG;
+  if (!(species->min_bond_length > 0) || !std::isfinite(species->min_bond_length) ||
+      !(species->diameter > 0) || !std::isfinite(species->diameter))
+    return SC_ERR_INVALID_ARG;
   if (n_filaments <= 0 || n_filaments > kMaxFilaments) return SC_ERR_INVALID_ARG;
   cudaStream_t st = (cudaStream_t)stream;
   int dev = 0;
@@ -230,9 +280,17 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
     if (spec_length > min_len) min_len = spec_length;
     if (0.0 > min_len) min_len = 0.0;
     if (std::sqrt(k.rcut2) > min_len) min_len = std::sqrt(k.rcut2);
-    int n1d = (int)std::floor(2 * desc->system_radius / min_len);
+    // The cell count is bounded while it is still a double: at most
+    // floor(cbrt(SC_NOALLOC_MAX_CELLS)) = 50 cells a side in 3D,
+    // floor(sqrt(SC_NOALLOC_MAX_CELLS)) = 362 in 2D, so no integer below
+    // can overflow or wrap.
+    const double per_side = 2 * desc->system_radius / min_len;
+    const double max_side =
+        std::floor(nd == 3 ? std::cbrt((double)kMaxCells) : std::sqrt((double)kMaxCells));
+    if (!std::isfinite(per_side) || !(per_side < max_side + 1.0)) return SC_ERR_INVALID_ARG;
+    int n1d = (int)std::floor(per_side);
     if (n1d <= 3) n1d = 3;
-    long long ncell = (long long)n1d * n1d * (nd == 3 ? n1d : 1);
+    const long long ncell = (long long)n1d * n1d * (nd == 3 ? n1d : 1);
     if (ncell > kMaxCells) return SC_ERR_INVALID_ARG;
     R.n1d = n1d;
     R.third = nd == 3 ? n1d : 1;

@@ -597,8 +597,8 @@ def test_non_finite_positions_are_reported():
 def test_invalid_inputs_are_rejected():
     """Inputs the library cannot take fail with an error status and a
     message, before any device work: no filaments, inconsistent site counts,
-    bad parameters, filaments past the 255-bond limit, negative step
-    counts."""
+    bad parameters, filaments past the 255-bond limit, cell grids too large
+    to count, negative step counts."""
     import simcore_b200 as sc
     system, fils, sites = _workload("A", 0.05, seed=1)
     with pytest.raises(sc.ScError):
@@ -614,6 +614,12 @@ def test_invalid_inputs_are_rejected():
     assert n > 256
     with pytest.raises(sc.ScError, match="255 bonds"):
         _ctx(system, [long_fil], np.zeros((n, 3)))
+    # Cell grids are bounded while their size is still a double: a radius of
+    # 2.4e6 (2^22 cells a side, whose cube wraps a 64-bit count to 0) and an
+    # infinite one are refused on the host.
+    for radius in (2.4e6, float("inf")):
+        with pytest.raises(sc.ScError, match="radius|cell grid"):
+            _ctx(dict(system, system_radius=radius), fils, sites)
     ctx = _ctx(system, fils, sites)
     with pytest.raises(sc.ScError):
         ctx.step(-1)

@@ -1,13 +1,14 @@
 """sc_pair_forces_noalloc: pair forces for callers that cannot allocate.
 
-An application that records its own CUDA graph cannot call cudaMalloc while
-capturing, and one whose device memory belongs to its own pool must not be
-grown behind its back; the no-allocation entry point serves both by working
-in a fixed scratch array inside the library.  This test calls it through the
-C ABI on buffers the test owns and checks its bond forces and torques
-against those of the regular entry points (sc_interact on a context just
-loaded with the same sites) -- FP64, so exactly equal -- on two calls in a
-row, the second finding the first call's data still in the scratch.
+An application whose device memory belongs to its own pool or caching
+allocator must not have it grown behind its back, and one that runs under a
+device-memory budget fixed at start-up cannot call cudaMalloc at all; the
+no-allocation entry point serves both by working in a fixed scratch array
+inside the library.  This test calls it through the C ABI on buffers the
+test owns and checks its bond forces and torques against those of the
+regular entry points (sc_interact on a context just loaded with the same
+sites) -- FP64, so exactly equal -- on two calls in a row, the second
+finding the first call's data still in the scratch.
 
 The file is named to be collected last, so that a run stopping at the first
 failure has already run every other test.  It passes alone in a fresh
@@ -113,6 +114,23 @@ def test_noalloc_rejects_bad_site_offsets():
     for bad in (swapped, short):
         assert bad[0] == 0 and bad[-1] == good[-1]  # only the device check can see it
         _call_noalloc(system, fils, sites, offsets=bad, expect=1)  # SC_ERR_INVALID_ARG
+    f_ref, t_ref = _reference_forces(system, fils, sites)
+    f, t = _call_noalloc(system, fils, sites)
+    assert np.array_equal(f, f_ref)
+    assert np.array_equal(t, t_ref)
+
+
+def test_noalloc_rejects_cell_grids_beyond_the_limit():
+    """The cell count is bounded on the host while it is still a double: a
+    large finite radius (2^22 cells a side would wrap a 64-bit cell count to
+    0) and an infinite one are refused before any launch, and a correct call
+    afterwards still gives the regular forces."""
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("A", 0.1, seed=14)
+    for radius in (2.4e6, 1e300, float("inf"), 60.0):
+        # 60: 104 cells a side in 3D, over the 50 the scratch holds
+        big = dict(system, system_radius=radius)
+        _call_noalloc(big, fils, sites, expect=1)  # SC_ERR_INVALID_ARG
     f_ref, t_ref = _reference_forces(system, fils, sites)
     f, t = _call_noalloc(system, fils, sites)
     assert np.array_equal(f, f_ref)
