@@ -36,6 +36,9 @@ sys.path.insert(0, ROOT)
 METRIC = "segment-steps/s, 1 B200: mixed+batched vs FP64 GPU at ≤1e-5 force err"
 UNIT = "segment-steps/s"
 I_STEPS_PER_STEP = 20
+# Points of the timed mixed trajectory at which the mixed-precision error is
+# measured (after every quarter of the timed steps).
+N_SNAPSHOTS = 4
 # DRAM bytes (read + write) of one k_integrate launch, mixed precision, from
 # ncu (cold cache), per workload captured: for B (96-site blocks) the mean of
 # a midstep launch (23.05 MB) and a full-step launch (40.69 MB), which
@@ -235,7 +238,8 @@ def kernel_times(ctx, n):
 
 
 def load_workload(name, seed):
-    """(system, filaments, sites, replicas, crosslinks) of a workload."""
+    """(system, filaments, sites, replicas, crosslinks) of a workload, made by
+    the library's insertion."""
     from simcore_b200 import workloads
     if name == "D":
         system, fils, sites, reps = workloads.make_replicas("D", seed=seed)
@@ -243,6 +247,15 @@ def load_workload(name, seed):
     system, fils, sites = workloads.make(name, 1.0, seed=seed)
     xl = workloads.crosslinks(name, sites, fils, 2 * system["system_radius"], seed=seed)
     return system, fils, sites, None, xl
+
+
+def workload_config(name):
+    """The `config` of both arms' JSON lines: the workload and the units of
+    the metric, nothing that depends on the arm."""
+    return {"workload": WORKLOAD_DESCS[name],
+            "segment": "one bond of a filament",
+            "step": "one reference i_step: a pair-force evaluation and an integrator half "
+                    "step, delta/2 of simulated time"}
 
 
 def new_context(sc, wl, prec, device):
@@ -261,13 +274,12 @@ def cpu_runs(wl, cores):
     code being unbuildable here.  Independent systems run one after another
     (the reference keeps static state: one simulation per process at a time),
     a leading subset of them.  Returns (kind, cores, [(make, bonds)], note),
-    make() creating one simulation."""
+    make() creating one simulation.  Uses the CPU checkers only (bond counts
+    by the oracle's rule): the CUDA library is not loaded here."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from checkers import Oracle, Reference
-    import simcore_b200 as sc
-    from simcore_b200 import workloads
+    from checkers import Oracle, Reference, oracle_n_bonds, workloads_module
     system, fils, sites, reps, xl = wl
-    bonds = lambda fs: sum(sc.filament_n_bonds(f) for f in fs)
+    bonds = lambda fs: sum(oracle_n_bonds(f) for f in fs)
     if xl is not None:
         def make_tethered():
             sim = Oracle(system, fils, sites)
@@ -287,14 +299,15 @@ def cpu_runs(wl, cores):
         # default bench run.)
         n_keep, nb_keep = 0, 0
         while n_keep < len(fils) and nb_keep < 100000:
-            nb_keep += sc.filament_n_bonds(fils[n_keep])
+            nb_keep += oracle_n_bonds(fils[n_keep])
             n_keep += 1
         ns_keep = nb_keep + n_keep
         sub = (system, fils[:n_keep], sites[:ns_keep])
         return kind, cores, [(lambda: make(*sub), nb_keep)], \
             "the first %d of %d filaments in the full box" % (n_keep, len(fils))
     runs, total = [], 0
-    for part in workloads.split_replicas(system, fils, sites, reps):
+    for part in workloads_module().split_replicas(system, fils, sites, reps,
+                                                  n_bonds=oracle_n_bonds):
         runs.append(((lambda p=part: make(*p)), bonds(part[1])))
         total += runs[-1][1]
         if total >= 100000:
@@ -315,6 +328,7 @@ def profile_only(args):
         layout = [int(v) for v in args.profile_layout.split(",")]
         ctx.set_integrator_layout(*layout)
     if args.profile_fused:
+        ctx.set_exact_near_parallel(False)
         ctx.set_fused_pairs(True)
     ctx.step(4)
     ctx.step(args.profile_steps)
@@ -343,20 +357,26 @@ def run_ours(args, rank, world, local_rank):
     system, fils, sites = wl[:3]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def timed_graph(ctx, k, flush_l2=True):
-        """k bench steps; returns per-step device ms (CUDA events)."""
+    def timed_graph(ctx, k, flush_l2=True, snapshots=None):
+        """k bench steps; returns per-step device ms (CUDA events).  With a
+        list `snapshots`, the positions after every quarter of the steps are
+        appended to it (read between launches, outside the timed launches)."""
         out = []
-        for _ in range(k):
+        marks = {max(1, (k * q) // N_SNAPSHOTS) for q in range(1, N_SNAPSHOTS + 1)}
+        for i in range(k):
             if flush_l2:
                 flush.zero_()
                 torch.cuda.synchronize()
             ctx.step_graph(I_STEPS_PER_STEP)
             out.append(ctx.graph_time_ms())
+            if snapshots is not None and i + 1 in marks:
+                snapshots.append((ctx.counters().i_step, ctx.sites()))
         return out
 
     results = {}
     contexts = {}
     layouts = {}
+    snaps = []  # (i_step, positions) along the timed mixed-precision trajectory
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if sampler:
         sampler.start()
@@ -371,7 +391,7 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         c0 = ctx.counters()
         t_start = time.perf_counter()
-        ms = timed_graph(ctx, args.steps)
+        ms = timed_graph(ctx, args.steps, snapshots=snaps if prec == "mixed" else None)
         torch.cuda.synchronize()
         if sampler:
             sampler.mark(t_start, time.perf_counter())
@@ -384,24 +404,16 @@ def run_ours(args, rank, world, local_rank):
     if sampler:
         results["clocks"] = sampler.stop()
 
-    # Mixed-precision force error on this workload: fresh contexts of both
-    # precisions on the initial positions evaluate the pair forces once; the
-    # mixed bond forces and torques are compared with the FP64 ones
-    # (max |dF| / max |F|), also with nearly parallel pairs evaluated from
-    # the FP64 sites (sc_set_exact_near_parallel; off in the timed runs).
-    errs = {}
-    for p_ in ("fp64", "mixed", "mixed_npx"):
-        cc = new_context(sc, wl, "fp64" if p_ == "fp64" else "mixed", local_rank)
-        if p_ == "mixed_npx":
-            cc.set_exact_near_parallel(True)
-        cc.interact()
-        errs[p_] = cc.bond_forces()
-        cc.close()
-
-    def rel_err(p_, i):
-        return float(np.abs(errs[p_][i] - errs["fp64"][i]).max() / np.abs(errs["fp64"][i]).max())
-
-    force_err, torque_err = rel_err("mixed", 0), rel_err("mixed", 1)
+    # Mixed precision against FP64, output by output (simcore_b200.accuracy):
+    # fresh contexts of both precisions on the same positions -- the inserted
+    # state and the snapshots of the timed mixed trajectory -- evaluate the
+    # pair forces and one integrator step with shared noise.
+    from simcore_b200.accuracy import max_errors, mixed_errors
+    sysd, fl, _, reps_, xl_ = wl
+    err_inserted = mixed_errors(sysd, fl, wl[2], reps_, xl_, device=local_rank)
+    err_traj = [dict(mixed_errors(sysd, fl, xyz, reps_, xl_, device=local_rank), i_step=ist)
+                for ist, xyz in snaps]
+    err_max = max_errors([err_inserted] + err_traj)
 
     # Roofline: per-launch CUDA-event durations of the two kernels of a
     # reference step, host-driven, on the context's stream; beside them the
@@ -409,9 +421,11 @@ def run_ours(args, rank, world, local_rank):
     # timed runs).
     kt = {p: kernel_times(contexts[p], 2 * I_STEPS_PER_STEP) for p in ("mixed", "fp64")}
     ctx = contexts["mixed"]
+    ctx.set_exact_near_parallel(False)  # the fusion evaluates every pair in FP32
     ctx.set_fused_pairs(True)
     t_fused = step_kernel_time(ctx, 2 * I_STEPS_PER_STEP)
     ctx.set_fused_pairs(False)
+    ctx.set_exact_near_parallel(True)
 
     # End to end through the C ABI with host buffers: every bench step
     # uploads the positions from pinned host memory, runs the 20 reference
@@ -469,23 +483,27 @@ def run_ours(args, rank, world, local_rank):
         "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair forces + f64 integrator",
         "data": "synthetic (seeded random insertion with overlap rejection)",
-        "config": {"workload": WORKLOAD_DESCS[args.workload], "precision": "mixed",
-                   "i_steps_per_step": I_STEPS_PER_STEP,
-                   "timed_unit": "one CUDA-graph launch of 20 reference steps (WHILE loop of 10 "
-                                 "midpoint BD steps with device-decided pair-list rebuilds)",
-                   "l2": "flushed by a 256 MiB write before every timed step",
-                   "parallelism": "replicas" if world > 1 else "single system",
-                   "pairs": r["n_pairs"], "rebuilds_in_timed_region": r["rebuilds"],
-                   "integrator_layout": {p: {"warp_max_sites": w, "block_sites": b}
-                                         for p, (w, b) in layouts.items()}},
+        "config": workload_config(args.workload),
+        "run": {"precision": "mixed", "i_steps_per_step": I_STEPS_PER_STEP,
+                "timed_unit": "one CUDA-graph launch of 20 reference steps (WHILE loop of 10 "
+                              "midpoint BD steps with device-decided pair-list rebuilds)",
+                "l2": "flushed by a 256 MiB write before every timed step",
+                "parallelism": "replicas" if world > 1 else "single system",
+                "pairs": r["n_pairs"], "rebuilds_in_timed_region": r["rebuilds"],
+                "integrator_layout": {p: {"warp_max_sites": w, "block_sites": b}
+                                      for p, (w, b) in layouts.items()}},
         "fp64": {"value": value64, "ms_per_step": r64["total_ms"] / args.steps,
                  "rebuilds_in_timed_region": r64["rebuilds"]},
         "mixed_over_fp64": value / value64,
-        "mixed_error": {"max_rel_bond_force": force_err, "max_rel_bond_torque": torque_err,
-                        "exact_near_parallel": {"max_rel_bond_force": rel_err("mixed_npx", 0),
-                                                "max_rel_bond_torque": rel_err("mixed_npx", 1)},
-                        "vs": "FP64 GPU path (bit-identical to the reference) on the same "
-                              "positions, one pair evaluation", "bound": 1e-5},
+        "mixed_error": {
+            "bound": 1e-5, "max": err_max, "inserted_state": err_inserted,
+            "trajectory": err_traj,
+            "vs": "FP64 GPU path (bit-identical to the reference) on the same positions: "
+                  "fresh contexts of both precisions evaluate the pair forces and one "
+                  "integrator step with shared noise; max |mixed - fp64| / max |fp64| per "
+                  "output (displacement = positions after the step - before)",
+            "states": "the inserted state and the timed mixed trajectory after every "
+                      "quarter of the timed steps"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": TRAFFIC_K_INTEGRATE_MIXED.get(args.workload),
@@ -504,8 +522,8 @@ def run_ours(args, rank, world, local_rank):
                                         "ms": t_int + t_pair, "achieved": step_achieved,
                                         "frac": step_achieved / peak},
                      "fused_pairs_option": {
-                         "kernel": "k_integrate<%d,mixed,fast,fused pairs> (sc_set_fused_pairs; "
-                                   "off in the timed runs)" % r["n_dim"],
+                         "kernel": "k_integrate<%d,mixed,fast,fused pairs> (sc_set_fused_pairs, "
+                                   "all pairs in FP32; off in the timed runs)" % r["n_dim"],
                          "avg_launch_ms": t_fused, "algorithmic_bytes_per_launch": b_fused,
                          "achieved": b_fused / (t_fused * 1e-3) / 1e9},
                      "reference_step_fp64": {"algorithmic_bytes": b_int64 + b_pair64,
@@ -555,7 +573,10 @@ def run_reference(args, rank, world):
     if not Reference.available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libscref.so (the reference's "
                 "own sources) was not built on this machine"}
-    kind, cores, runs, note = cpu_runs(load_workload(args.workload, 0), host_cores())
+    from checkers import oracle_workload
+    # The GPU arm's configuration, made by the oracle's insertion (bit for
+    # bit the library's): nothing of the CUDA library is loaded in this arm.
+    kind, cores, runs, note = cpu_runs(oracle_workload(args.workload, 0), host_cores())
     # Size each bench step to a bounded sample: at most 20 reference steps,
     # fewer if one step is slow, so that warm-up + timed steps stay short.
     # (The first system's simulation, built once -- the reference's set-up
@@ -588,11 +609,13 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded random insertion with overlap rejection)",
-        "config": {"workload": WORKLOAD_DESCS[args.workload], "i_steps_per_step": per_step,
-                   "implementation": ("reference C++ (object, site, bond, mesh, filament, cell, "
-                                      "cell_list, minimum_distance, linear_algebra) -O3 OpenMP"
-                                      if kind == "reference" else
-                                      "C restatement of the reference (tethers included)")},
+        "config": workload_config(args.workload),
+        "run": {"i_steps_per_step": per_step,
+                "implementation": ("reference C++ (object, site, bond, mesh, filament, cell, "
+                                   "cell_list, minimum_distance, linear_algebra) -O3 OpenMP"
+                                   if kind == "reference" else
+                                   "C restatement of the reference (tethers included)"),
+                "inputs": "the GPU arm's initial configuration, made by the oracle's insertion"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

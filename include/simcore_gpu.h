@@ -26,7 +26,6 @@
 #define SIMCORE_GPU_H
 
 #include <stddef.h>
-#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -194,15 +193,17 @@ sc_status sc_thermo_open(sc_ctx *ctx, const char *run_name, int n_steps);
 sc_status sc_get_thermo(sc_ctx *ctx, int max_records, int *n_records, int64_t *i_step,
                         double *tensor, double *pressure, double *volume);
 sc_status sc_get_potential_energy(sc_ctx *ctx, double *pote);
-/* Mixed precision only: evaluate nearly parallel pairs (FP32 |u1 x u2|^2
- * between 0 and 1e-5, within 0.18 degrees) from the FP64 sites, as the FP64
- * path does, in a second kernel after each pair stage.  FP32 orientations
- * cannot resolve the closest points of such pairs: their torques (and
- * forces) can be off by far more than 1e-5.  Off by default: the second
- * kernel costs about 10% of the step on workload B.  No counterpart in the
- * reference, whose pair stage is FP64 throughout. */
+/* Mixed precision only: nearly parallel pairs (FP32 |u1 x u2|^2 between 0
+ * and 1e-5, within 0.18 degrees) are evaluated from the FP64 sites, as the
+ * FP64 path evaluates them, by the last block of the pair kernel to finish.
+ * FP32 orientations cannot resolve the closest points of such pairs: their
+ * torques (and forces) could be off by far more than 1e-5.  On by default;
+ * sc_set_exact_near_parallel(ctx, 0) evaluates them in FP32 like every other
+ * pair.  No counterpart in the reference, whose pair stage is FP64
+ * throughout. */
 sc_status sc_set_exact_near_parallel(sc_ctx *ctx, int on);
-/* Fast mixed precision only (not with thermo or the option above): sc_step
+/* Fast mixed precision only, with the option above switched off (the fused
+ * evaluation is FP32 throughout) and without thermo: sc_step
  * and sc_step_graph evaluate each bond's pairs inside the integrator and
  * launch no pair stage.  The results are bit-identical to the separate pair
  * stage, and sc_get_bond_forces still returns the last step's evaluation.

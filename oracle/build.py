@@ -27,13 +27,13 @@ def _cc():
 
 def build_oracle(verbose=False):
     out = os.path.join(HERE, "libscoracle.so")
-    src = os.path.join(HERE, "sc_oracle.c")
+    srcs = [os.path.join(HERE, f) for f in ("sc_oracle.c", "sc_oracle_insert.c")]
     hdrs = [os.path.join(HERE, h) for h in ("sc_oracle.h", "sc_philox.h")]
     if os.path.exists(out) and all(os.path.getmtime(out) >= os.path.getmtime(p)
-                                   for p in [src] + hdrs):
+                                   for p in srcs + hdrs):
         return out
     cmd = [_cc(), "-O2", "-std=c99", "-fPIC", "-shared", "-ffp-contract=off",
-           "-o", out, src, "-lm"]
+           "-o", out] + srcs + ["-lm"]
     if verbose:
         print(" ".join(cmd))
     subprocess.check_call(cmd)

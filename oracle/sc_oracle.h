@@ -107,6 +107,17 @@ long sco_thermo_records(sco_sim *s, long max, long *i_step, double *tensor, doub
 void sco_get_stress(const sco_sim *s, double *stress);
 void sco_get_potential_energy(const sco_sim *s, double *pote);
 
+/* Seeded random insertion with overlap rejection (sc_oracle_insert.c):
+ * n_fil filaments of n_bonds[i] bonds, lengths and persistence lengths given,
+ * in a periodic box of radius system_radius; insertion_type 0 random, 1
+ * random_nematic, 2 random_polar.  Writes sum(n_bonds[i] + 1) x 3 doubles.
+ * Returns 0, 1 (invalid arguments) or 8 (a filament found no place within
+ * max_attempts). */
+int sco_insert_filaments(int n_dim, double system_radius, uint64_t seed, int n_fil,
+                         const int *n_bonds, const double *length,
+                         const double *persistence_length, double diameter,
+                         int insertion_type, int max_attempts, double *site_xyz);
+
 /* Philox4x32-10 block (for the known-answer test of the shared stream). */
 void sco_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 

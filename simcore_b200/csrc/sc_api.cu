@@ -110,7 +110,9 @@ struct sc_ctx {
   double graph_ms = 0.0;
   bool graph_fused = false;  // the captured steps evaluate their pairs in the integrator
   long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
-  bool npx = false;           // mixed: near-parallel pairs evaluated from FP64 sites
+  // Mixed: nearly parallel pairs evaluated from the FP64 sites, by the last
+  // block of the pair kernel (on by default; sc_set_exact_near_parallel).
+  bool npx = true;
   // The last step fused its pair evaluation into the integrator, so the
   // per-bond slots do not hold it yet (materialize_slots writes them).
   bool slots_stale = false;
@@ -1382,14 +1384,13 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       }
       // Kernels the graph ran: loop head, per BD step decide + tether + 2
       // steps + tail (the stopped step's too), per rebuild the captured
-      // sequence.  A step is its pair stage (unless fused), thermo, the
-      // near-parallel fix-up and one or two integrator kernels.
+      // sequence.  A step is its pair stage (unless fused), thermo and
+      // one or two integrator kernels.
       const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
       const long long per_bd =
           c->desc.interaction_flag
               ? 2 + (c->d.nx ? 1 : 0) +
-                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0) +
-                         (c->npx && c->prec ? 1 : 0))
+                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0))
               : 1 + 2 * int_l;
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
                      (nr1 - nr0) * c->rebuild_kernels;

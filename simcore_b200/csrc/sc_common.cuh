@@ -147,11 +147,11 @@ struct DevState {
   int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
   double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
   float *cf32;
-  // mixed pair stage with exact near-parallel pairs: those left to
-  // k_pair_fixup
+  // mixed pair stage with exact near-parallel pairs: those left to the
+  // FP64 fix-up of k_pair_eval's last block
   int *fix_list;           // one slot per pair
   int *fix_count;
-  unsigned *fix_done;
+  unsigned *fix_done;      // blocks of the current launch done (ticket)
   // thermo (kept while SysConst::thermo is set): per pair the dr its stress
   // was computed from and its potential, stored with the force
   double *pv64;            // 4 per pair: dr (3), pote

@@ -9,7 +9,8 @@
 //                  scatter order)
 //   pair forces    k_pair_eval   (InteractionManager::CalculatePairInteractions,
 //                                 one thread per pair, signed per-bond slots)
-//                  k_pair_fixup  (mixed, opt-in: nearly parallel pairs in FP64)
+//                                (mixed: its last block evaluates the nearly
+//                                 parallel pairs in FP64)
 //                  k_bond_sum    (ApplyPairInteractions into bond accumulators)
 //   thermo         k_thermo, k_potential (pair virial and pressure records,
 //                                 per-filament potential energy)
@@ -634,8 +635,10 @@ __device__ __forceinline__ void pair_eval_fp64_sites(const SysConst &k, const De
   c2[1] = make_float4(-(float)t2[1], -(float)t2[2], 0.f, 0.f);
 }
 
+// Returns whether the pair was listed for the FP64 fix-up (NPX) instead of
+// evaluated.
 template <int ND, int PREC, bool NPX>
-__device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
+__device__ __forceinline__ bool pair_eval_one(const SysConst &k, const DevState &d,
                                               const ReplicaConst &R, int rbuf, int p) {
   const int a = d.pa[p], b = d.pb[p];
   const int s1 = d.pos1[p], s2 = d.pos2[p];
@@ -675,9 +678,9 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
-    if (NPX && near_parallel<ND>(A, B)) {  // left to k_pair_fixup
+    if (NPX && near_parallel<ND>(A, B)) {  // left to the fix-up block
       d.fix_list[atomicAdd(d.fix_count, 1)] = p;
-      return;
+      return true;
     }
     float force[3], rec[4], t1[3], t2[3];
     const bool set = pair_force_f32<ND>(k, R.hf, A, B, st, force, t1, t2,
@@ -694,26 +697,21 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     c2[0] = make_float4(-force[0], -force[1], -force[2], -t2[0]);
     c2[1] = make_float4(-t2[1], -t2[2], 0.f, 0.f);
   }
+  return false;
 }
 
 // The nearly parallel pairs the NPX mixed pair stage left, evaluated from the
-// FP64 sites (pair_eval_fp64_sites).  The last block out resets the list
-// (ticket counter, no waiting) for the next pair stage.
+// FP64 sites (pair_eval_fp64_sites) by the threads of one block.  Not
+// inlined: its FP64 registers are its own, so the FP32 loop of k_pair_eval
+// keeps its register budget, and only the block that calls it pays for the
+// spills the budget forces here.
 template <int ND>
-__global__ void __launch_bounds__(128) k_pair_fixup(SysConst k, DevState d) {
-  const int n = *d.fix_count;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void pair_fixup_block(const SysConst &k, const DevState &d) {
+  const int n = *(volatile int *)d.fix_count;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const int p = d.fix_list[i];
     const int r = d.nrep == 1 ? 0 : rep_of_pair(d, p);
     pair_eval_fp64_sites<ND>(k, d, d.rep[r], p);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    if (atomicAdd(d.fix_done, 1u) == gridDim.x - 1) {
-      *d.fix_count = 0;
-      *d.fix_done = 0u;
-    }
   }
 }
 
@@ -721,20 +719,38 @@ __global__ void __launch_bounds__(128) k_pair_fixup(SysConst k, DevState d) {
 // whatever length the lists grow to between captures.  A single system's
 // list is the prefix of its segment; with several systems every slot checks
 // that it holds a current pair of its system.
-// NPX (mixed only): nearly parallel pairs go to k_pair_fixup.
+// NPX (mixed only): nearly parallel pairs are listed, and the last block to
+// finish (ticket counter, no waiting) evaluates the list in FP64 and resets
+// it for the next pair stage.
 template <int ND, int PREC, bool NPX>
-__global__ void __launch_bounds__(256) k_pair_eval(SysConst k, DevState d, int rbuf) {
+__global__ void __launch_bounds__(256, NPX ? 4 : 1) k_pair_eval(SysConst k, DevState d,
+                                                                int rbuf) {
+  bool listed = false;
   if (d.nrep == 1) {
     const ReplicaConst &R = d.rep[0];
     const int np = min(d.np_rep[0], R.pcap);
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
-      pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p);
-    return;
+      listed |= pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p);
+  } else {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
+         p += gridDim.x * blockDim.x) {
+      int r;
+      if (pair_live(d, p, r)) listed |= pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p);
+    }
   }
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
-       p += gridDim.x * blockDim.x) {
-    int r;
-    if (pair_live(d, p, r)) pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p);
+  if (!NPX) return;
+  __shared__ bool s_last;
+  if (listed) __threadfence();  // this thread's list entries, before the ticket
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(d.fix_done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();  // every other block's entries are visible past its ticket
+  pair_fixup_block<ND>(k, d);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *d.fix_count = 0;
+    *d.fix_done = 0u;
   }
 }
 
@@ -1205,10 +1221,7 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
     else if (!npx) k_pair_eval<2, 1, false><<<grid, 256, 0, st>>>(k, d, rbuf);
     else k_pair_eval<2, 1, true><<<grid, 256, 0, st>>>(k, d, rbuf);
   }
-  if (!npx) return 1;
-  if (k.n_dim == 3) k_pair_fixup<3><<<16, 128, 0, st>>>(k, d);
-  else k_pair_fixup<2><<<16, 128, 0, st>>>(k, d);
-  return 2;
+  return 1;
 }
 
 // ---------------------------------------------------------------------------

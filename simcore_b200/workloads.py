@@ -21,12 +21,25 @@ rejection (sc_insert_filaments); no dataset is involved.
 
 scale < 1 shrinks the filament count and the box volume together (same
 density) for parity tests at small sizes.
+
+The module needs only numpy.  The library is imported when a workload is
+made, for its insertion and bond-count rule, unless the caller passes its own
+(`insert`, `n_bonds`): a CPU checker can then build the same configuration
+without loading the CUDA library.
 """
 import math
 
 import numpy as np
 
-from . import filament_n_bonds, insert_filaments
+
+def _library_insert(*args, **kw):
+    from simcore_b200 import insert_filaments
+    return insert_filaments(*args, **kw)
+
+
+def _library_n_bonds(params):
+    from simcore_b200 import filament_n_bonds
+    return filament_n_bonds(params)
 
 MIN_BOND_LENGTH = 0.666
 DIAMETER = 1.0
@@ -46,7 +59,7 @@ WORKLOADS = {
 CROSSLINKS = {"E": dict(n_links=100000, k_spring=10.0, rest_length=1.0, reach=2.0)}
 
 
-def crosslinks(name, sites, filaments, side, scale=1.0, seed=0):
+def crosslinks(name, sites, filaments, side, scale=1.0, seed=0, n_bonds=None):
     """Static tethers of workload `name`: site pairs drawn uniformly from all
     pairs closer than `reach` (minimum image) that are not the same or
     adjacent sites of one filament.  Returns (site_a, site_b, k_spring,
@@ -60,7 +73,8 @@ def crosslinks(name, sites, filaments, side, scale=1.0, seed=0):
     pts[pts >= side] = 0.0
     tree = cKDTree(pts, boxsize=side)
     pairs = tree.query_pairs(c["reach"], output_type="ndarray")
-    n_sites = np.array([filament_n_bonds(f) + 1 for f in filaments])
+    n_bonds = n_bonds or _library_n_bonds
+    n_sites = np.array([n_bonds(f) + 1 for f in filaments])
     fil = np.repeat(np.arange(len(filaments)), n_sites)
     same = (fil[pairs[:, 0]] == fil[pairs[:, 1]]) & (np.abs(pairs[:, 0] - pairs[:, 1]) <= 1)
     pairs = pairs[~same]
@@ -80,7 +94,7 @@ REPLICAS = {"D": dict(n_dim=2, n_replicas=256, n_fil=(200, 2000), n_seg=16, lp=2
 
 
 def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
-                  interaction=True):
+                  interaction=True, insert=None):
     """Independent systems of workload `name`: returns (system, filaments,
     sites, replicas) for Context(..., replicas=replicas).  System r has
     N_r = round(U{lo..hi} * fil_scale) filaments (at least 2) in a periodic
@@ -92,6 +106,7 @@ def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
     lo, hi = w["n_fil"]
     counts = np.maximum(2, np.round(rng.integers(lo, hi + 1, nrep) * fil_scale)).astype(int)
     fil_area = w["n_seg"] + math.pi / 4
+    insert = insert or _library_insert
     filaments, blocks, replicas = [], [], []
     for r in range(nrep):
         n = int(counts[r])
@@ -100,8 +115,8 @@ def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
         lengths = n_seg.astype(np.float64)
         lp = np.full(n, w["lp"])
         rseed = seed * 1000 + r
-        blocks.append(insert_filaments(w["n_dim"], 0.5 * side, rseed, n_seg, lengths, lp,
-                                       diameter=DIAMETER))
+        blocks.append(insert(w["n_dim"], 0.5 * side, rseed, n_seg, lengths, lp,
+                             diameter=DIAMETER))
         filaments += [dict(length=float(lengths[i]), persistence_length=float(lp[i]),
                            diameter=DIAMETER, min_bond_length=MIN_BOND_LENGTH,
                            friction_ratio=FRICTION_RATIO) for i in range(n)]
@@ -113,13 +128,14 @@ def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
     return system, filaments, np.concatenate(blocks), replicas
 
 
-def split_replicas(system, filaments, sites, replicas):
+def split_replicas(system, filaments, sites, replicas, n_bonds=None):
     """Per-system (system, filaments, sites) triples of a replica batch, each
     as a stand-alone configuration."""
+    n_bonds = n_bonds or _library_n_bonds
     out, f0, s0 = [], 0, 0
     for rep in replicas:
         fils = filaments[f0:f0 + rep["n_filaments"]]
-        ns = sum(filament_n_bonds(f) + 1 for f in fils)
+        ns = sum(n_bonds(f) + 1 for f in fils)
         out.append((dict(system, system_radius=rep["system_radius"], seed=rep["seed"]), fils,
                     sites[s0:s0 + ns]))
         f0 += rep["n_filaments"]
@@ -133,7 +149,7 @@ def describe(name):
 
 
 def make(name, scale=1.0, seed=0, precision_seed=None, stoch=True, interaction=True,
-         n_seg=None, side=None):
+         n_seg=None, side=None, insert=None):
     """Returns (system, filaments, sites) for workload `name`.  For small test
     systems that full-length filaments would not fit: n_seg replaces the
     bonds per filament, side the box side (lower density)."""
@@ -155,8 +171,9 @@ def make(name, scale=1.0, seed=0, precision_seed=None, stoch=True, interaction=T
     else:
         lp = np.full(n_fil, w["lp"])
     lengths = n_seg.astype(np.float64)  # bond length 1
-    sites = insert_filaments(w["n_dim"], 0.5 * side, seed, n_seg, lengths, lp,
-                             diameter=DIAMETER, insertion=w.get("insertion", "random"))
+    insert = insert or _library_insert
+    sites = insert(w["n_dim"], 0.5 * side, seed, n_seg, lengths, lp,
+                   diameter=DIAMETER, insertion=w.get("insertion", "random"))
     system = dict(n_dim=w["n_dim"], system_radius=0.5 * side, delta=w["delta"],
                   wca_eps=1.0, wca_sig=1.0, f_cutoff=2000.0,
                   stoch_flag=1 if stoch else 0, interaction_flag=1 if interaction else 0,

@@ -270,3 +270,63 @@ class Reference(_Checker):
         polar, nem = np.zeros(3), np.zeros(9)
         self._call("global_order", _ptr(polar), _ptr(nem))
         return polar, nem.reshape(3, 3)
+
+
+# ---- inputs without the CUDA library -----------------------------------------
+
+INSERTION = {"random": 0, "random_nematic": 1, "random_polar": 2}
+
+
+def oracle_n_bonds(params):
+    """Bond count of a filament by the oracle's restatement of the
+    reference's rule (src/filament.cpp:142-147)."""
+    lib = ctypes.CDLL(ORACLE_SO)
+    lib.sco_filament_n_bonds.restype = ctypes.c_int
+    return lib.sco_filament_n_bonds(ctypes.byref(FilamentDesc(**params)))
+
+
+def oracle_insert(n_dim, system_radius, seed, n_bonds, lengths, persistence_lengths,
+                  diameter=1.0, max_attempts=10000, insertion="random"):
+    """The oracle's random insertion with overlap rejection; same arguments
+    and result as simcore_b200.insert_filaments (and the same configuration
+    for the same seed)."""
+    lib = ctypes.CDLL(ORACLE_SO)
+    lib.sco_insert_filaments.restype = ctypes.c_int
+    n_bonds = np.ascontiguousarray(n_bonds, dtype=np.int32)
+    lengths = np.ascontiguousarray(lengths, dtype=np.float64)
+    lps = np.ascontiguousarray(persistence_lengths, dtype=np.float64)
+    xyz = np.zeros((int(np.sum(n_bonds + 1)), 3))
+    rc = lib.sco_insert_filaments(ctypes.c_int(n_dim), ctypes.c_double(system_radius),
+                                  ctypes.c_uint64(seed), ctypes.c_int(len(n_bonds)),
+                                  _ptr(n_bonds), _ptr(lengths), _ptr(lps),
+                                  ctypes.c_double(diameter),
+                                  ctypes.c_int(INSERTION[insertion]),
+                                  ctypes.c_int(max_attempts), _ptr(xyz))
+    if rc != 0:
+        raise RuntimeError("oracle insertion failed (%d)" % rc)
+    return xyz
+
+
+def workloads_module():
+    """simcore_b200/workloads.py loaded on its own (numpy only), without the
+    package and so without the CUDA library."""
+    import importlib.util
+    path = os.path.join(ROOT, "simcore_b200", "workloads.py")
+    spec = importlib.util.spec_from_file_location("sc_workload_defs", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_workload(name, seed=0, scale=1.0):
+    """(system, filaments, sites, replicas, crosslinks) of a bench workload,
+    made by the oracle's insertion and bond-count rule: the configuration
+    the library's own insertion makes, without loading the library."""
+    wl = workloads_module()
+    if name in wl.REPLICAS:
+        system, fils, sites, reps = wl.make_replicas(name, seed=seed, insert=oracle_insert)
+        return system, fils, sites, reps, None
+    system, fils, sites = wl.make(name, scale, seed=seed, insert=oracle_insert)
+    xl = wl.crosslinks(name, sites, fils, 2 * system["system_radius"], scale=scale, seed=seed,
+                       n_bonds=oracle_n_bonds)
+    return system, fils, sites, None, xl

@@ -13,19 +13,39 @@ from checkers import Reference
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
+# Runs the reference arm in-process and then reports whether anything of
+# the CUDA library was loaded (module or shared object).
+_RUN_REFERENCE_ARM = """
+import sys
+sys.argv = ["bench.py", "--impl", "reference", "--workload", "A", "--steps", "1",
+            "--warmup", "3"]
+sys.path.insert(0, %r)
+import bench
+bench.main()
+maps = open("/proc/self/maps").read()
+print("LOADED", int("simcore_b200" in sys.modules), int("libsimcore_b200" in maps))
+"""
+
+
 @pytest.mark.skipif(not Reference.available(), reason="reference build not present")
 def test_reference_arm_prints_one_contract_line():
-    out = subprocess.run(
-        [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
-         "--workload", "A", "--steps", "1", "--warmup", "3"],
-        cwd=ROOT, capture_output=True, text=True, timeout=600)
+    """One JSON line in the contract's shape, with the GPU arm's `config`,
+    and the CUDA library neither imported nor mapped: the arm's inputs come
+    from the oracle's insertion."""
+    out = subprocess.run([sys.executable, "-c", _RUN_REFERENCE_ARM % ROOT],
+                         cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.strip()]
+    assert lines[-1] == "LOADED 0 0", lines[-1]
+    lines = lines[:-1]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference"
     assert d["unit"] == "segment-steps/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.workload_config("A")
     assert d["config"]["workload"].startswith("A:")
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["sample"]

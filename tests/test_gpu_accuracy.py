@@ -1,0 +1,98 @@
+"""Mixed precision against FP64, output by output, along trajectories.
+
+Every output of the mixed path -- bond forces and torques, site forces,
+tensions and the displacement of one step with shared noise -- stays within
+1e-5 (max |mixed - fp64| / max |fp64|) of the FP64 path on the same state,
+with the default settings (nearly parallel pairs evaluated from the FP64
+sites).  The states are snapshots of mixed-precision trajectories, where
+close and nearly parallel contacts form: a dense isotropic suspension, a
+nematic one of uneven lengths (nearly parallel pairs everywhere), a batch of
+independent 2D systems, and a tethered network of buckling filaments.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BOUND = 1e-5
+
+
+def _trajectory_errors(system, fils, sites, replicas=None, crosslinks=None, n_snap=4,
+                       every=40):
+    import simcore_b200 as sc
+    from simcore_b200.accuracy import mixed_errors, max_errors
+    ctx = sc.Context(system, fils, sites, precision="mixed", replicas=replicas)
+    if crosslinks is not None:
+        a, b, k, rest = crosslinks
+        ctx.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+    errs = [mixed_errors(system, fils, sites, replicas, crosslinks)]
+    for _ in range(n_snap):
+        ctx.step_graph(every)
+        errs.append(mixed_errors(system, fils, ctx.sites(), replicas, crosslinks))
+    ctx.close()
+    return max_errors(errs), errs
+
+
+def _check(errs):
+    worst, _ = errs
+    for name, e in worst.items():
+        assert e <= BOUND, (name, e, worst)
+
+
+def test_mixed_errors_isotropic_suspension():
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("B", 0.05, seed=21)
+    _check(_trajectory_errors(system, fils, sites))
+
+
+def test_mixed_errors_nematic_uneven_lengths():
+    """Nematic insertion starts every filament exactly parallel (both
+    precisions take the parallel branch); the noise then turns them by small
+    angles, which is where FP32 orientations cannot resolve closest points."""
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("C", 0.004, seed=22)
+    _check(_trajectory_errors(system, fils, sites, every=60))
+
+
+def test_mixed_errors_replica_batch():
+    from simcore_b200 import workloads
+    system, fils, sites, reps = workloads.make_replicas("D", n_replicas=4, fil_scale=0.2,
+                                                        seed=23)
+    _check(_trajectory_errors(system, fils, sites, replicas=reps))
+
+
+def test_mixed_errors_tethered_network():
+    from simcore_b200 import workloads
+    system, fils, sites = workloads.make("E", 0.02, seed=24)
+    xl = workloads.crosslinks("E", sites, fils, 2 * system["system_radius"], scale=0.02,
+                              seed=24)
+    _check(_trajectory_errors(system, fils, sites, crosslinks=xl, every=30))
+
+
+def test_near_parallel_pairs_off_is_the_fp32_evaluation():
+    """The default mixed path evaluates a pair at 1.7e-4 rad from the FP64
+    sites (within the bound of the FP64 torques); with that evaluation
+    switched off the pair is evaluated in FP32, from orientations that
+    cannot resolve its closest points, and the torques change."""
+    import simcore_b200 as sc
+    angle = 1.7e-4
+    j = np.arange(11.0)
+    sites = np.zeros((22, 3))
+    sites[:11, 0] = j - 5.0
+    sites[11:, 0] = -4.7 + j * np.cos(angle)
+    sites[11:, 2] = 1.05 + j * np.sin(angle)
+    system = dict(n_dim=3, system_radius=20.0, delta=1e-4, seed=1, stoch_flag=0)
+    fils = [dict(length=10.0, persistence_length=100.0, diameter=1.0, min_bond_length=0.666,
+                 friction_ratio=2.0)] * 2
+    out = {}
+    for mode in ("fp64", "mixed", "mixed_off"):
+        c = sc.Context(system, fils, sites, precision="fp64" if mode == "fp64" else "mixed")
+        if mode == "mixed_off":
+            c.set_exact_near_parallel(False)
+        c.interact()
+        out[mode] = c.bond_forces()
+        c.close()
+    t64 = out["fp64"][1]
+    scale = max(np.abs(t64).max(), np.abs(out["fp64"][0]).max())
+    assert np.abs(out["mixed"][1] - t64).max() <= BOUND * scale
+    assert not np.array_equal(out["mixed_off"][1], out["mixed"][1])

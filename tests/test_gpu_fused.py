@@ -21,8 +21,12 @@ def _split(ctx, n):
 
 
 def _pair(case):
-    """Two contexts of one mixed-precision workload, the first fused."""
+    """Two contexts of one mixed-precision workload, the first fused.  The
+    fusion evaluates every pair in FP32, so both contexts run with the FP64
+    evaluation of nearly parallel pairs (on by default) switched off."""
     a, b = _contexts(case)
+    for c in (a, b):
+        c.set_exact_near_parallel(False)
     a.set_fused_pairs(True)
     return a, b
 

@@ -139,10 +139,10 @@ def test_mixed_near_parallel_pairs(angle):
     """Two straight rods side by side 1.05 apart (inside the WCA range),
     overlapping, at a small angle.  Within about 0.2 degrees of parallel,
     FP32's 1 - c^2 is rounding alone and the closest points it finds can be
-    far off; with exact near-parallel pairs on, the mixed pair stage
-    evaluates those pairs from the FP64 sites (exactly parallel rods and
-    wider angles stay in FP32).  Forces and torques then match the FP64 path
-    to 1e-5 of the largest at every angle."""
+    far off; the default mixed pair stage evaluates those pairs from the
+    FP64 sites (exactly parallel rods and wider angles stay in FP32).
+    Forces and torques then match the FP64 path to 1e-5 of the largest at
+    every angle."""
     R = 20.0
     j = np.arange(11.0)
     sites = np.zeros((22, 3))
@@ -154,7 +154,6 @@ def test_mixed_near_parallel_pairs(angle):
                  friction_ratio=2.0)] * 2
     c64 = _ctx(system, fils, sites, "fp64")
     c32 = _ctx(system, fils, sites, "mixed")
-    c32.set_exact_near_parallel(True)
     assert len(c64.pairs()) > 0
     for c in (c64, c32):
         c.interact()
@@ -166,14 +165,12 @@ def test_mixed_near_parallel_pairs(angle):
 
 
 def test_exact_near_parallel_graph_matches_host():
-    """With exact near-parallel pairs on, the captured graph (which captures
-    the second kernel too) gives the host-driven loop's bits, on a batch of
-    independent 2D systems."""
+    """The captured graph, whose pair kernels evaluate nearly parallel pairs
+    from the FP64 sites in their last block, gives the host-driven loop's
+    bits, on a batch of independent 2D systems."""
     system, fils, sites, reps = _replica_batch(3, 0.05, seed=4)
     a = _ctx_replicas(system, fils, sites, reps, "mixed")
     b = _ctx_replicas(system, fils, sites, reps, "mixed")
-    for c in (a, b):
-        c.set_exact_near_parallel(True)
     a.step_graph(40)
     b.step(40)
     assert_same(a.sites(), b.sites(), "sites")

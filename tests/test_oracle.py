@@ -353,3 +353,28 @@ def test_ideal_pressure_without_contacts():
     assert np.array_equal(p, np.full(2, (ideal + ideal + ideal) / 3))
     assert not o.potential_energy().any()
     o.close()
+
+
+@pytest.mark.parametrize("name,scale", [("A", 1.0), ("B", 0.05), ("C", 0.004), ("E", 0.02)])
+def test_oracle_insertion_is_the_library_insertion(name, scale):
+    """The oracle's insertion (restated from the reference's distributions,
+    the shared Philox insertion stream and the longest-first order) gives
+    the library's host insertion bit for bit, so a CPU run of the reference's
+    code can start from the GPU run's configuration without loading the CUDA
+    library."""
+    import simcore_b200  # noqa: F401  (host insertion; no device needed)
+    from simcore_b200 import workloads
+    from checkers import oracle_insert, workloads_module
+    lib_sites = workloads.make(name, scale, seed=3)[2]
+    orc_sites = workloads_module().make(name, scale, seed=3, insert=oracle_insert)[2]
+    assert np.array_equal(lib_sites, orc_sites)
+
+
+def test_oracle_insertion_of_replica_batches():
+    from simcore_b200 import workloads
+    from checkers import oracle_insert, workloads_module
+    a = workloads.make_replicas("D", n_replicas=3, fil_scale=0.2, seed=5)
+    b = workloads_module().make_replicas("D", n_replicas=3, fil_scale=0.2, seed=5,
+                                         insert=oracle_insert)
+    assert np.array_equal(a[2], b[2])
+    assert a[3] == b[3]
