@@ -15,9 +15,12 @@ L2 is flushed (256 MiB write) before every timed launch.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 N > 1: one process per GPU under torch.distributed.run, each rank an
-independent replica (weak scaling, no data-path collective); the time is the
-max over ranks.  --impl reference times the reference's own CPU code
-(oracle/_ref, OpenMP over all host cores) on the same workload.
+independent replica (weak scaling, no data-path collective); with --workload
+D the 256 independent systems are shared out over the ranks instead (strong
+scaling; per-system counts gathered once at the end).  The time is the max
+over ranks.  --impl reference times the reference's own CPU code
+(oracle/_ref, OpenMP over all host cores) on the same configuration, made by
+the oracle's insertion, without loading the CUDA library.
 """
 import argparse
 import json
@@ -176,6 +179,17 @@ def reduce_max(value, dist):
     dev = "cuda" if backend == "nccl" else "cpu"
     t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(value, dist):
+    """Sum over ranks; dist may be None."""
+    if dist is None:
+        return float(value)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -353,7 +367,21 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
-    wl = load_workload(args.workload, replica_seed(rank))
+    scaling = "weak"
+    shard = None
+    if args.workload == "D" and world > 1:
+        # The 256 independent systems are shared out over the ranks, balanced
+        # by bonds (simcore_b200.sharding); each rank makes and runs only its
+        # share, and the total work is fixed.
+        from simcore_b200 import sharding
+        counts = workloads.replica_counts("D")
+        n_seg = workloads.REPLICAS["D"]["n_seg"]
+        shard = sharding.partition([int(c) * n_seg for c in counts], world)[rank]
+        system, fils, sites, reps = workloads.make_replicas("D", only=shard)
+        wl = (system, fils, sites, reps, None)
+        scaling = "strong"
+    else:
+        wl = load_workload(args.workload, replica_seed(rank))
     system, fils, sites = wl[:3]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -449,18 +477,32 @@ def run_ours(args, rank, world, local_rank):
         host_in, host_out = host_out, host_in
     e2e_total = reduce_max(float(sum(e2e_times)), dist)
 
+    per_system = None
+    if shard is not None:
+        # Per-system rebuild and pair counts of the mixed run, gathered from
+        # every rank in global system order.
+        from simcore_b200 import sharding
+        nr, npr = contexts["mixed"].replica_counters()
+        rows = [(int(a), int(b)) for a, b in zip(nr, npr)]
+        gathered = sharding.gather_by_system(rows, shard, len(workloads.replica_counts("D")),
+                                             dist)
+        per_system = {"systems": len(gathered),
+                      "rebuilds_total": sum(g[0] for g in gathered),
+                      "pairs_total": sum(g[1] for g in gathered),
+                      "systems_per_rank_this_rank": len(shard)}
     for c in contexts.values():
         c.close()
+    r = results["mixed"]
+    r64 = results["fp64"]
+    # Segment-steps of every rank (shares of independent systems differ in
+    # size); the time is the slowest rank's.
+    seg_steps = reduce_sum(r["n_bonds"] * I_STEPS_PER_STEP * args.steps, dist)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return None
-
-    r = results["mixed"]
-    r64 = results["fp64"]
     n_b = r["n_bonds"]
-    seg_steps = n_b * I_STEPS_PER_STEP * args.steps * world
     value = seg_steps / (r["total_ms"] * 1e-3)
     value64 = seg_steps / (r64["total_ms"] * 1e-3)
     peak, peak_kind = load_measured_peaks()
@@ -481,14 +523,17 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair forces + f64 integrator",
+        "scaling": scaling, "vs_baseline": None, "dtype": "f32 pair forces + f64 integrator",
         "data": "synthetic (seeded random insertion with overlap rejection)",
         "config": workload_config(args.workload),
         "run": {"precision": "mixed", "i_steps_per_step": I_STEPS_PER_STEP,
                 "timed_unit": "one CUDA-graph launch of 20 reference steps (WHILE loop of 10 "
                               "midpoint BD steps with device-decided pair-list rebuilds)",
                 "l2": "flushed by a 256 MiB write before every timed step",
-                "parallelism": "replicas" if world > 1 else "single system",
+                "parallelism": ("independent systems shared out over %d ranks" % world
+                                if shard is not None else
+                                "replicas" if world > 1 else "single system"),
+                "per_system": per_system,
                 "pairs": r["n_pairs"], "rebuilds_in_timed_region": r["rebuilds"],
                 "integrator_layout": {p: {"warp_max_sites": w, "block_sites": b}
                                       for p, (w, b) in layouts.items()}},

@@ -93,22 +93,30 @@ REPLICAS = {"D": dict(n_dim=2, n_replicas=256, n_fil=(200, 2000), n_seg=16, lp=2
                       area_fraction=0.1, delta=1e-4, n_steps=500)}
 
 
-def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
-                  interaction=True, insert=None):
-    """Independent systems of workload `name`: returns (system, filaments,
-    sites, replicas) for Context(..., replicas=replicas).  System r has
-    N_r = round(U{lo..hi} * fil_scale) filaments (at least 2) in a periodic
-    square of area N_r (n_seg + pi/4) / area_fraction (the reference's 2D
-    filament area, src/filament.cpp:385-388), noise seed seed * 1000 + r."""
+def replica_counts(name="D", n_replicas=None, fil_scale=1.0, seed=0):
+    """Filament count of every system of make_replicas (same arguments)."""
     w = REPLICAS[name]
     nrep = w["n_replicas"] if n_replicas is None else int(n_replicas)
     rng = np.random.default_rng(seed + 4242)
     lo, hi = w["n_fil"]
-    counts = np.maximum(2, np.round(rng.integers(lo, hi + 1, nrep) * fil_scale)).astype(int)
+    return np.maximum(2, np.round(rng.integers(lo, hi + 1, nrep) * fil_scale)).astype(int)
+
+
+def make_replicas(name="D", n_replicas=None, fil_scale=1.0, seed=0, stoch=True,
+                  interaction=True, insert=None, only=None):
+    """Independent systems of workload `name`: returns (system, filaments,
+    sites, replicas) for Context(..., replicas=replicas).  System r has
+    N_r = round(U{lo..hi} * fil_scale) filaments (at least 2) in a periodic
+    square of area N_r (n_seg + pi/4) / area_fraction (the reference's 2D
+    filament area, src/filament.cpp:385-388), noise seed seed * 1000 + r.
+    only: the indices of the systems to make (each is the same system it is
+    in the whole batch), in that order; default all."""
+    w = REPLICAS[name]
+    counts = replica_counts(name, n_replicas, fil_scale, seed)
     fil_area = w["n_seg"] + math.pi / 4
     insert = insert or _library_insert
     filaments, blocks, replicas = [], [], []
-    for r in range(nrep):
+    for r in (range(len(counts)) if only is None else only):
         n = int(counts[r])
         side = math.sqrt(n * fil_area / w["area_fraction"])
         n_seg = np.full(n, w["n_seg"], dtype=np.int32)
