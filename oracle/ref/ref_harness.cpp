@@ -22,6 +22,13 @@
 //   - FilamentSpecies::UpdatePositions         src/filament_species.cpp:59-85
 //   - Species::GetDrMax / ZeroDrTot / ZeroForces  include/simcore/species.hpp:105-127,198-203
 //   - Simulation::InsertSpecies tail           src/simulation.cpp:399-404
+//   - CrosslinkManager::UpdateCrosslinks -> CrosslinkSpecies::UpdatePositions
+//     for doubly-bound crosslinks that neither unbind nor move
+//                                              src/crosslink_manager.cpp:64-70,
+//                                              src/crosslink_species.cpp:218-258
+// The reference's own Crosslink and Anchor classes (src/crosslink.cpp,
+// src/anchor.cpp, compiled with a stand-in for the absent KMC headers) place
+// the crosslinks and compute and apply every tether force.
 // Insertion itself is replaced by loading a given configuration into each
 // filament (Mesh::GetSite(i)->SetPosition, then UpdateBondPositions and
 // UpdatePrevPositions, src/mesh.cpp:24,324,175), after which every Philox
@@ -59,6 +66,7 @@
 #define private public
 #define protected public
 #include "simcore/cell_list.hpp"
+#include "simcore/crosslink.hpp"
 #include "simcore/filament.hpp"
 #include "simcore/minimum_distance.hpp"
 #include "simcore/potential_manager.hpp"
@@ -121,6 +129,10 @@ struct RefSim {
   int n_thermo = 0;
   std::vector<double> thermo_rec;  // i_step, pressure tensor (9), pressure, volume
   std::unordered_map<const Object *, int> bond_gid;
+  // doubly-bound crosslinks (scref_add_crosslinks)
+  crosslink_parameters xparams;
+  std::vector<Crosslink> xlinks;
+  std::vector<int> site_fil, site_local;  // per global site: filament, index in it
   int n_threads = 0;
   int n_sites_total = 0;
   int n_bonds_total = 0;
@@ -264,9 +276,27 @@ struct RefSim {
           stress[n_dim * i + j] += ix->stress[n_dim * i + j];
     }
   }
+  // CrosslinkManager::UpdateCrosslinks (src/crosslink_manager.cpp:64-70) ->
+  // CrosslinkSpecies::UpdatePositions (src/crosslink_species.cpp:218-238):
+  // on even steps UpdateBoundCrosslinks (forces of every bound crosslink,
+  // applied in member order, then anchor motion and binding, :241-258);
+  // on odd steps the stored anchor forces are applied again.  The crosslinks
+  // are doubly bound with zero unbinding rate, no diffusion and no free
+  // crosslinks in solution, so binding changes nothing.
+  void UpdateCrosslinks() {
+    if (xlinks.empty()) return;
+    if (i_step % 2 == 0) {
+      for (auto &x : xlinks) x.UpdateCrosslinkForces();
+      for (auto &x : xlinks) x.ApplyTetherForces();
+      for (auto &x : xlinks) x.UpdateCrosslinkPositions();
+    } else {
+      for (auto &x : xlinks) x.ApplyTetherForces();
+    }
+  }
   void Interact() {
     if (!params.interaction_flag) return;  // no interactions, no boundaries
     CheckUpdateObjects();
+    UpdateCrosslinks();
     CheckUpdateInteractions();
     CalculatePairInteractions();
     ApplyPairInteractions();
@@ -438,6 +468,11 @@ void *scref_create(const scref_system *sys, int n_fil,
     return nullptr;
   }
   s->n_sites_total = site_cursor;
+  for (int i = 0; i < n_fil; ++i)
+    for (int j = 0; j < s->members[i].n_sites_; ++j) {
+      s->site_fil.push_back(i);
+      s->site_local.push_back(j);
+    }
 
   // Simulation::InsertSpecies tail: half-shell neighbours, then a forced
   // update that bins every bond and zeroes the displacement trackers.
@@ -713,6 +748,58 @@ void scref_get_dr_tot(void *h, double *dr) {
   int c = 0;
   for (auto &f : s->members)
     for (int j = 0; j < f.n_sites_; ++j, ++c) dr[c] = f.GetSite(j)->dr_tot_;
+}
+
+// Doubly-bound crosslinks between global sites site_a[k] and site_b[k],
+// made and attached by the reference's own code: Crosslink::Init with
+// crosslink parameters of zero unbinding rates, no diffusion or walking,
+// end pausing on, the given spring constants and rest length; each anchor
+// AttachObjLambda'd to the bond whose tail is its site (lambda 0), or, for a
+// filament's last site, to the last bond at its head (lambda = its length);
+// then SetDoubly.  Once, before the first step.  Returns 0, or -1 on a bad
+// site index or a repeated call.
+int scref_add_crosslinks(void *h, int n, const int *site_a, const int *site_b, double k_spring,
+                         double k_spring_compress, double rest_length) {
+  RefSim *s = (RefSim *)h;
+  if (!s || n < 0 || !s->xlinks.empty()) return -1;
+  crosslink_parameters &xp = s->xparams;
+  xp.num = n;
+  xp.k_spring = k_spring;
+  xp.k_spring_compress = k_spring_compress;
+  xp.rest_length = rest_length;
+  xp.static_flag = false;
+  xp.k_on_s = xp.k_on_d = 0;
+  xp.k_off_s = xp.k_off_d = 0;
+  xp.diffusion_s = xp.diffusion_d = 0;
+  xp.velocity_s = xp.velocity_d = 0;
+  xp.end_pausing = true;
+  xp.concentration = 0;
+  const int ns = (int)s->site_fil.size();
+  for (int q = 0; q < n; ++q)
+    if (site_a[q] < 0 || site_a[q] >= ns || site_b[q] < 0 || site_b[q] >= ns) return -1;
+  s->xlinks.reserve(n);
+  for (int q = 0; q < n; ++q) {
+    s->xlinks.emplace_back((unsigned long)(1000003u + (unsigned)q));
+    Crosslink &x = s->xlinks.back();
+    x.Init(&xp);
+    const int sites[2] = {site_a[q], site_b[q]};
+    for (int a = 0; a < 2; ++a) {
+      Filament &f = s->members[s->site_fil[sites[a]]];
+      const int j = s->site_local[sites[a]];
+      Bond *b = j < f.n_bonds_ ? f.GetBond(j) : f.GetBond(f.n_bonds_ - 1);
+      const double lambda = j < f.n_bonds_ ? 0.0 : b->GetLength();
+      x.anchors_[a].AttachObjLambda(b, lambda);
+    }
+    x.SetDoubly();
+  }
+  return 0;
+}
+
+// Crosslink::force_ of every crosslink (the tether force on anchor 0).
+void scref_get_crosslink_forces(void *h, double *out) {
+  RefSim *s = (RefSim *)h;
+  for (size_t q = 0; q < s->xlinks.size(); ++q)
+    for (int d = 0; d < 3; ++d) out[3 * q + d] = s->xlinks[q].force_[d];
 }
 
 }  // extern "C"

@@ -60,10 +60,16 @@ struct sco_sim {
   int n_thermo;
   long n_rec, rec_cap;
   double *rec; /* per record: i_step, pressure tensor (9), pressure, volume */
-  /* static crosslinks: anchor 2k+a of link k sits on bond xbond[2k+a], at its
-   * tail (xhead 0, lambda = 0) or head (xhead 1, lambda = bond length) */
+  /* mesh lambdas (Bond::mesh_lambda_, Mesh::true_length_): the summed
+   * current lengths of the bonds before each bond, and of a filament's
+   * bonds; the nominal length of each filament (Mesh::length_) */
+  double *bml, *ftl, *fL;
+  /* doubly-bound crosslinks: anchor 2k+a of link k is bound at mesh lambda
+   * xM[2k+a] of filament xfil[2k+a] and sits on bond xbond[2k+a] (set again
+   * from xM at every recomputation) */
   int nx;
-  int *xbond, *xhead;
+  int *xbond, *xfil, xerr;
+  double *xM;
   double xk, xkc, xrest;
   double *xc; /* 6 per anchor: the anchor's force_ and torque_ */
   double *xF; /* 3 per link: Crosslink::force_ */
@@ -173,7 +179,13 @@ static void bond_reinit(sco_sim *s, int b, int site1) {
 static void update_bond_positions(sco_sim *s, int f) {
   int s0 = s->fs_off[f], b0 = s->fb_off[f];
   int nbf = s->fb_off[f + 1] - b0, i, d;
-  for (i = 0; i < nbf; ++i) bond_reinit(s, b0 + i, s0 + i);
+  double true_length = 0;
+  for (i = 0; i < nbf; ++i) {
+    bond_reinit(s, b0 + i, s0 + i);
+    s->bml[b0 + i] = true_length;  /* Bond::SetMeshLambda (src/mesh.cpp:324-330) */
+    true_length += s->bl[b0 + i];
+  }
+  s->ftl[f] = true_length;
   for (i = 0; i < nbf; ++i)
     for (d = 0; d < s->n_dim; ++d) V3(s->u, s0 + i)[d] = V3(s->bu, b0 + i)[d];
   for (d = 0; d < s->n_dim; ++d)
@@ -534,28 +546,55 @@ static double get_dr_max(sco_sim *s) {
 
 /* ---- static crosslinks (config E) ----------------------------------------- */
 
-/* Anchor::UpdateAnchorPositionToBond (src/anchor.cpp:236-249) on a bond
- * re-initialised from its sites, then Object::UpdatePeriodic: the anchor's
- * scaled position, bond orientation, bond length and lambda. */
-static void anchor_state(const sco_sim *s, int anchor, double *sp, double *u,
-                         double *len, double *lambda) {
-  const int b = s->xbond[anchor];
-  const int site1 = b + filament_of_bond(s, b);
-  const double *r1 = V3(s->r, site1), *r2 = V3(s->r, site1 + 1);
-  double pos[3] = {0, 0, 0}, ap[3] = {0, 0, 0}, l = 0;
-  int i, n = s->n_dim;
-  for (i = 0; i < n; ++i) {
-    u[i] = r2[i] - r1[i];
-    l += u[i] * u[i];
+/* Anchor::UpdateAnchorPositionToMesh (src/anchor.cpp:45-68) of a bound,
+ * non-static anchor with end pausing: Anchor::CheckMesh (:180-201) clamps its
+ * mesh lambda to [0, true length]; Mesh::GetBondAtLambda (src/mesh.cpp:
+ * 667-675) picks a bond from the nominal bond length; Anchor::CalcBondLambda
+ * (:70-111) measures the lambda from that bond's mesh lambda and moves once
+ * to a neighbouring bond when it falls outside; Anchor::
+ * UpdateAnchorPositionToBond (:236-249) and Object::UpdatePeriodic place it.
+ * Returns the anchor's scaled position, orientation, bond length and lambda;
+ * its bond is recorded in xbond. */
+static void anchor_state(sco_sim *s, int anchor, double *sp, double *u, double *len,
+                         double *lambda) {
+  const int f = s->xfil[anchor], b0 = s->fb_off[f], nbf = s->fb_off[f + 1] - b0;
+  double M = s->xM[anchor], ap[3] = {0, 0, 0}, bl, lam;
+  int k, i, n = s->n_dim;
+  if (M < 0) M = 0;
+  else if (M > s->ftl[f]) M = s->ftl[f];
+  s->xM[anchor] = M;
+  if (M < 0) k = 0;
+  else if (M >= s->fL[f]) k = nbf - 1;
+  else k = (int)floor(M / s->fl[f]);
+  /* M / l can round up to the bond count just below the nominal length,
+   * where the reference would index past its bonds: kept on the last. */
+  if (k > nbf - 1) k = nbf - 1;
+  if (k < 0) k = 0;
+  lam = M - s->bml[b0 + k];
+  bl = s->bl[b0 + k];
+  if (lam < 0) {
+    if (k > 0) {
+      --k;
+      lam = M - s->bml[b0 + k];
+      bl = s->bl[b0 + k];
+    } else {
+      lam = 0;
+    }
+  } else if (lam > bl) {
+    if (k < nbf - 1) {
+      ++k;
+      lam = M - s->bml[b0 + k];
+      bl = s->bl[b0 + k];
+    } else {
+      lam = bl;
+    }
   }
-  l = sqrt(l);
-  for (i = 0; i < n; ++i) {
-    pos[i] = r1[i] + 0.5 * u[i];
-    u[i] /= l;
-  }
-  *len = l;
-  *lambda = s->xhead[anchor] ? l : 0.0;
-  for (i = 0; i < n; ++i) ap[i] = pos[i] - (0.5 * l - *lambda) * u[i];
+  if (lam < -1e-6 || lam > bl + 1e-6) s->xerr = 1; /* the reference stops here */
+  s->xbond[anchor] = b0 + k;
+  for (i = 0; i < 3; ++i) u[i] = V3(s->bu, b0 + k)[i];
+  for (i = 0; i < n; ++i) ap[i] = V3(s->bp, b0 + k)[i] - (0.5 * bl - lam) * u[i];
+  *len = bl;
+  *lambda = lam;
   periodic_bc(n, s->hinv, ap, sp);
 }
 
@@ -1058,6 +1097,7 @@ sco_sim *sco_create(const sco_system *sys, int n_fil, const sco_filament *fils,
   ALLOCD(s->dz, 3 * n_sites); ALLOCD(s->dt, n_sites);
   ALLOCD(s->bp, 3 * s->nb); ALLOCD(s->bs, 3 * s->nb); ALLOCD(s->bu, 3 * s->nb);
   ALLOCD(s->bl, s->nb); ALLOCD(s->bF, 3 * s->nb); ALLOCD(s->bT, 3 * s->nb);
+  ALLOCD(s->bml, s->nb); ALLOCD(s->ftl, n_fil); ALLOCD(s->fL, n_fil);
   ALLOCD(s->tens, s->nb); ALLOCD(s->bpote, s->nb);
   ALLOCD(s->w_cos, max_ns); ALLOCD(s->w_gl, max_ns); ALLOCD(s->w_gd, max_ns);
   ALLOCD(s->w_gu, max_ns); ALLOCD(s->w_dt, max_ns + 1); ALLOCD(s->w_db, max_ns + 1);
@@ -1074,6 +1114,7 @@ sco_sim *sco_create(const sco_system *sys, int n_fil, const sco_filament *fils,
     if (length > max_length) length = max_length;
     else if (length < min_length) length = min_length;
     s->fl[f] = length / nb; /* bond_length_ = length_ / n_bonds_ */
+    s->fL[f] = length;      /* length_ */
     s->flp[f] = fils[f].persistence_length;
     s->fd[f] = fils[f].diameter;
     /* Filament::SetDiffusion (src/filament.cpp:320-348) */
@@ -1115,7 +1156,8 @@ void sco_destroy(sco_sim *s) {
   free(s->r); free(s->rp); free(s->fr); free(s->F); free(s->tn); free(s->u);
   free(s->dz); free(s->dt); free(s->bp); free(s->bs); free(s->bu); free(s->bl);
   free(s->bF); free(s->bT); free(s->tens);
-  free(s->xbond); free(s->xhead); free(s->xc); free(s->xF);
+  free(s->xbond); free(s->xfil); free(s->xM); free(s->xc); free(s->xF);
+  free(s->bml); free(s->ftl); free(s->fL);
   free(s->pa); free(s->pb); free(s->pf); free(s->pdr); free(s->ppote);
   free(s->bpote); free(s->rec);
   free(s->w_cos); free(s->w_gl); free(s->w_gd); free(s->w_gu); free(s->w_dt);
@@ -1233,22 +1275,31 @@ int sco_add_crosslinks(sco_sim *s, int n, const int *site_a, const int *site_b,
   int k, a;
   if (s->nx || n <= 0) return -1;
   s->xbond = (int *)xcalloc(2 * (size_t)n, sizeof(int));
-  s->xhead = (int *)xcalloc(2 * (size_t)n, sizeof(int));
+  s->xfil = (int *)xcalloc(2 * (size_t)n, sizeof(int));
+  s->xM = (double *)xcalloc(2 * (size_t)n, sizeof(double));
   s->xc = (double *)xcalloc(12 * (size_t)n, sizeof(double));
   s->xF = (double *)xcalloc(3 * (size_t)n, sizeof(double));
+  /* Anchor::AttachObjLambda (src/anchor.cpp:284-316): on the bond whose tail
+   * is the site at lambda 0, or for a filament's last site on its last bond
+   * at lambda = that bond's length; the anchor's mesh lambda is the bond's
+   * plus lambda. */
   for (k = 0; k < n; ++k)
     for (a = 0; a < 2; ++a) {
       const int site = a == 0 ? site_a[k] : site_b[k];
-      int f = 0;
+      int f = 0, b;
+      double lambda;
       if (site < 0 || site >= s->ns) return -1;
       while (s->fs_off[f + 1] <= site) ++f;
       if (site - s->fs_off[f] < s->fb_off[f + 1] - s->fb_off[f]) {
-        s->xbond[2 * k + a] = site - f; /* bond j of site j: its tail */
-        s->xhead[2 * k + a] = 0;
+        b = site - f;
+        lambda = 0.0;
       } else {
-        s->xbond[2 * k + a] = site - f - 1; /* last site: head of the last bond */
-        s->xhead[2 * k + a] = 1;
+        b = site - f - 1;
+        lambda = s->bl[b];
       }
+      s->xbond[2 * k + a] = b;
+      s->xfil[2 * k + a] = f;
+      s->xM[2 * k + a] = s->bml[b] + lambda;
     }
   s->nx = n;
   s->xk = k_spring;

@@ -216,6 +216,8 @@ sc_status check_status(sc_ctx *c) {
   if (s & sc::ST_NAN) return fail(c, SC_ERR_NAN, "non-finite position or displacement");
   if (s & sc::ST_BAD_CELL) return fail(c, SC_ERR_NAN, "bond outside the cell grid (non-finite position)");
   if (s & sc::ST_LIST_OVERFLOW) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow");
+  if (s & sc::ST_TETHER)
+    return fail(c, SC_ERR_UNPHYSICAL, "a crosslink anchor moved off the bonds around its site");
   return SC_OK;
 }
 
@@ -1389,7 +1391,7 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
       const long long per_bd =
           c->desc.interaction_flag
-              ? 2 + (c->d.nx ? 1 : 0) +
+              ? 2 + (c->d.nx ? 2 : 0) +
                     2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0))
               : 1 + 2 * int_l;
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
@@ -1717,6 +1719,7 @@ std::vector<Region> state_regions(sc_ctx *c, long long pcap = -1) {
   if (d.nx) {
     v.push_back({d.xl_c, sizeof(double) * 16 * (size_t)d.nx});
     v.push_back({d.xl_F, sizeof(double) * 4 * (size_t)d.nx});
+    v.push_back({d.xl_M, sizeof(double) * 2 * (size_t)d.nx});
   }
   if (c->k.thermo) {  // pair virial records and the running virial sums
     if (c->prec == 0) v.push_back({d.pv64, sizeof(double) * 4 * P});
@@ -2089,9 +2092,31 @@ sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32
   if (!(k_spring >= 0) || !(rest_length >= 0))
     return fail(c, SC_ERR_INVALID_ARG, "bad spring constants");
   CK(cudaSetDevice(c->desc.device));
-  // Anchor on site j of a filament: tail of bond j; on the last site: head of
-  // the last bond (lambda = bond length, as an end-paused anchor).
-  std::vector<int> anchor(2 * (size_t)n);
+  // Anchor::AttachObjLambda (src/anchor.cpp:284-316): an anchor on site j of
+  // a filament is bound to bond j at lambda 0, one on the last site to the
+  // last bond at lambda = its length; its mesh lambda is the bond's (the
+  // summed lengths of the bonds before it, Mesh::UpdateBondPositions,
+  // src/mesh.cpp:324-330) plus lambda.  The lengths are Bond::ReInit's, from
+  // the loaded sites.
+  std::vector<double> xyz(3 * (size_t)c->ns);
+  CKS(copy_soa3(c, c->d.r, c->ns, xyz.data()));
+  std::vector<double> blen(c->nb), bml(c->nb);
+  for (int f = 0; f < c->nf; ++f) {
+    double true_length = 0.0;
+    for (int s0 = c->site_off[f]; s0 < c->site_off[f + 1] - 1; ++s0) {
+      double l = 0.0;
+      for (int i = 0; i < c->nd; ++i) {
+        const double u = xyz[3 * (size_t)(s0 + 1) + i] - xyz[3 * (size_t)s0 + i];
+        l += u * u;
+      }
+      const int b = s0 - f;
+      blen[b] = std::sqrt(l);
+      bml[b] = true_length;
+      true_length += blen[b];
+    }
+  }
+  std::vector<int> bond(2 * (size_t)n), xfil(2 * (size_t)n);
+  std::vector<double> xM(2 * (size_t)n);
   for (int x = 0; x < n; ++x)
     for (int a = 0; a < 2; ++a) {
       const int site = a == 0 ? site_a[x] : site_b[x];
@@ -2100,35 +2125,54 @@ sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32
       const int f = (int)(std::upper_bound(c->site_off.begin(), c->site_off.end(), site) -
                           c->site_off.begin()) - 1;
       const bool last = site == c->site_off[f + 1] - 1;
-      const int bond = last ? site - f - 1 : site - f;
-      anchor[2 * (size_t)x + a] = bond << 1 | (last ? 1 : 0);
-      if (a == 1 && c->fil_rep[f] != c->fil_rep[(int)(std::upper_bound(c->site_off.begin(),
-                                                                        c->site_off.end(),
-                                                                        site_a[x]) -
-                                                       c->site_off.begin()) - 1])
+      const int b = last ? site - f - 1 : site - f;
+      const size_t A = 2 * (size_t)x + a;
+      bond[A] = b;
+      xfil[A] = f;
+      xM[A] = bml[b] + (last ? blen[b] : 0.0);
+      if (a == 1 && c->fil_rep[f] != c->fil_rep[xfil[A - 1]])
         return fail(c, SC_ERR_INVALID_ARG, "crosslink %d joins two systems", x);
     }
-  // Per-bond anchor lists, ascending anchor id (link order, anchor 0 first).
-  std::vector<int> off(c->nb + 1, 0), ent(2 * (size_t)n);
-  for (int e = 0; e < 2 * n; ++e) off[(anchor[e] >> 1) + 1]++;
+  // Per-bond anchor lists, ascending anchor id (link order, anchor 0 first):
+  // each anchor on its bond and that bond's neighbours in the filament, the
+  // bonds it can move to as the filament's bonds stretch.
+  auto first_bond = [&](int f) { return c->site_off[f] - f; };
+  auto last_bond = [&](int f) { return c->site_off[f + 1] - f - 2; };
+  std::vector<int> off(c->nb + 1, 0), ent;
+  for (int A = 0; A < 2 * n; ++A)
+    for (int b = std::max(bond[A] - 1, first_bond(xfil[A]));
+         b <= std::min(bond[A] + 1, last_bond(xfil[A])); ++b)
+      off[b + 1]++;
   for (int b = 0; b < c->nb; ++b) off[b + 1] += off[b];
+  ent.resize(off[c->nb]);
   {
     std::vector<int> fill(off.begin(), off.end() - 1);
-    for (int e = 0; e < 2 * n; ++e) ent[fill[anchor[e] >> 1]++] = e;
+    for (int A = 0; A < 2 * n; ++A)
+      for (int b = std::max(bond[A] - 1, first_bond(xfil[A]));
+           b <= std::min(bond[A] + 1, last_bond(xfil[A])); ++b)
+        ent[fill[b]++] = A;
   }
-  auto up = [&](int **dst, const std::vector<int> &v) -> sc_status {
-    int *q = nullptr;
+  auto up = [&](auto **dst, const auto &v) -> sc_status {
+    using T = typename std::remove_reference<decltype(v)>::type::value_type;
+    T *q = nullptr;
     CKS(dalloc(c, &q, v.size()));
-    CK(cudaMemcpyAsync(q, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(q, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->st));
     *dst = q;
     return SC_OK;
   };
-  int *q = nullptr;
-  CKS(up(&q, anchor)); c->d.xl_anchor = q;
-  CKS(up(&q, off)); c->d.xb_off = q;
-  CKS(up(&q, ent)); c->d.xb_ent = q;
-  CKS(dalloc(c, &c->d.xl_c, 16 * (size_t)n));
-  CK(cudaMemsetAsync(c->d.xl_c, 0, sizeof(double) * 16 * (size_t)n, c->st));
+  int *qi = nullptr;
+  double *qd = nullptr;
+  CKS(up(&qi, xfil)); c->d.xl_fil = qi;
+  CKS(up(&qi, off)); c->d.xb_off = qi;
+  CKS(up(&qi, ent)); c->d.xb_ent = qi;
+  CKS(up(&qd, xM)); c->d.xl_M = qd;
+  CKS(up(&qd, c->fil_len)); c->d.fil_L = qd;
+  CKS(dalloc(c, &c->d.bml, (size_t)c->nb));
+  CKS(dalloc(c, &c->d.ftl, (size_t)c->nf));
+  // Anchor records: zero force and torque on the attach bond.
+  std::vector<double> rec(16 * (size_t)n, 0.0);
+  for (int A = 0; A < 2 * n; ++A) rec[8 * (size_t)A + 6] = (double)bond[A];
+  CKS(up(&qd, rec)); c->d.xl_c = qd;
   CKS(dalloc(c, &c->d.xl_F, 4 * (size_t)n));
   CK(cudaMemsetAsync(c->d.xl_F, 0, sizeof(double) * 4 * (size_t)n, c->st));
   CK(cudaStreamSynchronize(c->st));

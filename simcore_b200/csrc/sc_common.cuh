@@ -29,7 +29,8 @@ enum : unsigned {
   ST_LIST_OVERFLOW = 2u,  // pair list did not fit
   ST_UNPHYSICAL = 4u,     // accumulated displacement above 10000
   ST_BAD_CELL = 8u,       // cell index out of range (non-finite position)
-  ST_BAD_INPUT = 16u      // caller's device data out of range (site offsets)
+  ST_BAD_INPUT = 16u,     // caller's device data out of range (site offsets)
+  ST_TETHER = 32u         // a crosslink anchor left the bonds it can sit on
 };
 
 // Bond geometry for the FP64 pair stage: the reference's Bond state after
@@ -165,11 +166,17 @@ struct DevState {
   int th_cap, th_gx, th_n;
   // static crosslinks (harmonic tethers between two bonds)
   int nx;                  // links
-  const int *xl_anchor;    // 2 per link: bond << 1 | head (anchor at the bond's head)
-  double *xl_c;            // 8 per anchor: force (3), torque (3), pad (2)
+  const int *xl_fil;       // 2 per link: filament of each anchor
+  double *xl_M;            // 2 per link: mesh lambda of each anchor (Anchor::mesh_lambda_)
+  double *xl_c;            // 8 per anchor: force (3), torque (3), its bond, pad
   double *xl_F;            // 4 per link: tether force (Crosslink::force_), pad
   const int *xb_off;       // nb+1 CSR of anchors per bond
-  const int *xb_ent;       // anchor ids (2 link + a), ascending per bond
+  const int *xb_ent;       // anchor ids (2 link + a), ascending per bond: an anchor is
+                           // listed on the bond it was attached to and on both of its
+                           // neighbours, and counts on the one it sits on
+  double *bml;             // nb: mesh lambda of every bond (Bond::mesh_lambda_)
+  double *ftl;             // nf: summed current bond lengths (Mesh::true_length_)
+  const double *fil_L;     // nf: nominal filament length (Mesh::length_)
   // capture (optional)
   double *cap_F[3];
   double *cap_T;

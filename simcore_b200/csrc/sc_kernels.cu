@@ -778,51 +778,144 @@ __global__ void k_bond_sum(DevState d) {
 // PointPoint (src/minimum_distance.cpp:71-101); each anchor's force and its
 // torque (lambda - l/2) u x f are stored as Anchor::ApplyAnchorForces
 // (src/anchor.cpp:132-146) computes them, for re-use on the odd step.
+// Mesh::UpdateBondPositions' mesh lambdas (src/mesh.cpp:324-330): one thread
+// per filament sums its bonds' current lengths in order, each bond taking
+// the sum before it, and records the total (Mesh::true_length_).  The
+// lengths are Bond::ReInit's (src/bond.cpp:22-37), from the sites.
+template <int ND>
+__global__ void k_mesh_lambda(DevState d) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= d.nf) return;
+  const int s0 = d.fil[f].site0, nbf = d.fil[f].n - 1, b0 = s0 - f;
+  double true_length = 0.0;
+  double r1[3], r2[3];
+#pragma unroll
+  for (int i = 0; i < ND; ++i) r1[i] = d.r[i][s0];
+  for (int q = 0; q < nbf; ++q) {
+    double l = 0.0;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) {
+      r2[i] = d.r[i][s0 + q + 1];
+      const double u = r2[i] - r1[i];
+      l += u * u;
+    }
+    l = sqrt(l);
+    d.bml[b0 + q] = true_length;
+    true_length += l;
+#pragma unroll
+    for (int i = 0; i < ND; ++i) r1[i] = r2[i];
+  }
+  d.ftl[f] = true_length;
+}
+
+// Bond::ReInit of bond b from its sites (src/bond.cpp:22-37): unwrapped
+// centre, unit orientation, length.
+template <int ND>
+__device__ __forceinline__ double bond_reinit(const DevState &d, int b, double pos[3],
+                                              double u[3]) {
+  const int s1 = b + d.bond_fil[b];
+  double l = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) pos[i] = u[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    u[i] = d.r[i][s1 + 1] - d.r[i][s1];
+    l += u[i] * u[i];
+  }
+  l = sqrt(l);
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    pos[i] = d.r[i][s1] + 0.5 * u[i];
+    u[i] /= l;
+  }
+  return l;
+}
+
+// Crosslink tethers, recomputed on even steps (CrosslinkSpecies::
+// UpdateBoundCrosslinks, src/crosslink_species.cpp:218-258), one thread per
+// link, after k_mesh_lambda.  Each anchor follows its mesh lambda as the
+// reference's Anchor::UpdateAnchorPositionToMesh (src/anchor.cpp:45-68)
+// does for a bound anchor with end pausing: CheckMesh (:180-201) clamps the
+// mesh lambda to [0, true length]; Mesh::GetBondAtLambda (src/mesh.cpp:
+// 667-675) picks a bond from the nominal bond length; CalcBondLambda
+// (:70-111) measures lambda from that bond's mesh lambda and moves once to
+// a neighbouring bond when lambda falls outside it; UpdateAnchorPositionToBond
+// (:236-249) places the anchor, then periodic_boundary_conditions.  The
+// tether follows Crosslink::CalculateTetherForces (src/crosslink.cpp:
+// 247-275) with MinimumDistance::PointPoint (src/minimum_distance.cpp:
+// 71-101); each anchor's force, torque and bond are stored as Anchor::
+// ApplyAnchorForces (src/anchor.cpp:132-146) uses them, for re-use on the
+// odd step.  An anchor that leaves the bonds it is listed on, or whose lambda
+// ends outside its bond (where the reference stops with an error), sets
+// ST_TETHER.
 template <int ND>
 __global__ void k_tether(SysConst k, DevState d) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= d.nx) return;
   if (*d.status & ST_LIST_OVERFLOW) return;  // the step stopped at its rebuild
-  // Both anchors lie in one system (checked when the links are added).
-  const ReplicaConst &Rx = d.rep[rep_of_bond(d, d.xl_anchor[2 * x] >> 1)];
   double sp[2][3], ua[2][3], len[2], lam[2];
+  int bond[2];
+  int rep = 0;
 #pragma unroll
   for (int a = 0; a < 2; ++a) {
-    const int code = d.xl_anchor[2 * x + a];
-    const int b = code >> 1;
-    const int s1 = b + d.bond_fil[b];
-    double r1[3], r2[3], pos[3] = {0, 0, 0}, ap[3] = {0, 0, 0};
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      r1[i] = d.r[i][s1];
-      r2[i] = d.r[i][s1 + 1];
+    const int A = 2 * x + a;
+    const int f = d.xl_fil[A];
+    const FilConst &fc = d.fil[f];
+    const int nbf = fc.n - 1, b0 = fc.site0 - f;
+    rep = fc.rep;  // both anchors lie in one system (checked when the links are added)
+    const double tl = d.ftl[f];
+    double M = d.xl_M[A];
+    if (M < 0) M = 0;
+    else if (M > tl) M = tl;
+    d.xl_M[A] = M;
+    int kb;
+    if (M < 0) kb = 0;
+    else if (M >= d.fil_L[f]) kb = nbf - 1;
+    else kb = (int)floor(M / fc.l);
+    // (M / l can round up to the bond count just below the nominal length,
+    // where the reference would index past its bonds: kept on the last.)
+    kb = min(max(kb, 0), nbf - 1);
+    double pos[3], u[3];
+    double bl = bond_reinit<ND>(d, b0 + kb, pos, u);
+    double lm = M - d.bml[b0 + kb];
+    if (lm < 0) {
+      if (kb > 0) {
+        --kb;
+        bl = bond_reinit<ND>(d, b0 + kb, pos, u);
+        lm = M - d.bml[b0 + kb];
+      } else {
+        lm = 0;
+      }
+    } else if (lm > bl) {
+      if (kb < nbf - 1) {
+        ++kb;
+        bl = bond_reinit<ND>(d, b0 + kb, pos, u);
+        lm = M - d.bml[b0 + kb];
+      } else {
+        lm = bl;
+      }
     }
-    double l = 0.0;
+    bool listed = false;
+    for (int e = d.xb_off[b0 + kb]; e < d.xb_off[b0 + kb + 1]; ++e) listed |= d.xb_ent[e] == A;
+    if (lm < -1e-6 || lm > bl + 1e-6 || !listed) atomicOr(d.status, ST_TETHER);
+    bond[a] = b0 + kb;
+    len[a] = bl;
+    lam[a] = lm;
+    double ap[3] = {0, 0, 0};
 #pragma unroll
-    for (int i = 0; i < 3; ++i) ua[a][i] = 0.0;
+    for (int i = 0; i < 3; ++i) ua[a][i] = u[i];
 #pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      ua[a][i] = r2[i] - r1[i];
-      l += ua[a][i] * ua[a][i];
-    }
-    l = sqrt(l);
-#pragma unroll
-    for (int i = 0; i < ND; ++i) {
-      pos[i] = r1[i] + 0.5 * ua[a][i];
-      ua[a][i] /= l;
-    }
-    len[a] = l;
-    lam[a] = (code & 1) ? l : 0.0;
-#pragma unroll
-    for (int i = 0; i < ND; ++i) ap[i] = pos[i] - (0.5 * l - lam[a]) * ua[a][i];
+    for (int i = 0; i < ND; ++i) ap[i] = pos[i] - (0.5 * bl - lm) * u[i];
+    const ReplicaConst &R = d.rep[rep];
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
       double v = 0.0;
 #pragma unroll
-      for (int j = 0; j < ND; ++j) v += Rx.hinv[ND * i + j] * ap[j];
+      for (int j = 0; j < ND; ++j) v += R.hinv[ND * i + j] * ap[j];
       sp[a][i] = v - nint(v);
     }
   }
+  const ReplicaConst &Rx = d.rep[rep];
   double dr[3] = {0, 0, 0}, dr2 = 0.0, f[3] = {0, 0, 0};
   double ds[3] = {0, 0, 0};
 #pragma unroll
@@ -855,7 +948,7 @@ __global__ void k_tether(SysConst k, DevState d) {
     cross3(dl, c, t);
     double4 *o = reinterpret_cast<double4 *>(d.xl_c) + 2 * (size_t)(2 * x + a);
     o[0] = make_double4(c[0], c[1], c[2], t[0]);
-    o[1] = make_double4(t[1], t[2], 0.0, 0.0);
+    o[1] = make_double4(t[1], t[2], (double)bond[a], 0.0);
   }
 }
 
@@ -1374,9 +1467,14 @@ int launch_potential(const DevState &d, int prec, double *out, cudaStream_t st) 
 
 int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st) {
   if (d.nx == 0) return 0;
-  if (k.n_dim == 3) k_tether<3><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
-  else k_tether<2><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
-  return 1;
+  if (k.n_dim == 3) {
+    k_mesh_lambda<3><<<cdiv(d.nf, 128), 128, 0, st>>>(d);
+    k_tether<3><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
+  } else {
+    k_mesh_lambda<2><<<cdiv(d.nf, 128), 128, 0, st>>>(d);
+    k_tether<2><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
+  }
+  return 2;
 }
 
 int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st) {

@@ -99,13 +99,15 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float x) {
 // Sum of one bond's crosslink anchor contributions in link order, as
 // CrosslinkSpecies::ApplyCrosslinkTetherForces adds them to Bond::force_ /
 // torque_ before the pair path (src/crosslink_species.cpp:260-266,
-// src/anchor.cpp:132-146): ND force components, 3 torque components.
+// src/anchor.cpp:132-146): ND force components, 3 torque components.  Of
+// the anchors listed on the bond, those that sit on it count.
 template <int ND>
 __device__ __forceinline__ void bond_xlink_sum(const DevState &d, int b, double F[3],
                                                double T[3]) {
   const int e0 = d.xb_off[b], e1 = d.xb_off[b + 1];
   for (int e = e0; e < e1; ++e) {
     const double2 *c = reinterpret_cast<const double2 *>(d.xl_c) + 4 * (size_t)d.xb_ent[e];
+    if ((int)c[3].x != b) continue;
     const double2 v0 = c[0], v1 = c[1], v2 = c[2];
     F[0] += v0.x;
     F[1] += v0.y;

@@ -254,6 +254,25 @@ class Reference(_Checker):
         self._call("get_frictions", *[_ptr(a) for a in out])
         return out
 
+    def add_crosslinks(self, site_a, site_b, k_spring=10.0, k_spring_compress=-1.0,
+                       rest_length=0.0):
+        """Doubly-bound crosslinks made and attached by the reference's own
+        Crosslink and Anchor code (zero unbinding rate, no diffusion)."""
+        a = np.ascontiguousarray(site_a, dtype=np.int32)
+        b = np.ascontiguousarray(site_b, dtype=np.int32)
+        self.n_links = int(a.size)
+        self.lib.scref_add_crosslinks.restype = ctypes.c_int
+        rc = self._call("add_crosslinks", ctypes.c_int(a.size), _ptr(a), _ptr(b),
+                        ctypes.c_double(k_spring), ctypes.c_double(k_spring_compress),
+                        ctypes.c_double(rest_length))
+        if rc != 0:
+            raise RuntimeError("reference rejected the crosslinks")
+
+    def crosslink_forces(self):
+        f = np.zeros((getattr(self, "n_links", 0), 3))
+        self._call("get_crosslink_forces", _ptr(f))
+        return f
+
     def write_spec_frame(self, path):
         """Appends one spec frame, written by the reference's own writers."""
         if self._call("write_spec_frame", ctypes.c_char_p(path.encode())) != 0:

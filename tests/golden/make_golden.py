@@ -7,7 +7,9 @@ oracle/ref/Makefile).  Run where the reference tree is present:
 Each fixture holds a seeded initial configuration (random insertion with
 overlap rejection) and the reference's state after a fixed number of steps;
 the thermo_* fixtures hold its pressure records and potential energies, the
-format_* ones a spec and a posit frame as its own writers write them.
+format_* ones a spec and a posit frame as its own writers write them, the
+tether_* ones a run with doubly-bound crosslinks of its own Crosslink and
+Anchor code.
 tests/test_oracle.py requires the C oracle to reproduce every array bit for
 bit; the GPU tests require the CUDA path to match the oracle the same way.
 """
@@ -134,6 +136,44 @@ def make_format_case(name, c):
     return out
 
 
+# Doubly-bound crosslinks placed, updated and applied by the reference's own
+# Crosslink and Anchor code (anchors follow their mesh lambda as the bonds
+# stretch, and move between neighbouring bonds), with the tether forces
+# recomputed on even steps and re-applied on odd ones.
+TETHER_CASES = {
+    "tether_3d": dict(n_dim=3, R=10.0, n_fil=20, n_seg=20, lp=50.0, delta=1e-4, seed=41,
+                      steps=41, links=0.002, k=10.0, kc=-1.0, rest=1.0),
+    "tether_2d": dict(n_dim=2, R=24.0, n_fil=24, n_seg=16, lp=50.0, delta=1e-4, seed=42,
+                      steps=41, links=0.002, k=10.0, kc=4.0, rest=1.5),
+}
+
+
+def make_tether_case(name, c):
+    from simcore_b200 import workloads
+    nb = np.full(c["n_fil"], c["n_seg"], dtype=np.int32)
+    sites = sc.insert_filaments(c["n_dim"], c["R"], c["seed"], nb, nb.astype(float),
+                                np.full(c["n_fil"], c["lp"]))
+    system = dict(n_dim=c["n_dim"], system_radius=c["R"], delta=c["delta"], seed=c["seed"])
+    fils = [dict(length=float(c["n_seg"]), persistence_length=c["lp"], diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * c["n_fil"]
+    a, b, _, _ = workloads.crosslinks("E", sites, fils, 2 * c["R"], scale=c["links"],
+                                      seed=c["seed"])
+    ref = Reference(system, fils, sites, n_threads=2)
+    ref.add_crosslinks(a, b, k_spring=c["k"], k_spring_compress=c["kc"], rest_length=c["rest"])
+    ref.step(c["steps"])
+    f, t = ref.bond_forces()
+    out = dict(
+        system=np.array([c["n_dim"], c["R"], c["delta"], c["seed"], c["lp"], c["n_seg"],
+                         c["n_fil"], c["steps"]], dtype=np.float64),
+        links=np.array([c["k"], c["kc"], c["rest"]]), site_a=a, site_b=b,
+        sites0=sites, sites=ref.sites(), prev_sites=ref.prev_sites(), bond_force=f,
+        bond_torque=t, tensions=ref.tensions(), crosslink_forces=ref.crosslink_forces(),
+        n_rebuilds=np.array([ref.n_rebuilds]))
+    ref.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return out
+
+
 if __name__ == "__main__":
     # Arguments: the names of the cases to (re)generate; none = all.
     if not Reference.available():
@@ -155,3 +195,9 @@ if __name__ == "__main__":
             continue
         o = make_format_case(name, c)
         print(name, "spec bytes", len(o["spec_frame"]), "posit bytes", len(o["posit_frame"]))
+    for name, c in TETHER_CASES.items():
+        if want and name not in want:
+            continue
+        o = make_tether_case(name, c)
+        print(name, "links", len(o["site_a"]), "max tether force",
+              float(np.abs(o["crosslink_forces"]).max()))

@@ -320,6 +320,35 @@ def test_crosslinks_mixed_close():
     assert np.abs(x32 - x64).max() <= 1e-5 * np.abs(x64).max()
 
 
+@pytest.mark.parametrize("name", ["tether_3d", "tether_2d"])
+def test_crosslinks_match_reference_fixture(name):
+    """Doubly-bound crosslinks run by the reference's own Crosslink and
+    Anchor code (tests/golden/make_golden.py, tether_* fixtures): anchors
+    follow their mesh lambda and move between neighbouring bonds as the
+    bonds stretch.  The FP64 GPU path, host-driven and through the captured
+    graph, gives the reference's bits."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    nd, R, delta, seed, lp, nseg, nfil, steps = g["system"]
+    k, kc, rest = g["links"]
+    system = dict(n_dim=int(nd), system_radius=R, delta=delta, seed=int(seed))
+    fils = [dict(length=float(nseg), persistence_length=lp, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * int(nfil)
+    for graph in (False, True):
+        ctx = _ctx(system, fils, g["sites0"])
+        ctx.add_crosslinks(g["site_a"], g["site_b"], k_spring=k, k_spring_compress=kc,
+                           rest_length=rest)
+        (ctx.step_graph if graph else ctx.step)(int(steps))
+        f, t = ctx.bond_forces()
+        nd = int(nd)
+        assert_same(ctx.sites()[:, :nd], g["sites"][:, :nd], "sites")
+        assert_same(ctx.prev_sites()[:, :nd], g["prev_sites"][:, :nd], "prev sites")
+        assert_same(f[:, :nd], g["bond_force"][:, :nd], "bond forces")
+        assert_same(t, g["bond_torque"], "bond torques")
+        assert_same(ctx.crosslink_forces(), g["crosslink_forces"], "tether forces")
+        ctx.close()
+
+
 def test_fp64_uneven_lengths_bitwise():
     """Workload C's length and stiffness spread (5 to 200 bonds, log-uniform;
     lp uniform in [10, 1000]) on 100 filaments: 256-site integrator blocks

@@ -378,3 +378,57 @@ def test_oracle_insertion_of_replica_batches():
                                          insert=oracle_insert)
     assert np.array_equal(a[2], b[2])
     assert a[3] == b[3]
+
+
+TETHER_GOLDEN = [p for p in _ALL_GOLDEN if os.path.basename(p).startswith("tether_")]
+
+
+@pytest.mark.parametrize("path", TETHER_GOLDEN, ids=os.path.basename)
+def test_oracle_reproduces_reference_tether_fixture(path):
+    """Doubly-bound crosslinks as the reference's own Crosslink and Anchor
+    code runs them (tests/golden/make_golden.py, tether_* fixtures): anchors
+    keep their mesh lambda while the bonds stretch, move between neighbouring
+    bonds, and apply their tether forces on even steps and again on odd
+    ones.  The oracle reproduces positions, bond forces and torques, tensions
+    and tether forces bit for bit."""
+    g = np.load(path)
+    nd, R, delta, seed, lp, nseg, nfil, steps = g["system"]
+    k, kc, rest = g["links"]
+    system = dict(n_dim=int(nd), system_radius=R, delta=delta, seed=int(seed))
+    fils = [dict(length=float(nseg), persistence_length=lp, diameter=1.0,
+                 min_bond_length=0.666, friction_ratio=2.0)] * int(nfil)
+    o = Oracle(system, fils, g["sites0"])
+    o.add_crosslinks(g["site_a"], g["site_b"], k_spring=k, k_spring_compress=kc,
+                     rest_length=rest)
+    o.step(int(steps))
+    f, t = o.bond_forces()
+    for name, got in (("sites", o.sites()), ("prev_sites", o.prev_sites()),
+                      ("bond_force", f), ("bond_torque", t), ("tensions", o.tensions()),
+                      ("crosslink_forces", o.crosslink_forces())):
+        assert np.array_equal(got, g[name]), name
+    assert o.n_rebuilds == int(g["n_rebuilds"][0])
+    o.close()
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build not present")
+def test_oracle_and_reference_tethers_side_by_side():
+    """A tethered network of buckling filaments (workload E's parameters at
+    small size), the oracle and the reference's own code stepped together:
+    equal bits every step."""
+    from checkers import oracle_insert, oracle_n_bonds, workloads_module
+    wl = workloads_module()
+    system, fils, sites = wl.make("E", 0.01, seed=4, insert=oracle_insert)
+    a, b, k, rest = wl.crosslinks("E", sites, fils, 2 * system["system_radius"], scale=0.01,
+                                  seed=4, n_bonds=oracle_n_bonds)
+    o = Oracle(system, fils, sites)
+    r = Reference(system, fils, sites)
+    for c in (o, r):
+        c.add_crosslinks(a, b, k_spring=k, rest_length=rest)
+    for _ in range(12):
+        o.step(1)
+        r.step(1)
+        assert np.array_equal(o.crosslink_forces(), r.crosslink_forces())
+        assert np.array_equal(o.bond_forces()[0], r.bond_forces()[0])
+        assert np.array_equal(o.sites(), r.sites())
+    o.close()
+    r.close()
