@@ -169,6 +169,25 @@ sc_status sc_analysis_sample(sc_ctx *ctx, int n_bins);
 sc_status sc_analysis_results(sc_ctx *ctx, double *mse2e, double *mse2e_err, int64_t *n_samples,
                               int32_t *max_joints, int64_t *theta_hist);
 sc_status sc_global_order(sc_ctx *ctx, double *polar, double *nematic);
+/* Centre-of-mass diffusion on the device, per system: the reference's
+ * diffusion analysis (SpherocylinderSpecies::InitDiffusionAnalysis,
+ * DiffusionAnalysis, CalculateMSD, CalculateVCF, FinalizeDiffusionAnalysis,
+ * src/spherocylinder_species.cpp:30-134) applied to the filaments' average
+ * positions and orientations (Filament::UpdateAvgPosition, src/filament.cpp:
+ * 953-968).  sc_diffusion_init(ctx, interval) takes the current averages as
+ * time origins and clears the sums; every sc_diffusion_sample adds window
+ * point t (0 .. interval-1) of the mean square displacement <|r - r0|^2>
+ * and the orientation correlation <u . u0> over each system's filaments,
+ * each weighted by the inverse of its variance over the filaments, and
+ * after the last point of a window takes new origins.  sc_diffusion_results
+ * gives per system and window point (n_replicas x interval) the weighted
+ * means and their errors, as FinalizeDiffusionAnalysis computes them.  The
+ * sums over filaments run in a fixed order other than the reference's
+ * serial one (agreement to rounding). */
+sc_status sc_diffusion_init(sc_ctx *ctx, int interval);
+sc_status sc_diffusion_sample(sc_ctx *ctx);
+sc_status sc_diffusion_results(sc_ctx *ctx, double *msd, double *msd_err, double *vcf,
+                               double *vcf_err);
 /* Thermo (InteractionManager::CalculatePressure, src/interaction_manager.cpp:
  * 500-517, 535-559, called by Simulation::Statistics every n_thermo steps).
  * sc_set_thermo(ctx, n) makes every step add its pairs' virial -dr x F (each

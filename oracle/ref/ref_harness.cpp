@@ -129,6 +129,16 @@ struct RefSim {
   int n_thermo = 0;
   std::vector<double> thermo_rec;  // i_step, pressure tensor (9), pressure, volume
   std::unordered_map<const Object *, int> bond_gid;
+  // FilamentSpecies analyses (scref_analysis_*): mse2e_, mse2e2_, n_samples_,
+  // n_bins_, theta_histogram_ (src/filament_species.cpp:366-456)
+  double mse2e = 0, mse2e2 = 0;
+  long an_samples = 0;
+  int n_bins = 0;
+  std::vector<std::vector<int>> theta_histogram;
+  // diffusion analysis (scref_diffusion_*): SpherocylinderSpecies' time-
+  // origin averaged MSD and orientation correlation, on filament averages
+  int dif_interval = 0, dif_time = 0;
+  std::vector<double> pos0, u0, msd, msd_err, vcf, vcf_err;
   // doubly-bound crosslinks (scref_add_crosslinks)
   crosslink_parameters xparams;
   std::vector<Crosslink> xlinks;
@@ -793,6 +803,147 @@ int scref_add_crosslinks(void *h, int n, const int *site_a, const int *site_b, d
     x.SetDoubly();
   }
   return 0;
+}
+
+// FilamentSpecies::RunMse2eAnalysis and RunThetaAnalysis (src/filament_species.
+// cpp:569-610) over the members, as the reference runs them after a step:
+// head-to-tail distance from the current sites, joint cosines from
+// Filament::GetThetas (the cosines CalculateAngles took at the start of the
+// last step's integration).  The histogram is sized at the first sample as
+// InitThetaAnalysis sizes it (:417-456), with n_bins bins.
+void scref_analysis_sample(void *h, int n_bins) {
+  RefSim *s = (RefSim *)h;
+  const int nd = s->params.n_dim;
+  if (s->theta_histogram.empty()) {
+    s->n_bins = n_bins;
+    const int nbonds = s->members.back().GetNBonds();
+    s->theta_histogram.assign(nbonds - 1, std::vector<int>(n_bins, 0));
+  }
+  for (auto it = s->members.begin(); it != s->members.end(); ++it) {
+    double const *const head_pos = it->GetHeadPosition();
+    double const *const tail_pos = it->GetTailPosition();
+    double mse2e_temp = 0.0;
+    for (int i = 0; i < nd; ++i) {
+      double temp = (head_pos[i] - tail_pos[i]);
+      mse2e_temp += temp * temp;
+    }
+    s->mse2e += mse2e_temp;
+    s->mse2e2 += mse2e_temp * mse2e_temp;
+  }
+  s->an_samples++;
+  for (auto it = s->members.begin(); it != s->members.end(); ++it) {
+    std::vector<double> const *const thetas = it->GetThetas();
+    for (int i = 0; i < (it->GetNBonds() - 1); ++i) {
+      int bin_number = (int)floor((1 + (*thetas)[i]) * (s->n_bins / 2));
+      if (bin_number == s->n_bins) bin_number = s->n_bins - 1;
+      else if (bin_number == -1) bin_number = 0;
+      s->theta_histogram[i][bin_number]++;
+    }
+  }
+}
+
+// FilamentSpecies::FinalizeMse2eAnalysis (src/filament_species.cpp:686-698)
+// on copies of the sums, and the histogram (joints x bins).
+void scref_analysis_results(void *h, double *mean, double *err, long *n_samples, int *n_joints,
+                            long *hist) {
+  RefSim *s = (RefSim *)h;
+  const int num = (int)s->members.size();
+  double m = s->mse2e, m2 = s->mse2e2;
+  m /= s->an_samples * num;
+  m2 /= s->an_samples * num;
+  if (mean) *mean = m;
+  if (err) *err = sqrt((m2 - m * m) / (num * s->an_samples));
+  if (n_samples) *n_samples = s->an_samples;
+  if (n_joints) *n_joints = (int)s->theta_histogram.size();
+  if (hist)
+    for (size_t j = 0; j < s->theta_histogram.size(); ++j)
+      for (int b = 0; b < s->n_bins; ++b) hist[j * s->n_bins + b] = s->theta_histogram[j][b];
+}
+
+// The reference's diffusion analysis (SpherocylinderSpecies::
+// InitDiffusionAnalysis, DiffusionAnalysis, UpdateInitPositions, CalculateMSD,
+// CalculateVCF, FinalizeDiffusionAnalysis; src/spherocylinder_species.cpp:
+// 30-134) applied to the filaments' average positions and orientations
+// (Filament::UpdateAvgPosition, src/filament.cpp:953-968, which every
+// UpdatePosition runs): a time-origin average over windows of `interval`
+// samples, each window's points weighted by the inverse variance over the
+// members.
+void scref_diffusion_init(void *h, int interval) {
+  RefSim *s = (RefSim *)h;
+  const int n = (int)s->members.size(), nd = s->params.n_dim;
+  s->dif_interval = interval;
+  s->dif_time = 0;
+  s->pos0.assign((size_t)n * nd, 0.0);
+  s->u0.assign((size_t)n * nd, 0.0);
+  s->msd.assign(interval, 0.0);
+  s->msd_err.assign(interval, 0.0);
+  s->vcf.assign(interval, 0.0);
+  s->vcf_err.assign(interval, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < nd; ++j) {
+      s->pos0[(size_t)i * nd + j] = s->members[i].GetPosition()[j];
+      s->u0[(size_t)i * nd + j] = s->members[i].GetOrientation()[j];
+    }
+}
+
+void scref_diffusion_sample(void *h) {
+  RefSim *s = (RefSim *)h;
+  const int n = (int)s->members.size(), nd = s->params.n_dim;
+  {  // CalculateMSD
+    double avg_sqr_dist = 0.0, avg_sqr_dist_sqr = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double sqr_diff = 0;
+      double const *const position = s->members[i].GetPosition();
+      for (int j = 0; j < nd; ++j) {
+        double r_diff = position[j] - s->pos0[(size_t)i * nd + j];
+        sqr_diff += SQR(r_diff);
+      }
+      avg_sqr_dist += sqr_diff;
+      avg_sqr_dist_sqr += SQR(sqr_diff);
+    }
+    avg_sqr_dist /= n;
+    avg_sqr_dist_sqr /= n;
+    double stdev2 = avg_sqr_dist_sqr - SQR(avg_sqr_dist);
+    s->msd[s->dif_time] += avg_sqr_dist / stdev2;
+    s->msd_err[s->dif_time] += 1.0 / stdev2;
+  }
+  {  // CalculateVCF
+    double avg_udotu0 = 0.0, avg_udotu0_sqr = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double udotu0 = 0.0;
+      double const *const orientation = s->members[i].GetOrientation();
+      for (int j = 0; j < nd; ++j) udotu0 += orientation[j] * s->u0[(size_t)i * nd + j];
+      avg_udotu0 += udotu0;
+      avg_udotu0_sqr += udotu0 * udotu0;
+    }
+    avg_udotu0 /= n;
+    avg_udotu0_sqr /= n;
+    double stdev2 = avg_udotu0_sqr - SQR(avg_udotu0);
+    s->vcf[s->dif_time] += avg_udotu0 / stdev2;
+    s->vcf_err[s->dif_time] += 1.0 / stdev2;
+  }
+  if (++s->dif_time == s->dif_interval) {  // UpdateInitPositions
+    s->dif_time = 0;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < nd; ++j) {
+        s->pos0[(size_t)i * nd + j] = s->members[i].GetPosition()[j];
+        s->u0[(size_t)i * nd + j] = s->members[i].GetOrientation()[j];
+      }
+  }
+}
+
+// FinalizeDiffusionAnalysis' quotients (on copies): msd, its error, vcf and
+// its error per window point.
+void scref_diffusion_results(void *h, double *msd, double *msd_err, double *vcf,
+                             double *vcf_err) {
+  RefSim *s = (RefSim *)h;
+  const int n = (int)s->members.size();
+  for (int t = 0; t < s->dif_interval; ++t) {
+    msd[t] = s->msd[t] / s->msd_err[t];
+    vcf[t] = s->vcf[t] / s->vcf_err[t];
+    msd_err[t] = 1.0 / sqrt(n * s->msd_err[t]);
+    vcf_err[t] = 1.0 / sqrt(n * s->vcf_err[t]);
+  }
 }
 
 // Crosslink::force_ of every crosslink (the tether force on anchor 0).

@@ -38,7 +38,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_set_noise_key", "sc_output_open", "sc_output_write", "sc_output_close",
             "sc_analysis_sample", "sc_analysis_results", "sc_global_order",
             "sc_set_thermo", "sc_thermo_open", "sc_get_thermo", "sc_get_potential_energy",
-            "sc_set_exact_near_parallel", "sc_set_fused_pairs"]
+            "sc_set_exact_near_parallel", "sc_set_fused_pairs", "sc_diffusion_init",
+            "sc_diffusion_sample", "sc_diffusion_results"]
 
 
 class ScError(RuntimeError):
@@ -371,6 +372,23 @@ class Context:
         q = np.zeros((R, 9))
         self._check(lib.sc_global_order(self.h, _p(p), _p(q)))
         return p, q
+
+    def diffusion_init(self, interval):
+        """Centre-of-mass diffusion analysis: current filament averages as
+        time origins, windows of `interval` samples."""
+        self._check(lib.sc_diffusion_init(self.h, int(interval)))
+        self._dif_interval = int(interval)
+
+    def diffusion_sample(self):
+        self._check(lib.sc_diffusion_sample(self.h))
+
+    def diffusion_results(self):
+        """(msd, msd_err, vcf, vcf_err), each (systems, interval); a single
+        system's arrays drop the systems axis."""
+        R, T = self.n_replicas, self._dif_interval
+        out = [np.zeros((R, T)) for _ in range(4)]
+        self._check(lib.sc_diffusion_results(self.h, *[_p(a) for a in out]))
+        return tuple(a[0] for a in out) if R == 1 else tuple(out)
 
     def set_exact_near_parallel(self, on=True):
         """Mixed precision: nearly parallel pairs evaluated from the FP64 sites."""

@@ -45,6 +45,14 @@ struct sc_ctx {
     double *order = nullptr;   // 12 per system
   } an;
 
+  // diffusion analysis (sc_diffusion_*): window of `interval` samples, the
+  // next sample's point, origins and per-system sums (4 x interval each)
+  struct Diffusion {
+    int interval = 0, t = 0;
+    long long n_samples = 0;
+    double *avg = nullptr, *pos0 = nullptr, *u0 = nullptr, *acc = nullptr;
+  } dif;
+
   // reference-format output (sc_output_*): one spec and one posit file per
   // system, frames snapshotted on the device and copied on out_st
   struct Output {
@@ -2060,6 +2068,75 @@ sc_status sc_analysis_results(sc_ctx *c, double *mse2e, double *mse2e_err, int64
   }
   if (theta_hist)
     for (size_t i = 0; i < hist.size(); ++i) theta_hist[i] = hist[i];
+  return SC_OK;
+}
+
+sc_status sc_diffusion_init(sc_ctx *c, int interval) {
+  if (!c || !c->loaded || interval < 1) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  sc_ctx::Diffusion &a = c->dif;
+  const size_t nrep = c->reps.size();
+  if (!a.avg) {
+    CKS(dalloc(c, &a.avg, 9 * (size_t)c->nf));
+    CKS(dalloc(c, &a.pos0, 3 * (size_t)c->nf));
+    CKS(dalloc(c, &a.u0, 3 * (size_t)c->nf));
+  }
+  if (a.interval != interval) {
+    dfree(c, a.acc);
+    a.acc = nullptr;
+    CKS(dalloc(c, &a.acc, 4 * nrep * (size_t)interval));
+  }
+  CK(cudaMemsetAsync(a.acc, 0, sizeof(double) * 4 * nrep * interval, c->st));
+  a.interval = interval;
+  a.t = 0;
+  a.n_samples = 0;
+  // SpherocylinderSpecies::UpdateInitPositions: the current averages.
+  c->launches += sc::launch_filament_averages(c->k, c->d, a.avg, c->st);
+  c->launches += sc::launch_aos_to_origins(c->nf, a.avg, a.pos0, a.u0, c->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return SC_OK;
+}
+
+sc_status sc_diffusion_sample(sc_ctx *c) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  sc_ctx::Diffusion &a = c->dif;
+  if (!a.acc) return fail(c, SC_ERR_INVALID_ARG, "sc_diffusion_sample needs sc_diffusion_init");
+  CK(cudaSetDevice(c->desc.device));
+  const int restart = a.t + 1 == a.interval ? 1 : 0;
+  c->launches += sc::launch_filament_averages(c->k, c->d, a.avg, c->st);
+  c->launches += sc::launch_diffusion_sample(c->k, c->d, a.avg, a.pos0, a.u0, a.acc, a.t,
+                                             a.interval, restart, c->st);
+  CK(cudaGetLastError());
+  a.t = restart ? 0 : a.t + 1;
+  a.n_samples++;
+  return SC_OK;
+}
+
+sc_status sc_diffusion_results(sc_ctx *c, double *msd, double *msd_err, double *vcf,
+                               double *vcf_err) {
+  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
+  sc_ctx::Diffusion &a = c->dif;
+  if (!a.acc) return fail(c, SC_ERR_INVALID_ARG, "sc_diffusion_results needs sc_diffusion_init");
+  CK(cudaSetDevice(c->desc.device));
+  const int nrep = (int)c->reps.size(), T = a.interval;
+  std::vector<double> acc(4 * (size_t)nrep * T);
+  CK(cudaMemcpyAsync(acc.data(), a.acc, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  // SpherocylinderSpecies::FinalizeDiffusionAnalysis
+  // (src/spherocylinder_species.cpp:125-134).
+  for (int r = 0; r < nrep; ++r) {
+    const double *o = acc.data() + 4 * (size_t)T * r;
+    const double n = c->reps[r].nf;
+    for (int t = 0; t < T; ++t) {
+      const size_t i = (size_t)r * T + t;
+      if (msd) msd[i] = o[t] / o[T + t];
+      if (vcf) vcf[i] = o[2 * T + t] / o[3 * T + t];
+      if (msd_err) msd_err[i] = 1.0 / std::sqrt(n * o[T + t]);
+      if (vcf_err) vcf_err[i] = 1.0 / std::sqrt(n * o[3 * T + t]);
+    }
+  }
   return SC_OK;
 }
 

@@ -964,6 +964,17 @@ __global__ void k_aos_to_soa(int n, int nd, const double *aos, DevState d) {
   }
 }
 
+// Filament averages (9 per filament) -> diffusion origins: average position
+// (3) and average orientation (3) per filament.
+__global__ void k_avg_to_origins(int nf, const double *avg, double *pos0, double *u0) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  for (int j = 0; j < 3; ++j) {
+    pos0[3 * (size_t)f + j] = avg[9 * (size_t)f + j];
+    u0[3 * (size_t)f + j] = avg[9 * (size_t)f + 6 + j];
+  }
+}
+
 template <class T>
 __global__ void k_soa_to_aos(int n, const T *x, const T *y, const T *z, double *aos) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1074,6 +1085,58 @@ __global__ void __launch_bounds__(256) k_analysis_sample(DevState d, int n_bins,
   }
 }
 
+// The reference's diffusion analysis (SpherocylinderSpecies::CalculateMSD,
+// CalculateVCF, UpdateInitPositions; src/spherocylinder_species.cpp:62-121)
+// on the filaments' average positions and orientations (avg, 9 per filament
+// from k_filament_averages: Filament::UpdateAvgPosition), one block per
+// system: the mean over its filaments of |r - r0|^2 and of u . u0 and their
+// second moments, each weighted by the inverse variance into window point t
+// of acc (per system: msd, msd weight, vcf, vcf weight, each `interval`
+// long); when the window closes (restart) the current averages become the
+// new origins (pos0, u0: 3 each per filament).
+template <int ND>
+__global__ void __launch_bounds__(256) k_diffusion_sample(DevState d, const double *avg,
+                                                          double *pos0, double *u0,
+                                                          double *acc, int t, int interval,
+                                                          int restart) {
+  __shared__ double tmp[8];
+  const int r = blockIdx.x;
+  const ReplicaConst &R = d.rep[r];
+  double q[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int f = R.f0 + threadIdx.x; f < R.f0 + R.nf; f += blockDim.x) {
+    const double *a = avg + 9 * (size_t)f;
+    double sqr_diff = 0.0, udotu0 = 0.0;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      const double r_diff = a[j] - pos0[3 * (size_t)f + j];
+      sqr_diff += r_diff * r_diff;
+    }
+#pragma unroll
+    for (int j = 0; j < ND; ++j) udotu0 += a[6 + j] * u0[3 * (size_t)f + j];
+    q[0] += sqr_diff;
+    q[1] += sqr_diff * sqr_diff;
+    q[2] += udotu0;
+    q[3] += udotu0 * udotu0;
+  }
+  for (int k2 = 0; k2 < 4; ++k2) q[k2] = block_sum256(q[k2], tmp);
+  if (threadIdx.x == 0) {
+    double *o = acc + 4 * (size_t)interval * r;
+    const double n = R.nf;
+    const double m = q[0] / n, m2 = q[1] / n, v = q[2] / n, v2 = q[3] / n;
+    const double s_msd = m2 - m * m, s_vcf = v2 - v * v;
+    o[t] += m / s_msd;
+    o[interval + t] += 1.0 / s_msd;
+    o[2 * interval + t] += v / s_vcf;
+    o[3 * interval + t] += 1.0 / s_vcf;
+  }
+  if (restart)  // each thread replaces only the origins it read
+    for (int f = R.f0 + threadIdx.x; f < R.f0 + R.nf; f += blockDim.x)
+      for (int j = 0; j < 3; ++j) {
+        pos0[3 * (size_t)f + j] = avg[9 * (size_t)f + j];
+        u0[3 * (size_t)f + j] = avg[9 * (size_t)f + 6 + j];
+      }
+}
+
 // FilamentSpecies::RunGlobalOrderAnalysis (src/filament_species.cpp:486-535)
 // with Filament::GetPolarOrder / GetNematicOrder (src/filament.cpp:488-516):
 // per system, the mean over filaments of the mean bond orientation (3) and
@@ -1132,6 +1195,22 @@ int launch_analysis_sample(const SysConst &k, const DevState &d, int n_bins, int
                            double *acc, int *hist, cudaStream_t st) {
   if (k.n_dim == 3) k_analysis_sample<3><<<d.nrep, 256, 0, st>>>(d, n_bins, max_joints, acc, hist);
   else k_analysis_sample<2><<<d.nrep, 256, 0, st>>>(d, n_bins, max_joints, acc, hist);
+  return 1;
+}
+
+int launch_aos_to_origins(int nf, const double *avg, double *pos0, double *u0,
+                          cudaStream_t st) {
+  k_avg_to_origins<<<cdiv(nf, 256), 256, 0, st>>>(nf, avg, pos0, u0);
+  return 1;
+}
+
+int launch_diffusion_sample(const SysConst &k, const DevState &d, const double *avg,
+                            double *pos0, double *u0, double *acc, int t, int interval,
+                            int restart, cudaStream_t st) {
+  if (k.n_dim == 3)
+    k_diffusion_sample<3><<<d.nrep, 256, 0, st>>>(d, avg, pos0, u0, acc, t, interval, restart);
+  else
+    k_diffusion_sample<2><<<d.nrep, 256, 0, st>>>(d, avg, pos0, u0, acc, t, interval, restart);
   return 1;
 }
 

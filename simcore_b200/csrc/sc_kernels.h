@@ -20,6 +20,16 @@ int scan_temp_ints(long long n);
 int launch_analysis_sample(const SysConst &k, const DevState &d, int n_bins, int max_joints,
                            double *acc, int *hist, cudaStream_t st);
 int launch_global_order(const SysConst &k, const DevState &d, double *out, cudaStream_t st);
+// Diffusion analysis: one sample at window point t of every system's MSD and
+// orientation correlation, from the filament averages avg; restart replaces
+// the origins pos0 / u0 with the current averages.
+int launch_diffusion_sample(const SysConst &k, const DevState &d, const double *avg,
+                            double *pos0, double *u0, double *acc, int t, int interval,
+                            int restart, cudaStream_t st);
+// Diffusion origins (average position and orientation, 3 each per filament)
+// from the filament averages.
+int launch_aos_to_origins(int nf, const double *avg, double *pos0, double *u0,
+                          cudaStream_t st);
 // Per filament average position, its scaled image and average orientation
 // (9 doubles each).
 int launch_filament_averages(const SysConst &k, const DevState &d, double *out, cudaStream_t st);
@@ -61,7 +71,7 @@ int launch_zero_dr(const DevState &d, cudaStream_t st);
 // Grid sized for `expected` pairs (one system) or every slot (several); the
 // kernel strides over the actual pairs.
 // npx (mixed only): nearly parallel pairs are evaluated from the FP64
-// sites by a second kernel.
+// sites by the kernel's last block.
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
                  int expected, cudaStream_t st, bool npx = false);
 // Crosslink tethers of an even step into the per-anchor contributions.

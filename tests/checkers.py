@@ -273,6 +273,34 @@ class Reference(_Checker):
         self._call("get_crosslink_forces", _ptr(f))
         return f
 
+    def analysis_sample(self, n_bins=100):
+        """FilamentSpecies::RunMse2eAnalysis + RunThetaAnalysis, as the
+        reference runs them after a step."""
+        self._call("analysis_sample", ctypes.c_int(n_bins))
+        self._n_bins = n_bins
+
+    def analysis_results(self):
+        """(mse2e mean, its error, samples, histogram (joints, bins))."""
+        m, e = ctypes.c_double(), ctypes.c_double()
+        n, j = ctypes.c_long(), ctypes.c_int()
+        self._call("analysis_results", ctypes.byref(m), ctypes.byref(e), ctypes.byref(n),
+                   ctypes.byref(j), None)
+        hist = np.zeros((j.value, self._n_bins), dtype=np.int64)
+        self._call("analysis_results", None, None, None, None, _ptr(hist))
+        return m.value, e.value, n.value, hist
+
+    def diffusion_init(self, interval):
+        self._call("diffusion_init", ctypes.c_int(interval))
+        self._dif_interval = interval
+
+    def diffusion_sample(self):
+        self._call("diffusion_sample")
+
+    def diffusion_results(self):
+        out = [np.zeros(self._dif_interval) for _ in range(4)]
+        self._call("diffusion_results", *[_ptr(a) for a in out])
+        return tuple(out)
+
     def write_spec_frame(self, path):
         """Appends one spec frame, written by the reference's own writers."""
         if self._call("write_spec_frame", ctypes.c_char_p(path.encode())) != 0:

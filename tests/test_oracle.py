@@ -432,3 +432,29 @@ def test_oracle_and_reference_tethers_side_by_side():
         assert np.array_equal(o.sites(), r.sites())
     o.close()
     r.close()
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build not present")
+def test_reference_analysis_hooks_run():
+    """The checker's analysis hooks (the reference's RunMse2eAnalysis /
+    RunThetaAnalysis and diffusion analysis on its own filaments) give a
+    mean-square end-to-end distance below L^2, one histogram count per joint
+    and filament, and finite diffusion means."""
+    from checkers import oracle_insert
+    nb = np.full(10, 12, dtype=np.int32)
+    sites = oracle_insert(3, 12.0, 3, nb, nb.astype(float), np.full(10, 20.0))
+    system = dict(n_dim=3, system_radius=12.0, delta=2e-4, seed=3)
+    fils = [dict(length=12.0, persistence_length=20.0, diameter=1.0, min_bond_length=0.666,
+                 friction_ratio=2.0)] * 10
+    r = Reference(system, fils, sites)
+    r.diffusion_init(3)
+    for _ in range(6):
+        r.step(4)
+        r.analysis_sample(20)
+        r.diffusion_sample()
+    m, e, n, hist = r.analysis_results()
+    assert 0 < m < 144.0 and e > 0 and n == 6
+    assert hist.shape == (11, 20) and hist.sum() == 6 * 10 * 11
+    for a in r.diffusion_results():
+        assert np.all(np.isfinite(a))
+    r.close()
