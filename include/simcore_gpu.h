@@ -214,7 +214,7 @@ sc_status sc_get_thermo(sc_ctx *ctx, int max_records, int *n_records, int64_t *i
 sc_status sc_get_potential_energy(sc_ctx *ctx, double *pote);
 /* Mixed precision only: nearly parallel pairs (FP32 |u1 x u2|^2 between 0
  * and 1e-5, within 0.18 degrees) are evaluated from the FP64 sites, as the
- * FP64 path evaluates them, by the last block of the pair kernel to finish.
+ * FP64 path evaluates them, by a one-block kernel after the pair stage.
  * FP32 orientations cannot resolve the closest points of such pairs: their
  * torques (and forces) could be off by far more than 1e-5.  On by default;
  * sc_set_exact_near_parallel(ctx, 0) evaluates them in FP32 like every other

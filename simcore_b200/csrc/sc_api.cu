@@ -13,6 +13,7 @@
 
 #include "sc_common.cuh"
 #include "sc_kernels.h"
+#include "sc_launch.h"
 #include "simcore_gpu.h"
 
 using sc::DevState;
@@ -118,8 +119,8 @@ struct sc_ctx {
   double graph_ms = 0.0;
   bool graph_fused = false;  // the captured steps evaluate their pairs in the integrator
   long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
-  // Mixed: nearly parallel pairs evaluated from the FP64 sites, by the last
-  // block of the pair kernel (on by default; sc_set_exact_near_parallel).
+  // Mixed: nearly parallel pairs evaluated from the FP64 sites by a one-block
+  // kernel after each pair stage (on by default; sc_set_exact_near_parallel).
   bool npx = true;
   // The last step fused its pair evaluation into the integrator, so the
   // per-bond slots do not hold it yet (materialize_slots writes them).
@@ -364,14 +365,12 @@ sc_status alloc_store(sc_ctx *c, long long total, PairStore &q) {
   return s;
 }
 
-// The counters of the near-parallel list (k_pair_eval's last block leaves
-// them zero after every pair stage), zeroed once.
+// The counters of the near-parallel list (k_pair_fixup leaves the count
+// zero after every pair stage), zeroed once.
 sc_status alloc_fixup_counters(sc_ctx *c) {
   if (c->d.fix_count) return SC_OK;
   CKS(dalloc(c, &c->d.fix_count, 1));
-  CKS(dalloc(c, &c->d.fix_done, 1));
   CK(cudaMemsetAsync(c->d.fix_count, 0, sizeof(int), c->st));
-  CK(cudaMemsetAsync(c->d.fix_done, 0, sizeof(unsigned), c->st));
   return SC_OK;
 }
 
@@ -456,12 +455,19 @@ sc_status sync_pair_count(sc_ctx *c) {
 // pair lists in the reference's order into their segments, build their
 // per-bond pair entries, zero their displacement trackers.  Device work only
 // (capturable); a list longer than its segment sets the overflow bit.
-void rebuild_enqueue(sc_ctx *c) {
+void rebuild_enqueue(sc_ctx *c, bool first_in_graph = false) {
   const SysConst &k = c->k;
   const long long before = c->launches;
   const DevState &d = c->d;
   if (c->desc.interaction_flag) {
-    c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
+    if (first_in_graph) {
+      // Captured, the rebuild's first kernel starts the conditional body:
+      // no kernel before it to overlap.
+      sc::PdlOff off;
+      c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
+    } else {
+      c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
+    }
     c->launches += sc::launch_exclusive_scan(c->cell_count, c->cell_start, k.n_cells,
                                              c->scan_tmp, c->st, c->cell_occ);
     c->launches += sc::launch_bin_scatter(d, c->key, c->cell_start, c->cell_count, c->sorted,
@@ -1309,7 +1315,7 @@ static sc_status build_graph(sc_ctx *c) {
     cudaGraph_t rb = ip.conditional.phGraph_out[0];
     CK(cudaStreamBeginCaptureToGraph(c->st, rb, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     long long launches = c->launches;
-    rebuild_enqueue(c);
+    rebuild_enqueue(c, true);
     c->launches = launches;
     CK(cudaStreamEndCapture(c->st, &rb));
     tail.push_back(inode);
@@ -1320,13 +1326,28 @@ static sc_status build_graph(sc_ctx *c) {
   c->graph_fused = fuse;
   for (int half = 0; half < 2; ++half) {
     const int rb = half == 0 ? c->rbuf : 1 - c->rbuf;
+    // The body's first kernel follows the conditional rebuild node (or the
+    // body's start), not a kernel: it is launched without the programmatic
+    // attribute.
     // The second half is the even (full) step: crosslink tethers first.
     if (half == 1 && interaction) sc::launch_tether(c->k, c->d, c->st);
-    if (interaction && !fuse)
-      sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
+    if (interaction && !fuse) {
+      if (half == 0) {
+        sc::PdlOff off;
+        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
+      } else {
+        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
+      }
+    }
     if (interaction && c->k.thermo) sc::launch_thermo(c->k, c->d, c->prec, c->st);
-    sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
-                         c->capture, c->prec, c->fast, c->st, fuse);
+    if (half == 0 && (!interaction || fuse)) {
+      sc::PdlOff off;
+      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1, rb, interaction, c->capture, c->prec,
+                           c->fast, c->st, fuse);
+    } else {
+      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
+                           c->capture, c->prec, c->fast, c->st, fuse);
+    }
   }
   sc::launch_loop_tail(c->d, c->desc.stoch_flag ? 1 : 0, h_loop, c->st);
   CK(cudaStreamEndCapture(c->st, &body));
@@ -1394,13 +1415,14 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       }
       // Kernels the graph ran: loop head, per BD step decide + tether + 2
       // steps + tail (the stopped step's too), per rebuild the captured
-      // sequence.  A step is its pair stage (unless fused), thermo and
-      // one or two integrator kernels.
+      // sequence.  A step is its pair stage (unless fused), the
+      // near-parallel fix-up, thermo and one or two integrator kernels.
       const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
       const long long per_bd =
           c->desc.interaction_flag
               ? 2 + (c->d.nx ? 2 : 0) +
-                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0))
+                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0) +
+                         (c->npx && c->prec && !c->graph_fused ? 1 : 0))
               : 1 + 2 * int_l;
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
                      (nr1 - nr0) * c->rebuild_kernels;

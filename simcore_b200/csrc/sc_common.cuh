@@ -23,6 +23,21 @@ __device__ __forceinline__ double sign_of(double a, double b) {  // SIGN(a, b)
 }
 __device__ __forceinline__ int signof(double x) { return x >= 0.0 ? 1 : -1; }
 
+// Programmatic dependent launch (sm_90 and later).  A kernel launched with
+// programmatic stream serialization may begin while the kernel before it in
+// the stream is still finishing.  grid_dep_sync() blocks the calling thread
+// until that kernel, and so every kernel before it, has completed with its
+// writes visible, then lets the next kernel in the stream launch: its blocks
+// take SM slots as this kernel's retire, and run their own loads of older
+// data before they wait in turn.  Every kernel of the step and rebuild
+// sequences calls it before its first access to data the kernel just before
+// it writes (or reads, for data it writes itself); in a kernel launched
+// without the attribute it returns at once.
+__device__ __forceinline__ void grid_dep_sync() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Status bits set by kernels; the host maps them to sc_status codes.
 enum : unsigned {
   ST_NAN = 1u,            // non-finite position or force
@@ -148,11 +163,10 @@ struct DevState {
   int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
   double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
   float *cf32;
-  // mixed pair stage with exact near-parallel pairs: those left to the
-  // FP64 fix-up of k_pair_eval's last block
+  // mixed pair stage with exact near-parallel pairs: those left to
+  // k_pair_fixup
   int *fix_list;           // one slot per pair
   int *fix_count;
-  unsigned *fix_done;      // blocks of the current launch done (ticket)
   // thermo (kept while SysConst::thermo is set): per pair the dr its stress
   // was computed from and its potential, stored with the force
   double *pv64;            // 4 per pair: dr (3), pote

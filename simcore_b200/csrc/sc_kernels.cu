@@ -9,8 +9,7 @@
 //                  scatter order)
 //   pair forces    k_pair_eval   (InteractionManager::CalculatePairInteractions,
 //                                 one thread per pair, signed per-bond slots)
-//                                (mixed: its last block evaluates the nearly
-//                                 parallel pairs in FP64)
+//                  k_pair_fixup  (mixed: the nearly parallel pairs in FP64)
 //                  k_bond_sum    (ApplyPairInteractions into bond accumulators)
 //   thermo         k_thermo, k_potential (pair virial and pressure records,
 //                                 per-filament potential energy)
@@ -19,8 +18,11 @@
 //   utilities      exclusive scan, geometry init, displacement reset.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "sc_common.cuh"
 #include "sc_kernels.h"
+#include "sc_launch.h"
 #include "sc_pair.cuh"
 #include "sc_step.cuh"
 #include "sc_step_warp.cuh"
@@ -96,6 +98,7 @@ __global__ void k_bond_cells(SysConst k, DevState d, int *xyz) {
 // and cell counts.
 template <int ND>
 __global__ void k_bin_count(SysConst k, DevState d, int *key, int *cell_count) {
+  grid_dep_sync();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   bool active = b < d.nb;
   int c = -1;
@@ -123,6 +126,7 @@ __global__ void k_bin_count(SysConst k, DevState d, int *key, int *cell_count) {
 // zero so the count array is ready for the next rebuild without clearing.
 __global__ void k_bin_scatter(DevState d, const int *key, const int *cell_start,
                               int *cell_count, int *sorted) {
+  grid_dep_sync();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb || !d.due[rep_of_bond(d, b)]) return;
   int c = key[b];
@@ -203,6 +207,7 @@ __device__ __forceinline__ bool cell_occupied(const unsigned *occ, int c) {
 // reads another cell's members, which their heads are sorting meanwhile.
 __global__ void k_cell_sort_count(SysConst k, DevState d, int nb, const int *key, int *sorted,
                                   const int *cell_start, int *pair_count, const unsigned *occ) {
+  grid_dep_sync();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nb) return;
   if (q >= cell_start[k.n_cells]) {
@@ -280,6 +285,7 @@ __device__ __forceinline__ void rep_pairs(const DevState &d, int r, const int *c
 __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
                             const int *sorted, const int *cell_start,
                             const int *pair_off, int *deg, int prec, const unsigned *occ) {
+  grid_dep_sync();
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q < d.nrep) rep_pairs(d, q, cell_start, pair_off);
   if (q >= cell_start[k.n_cells]) return;
@@ -338,6 +344,7 @@ __global__ void k_pair_emit(SysConst k, DevState d, int nb, const int *key,
 // Per-bond entry ranges of the rebuilt systems, inside their slot segments,
 // from the exclusive scan of the degrees over all bonds.
 __global__ void k_csr_offsets(DevState d, const int *deg_off, const int *deg) {
+  grid_dep_sync();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
   const int r = rep_of_bond(d, b);
@@ -369,6 +376,7 @@ __device__ __forceinline__ bool pair_live(const DevState &d, int p, int &r) {
 // Entries (pair << 1 | role) of every bond of the rebuilt systems; role 0 =
 // obj1, 1 = obj2.  The degree array is decremented back to zero.
 __global__ void k_csr_fill(DevState d, int *deg) {
+  grid_dep_sync();
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= d.pcap_total) return;
   int r;
@@ -384,6 +392,7 @@ __global__ void k_csr_fill(DevState d, int *deg) {
 // reference's serial ApplyPairInteractions adds them to the bond, then
 // records the slot of each (pair, role) entry.
 __global__ void k_csr_sort_pos(DevState d) {
+  grid_dep_sync();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb || !d.due[rep_of_bond(d, b)]) return;
   int e0 = d.e_off[b], e1 = e0 + d.e_cnt[b];
@@ -406,6 +415,7 @@ __global__ void k_csr_sort_pos(DevState d) {
 // InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321) for
 // the systems rebuilt in this pass.
 __global__ void k_zero_dr(DevState d) {
+  grid_dep_sync();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) *d.n_rebuilds += 1;
   if (i < d.nrep && d.due[i]) {
@@ -456,6 +466,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *tmp, int &total)
 // Sum of each tile of SCAN_TILE elements.
 template <bool VEC>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const int *in, int n, int *tile_sums) {
+  grid_dep_sync();
   __shared__ int red[SCAN_BLOCK / 32];
   const int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
   int sum = 0;
@@ -485,6 +496,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_reduce(const int *in, int n
 template <bool VEC>
 __global__ void __launch_bounds__(SCAN_BLOCK) k_scan_down(const int *in, int *out, int n,
                                                          const int *tile_sums, unsigned *occ) {
+  grid_dep_sync();
   __shared__ int tmp[SCAN_BLOCK / 32];
   __shared__ int red[SCAN_BLOCK / 32];
   // Sum of the earlier tiles: independent loads, then a block reduction.
@@ -635,10 +647,8 @@ __device__ __forceinline__ void pair_eval_fp64_sites(const SysConst &k, const De
   c2[1] = make_float4(-(float)t2[1], -(float)t2[2], 0.f, 0.f);
 }
 
-// Returns whether the pair was listed for the FP64 fix-up (NPX) instead of
-// evaluated.
 template <int ND, int PREC, bool NPX>
-__device__ __forceinline__ bool pair_eval_one(const SysConst &k, const DevState &d,
+__device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
                                               const ReplicaConst &R, int rbuf, int p) {
   const int a = d.pa[p], b = d.pb[p];
   const int s1 = d.pos1[p], s2 = d.pos2[p];
@@ -678,9 +688,9 @@ __device__ __forceinline__ bool pair_eval_one(const SysConst &k, const DevState 
     const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
-    if (NPX && near_parallel<ND>(A, B)) {  // left to the fix-up block
+    if (NPX && near_parallel<ND>(A, B)) {  // left to k_pair_fixup
       d.fix_list[atomicAdd(d.fix_count, 1)] = p;
-      return true;
+      return;
     }
     float force[3], rec[4], t1[3], t2[3];
     const bool set = pair_force_f32<ND>(k, R.hf, A, B, st, force, t1, t2,
@@ -697,60 +707,45 @@ __device__ __forceinline__ bool pair_eval_one(const SysConst &k, const DevState 
     c2[0] = make_float4(-force[0], -force[1], -force[2], -t2[0]);
     c2[1] = make_float4(-t2[1], -t2[2], 0.f, 0.f);
   }
-  return false;
 }
 
-// The nearly parallel pairs the NPX mixed pair stage left, evaluated from the
-// FP64 sites (pair_eval_fp64_sites) by the threads of one block.  Not
-// inlined: its FP64 registers are its own, so the FP32 loop of k_pair_eval
-// keeps its register budget, and only the block that calls it pays for the
-// spills the budget forces here.
+// The nearly parallel pairs the NPX mixed pair stage listed, evaluated from
+// the FP64 sites (pair_eval_fp64_sites), then the list reset for the next
+// pair stage.  One block: the list is short (most steps of most workloads
+// have none), and this kernel's registers and spills stay out of the FP32
+// pair kernel.
 template <int ND>
-__device__ __forceinline__ void pair_fixup_block(const SysConst &k, const DevState &d) {
-  const int n = *(volatile int *)d.fix_count;
+__global__ void __launch_bounds__(128) k_pair_fixup(SysConst k, DevState d) {
+  grid_dep_sync();
+  const int n = *d.fix_count;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const int p = d.fix_list[i];
     const int r = d.nrep == 1 ? 0 : rep_of_pair(d, p);
     pair_eval_fp64_sites<ND>(k, d, d.rep[r], p);
   }
+  __syncthreads();
+  if (threadIdx.x == 0) *d.fix_count = 0;
 }
 
 // Grid-stride over the pair slots, so a captured launch stays correct
 // whatever length the lists grow to between captures.  A single system's
 // list is the prefix of its segment; with several systems every slot checks
 // that it holds a current pair of its system.
-// NPX (mixed only): nearly parallel pairs are listed, and the last block to
-// finish (ticket counter, no waiting) evaluates the list in FP64 and resets
-// it for the next pair stage.
+// NPX (mixed only): nearly parallel pairs are listed for k_pair_fixup.
 template <int ND, int PREC, bool NPX>
-__global__ void __launch_bounds__(256, NPX ? 4 : 1) k_pair_eval(SysConst k, DevState d,
-                                                                int rbuf) {
-  bool listed = false;
+__global__ void __launch_bounds__(256) k_pair_eval(SysConst k, DevState d, int rbuf) {
+  grid_dep_sync();
   if (d.nrep == 1) {
     const ReplicaConst &R = d.rep[0];
     const int np = min(d.np_rep[0], R.pcap);
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
-      listed |= pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p);
-  } else {
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
-         p += gridDim.x * blockDim.x) {
-      int r;
-      if (pair_live(d, p, r)) listed |= pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p);
-    }
+      pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p);
+    return;
   }
-  if (!NPX) return;
-  __shared__ bool s_last;
-  if (listed) __threadfence();  // this thread's list entries, before the ticket
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(d.fix_done, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();  // every other block's entries are visible past its ticket
-  pair_fixup_block<ND>(k, d);
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    *d.fix_count = 0;
-    *d.fix_done = 0u;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
+       p += gridDim.x * blockDim.x) {
+    int r;
+    if (pair_live(d, p, r)) pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p);
   }
 }
 
@@ -758,6 +753,7 @@ __global__ void __launch_bounds__(256, NPX ? 4 : 1) k_pair_eval(SysConst k, DevS
 // for sc_interact and the getters.
 template <int ND, int PREC>
 __global__ void k_bond_sum(DevState d) {
+  grid_dep_sync();
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
   double F[3], T[3];
@@ -784,6 +780,7 @@ __global__ void k_bond_sum(DevState d) {
 // lengths are Bond::ReInit's (src/bond.cpp:22-37), from the sites.
 template <int ND>
 __global__ void k_mesh_lambda(DevState d) {
+  grid_dep_sync();
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= d.nf) return;
   const int s0 = d.fil[f].site0, nbf = d.fil[f].n - 1, b0 = s0 - f;
@@ -850,6 +847,7 @@ __device__ __forceinline__ double bond_reinit(const DevState &d, int b, double p
 // ST_TETHER.
 template <int ND>
 __global__ void k_tether(SysConst k, DevState d) {
+  grid_dep_sync();
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x >= d.nx) return;
   if (*d.status & ST_LIST_OVERFLOW) return;  // the step stopped at its rebuild
@@ -1181,6 +1179,20 @@ __global__ void __launch_bounds__(256) k_global_order(DevState d, double *out) {
 
 static inline int cdiv(long long a, int b) { return (int)((a + b - 1) / b); }
 
+// Programmatic dependent launch: on unless SIMCORE_PDL=0; PdlOff switches it
+// off for the launches of its thread while it lives.
+static bool pdl_default() {
+  const char *v = std::getenv("SIMCORE_PDL");
+  return !(v && v[0] == '0');
+}
+static thread_local bool t_pdl_off = false;
+bool pdl_enabled() {
+  static const bool on = pdl_default();
+  return on && !t_pdl_off;
+}
+PdlOff::PdlOff() : prev(t_pdl_off) { t_pdl_off = true; }
+PdlOff::~PdlOff() { t_pdl_off = prev; }
+
 void launch_init_geometry(const SysConst &k, const DevState &d, int buf,
                           int prec, cudaStream_t st, bool write_ub) {
   if (d.nb == 0) return;
@@ -1250,19 +1262,19 @@ int launch_exclusive_scan(const int *in, int *out, long long n, int *tmp, cudaSt
   if (tiles == 0) tiles = 1;
   const bool vec = (((uintptr_t)in | (uintptr_t)out) & 15u) == 0;
   if (vec) {
-    k_scan_reduce<true><<<tiles, SCAN_BLOCK, 0, st>>>(in, (int)n, tmp);
-    k_scan_down<true><<<tiles, SCAN_BLOCK, 0, st>>>(in, out, (int)n, tmp, occ);
+    launch_pdl(k_scan_reduce<true>, dim3(tiles), dim3(SCAN_BLOCK), 0, st, in, (int)n, tmp);
+    launch_pdl(k_scan_down<true>, dim3(tiles), dim3(SCAN_BLOCK), 0, st, in, out, (int)n, tmp, occ);
   } else {
-    k_scan_reduce<false><<<tiles, SCAN_BLOCK, 0, st>>>(in, (int)n, tmp);
-    k_scan_down<false><<<tiles, SCAN_BLOCK, 0, st>>>(in, out, (int)n, tmp, occ);
+    launch_pdl(k_scan_reduce<false>, dim3(tiles), dim3(SCAN_BLOCK), 0, st, in, (int)n, tmp);
+    launch_pdl(k_scan_down<false>, dim3(tiles), dim3(SCAN_BLOCK), 0, st, in, out, (int)n, tmp, occ);
   }
   return 2;
 }
 
 int launch_bin_count(const SysConst &k, const DevState &d, int *key,
                      int *cell_count, cudaStream_t st) {
-  if (k.n_dim == 3) k_bin_count<3><<<cdiv(d.nb, 256), 256, 0, st>>>(k, d, key, cell_count);
-  else k_bin_count<2><<<cdiv(d.nb, 256), 256, 0, st>>>(k, d, key, cell_count);
+  if (k.n_dim == 3) launch_pdl(k_bin_count<3>, dim3(cdiv(d.nb, 256)), dim3(256), 0, st, k, d, key, cell_count);
+  else launch_pdl(k_bin_count<2>, dim3(cdiv(d.nb, 256)), dim3(256), 0, st, k, d, key, cell_count);
   return 1;
 }
 
@@ -1275,14 +1287,14 @@ int launch_bond_cells(const SysConst &k, const DevState &d, int *xyz,
 
 int launch_bin_scatter(const DevState &d, const int *key, const int *cell_start,
                        int *cell_count, int *sorted, cudaStream_t st) {
-  k_bin_scatter<<<cdiv(d.nb, 256), 256, 0, st>>>(d, key, cell_start, cell_count, sorted);
+  launch_pdl(k_bin_scatter, dim3(cdiv(d.nb, 256)), dim3(256), 0, st, d, key, cell_start, cell_count, sorted);
   return 1;
 }
 
 int launch_cell_sort_count(const SysConst &k, const DevState &d, const int *key,
                            int *sorted, const int *cell_start, int *pair_count,
                            cudaStream_t st, const unsigned *occ) {
-  k_cell_sort_count<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted, cell_start,
+  launch_pdl(k_cell_sort_count, dim3(cdiv(d.nb, 128)), dim3(128), 0, st, k, d, d.nb, key, sorted, cell_start,
                                                      pair_count, occ);
   return 1;
 }
@@ -1291,15 +1303,15 @@ int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      const int *sorted, const int *cell_start,
                      const int *pair_off, int *deg, int prec,
                      cudaStream_t st, const unsigned *occ) {
-  k_pair_emit<<<cdiv(d.nb, 128), 128, 0, st>>>(k, d, d.nb, key, sorted, cell_start,
+  launch_pdl(k_pair_emit, dim3(cdiv(d.nb, 128)), dim3(128), 0, st, k, d, d.nb, key, sorted, cell_start,
                                                pair_off, deg, prec, occ);
   return 1;
 }
 
 int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st) {
-  k_csr_offsets<<<cdiv(d.nb, 256), 256, 0, st>>>(d, deg_off, deg);
-  k_csr_fill<<<cdiv(d.pcap_total > 0 ? d.pcap_total : 1, 256), 256, 0, st>>>(d, deg);
-  k_csr_sort_pos<<<cdiv(d.nb, 256), 256, 0, st>>>(d);
+  launch_pdl(k_csr_offsets, dim3(cdiv(d.nb, 256)), dim3(256), 0, st, d, deg_off, deg);
+  launch_pdl(k_csr_fill, dim3(cdiv(d.pcap_total > 0 ? d.pcap_total : 1, 256)), dim3(256), 0, st, d, deg);
+  launch_pdl(k_csr_sort_pos, dim3(cdiv(d.nb, 256)), dim3(256), 0, st, d);
   return 3;
 }
 
@@ -1348,7 +1360,10 @@ __global__ void k_loop_tail(DevState d, int stoch, cudaGraphConditionalHandle h)
   cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
 }
 
-__global__ void k_advance_mcount(DevState d) { *d.mcount += 1ull; }
+__global__ void k_advance_mcount(DevState d) {
+  grid_dep_sync();
+  *d.mcount += 1ull;
+}
 
 int launch_decide(const SysConst &k, const DevState &d,
                   cudaGraphConditionalHandle h, cudaStream_t st) {
@@ -1369,13 +1384,13 @@ int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
 }
 
 int launch_advance_mcount(const DevState &d, cudaStream_t st) {
-  k_advance_mcount<<<1, 1, 0, st>>>(d);
+  launch_pdl(k_advance_mcount, dim3(1), dim3(1), 0, st, d);
   return 1;
 }
 
 int launch_zero_dr(const DevState &d, cudaStream_t st) {
   const int n = d.ns > d.nrep ? d.ns : d.nrep;
-  k_zero_dr<<<cdiv(n > 0 ? n : 1, 256), 256, 0, st>>>(d);
+  launch_pdl(k_zero_dr, dim3(cdiv(n > 0 ? n : 1, 256)), dim3(256), 0, st, d);
   return 1;
 }
 
@@ -1385,15 +1400,18 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
   int grid = cdiv(expected > 0 ? expected : 1, 256);
   npx = npx && prec != 0;
   if (k.n_dim == 3) {
-    if (prec == 0) k_pair_eval<3, 0, false><<<grid, 256, 0, st>>>(k, d, rbuf);
-    else if (!npx) k_pair_eval<3, 1, false><<<grid, 256, 0, st>>>(k, d, rbuf);
-    else k_pair_eval<3, 1, true><<<grid, 256, 0, st>>>(k, d, rbuf);
+    if (prec == 0) launch_pdl(k_pair_eval<3, 0, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
+    else if (!npx) launch_pdl(k_pair_eval<3, 1, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
+    else launch_pdl(k_pair_eval<3, 1, true>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
   } else {
-    if (prec == 0) k_pair_eval<2, 0, false><<<grid, 256, 0, st>>>(k, d, rbuf);
-    else if (!npx) k_pair_eval<2, 1, false><<<grid, 256, 0, st>>>(k, d, rbuf);
-    else k_pair_eval<2, 1, true><<<grid, 256, 0, st>>>(k, d, rbuf);
+    if (prec == 0) launch_pdl(k_pair_eval<2, 0, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
+    else if (!npx) launch_pdl(k_pair_eval<2, 1, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
+    else launch_pdl(k_pair_eval<2, 1, true>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
   }
-  return 1;
+  if (!npx) return 1;
+  if (k.n_dim == 3) launch_pdl(k_pair_fixup<3>, dim3(1), dim3(128), 0, st, k, d);
+  else launch_pdl(k_pair_fixup<2>, dim3(1), dim3(128), 0, st, k, d);
+  return 2;
 }
 
 // ---------------------------------------------------------------------------
@@ -1412,6 +1430,7 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
 // agrees to rounding, and is the same on every run.
 template <int ND, int PREC>
 __global__ void __launch_bounds__(256) k_thermo(SysConst k, DevState d) {
+  grid_dep_sync();
   if (*d.status & ST_LIST_OVERFLOW) return;  // the step stopped at its rebuild
   const int r = blockIdx.y;
   const ReplicaConst &R = d.rep[r];
@@ -1529,11 +1548,11 @@ __global__ void k_potential(DevState d, double *out) {
 int launch_thermo(const SysConst &k, const DevState &d, int prec, cudaStream_t st) {
   const dim3 grid(d.th_gx, d.nrep);
   if (k.n_dim == 3) {
-    if (prec == 0) k_thermo<3, 0><<<grid, 256, 0, st>>>(k, d);
-    else k_thermo<3, 1><<<grid, 256, 0, st>>>(k, d);
+    if (prec == 0) launch_pdl(k_thermo<3, 0>, dim3(grid), dim3(256), 0, st, k, d);
+    else launch_pdl(k_thermo<3, 1>, dim3(grid), dim3(256), 0, st, k, d);
   } else {
-    if (prec == 0) k_thermo<2, 0><<<grid, 256, 0, st>>>(k, d);
-    else k_thermo<2, 1><<<grid, 256, 0, st>>>(k, d);
+    if (prec == 0) launch_pdl(k_thermo<2, 0>, dim3(grid), dim3(256), 0, st, k, d);
+    else launch_pdl(k_thermo<2, 1>, dim3(grid), dim3(256), 0, st, k, d);
   }
   return 1;
 }
@@ -1547,11 +1566,11 @@ int launch_potential(const DevState &d, int prec, double *out, cudaStream_t st) 
 int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st) {
   if (d.nx == 0) return 0;
   if (k.n_dim == 3) {
-    k_mesh_lambda<3><<<cdiv(d.nf, 128), 128, 0, st>>>(d);
-    k_tether<3><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
+    launch_pdl(k_mesh_lambda<3>, dim3(cdiv(d.nf, 128)), dim3(128), 0, st, d);
+    launch_pdl(k_tether<3>, dim3(cdiv(d.nx, 128)), dim3(128), 0, st, k, d);
   } else {
-    k_mesh_lambda<2><<<cdiv(d.nf, 128), 128, 0, st>>>(d);
-    k_tether<2><<<cdiv(d.nx, 128), 128, 0, st>>>(k, d);
+    launch_pdl(k_mesh_lambda<2>, dim3(cdiv(d.nf, 128)), dim3(128), 0, st, d);
+    launch_pdl(k_tether<2>, dim3(cdiv(d.nx, 128)), dim3(128), 0, st, k, d);
   }
   return 2;
 }
@@ -1559,11 +1578,11 @@ int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st) {
 int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st) {
   int grid = cdiv(d.nb, 256);
   if (k.n_dim == 3) {
-    if (prec == 0) k_bond_sum<3, 0><<<grid, 256, 0, st>>>(d);
-    else k_bond_sum<3, 1><<<grid, 256, 0, st>>>(d);
+    if (prec == 0) launch_pdl(k_bond_sum<3, 0>, dim3(grid), dim3(256), 0, st, d);
+    else launch_pdl(k_bond_sum<3, 1>, dim3(grid), dim3(256), 0, st, d);
   } else {
-    if (prec == 0) k_bond_sum<2, 0><<<grid, 256, 0, st>>>(d);
-    else k_bond_sum<2, 1><<<grid, 256, 0, st>>>(d);
+    if (prec == 0) launch_pdl(k_bond_sum<2, 0>, dim3(grid), dim3(256), 0, st, d);
+    else launch_pdl(k_bond_sum<2, 1>, dim3(grid), dim3(256), 0, st, d);
   }
   return 1;
 }
@@ -1611,7 +1630,7 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
   if (d.n_wg > 0) {
     const int grid = cdiv(d.n_wg, kIntWarps);
 #define SC_INTEGRATE_WARP(ND, P)                                              \
-  k_integrate_warp<ND, P, false><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf, \
+  launch_pdl(k_integrate_warp<ND, P, false>, dim3(grid), dim3(kIntWarps * 32), 0, st, k, d, midstep, rbuf, \
                                                                   interaction, capture)
     if (k.n_dim == 3) {
       if (prec == 0) SC_INTEGRATE_WARP(3, 0); else SC_INTEGRATE_WARP(3, 1);
@@ -1624,7 +1643,7 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
   if (nblocks == 0) return launched;
   size_t smem = integrate_smem_bytes(C);
 #define SC_INTEGRATE(ND, P, MC)                                              \
-  k_integrate<ND, P, false, MC><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf, \
+  launch_pdl(k_integrate<ND, P, false, MC>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf, \
                                                           interaction, capture)
   if (C <= 128) {
     if (k.n_dim == 3) {

@@ -71,7 +71,7 @@ int launch_zero_dr(const DevState &d, cudaStream_t st);
 // Grid sized for `expected` pairs (one system) or every slot (several); the
 // kernel strides over the actual pairs.
 // npx (mixed only): nearly parallel pairs are evaluated from the FP64
-// sites by the kernel's last block.
+// sites by a second, one-block kernel.
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
                  int expected, cudaStream_t st, bool npx = false);
 // Crosslink tethers of an even step into the per-anchor contributions.

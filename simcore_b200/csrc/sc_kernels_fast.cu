@@ -7,6 +7,7 @@
 
 #include "sc_common.cuh"
 #include "sc_kernels.h"
+#include "sc_launch.h"
 #include "sc_pair.cuh"
 #include "sc_step.cuh"
 #include "sc_step_warp.cuh"
@@ -41,20 +42,20 @@ static int launch_fast(const SysConst &k, const DevState &d, int nblocks, int C,
   int launched = 0;
   if (d.n_wg > 0) {
     const int grid = (d.n_wg + kIntWarps - 1) / kIntWarps;
-    k_integrate_warp<ND, 1, true, FUSE><<<grid, kIntWarps * 32, 0, st>>>(k, d, midstep, rbuf,
+    launch_pdl(k_integrate_warp<ND, 1, true, FUSE>, dim3(grid), dim3(kIntWarps * 32), 0, st, k, d, midstep, rbuf,
                                                                         interaction, capture);
     ++launched;
   }
   if (nblocks == 0) return launched;
   const size_t smem = integrate_smem_bytes(C);
   if (C <= 128)
-    k_integrate<ND, 1, true, 128, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
+    launch_pdl(k_integrate<ND, 1, true, 128, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
                                                                   interaction, capture);
   else if (C <= 192)
-    k_integrate<ND, 1, true, 192, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
+    launch_pdl(k_integrate<ND, 1, true, 192, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
                                                                   interaction, capture);
   else
-    k_integrate<ND, 1, true, 256, FUSE><<<nblocks, C, smem, st>>>(k, d, midstep, rbuf,
+    launch_pdl(k_integrate<ND, 1, true, 256, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
                                                                   interaction, capture);
   return launched + 1;
 }

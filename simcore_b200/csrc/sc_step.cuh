@@ -450,6 +450,10 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
 
   const int blk = blockIdx.x;
   const int t = threadIdx.x;
+  // Without a pair stage in between (fused pairs, or no interactions) the
+  // kernel before this one may be the previous integrator step, whose
+  // writes every load below reads: wait for it first.
+  if (FUSE || !interaction) grid_dep_sync();
   // A rebuild of this step whose list outgrew its segment stops the step
   // before its first store (uniform over the grid: nothing in this kernel
   // sets that bit), so the host can grow the list and redo the step.
@@ -502,6 +506,11 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     u[0] = d.ub[0][b];
     u[1] = d.ub[1][b];
     u[2] = d.ub[2][b];
+  }
+  // Everything above is the previous integrator step's or older; the pair
+  // stage just before this kernel writes the bond slots read below.
+  grid_dep_sync();
+  if (has_bond) {
     if (interaction) {
       // (The fused evaluation follows the pair list only when the rebuild
       // of this step completed it.)

@@ -37,6 +37,10 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
   const int t = threadIdx.x & 31;
   const int w = blockIdx.x * kIntWarps + (threadIdx.x >> 5);
   if (w >= d.n_wg) return;  // whole warps only: nothing below synchronises the block
+  // Without a pair stage in between (fused pairs, or no interactions) the
+  // kernel before this one may be the previous integrator step, whose
+  // writes every load below reads: wait for it first.
+  if (FUSE || !interaction) grid_dep_sync();
   double *sm = s_all[threadIdx.x >> 5];
   double *scos = sm;         // cos(theta) of joint j at lane j      32
   double *sa = sm + 32;      // Thomas lower diagonal                 32
@@ -84,6 +88,9 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
     }
     if (interaction) dtot = d.dt[g];
   }
+  // Everything above is the previous integrator step's or older; the pair
+  // stage just before this kernel writes the bond slots read below.
+  grid_dep_sync();
   double bF[3] = {0, 0, 0}, bT[3] = {0, 0, 0};
   if (has_bond && interaction) {
     // (The fused evaluation follows the pair list only when the rebuild of

@@ -46,11 +46,13 @@ def test_mixed_errors_isotropic_suspension():
 
 
 def test_mixed_errors_nematic_uneven_lengths():
-    """Nematic insertion starts every filament exactly parallel (both
+    """Workload C's stiffness spread and nematic insertion with 20-bond
+    filaments in a dense box (500 filaments, side 40: about 28,000 contacts).
+    Nematic insertion starts every filament exactly parallel (both
     precisions take the parallel branch); the noise then turns them by small
     angles, which is where FP32 orientations cannot resolve closest points."""
     from simcore_b200 import workloads
-    system, fils, sites = workloads.make("C", 0.004, seed=22)
+    system, fils, sites = workloads.make("C", 0.01, seed=22, n_seg=20, side=40.0)
     _check(_trajectory_errors(system, fils, sites, every=60))
 
 
