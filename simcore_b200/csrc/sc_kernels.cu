@@ -9,7 +9,7 @@
 //                  scatter order)
 //   pair forces    k_pair_eval   (InteractionManager::CalculatePairInteractions,
 //                                 one thread per pair, signed per-bond slots)
-//                  k_pair_fixup  (mixed: the nearly parallel pairs in FP64)
+//                                (mixed: nearly parallel pairs in FP64)
 //                  k_bond_sum    (ApplyPairInteractions into bond accumulators)
 //   thermo         k_thermo, k_potential (pair virial and pressure records,
 //                                 per-filament potential energy)
@@ -647,6 +647,46 @@ __device__ __forceinline__ void pair_eval_fp64_sites(const SysConst &k, const De
   c2[1] = make_float4(-(float)t2[1], -(float)t2[2], 0.f, 0.f);
 }
 
+// What the FP64 evaluation of one nearly parallel pair reads and writes,
+// passed by value so that the evaluation can be a separate function.
+struct NearParallelArgs {
+  const double *r0, *r1, *r2;
+  const int *bond_fil, *pa, *pb, *pos1, *pos2;
+  float *pf32, *pv32, *cf32;
+  const ReplicaConst *R;
+  double rcut2, c12, c6, fcut, eps;
+  int thermo;
+};
+
+// One nearly parallel pair of the mixed pair stage, evaluated from the FP64
+// sites (pair_eval_fp64_sites) by the thread that met it.  Not inlined: the
+// FP64 evaluation's registers and spills stay in this function, which runs
+// for a few pairs in ten thousand, and the FP32 path of k_pair_eval keeps its
+// register budget.
+template <int ND>
+__device__ __noinline__ void eval_near_parallel(NearParallelArgs a, int p) {
+  SysConst k;
+  k.rcut2 = a.rcut2;
+  k.c12 = a.c12;
+  k.c6 = a.c6;
+  k.fcut = a.fcut;
+  k.eps = a.eps;
+  k.thermo = a.thermo;
+  DevState d;
+  d.r[0] = const_cast<double *>(a.r0);
+  d.r[1] = const_cast<double *>(a.r1);
+  d.r[2] = const_cast<double *>(a.r2);
+  d.bond_fil = a.bond_fil;
+  d.pa = const_cast<int *>(a.pa);
+  d.pb = const_cast<int *>(a.pb);
+  d.pos1 = const_cast<int *>(a.pos1);
+  d.pos2 = const_cast<int *>(a.pos2);
+  d.pf32 = a.pf32;
+  d.pv32 = a.pv32;
+  d.cf32 = a.cf32;
+  pair_eval_fp64_sites<ND>(k, d, *a.R, p);
+}
+
 template <int ND, int PREC, bool NPX>
 __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
                                               const ReplicaConst &R, int rbuf, int p) {
@@ -688,8 +728,27 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
-    if (NPX && near_parallel<ND>(A, B)) {  // left to k_pair_fixup
-      d.fix_list[atomicAdd(d.fix_count, 1)] = p;
+    if (NPX && near_parallel<ND>(A, B)) {
+      NearParallelArgs na;
+      na.r0 = d.r[0];
+      na.r1 = d.r[1];
+      na.r2 = d.r[2];
+      na.bond_fil = d.bond_fil;
+      na.pa = d.pa;
+      na.pb = d.pb;
+      na.pos1 = d.pos1;
+      na.pos2 = d.pos2;
+      na.pf32 = d.pf32;
+      na.pv32 = d.pv32;
+      na.cf32 = d.cf32;
+      na.R = &R;
+      na.rcut2 = k.rcut2;
+      na.c12 = k.c12;
+      na.c6 = k.c6;
+      na.fcut = k.fcut;
+      na.eps = k.eps;
+      na.thermo = k.thermo;
+      eval_near_parallel<ND>(na, p);
       return;
     }
     float force[3], rec[4], t1[3], t2[3];
@@ -709,31 +768,14 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
   }
 }
 
-// The nearly parallel pairs the NPX mixed pair stage listed, evaluated from
-// the FP64 sites (pair_eval_fp64_sites), then the list reset for the next
-// pair stage.  One block: the list is short (most steps of most workloads
-// have none), and this kernel's registers and spills stay out of the FP32
-// pair kernel.
-template <int ND>
-__global__ void __launch_bounds__(128) k_pair_fixup(SysConst k, DevState d) {
-  grid_dep_sync();
-  const int n = *d.fix_count;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const int p = d.fix_list[i];
-    const int r = d.nrep == 1 ? 0 : rep_of_pair(d, p);
-    pair_eval_fp64_sites<ND>(k, d, d.rep[r], p);
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) *d.fix_count = 0;
-}
-
 // Grid-stride over the pair slots, so a captured launch stays correct
 // whatever length the lists grow to between captures.  A single system's
 // list is the prefix of its segment; with several systems every slot checks
 // that it holds a current pair of its system.
-// NPX (mixed only): nearly parallel pairs are listed for k_pair_fixup.
+// NPX (mixed only): nearly parallel pairs are evaluated in FP64
+// (eval_near_parallel) by the thread that meets them.
 template <int ND, int PREC, bool NPX>
-__global__ void __launch_bounds__(256) k_pair_eval(SysConst k, DevState d, int rbuf) {
+__global__ void __launch_bounds__(256, NPX ? 5 : 1) k_pair_eval(SysConst k, DevState d, int rbuf) {
   grid_dep_sync();
   if (d.nrep == 1) {
     const ReplicaConst &R = d.rep[0];
@@ -1408,10 +1450,7 @@ int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
     else if (!npx) launch_pdl(k_pair_eval<2, 1, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
     else launch_pdl(k_pair_eval<2, 1, true>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
   }
-  if (!npx) return 1;
-  if (k.n_dim == 3) launch_pdl(k_pair_fixup<3>, dim3(1), dim3(128), 0, st, k, d);
-  else launch_pdl(k_pair_fixup<2>, dim3(1), dim3(128), 0, st, k, d);
-  return 2;
+  return 1;
 }
 
 // ---------------------------------------------------------------------------

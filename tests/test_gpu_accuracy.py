@@ -64,8 +64,11 @@ def test_mixed_errors_replica_batch():
 
 
 def test_mixed_errors_tethered_network():
+    """Workload E's density, stiffness and tethers with 10-bond filaments, so
+    that filaments are shorter than the small box (longer ones would overlap
+    their own periodic images)."""
     from simcore_b200 import workloads
-    system, fils, sites = workloads.make("E", 0.02, seed=24)
+    system, fils, sites = workloads.make("E", 0.02, seed=24, n_seg=10)
     xl = workloads.crosslinks("E", sites, fils, 2 * system["system_radius"], scale=0.02,
                               seed=24)
     _check(_trajectory_errors(system, fils, sites, crosslinks=xl, every=30))
