@@ -593,14 +593,22 @@ __device__ __forceinline__ void bond_geom_from_sites(const DevState &d, const Re
   G.pad = 0.0;
 }
 
-// Nearly parallel segments in the mixed pair stage: |u1 x u2|^2 in FP32
-// (accurate where 1 - (u1 . u2)^2 is rounding alone) above 0 and below
-// 1e-5, i.e. within 0.18 degrees.  For them the closest points depend on
-// orientation bits FP32 does not hold, so they are evaluated in FP64, from
-// the sites (pair_eval_fp64_sites).  Exactly parallel FP32 orientations take the parallel branch
-// in both precisions (their FP64 1 - c^2 is below the reference's 1e-12).
+// Nearly parallel contacts of the mixed pair stage, which FP32 cannot
+// evaluate: segments within 0.18 degrees of parallel (FP32 |u1 x u2|^2,
+// accurate where 1 - (u1 . u2)^2 is rounding alone, above 0 and below 1e-5)
+// that lie side by side -- their projections on A's axis overlap, or nearly
+// -- and near enough to interact, or that carry a stored force.  Side by
+// side, the closest points can be anywhere along the overlap, and which end
+// the reference picks hangs on orientation bits FP32 does not hold; such
+// pairs are evaluated in FP64, from the sites (pair_eval_fp64_sites).
+// Nearly parallel segments that do not overlap (the next-nearest bonds of a
+// straight filament) meet at a unique pair of facing ends, which FP32 finds.
+// Exactly parallel FP32 orientations take the parallel branch in both
+// precisions (their FP64 1 - c^2 is below the reference's 1e-12).
 template <int ND>
-__device__ __forceinline__ bool near_parallel(const BondGeomF32 &A, const BondGeomF32 &B) {
+__device__ __forceinline__ bool near_parallel(const SysConst &k, const float *hf,
+                                              const BondGeomF32 &A, const BondGeomF32 &B,
+                                              const float4 &st) {
   float s2;
   const float cz = __fmaf_rn(A.u[0], B.u[1], -A.u[1] * B.u[0]);
   if (ND == 3) {
@@ -610,7 +618,26 @@ __device__ __forceinline__ bool near_parallel(const BondGeomF32 &A, const BondGe
   } else {
     s2 = cz * cz;
   }
-  return s2 > 0.f && s2 < 1e-5f;
+  if (!(s2 > 0.f && s2 < 1e-5f)) return false;
+  float dr[3] = {0.f, 0.f, 0.f}, a1 = 0.f, r2 = 0.f;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < ND; ++j) {
+      const int32_t dq = (int32_t)((uint32_t)B.q[j] - (uint32_t)A.q[j]);
+      acc = __fmaf_rn(hf[ND * i + j], (float)dq * 2.3283064365386963e-10f, acc);
+    }
+    dr[i] = acc;
+  }
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    a1 = __fmaf_rn(dr[i], A.u[i], a1);
+    r2 = __fmaf_rn(dr[i], dr[i], r2);
+  }
+  if (fabsf(a1) > A.hl + B.hl + 0.25f) return false;  // end to end: facing ends
+  const bool loaded = st.x != 0.f || st.y != 0.f || st.z != 0.f;
+  return loaded || r2 - a1 * a1 < 1.5f * k.rcut2f;
 }
 
 // A nearly parallel pair of the mixed pair stage, evaluated as the FP64 path
@@ -728,7 +755,7 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
-    if (NPX && near_parallel<ND>(A, B)) {
+    if (NPX && near_parallel<ND>(k, R.hf, A, B, st)) {
       NearParallelArgs na;
       na.r0 = d.r[0];
       na.r1 = d.r[1];
