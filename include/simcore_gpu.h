@@ -105,7 +105,9 @@ const char *sc_last_error(const sc_ctx *ctx);
  * src/simulation.cpp:261-405 minus the random insertion): n filaments with
  * their parameters and site positions (n_sites_total x 3 doubles, each
  * filament's sites tail to head).  Builds the initial pair list as the
- * forced update that ends the reference's insertion does. */
+ * forced update that ends the reference's insertion does.  A filament has at
+ * most 511 bonds (the reference's max_length of 500 at min_bond_length
+ * 0.666 gives 500). */
 sc_status sc_add_filaments(sc_ctx *ctx, int n, const sc_filament_params *p,
                            const double *site_xyz, int64_t n_sites_total);
 
@@ -286,7 +288,7 @@ sc_status sc_set_fast_integrator(sc_ctx *ctx, int on);
  * filaments of at most warp_max_sites sites (<= 32) run on the
  * warp-synchronous kernel, one warp per group of whole filaments; longer
  * ones on the block kernel, block_sites sites per block (a multiple of 32 up
- * to 256, at least the longest such filament; 0 picks 128 or 256).
+ * to 512, at least the longest such filament; 0 picks 128, 256 or 512).
  * warp_max_sites 0 puts every filament on the block kernel. */
 sc_status sc_set_integrator_layout(sc_ctx *ctx, int warp_max_sites, int block_sites);
 /* Autotuner for the layout above: times every candidate on the context's

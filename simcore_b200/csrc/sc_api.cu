@@ -83,7 +83,7 @@ struct sc_ctx {
   // integrator blocks
   int nblocks = 0, C = 128;
   int warp_sites = 32;             // longest filament for the warp-synchronous kernel
-  int block_sites = 0;             // sites per block of the block kernel (0: 128 or 256)
+  int block_sites = 0;             // sites per block of the block kernel (0: 128, 256 or 512)
 
   // control state
   long long i_step = 0, n_rebuilds = 0, launches = 0;
@@ -576,7 +576,8 @@ sc_status layout_integrator(sc_ctx *c) {
   auto short_fil = [&](int f) { return off[f + 1] - off[f] <= c->warp_sites; };
   for (int f = 0; f < n; ++f)
     if (!short_fil(f)) max_long = std::max(max_long, off[f + 1] - off[f]);
-  c->C = c->block_sites > 0 ? c->block_sites : (max_long <= 128 ? 128 : 256);
+  c->C = c->block_sites > 0 ? c->block_sites
+                            : (max_long <= 128 ? 128 : max_long <= 256 ? 256 : 512);
   if (max_long > c->C)
     return fail(c, SC_ERR_INVALID_ARG, "a %d-site filament does not fit %d-site blocks", max_long,
                 c->C);
@@ -975,8 +976,8 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
   if (ns != n_sites_total)
     return fail(c, SC_ERR_INVALID_ARG, "n_sites_total %lld != %lld implied by the lengths",
                 (long long)n_sites_total, ns);
-  if (max_ns > 256)
-    return fail(c, SC_ERR_INVALID_ARG, "filaments longer than 255 bonds are not supported");
+  if (max_ns > 512)
+    return fail(c, SC_ERR_INVALID_ARG, "filaments longer than 511 bonds are not supported");
   if (ns > (1ll << 30)) return fail(c, SC_ERR_INVALID_ARG, "too many sites");
   const int nsi = (int)ns, nbi = nsi - n;
   c->nf = n;
@@ -1510,8 +1511,8 @@ sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
 
 sc_status sc_set_integrator_layout(sc_ctx *c, int warp_max_sites, int block_sites) {
   if (!c || !c->loaded || warp_max_sites < 0 || warp_max_sites > 32) return SC_ERR_INVALID_ARG;
-  if (block_sites != 0 && (block_sites < 32 || block_sites > 256 || block_sites % 32))
-    return fail(c, SC_ERR_INVALID_ARG, "block_sites must be 0 or a multiple of 32 in [32, 256]");
+  if (block_sites != 0 && (block_sites < 32 || block_sites > 512 || block_sites % 32))
+    return fail(c, SC_ERR_INVALID_ARG, "block_sites must be 0 or a multiple of 32 in [32, 512]");
   CK(cudaSetDevice(c->desc.device));
   const int ow = c->warp_sites, ob = c->block_sites;
   c->warp_sites = warp_max_sites;
@@ -1583,8 +1584,8 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
       cand.push_back({w, 0});
       continue;
     }
-    for (int bsz : {64, 96, 128, 160, 192, 256})
-      if (bsz >= longest) cand.push_back({w, bsz});
+    for (int bsz : {64, 96, 128, 160, 192, 256, 512})
+      if (bsz >= longest && (bsz < 512 || longest > 256)) cand.push_back({w, bsz});
   }
   // Save what the integrator writes.
   const int wbuf = 1 - c->rbuf;

@@ -1677,11 +1677,16 @@ void prepare_integrate(int C) {
     set_attr<3, 1, 192>(smem);
     set_attr<2, 0, 192>(smem);
     set_attr<2, 1, 192>(smem);
-  } else {
+  } else if (C <= 256) {
     set_attr<3, 0, 256>(smem);
     set_attr<3, 1, 256>(smem);
     set_attr<2, 0, 256>(smem);
     set_attr<2, 1, 256>(smem);
+  } else {
+    set_attr<3, 0, 512>(smem);
+    set_attr<3, 1, 512>(smem);
+    set_attr<2, 0, 512>(smem);
+    set_attr<2, 1, 512>(smem);
   }
   prepare_integrate_fast(C);
 }
@@ -1723,11 +1728,17 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
     } else {
       if (prec == 0) SC_INTEGRATE(2, 0, 192); else SC_INTEGRATE(2, 1, 192);
     }
-  } else {
+  } else if (C <= 256) {
     if (k.n_dim == 3) {
       if (prec == 0) SC_INTEGRATE(3, 0, 256); else SC_INTEGRATE(3, 1, 256);
     } else {
       if (prec == 0) SC_INTEGRATE(2, 0, 256); else SC_INTEGRATE(2, 1, 256);
+    }
+  } else {
+    if (k.n_dim == 3) {
+      if (prec == 0) SC_INTEGRATE(3, 0, 512); else SC_INTEGRATE(3, 1, 512);
+    } else {
+      if (prec == 0) SC_INTEGRATE(2, 0, 512); else SC_INTEGRATE(2, 1, 512);
     }
   }
 #undef SC_INTEGRATE

@@ -30,9 +30,12 @@ void prepare_integrate_fast(int C) {
   } else if (C <= 192) {
     set_attr_fast<3, 192>(smem);
     set_attr_fast<2, 192>(smem);
-  } else {
+  } else if (C <= 256) {
     set_attr_fast<3, 256>(smem);
     set_attr_fast<2, 256>(smem);
+  } else {
+    set_attr_fast<3, 512>(smem);
+    set_attr_fast<2, 512>(smem);
   }
 }
 
@@ -54,8 +57,11 @@ static int launch_fast(const SysConst &k, const DevState &d, int nblocks, int C,
   else if (C <= 192)
     launch_pdl(k_integrate<ND, 1, true, 192, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
                                                                   interaction, capture);
-  else
+  else if (C <= 256)
     launch_pdl(k_integrate<ND, 1, true, 256, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
+                                                                  interaction, capture);
+  else
+    launch_pdl(k_integrate<ND, 1, true, 512, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
                                                                   interaction, capture);
   return launched + 1;
 }

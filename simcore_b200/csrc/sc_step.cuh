@@ -404,7 +404,8 @@ __device__ __forceinline__ void pcr_block(double *a, double *b, double *c, doubl
 }
 
 // Rows of the longest system (bonds of the longest filament) above which the
-// fast 256-site integrator solves by pcr_block instead of Thomas lanes.
+// fast 256- and 512-site integrators solve by pcr_block instead of Thomas
+// lanes.
 constexpr int kPcrMinRows = 32;
 
 template <int MAXC, bool FAST>
@@ -413,7 +414,7 @@ struct IntegrateBounds {
   // also holds 4 blocks of 192 sites per SM (2 waves of 17-filament blocks
   // for 20,000 11-site filaments on 148 SMs).
   static constexpr int min_blocks =
-      MAXC <= 128 ? (FAST ? 6 : 5) : MAXC <= 192 ? (FAST ? 4 : 3) : 2;
+      MAXC <= 128 ? (FAST ? 6 : 5) : MAXC <= 192 ? (FAST ? 4 : 3) : MAXC <= 256 ? 2 : 1;
 };
 
 // FUSE (fast mixed step only): each bond evaluates its own pairs

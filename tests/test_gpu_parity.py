@@ -349,6 +349,35 @@ def test_crosslinks_match_reference_fixture(name):
         ctx.close()
 
 
+def test_fp64_filaments_up_to_500_bonds_bitwise():
+    """The reference's longest filaments (max_length 500: 500 bonds at
+    min_bond_length 0.666) run on 512-site integrator blocks: bit-identical to
+    the oracle over host-driven and captured steps, and the mixed path (block
+    PCR) close to it."""
+    import simcore_b200 as sc
+    lengths = [500.0, 420.0, 300.0, 12.0]
+    n_bonds = np.array([int(L) for L in lengths], dtype=np.int32)
+    fils = [dict(length=L, persistence_length=200.0, diameter=1.0, min_bond_length=0.666,
+                 friction_ratio=2.0) for L in lengths]
+    assert [sc.filament_n_bonds(f) for f in fils] == list(n_bonds)
+    sites = sc.insert_filaments(3, 300.0, 3, n_bonds, np.array(lengths), np.full(4, 200.0))
+    system = dict(n_dim=3, system_radius=300.0, delta=1e-4, seed=3)
+    ctx = _ctx(system, fils, sites)
+    o = Oracle(system, fils, sites)
+    ctx.step(3)
+    o.step(3)
+    compare_state(ctx, o, 3, capture=False)
+    ctx.step_graph(40)
+    o.step(40)
+    assert_same(ctx.sites(), o.sites(), "sites")
+    mixed = _ctx(system, fils, sites, "mixed")
+    exact = Oracle(system, fils, sites)
+    mixed.step(3)
+    exact.step(3)
+    d, want = mixed.sites() - sites, exact.sites() - sites
+    assert np.abs(d - want).max() <= 1e-6 * np.abs(want).max()
+
+
 def test_fp64_uneven_lengths_bitwise():
     """Workload C's length and stiffness spread (5 to 200 bonds, log-uniform;
     lp uniform in [10, 1000]) on 100 filaments: 256-site integrator blocks
@@ -620,10 +649,55 @@ def test_non_finite_positions_are_reported():
     assert e.value.code == 3
 
 
+@pytest.mark.parametrize("graph", [False, True])
+def test_unphysical_displacement_is_reported(graph):
+    """A filament moved by 80 (set_sites) accumulates 2 x 80^2 > 10000 in its
+    displacement tracker at the next full step, which the reference rejects
+    as an "Unphysical result" (include/simcore/species.hpp:114-118): the step
+    fails with SC_ERR_UNPHYSICAL, host-driven and inside a captured run."""
+    import simcore_b200 as sc
+    system, fils, sites = _workload("B", 0.02, seed=14)
+    ctx = _ctx(system, fils, sites, "mixed")
+    ctx.step(2)
+    moved = ctx.sites()
+    moved[:11, 0] += 80.0  # the first filament
+    ctx.set_sites(moved)
+    with pytest.raises(sc.ScError) as e:
+        if graph:
+            ctx.step_graph(20)
+        else:
+            ctx.step(6)
+        ctx.synchronize()
+    assert e.value.code == 7  # SC_ERR_UNPHYSICAL
+
+
+def test_replica_list_overflow_is_reported():
+    """Independent systems keep fixed pair segments (half again the initial
+    list, plus 1,024).  Squeezing one small system's filaments into 0.3 of
+    its box (shifts far below the unphysical bound) multiplies its density by
+    eleven; the rebuild that follows outgrows the segment:
+    SC_ERR_LIST_OVERFLOW."""
+    import simcore_b200 as sc
+    from simcore_b200 import workloads
+    system, fils, sites, reps = workloads.make_replicas("D", n_replicas=3, fil_scale=0.02,
+                                                        seed=15)
+    ctx = _ctx_replicas(system, fils, sites, reps, "mixed")
+    ctx.step(2)
+    xyz = ctx.sites()
+    n0 = reps[0]["n_filaments"] * 17  # sites of system 0 (16 bonds a filament)
+    xyz[:n0, :2] *= 0.3
+    assert 0.7 * np.abs(xyz[:n0, :2]).max() / 0.3 < 65.0
+    ctx.set_sites(xyz)
+    with pytest.raises(sc.ScError) as e:
+        ctx.step(8)
+        ctx.synchronize()
+    assert e.value.code == 4  # SC_ERR_LIST_OVERFLOW
+
+
 def test_invalid_inputs_are_rejected():
     """Inputs the library cannot take fail with an error status and a
     message, before any device work: no filaments, inconsistent site counts,
-    bad parameters, filaments past the 255-bond limit, cell grids too large
+    bad parameters, filaments past the 511-bond limit, cell grids too large
     to count, negative step counts."""
     import simcore_b200 as sc
     system, fils, sites = _workload("A", 0.05, seed=1)
@@ -635,10 +709,10 @@ def test_invalid_inputs_are_rejected():
     bad[0]["length"] = 0.0
     with pytest.raises(sc.ScError, match="bad parameters"):
         _ctx(system, bad, sites)
-    long_fil = dict(fils[0], length=300.0)
+    long_fil = dict(fils[0], length=400.0, min_bond_length=0.5)
     n = sc.filament_n_bonds(long_fil) + 1
-    assert n > 256
-    with pytest.raises(sc.ScError, match="255 bonds"):
+    assert n > 512
+    with pytest.raises(sc.ScError, match="511 bonds"):
         _ctx(system, [long_fil], np.zeros((n, 3)))
     # Cell grids are bounded while their size is still a double: a radius of
     # 2.4e6 (2^22 cells a side, whose cube wraps a 64-bit count to 0) and an
