@@ -390,6 +390,18 @@ int sc_insert_filaments(int n_dim, double system_radius, uint64_t seed,
                         int n_fil, const int *n_bonds, const double *length,
                         const double *persistence_length, double diameter,
                         int insertion_type, int max_attempts, double *site_xyz);
+/* The same insertion with the overlap tests on GPU `device`: the result is
+ * sc_insert_filaments' for the same arguments, bit for bit.  Candidates of
+ * the next filaments are drawn on the host at the stream positions they
+ * take if every earlier one succeeds; the GPU tests each candidate bond
+ * against the accepted bonds and the earlier candidates of the batch, and
+ * the candidates before the first one that overlaps are accepted.  No
+ * counterpart beyond the reference's insertion (src/simulation.cpp:261-405),
+ * which runs serially. */
+int sc_insert_filaments_gpu(int device, int n_dim, double system_radius, uint64_t seed,
+                            int n_fil, const int *n_bonds, const double *length,
+                            const double *persistence_length, double diameter,
+                            int insertion_type, int max_attempts, double *site_xyz);
 
 #ifdef __cplusplus
 }

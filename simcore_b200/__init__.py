@@ -39,7 +39,7 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_analysis_sample", "sc_analysis_results", "sc_global_order",
             "sc_set_thermo", "sc_thermo_open", "sc_get_thermo", "sc_get_potential_energy",
             "sc_set_exact_near_parallel", "sc_set_fused_pairs", "sc_diffusion_init",
-            "sc_diffusion_sample", "sc_diffusion_results"]
+            "sc_diffusion_sample", "sc_diffusion_results", "sc_insert_filaments_gpu"]
 
 
 class ScError(RuntimeError):
@@ -106,17 +106,22 @@ INSERTION = {"random": 0, "random_nematic": 1, "random_polar": 2}
 
 
 def insert_filaments(n_dim, system_radius, seed, n_bonds, lengths, persistence_lengths,
-                     diameter=1.0, max_attempts=10000, insertion="random"):
-    """Seeded random insertion with overlap rejection (host).  Returns sites."""
+                     diameter=1.0, max_attempts=10000, insertion="random", device=None):
+    """Seeded random insertion with overlap rejection.  Returns sites.  With
+    a device, the overlap tests run on that GPU (sc_insert_filaments_gpu);
+    the result is the same, bit for bit."""
     n_bonds = np.ascontiguousarray(n_bonds, dtype=np.int32)
     lengths = np.ascontiguousarray(lengths, dtype=np.float64)
     lps = np.ascontiguousarray(persistence_lengths, dtype=np.float64)
     xyz = np.zeros((int(np.sum(n_bonds + 1)), 3))
-    rc = lib.sc_insert_filaments(ctypes.c_int(n_dim), ctypes.c_double(system_radius),
-                                 ctypes.c_uint64(seed), ctypes.c_int(len(n_bonds)),
-                                 _p(n_bonds), _p(lengths), _p(lps), ctypes.c_double(diameter),
-                                 ctypes.c_int(INSERTION[insertion]),
-                                 ctypes.c_int(max_attempts), _p(xyz))
+    args = (ctypes.c_int(n_dim), ctypes.c_double(system_radius), ctypes.c_uint64(seed),
+            ctypes.c_int(len(n_bonds)), _p(n_bonds), _p(lengths), _p(lps),
+            ctypes.c_double(diameter), ctypes.c_int(INSERTION[insertion]),
+            ctypes.c_int(max_attempts), _p(xyz))
+    if device is None:
+        rc = lib.sc_insert_filaments(*args)
+    else:
+        rc = lib.sc_insert_filaments_gpu(ctypes.c_int(device), *args)
     if rc != SC_OK:
         raise ScError(rc, "random insertion failed")
     return xyz

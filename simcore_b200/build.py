@@ -16,7 +16,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsimcore_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["sc_kernels.cu", "sc_kernels_fast.cu", "sc_api.cu", "sc_noalloc.cu"]
+CU_SOURCES = ["sc_kernels.cu", "sc_kernels_fast.cu", "sc_api.cu", "sc_noalloc.cu",
+              "sc_insert_gpu.cu"]
 # Units compiled with FMA contraction (everything else keeps --fmad=false).
 FMAD_SOURCES = {"sc_kernels_fast.cu"}
 CPP_SOURCES = ["sc_insert.cpp"]

@@ -123,6 +123,78 @@ struct Grid {
 
 }  // namespace
 
+// One insertion attempt of a filament of nb bonds (length `length`,
+// persistence length lp) drawn from the stream (k0, k1) at position k:
+// site positions (3 (nb + 1)), bond centres and unit axes (3 nb each).
+// Returns the stream position after the attempt's draws; the number of draws
+// depends only on the insertion type, n_dim and nb.
+uint64_t sc_insert_candidate(int n_dim, double system_radius, double diameter,
+                             int insertion_type, int nb, double length, double lp,
+                             uint32_t k0, uint32_t k1, uint64_t k, double *pos, double *cen,
+                             double *axis) {
+  Stream rng{k0, k1, k};
+  const double l = length / nb;
+  std::memset(pos, 0, sizeof(double) * 3 * (nb + 1));
+  std::memset(cen, 0, sizeof(double) * 3 * nb);
+  std::memset(axis, 0, sizeof(double) * 3 * nb);
+  double u[3] = {0, 0, 0}, p[3] = {0, 0, 0};
+  if (insertion_type == SC_INSERT_RANDOM) {
+    // RNG::RandomUnitVector (src/rng.cpp:34-49)
+    double w = 1.0;
+    if (n_dim == 3) {
+      double z = 2.0 * rng.uniform() - 1.0;
+      w = std::sqrt(1 - z * z);
+      u[2] = z;
+    }
+    double t = 2.0 * M_PI * rng.uniform();
+    u[0] = w * std::cos(t);
+    u[1] = w * std::sin(t);
+  } else {
+    // Filament::InsertFirstBond, random_nematic / random_polar
+    // (src/filament.cpp:195-202): along +-z (+-y in 2D), straight.
+    u[n_dim - 1] = insertion_type == SC_INSERT_RANDOM_POLAR
+                       ? 1.0
+                       : (rng.uniform() > 0.5 ? 1.0 : -1.0);
+  }
+  // RNG::RandomCoordinate, box/none (src/rng.cpp:50-66)
+  for (int i = 0; i < n_dim; ++i) p[i] = (2.0 * rng.uniform() - 1.0) * (system_radius - diameter);
+  for (int i = 0; i < n_dim; ++i) p[i] -= 0.5 * u[i] * length;
+  for (int i = 0; i < 3; ++i) pos[i] = p[i];
+  for (int b = 0; b < nb; ++b) {
+    if (b > 0 && insertion_type == SC_INSERT_RANDOM) {
+      // Filament::GenerateProbableOrientation
+      double kk = lp / l, theta;
+      if (lp == 0) {
+        theta = rng.uniform() * M_PI;
+      } else if (lp < 100) {
+        theta = std::acos(std::log(std::exp(-kk) + 2.0 * rng.uniform() * std::sinh(kk)) / kk);
+      } else {
+        theta = std::acos((std::log(2.0 * rng.uniform()) - std::log(2.0) + kk) / kk);
+      }
+      double nu[3] = {0, 0, 0};
+      if (n_dim == 2) {
+        theta = (rng.uniform() < 0.5 ? -1 : 1) * theta;
+        nu[0] = std::cos(theta);
+        nu[1] = std::sin(theta);
+      } else {
+        double phi = rng.uniform() * 2.0 * M_PI;
+        nu[0] = std::sin(theta) * std::cos(phi);
+        nu[1] = std::sin(theta) * std::sin(phi);
+        nu[2] = std::cos(theta);
+      }
+      rotate_relative(n_dim, nu, u);
+      double m = std::sqrt(dot3(nu, nu));
+      for (int i = 0; i < 3; ++i) u[i] = nu[i] / m;
+    }
+    for (int i = 0; i < n_dim; ++i) pos[3 * (b + 1) + i] = pos[3 * b + i] + l * u[i];
+    for (int i = 0; i < n_dim; ++i) {
+      cen[3 * b + i] = pos[3 * b + i] + 0.5 * l * u[i];
+      axis[3 * b + i] = u[i];
+    }
+  }
+  return rng.k;
+}
+
 extern "C" int sc_insert_filaments(int n_dim, double system_radius,
                                    uint64_t seed, int n_fil,
                                    const int *n_bonds, const double *length,
@@ -161,67 +233,12 @@ extern "C" int sc_insert_filaments(int n_dim, double system_radius,
     const double l = length[f] / nb, lp = persistence_length[f];
     bool placed = false;
     for (int attempt = 0; attempt < max_attempts && !placed; ++attempt) {
-      pos.assign(3 * (nb + 1), 0.0);
-      cen.assign(3 * nb, 0.0);
-      axis.assign(3 * nb, 0.0);
-      double u[3] = {0, 0, 0}, p[3] = {0, 0, 0};
-      if (insertion_type == SC_INSERT_RANDOM) {
-        // RNG::RandomUnitVector (src/rng.cpp:34-49)
-        double w = 1.0;
-        if (n_dim == 3) {
-          double z = 2.0 * rng.uniform() - 1.0;
-          w = std::sqrt(1 - z * z);
-          u[2] = z;
-        }
-        double t = 2.0 * M_PI * rng.uniform();
-        u[0] = w * std::cos(t);
-        u[1] = w * std::sin(t);
-      } else {
-        // Filament::InsertFirstBond, random_nematic / random_polar
-        // (src/filament.cpp:195-202): along +-z (+-y in 2D), straight.
-        u[n_dim - 1] = insertion_type == SC_INSERT_RANDOM_POLAR
-                           ? 1.0
-                           : (rng.uniform() > 0.5 ? 1.0 : -1.0);
-      }
-      // RNG::RandomCoordinate, box/none (src/rng.cpp:50-66)
-      for (int i = 0; i < n_dim; ++i)
-        p[i] = (2.0 * rng.uniform() - 1.0) * (system_radius - diameter);
-      for (int i = 0; i < n_dim; ++i) p[i] -= 0.5 * u[i] * length[f];
-      for (int i = 0; i < 3; ++i) pos[i] = p[i];
-      for (int b = 0; b < nb; ++b) {
-        if (b > 0 && insertion_type == SC_INSERT_RANDOM) {
-          // Filament::GenerateProbableOrientation
-          double k = lp / l, theta;
-          if (lp == 0) {
-            theta = rng.uniform() * M_PI;
-          } else if (lp < 100) {
-            theta = std::acos(std::log(std::exp(-k) +
-                                       2.0 * rng.uniform() * std::sinh(k)) /
-                              k);
-          } else {
-            theta = std::acos((std::log(2.0 * rng.uniform()) - std::log(2.0) + k) / k);
-          }
-          double nu[3] = {0, 0, 0};
-          if (n_dim == 2) {
-            theta = (rng.uniform() < 0.5 ? -1 : 1) * theta;
-            nu[0] = std::cos(theta);
-            nu[1] = std::sin(theta);
-          } else {
-            double phi = rng.uniform() * 2.0 * M_PI;
-            nu[0] = std::sin(theta) * std::cos(phi);
-            nu[1] = std::sin(theta) * std::sin(phi);
-            nu[2] = std::cos(theta);
-          }
-          rotate_relative(n_dim, nu, u);
-          double m = std::sqrt(dot3(nu, nu));
-          for (int i = 0; i < 3; ++i) u[i] = nu[i] / m;
-        }
-        for (int i = 0; i < n_dim; ++i) pos[3 * (b + 1) + i] = pos[3 * b + i] + l * u[i];
-        for (int i = 0; i < n_dim; ++i) {
-          cen[3 * b + i] = pos[3 * b + i] + 0.5 * l * u[i];
-          axis[3 * b + i] = u[i];
-        }
-      }
+      pos.resize(3 * (nb + 1));
+      cen.resize(3 * nb);
+      axis.resize(3 * nb);
+      rng.k = sc_insert_candidate(n_dim, system_radius, diameter, insertion_type, nb, length[f],
+                                  persistence_length[f], rng.k0, rng.k1, rng.k, pos.data(),
+                                  cen.data(), axis.data());
       // Overlap test against accepted bonds.
       bool overlap = false;
       for (int b = 0; b < nb && !overlap; ++b) {
