@@ -276,13 +276,12 @@ struct PairStore {
   int *pa = nullptr, *pb = nullptr, *pos1 = nullptr, *pos2 = nullptr, *e_ent = nullptr;
   double *pf64 = nullptr, *cf64 = nullptr, *pv64 = nullptr;
   float *pf32 = nullptr, *cf32 = nullptr, *pv32 = nullptr;
-  int *fix_list = nullptr;
 };
 
 void free_store(sc_ctx *c, PairStore &q) {
   for (void *p : {(void *)q.pa, (void *)q.pb, (void *)q.pos1, (void *)q.pos2, (void *)q.pf64,
                   (void *)q.pf32, (void *)q.cf64, (void *)q.cf32, (void *)q.e_ent,
-                  (void *)q.pv64, (void *)q.pv32, (void *)q.fix_list})
+                  (void *)q.pv64, (void *)q.pv32})
     dfree(c, p);
   q = PairStore{};
 }
@@ -301,7 +300,6 @@ PairStore current_store(const sc_ctx *c) {
   q.pf32 = d.pf32;
   q.cf32 = d.cf32;
   q.pv32 = d.pv32;
-  q.fix_list = d.fix_list;
   return q;
 }
 
@@ -321,7 +319,6 @@ void install_store(sc_ctx *c, const PairStore &q) {
   d.pf32 = q.pf32;
   d.cf32 = q.cf32;
   d.pv32 = q.pv32;
-  d.fix_list = q.fix_list;
 }
 
 // New pair arrays for `total` slots, with the context's precision and
@@ -356,22 +353,12 @@ sc_status alloc_store(sc_ctx *c, long long total, PairStore &q) {
         CKS(dalloc(c, &q.pv32, 4 * n));
         CK(cudaMemsetAsync(q.pv32, 0, sizeof(float) * 4 * n, c->st));
       }
-      if (c->npx) CKS(dalloc(c, &q.fix_list, n));
     }
     return SC_OK;
   };
   const sc_status s = all();
   if (s != SC_OK) free_store(c, q);
   return s;
-}
-
-// The counters of the near-parallel list (k_pair_fixup leaves the count
-// zero after every pair stage), zeroed once.
-sc_status alloc_fixup_counters(sc_ctx *c) {
-  if (c->d.fix_count) return SC_OK;
-  CKS(dalloc(c, &c->d.fix_count, 1));
-  CK(cudaMemsetAsync(c->d.fix_count, 0, sizeof(int), c->st));
-  return SC_OK;
 }
 
 // Pair storage for segments of the given capacities, one per system, back
@@ -383,7 +370,6 @@ sc_status layout_pairs(sc_ctx *c, const std::vector<long long> &caps) {
   long long total = 0;
   for (long long x : caps) total += x;
   if (total >= (1ll << 30)) return fail(c, SC_ERR_LIST_OVERFLOW, "pair lists of %lld slots too large", total);
-  if (c->prec != 0 && c->npx) CKS(alloc_fixup_counters(c));
   PairStore q;
   CKS(alloc_store(c, total, q));
   install_store(c, q);
@@ -1414,16 +1400,16 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
         CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
         c->graph_ms += ms;
       }
-      // Kernels the graph ran: loop head, per BD step decide + tether + 2
-      // steps + tail (the stopped step's too), per rebuild the captured
-      // sequence.  A step is its pair stage (unless fused), the
-      // near-parallel fix-up, thermo and one or two integrator kernels.
+      // Kernels the graph ran: loop head, per BD step decide + the two
+      // tether kernels (mesh lambdas, anchor forces) + 2 steps + tail (the
+      // stopped step's too), per rebuild the captured sequence.  A step is
+      // its pair kernel (unless fused; near-parallel pairs are evaluated in
+      // place), thermo and one or two integrator kernels.
       const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
       const long long per_bd =
           c->desc.interaction_flag
               ? 2 + (c->d.nx ? 2 : 0) +
-                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0) +
-                         (c->npx && c->prec && !c->graph_fused ? 1 : 0))
+                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0))
               : 1 + 2 * int_l;
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
                      (nr1 - nr0) * c->rebuild_kernels;
@@ -2507,10 +2493,6 @@ sc_status sc_set_exact_near_parallel(sc_ctx *c, int on) {
   if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
   if (c->prec == 0 || c->npx == (on != 0)) return SC_OK;
   CK(cudaSetDevice(c->desc.device));
-  if (on) {
-    CKS(alloc_fixup_counters(c));
-    if (!c->d.fix_list) CKS(dalloc(c, &c->d.fix_list, (size_t)(c->pcap > 0 ? c->pcap : 1)));
-  }
   c->npx = on != 0;
   CK(cudaStreamSynchronize(c->st));
   drop_graph(c);

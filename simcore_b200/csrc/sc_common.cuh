@@ -163,10 +163,6 @@ struct DevState {
   int *pos1, *pos2;        // slot of each pair's obj1 / obj2 entry
   double *cf64;            // per slot, 8 values: signed force (3), torque (3), pad (2)
   float *cf32;
-  // mixed pair stage with exact near-parallel pairs: those left to
-  // k_pair_fixup
-  int *fix_list;           // one slot per pair
-  int *fix_count;
   // thermo (kept while SysConst::thermo is set): per pair the dr its stress
   // was computed from and its potential, stored with the force
   double *pv64;            // 4 per pair: dr (3), pote

@@ -464,9 +464,22 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   const int count = d.blk_ns[blk];
   const int f0 = d.blk_f0[blk];
   const int nfb = d.blk_nf[blk];
+  __shared__ double s_hinv[9];  // the block's system (blocks never mix systems)
+  __shared__ uint32_t s_seed;
+  // Every global load the step needs is issued here, before the first
+  // barrier: the filament constants, the renormalisation state and the
+  // block's system constants, below the site state.
+  int pre_sw = 0, pre_nn = 0;
   if (t < nfb) {
     sfil[t] = d.fil[f0 + t];
     sflag[t] = 0;
+    pre_sw = d.f_switch[f0 + t];
+    pre_nn = d.f_nnorm[f0 + t];
+  }
+  if (t < 10) {
+    const ReplicaConst &Rb = d.rep[d.nrep == 1 ? 0 : d.fil[f0].rep];
+    if (t < 9) s_hinv[t] = Rb.hinv[t];
+    else s_seed = Rb.seed;
   }
   const bool active = t < count;
   const int g = s0 + t;
@@ -623,7 +636,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
       if (active) {  // ConstructUnprojectedRandomForces (:518-548)
         uint32_t w[4];
         sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
-                              d.rep[fc.rep].seed, (uint32_t)fc.f_local, w);
+                              s_seed, (uint32_t)fc.f_local, w);
         double xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
 #pragma unroll
         for (int i = 0; i < ND; ++i)
@@ -948,7 +961,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
     const double l = sfil[t].l;
     const int fg = f0 + t;
-    int sw = d.f_switch[fg], nnorm = d.f_nnorm[fg];
+    int sw = pre_sw, nnorm = pre_nn;
     if (sflag[t]) {
       sw = !sw;
       nnorm = 0;
@@ -1002,7 +1015,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
       for (int i = 0; i < ND; ++i) {
         s[i] = 0.0;
 #pragma unroll
-        for (int jj = 0; jj < ND; ++jj) s[i] += d.rep[fc.rep].hinv[ND * i + jj] * pos[jj];
+        for (int jj = 0; jj < ND; ++jj) s[i] += s_hinv[ND * i + jj] * pos[jj];
         s[i] -= nint(s[i]);
       }
       store_geom<ND>(d, 1 - rbuf, b, s, ub, len, PREC);
