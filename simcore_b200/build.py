@@ -16,8 +16,9 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsimcore_b200.so")
 BUILD_DIR = os.path.join(ROOT, "_build")
 
-CU_SOURCES = ["sc_kernels.cu", "sc_kernels_fast.cu", "sc_api.cu", "sc_noalloc.cu",
-              "sc_insert_gpu.cu"]
+CU_SOURCES = ["sc_kernels.cu", "sc_kernels_fast.cu", "sc_api.cu", "sc_graph.cu", "sc_autotune.cu",
+              "sc_state.cu", "sc_output.cu", "sc_analysis.cu", "sc_xlinks.cu", "sc_noalloc.cu",
+              "sc_insert_gpu.cu", "sc_rebuild.cu"]
 # Units compiled with FMA contraction (everything else keeps --fmad=false).
 FMAD_SOURCES = {"sc_kernels_fast.cu"}
 CPP_SOURCES = ["sc_insert.cpp"]

@@ -1,141 +1,9 @@
-// C ABI of the B200 filament step (include/simcore_gpu.h): context,
-// device memory, rebuild orchestration and the step loop.
-#include <cuda_runtime.h>
+// C ABI of the B200 filament step (include/simcore_gpu.h): context, systems
+// and filaments, the reference step, state access.  The shared helpers of
+// sc_context.h are defined here.
+#include "sc_context.h"
 
-#include <algorithm>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <string>
-#include <type_traits>
-#include <vector>
-
-#include "sc_common.cuh"
-#include "sc_kernels.h"
-#include "sc_launch.h"
-#include "simcore_gpu.h"
-
-using sc::DevState;
-using sc::SysConst;
-
-struct sc_ctx {
-  sc_system_desc desc{};
-  int nd = 3;
-  int prec = 0;
-  SysConst k{};
-  DevState d{};
-  cudaStream_t st = nullptr;
-  std::string err;
-  std::vector<void *> allocs;  // every device allocation, freed at destroy
-
-  // host mirrors
-  int nf = 0, ns = 0, nb = 0;
-  std::vector<int> site_off;
-  std::vector<int> bond_fil;
-  std::vector<int> fil_rep;        // system of each filament
-  // per filament, for output files: diameter, length, bond length, lp
-  std::vector<double> fil_diam, fil_len, fil_bl, fil_lp;
-
-  // analyses (sc_analysis_*): device accumulators
-  struct Analysis {
-    int n_bins = 0, max_joints = 0;
-    long long n_samples = 0;
-    double *acc = nullptr;     // 2 per system
-    int *hist = nullptr;       // nrep x max_joints x n_bins
-    double *order = nullptr;   // 12 per system
-  } an;
-
-  // diffusion analysis (sc_diffusion_*): window of `interval` samples, the
-  // next sample's point, origins and per-system sums (4 x interval each)
-  struct Diffusion {
-    int interval = 0, t = 0;
-    long long n_samples = 0;
-    double *avg = nullptr, *pos0 = nullptr, *u0 = nullptr, *acc = nullptr;
-  } dif;
-
-  // reference-format output (sc_output_*): one spec and one posit file per
-  // system, frames snapshotted on the device and copied on out_st
-  struct Output {
-    bool open = false;
-    int n_steps = 0, n_posit = 0, n_spec = 0;
-    std::vector<FILE *> spec, posit;   // per system (null when not written)
-    cudaStream_t out_st = nullptr;
-    cudaEvent_t taken = nullptr, copied = nullptr;
-    double *d_snap = nullptr;          // positions (3 ns) then averages (9 nf)
-    double *h_snap = nullptr;          // pinned copy
-    bool pending_spec = false, pending_posit = false;
-  } out;
-  bool loaded = false;
-
-  // systems (replicas): host copy of the device table
-  std::vector<sc::ReplicaConst> reps;
-  std::vector<int> np_rep;         // pairs per system (last read back)
-
-  // cell list and pair list storage
-  int *key = nullptr, *cell_count = nullptr, *cell_start = nullptr;
-  unsigned *cell_occ = nullptr;  // one bit per cell: occupied in the last rebuild
-  int *sorted = nullptr, *pair_count = nullptr, *pair_off = nullptr;
-  int *deg = nullptr, *deg_off = nullptr, *scan_tmp = nullptr, *cells_xyz = nullptr;
-  double *stage = nullptr;         // interleaved host-transfer staging, 3 * max(ns, nb)
-  long long np = 0, pcap = 0;      // pairs and slots of all systems
-
-  // integrator blocks
-  int nblocks = 0, C = 128;
-  int warp_sites = 32;             // longest filament for the warp-synchronous kernel
-  int block_sites = 0;             // sites per block of the block kernel (0: 128, 256 or 512)
-
-  // control state
-  long long i_step = 0, n_rebuilds = 0, launches = 0;
-  int midstep = 1;                 // FilamentSpecies::midstep_
-  unsigned long long mcount = 0;   // midsteps that drew noise
-  int rbuf = 0;                    // geometry buffer read by the next pair stage
-  int capture = 0;
-  bool fast = true;                // mixed precision: contraction/reciprocal integrator
-  bool pairs_ready = false;        // pair contributions of the next update exist
-
-  // pinned readback slots
-  struct Readback {
-    unsigned long long dr_bits;
-    unsigned status;
-    int total;
-  } *hb = nullptr;
-  unsigned long long *h_dr = nullptr;  // per system displacement maxima
-  int *h_np = nullptr;                 // per system pair counts
-  int *h_due = nullptr;                // per system rebuild flags
-
-  // CUDA graph: a WHILE loop of BD steps (sc_step_graph)
-  cudaGraphExec_t graph_exec = nullptr;
-  int graph_rbuf = -1;             // geometry buffer parity the graph was built for
-  int *h_loop = nullptr;           // pinned loop count
-
-  // optional per-launch timing of the step kernel (host-driven path)
-  long long rebuild_kernels = 0;    // kernels in one rebuild sequence
-  bool timing = false;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  double timed_ms = 0.0;
-  long long timed_launches = 0;
-  cudaEvent_t gev0 = nullptr, gev1 = nullptr;  // around each graph launch
-  double graph_ms = 0.0;
-  bool graph_fused = false;  // the captured steps evaluate their pairs in the integrator
-  long long n_regrowths = 0;  // pair lists grown after an overflowing rebuild
-  // Mixed: nearly parallel pairs evaluated from the FP64 sites by a one-block
-  // kernel after each pair stage (on by default; sc_set_exact_near_parallel).
-  bool npx = true;
-  // The last step fused its pair evaluation into the integrator, so the
-  // per-bond slots do not hold it yet (materialize_slots writes them).
-  bool slots_stale = false;
-  bool fuse_pairs = false;  // sc_set_fused_pairs
-
-  // thermo (sc_set_thermo): records are produced on the device every th_n
-  // steps and pulled into th_host (and the open .thermo files)
-  long long th_i0 = 0;            // i_step when the records started
-  long long th_pulled = 0;        // records copied to the host
-  std::vector<double> th_host;    // pulled, not yet returned: per record nrep x 12
-  std::vector<FILE *> th_files;   // per system, while a .thermo file is open
-};
-
-namespace {
+namespace scapi {
 
 sc_status fail(sc_ctx *c, sc_status code, const char *fmt, ...) {
   char buf[512];
@@ -145,35 +13,6 @@ sc_status fail(sc_ctx *c, sc_status code, const char *fmt, ...) {
   va_end(ap);
   if (c) c->err = buf;
   return code;
-}
-
-#define CK(call)                                                          \
-  do {                                                                    \
-    cudaError_t e_ = (call);                                              \
-    if (e_ != cudaSuccess)                                                \
-      return fail(c, SC_ERR_CUDA, "%s: %s (%s:%d)", #call,                \
-                  cudaGetErrorString(e_), __FILE__, __LINE__);            \
-  } while (0)
-
-#define CKS(expr)                     \
-  do {                                \
-    sc_status s_ = (expr);            \
-    if (s_ != SC_OK) return s_;       \
-  } while (0)
-
-template <class T>
-sc_status dalloc(sc_ctx *c, T **p, size_t n) {
-  void *q = nullptr;
-  size_t bytes = sizeof(T) * (n ? n : 1);
-  cudaError_t e = cudaMalloc(&q, bytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    return fail(c, SC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", bytes,
-                cudaGetErrorString(e));
-  }
-  c->allocs.push_back(q);
-  *p = (T *)q;
-  return SC_OK;
 }
 
 void dfree(sc_ctx *c, void *p) {
@@ -241,8 +80,6 @@ sc_status readback(sc_ctx *c) {
   return check_status(c);
 }
 
-constexpr int kThermoMaxBlocks = 296;  // two per SM
-
 void drop_graph(sc_ctx *c) {
   if (c->graph_exec) {
     cudaGraphExecDestroy(c->graph_exec);
@@ -270,13 +107,6 @@ sc_status upload_reps(sc_ctx *c) {
   drop_graph(c);  // kernel parameters changed
   return SC_OK;
 }
-
-// The pair-list arrays of a context (DevState's pair members).
-struct PairStore {
-  int *pa = nullptr, *pb = nullptr, *pos1 = nullptr, *pos2 = nullptr, *e_ent = nullptr;
-  double *pf64 = nullptr, *cf64 = nullptr, *pv64 = nullptr;
-  float *pf32 = nullptr, *cf32 = nullptr, *pv32 = nullptr;
-};
 
 void free_store(sc_ctx *c, PairStore &q) {
   for (void *p : {(void *)q.pa, (void *)q.pb, (void *)q.pos1, (void *)q.pos2, (void *)q.pf64,
@@ -441,33 +271,13 @@ sc_status sync_pair_count(sc_ctx *c) {
 // pair lists in the reference's order into their segments, build their
 // per-bond pair entries, zero their displacement trackers.  Device work only
 // (capturable); a list longer than its segment sets the overflow bit.
-void rebuild_enqueue(sc_ctx *c, bool first_in_graph = false) {
-  const SysConst &k = c->k;
+void rebuild_enqueue(sc_ctx *c, bool first_in_graph) {
   const long long before = c->launches;
   const DevState &d = c->d;
-  if (c->desc.interaction_flag) {
-    if (first_in_graph) {
-      // Captured, the rebuild's first kernel starts the conditional body:
-      // no kernel before it to overlap.
-      sc::PdlOff off;
-      c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
-    } else {
-      c->launches += sc::launch_bin_count(k, d, c->key, c->cell_count, c->st);
-    }
-    c->launches += sc::launch_exclusive_scan(c->cell_count, c->cell_start, k.n_cells,
-                                             c->scan_tmp, c->st, c->cell_occ);
-    c->launches += sc::launch_bin_scatter(d, c->key, c->cell_start, c->cell_count, c->sorted,
-                                          c->st);
-    c->launches += sc::launch_cell_sort_count(k, d, c->key, c->sorted, c->cell_start,
-                                              c->pair_count, c->st, c->cell_occ);
-    c->launches += sc::launch_exclusive_scan(c->pair_count, c->pair_off, c->nb,
-                                             c->scan_tmp, c->st);
-    c->launches += sc::launch_pair_emit(k, d, c->key, c->sorted, c->cell_start,
-                                        c->pair_off, c->deg, c->prec, c->st, c->cell_occ);
-    c->launches += sc::launch_exclusive_scan(c->deg, c->deg_off, c->nb, c->scan_tmp, c->st);
-    c->launches += sc::launch_csr(d, c->deg, c->deg_off, c->st);
-  }
-  c->launches += sc::launch_zero_dr(d, c->st);
+  if (c->desc.interaction_flag)
+    c->launches += sc::launch_rebuild(c->k, d, c->rb, c->prec, c->st, first_in_graph);
+  else
+    c->launches += sc::launch_zero_dr(d, c->st);
   c->rebuild_kernels = c->launches - before;
 }
 
@@ -476,9 +286,8 @@ void rebuild_enqueue(sc_ctx *c, bool first_in_graph = false) {
 // (binning is a pure function of the positions, so the second pass gives the
 // same list); with several systems an overflow is reported, unless
 // allow_overflow (the initial pass, whose caller sizes the segments).
-sc_status grow_after_overflow(sc_ctx *c);
 
-sc_status rebuild(sc_ctx *c, bool allow_overflow = false) {
+sc_status rebuild(sc_ctx *c, bool allow_overflow) {
   for (int attempt = 0; attempt < 3; ++attempt) {
     rebuild_enqueue(c);
     CK(cudaGetLastError());
@@ -607,25 +416,11 @@ sc_status layout_integrator(sc_ctx *c) {
   CKS(up(&d.wg_ns, wg_ns));
   CK(cudaStreamSynchronize(c->st));
   c->nblocks = (int)blk_f0.size();
+  d.blk_maxf = 0;
+  for (int v : blk_nf) d.blk_maxf = std::max(d.blk_maxf, v);
   d.n_wg = (int)wg_f0.size();
   sc::prepare_integrate(c->C);
   drop_graph(c);
-  return SC_OK;
-}
-
-// Records CUDA events around one launch when kernel timing is on.
-template <class F>
-sc_status timed(sc_ctx *c, F launch) {
-  if (c->timing) CK(cudaEventRecord(c->ev0, c->st));
-  c->launches += launch();
-  if (c->timing) {
-    CK(cudaEventRecord(c->ev1, c->st));
-    CK(cudaEventSynchronize(c->ev1));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    c->timed_ms += ms;
-    c->timed_launches += 1;
-  }
   return SC_OK;
 }
 
@@ -756,22 +551,6 @@ sc_status materialize_slots(sc_ctx *c) {
   return SC_OK;
 }
 
-template <class T>
-sc_status copy_soa3(sc_ctx *c, T *const *src, int n, double *xyz) {
-  // Interleave on the device, then one copy into the caller's buffer (at
-  // full link speed when that buffer is pinned).
-  c->launches += sc::launch_soa_to_aos(n, src[0], src[1], src[2], c->stage, c->st);
-  CK(cudaMemcpyAsync(xyz, c->stage, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost,
-                     c->st));
-  CK(cudaStreamSynchronize(c->st));
-  return SC_OK;
-}
-
-template <class T>
-void put(FILE *f, const T &v) {
-  std::fwrite(&v, sizeof(T), 1, f);
-}
-
 // Writes the frame whose copy has completed.
 sc_status output_flush(sc_ctx *c) {
   sc_ctx::Output &o = c->out;
@@ -808,7 +587,10 @@ sc_status output_flush(sc_ctx *c) {
   o.pending_spec = o.pending_posit = false;
   return SC_OK;
 }
-}  // namespace
+
+}  // namespace scapi
+
+using namespace scapi;
 
 extern "C" {
 
@@ -1114,7 +896,7 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
       R.third = c->nd == 3 ? n1d : 1;
       R.n_cells = (int)std::min<long long>(ncell, 1ll << 30);
       R.cell0 = (int)std::min<long long>(cells, 1ll << 30);
-      cells += ncell;
+      cells += (ncell + 31) & ~31ll;  // every system's cells start at a multiple of 32
       const double cl = (double)2 * radius[r] / n1d;
       R.dr_update = 0.25 * cl * cl;
       R.seed = seed[r];
@@ -1149,19 +931,26 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
       return fail(c, SC_ERR_OOM, "pinned allocation failed");
     }
   c->np_rep.assign(nrep, 0);
-  CKS(dalloc(c, &c->key, nbi));
-  CKS(dzero(&c->cell_count, (size_t)k.n_cells));
-  CKS(dalloc(c, &c->cell_start, (size_t)k.n_cells + 1));
-  CKS(dalloc(c, &c->cell_occ, (size_t)k.n_cells / 32 + 1));
-  CKS(dalloc(c, &c->sorted, nbi));
-  CKS(dalloc(c, &c->pair_count, nbi));
-  CKS(dzero(&c->pair_off, (size_t)nbi + 1));
-  CKS(dzero(&c->deg, nbi));
-  CKS(dzero(&c->deg_off, (size_t)nbi + 1));
+  {
+    sc::RebuildBufs &rb = c->rb;
+    rb.n_groups = (int)(k.n_cells / 32);
+    CKS(dalloc(c, &rb.key, nbi));
+    CKS(dzero(&rb.gcount, (size_t)rb.n_groups));
+    CKS(dalloc(c, &rb.gstart, (size_t)rb.n_groups + 1));
+    CKS(dalloc(c, &rb.tmp, nbi));
+    CKS(dalloc(c, &rb.skey, nbi));
+    CKS(dalloc(c, &rb.sval, nbi));
+    CKS(dzero(&rb.range, (size_t)k.n_cells));
+    CKS(dzero(&rb.occ, (size_t)rb.n_groups));
+    CKS(dalloc(c, &rb.pair_count, nbi));
+    CKS(dzero(&rb.pair_off, (size_t)nbi + 1));
+    CKS(dzero(&rb.deg, nbi));
+    CKS(dzero(&rb.deg_off, (size_t)nbi + 1));
+    CKS(dalloc(c, &rb.scan_tmp,
+               (size_t)std::max(sc::scan_temp_ints(rb.n_groups), sc::scan_temp_ints(nbi))));
+  }
   CKS(dzero(&d.e_off, nbi));
   CKS(dzero(&d.e_cnt, nbi));
-  CKS(dalloc(c, &c->scan_tmp,
-             (size_t)std::max(sc::scan_temp_ints(k.n_cells), sc::scan_temp_ints(nbi))));
   CKS(dalloc(c, &c->cells_xyz, 3 * (size_t)nbi));
   CKS(dalloc(c, &c->stage, 3 * (size_t)std::max(nsi, nbi)));
 
@@ -1255,191 +1044,6 @@ sc_status sc_step(sc_ctx *c, int n) {
   return SC_OK;
 }
 
-// Captures one graph: WHILE (loop_count > 0) { decide -> IF(rebuild) ->
-// midstep -> full step -> tail }.  Built for the current geometry-buffer
-// parity; every BD step returns the parity to where it started.
-static sc_status build_graph(sc_ctx *c) {
-  drop_graph(c);
-  cudaGraph_t g = nullptr;
-  CK(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle h_loop;
-  CK(cudaGraphConditionalHandleCreate(&h_loop, g, 0, 0));
-  // head kernel: sets the loop condition
-  CK(cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  sc::launch_loop_head(c->d, h_loop, c->st);
-  cudaStreamCaptureStatus cs;
-  const cudaGraphNode_t *deps = nullptr;
-  size_t ndeps = 0;
-  CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, nullptr, &deps, &ndeps));
-  std::vector<cudaGraphNode_t> head(deps, deps + ndeps);
-  CK(cudaStreamEndCapture(c->st, &g));
-  // WHILE node
-  cudaGraphNodeParams wp = {};
-  wp.type = cudaGraphNodeTypeConditional;
-  wp.conditional.handle = h_loop;
-  wp.conditional.type = cudaGraphCondTypeWhile;
-  wp.conditional.size = 1;
-  cudaGraphNode_t wnode;
-  CK(cudaGraphAddNode(&wnode, g, head.data(), head.size(), &wp));
-  cudaGraph_t body = wp.conditional.phGraph_out[0];
-  const int interaction = c->desc.interaction_flag ? 1 : 0;
-  std::vector<cudaGraphNode_t> tail;
-  if (interaction) {
-    cudaGraphConditionalHandle h_if;
-    CK(cudaGraphConditionalHandleCreate(&h_if, body, 0, 0));
-    CK(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    sc::launch_decide(c->k, c->d, h_if, c->st);
-    CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, nullptr, &deps, &ndeps));
-    std::vector<cudaGraphNode_t> dec(deps, deps + ndeps);
-    CK(cudaStreamEndCapture(c->st, &body));
-    cudaGraphNodeParams ip = {};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = h_if;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    cudaGraphNode_t inode;
-    CK(cudaGraphAddNode(&inode, body, dec.data(), dec.size(), &ip));
-    cudaGraph_t rb = ip.conditional.phGraph_out[0];
-    CK(cudaStreamBeginCaptureToGraph(c->st, rb, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    long long launches = c->launches;
-    rebuild_enqueue(c, true);
-    c->launches = launches;
-    CK(cudaStreamEndCapture(c->st, &rb));
-    tail.push_back(inode);
-  }
-  CK(cudaStreamBeginCaptureToGraph(c->st, body, tail.empty() ? nullptr : tail.data(), nullptr,
-                                   tail.size(), cudaStreamCaptureModeRelaxed));
-  const bool fuse = fused_pairs(c);
-  c->graph_fused = fuse;
-  for (int half = 0; half < 2; ++half) {
-    const int rb = half == 0 ? c->rbuf : 1 - c->rbuf;
-    // The body's first kernel follows the conditional rebuild node (or the
-    // body's start), not a kernel: it is launched without the programmatic
-    // attribute.
-    // The second half is the even (full) step: crosslink tethers first.
-    if (half == 1 && interaction) sc::launch_tether(c->k, c->d, c->st);
-    if (interaction && !fuse) {
-      if (half == 0) {
-        sc::PdlOff off;
-        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
-      } else {
-        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
-      }
-    }
-    if (interaction && c->k.thermo) sc::launch_thermo(c->k, c->d, c->prec, c->st);
-    if (half == 0 && (!interaction || fuse)) {
-      sc::PdlOff off;
-      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1, rb, interaction, c->capture, c->prec,
-                           c->fast, c->st, fuse);
-    } else {
-      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, half == 0 ? 1 : 0, rb, interaction,
-                           c->capture, c->prec, c->fast, c->st, fuse);
-    }
-  }
-  sc::launch_loop_tail(c->d, c->desc.stoch_flag ? 1 : 0, h_loop, c->st);
-  CK(cudaStreamEndCapture(c->st, &body));
-  CK(cudaGetLastError());
-  cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) {
-    c->graph_exec = nullptr;
-    return fail(c, SC_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
-  }
-  c->graph_rbuf = c->rbuf;
-  return SC_OK;
-}
-
-sc_status sc_step_graph(sc_ctx *c, int n) {
-  if (!c || !c->loaded || n < 0) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  // Align to a midstep with the host-driven loop, then run whole BD steps.
-  if (!c->midstep && n > 0) {
-    CKS(step_once(c));
-    --n;
-  }
-  int bd = n / 2;
-  if (bd > 0) {
-    CKS(thermo_reserve(c, 2 * (long long)bd));
-    // The list must have room to grow by half before a captured run.
-    CKS(sync_pair_count(c));
-    if (c->reps.size() == 1 && c->np + c->np / 2 > c->pcap)
-      CKS(ensure_pair_capacity(c, c->np + c->np / 2));
-    if (!c->gev0) {
-      CK(cudaEventCreate(&c->gev0));
-      CK(cudaEventCreate(&c->gev1));
-    }
-    c->graph_ms = 0.0;
-    // A rebuild whose list outgrows its segment stops the run at that BD
-    // step, with nothing past the rebuild done; the list then grows, the
-    // rebuild is redone host-side and the run resumes with that step.
-    for (int attempt = 0; bd > 0; ++attempt) {
-      if (attempt == 8) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list kept overflowing inside captured runs");
-      if (!c->graph_exec || c->graph_rbuf != c->rbuf) CKS(build_graph(c));
-      *c->h_loop = bd;
-      CK(cudaMemcpyAsync(c->d.loop_count, c->h_loop, sizeof(int), cudaMemcpyHostToDevice, c->st));
-      long long nr0 = 0, nr1 = 0;
-      CK(cudaMemcpyAsync(&nr0, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-      CK(cudaEventRecord(c->gev0, c->st));
-      CK(cudaGraphLaunch(c->graph_exec, c->st));
-      CK(cudaEventRecord(c->gev1, c->st));
-      CK(cudaMemcpyAsync(&nr1, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-      CK(cudaMemcpyAsync(c->h_loop, c->d.loop_count, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-      c->pairs_ready = false;
-      CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                         c->st));
-      CK(cudaStreamSynchronize(c->st));
-      const unsigned st = c->hb->status;
-      const bool overflow = (st & sc::ST_LIST_OVERFLOW) != 0u;
-      // BD steps completed: all of them, or those before the stopped one.
-      const int done = overflow ? bd - *c->h_loop : bd;
-      if (c->graph_fused && done > 0) c->slots_stale = true;
-      c->i_step += 2 * (long long)done;
-      if (c->desc.stoch_flag) c->mcount += done;
-      {
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
-        c->graph_ms += ms;
-      }
-      // Kernels the graph ran: loop head, per BD step decide + the two
-      // tether kernels (mesh lambdas, anchor forces) + 2 steps + tail (the
-      // stopped step's too), per rebuild the captured sequence.  A step is
-      // its pair kernel (unless fused; near-parallel pairs are evaluated in
-      // place), thermo and one or two integrator kernels.
-      const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
-      const long long per_bd =
-          c->desc.interaction_flag
-              ? 2 + (c->d.nx ? 2 : 0) +
-                    2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0))
-              : 1 + 2 * int_l;
-      c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
-                     (nr1 - nr0) * c->rebuild_kernels;
-      bd -= done;
-      if (!overflow) {
-        CKS(readback(c));
-        break;
-      }
-      if (st & ~sc::ST_LIST_OVERFLOW) {
-        CKS(readback(c));  // reports the other error
-        return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow inside a captured run");
-      }
-      if (c->reps.size() != 1)
-        return fail(c, SC_ERR_LIST_OVERFLOW, "a system's pair list outgrew its segment inside a captured run");
-      const unsigned clear = 0u;
-      CK(cudaMemcpyAsync(c->d.status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice, c->st));
-      CKS(sync_pair_count(c));
-      CKS(grow_after_overflow(c));
-      // The stopped step's due flag is still set: redo its rebuild, with
-      // headroom for the rest of the run.
-      CKS(rebuild(c));
-      if (c->np + c->np / 2 > c->pcap) CKS(ensure_pair_capacity(c, c->np + c->np / 2));
-    }
-    unsigned st = c->hb->status;
-    if (st & sc::ST_UNPHYSICAL) return fail(c, SC_ERR_UNPHYSICAL, "Unphysical result");
-  }
-  if (n % 2) CKS(step_once(c));
-  return SC_OK;
-}
-
 sc_status sc_synchronize(sc_ctx *c) {
   if (!c) return SC_ERR_INVALID_ARG;
   CK(cudaSetDevice(c->desc.device));
@@ -1493,794 +1097,6 @@ sc_status sc_get_bond_forces(sc_ctx *c, double *f, double *t) {
   CK(cudaGetLastError());
   CKS(copy_soa3(c, c->d.bF, c->nb, f));
   return copy_soa3(c, c->d.bT, c->nb, t);
-}
-
-sc_status sc_set_integrator_layout(sc_ctx *c, int warp_max_sites, int block_sites) {
-  if (!c || !c->loaded || warp_max_sites < 0 || warp_max_sites > 32) return SC_ERR_INVALID_ARG;
-  if (block_sites != 0 && (block_sites < 32 || block_sites > 512 || block_sites % 32))
-    return fail(c, SC_ERR_INVALID_ARG, "block_sites must be 0 or a multiple of 32 in [32, 512]");
-  CK(cudaSetDevice(c->desc.device));
-  const int ow = c->warp_sites, ob = c->block_sites;
-  c->warp_sites = warp_max_sites;
-  c->block_sites = block_sites;
-  sc_status st = layout_integrator(c);
-  if (st != SC_OK) {
-    c->warp_sites = ow;
-    c->block_sites = ob;
-    layout_integrator(c);
-  }
-  return st;
-}
-
-// Integrator autotuner.  Candidate layouts (warp kernel or not, block size)
-// are timed on the context's own state: the arrays the integrator writes are
-// saved first and restored afterwards, so the simulation is unchanged.  The
-// fastest layout is applied and, with a cache file, recorded per shape (device,
-// precision, filament count and site range) so later contexts skip the timing.
-sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
-                      int *block_sites_out) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  cudaDeviceProp prop;
-  CK(cudaGetDeviceProperties(&prop, c->desc.device));
-  int min_n = 1 << 30, max_n = 0;
-  for (int f = 0; f < c->nf; ++f) {
-    const int nn = c->site_off[f + 1] - c->site_off[f];
-    min_n = std::min(min_n, nn);
-    max_n = std::max(max_n, nn);
-  }
-  char key[512];
-  const bool fuse = fused_pairs(c);
-  std::snprintf(key, sizeof(key), "v2|%s|sm%d|nd%d|prec%d|fast%d|fuse%d|nf%d|ns%d|n%d-%d",
-                prop.name, prop.multiProcessorCount, c->nd, c->prec,
-                (c->prec == 1 && c->fast) ? 1 : 0, fuse ? 1 : 0, c->nf, c->ns, min_n, max_n);
-  auto finish = [&](int w, int b) -> sc_status {
-    if (warp_sites_out) *warp_sites_out = w;
-    if (block_sites_out) *block_sites_out = b;
-    return SC_OK;
-  };
-  if (cache_path) {
-    if (FILE *fp = std::fopen(cache_path, "r")) {
-      char line[768];
-      int w = -1, b = -1;
-      while (std::fgets(line, sizeof(line), fp)) {
-        char *tab = std::strchr(line, '\t');
-        if (!tab) continue;
-        *tab = 0;
-        int ww, bb;
-        if (std::strcmp(line, key) == 0 && std::sscanf(tab + 1, "%d %d", &ww, &bb) == 2) {
-          w = ww;
-          b = bb;
-        }
-      }
-      std::fclose(fp);
-      if (w >= 0) {
-        CKS(sc_set_integrator_layout(c, w, b));
-        return finish(w, b);
-      }
-    }
-  }
-  // Candidates: every block size that holds the longest block-kernel
-  // filament, with and without the warp kernel for filaments of <= 32 sites.
-  std::vector<std::pair<int, int>> cand;
-  for (int w : {32, 0}) {
-    if (w == 32 && min_n > 32) continue;
-    const int longest = w == 32 ? (max_n > 32 ? max_n : 0) : max_n;
-    if (longest == 0) {
-      cand.push_back({w, 0});
-      continue;
-    }
-    for (int bsz : {64, 96, 128, 160, 192, 256, 512})
-      if (bsz >= longest && (bsz < 512 || longest > 256)) cand.push_back({w, bsz});
-  }
-  // Save what the integrator writes.
-  const int wbuf = 1 - c->rbuf;
-  std::vector<std::pair<void *, size_t>> regions;
-  for (int i = 0; i < 3; ++i) {
-    regions.push_back({c->d.r[i], sizeof(double) * c->ns});
-    regions.push_back({c->d.rp[i], sizeof(double) * c->ns});
-    regions.push_back({c->d.fr[i], sizeof(double) * c->ns});
-    regions.push_back({c->d.ub[i], sizeof(double) * c->nb});
-  }
-  regions.push_back({c->d.dt, sizeof(double) * c->ns});
-  regions.push_back({c->d.f_switch, sizeof(int) * c->nf});
-  regions.push_back({c->d.f_nnorm, sizeof(int) * c->nf});
-  if (c->prec == 0) regions.push_back({c->d.g64[wbuf], sizeof(sc::BondGeomF64) * c->nb});
-  else regions.push_back({c->d.g32[wbuf], sizeof(sc::BondGeomF32) * c->nb});
-  regions.push_back({c->d.dr_max_bits, sizeof(unsigned long long) * c->d.nrep});
-  regions.push_back({c->d.status, sizeof(unsigned)});
-  if (fuse) regions.push_back({c->d.pf32, sizeof(float) * 4 * c->d.pcap_total});
-  size_t total = 0;
-  for (auto &r : regions) total += (r.second + 255) & ~(size_t)255;
-  char *save = nullptr;
-  CKS(dalloc(c, &save, total));
-  auto copy_all = [&](bool to_save) -> sc_status {
-    size_t off = 0;
-    for (auto &r : regions) {
-      void *dst = to_save ? (void *)(save + off) : r.first;
-      const void *src = to_save ? (const void *)r.first : (const void *)(save + off);
-      CK(cudaMemcpyAsync(dst, src, r.second, cudaMemcpyDeviceToDevice, c->st));
-      off += (r.second + 255) & ~(size_t)255;
-    }
-    return SC_OK;
-  };
-  CKS(copy_all(true));
-  const int ow = c->warp_sites, ob = c->block_sites;
-  const int interaction = c->desc.interaction_flag ? 1 : 0;
-  float best = 1e30f;
-  std::pair<int, int> best_lay{ow, ob};
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  sc_status st = SC_OK;
-  for (auto lay : cand) {
-    c->warp_sites = lay.first;
-    c->block_sites = lay.second;
-    st = layout_integrator(c);
-    if (st != SC_OK) break;
-    for (int it = 0; it < 2; ++it)
-      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1 - it, c->rbuf, interaction, 0,
-                           c->prec, c->fast, c->st, fuse);
-    cudaEventRecord(e0, c->st);
-    for (int it = 0; it < 8; ++it)
-      sc::launch_integrate(c->k, c->d, c->nblocks, c->C, 1 - (it & 1), c->rbuf, interaction, 0,
-                           c->prec, c->fast, c->st, fuse);
-    cudaEventRecord(e1, c->st);
-    if (cudaEventSynchronize(e1) != cudaSuccess) {
-      st = fail(c, SC_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
-      break;
-    }
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    if (ms < best) {
-      best = ms;
-      best_lay = lay;
-    }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  CKS(copy_all(false));
-  CK(cudaStreamSynchronize(c->st));
-  dfree(c, save);
-  CKS(st);
-  c->warp_sites = best_lay.first;
-  c->block_sites = best_lay.second;
-  CKS(layout_integrator(c));
-  if (cache_path) {
-    if (FILE *fp = std::fopen(cache_path, "a")) {
-      std::fprintf(fp, "%s\t%d %d %.2f\n", key, best_lay.first, best_lay.second,
-                   1000.0 * best / 8);
-      std::fclose(fp);
-    }
-  }
-  return finish(best_lay.first, best_lay.second);
-}
-
-// ---------------------------------------------------------------------------
-// Checkpoint / restore: every piece of state a later step reads, so that a
-// restored context continues bit for bit.
-
-namespace {
-struct CkptHeader {
-  char magic[8];       // "SCB200CK"
-  int32_t version, nd, prec, nrep, nf, ns, nb, nx;
-  int32_t midstep, rbuf, stoch, pad;
-  int64_t i_step;
-  uint64_t mcount;
-  int64_t n_rebuilds;
-  int64_t payload_bytes;  // everything after the header
-  uint64_t payload_hash;  // payload_hash() of those bytes
-};
-constexpr int32_t kCkptVersion = 2;
-
-// 64-bit FNV-1a over 8-byte words (then the tail bytes): any change to a
-// checkpoint's payload changes it, in one host pass at memory speed.
-uint64_t payload_hash(const char *p, size_t n) {
-  uint64_t h = 1469598103934665603ull;
-  size_t i = 0;
-  for (; i + 8 <= n; i += 8) {
-    uint64_t w;
-    std::memcpy(&w, p + i, 8);
-    h = (h ^ w) * 1099511628211ull;
-  }
-  for (; i < n; ++i) h = (h ^ (unsigned char)p[i]) * 1099511628211ull;
-  return h;
-}
-
-// Device regions of a checkpoint, in file order.  Pair-list regions are
-// sized for P pair slots (recorded per system first); the pointers are the
-// context's own, valid when P is its current capacity.  Index regions carry
-// their kind, for the range checks of a restore.
-enum RegionKind { RK_DATA, RK_NP, RK_EOFF, RK_ECNT, RK_PA, RK_PB, RK_POS1, RK_POS2, RK_EENT };
-struct Region {
-  void *ptr;
-  size_t bytes;
-  RegionKind kind = RK_DATA;
-};
-
-std::vector<Region> state_regions(sc_ctx *c, long long pcap = -1) {
-  std::vector<Region> v;
-  const DevState &d = c->d;
-  const size_t ns = c->ns, nb = c->nb, nf = c->nf, nrep = c->d.nrep;
-  for (int i = 0; i < 3; ++i) v.push_back({d.r[i], sizeof(double) * ns});
-  for (int i = 0; i < 3; ++i) v.push_back({d.rp[i], sizeof(double) * ns});
-  for (int i = 0; i < 3; ++i) v.push_back({d.fr[i], sizeof(double) * ns});
-  for (int i = 0; i < 3; ++i) v.push_back({d.dz[i], sizeof(double) * ns});
-  v.push_back({d.dt, sizeof(double) * ns});
-  v.push_back({d.f_switch, sizeof(int) * nf});
-  v.push_back({d.f_nnorm, sizeof(int) * nf});
-  v.push_back({d.dr_max_bits, sizeof(unsigned long long) * nrep});
-  v.push_back({d.np_rep, sizeof(int) * nrep, RK_NP});
-  v.push_back({d.rep_rebuilds, sizeof(long long) * nrep});
-  v.push_back({d.e_off, sizeof(int) * nb, RK_EOFF});
-  v.push_back({d.e_cnt, sizeof(int) * nb, RK_ECNT});
-  // Bond orientations and the geometry the next pair stage reads, as the
-  // integrator wrote them (the fast integrator's bits differ from a
-  // re-derivation).
-  for (int i = 0; i < 3; ++i) v.push_back({d.ub[i], sizeof(double) * nb});
-  if (c->prec == 0) v.push_back({d.g64[c->rbuf], sizeof(sc::BondGeomF64) * nb});
-  else v.push_back({d.g32[c->rbuf], sizeof(sc::BondGeomF32) * nb});
-  const size_t P = (size_t)(pcap >= 0 ? pcap : c->pcap);
-  v.push_back({d.pa, sizeof(int) * P, RK_PA});
-  v.push_back({d.pb, sizeof(int) * P, RK_PB});
-  v.push_back({d.pos1, sizeof(int) * P, RK_POS1});  // where each pair writes its two
-  v.push_back({d.pos2, sizeof(int) * P, RK_POS2});  // contributions
-  v.push_back({d.e_ent, sizeof(int) * 2 * P, RK_EENT});
-  if (c->prec == 0) {
-    v.push_back({d.pf64, sizeof(double) * 4 * P});
-    v.push_back({d.cf64, sizeof(double) * 16 * P});
-  } else {
-    v.push_back({d.pf32, sizeof(float) * 4 * P});
-    v.push_back({d.cf32, sizeof(float) * 16 * P});
-  }
-  if (d.nx) {
-    v.push_back({d.xl_c, sizeof(double) * 16 * (size_t)d.nx});
-    v.push_back({d.xl_F, sizeof(double) * 4 * (size_t)d.nx});
-    v.push_back({d.xl_M, sizeof(double) * 2 * (size_t)d.nx});
-  }
-  if (c->k.thermo) {  // pair virial records and the running virial sums
-    if (c->prec == 0) v.push_back({d.pv64, sizeof(double) * 4 * P});
-    else v.push_back({d.pv32, sizeof(float) * 4 * P});
-    v.push_back({d.th_acc, sizeof(double) * 9 * nrep});
-    v.push_back({d.th_istep, sizeof(long long) * nrep});
-  }
-  return v;
-}
-}  // namespace
-
-sc_status sc_checkpoint(sc_ctx *c, void *buf, size_t cap, size_t *size) {
-  if (!c || !c->loaded || !size) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  const int nrep = c->d.nrep;
-  auto regions = state_regions(c);
-  size_t need = sizeof(CkptHeader) + sizeof(int32_t) * nrep;
-  for (auto &r : regions) need += r.bytes;
-  *size = need;
-  if (!buf) return SC_OK;
-  if (cap < need) return fail(c, SC_ERR_INVALID_ARG, "checkpoint needs %zu bytes", need);
-  CKS(materialize_slots(c));
-  CKS(readback(c));
-  long long nr = 0;
-  CK(cudaMemcpyAsync(&nr, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  CkptHeader h;
-  std::memset(&h, 0, sizeof(h));
-  std::memcpy(h.magic, "SCB200CK", 8);
-  h.version = kCkptVersion;
-  h.nd = c->nd;
-  h.prec = c->prec;
-  h.nrep = nrep;
-  h.nf = c->nf;
-  h.ns = c->ns;
-  h.nb = c->nb;
-  h.nx = c->d.nx;
-  h.midstep = c->midstep;
-  h.rbuf = c->rbuf;
-  h.stoch = c->desc.stoch_flag;
-  h.i_step = c->i_step;
-  h.mcount = c->mcount;
-  h.n_rebuilds = nr;
-  h.payload_bytes = (int64_t)(need - sizeof(h));
-  char *out = (char *)buf + sizeof(h);
-  for (int r = 0; r < nrep; ++r) {
-    const int32_t pc = c->reps[r].pcap;
-    std::memcpy(out, &pc, sizeof(pc));
-    out += sizeof(pc);
-  }
-  for (auto &r : regions) {
-    CK(cudaMemcpyAsync(out, r.ptr, r.bytes, cudaMemcpyDeviceToHost, c->st));
-    out += r.bytes;
-  }
-  CK(cudaStreamSynchronize(c->st));
-  h.payload_hash = payload_hash((const char *)buf + sizeof(h), need - sizeof(h));
-  std::memcpy(buf, &h, sizeof(h));
-  return SC_OK;
-}
-
-// The index ranges of a checkpoint's pair lists, checked on the host before
-// anything is uploaded, so that no blob can send a later launch outside its
-// arrays: system r's live pairs join two of its bonds and write two of its
-// slots, and every entry of its bonds names one of its live pairs.
-sc_status check_pair_indices(sc_ctx *c, const std::vector<long long> &caps,
-                             const std::vector<Region> &regions, const char *payload) {
-  const int32_t *ix[RK_EENT + 1] = {};
-  for (const Region &r : regions) {
-    if (r.kind != RK_DATA) ix[r.kind] = (const int32_t *)payload;
-    payload += r.bytes;
-  }
-  const int32_t *np = ix[RK_NP], *e_off = ix[RK_EOFF], *e_cnt = ix[RK_ECNT];
-  const int32_t *pa = ix[RK_PA], *pb = ix[RK_PB], *pos1 = ix[RK_POS1], *pos2 = ix[RK_POS2];
-  const int32_t *e_ent = ix[RK_EENT];
-  long long p0 = 0;
-  for (size_t r = 0; r < caps.size(); ++r) {
-    const sc::ReplicaConst &R = c->reps[r];
-    const long long n = np[r], cap = caps[r], s0 = 2 * p0, s1 = 2 * (p0 + cap);
-    if (n < 0 || n > cap)
-      return fail(c, SC_ERR_INVALID_ARG, "checkpoint: system %zu holds %lld pairs", r, n);
-    for (long long p = p0; p < p0 + n; ++p)
-      if (pa[p] < R.b0 || pa[p] >= R.b0 + R.nb || pb[p] < R.b0 || pb[p] >= R.b0 + R.nb ||
-          pos1[p] < s0 || pos1[p] >= s1 || pos2[p] < s0 || pos2[p] >= s1)
-        return fail(c, SC_ERR_INVALID_ARG, "checkpoint: pair %lld out of range", p);
-    for (long long b = R.b0; b < R.b0 + R.nb; ++b) {
-      const long long e0 = e_off[b], ec = e_cnt[b];
-      if (ec < 0 || e0 < s0 || e0 + ec > s1)
-        return fail(c, SC_ERR_INVALID_ARG, "checkpoint: bond %lld entries out of range", b);
-      for (long long e = e0; e < e0 + ec; ++e)
-        if (e_ent[e] < 0 || (e_ent[e] >> 1) < p0 || (e_ent[e] >> 1) >= p0 + n)
-          return fail(c, SC_ERR_INVALID_ARG, "checkpoint: entry %lld out of range", e);
-    }
-    p0 += cap;
-  }
-  return SC_OK;
-}
-
-sc_status sc_restore(sc_ctx *c, const void *buf, size_t size) {
-  if (!c || !c->loaded || !buf) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  CkptHeader h;
-  if (size < sizeof(h)) return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
-  std::memcpy(&h, buf, sizeof(h));
-  if (std::memcmp(h.magic, "SCB200CK", 8) != 0 || h.version != kCkptVersion)
-    return fail(c, SC_ERR_INVALID_ARG, "not a checkpoint of this library (version %d)",
-                kCkptVersion);
-  if (h.nd != c->nd || h.prec != c->prec || h.nrep != c->d.nrep || h.nf != c->nf ||
-      h.ns != c->ns || h.nb != c->nb || h.nx != c->d.nx)
-    return fail(c, SC_ERR_INVALID_ARG, "checkpoint of a different system shape");
-  if (h.payload_bytes < 0 || size - sizeof(h) < (size_t)h.payload_bytes)
-    return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
-  const char *payload = (const char *)buf + sizeof(h);
-  if (payload_hash(payload, (size_t)h.payload_bytes) != h.payload_hash)
-    return fail(c, SC_ERR_INVALID_ARG, "checkpoint corrupted (payload hash differs)");
-  if ((h.rbuf != 0 && h.rbuf != 1) || (h.midstep != 0 && h.midstep != 1))
-    return fail(c, SC_ERR_INVALID_ARG, "checkpoint: bad step state");
-  // Everything is checked before the context changes.
-  const int nrep = h.nrep;
-  const char *in = payload;
-  if ((size_t)h.payload_bytes < sizeof(int32_t) * nrep)
-    return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
-  std::vector<long long> caps(nrep);
-  long long total = 0;
-  for (int r = 0; r < nrep; ++r) {
-    int32_t pc;
-    std::memcpy(&pc, in, sizeof(pc));
-    in += sizeof(pc);
-    if (pc < 1) return fail(c, SC_ERR_INVALID_ARG, "checkpoint: system %d has %d pair slots", r, pc);
-    caps[r] = pc;
-    total += pc;
-  }
-  if (total >= (1ll << 30)) return fail(c, SC_ERR_INVALID_ARG, "checkpoint: %lld pair slots", total);
-  {
-    const auto sized = state_regions(c, total);
-    size_t need = sizeof(int32_t) * nrep;
-    for (auto &r : sized) need += r.bytes;
-    if ((size_t)h.payload_bytes < need) return fail(c, SC_ERR_INVALID_ARG, "checkpoint truncated");
-    CKS(check_pair_indices(c, caps, sized, in));
-  }
-  // The checkpoint's segments; a failed allocation leaves the context as it
-  // was.  Then rbuf selects the geometry buffer the checkpoint fills.
-  CKS(layout_pairs(c, caps));
-  c->rbuf = h.rbuf;
-  auto regions = state_regions(c);
-  for (auto &r : regions) {
-    CK(cudaMemcpyAsync(r.ptr, in, r.bytes, cudaMemcpyHostToDevice, c->st));
-    in += r.bytes;
-  }
-  const long long nr = h.n_rebuilds;
-  CK(cudaMemcpyAsync(c->d.n_rebuilds, &nr, sizeof(long long), cudaMemcpyHostToDevice, c->st));
-  const unsigned long long mc = h.mcount;
-  CK(cudaMemcpyAsync(c->d.mcount, &mc, sizeof(mc), cudaMemcpyHostToDevice, c->st));
-  const unsigned zero = 0;
-  CK(cudaMemcpyAsync(c->d.status, &zero, sizeof(zero), cudaMemcpyHostToDevice, c->st));
-  c->i_step = h.i_step;
-  c->mcount = h.mcount;
-  c->midstep = h.midstep;
-  c->pairs_ready = false;
-  c->slots_stale = false;  // the checkpoint's slots hold its last evaluation
-  if (c->k.thermo) {  // records restart from the restored step
-    CK(cudaMemsetAsync(c->d.th_nrec, 0, sizeof(long long) * c->d.nrep, c->st));
-    CK(cudaMemsetAsync(c->d.th_ticket, 0, sizeof(unsigned) * c->d.nrep, c->st));
-    c->th_i0 = c->i_step;
-    c->th_pulled = 0;
-    c->th_host.clear();
-  }
-  // The FP64 record of mixed precision serves only the geometry getter.
-  if (c->prec != 0) sc::launch_init_geometry(c->k, c->d, 0, 0, c->st, false);
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(c->st));
-  CKS(sync_pair_count(c));
-  drop_graph(c);
-  return SC_OK;
-}
-
-sc_status sc_set_noise_key(sc_ctx *c, int replica, uint32_t seed) {
-  if (!c || !c->loaded || replica < -1 || replica >= c->d.nrep) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  for (int r = 0; r < c->d.nrep; ++r)
-    if (replica < 0 || r == replica) c->reps[r].seed = seed;
-  return upload_reps(c);
-}
-
-// ---------------------------------------------------------------------------
-// Reference-format output files: the filament species' spec and posit files
-// (SpeciesBase::InitSpecFile / InitPositFile, src/species_base.cpp:13-70;
-// Species::WriteSpecs / WritePosits, include/simcore/species.hpp:221-233;
-// Mesh::WriteSpec, src/mesh.cpp:482-492; Filament::WriteSpec / WritePosit,
-// src/filament.cpp:1314-1361), at the cadence of OutputManager::WriteOutputs
-// (include/simcore/output_manager.hpp:112-127).
-
-
-sc_status sc_output_open(sc_ctx *c, const char *run_name, const char *species_name, int n_steps,
-                         int n_posit, int n_spec) {
-  if (!c || !c->loaded || !run_name || !species_name || n_steps < 0 || n_posit < 0 ||
-      n_spec < 0)
-    return SC_ERR_INVALID_ARG;
-  if (c->out.open) return fail(c, SC_ERR_INVALID_ARG, "output already open");
-  CK(cudaSetDevice(c->desc.device));
-  sc_ctx::Output &o = c->out;
-  o.n_steps = n_steps;
-  o.n_posit = n_posit;
-  o.n_spec = n_spec;
-  const size_t nrep = c->reps.size();
-  o.spec.assign(nrep, nullptr);
-  o.posit.assign(nrep, nullptr);
-  for (size_t r = 0; r < nrep; ++r) {
-    std::string run = run_name;
-    if (nrep > 1) {
-      char sfx[32];
-      std::snprintf(sfx, sizeof(sfx), "_r%03zu", r);
-      run += sfx;
-    }
-    const std::string base = run + "_filament_" + species_name;
-    for (int kind = 0; kind < 2; ++kind) {
-      const int cadence = kind == 0 ? n_spec : n_posit;
-      if (cadence <= 0) continue;
-      const std::string name = base + (kind == 0 ? ".spec" : ".posit");
-      FILE *f = std::fopen(name.c_str(), "wb");
-      if (!f) return fail(c, SC_ERR_INVALID_ARG, "cannot open %s", name.c_str());
-      put(f, (int32_t)n_steps);
-      put(f, (int32_t)cadence);
-      put(f, c->desc.delta);
-      (kind == 0 ? o.spec : o.posit)[r] = f;
-    }
-  }
-  const size_t doubles = 3 * (size_t)c->ns + 9 * (size_t)c->nf;
-  CKS(dalloc(c, &o.d_snap, doubles));
-  if (cudaHostAlloc((void **)&o.h_snap, sizeof(double) * doubles, cudaHostAllocDefault) !=
-      cudaSuccess) {
-    cudaGetLastError();
-    return fail(c, SC_ERR_OOM, "pinned allocation failed");
-  }
-  CK(cudaStreamCreateWithFlags(&o.out_st, cudaStreamNonBlocking));
-  CK(cudaEventCreateWithFlags(&o.taken, cudaEventDisableTiming));
-  CK(cudaEventCreateWithFlags(&o.copied, cudaEventDisableTiming));
-  o.open = true;
-  return SC_OK;
-}
-
-sc_status sc_output_write(sc_ctx *c) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  sc_ctx::Output &o = c->out;
-  if (!o.open) return fail(c, SC_ERR_INVALID_ARG, "output not open");
-  CK(cudaSetDevice(c->desc.device));
-  const bool spec = o.n_spec > 0 && c->i_step % o.n_spec == 0;
-  const bool posit = o.n_posit > 0 && c->i_step % o.n_posit == 0;
-  if (!spec && !posit) return SC_OK;
-  CKS(output_flush(c));  // the previous frame, whose copy overlapped the steps since
-  // Snapshot on the simulation stream, copy on the output stream.
-  if (spec)
-    c->launches += sc::launch_soa_to_aos(c->ns, c->d.r[0], c->d.r[1], c->d.r[2], o.d_snap, c->st);
-  if (posit)
-    c->launches += sc::launch_filament_averages(c->k, c->d, o.d_snap + 3 * (size_t)c->ns, c->st);
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(o.taken, c->st));
-  CK(cudaStreamWaitEvent(o.out_st, o.taken, 0));
-  if (spec)
-    CK(cudaMemcpyAsync(o.h_snap, o.d_snap, sizeof(double) * 3 * (size_t)c->ns,
-                       cudaMemcpyDeviceToHost, o.out_st));
-  if (posit)
-    CK(cudaMemcpyAsync(o.h_snap + 3 * (size_t)c->ns, o.d_snap + 3 * (size_t)c->ns,
-                       sizeof(double) * 9 * (size_t)c->nf, cudaMemcpyDeviceToHost, o.out_st));
-  CK(cudaEventRecord(o.copied, o.out_st));
-  o.pending_spec = spec;
-  o.pending_posit = posit;
-  return SC_OK;
-}
-
-sc_status sc_output_close(sc_ctx *c) {
-  if (!c) return SC_ERR_INVALID_ARG;
-  sc_ctx::Output &o = c->out;
-  if (!o.open) return SC_OK;
-  cudaSetDevice(c->desc.device);
-  sc_status st = output_flush(c);
-  for (FILE *f : o.spec)
-    if (f) std::fclose(f);
-  for (FILE *f : o.posit)
-    if (f) std::fclose(f);
-  o.spec.clear();
-  o.posit.clear();
-  if (o.out_st) cudaStreamSynchronize(o.out_st);
-  if (o.h_snap) cudaFreeHost(o.h_snap);
-  if (o.d_snap) dfree(c, o.d_snap);
-  if (o.taken) cudaEventDestroy(o.taken);
-  if (o.copied) cudaEventDestroy(o.copied);
-  if (o.out_st) cudaStreamDestroy(o.out_st);
-  o = sc_ctx::Output{};
-  return st;
-}
-
-// ---------------------------------------------------------------------------
-// Filament analyses on the device (FilamentSpecies::RunAnalysis family).
-
-sc_status sc_analysis_sample(sc_ctx *c, int n_bins) {
-  if (!c || !c->loaded || n_bins < 1) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  sc_ctx::Analysis &a = c->an;
-  if (a.n_bins && a.n_bins != n_bins)
-    return fail(c, SC_ERR_INVALID_ARG, "histogram bins changed between samples");
-  if (!a.acc) {
-    int maxn = 0;
-    for (int f = 0; f < c->nf; ++f) maxn = std::max(maxn, c->site_off[f + 1] - c->site_off[f]);
-    a.n_bins = n_bins;
-    a.max_joints = std::max(1, maxn - 2);
-    const size_t nrep = c->reps.size();
-    CKS(dalloc(c, &a.acc, 2 * nrep));
-    CK(cudaMemsetAsync(a.acc, 0, sizeof(double) * 2 * nrep, c->st));
-    CKS(dalloc(c, &a.hist, nrep * a.max_joints * (size_t)n_bins));
-    CK(cudaMemsetAsync(a.hist, 0, sizeof(int) * nrep * a.max_joints * (size_t)n_bins, c->st));
-  }
-  c->launches += sc::launch_analysis_sample(c->k, c->d, a.n_bins, a.max_joints, a.acc, a.hist, c->st);
-  CK(cudaGetLastError());
-  a.n_samples++;
-  return SC_OK;
-}
-
-sc_status sc_analysis_results(sc_ctx *c, double *mse2e, double *mse2e_err, int64_t *n_samples,
-                              int32_t *max_joints, int64_t *theta_hist) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  sc_ctx::Analysis &a = c->an;
-  const int nrep = (int)c->reps.size();
-  if (n_samples) *n_samples = a.n_samples;
-  if (max_joints) *max_joints = a.max_joints;
-  if (!a.acc || a.n_samples == 0) return SC_OK;
-  std::vector<double> acc(2 * (size_t)nrep);
-  CK(cudaMemcpyAsync(acc.data(), a.acc, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost, c->st));
-  std::vector<int> hist((size_t)nrep * a.max_joints * a.n_bins);
-  CK(cudaMemcpyAsync(hist.data(), a.hist, sizeof(int) * hist.size(), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  // FilamentSpecies::FinalizeMse2eAnalysis (src/filament_species.cpp:686-698).
-  for (int r = 0; r < nrep; ++r) {
-    const double num = c->reps[r].nf, ns = (double)a.n_samples;
-    const double m = acc[2 * r] / (ns * num), m2 = acc[2 * r + 1] / (ns * num);
-    if (mse2e) mse2e[r] = m;
-    if (mse2e_err) mse2e_err[r] = std::sqrt((m2 - m * m) / (num * ns));
-  }
-  if (theta_hist)
-    for (size_t i = 0; i < hist.size(); ++i) theta_hist[i] = hist[i];
-  return SC_OK;
-}
-
-sc_status sc_diffusion_init(sc_ctx *c, int interval) {
-  if (!c || !c->loaded || interval < 1) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  sc_ctx::Diffusion &a = c->dif;
-  const size_t nrep = c->reps.size();
-  if (!a.avg) {
-    CKS(dalloc(c, &a.avg, 9 * (size_t)c->nf));
-    CKS(dalloc(c, &a.pos0, 3 * (size_t)c->nf));
-    CKS(dalloc(c, &a.u0, 3 * (size_t)c->nf));
-  }
-  if (a.interval != interval) {
-    dfree(c, a.acc);
-    a.acc = nullptr;
-    CKS(dalloc(c, &a.acc, 4 * nrep * (size_t)interval));
-  }
-  CK(cudaMemsetAsync(a.acc, 0, sizeof(double) * 4 * nrep * interval, c->st));
-  a.interval = interval;
-  a.t = 0;
-  a.n_samples = 0;
-  // SpherocylinderSpecies::UpdateInitPositions: the current averages.
-  c->launches += sc::launch_filament_averages(c->k, c->d, a.avg, c->st);
-  c->launches += sc::launch_aos_to_origins(c->nf, a.avg, a.pos0, a.u0, c->st);
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(c->st));
-  return SC_OK;
-}
-
-sc_status sc_diffusion_sample(sc_ctx *c) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  sc_ctx::Diffusion &a = c->dif;
-  if (!a.acc) return fail(c, SC_ERR_INVALID_ARG, "sc_diffusion_sample needs sc_diffusion_init");
-  CK(cudaSetDevice(c->desc.device));
-  const int restart = a.t + 1 == a.interval ? 1 : 0;
-  c->launches += sc::launch_filament_averages(c->k, c->d, a.avg, c->st);
-  c->launches += sc::launch_diffusion_sample(c->k, c->d, a.avg, a.pos0, a.u0, a.acc, a.t,
-                                             a.interval, restart, c->st);
-  CK(cudaGetLastError());
-  a.t = restart ? 0 : a.t + 1;
-  a.n_samples++;
-  return SC_OK;
-}
-
-sc_status sc_diffusion_results(sc_ctx *c, double *msd, double *msd_err, double *vcf,
-                               double *vcf_err) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  sc_ctx::Diffusion &a = c->dif;
-  if (!a.acc) return fail(c, SC_ERR_INVALID_ARG, "sc_diffusion_results needs sc_diffusion_init");
-  CK(cudaSetDevice(c->desc.device));
-  const int nrep = (int)c->reps.size(), T = a.interval;
-  std::vector<double> acc(4 * (size_t)nrep * T);
-  CK(cudaMemcpyAsync(acc.data(), a.acc, sizeof(double) * acc.size(), cudaMemcpyDeviceToHost,
-                     c->st));
-  CK(cudaStreamSynchronize(c->st));
-  // SpherocylinderSpecies::FinalizeDiffusionAnalysis
-  // (src/spherocylinder_species.cpp:125-134).
-  for (int r = 0; r < nrep; ++r) {
-    const double *o = acc.data() + 4 * (size_t)T * r;
-    const double n = c->reps[r].nf;
-    for (int t = 0; t < T; ++t) {
-      const size_t i = (size_t)r * T + t;
-      if (msd) msd[i] = o[t] / o[T + t];
-      if (vcf) vcf[i] = o[2 * T + t] / o[3 * T + t];
-      if (msd_err) msd_err[i] = 1.0 / std::sqrt(n * o[T + t]);
-      if (vcf_err) vcf_err[i] = 1.0 / std::sqrt(n * o[3 * T + t]);
-    }
-  }
-  return SC_OK;
-}
-
-sc_status sc_global_order(sc_ctx *c, double *polar, double *nematic) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  sc_ctx::Analysis &a = c->an;
-  const int nrep = (int)c->reps.size();
-  if (!a.order) CKS(dalloc(c, &a.order, 12 * (size_t)nrep));
-  c->launches += sc::launch_global_order(c->k, c->d, a.order, c->st);
-  CK(cudaGetLastError());
-  std::vector<double> o(12 * (size_t)nrep);
-  CK(cudaMemcpyAsync(o.data(), a.order, sizeof(double) * o.size(), cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  for (int r = 0; r < nrep; ++r) {
-    for (int i = 0; i < 3; ++i)
-      if (polar) polar[3 * (size_t)r + i] = o[12 * (size_t)r + i];
-    for (int i = 0; i < 9; ++i)
-      if (nematic) nematic[9 * (size_t)r + i] = o[12 * (size_t)r + 3 + i];
-  }
-  return SC_OK;
-}
-
-sc_status sc_add_crosslinks(sc_ctx *c, int n, const int32_t *site_a, const int32_t *site_b,
-                            double k_spring, double k_spring_compress, double rest_length) {
-  if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
-  if (c->d.nx) return fail(c, SC_ERR_INVALID_ARG, "crosslinks already added");
-  if (c->i_step != 0) return fail(c, SC_ERR_INVALID_ARG, "crosslinks must be added before the first step");
-  if (n <= 0 || !site_a || !site_b) return fail(c, SC_ERR_INVALID_ARG, "bad crosslink arrays");
-  if (!(k_spring >= 0) || !(rest_length >= 0))
-    return fail(c, SC_ERR_INVALID_ARG, "bad spring constants");
-  CK(cudaSetDevice(c->desc.device));
-  // Anchor::AttachObjLambda (src/anchor.cpp:284-316): an anchor on site j of
-  // a filament is bound to bond j at lambda 0, one on the last site to the
-  // last bond at lambda = its length; its mesh lambda is the bond's (the
-  // summed lengths of the bonds before it, Mesh::UpdateBondPositions,
-  // src/mesh.cpp:324-330) plus lambda.  The lengths are Bond::ReInit's, from
-  // the loaded sites.
-  std::vector<double> xyz(3 * (size_t)c->ns);
-  CKS(copy_soa3(c, c->d.r, c->ns, xyz.data()));
-  std::vector<double> blen(c->nb), bml(c->nb);
-  for (int f = 0; f < c->nf; ++f) {
-    double true_length = 0.0;
-    for (int s0 = c->site_off[f]; s0 < c->site_off[f + 1] - 1; ++s0) {
-      double l = 0.0;
-      for (int i = 0; i < c->nd; ++i) {
-        const double u = xyz[3 * (size_t)(s0 + 1) + i] - xyz[3 * (size_t)s0 + i];
-        l += u * u;
-      }
-      const int b = s0 - f;
-      blen[b] = std::sqrt(l);
-      bml[b] = true_length;
-      true_length += blen[b];
-    }
-  }
-  std::vector<int> bond(2 * (size_t)n), xfil(2 * (size_t)n);
-  std::vector<double> xM(2 * (size_t)n);
-  for (int x = 0; x < n; ++x)
-    for (int a = 0; a < 2; ++a) {
-      const int site = a == 0 ? site_a[x] : site_b[x];
-      if (site < 0 || site >= c->ns)
-        return fail(c, SC_ERR_INVALID_ARG, "crosslink %d: site %d out of range", x, site);
-      const int f = (int)(std::upper_bound(c->site_off.begin(), c->site_off.end(), site) -
-                          c->site_off.begin()) - 1;
-      const bool last = site == c->site_off[f + 1] - 1;
-      const int b = last ? site - f - 1 : site - f;
-      const size_t A = 2 * (size_t)x + a;
-      bond[A] = b;
-      xfil[A] = f;
-      xM[A] = bml[b] + (last ? blen[b] : 0.0);
-      if (a == 1 && c->fil_rep[f] != c->fil_rep[xfil[A - 1]])
-        return fail(c, SC_ERR_INVALID_ARG, "crosslink %d joins two systems", x);
-    }
-  // Per-bond anchor lists, ascending anchor id (link order, anchor 0 first):
-  // each anchor on its bond and that bond's neighbours in the filament, the
-  // bonds it can move to as the filament's bonds stretch.
-  auto first_bond = [&](int f) { return c->site_off[f] - f; };
-  auto last_bond = [&](int f) { return c->site_off[f + 1] - f - 2; };
-  std::vector<int> off(c->nb + 1, 0), ent;
-  for (int A = 0; A < 2 * n; ++A)
-    for (int b = std::max(bond[A] - 1, first_bond(xfil[A]));
-         b <= std::min(bond[A] + 1, last_bond(xfil[A])); ++b)
-      off[b + 1]++;
-  for (int b = 0; b < c->nb; ++b) off[b + 1] += off[b];
-  ent.resize(off[c->nb]);
-  {
-    std::vector<int> fill(off.begin(), off.end() - 1);
-    for (int A = 0; A < 2 * n; ++A)
-      for (int b = std::max(bond[A] - 1, first_bond(xfil[A]));
-           b <= std::min(bond[A] + 1, last_bond(xfil[A])); ++b)
-        ent[fill[b]++] = A;
-  }
-  auto up = [&](auto **dst, const auto &v) -> sc_status {
-    using T = typename std::remove_reference<decltype(v)>::type::value_type;
-    T *q = nullptr;
-    CKS(dalloc(c, &q, v.size()));
-    CK(cudaMemcpyAsync(q, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, c->st));
-    *dst = q;
-    return SC_OK;
-  };
-  int *qi = nullptr;
-  double *qd = nullptr;
-  CKS(up(&qi, xfil)); c->d.xl_fil = qi;
-  CKS(up(&qi, off)); c->d.xb_off = qi;
-  CKS(up(&qi, ent)); c->d.xb_ent = qi;
-  CKS(up(&qd, xM)); c->d.xl_M = qd;
-  CKS(up(&qd, c->fil_len)); c->d.fil_L = qd;
-  CKS(dalloc(c, &c->d.bml, (size_t)c->nb));
-  CKS(dalloc(c, &c->d.ftl, (size_t)c->nf));
-  // Anchor records: zero force and torque on the attach bond.
-  std::vector<double> rec(16 * (size_t)n, 0.0);
-  for (int A = 0; A < 2 * n; ++A) rec[8 * (size_t)A + 6] = (double)bond[A];
-  CKS(up(&qd, rec)); c->d.xl_c = qd;
-  CKS(dalloc(c, &c->d.xl_F, 4 * (size_t)n));
-  CK(cudaMemsetAsync(c->d.xl_F, 0, sizeof(double) * 4 * (size_t)n, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  c->k.xk = k_spring;
-  c->k.xkc = k_spring_compress;
-  c->k.xrest = rest_length;
-  c->d.nx = n;
-  drop_graph(c);  // kernel parameters changed
-  return SC_OK;
-}
-
-sc_status sc_get_crosslink_forces(sc_ctx *c, double *f) {
-  if (!c || !c->loaded || !f) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  if (c->d.nx == 0) return SC_OK;
-  std::vector<double> tmp(4 * (size_t)c->d.nx);
-  CK(cudaMemcpyAsync(tmp.data(), c->d.xl_F, sizeof(double) * tmp.size(), cudaMemcpyDeviceToHost,
-                     c->st));
-  CK(cudaStreamSynchronize(c->st));
-  for (int x = 0; x < c->d.nx; ++x)
-    for (int i = 0; i < 3; ++i) f[3 * (size_t)x + i] = tmp[4 * (size_t)x + i];
-  return SC_OK;
 }
 
 sc_status sc_get_bond_geometry(sc_ctx *c, double *pos, double *spos, double *u,
@@ -2372,120 +1188,6 @@ sc_status sc_get_pairs(sc_ctx *c, int32_t *pairs, int64_t cap, int64_t *n_pairs)
       pairs[2 * out + 1] = b[i];
     }
   }
-  return SC_OK;
-}
-
-// ---- thermo ----------------------------------------------------------------
-
-sc_status sc_set_thermo(sc_ctx *c, int n_thermo) {
-  if (!c || !c->loaded || n_thermo < 0) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  DevState &d = c->d;
-  const int nrep = d.nrep;
-  if (c->k.thermo) CKS(thermo_pull(c));
-  if (n_thermo == 0) {
-    for (FILE *f : c->th_files)
-      if (f) std::fclose(f);
-    c->th_files.clear();
-    c->k.thermo = 0;
-    d.th_n = 0;
-    drop_graph(c);
-    return SC_OK;
-  }
-  if (!c->desc.interaction_flag)
-    return fail(c, SC_ERR_INVALID_ARG, "thermo needs pair interactions");
-  if (!d.th_part) {
-    CKS(dalloc(c, &d.th_part, (size_t)nrep * kThermoMaxBlocks * 9));
-    CKS(dalloc(c, &d.th_ticket, nrep));
-    CKS(dalloc(c, &d.th_acc, 9 * (size_t)nrep));
-    CKS(dalloc(c, &d.th_istep, nrep));
-    CKS(dalloc(c, &d.th_nrec, nrep));
-    d.th_cap = 256;
-    CKS(dalloc(c, &d.th_rec, 12 * (size_t)nrep * d.th_cap));
-  }
-  if (!(c->prec == 0 ? (void *)d.pv64 : (void *)d.pv32)) {
-    // Per-pair virial records, zeroed (a pair not evaluated since the list
-    // was built has stress and potential 0).
-    const size_t n = (size_t)(c->pcap > 0 ? c->pcap : 1);
-    if (c->prec == 0) {
-      CKS(dalloc(c, &d.pv64, 4 * n));
-      CK(cudaMemsetAsync(d.pv64, 0, sizeof(double) * 4 * n, c->st));
-    } else {
-      CKS(dalloc(c, &d.pv32, 4 * n));
-      CK(cudaMemsetAsync(d.pv32, 0, sizeof(float) * 4 * n, c->st));
-    }
-  }
-  std::vector<long long> ist(nrep, c->i_step);
-  CK(cudaMemsetAsync(d.th_ticket, 0, sizeof(unsigned) * nrep, c->st));
-  CK(cudaMemsetAsync(d.th_acc, 0, sizeof(double) * 9 * nrep, c->st));
-  CK(cudaMemsetAsync(d.th_nrec, 0, sizeof(long long) * nrep, c->st));
-  CK(cudaMemcpyAsync(d.th_istep, ist.data(), sizeof(long long) * nrep, cudaMemcpyHostToDevice,
-                     c->st));
-  CK(cudaStreamSynchronize(c->st));
-  c->th_i0 = c->i_step;
-  c->th_pulled = 0;
-  d.th_n = n_thermo;
-  c->k.thermo = 1;
-  drop_graph(c);
-  return SC_OK;
-}
-
-sc_status sc_thermo_open(sc_ctx *c, const char *run_name, int n_steps) {
-  if (!c || !c->loaded || !run_name || n_steps < 0) return SC_ERR_INVALID_ARG;
-  if (!c->k.thermo) return fail(c, SC_ERR_INVALID_ARG, "thermo is off");
-  if (!c->th_files.empty()) return fail(c, SC_ERR_INVALID_ARG, "thermo file already open");
-  CK(cudaSetDevice(c->desc.device));
-  CKS(thermo_pull(c));  // records taken before the file opened stay out of it
-  const size_t nrep = c->reps.size();
-  c->th_files.assign(nrep, nullptr);
-  for (size_t r = 0; r < nrep; ++r) {
-    std::string name = run_name;
-    if (nrep > 1) {
-      char sfx[32];
-      std::snprintf(sfx, sizeof(sfx), "_r%03zu", r);
-      name += sfx;
-    }
-    name += ".thermo";
-    FILE *f = std::fopen(name.c_str(), "wb");
-    if (!f) return fail(c, SC_ERR_INVALID_ARG, "cannot open %s", name.c_str());
-    // OutputManager::InitThermo (include/simcore/output_manager.hpp:156-168)
-    put(f, (int32_t)n_steps);
-    put(f, (int32_t)c->d.th_n);
-    put(f, c->desc.delta);
-    put(f, (int32_t)c->nd);
-    c->th_files[r] = f;
-  }
-  return SC_OK;
-}
-
-sc_status sc_get_thermo(sc_ctx *c, int max_records, int *n_records, int64_t *i_step,
-                        double *tensor, double *pressure, double *volume) {
-  if (!c || !c->loaded || max_records < 0 || !n_records) return SC_ERR_INVALID_ARG;
-  CK(cudaSetDevice(c->desc.device));
-  CKS(thermo_pull(c));
-  const size_t nrep = c->reps.size(), per = 12 * nrep;
-  const size_t n = std::min(c->th_host.size() / per, (size_t)max_records);
-  for (size_t k = 0; k < n; ++k)
-    for (size_t r = 0; r < nrep; ++r) {
-      const double *q = c->th_host.data() + per * k + 12 * r;
-      if (i_step && r == 0) i_step[k] = (int64_t)q[0];
-      if (tensor) std::memcpy(tensor + 9 * (k * nrep + r), q + 1, sizeof(double) * 9);
-      if (pressure) pressure[k * nrep + r] = q[10];
-      if (volume) volume[k * nrep + r] = q[11];
-    }
-  c->th_host.erase(c->th_host.begin(), c->th_host.begin() + per * n);
-  *n_records = (int)n;
-  return SC_OK;
-}
-
-sc_status sc_get_potential_energy(sc_ctx *c, double *pote) {
-  if (!c || !c->loaded || !pote) return SC_ERR_INVALID_ARG;
-  if (!c->k.thermo) return fail(c, SC_ERR_INVALID_ARG, "potential energies need thermo on");
-  CK(cudaSetDevice(c->desc.device));
-  c->launches += sc::launch_potential(c->d, c->prec, c->stage, c->st);
-  CK(cudaGetLastError());
-  CK(cudaMemcpyAsync(pote, c->stage, sizeof(double) * c->nf, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
   return SC_OK;
 }
 

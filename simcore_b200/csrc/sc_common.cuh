@@ -139,6 +139,7 @@ struct DevState {
   const int *blk_f0;       // per block: first filament
   const int *blk_nf;       // per block: filament count
   const int *blk_ns;       // per block: site count
+  int blk_maxf;            // most filaments in one block (shared-memory size)
   // integrator warp groups (filaments of at most 32 sites): runs of whole
   // filaments, one lane per site
   int n_wg;

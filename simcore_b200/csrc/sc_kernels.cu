@@ -23,6 +23,7 @@
 #include "sc_common.cuh"
 #include "sc_kernels.h"
 #include "sc_launch.h"
+#include "sc_cells.cuh"
 #include "sc_pair.cuh"
 #include "sc_step.cuh"
 #include "sc_step_warp.cuh"
@@ -51,41 +52,6 @@ __global__ void k_init_geometry(SysConst k, DevState d, int buf, int prec, int w
 
 // ---------------------------------------------------------------------------
 // Cell list.
-
-// CellList::FindCellCoords (src/cell_list.cpp:139-157) on the bond's scaled
-// position, recomputed exactly from its sites; the cell index within the
-// bond's system.
-template <int ND>
-__device__ __forceinline__ int bond_cell(const DevState &d, const ReplicaConst &R, int b,
-                                         int *xyz) {
-  int f = d.bond_fil[b];
-  int site = b + f;
-  double r1[3], r2[3], s[3], u[3], len;
-  for (int i = 0; i < 3; ++i) {
-    r1[i] = d.r[i][site];
-    r2[i] = d.r[i][site + 1];
-  }
-  bond_from_sites<ND>(R.hinv, r1, r2, s, u, len);
-  int c[3] = {0, 0, 0};
-  bool bad = false;
-#pragma unroll
-  for (int i = 0; i < ND; ++i) {
-    double x = s[i] + 0.5;
-    double fl = floor(R.n1d * x);
-    int cc = (fl >= 0.0 && fl <= (double)R.n1d) ? (int)fl : -1;
-    if (cc == R.n1d) cc -= 1;
-    if (cc < 0) {
-      bad = true;
-      cc = 0;
-    }
-    c[i] = cc;
-  }
-  if (bad) atomicOr(d.status, ST_BAD_CELL);
-  xyz[0] = c[0];
-  xyz[1] = c[1];
-  xyz[2] = c[2];
-  return (c[0] * R.n1d + c[1]) * R.third + c[2];
-}
 
 template <int ND>
 __global__ void k_bond_cells(SysConst k, DevState d, int *xyz) {
@@ -132,66 +98,6 @@ __global__ void k_bin_scatter(DevState d, const int *key, const int *cell_start,
   int c = key[b];
   int slot = atomicSub(&cell_count[c], 1) - 1;
   sorted[cell_start[c] + slot] = b;
-}
-
-// Pairs that ProcessPairInteraction marks no_interaction and the first
-// evaluation after a rebuild culls (src/interaction_manager.cpp:341-367,
-// 485-497): all pairs without like-like interactions, and bonds of one
-// filament that share a site (Bond::HasNeighbor, src/bond.cpp:118-121).
-__device__ __forceinline__ bool pair_excluded(const SysConst &k,
-                                              const DevState &d, int a, int b) {
-  if (!k.like_like) return true;
-  if (d.bond_fil[a] == d.bond_fil[b]) {
-    int diff = a - b;
-    if (diff <= 1 && diff >= -1) return true;
-  }
-  return false;
-}
-
-// Half-shell neighbour cells of (x, y, z) in the order of
-// CellList::AssignCellNeighbors(false) (src/cell_list.cpp:206-262), as
-// indices within the system, without compaction: entry kk (a compile-time
-// index) is the kk-th candidate of its loops -- (x+1, y, z); (x-1..x+1,
-// y+1, z); then, in 3D, (x-1..x+1, y-1..y+1, z+1), x fastest -- with
-// periodic wrap, and bit kk of the returned mask says it is kept (it is not
-// the cell itself, which wrap can give on small grids).  Visiting the set
-// bits in order visits the reference's neighbour list in its order, with
-// every index in registers.
-__device__ __forceinline__ unsigned half_shell_fixed(const SysConst &k, const ReplicaConst &R,
-                                                     int x, int y, int z, int out[13]) {
-  const int n1d = R.n1d;
-  unsigned mask = 0;
-#pragma unroll
-  for (int kk = 0; kk < 13; ++kk) {
-    const int dz = kk < 4 ? 0 : 1;
-    const int dy = kk == 0 ? 0 : (kk < 4 ? 1 : (kk - 4) / 3 - 1);
-    const int dx = kk == 0 ? 1 : (kk < 4 ? kk - 2 : (kk - 4) % 3 - 1);
-    int nx = x + dx, ny = y + dy, nz = z + dz;
-    if (nx < 0) nx = n1d - 1;
-    else if (nx == n1d) nx = 0;
-    if (ny < 0) ny = n1d - 1;
-    else if (ny == n1d) ny = 0;
-    if (nz == n1d) nz = 0;
-    out[kk] = (nx * n1d + ny) * R.third + nz;
-    const bool keep = (kk < 4 || k.n_dim == 3) && !(nx == x && ny == y && nz == z);
-    mask |= keep ? (1u << kk) : 0u;
-  }
-  return mask;
-}
-
-__device__ __forceinline__ void cell_coords(const ReplicaConst &R, int c, int &x, int &y,
-                                            int &z) {
-  z = c % R.third;
-  int t = c / R.third;
-  y = t % R.n1d;
-  x = t / R.n1d;
-}
-
-// Whether cell c holds a bond, from the occupancy bits the cell scan wrote
-// (a small array that stays in cache, unlike the cell offsets); without
-// them, every cell is looked up.
-__device__ __forceinline__ bool cell_occupied(const unsigned *occ, int c) {
-  return !occ || ((occ[c >> 5] >> (c & 31)) & 1u);
 }
 
 // One thread per cell head (first entry of a cell in the sorted order):
@@ -264,18 +170,6 @@ __global__ void k_cell_sort_count(SysConst k, DevState d, int nb, const int *key
     }
   }
   pair_count[q] = cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
-}
-
-// Pairs of rebuilt system r: the span of its cells' offsets.  A list longer
-// than its segment sets the overflow bit (the count is kept so the host can
-// size the segment).
-__device__ __forceinline__ void rep_pairs(const DevState &d, int r, const int *cell_start,
-                                          const int *pair_off) {
-  if (!d.due[r]) return;
-  const ReplicaConst &R = d.rep[r];
-  const int np = pair_off[cell_start[R.cell0 + R.n_cells]] - pair_off[cell_start[R.cell0]];
-  d.np_rep[r] = np;
-  if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
 }
 
 // Writes each cell's pairs at its offset in its system's pair segment, in the
@@ -352,25 +246,6 @@ __global__ void k_csr_offsets(DevState d, const int *deg_off, const int *deg) {
   const ReplicaConst &R = d.rep[r];
   d.e_off[b] = 2 * R.p0 + (deg_off[b] - deg_off[R.b0]);
   d.e_cnt[b] = deg[b];
-}
-
-// System of pair slot p (the segment that holds it).
-__device__ __forceinline__ int rep_of_pair(const DevState &d, int p) {
-  int lo = 0, hi = d.nrep - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (d.rep[mid].p0 <= p) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Slot p holds a current pair of its system.
-__device__ __forceinline__ bool pair_live(const DevState &d, int p, int &r) {
-  r = rep_of_pair(d, p);
-  const ReplicaConst &R = d.rep[r];
-  const int local = p - R.p0;
-  return local < R.pcap && local < d.np_rep[r];
 }
 
 // Entries (pair << 1 | role) of every bond of the rebuilt systems; role 0 =
@@ -714,11 +589,22 @@ __device__ __noinline__ void eval_near_parallel(NearParallelArgs a, int p) {
   pair_eval_fp64_sites<ND>(k, d, *a.R, p);
 }
 
+// Pair slot indices, written by the rebuild: a pair kernel may load them
+// before it waits for the kernel just before it (which never writes them).
+struct PairIdx {
+  int a, b, s1, s2;
+};
+__device__ __forceinline__ PairIdx pair_idx(const DevState &d, int p) {
+  return PairIdx{d.pa[p], d.pb[p], d.pos1[p], d.pos2[p]};
+}
+
 template <int ND, int PREC, bool NPX>
+
 __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
-                                              const ReplicaConst &R, int rbuf, int p) {
-  const int a = d.pa[p], b = d.pb[p];
-  const int s1 = d.pos1[p], s2 = d.pos2[p];
+                                              const ReplicaConst &R, int rbuf, int p,
+                                              const PairIdx &ix) {
+  const int a = ix.a, b = ix.b;
+  const int s1 = ix.s1, s2 = ix.s2;
   if (PREC == 0) {
     const BondGeomF64 A = d.g64[rbuf][a], B = d.g64[rbuf][b];
     double2 *stale = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)p;
@@ -801,20 +687,28 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
 // that it holds a current pair of its system.
 // NPX (mixed only): nearly parallel pairs are evaluated in FP64
 // (eval_near_parallel) by the thread that meets them.
+// The list and its slot indices date from the last rebuild, whose kernels
+// completed before the kernel just before this one waited (every kernel
+// waits before it lets the next one start): they are loaded before the
+// wait; the bond geometry, which that kernel may be writing, after it.
 template <int ND, int PREC, bool NPX>
-__global__ void __launch_bounds__(256, NPX ? 5 : 1) k_pair_eval(SysConst k, DevState d, int rbuf) {
-  grid_dep_sync();
+__global__ void __launch_bounds__(256, NPX ? 4 : 1) k_pair_eval(SysConst k, DevState d, int rbuf) {
   if (d.nrep == 1) {
     const ReplicaConst &R = d.rep[0];
     const int np = min(d.np_rep[0], R.pcap);
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < np; p += gridDim.x * blockDim.x)
-      pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p);
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    PairIdx ix = {0, 0, 0, 0};
+    if (p < np) ix = pair_idx(d, p);
+    grid_dep_sync();
+    for (bool first = true; p < np; p += gridDim.x * blockDim.x, first = false)
+      pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p, first ? ix : pair_idx(d, p));
     return;
   }
+  grid_dep_sync();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
        p += gridDim.x * blockDim.x) {
     int r;
-    if (pair_live(d, p, r)) pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p);
+    if (pair_live(d, p, r)) pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p, pair_idx(d, p));
   }
 }
 
@@ -826,7 +720,7 @@ __global__ void k_bond_sum(DevState d) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= d.nb) return;
   double F[3], T[3];
-  bond_pair_sum<ND, PREC>(d, b, F, T);
+  bond_pair_sum<ND, PREC>(d, b, d.e_off[b], d.e_off[b] + d.e_cnt[b], F, T);
   for (int i = 0; i < 3; ++i) {
     d.bF[i][b] = F[i];
     d.bT[i][b] = T[i];
@@ -1653,20 +1547,22 @@ int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t
   return 1;
 }
 
-size_t integrate_smem_bytes(int C) {
+size_t integrate_smem_bytes(int C, int max_filaments) {
   // (shared by both integrator units)
-  return sizeof(double) * integrate_smem_doubles(C) + sizeof(FilConst) * (size_t)(C / 2) +
-         sizeof(int) * (size_t)(C / 2);
+  return sizeof(double) * integrate_smem_doubles(C) + sizeof(int) * (size_t)(C / 2) +
+         sizeof(FilConst) * (size_t)max_filaments;
 }
 
 template <int ND, int PREC, int MAXC>
 static void set_attr(size_t smem) {
   cudaFuncSetAttribute(k_integrate<ND, PREC, false, MAXC>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_integrate<ND, PREC, false, MAXC, false, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 void prepare_integrate(int C) {
-  size_t smem = integrate_smem_bytes(C);
+  size_t smem = integrate_smem_bytes(C, C / 2);
   if (C <= 128) {
     set_attr<3, 0, 128>(smem);
     set_attr<3, 1, 128>(smem);
@@ -1712,10 +1608,12 @@ int launch_integrate(const SysConst &k, const DevState &d, int nblocks, int C,
     ++launched;
   }
   if (nblocks == 0) return launched;
-  size_t smem = integrate_smem_bytes(C);
-#define SC_INTEGRATE(ND, P, MC)                                              \
-  launch_pdl(k_integrate<ND, P, false, MC>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf, \
-                                                          interaction, capture)
+  size_t smem = integrate_smem_bytes(C, d.blk_maxf);
+#define SC_INTEGRATE(ND, P, MC)                                                                  \
+  ((C == MC) ? launch_pdl(k_integrate<ND, P, false, MC, false, true>, dim3(nblocks), dim3(C), smem, \
+                          st, k, d, midstep, rbuf, interaction, capture)                        \
+             : launch_pdl(k_integrate<ND, P, false, MC>, dim3(nblocks), dim3(C), smem, st, k, d,  \
+                          midstep, rbuf, interaction, capture))
   if (C <= 128) {
     if (k.n_dim == 3) {
       if (prec == 0) SC_INTEGRATE(3, 0, 128); else SC_INTEGRATE(3, 1, 128);

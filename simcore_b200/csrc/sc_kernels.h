@@ -60,6 +60,31 @@ int launch_pair_emit(const SysConst &k, const DevState &d, const int *key,
                      cudaStream_t st, const unsigned *occ = nullptr);
 // Per-bond entry lists; deg_off is the exclusive scan of deg over all bonds.
 int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st);
+// Scratch of a context's rebuild (sc_rebuild.cu).  Sizes: key, tmp, skey,
+// sval, pair_count, deg: nb; gcount: n_groups; gstart: n_groups + 1;
+// pair_off, deg_off: nb + 1; range: n_cells; occ: n_groups words;
+// scan_tmp: scan_temp_ints(max(n_groups, nb)).  gcount, deg, range and occ
+// start zeroed.
+struct RebuildBufs {
+  int n_groups;        // groups of 32 cells: n_cells / 32 (each system's cells
+                       // start at a multiple of 32)
+  uint32_t *key;       // cell key of every bond, bond order (n_cells: not rebuilt)
+  int *gcount;         // bonds per group (zero between rebuilds)
+  int *gstart;         // first sorted entry of each group
+  int *tmp;            // bonds by group, any order inside a group
+  uint32_t *skey;      // sorted cell keys
+  int *sval;           // sorted bond ids
+  int2 *range;         // per cell: [start, end) in the sorted order
+  unsigned *occ;       // per cell: occupied in the last rebuild of its system
+  int *pair_count, *pair_off;
+  int *deg, *deg_off;
+  int *scan_tmp;
+};
+// The whole rebuild of the systems flagged in d.due; returns the kernels
+// launched.  first_in_graph: the first kernel opens a captured conditional
+// body (launched without the programmatic-dependence attribute).
+int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, int prec,
+                   cudaStream_t st, bool first_in_graph);
 int launch_decide(const SysConst &k, const DevState &d,
                   cudaGraphConditionalHandle h, cudaStream_t st);
 int launch_loop_head(const DevState &d, cudaGraphConditionalHandle h,
@@ -82,7 +107,7 @@ int launch_thermo(const SysConst &k, const DevState &d, int prec, cudaStream_t s
 // Potential energy of every filament from the pair records.
 int launch_potential(const DevState &d, int prec, double *out, cudaStream_t st);
 int launch_bond_sum(const SysConst &k, const DevState &d, int prec, cudaStream_t st);
-size_t integrate_smem_bytes(int C);
+size_t integrate_smem_bytes(int C, int max_filaments);
 void prepare_integrate(int C);
 // fast: the contraction/reciprocal variant (mixed precision only).
 // fuse (fast mixed only): the integrator evaluates the pairs itself, in place

@@ -20,10 +20,27 @@ static void set_attr_fast(size_t smem) {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC, true>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC, false, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_integrate<ND, 1, true, MAXC, true, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// The block kernel compiled for up to MAXC sites, with compile-time offsets
+// when the block has exactly MAXC.
+template <int ND, bool FUSE, int MAXC>
+static void launch_block_fast(const SysConst &k, const DevState &d, int nblocks, int C, size_t smem,
+                              int midstep, int rbuf, int interaction, int capture, cudaStream_t st) {
+  if (C == MAXC)
+    launch_pdl(k_integrate<ND, 1, true, MAXC, FUSE, true>, dim3(nblocks), dim3(C), smem, st, k, d,
+               midstep, rbuf, interaction, capture);
+  else
+    launch_pdl(k_integrate<ND, 1, true, MAXC, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d,
+               midstep, rbuf, interaction, capture);
 }
 
 void prepare_integrate_fast(int C) {
-  size_t smem = integrate_smem_bytes(C);
+  size_t smem = integrate_smem_bytes(C, C / 2);
   if (C <= 128) {
     set_attr_fast<3, 128>(smem);
     set_attr_fast<2, 128>(smem);
@@ -50,19 +67,15 @@ static int launch_fast(const SysConst &k, const DevState &d, int nblocks, int C,
     ++launched;
   }
   if (nblocks == 0) return launched;
-  const size_t smem = integrate_smem_bytes(C);
+  const size_t smem = integrate_smem_bytes(C, d.blk_maxf);
   if (C <= 128)
-    launch_pdl(k_integrate<ND, 1, true, 128, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
-                                                                  interaction, capture);
+    launch_block_fast<ND, FUSE, 128>(k, d, nblocks, C, smem, midstep, rbuf, interaction, capture, st);
   else if (C <= 192)
-    launch_pdl(k_integrate<ND, 1, true, 192, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
-                                                                  interaction, capture);
+    launch_block_fast<ND, FUSE, 192>(k, d, nblocks, C, smem, midstep, rbuf, interaction, capture, st);
   else if (C <= 256)
-    launch_pdl(k_integrate<ND, 1, true, 256, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
-                                                                  interaction, capture);
+    launch_block_fast<ND, FUSE, 256>(k, d, nblocks, C, smem, midstep, rbuf, interaction, capture, st);
   else
-    launch_pdl(k_integrate<ND, 1, true, 512, FUSE>, dim3(nblocks), dim3(C), smem, st, k, d, midstep, rbuf,
-                                                                  interaction, capture);
+    launch_block_fast<ND, FUSE, 512>(k, d, nblocks, C, smem, midstep, rbuf, interaction, capture, st);
   return launched + 1;
 }
 

@@ -1,0 +1,394 @@
+// Pair-list rebuild of a context (InteractionManager::UpdateInteractions,
+// src/interaction_manager.cpp:211-231, over CellList::MakePairs,
+// src/cell_list.cpp:139-199, and Cell::MakePairs, src/cell.cpp:14-70).
+//
+// The bonds of the rebuilt systems are sorted by cell with a two-level
+// (most-significant-digit first) radix sort on the cell key: a counting pass
+// on the high digits -- the group of 32 consecutive cells, one occupancy word
+// -- and then, inside every group, each bond's rank by (cell, bond id).  The
+// ranking keeps every cell's bonds in bond order, the order in which
+// Cell::AddObj appends them.  The counting pass scans one counter per group
+// (n_cells / 32 of them), not the cell grid; cell ranges and occupancy bits
+// are written where cells start and end in the sorted order.
+//
+//   k_rb_keys      cell key of every bond, group counts; clears the
+//                  occupancy words of the rebuilt systems
+//   (scan)         group offsets
+//   k_rb_scatter   bonds into their groups (counts back to zero)
+//   k_rb_rank      stable order inside each group; cell ranges and bits
+//   k_rb_count     pairs of every cell (head entry of the sorted order)
+//   (scan)         pair offsets
+//   k_rb_emit      pairs in the reference's order, per-bond degrees
+//   (scan)         entry offsets
+//   k_rb_csr_fill  entries (pair << 1 | role) of every bond
+//   k_rb_csr_sort  entries in pair order, slots of both roles, ranges
+//   k_rb_finish    ZeroDrTot and the rebuild counters
+#include <cuda_runtime.h>
+
+#include "sc_cells.cuh"
+#include "sc_common.cuh"
+#include "sc_kernels.h"
+#include "sc_launch.h"
+
+namespace sc {
+
+// Bonds of the rebuilt systems: cell key (system's first cell + cell within
+// it) and warp-aggregated group counts; others get the sentinel n_cells.
+// Clears the occupancy words of the rebuilt systems (each system's cells
+// start at a multiple of 32: a word, a group, belongs to one system).
+template <int ND>
+__global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nthreads = gridDim.x * blockDim.x;
+  for (int r = 0; r < d.nrep; ++r) {
+    if (!d.due[r]) continue;
+    const ReplicaConst &R = d.rep[r];
+    const int w0 = R.cell0 >> 5, w1 = (R.cell0 + R.n_cells + 31) >> 5;
+    for (int w = w0 + tid; w < w1; w += nthreads) rb.occ[w] = 0u;
+  }
+  const int b = tid;
+  bool in = false;
+  int g = 0;
+  if (b < d.nb) {
+    uint32_t c = (uint32_t)k.n_cells;
+    const int r = rep_of_bond(d, b);
+    if (d.due[r]) {
+      const ReplicaConst &R = d.rep[r];
+      int xyz[3];
+      c = (uint32_t)(R.cell0 + bond_cell<ND>(d, R, b, xyz));
+      in = true;
+      g = (int)(c >> 5);
+    }
+    rb.key[b] = c;
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, in);
+  if (in) {
+    const unsigned peers = __match_any_sync(mask, g);
+    if ((int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&rb.gcount[g], __popc(peers));
+  }
+}
+
+// Each rebuilt bond into its group's range of the scanned offsets (any
+// order inside the group); decrements the counts back to zero, ready for
+// the next rebuild.
+__global__ void k_rb_scatter(DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb || !d.due[rep_of_bond(d, b)]) return;
+  const int g = (int)(rb.key[b] >> 5);
+  const int slot = atomicSub(&rb.gcount[g], 1) - 1;
+  rb.tmp[rb.gstart[g] + slot] = b;
+}
+
+// Sorted position of every rebuilt bond: its group's first entry plus the
+// number of bonds of the group that come before it by (cell, bond id).  The
+// first of a cell writes the cell's start and occupancy bit, the last its
+// end.
+__global__ void k_rb_rank(DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= rb.gstart[rb.n_groups]) return;
+  const int b = rb.tmp[q];
+  const uint32_t c = rb.key[b];
+  const int g = (int)(c >> 5);
+  const int s = rb.gstart[g], e = rb.gstart[g + 1];
+  int rank = 0;
+  bool first = true, last = true;
+  for (int j = s; j < e; ++j) {
+    const int bj = rb.tmp[j];
+    const uint32_t cj = rb.key[bj];
+    rank += (cj < c || (cj == c && bj < b)) ? 1 : 0;
+    if (cj == c) {
+      first = first && !(bj < b);
+      last = last && !(bj > b);
+    }
+  }
+  const int pos = s + rank;
+  rb.skey[pos] = c;
+  rb.sval[pos] = b;
+  if (first) {
+    rb.range[c].x = pos;
+    atomicOr(&rb.occ[c >> 5], 1u << (c & 31));
+  }
+  if (last) rb.range[c].y = pos + 1;
+}
+
+__device__ __forceinline__ bool occupied(const unsigned *occ, int c) {
+  return (occ[c >> 5] >> (c & 31)) & 1u;
+}
+
+// Sorted span [lo, hi) of system R's bonds: its groups' entries.
+__device__ __forceinline__ int sys_lo(const RebuildBufs &rb, const ReplicaConst &R) {
+  return rb.gstart[R.cell0 >> 5];
+}
+__device__ __forceinline__ int sys_hi(const RebuildBufs &rb, const ReplicaConst &R) {
+  return rb.gstart[(R.cell0 + R.n_cells + 31) >> 5];
+}
+
+// Pairs the cell whose head is sorted entry q contributes (zero for the
+// other entries): m (m - 1) / 2 inside it plus m * m_nbr with each kept
+// half-shell neighbour, less one for each bond whose filament neighbour
+// (b - 1 or b + 1) lies in the cell itself (counted once) or in a
+// neighbour -- the pairs pair_excluded drops.
+__global__ void k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= d.nb) return;
+  int cnt_out = 0;
+  const int n_due = rb.gstart[rb.n_groups];
+  if (q < n_due && k.like_like) {
+    const int c = (int)rb.skey[q];
+    if (q == 0 || (int)rb.skey[q - 1] != c) {
+      const int m = rb.range[c].y - q;
+      const int *it = rb.sval + q;
+      const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, it[0]) : 0];
+      int x, y, z, nbr[13];
+      cell_coords(R, c - R.cell0, x, y, z);
+      const unsigned keep = half_shell_fixed(k, R, x, y, z, nbr);
+      long long cnt = (long long)m * (m - 1) / 2;
+#pragma unroll
+      for (int kk = 0; kk < 13; ++kk) {
+        nbr[kk] += R.cell0;
+        if ((keep >> kk) & 1u) {
+          if (occupied(rb.occ, nbr[kk])) {
+            const int2 g = rb.range[nbr[kk]];
+            cnt += (long long)m * (g.y - g.x);
+          }
+        } else {
+          nbr[kk] = -1;  // matches no cell key
+        }
+      }
+      for (int i = 0; i < m; ++i) {
+        const int a = it[i], fa = d.bond_fil[a];
+        if (a + 1 < d.nb && d.bond_fil[a + 1] == fa) {
+          const int ka = (int)rb.key[a + 1];
+          if (ka == c) --cnt;  // each adjacent pair inside the cell, once
+#pragma unroll
+          for (int kk = 0; kk < 13; ++kk) cnt -= ka == nbr[kk];
+        }
+        if (a > 0 && d.bond_fil[a - 1] == fa) {
+          const int ka = (int)rb.key[a - 1];
+#pragma unroll
+          for (int kk = 0; kk < 13; ++kk) cnt -= ka == nbr[kk];
+        }
+      }
+      cnt_out = cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
+    }
+  }
+  rb.pair_count[q] = cnt_out;
+}
+
+// Writes each cell's pairs at its offset in its system's pair segment, in the
+// reference's list order (Cell::MakePairs, src/cell.cpp:14-22): pairs inside
+// the cell, then with each half-shell neighbour in order; clears each new
+// pair's stored force and counts per-bond entries.  Only the non-empty
+// neighbours are visited (a warp steps through as many as its busiest lane
+// has, not all 13).  Threads q < nrep record their system's pair count (a
+// list longer than its segment sets the overflow bit; the count is kept so
+// the host can size the segment).
+__global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
+  grid_dep_sync();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < d.nrep && d.due[q]) {
+    const ReplicaConst &R = d.rep[q];
+    const int np = rb.pair_off[sys_hi(rb, R)] - rb.pair_off[sys_lo(rb, R)];
+    d.np_rep[q] = np;
+    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+  }
+  if (q >= rb.gstart[rb.n_groups] || !k.like_like) return;
+  const int c = (int)rb.skey[q];
+  if (q > 0 && (int)rb.skey[q - 1] == c) return;
+  const int *it = rb.sval + q;
+  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, it[0]) : 0];
+  const int m = rb.range[c].y - q;
+  const int p0 = R.p0, pcap = R.pcap;
+  int p = rb.pair_off[q] - rb.pair_off[sys_lo(rb, R)];
+  int x, y, z, nbr[13];
+  cell_coords(R, c - R.cell0, x, y, z);
+  const unsigned keep = half_shell_fixed(k, R, x, y, z, nbr);
+  int s0[13], s1[13];
+  unsigned busy = 0;
+#pragma unroll
+  for (int kk = 0; kk < 13; ++kk) {  // all ranges loaded together
+    s0[kk] = s1[kk] = 0;
+    const int cn = R.cell0 + nbr[kk];
+    if (((keep >> kk) & 1u) && occupied(rb.occ, cn)) {
+      const int2 g = rb.range[cn];
+      s0[kk] = g.x;
+      s1[kk] = g.y;
+      busy |= 1u << kk;
+    }
+  }
+  auto emit = [&](int a, int b) {
+    if (pair_excluded(k, d, a, b)) return;
+    if (p < pcap) {
+      const int g = p0 + p;
+      d.pa[g] = a;
+      d.pb[g] = b;
+      if (prec == 0) {
+        double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)g;
+        st[0] = make_double2(0.0, 0.0);
+        st[1] = make_double2(0.0, 0.0);
+        if (d.pv64) {  // a new Interaction's stress and potential are 0
+          double2 *v = reinterpret_cast<double2 *>(d.pv64) + 2 * (size_t)g;
+          v[0] = make_double2(0.0, 0.0);
+          v[1] = make_double2(0.0, 0.0);
+        }
+      } else {
+        reinterpret_cast<float4 *>(d.pf32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (d.pv32) reinterpret_cast<float4 *>(d.pv32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      atomicAdd(&rb.deg[a], 1);
+      atomicAdd(&rb.deg[b], 1);
+    }
+    ++p;
+  };
+  for (int i = 0; i < m - 1; ++i)
+    for (int j = i + 1; j < m; ++j) emit(it[i], it[j]);
+  while (busy) {
+    const int kk = __ffs(busy) - 1;
+    busy &= busy - 1;
+    int lo = 0, hi = 0;
+#pragma unroll
+    for (int q2 = 0; q2 < 13; ++q2)
+      if (q2 == kk) {
+        lo = s0[q2];
+        hi = s1[q2];
+      }
+    for (int i = 0; i < m; ++i)
+      for (int j = lo; j < hi; ++j) emit(it[i], rb.sval[j]);
+  }
+}
+
+// First entry slot of bond b (rebuilt system R): its system's slots start at
+// 2 p0, its bonds' entries follow in bond order.
+__device__ __forceinline__ int entry_first(const RebuildBufs &rb, const ReplicaConst &R, int b) {
+  return 2 * R.p0 + (rb.deg_off[b] - rb.deg_off[R.b0]);
+}
+
+// Entries (pair << 1 | role; role 0 = obj1, 1 = obj2) of every bond of the
+// rebuilt systems, in any order; the degrees are decremented back to zero.
+__global__ void k_rb_csr_fill(DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= d.pcap_total) return;
+  int r;
+  if (!pair_live(d, p, r) || !d.due[r]) return;
+  const ReplicaConst &R = d.rep[r];
+  const int a = d.pa[p], b = d.pb[p];
+  const int sa = atomicSub(&rb.deg[a], 1) - 1;
+  const int sb = atomicSub(&rb.deg[b], 1) - 1;
+  d.e_ent[entry_first(rb, R, a) + sa] = p << 1;
+  d.e_ent[entry_first(rb, R, b) + sb] = (p << 1) | 1;
+}
+
+// Each bond's entries sorted by pair index -- the order in which the
+// reference's serial ApplyPairInteractions adds them to the bond -- in
+// registers up to kRegEntries of them; the slot of each (pair, role)
+// entry; the bond's entry range.
+constexpr int kRegEntries = 16;
+
+__global__ void k_rb_csr_sort(DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= d.nb) return;
+  const int r = rep_of_bond(d, b);
+  if (!d.due[r]) return;
+  const ReplicaConst &R = d.rep[r];
+  const int e0 = entry_first(rb, R, b), n = rb.deg_off[b + 1] - rb.deg_off[b];
+  d.e_off[b] = e0;
+  d.e_cnt[b] = n;
+  int *e = d.e_ent + e0;
+  if (n <= kRegEntries) {
+    int v[kRegEntries];
+#pragma unroll
+    for (int i = 0; i < kRegEntries; ++i) v[i] = i < n ? e[i] : 0x7fffffff;
+    // Odd-even transposition sort: kRegEntries rounds sort kRegEntries keys.
+#pragma unroll
+    for (int round = 0; round < kRegEntries; ++round) {
+#pragma unroll
+      for (int i = round & 1; i + 1 < kRegEntries; i += 2) {
+        const int lo = min(v[i], v[i + 1]), hi = max(v[i], v[i + 1]);
+        v[i] = lo;
+        v[i + 1] = hi;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kRegEntries; ++i) {
+      if (i < n) {
+        e[i] = v[i];
+        if (v[i] & 1) d.pos2[v[i] >> 1] = e0 + i;
+        else d.pos1[v[i] >> 1] = e0 + i;
+      }
+    }
+    return;
+  }
+  for (int i = 1; i < n; ++i) {
+    const int v = e[i];
+    int j = i - 1;
+    while (j >= 0 && e[j] > v) {
+      e[j + 1] = e[j];
+      --j;
+    }
+    e[j + 1] = v;
+  }
+  for (int i = 0; i < n; ++i) {
+    const int ent = e[i];
+    if (ent & 1) d.pos2[ent >> 1] = e0 + i;
+    else d.pos1[ent >> 1] = e0 + i;
+  }
+}
+
+// InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321) for
+// the rebuilt systems, and the rebuild counters.
+__global__ void k_rb_finish(DevState d) {
+  grid_dep_sync();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *d.n_rebuilds += 1;
+  if (i < d.nrep && d.due[i]) {
+    d.dr_max_bits[i] = 0ull;
+    d.rep_rebuilds[i] += 1;
+  }
+  if (i >= d.ns) return;
+  if (!d.due[d.fil[d.site_fil[i]].rep]) return;
+  d.dz[0][i] = d.r[0][i];
+  d.dz[1][i] = d.r[1][i];
+  d.dz[2][i] = d.r[2][i];
+  d.dt[i] = 0.0;
+}
+
+int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, int prec,
+                   cudaStream_t st, bool first_in_graph) {
+  int launched = 0;
+  const int nb = d.nb > 0 ? d.nb : 1;
+  const int g256 = (nb + 255) / 256;
+  if (first_in_graph) {
+    // Captured, the first kernel starts the conditional body: no kernel
+    // before it to overlap.
+    PdlOff off;
+    if (k.n_dim == 3) launch_pdl(k_rb_keys<3>, dim3(g256), dim3(256), 0, st, k, d, rb);
+    else launch_pdl(k_rb_keys<2>, dim3(g256), dim3(256), 0, st, k, d, rb);
+  } else {
+    if (k.n_dim == 3) launch_pdl(k_rb_keys<3>, dim3(g256), dim3(256), 0, st, k, d, rb);
+    else launch_pdl(k_rb_keys<2>, dim3(g256), dim3(256), 0, st, k, d, rb);
+  }
+  ++launched;
+  launched += launch_exclusive_scan(rb.gcount, rb.gstart, rb.n_groups, rb.scan_tmp, st);
+  launch_pdl(k_rb_scatter, dim3(g256), dim3(256), 0, st, d, rb);
+  launch_pdl(k_rb_rank, dim3(g256), dim3(256), 0, st, d, rb);
+  launch_pdl(k_rb_count, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb);
+  launched += 3;
+  launched += launch_exclusive_scan(rb.pair_count, rb.pair_off, d.nb, rb.scan_tmp, st);
+  launch_pdl(k_rb_emit, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb, prec);
+  ++launched;
+  launched += launch_exclusive_scan(rb.deg, rb.deg_off, d.nb, rb.scan_tmp, st);
+  launch_pdl(k_rb_csr_fill, dim3((d.pcap_total > 0 ? d.pcap_total + 255 : 256) / 256), dim3(256),
+             0, st, d, rb);
+  launch_pdl(k_rb_csr_sort, dim3(g256), dim3(256), 0, st, d, rb);
+  const int gfin = ((d.ns > d.nrep ? d.ns : d.nrep) + 255) / 256;
+  launch_pdl(k_rb_finish, dim3(gfin > 0 ? gfin : 1), dim3(256), 0, st, d);
+  return launched + 3;
+}
+
+}  // namespace sc

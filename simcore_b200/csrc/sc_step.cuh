@@ -122,11 +122,12 @@ __device__ __forceinline__ void bond_xlink_sum(const DevState &d, int b, double 
 // bond's pair contributions in slot (= pair) order.  FP64 sums as the
 // reference accumulates them; in mixed precision FP32 sums with Kahan
 // compensation, added to the FP64 crosslink sum.  A pair slot is 8 values: force (3), torque (3),
-// padding (2).
+// padding (2).  [e0, e1) is the bond's slot range (e_off, e_off + e_cnt),
+// which the integrators load before they wait for the pair stage: the
+// rebuild wrote it, before the pair stage ran.
 template <int ND, int PREC>
-__device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F[3],
-                                              double T[3]) {
-  const int e0 = d.e_off[b], e1 = e0 + d.e_cnt[b];
+__device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, int e0, int e1,
+                                              double F[3], double T[3]) {
   F[0] = F[1] = F[2] = 0.0;
   T[0] = T[1] = T[2] = 0.0;
   if (d.nx) bond_xlink_sum<ND>(d, b, F, T);
@@ -146,7 +147,7 @@ __device__ __forceinline__ void bond_pair_sum(const DevState &d, int b, double F
     float sF[3] = {0.f, 0.f, 0.f}, cF[3] = {0.f, 0.f, 0.f};
     float sT[3] = {0.f, 0.f, 0.f}, cT[3] = {0.f, 0.f, 0.f};
     const float4 *c = reinterpret_cast<const float4 *>(d.cf32) + 2 * (size_t)e0;
-#pragma unroll 2
+#pragma unroll 4
     for (int e = e0; e < e1; ++e, c += 2) {
       const float4 v0 = c[0], v1 = c[1];
       kahan_add(sF[0], cF[0], v0.x);
@@ -266,6 +267,17 @@ __device__ __forceinline__ double recip_nr(double x) {
   return fma(y, e, y);
 }
 
+// ((double)w + 0.5) * 2^-32 - 0.5 for a 32-bit Philox word w, the noise's
+// uniform on (-1/2, 1/2).  w + 1/2 is formed exactly from bits -- 2^51 + w +
+// 1/2 is the double with exponent 51 and mantissa 2w + 1 -- instead of by an
+// integer-to-double conversion; the product with 2^-32 is exact, so the
+// result has the same bits as the expression above.
+__device__ __forceinline__ double centered_uniform(uint32_t w) {
+  const double h =
+      __longlong_as_double(0x4320000000000000ll | (((long long)w << 1) | 1ll)) - 2251799813685248.0;
+  return h * 2.3283064365386963e-10 - 0.5;
+}
+
 // FAST: one Newton reciprocal per row instead of two divisions.
 __device__ __forceinline__ void thomas_fast(double *a, const double *b, double *c,
                                             double *d, int n) {
@@ -300,6 +312,91 @@ __device__ __forceinline__ void solve_tridiag(double *a, const double *b, double
   else thomas(a, b, c, d, n);
 }
 
+// Two-sided ("twisted") elimination of one tridiagonal system of n rows for
+// the fast integrator (van der Vorst, "Large tridiagonal and block
+// tridiagonal linear systems on vector and parallel computers", Parallel
+// Computing 5:45-54, 1987): a pair of lanes of one warp, the top lane
+// eliminating rows 0..m-1 downwards and the bottom lane rows n-1..m+1
+// upwards, meet at row m = n/2, then substitute back outwards.  Half the
+// sequential depth of thomas_fast, the same layout (row r: lower coefficient
+// a[r-1], diagonal b[r], upper c[r], right-hand side d[r]); the solution
+// ends in d.  Both lanes of the pair (lanes 2k, 2k+1) call it, and both run
+// one instruction stream: P[r] is the coupling to the row eliminated before
+// (a[r-1] going down, c[r] going up), Q[r] the one towards row m, which the
+// elimination overwrites with its reduced value.
+__device__ __forceinline__ void thomas_twisted(double *a, const double *b, double *c,
+                                               double *d, int n, bool top) {
+  const unsigned pair = 3u << ((threadIdx.x & 31) & 30);
+  const int m = n >> 1;
+  const int steps = top ? m : n - 1 - m;
+  const int dir = top ? 1 : -1;
+  const int r0 = top ? 0 : n - 1;
+  const double *P = top ? a - 1 : c;
+  double *Q = top ? c : a - 1;
+  double u = 0.0, v = 0.0;  // reduced (Q, d) of the last row eliminated
+  if (steps > 0) {
+    const double rr = recip_nr(b[r0]);
+    u = Q[r0] * rr;
+    v = d[r0] * rr;
+    Q[r0] = u;
+    d[r0] = v;
+    int r = r0 + dir;
+    for (int st = 1; st < steps; ++st, r += dir) {
+      const double pc = P[r];
+      const double ri = recip_nr(b[r] - pc * u);
+      const double un = Q[r] * ri;
+      const double vn = (d[r] - pc * v) * ri;
+      Q[r] = un;
+      d[r] = vn;
+      u = un;
+      v = vn;
+    }
+  }
+  const double u2 = __shfl_xor_sync(pair, u, 1), v2 = __shfl_xor_sync(pair, v, 1);
+  const double tu = top ? u : u2, tv = top ? v : v2;  // row m-1: c', d'
+  const double bu = top ? u2 : u, bv = top ? v2 : v;  // row m+1: a', d'
+  double num = d[m], den = b[m];
+  if (m >= 1) {
+    num -= a[m - 1] * tv;
+    den -= a[m - 1] * tu;
+  }
+  if (m + 1 <= n - 1) {
+    num -= c[m] * bv;
+    den -= c[m] * bu;
+  }
+  double x = num * recip_nr(den);
+  __syncwarp(pair);  // both lanes have read row m
+  if (top) d[m] = x;
+  int r = m - dir;
+  for (int st = 0; st < steps; ++st, r -= dir) {
+    x = d[r] - Q[r] * x;
+    d[r] = x;
+  }
+}
+
+// Metric determinants of filament q of a block (CalculateBendingForces,
+// src/filament.cpp:627-660): det_t forward and det_b backward, each on its
+// own lane; filament q's values start at slot (first site) + q.
+__device__ __forceinline__ void det_forward(double *sdt, const double *scos, const FilConst &f,
+                                            int s0, int q) {
+  const int fb0 = f.site0 - s0, nn = f.n;
+  double *dt = sdt + fb0 + q;
+  const double *cs = scos + fb0;
+  dt[0] = 1;
+  dt[1] = 2;
+  for (int i = 2; i < nn; ++i) dt[i] = 2 * dt[i - 1] - (-cs[i - 2]) * (-cs[i - 2]) * dt[i - 2];
+}
+__device__ __forceinline__ void det_backward(double *sdb, const double *scos, const FilConst &f,
+                                             int s0, int q) {
+  const int fb0 = f.site0 - s0, nn = f.n;
+  double *db = sdb + fb0 + q;
+  const double *cs = scos + fb0;
+  db[nn] = 1;
+  db[nn - 1] = 2;
+  for (int i = 2; i < nn; ++i)
+    db[nn - i] = 2 * db[nn - i + 1] - (-cs[nn - i - 1]) * (-cs[nn - i - 1]) * db[nn - i + 2];
+}
+
 // v /= |v| over ND components.  Exact: the reference's normalize_vector
 // (src/linear_algebra.cpp:26-35).  FAST: one rsqrt and ND products.
 template <int ND, bool FAST>
@@ -327,9 +424,10 @@ __device__ __forceinline__ double dotn(const double *a, const double *b) {
   return m;
 }
 
-// Shared-memory words of one integrator block of C sites.
+// Shared-memory words of one integrator block of C sites (the doubles; C/2
+// renormalisation flags and the block's filament constants follow).
 __host__ __device__ constexpr size_t integrate_smem_doubles(int C) {
-  return 27 * (size_t)C;
+  return 24 * (size_t)C;
 }
 
 // 8-byte asynchronous global -> shared copy (cp.async), completed by
@@ -419,14 +517,15 @@ struct IntegrateBounds {
 
 // FUSE (fast mixed step only): each bond evaluates its own pairs
 // (bond_pair_eval_sum) instead of summing the pair stage's slots.
-template <int ND, int PREC, bool FAST, int MAXC, bool FUSE = false>
+// FIXC: launched with exactly MAXC threads, so every shared-memory offset is
+// a compile-time constant.
+template <int ND, int PREC, bool FAST, int MAXC, bool FUSE = false, bool FIXC = false>
 __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     k_integrate(SysConst k, DevState d, int midstep, int rbuf, int interaction,
                 int capture) {
   extern __shared__ double smem[];
-  const int C = blockDim.x;
-  double *sr = smem;            // positions            3C
-  double *su = sr + 3 * C;      // site orientations    3C
+  const int C = FIXC ? MAXC : (int)blockDim.x;
+  double *su = smem;            // site orientations    3C
   double *stn = su + 3 * C;     // tangents             3C
   double *sfr = stn + 3 * C;    // random forces; bond torques in P0-P1  3C
   double *sbF = sfr + 3 * C;    // bond forces, then gamma^-1 F          3C
@@ -436,15 +535,19 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   double *sb = sa + C;          // diagonal             C
   double *sc = sb + C;          // upper diagonal       C
   double *skeff = sc + C;       // k_eff                C
-  // The metric determinants live only in the bending stage, after the
-  // random-force solve has been read and before the tension system is
-  // written: they share the Thomas arrays (sT, sa, sb, sc).
-  double *sdt = sT;             // det_t                2C
-  double *sdb = sT + 2 * C;     // det_b                2C
   double *srp = skeff + C;      // full step: prefetched previous positions 3C
   double *sfp = srp + 3 * C;    // full step: prefetched projected noise     3C
-  FilConst *sfil = (FilConst *)(sfp + 3 * C);   // C/2 filaments
-  int *sflag = (int *)(sfil + C / 2);           // C/2 renormalisation flags
+  // New positions (P5 on) take the slots of the previous positions: each
+  // thread reads its own previous position before it writes its new one.
+  double *sr = srp;             // positions            3C
+  // The metric determinants (P3): in a midstep in the prefetch area, which
+  // only full steps use, so that they are computed alongside the
+  // random-force solve; in a full step in the Thomas arrays (sT, sa, sb,
+  // sc), free between the two solves' uses.
+  double *sdt = midstep ? srp : sT;  // det_t     2C
+  double *sdb = sdt + 2 * C;         // det_b     2C
+  int *sflag = (int *)(sfp + 3 * C);            // C/2 renormalisation flags
+  FilConst *sfil = (FilConst *)(sflag + C / 2); // the block's filaments
   __shared__ double s_drmax[32];
 
 #define V(arr, slot, comp) arr[(comp) * C + (slot)]
@@ -514,12 +617,17 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
       cp_async_commit();
     }
   }
+  int e0 = 0, e1 = 0;  // the bond's pair slots
   if (has_bond) {
     // Site orientation = orientation of its bond as Bond::ReInit left it
     // (Mesh::UpdateSiteOrientations, src/mesh.cpp:168-173).
     u[0] = d.ub[0][b];
     u[1] = d.ub[1][b];
     u[2] = d.ub[2][b];
+    if (!FUSE && interaction) {
+      e0 = d.e_off[b];
+      e1 = e0 + d.e_cnt[b];
+    }
   }
   // Everything above is the previous integrator step's or older; the pair
   // stage just before this kernel writes the bond slots read below.
@@ -533,7 +641,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
           bond_pair_eval_sum<ND>(k, d, d.rep[d.nrep == 1 ? 0 : d.fil[f].rep].hf, rbuf, b,
                                  bF, bT);
       } else {
-        bond_pair_sum<ND, PREC>(d, b, bF, bT);
+        bond_pair_sum<ND, PREC>(d, b, e0, e1, bF, bT);
       }
     }
   }
@@ -549,6 +657,27 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   if (FAST && MAXC > 128)
     for (int q = 0; q < nfb; ++q) max_rows = max(max_rows, sfil[q].n - 1);
   const bool pcr = FAST && MAXC > 128 && max_rows > kPcrMinRows;
+  // Sequential solves: the exact step keeps the reference's Thomas order on
+  // one lane per filament; the fast step solves from both ends on lanes
+  // 2q, 2q+1.
+  auto solve_rows = [&](int lane_t) {
+    if (FAST) {
+      if (lane_t < 2 * nfb) {
+        const FilConst &f = sfil[lane_t >> 1];
+        const int fb0 = f.site0 - s0;
+        thomas_twisted(sa + fb0, sb + fb0, sc + fb0, sT + fb0, f.n - 1, (lane_t & 1) == 0);
+      }
+    } else if (lane_t < nfb) {
+      const int fb0 = sfil[lane_t].site0 - s0;
+      solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[lane_t].n - 1);
+    }
+  };
+  // Midstep determinants on warps the random-force solve leaves idle: lanes
+  // from g_dt (forward) and g_db (backward), when three warp-aligned groups
+  // fit in the block.
+  const int g_dt = ((FAST ? 2 * nfb : nfb) + 31) & ~31;
+  const int g_db = g_dt + ((nfb + 31) & ~31);
+  const bool dets_early = g_db + nfb <= C;
   if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
     d.rp[0][g] = r[0];
     d.rp[1][g] = r[1];
@@ -640,7 +769,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
         double xi[3] = {0, 0, 0}, xt[3] = {0, 0, 0};
 #pragma unroll
         for (int i = 0; i < ND; ++i)
-          xi[i] = ((double)w[i] + 0.5) * 2.3283064365386963e-10 - 0.5;
+          xi[i] = centered_uniform(w[i]);
         if (FAST) {
           // (t t^T) xi = (t . xi) t
           const double txi = dotn<ND>(tn, xi);
@@ -678,9 +807,12 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
       __syncthreads();
       if (pcr) {
         pcr_block(sa, sb, sc, sT, has_bond, t, base, base + n - 2, max_rows);
-      } else if (t < nfb) {
-        const int fb0 = sfil[t].site0 - s0;
-        solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[t].n - 1);
+      } else {
+        solve_rows(t);
+        if (dets_early) {  // the determinants, on lanes of other warps meanwhile
+          if (t >= g_dt && t - g_dt < nfb) det_forward(sdt, scos, sfil[t - g_dt], s0, t - g_dt);
+          else if (t >= g_db && t - g_db < nfb) det_backward(sdb, scos, sfil[t - g_db], s0, t - g_db);
+        }
       }
       __syncthreads();
       if (active) {
@@ -715,27 +847,13 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   }
 
   // ---- P3: bending and metric forces (:608-776) ---------------------------
-  // The determinants below are written over the projection's solution in
-  // sT, which every thread has just read: all reads first.
-  if (midstep && k.stoch) __syncthreads();
-  if (t < nfb) {  // det_t of filament t, forward
-    const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
-    double *dt = sdt + fb0 + t;
-    const double *cs = scos + fb0;
-    dt[0] = 1;
-    dt[1] = 2;
-    for (int i = 2; i < nn; ++i) dt[i] = 2 * dt[i - 1] - (-cs[i - 2]) * (-cs[i - 2]) * dt[i - 2];
-  } else if (t >= C / 2 && t - C / 2 < nfb) {  // det_b of filament t - C/2, backward
-    const int q = t - C / 2;
-    const int fb0 = sfil[q].site0 - s0, nn = sfil[q].n;
-    double *db = sdb + fb0 + q;
-    const double *cs = scos + fb0;
-    db[nn] = 1;
-    db[nn - 1] = 2;
-    for (int i = 2; i < nn; ++i)
-      db[nn - i] = 2 * db[nn - i + 1] - (-cs[nn - i - 1]) * (-cs[nn - i - 1]) * db[nn - i + 2];
+  // (The determinants do not share memory with the projection's solution,
+  // which every thread has just read.)
+  if (!(dets_early && midstep && k.stoch && !pcr)) {
+    if (t < nfb) det_forward(sdt, scos, sfil[t], s0, t);
+    else if (t >= C / 2 && t - C / 2 < nfb) det_backward(sdb, scos, sfil[t - C / 2], s0, t - C / 2);
+    __syncthreads();
   }
-  __syncthreads();
   if (active && j < n - 2) {
     const int dbase = base + lf;
     const double det_g = sdt[dbase + n - 1];
@@ -889,12 +1007,8 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     }
   }
   __syncthreads();
-  if (pcr) {
-    pcr_block(sa, sb, sc, sT, has_bond, t, base, base + n - 2, max_rows);
-  } else if (t < nfb) {
-    const int fb0 = sfil[t].site0 - s0;
-    solve_tridiag<FAST>(sa + fb0, sb + fb0, sc + fb0, sT + fb0, sfil[t].n - 1);
-  }
+  if (pcr) pcr_block(sa, sb, sc, sT, has_bond, t, base, base + n - 2, max_rows);
+  else solve_rows(t);
   __syncthreads();
 
   // ---- P5: UpdateSitePositions (:840-927), CheckBondLengths (:934-951) ----

@@ -88,6 +88,11 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
     }
     if (interaction) dtot = d.dt[g];
   }
+  int e0 = 0, e1 = 0;  // the bond's pair slots (written by the rebuild)
+  if (!FUSE && has_bond && interaction) {
+    e0 = d.e_off[b];
+    e1 = e0 + d.e_cnt[b];
+  }
   // Everything above is the previous integrator step's or older; the pair
   // stage just before this kernel writes the bond slots read below.
   grid_dep_sync();
@@ -98,7 +103,7 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
     if (FUSE) {
       if (!overflowed) bond_pair_eval_sum<ND>(k, d, d.rep[fc.rep].hf, rbuf, b, bF, bT);
     } else {
-      bond_pair_sum<ND, PREC>(d, b, bF, bT);
+      bond_pair_sum<ND, PREC>(d, b, e0, e1, bF, bT);
     }
   }
   if (!has_bond) u[0] = u[1] = u[2] = 0.0;
@@ -108,7 +113,7 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
     sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
                           d.rep[fc.rep].seed, (uint32_t)fc.f_local, wv);
 #pragma unroll
-    for (int i = 0; i < ND; ++i) xi[i] = ((double)wv[i] + 0.5) * 2.3283064365386963e-10 - 0.5;
+    for (int i = 0; i < ND; ++i) xi[i] = centered_uniform(wv[i]);
   }
   if (overflowed) return;  // the whole warp: the bit is uniform
   if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
