@@ -507,7 +507,8 @@ bool fused_pairs(const sc_ctx *c) {
 // The pair stage of one step, then the step's thermo accumulation.
 sc_status pair_stage(sc_ctx *c) {
   CKS(timed(c, [&] {
-    return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st, c->npx);
+    return sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st, c->npx,
+                            c->pair_block);
   }));
   c->slots_stale = false;
   if (c->k.thermo) c->launches += sc::launch_thermo(c->k, c->d, c->prec, c->st);
@@ -545,7 +546,8 @@ sc_status step_once(sc_ctx *c) {
 // force, so the slots are those a separate pair stage would have left.
 sc_status materialize_slots(sc_ctx *c) {
   if (!c->slots_stale) return SC_OK;
-  c->launches += sc::launch_pairs(c->k, c->d, 1 - c->rbuf, c->prec, (int)c->np, c->st, false);
+  c->launches += sc::launch_pairs(c->k, c->d, 1 - c->rbuf, c->prec, (int)c->np, c->st, false,
+                                 c->pair_block);
   CK(cudaGetLastError());
   c->slots_stale = false;
   return SC_OK;

@@ -23,11 +23,12 @@ sc_status sc_set_integrator_layout(sc_ctx *c, int warp_max_sites, int block_site
   return st;
 }
 
-// Integrator autotuner.  Candidate layouts (warp kernel or not, block size)
-// are timed on the context's own state: the arrays the integrator writes are
-// saved first and restored afterwards, so the simulation is unchanged.  The
-// fastest layout is applied and, with a cache file, recorded per shape (device,
-// precision, filament count and site range) so later contexts skip the timing.
+// Autotuner.  Candidate integrator layouts (warp kernel or not, block size)
+// and pair-kernel block sizes (128 or 256 threads) are timed on the
+// context's own state: the arrays they write are saved first and restored
+// afterwards, so the simulation is unchanged.  The fastest choices are
+// applied and, with a cache file, recorded per shape (device, precision,
+// filament count and site range) so later contexts skip the timing.
 sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
                       int *block_sites_out) {
   if (!c || !c->loaded) return SC_ERR_INVALID_ARG;
@@ -42,7 +43,7 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   }
   char key[512];
   const bool fuse = fused_pairs(c);
-  std::snprintf(key, sizeof(key), "v2|%s|sm%d|nd%d|prec%d|fast%d|fuse%d|nf%d|ns%d|n%d-%d",
+  std::snprintf(key, sizeof(key), "v3|%s|sm%d|nd%d|prec%d|fast%d|fuse%d|nf%d|ns%d|n%d-%d",
                 prop.name, prop.multiProcessorCount, c->nd, c->prec,
                 (c->prec == 1 && c->fast) ? 1 : 0, fuse ? 1 : 0, c->nf, c->ns, min_n, max_n);
   auto finish = [&](int w, int b) -> sc_status {
@@ -53,20 +54,25 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   if (cache_path) {
     if (FILE *fp = std::fopen(cache_path, "r")) {
       char line[768];
-      int w = -1, b = -1;
+      int w = -1, b = -1, pb = 256;
       while (std::fgets(line, sizeof(line), fp)) {
         char *tab = std::strchr(line, '\t');
         if (!tab) continue;
         *tab = 0;
-        int ww, bb;
-        if (std::strcmp(line, key) == 0 && std::sscanf(tab + 1, "%d %d", &ww, &bb) == 2) {
+        int ww, bb, pp;
+        float ms;
+        if (std::strcmp(line, key) == 0 &&
+            std::sscanf(tab + 1, "%d %d %f %d", &ww, &bb, &ms, &pp) == 4) {
           w = ww;
           b = bb;
+          pb = pp == 128 ? 128 : 256;
         }
       }
       std::fclose(fp);
       if (w >= 0) {
         CKS(sc_set_integrator_layout(c, w, b));
+        c->pair_block = pb;
+        drop_graph(c);
         return finish(w, b);
       }
     }
@@ -101,6 +107,21 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   regions.push_back({c->d.dr_max_bits, sizeof(unsigned long long) * c->d.nrep});
   regions.push_back({c->d.status, sizeof(unsigned)});
   if (fuse) regions.push_back({c->d.pf32, sizeof(float) * 4 * c->d.pcap_total});
+  // The pair kernel's timing rewrites the per-bond slots, stored forces and
+  // virial records from the current geometry: save those too.
+  const bool tune_pairs = c->desc.interaction_flag && !fuse && c->np > 0;
+  if (tune_pairs) {
+    const size_t np = (size_t)c->d.pcap_total;
+    if (c->prec == 0) {
+      regions.push_back({c->d.cf64, sizeof(double) * 16 * np});
+      if (!fuse) regions.push_back({c->d.pf64, sizeof(double) * 4 * np});
+      if (c->d.pv64) regions.push_back({c->d.pv64, sizeof(double) * 4 * np});
+    } else {
+      regions.push_back({c->d.cf32, sizeof(float) * 16 * np});
+      regions.push_back({c->d.pf32, sizeof(float) * 4 * np});
+      if (c->d.pv32) regions.push_back({c->d.pv32, sizeof(float) * 4 * np});
+    }
+  }
   size_t total = 0;
   for (auto &r : regions) total += (r.second + 255) & ~(size_t)255;
   char *save = nullptr;
@@ -148,6 +169,29 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
       best_lay = lay;
     }
   }
+  // Pair kernel: threads per block, timed on the current geometry.
+  int best_pb = c->pair_block;
+  if (st == SC_OK && tune_pairs) {
+    float best_p = 1e30f;
+    for (int pb : {256, 128}) {
+      for (int it = 0; it < 2; ++it)
+        sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st, c->npx, pb);
+      cudaEventRecord(e0, c->st);
+      for (int it = 0; it < 8; ++it)
+        sc::launch_pairs(c->k, c->d, c->rbuf, c->prec, (int)c->np, c->st, c->npx, pb);
+      cudaEventRecord(e1, c->st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) {
+        st = fail(c, SC_ERR_CUDA, "autotune: %s", cudaGetErrorString(cudaGetLastError()));
+        break;
+      }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_p) {
+        best_p = ms;
+        best_pb = pb;
+      }
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   CKS(copy_all(false));
@@ -156,11 +200,12 @@ sc_status sc_autotune(sc_ctx *c, const char *cache_path, int *warp_sites_out,
   CKS(st);
   c->warp_sites = best_lay.first;
   c->block_sites = best_lay.second;
+  c->pair_block = best_pb;
   CKS(layout_integrator(c));
   if (cache_path) {
     if (FILE *fp = std::fopen(cache_path, "a")) {
-      std::fprintf(fp, "%s\t%d %d %.2f\n", key, best_lay.first, best_lay.second,
-                   1000.0 * best / 8);
+      std::fprintf(fp, "%s\t%d %d %.2f %d\n", key, best_lay.first, best_lay.second,
+                   1000.0 * best / 8, best_pb);
       std::fclose(fp);
     }
   }

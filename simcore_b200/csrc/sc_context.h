@@ -94,6 +94,7 @@ struct sc_ctx {
   int nblocks = 0, C = 128;
   int warp_sites = 32;             // longest filament for the warp-synchronous kernel
   int block_sites = 0;             // sites per block of the block kernel (0: 128, 256 or 512)
+  int pair_block = 256;            // threads per block of the pair kernel (128 or 256)
 
   // control state
   long long i_step = 0, n_rebuilds = 0, launches = 0;

@@ -72,9 +72,11 @@ static sc_status build_graph(sc_ctx *c) {
     if (interaction && !fuse) {
       if (half == 0) {
         sc::PdlOff off;
-        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
+        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx,
+                         c->pair_block);
       } else {
-        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx);
+        sc::launch_pairs(c->k, c->d, rb, c->prec, (int)(c->np + c->np / 8), c->st, c->npx,
+                         c->pair_block);
       }
     }
     if (interaction && c->k.thermo) sc::launch_thermo(c->k, c->d, c->prec, c->st);

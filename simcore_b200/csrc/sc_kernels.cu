@@ -691,8 +691,9 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
 // completed before the kernel just before this one waited (every kernel
 // waits before it lets the next one start): they are loaded before the
 // wait; the bond geometry, which that kernel may be writing, after it.
-template <int ND, int PREC, bool NPX>
-__global__ void __launch_bounds__(256, NPX ? 4 : 1) k_pair_eval(SysConst k, DevState d, int rbuf) {
+template <int ND, int PREC, bool NPX, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, NPX ? 1024 / BLOCK : 1)
+    k_pair_eval(SysConst k, DevState d, int rbuf) {
   if (d.nrep == 1) {
     const ReplicaConst &R = d.rep[0];
     const int np = min(d.np_rep[0], R.pcap);
@@ -1357,20 +1358,28 @@ int launch_zero_dr(const DevState &d, cudaStream_t st) {
   return 1;
 }
 
-int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
-                 int expected, cudaStream_t st, bool npx) {
-  if (d.nrep > 1) expected = d.pcap_total;
-  int grid = cdiv(expected > 0 ? expected : 1, 256);
-  npx = npx && prec != 0;
+template <int BLOCK>
+static void launch_pairs_block(const SysConst &k, const DevState &d, int rbuf, int prec, int grid,
+                               cudaStream_t st, bool npx) {
   if (k.n_dim == 3) {
-    if (prec == 0) launch_pdl(k_pair_eval<3, 0, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
-    else if (!npx) launch_pdl(k_pair_eval<3, 1, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
-    else launch_pdl(k_pair_eval<3, 1, true>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
+    if (prec == 0) launch_pdl(k_pair_eval<3, 0, false, BLOCK>, dim3(grid), dim3(BLOCK), 0, st, k, d, rbuf);
+    else if (!npx) launch_pdl(k_pair_eval<3, 1, false, BLOCK>, dim3(grid), dim3(BLOCK), 0, st, k, d, rbuf);
+    else launch_pdl(k_pair_eval<3, 1, true, BLOCK>, dim3(grid), dim3(BLOCK), 0, st, k, d, rbuf);
   } else {
-    if (prec == 0) launch_pdl(k_pair_eval<2, 0, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
-    else if (!npx) launch_pdl(k_pair_eval<2, 1, false>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
-    else launch_pdl(k_pair_eval<2, 1, true>, dim3(grid), dim3(256), 0, st, k, d, rbuf);
+    if (prec == 0) launch_pdl(k_pair_eval<2, 0, false, BLOCK>, dim3(grid), dim3(BLOCK), 0, st, k, d, rbuf);
+    else if (!npx) launch_pdl(k_pair_eval<2, 1, false, BLOCK>, dim3(grid), dim3(BLOCK), 0, st, k, d, rbuf);
+    else launch_pdl(k_pair_eval<2, 1, true, BLOCK>, dim3(grid), dim3(BLOCK), 0, st, k, d, rbuf);
   }
+}
+
+int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
+                 int expected, cudaStream_t st, bool npx, int block) {
+  if (d.nrep > 1) expected = d.pcap_total;
+  npx = npx && prec != 0;
+  if (block == 128)
+    launch_pairs_block<128>(k, d, rbuf, prec, cdiv(expected > 0 ? expected : 1, 128), st, npx);
+  else
+    launch_pairs_block<256>(k, d, rbuf, prec, cdiv(expected > 0 ? expected : 1, 256), st, npx);
   return 1;
 }
 

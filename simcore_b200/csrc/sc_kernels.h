@@ -94,11 +94,15 @@ int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
 int launch_advance_mcount(const DevState &d, cudaStream_t st);
 int launch_zero_dr(const DevState &d, cudaStream_t st);
 // Grid sized for `expected` pairs (one system) or every slot (several); the
-// kernel strides over the actual pairs.
-// npx (mixed only): nearly parallel pairs are evaluated from the FP64
-// sites by a second, one-block kernel.
+// kernel strides over the actual pairs.  block: threads per block, 128 or 256
+// (the autotuner's choice).
+// npx (mixed only): nearly parallel pairs are evaluated in FP64 from the
+// sites, in place.  The kernel loads the pair list and slot indices before
+// it waits on the kernel launched just before it (programmatic dependent
+// launch): that kernel must not write them -- the last kernel of a rebuild
+// does not -- or the launch must be made without the overlap (PdlOff).
 int launch_pairs(const SysConst &k, const DevState &d, int rbuf, int prec,
-                 int expected, cudaStream_t st, bool npx = false);
+                 int expected, cudaStream_t st, bool npx = false, int block = 256);
 // Crosslink tethers of an even step into the per-anchor contributions.
 int launch_tether(const SysConst &k, const DevState &d, cudaStream_t st);
 // Thermo: one step's pair virial per system, the pressure record every

@@ -25,6 +25,7 @@
 
 #include "sc_common.cuh"
 #include "sc_kernels.h"
+#include "sc_launch.h"
 #include "simcore_gpu.h"
 
 namespace {
@@ -376,7 +377,12 @@ extern "C" sc_status sc_pair_forces_noalloc(const sc_system_desc *desc,
   sc::launch_pair_emit(k, d, key, sorted, cell_start, pair_off, deg, 0, st);
   sc::launch_exclusive_scan(deg, deg_off, nb, scan_tmp, st);
   sc::launch_csr(d, deg, deg_off, st);
-  sc::launch_pairs(k, d, 0, 0, kMaxPairs, st);
+  {
+    // The pair kernel reads its slot indices before it waits on the kernel
+    // before it, which here writes them: launched without the overlap.
+    sc::PdlOff off;
+    sc::launch_pairs(k, d, 0, 0, kMaxPairs, st);
+  }
   sc::launch_bond_sum(k, d, 0, st);
   k_noalloc_pack<<<nb / 256 + 1, 256, 0, st>>>(nb, d, d_bond_force, d_bond_torque);
   NA_CK(cudaGetLastError());

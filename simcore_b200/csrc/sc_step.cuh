@@ -540,6 +540,9 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // New positions (P5 on) take the slots of the previous positions: each
   // thread reads its own previous position before it writes its new one.
   double *sr = srp;             // positions            3C
+  // Midstep random forces (P2), read by the projection rows only, before
+  // the determinants are written over them.
+  double *sfn = sfp;            // 3C
   // The metric determinants (P3): in a midstep in the prefetch area, which
   // only full steps use, so that they are computed alongside the
   // random-force solve; in a full step in the Thomas arrays (sT, sa, sb,
@@ -632,24 +635,29 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // Everything above is the previous integrator step's or older; the pair
   // stage just before this kernel writes the bond slots read below.
   grid_dep_sync();
-  if (has_bond) {
-    if (interaction) {
-      // (The fused evaluation follows the pair list only when the rebuild
-      // of this step completed it.)
-      if (FUSE) {
-        if (!overflowed)
-          bond_pair_eval_sum<ND>(k, d, d.rep[d.nrep == 1 ? 0 : d.fil[f].rep].hf, rbuf, b,
-                                 bF, bT);
-      } else {
-        bond_pair_sum<ND, PREC>(d, b, e0, e1, bF, bT);
-      }
-    }
-  }
-  __syncthreads();
-  if (overflowed) {
+  if (overflowed) {  // uniform over the grid
     cp_async_wait_all();  // no copy into this block's shared memory outlives it
     return;
   }
+  if (has_bond && interaction) {
+    if (FUSE)
+      bond_pair_eval_sum<ND>(k, d, d.rep[d.nrep == 1 ? 0 : d.fil[f].rep].hf, rbuf, b, bF, bT);
+    else
+      bond_pair_sum<ND, PREC>(d, b, e0, e1, bF, bT);
+  }
+  if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
+    d.rp[0][g] = r[0];
+    d.rp[1][g] = r[1];
+    d.rp[2][g] = r[2];
+  }
+  if (has_bond) {
+    for (int i = 0; i < 3; ++i) {
+      V(su, t, i) = u[i];
+      V(sbF, t, i) = bF[i];
+      V(sfr, t, i) = bT[i];
+    }
+  }
+  __syncthreads();  // the staged filament constants and the bond values
   const FilConst &fc = sfil[active ? lf : 0];  // read from shared memory on use
   // Fast 256-site blocks with a long filament solve by parallel cyclic
   // reduction (uniform over the block).
@@ -678,19 +686,6 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   const int g_dt = ((FAST ? 2 * nfb : nfb) + 31) & ~31;
   const int g_db = g_dt + ((nfb + 31) & ~31);
   const bool dets_early = g_db + nfb <= C;
-  if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
-    d.rp[0][g] = r[0];
-    d.rp[1][g] = r[1];
-    d.rp[2][g] = r[2];
-  }
-  if (has_bond) {
-    for (int i = 0; i < 3; ++i) {
-      V(su, t, i) = u[i];
-      V(sbF, t, i) = bF[i];
-      V(sfr, t, i) = bT[i];
-    }
-  }
-  __syncthreads();
   if (active && j == n - 1) {
     for (int i = 0; i < 3; ++i) u[i] = V(su, t - 1, i);
   }
@@ -756,7 +751,10 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   if (active && j == n - 1) {
     for (int i = 0; i < 3; ++i) V(su, t, i) = u[i];
   }
-  __syncthreads();
+  // A noisy midstep writes its random forces to the prefetch area (unused in
+  // midsteps), not over the bond torques P1 reads, and nothing before its
+  // next barrier reads what P1 wrote: only other steps need a barrier here.
+  if (!(midstep && k.stoch)) __syncthreads();
 
   // ---- P2: random forces, projection, previous positions -----------------
   double fr[3] = {0, 0, 0};
@@ -789,14 +787,14 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
 #pragma unroll
         for (int i = 0; i < ND; ++i)
           fr[i] = fc.sperp * xi[i] + (fc.spar - fc.sperp) * xt[i];
-        for (int i = 0; i < 3; ++i) V(sfr, t, i) = fr[i];
+        for (int i = 0; i < 3; ++i) V(sfn, t, i) = fr[i];
       }
       __syncthreads();
       // GeometricallyProjectRandomForces (:550-599)
       if (has_bond) {
         double tmp[3];
 #pragma unroll
-        for (int i = 0; i < ND; ++i) tmp[i] = V(sfr, t + 1, i) - fr[i];
+        for (int i = 0; i < ND; ++i) tmp[i] = V(sfn, t + 1, i) - fr[i];
         sT[t] = dotn<ND>(tmp, u);
         sb[t] = 2;
         if (j > 0) {
@@ -854,30 +852,34 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     else if (t >= C / 2 && t - C / 2 < nfb) det_backward(sdb, scos, sfil[t - C / 2], s0, t - C / 2);
     __syncthreads();
   }
-  if (active && j < n - 2) {
+  if (!FAST && active && j < n - 2) {
     const int dbase = base + lf;
     const double det_g = sdt[dbase + n - 1];
-    if (FAST) {
-      const double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] * recip_nr(det_g);
-      skeff[t] = (fc.kappa + fc.l * ginv) * recip_nr(fc.l2);
-    } else {
-      double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] / det_g;
-      skeff[t] = (fc.kappa + fc.l * ginv) / fc.l2;
-    }
+    double ginv = scos[t] * sdt[dbase + j] * sdb[dbase + j + 3] / det_g;
+    skeff[t] = (fc.kappa + fc.l * ginv) / fc.l2;
   }
-  __syncthreads();
+  if (!FAST) __syncthreads();
   if (active && FAST) {
+    // Each site forms the k_eff of the (up to) three joints its stencil
+    // uses from the determinants and cosines, instead of reading them from
+    // a barrier later.
+    const int dbase = base + lf;
+    const double rdet = recip_nr(sdt[dbase + n - 1]), rl2 = recip_nr(fc.l2);
+    auto keff_at = [&](int jj) {
+      const double ginv = scos[base + jj] * sdt[dbase + jj] * sdb[dbase + jj + 3] * rdet;
+      return (fc.kappa + fc.l * ginv) * rl2;
+    };
     // (I - u2 u2^T) u1 = u1 - (u1 . u2) u2 with the cosines of
     // CalculateAngles: the reference's three stencil terms in vector form.
     double fs[3] = {0, 0, 0};
     const int kk = j;
     if (kk > 1) {
-      const double ke = skeff[t - 2], c = scos[t - 2];
+      const double ke = keff_at(j - 2), c = scos[t - 2];
 #pragma unroll
       for (int i = 0; i < ND; ++i) fs[i] += ke * (V(su, t - 2, i) - c * V(su, t - 1, i));
     }
     if (kk > 0 && kk < n - 1) {
-      const double ke = skeff[t - 1], c = scos[t - 1];
+      const double ke = keff_at(j - 1), c = scos[t - 1];
 #pragma unroll
       for (int i = 0; i < ND; ++i) {
         const double um = V(su, t - 1, i);
@@ -885,7 +887,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
       }
     }
     if (kk < n - 2) {
-      const double ke = skeff[t], c = scos[t];
+      const double ke = keff_at(j), c = scos[t];
 #pragma unroll
       for (int i = 0; i < ND; ++i) fs[i] -= ke * (V(su, t + 1, i) - c * u[i]);
     }
@@ -1053,6 +1055,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
 #pragma unroll
     for (int i = 0; i < ND; ++i) V(su, t, i) = rd[i];
   }
+  bool stretched = false;
   if (active && j >= 1) {
     double a = 0.0;
 #pragma unroll
@@ -1063,14 +1066,16 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     if (FAST) {
       // |l - |dr|| / l > 1e-3 without the root and the quotient
       const double lo = fc.l * (1.0 - 1e-3), hi = fc.l * (1.0 + 1e-3);
-      if (a < lo * lo || a > hi * hi) sflag[lf] = 1;
+      stretched = a < lo * lo || a > hi * hi;
     } else {
       a = sqrt(a);
       double err = dabs(fc.l - a) / fc.l;
-      if (err > 1e-3) sflag[lf] = 1;
+      stretched = err > 1e-3;
     }
+    if (stretched) sflag[lf] = 1;
   }
-  __syncthreads();
+  // Positions change below only in a block with a filament to renormalise.
+  const int any_renorm = __syncthreads_or(stretched);
   if (t < nfb) {
     const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
     const double l = sfil[t].l;
@@ -1095,7 +1100,7 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     d.f_switch[fg] = sw;
     d.f_nnorm[fg] = nnorm;
   }
-  __syncthreads();
+  if (any_renorm) __syncthreads();
 
   // ---- P6: bond geometry (Mesh::UpdateBondPositions), state write-back ----
   double my_dr = 0.0;
