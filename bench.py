@@ -43,10 +43,12 @@ I_STEPS_PER_STEP = 20
 # measured (after every quarter of the timed steps).
 N_SNAPSHOTS = 4
 # DRAM bytes (read + write) of one k_integrate launch, mixed precision, from
-# ncu (cold cache), per workload captured: for B (96-site blocks) the mean of
-# a midstep launch (23.05 MB) and a full-step launch (40.69 MB), which
-# alternate.  Workloads without a capture report null.
-TRAFFIC_K_INTEGRATE_MIXED = {"B": 31.87e6}
+# ncu (cold cache), per workload captured, with the block layout the timed
+# runs use: for B (192-site blocks) the mean of a midstep launch (24.41 MB)
+# and a full-step launch (41.94 MB), which alternate.  Workloads without a
+# capture report null.
+TRAFFIC_K_INTEGRATE_MIXED = {"B": 33.18e6}
+TRAFFIC_LAYOUT = {"B": "0,192"}
 WORKLOAD_DESCS = {
     "A": "A: 100 filaments x 20 bonds (2,000 segments, 2,100 sites), 3D periodic cube side 50, "
          "lp 500, WCA eps=sigma=1, dt 1e-4, noise on",
@@ -556,9 +558,10 @@ def run_ours(args, rank, world, local_rank):
                                "step, all %d filaments)" % (r["n_dim"], r["n_fil"]),
                      "algorithmic_bytes_per_launch": b_int, "avg_launch_ms": t_int,
                      "peak_kind": peak_kind + " hbm_gbs",
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
-                                       "launch of bench.py --profile-steps 8 --profile-layout "
-                                       "0,96 (cold cache)",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, mean "
+                                       "of a midstep and a full-step launch of bench.py "
+                                       "--profile-steps 8 --profile-layout %s (cold cache)"
+                                       % TRAFFIC_LAYOUT.get(args.workload, "-"),
                      "pair_kernel": {"kernel": "k_pair_eval (mixed)", "avg_launch_ms": t_pair,
                                      "algorithmic_bytes_per_launch": b_pair,
                                      "achieved": b_pair / (t_pair * 1e-3) / 1e9},
