@@ -214,15 +214,19 @@ sc_status sc_thermo_open(sc_ctx *ctx, const char *run_name, int n_steps);
 sc_status sc_get_thermo(sc_ctx *ctx, int max_records, int *n_records, int64_t *i_step,
                         double *tensor, double *pressure, double *volume);
 sc_status sc_get_potential_energy(sc_ctx *ctx, double *pote);
-/* Mixed precision only: nearly parallel pairs (FP32 |u1 x u2|^2 between 0
- * and 1e-5, within 0.18 degrees) are evaluated from the FP64 sites, as the
- * FP64 path evaluates them, by a one-block kernel after the pair stage.
- * FP32 orientations cannot resolve the closest points of such pairs: their
- * torques (and forces) could be off by far more than 1e-5.  On by default;
- * sc_set_exact_near_parallel(ctx, 0) evaluates them in FP32 like every other
- * pair.  No counterpart in the reference, whose pair stage is FP64
- * throughout. */
+/* Mixed precision only: nearly parallel pairs side by side (FP32
+ * |u1 x u2|^2 between 0 and the threshold, 1e-5 by default; the centres'
+ * separation along u1 within the two half-lengths plus 0.25; a stored force
+ * or a perpendicular separation within 1.5 cutoffs) are evaluated from the
+ * FP64 sites, as the FP64 path evaluates them, by the pair kernel's thread
+ * that meets them.  FP32 orientations cannot resolve the closest points of
+ * such pairs: their torques (and forces) could be off by far more than
+ * 1e-5.  On by default; sc_set_exact_near_parallel(ctx, 0) evaluates them in
+ * FP32 like every other pair; sc_set_near_parallel_threshold sets the
+ * threshold on |u1 x u2|^2 (0 to 1).  No counterpart in the reference, whose
+ * pair stage is FP64 throughout. */
 sc_status sc_set_exact_near_parallel(sc_ctx *ctx, int on);
+sc_status sc_set_near_parallel_threshold(sc_ctx *ctx, double s2);
 /* Fast mixed precision only, with the option above switched off (the fused
  * evaluation is FP32 throughout) and without thermo: sc_step
  * and sc_step_graph evaluate each bond's pairs inside the integrator and

@@ -38,7 +38,8 @@ EXPORTED = ["sc_create", "sc_destroy", "sc_last_error", "sc_add_filaments",
             "sc_set_noise_key", "sc_output_open", "sc_output_write", "sc_output_close",
             "sc_analysis_sample", "sc_analysis_results", "sc_global_order",
             "sc_set_thermo", "sc_thermo_open", "sc_get_thermo", "sc_get_potential_energy",
-            "sc_set_exact_near_parallel", "sc_set_fused_pairs", "sc_diffusion_init",
+            "sc_set_exact_near_parallel", "sc_set_near_parallel_threshold",
+            "sc_set_fused_pairs", "sc_diffusion_init",
             "sc_diffusion_sample", "sc_diffusion_results", "sc_insert_filaments_gpu"]
 
 
@@ -398,6 +399,10 @@ class Context:
     def set_exact_near_parallel(self, on=True):
         """Mixed precision: nearly parallel pairs evaluated from the FP64 sites."""
         self._check(lib.sc_set_exact_near_parallel(self.h, 1 if on else 0))
+
+    def set_near_parallel_threshold(self, s2):
+        """Mixed precision: |u1 x u2|^2 below which side-by-side pairs are FP64."""
+        self._check(lib.sc_set_near_parallel_threshold(self.h, ctypes.c_double(s2)))
 
     def set_fused_pairs(self, on=True):
         """Fast mixed precision: the integrator evaluates the pairs itself (no

@@ -30,15 +30,20 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / scale) if scale > 0 else float(np.abs(a).max())
 
 
-def mixed_errors(system, filaments, sites, replicas=None, crosslinks=None, device=0):
+def mixed_errors(system, filaments, sites, replicas=None, crosslinks=None, device=0,
+                 near_parallel_threshold=None):
     """Max relative error of every output of the mixed path against FP64 on
     the state `sites` (see the module docstring).  crosslinks: optional
-    (site_a, site_b, k_spring, rest_length) of static tethers."""
+    (site_a, site_b, k_spring, rest_length) of static tethers.
+    near_parallel_threshold: the mixed context's threshold on |u1 x u2|^2
+    (sc_set_near_parallel_threshold), when not the default."""
     res = {}
     for prec in ("fp64", "mixed"):
         ctx = Context(system, filaments, sites, precision=prec, device=device,
                       replicas=replicas)
         try:
+            if prec == "mixed" and near_parallel_threshold is not None:
+                ctx.set_near_parallel_threshold(near_parallel_threshold)
             if crosslinks is not None:
                 a, b, k, rest = crosslinks
                 ctx.add_crosslinks(a, b, k_spring=k, rest_length=rest)

@@ -63,6 +63,8 @@ sc_status check_status(sc_ctx *c) {
   unsigned s = c->hb->status;
   if (s & sc::ST_NAN) return fail(c, SC_ERR_NAN, "non-finite position or displacement");
   if (s & sc::ST_BAD_CELL) return fail(c, SC_ERR_NAN, "bond outside the cell grid (non-finite position)");
+  if (s & sc::ST_TIMEOUT)
+    return fail(c, SC_ERR_TIMEOUT, "the rebuild's pair pass gave up waiting on a tile");
   if (s & sc::ST_LIST_OVERFLOW) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow");
   if (s & sc::ST_TETHER)
     return fail(c, SC_ERR_UNPHYSICAL, "a crosslink anchor moved off the bonds around its site");
@@ -648,6 +650,7 @@ sc_status sc_create(const sc_system_desc *desc, sc_ctx **out) {
   k.epsf = (float)desc->wca_eps;
   k.stoch = desc->stoch_flag ? 1 : 0;
   k.like_like = desc->like_like_interactions ? 1 : 0;
+  k.npx_s2 = 1e-5f;
   CK(cudaMalloc((void **)&c->d.status, sizeof(unsigned)));
   c->allocs.push_back(c->d.status);
   CK(cudaMalloc((void **)&c->d.mcount, sizeof(unsigned long long)));
@@ -948,6 +951,9 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
     CKS(dzero(&rb.pair_off, (size_t)nbi + 1));
     CKS(dzero(&rb.deg, nbi));
     CKS(dzero(&rb.deg_off, (size_t)nbi + 1));
+    rb.n_tiles = sc::rebuild_pair_tiles((int)nbi);
+    CKS(dzero(&rb.tile_status, (size_t)rb.n_tiles));
+    CKS(dzero(&rb.ticket, 1));
     CKS(dalloc(c, &rb.scan_tmp,
                (size_t)std::max(sc::scan_temp_ints(rb.n_groups), sc::scan_temp_ints(nbi))));
   }
@@ -1190,6 +1196,15 @@ sc_status sc_get_pairs(sc_ctx *c, int32_t *pairs, int64_t cap, int64_t *n_pairs)
       pairs[2 * out + 1] = b[i];
     }
   }
+  return SC_OK;
+}
+
+sc_status sc_set_near_parallel_threshold(sc_ctx *c, double s2) {
+  if (!c || !c->loaded || !(s2 >= 0.0) || !(s2 <= 1.0)) return SC_ERR_INVALID_ARG;
+  CK(cudaSetDevice(c->desc.device));
+  CK(cudaStreamSynchronize(c->st));
+  c->k.npx_s2 = (float)s2;
+  drop_graph(c);
   return SC_OK;
 }
 

@@ -45,7 +45,8 @@ enum : unsigned {
   ST_UNPHYSICAL = 4u,     // accumulated displacement above 10000
   ST_BAD_CELL = 8u,       // cell index out of range (non-finite position)
   ST_BAD_INPUT = 16u,     // caller's device data out of range (site offsets)
-  ST_TETHER = 32u         // a crosslink anchor left the bonds it can sit on
+  ST_TETHER = 32u,        // a crosslink anchor left the bonds it can sit on
+  ST_TIMEOUT = 64u        // a bounded device wait gave up (the rebuild's pair pass)
 };
 
 // Bond geometry for the FP64 pair stage: the reference's Bond state after
@@ -82,6 +83,7 @@ struct SysConst {
   double eps;             // WCA epsilon (the potential's shift)
   float epsf;
   int thermo;             // pair virial and potential records kept
+  float npx_s2;           // mixed: |u1 x u2|^2 below which a side-by-side pair is FP64
 };
 
 // One independent periodic system (a replica) of a context: its box, cell

@@ -493,7 +493,7 @@ __device__ __forceinline__ bool near_parallel(const SysConst &k, const float *hf
   } else {
     s2 = cz * cz;
   }
-  if (!(s2 > 0.f && s2 < 1e-5f)) return false;
+  if (!(s2 > 0.f && s2 < k.npx_s2)) return false;
   float dr[3] = {0.f, 0.f, 0.f}, a1 = 0.f, r2 = 0.f;
 #pragma unroll
   for (int i = 0; i < ND; ++i) {
@@ -598,9 +598,11 @@ __device__ __forceinline__ PairIdx pair_idx(const DevState &d, int p) {
   return PairIdx{d.pa[p], d.pb[p], d.pos1[p], d.pos2[p]};
 }
 
+// One pair of the pair stage.  Mixed with NPX: returns false, having
+// written nothing, for a nearly parallel pair, which the caller evaluates in
+// FP64 (eval_near_parallel) outside its loop over pairs.
 template <int ND, int PREC, bool NPX>
-
-__device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState &d,
+__device__ __forceinline__ bool pair_eval_one(const SysConst &k, const DevState &d,
                                               const ReplicaConst &R, int rbuf, int p,
                                               const PairIdx &ix) {
   const int a = ix.a, b = ix.b;
@@ -637,33 +639,12 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     c2[0] = make_double2(-force[0], -force[1]);
     c2[1] = make_double2(-force[2], -t2[0]);
     c2[2] = make_double2(-t2[1], -t2[2]);
+    return true;
   } else {
     const BondGeomF32 A = d.g32[rbuf][a], B = d.g32[rbuf][b];
     float4 *stale = reinterpret_cast<float4 *>(d.pf32) + (size_t)p;
     const float4 st = *stale;
-    if (NPX && near_parallel<ND>(k, R.hf, A, B, st)) {
-      NearParallelArgs na;
-      na.r0 = d.r[0];
-      na.r1 = d.r[1];
-      na.r2 = d.r[2];
-      na.bond_fil = d.bond_fil;
-      na.pa = d.pa;
-      na.pb = d.pb;
-      na.pos1 = d.pos1;
-      na.pos2 = d.pos2;
-      na.pf32 = d.pf32;
-      na.pv32 = d.pv32;
-      na.cf32 = d.cf32;
-      na.R = &R;
-      na.rcut2 = k.rcut2;
-      na.c12 = k.c12;
-      na.c6 = k.c6;
-      na.fcut = k.fcut;
-      na.eps = k.eps;
-      na.thermo = k.thermo;
-      eval_near_parallel<ND>(na, p);
-      return;
-    }
+    if (NPX && near_parallel<ND>(k, R.hf, A, B, st)) return false;
     float force[3], rec[4], t1[3], t2[3];
     const bool set = pair_force_f32<ND>(k, R.hf, A, B, st, force, t1, t2,
                                         k.thermo ? rec : nullptr);
@@ -678,7 +659,34 @@ __device__ __forceinline__ void pair_eval_one(const SysConst &k, const DevState 
     c1[1] = make_float4(t1[1], t1[2], 0.f, 0.f);
     c2[0] = make_float4(-force[0], -force[1], -force[2], -t2[0]);
     c2[1] = make_float4(-t2[1], -t2[2], 0.f, 0.f);
+    return true;
   }
+}
+
+// A nearly parallel pair of the mixed pair stage, in FP64 from the sites.
+template <int ND>
+__device__ __forceinline__ void near_parallel_fp64(const SysConst &k, const DevState &d,
+                                                   const ReplicaConst &R, int p) {
+  NearParallelArgs na;
+  na.r0 = d.r[0];
+  na.r1 = d.r[1];
+  na.r2 = d.r[2];
+  na.bond_fil = d.bond_fil;
+  na.pa = d.pa;
+  na.pb = d.pb;
+  na.pos1 = d.pos1;
+  na.pos2 = d.pos2;
+  na.pf32 = d.pf32;
+  na.pv32 = d.pv32;
+  na.cf32 = d.cf32;
+  na.R = &R;
+  na.rcut2 = k.rcut2;
+  na.c12 = k.c12;
+  na.c6 = k.c6;
+  na.fcut = k.fcut;
+  na.eps = k.eps;
+  na.thermo = k.thermo;
+  eval_near_parallel<ND>(na, p);
 }
 
 // Grid-stride over the pair slots, so a captured launch stays correct
@@ -701,15 +709,25 @@ __global__ void __launch_bounds__(BLOCK, NPX ? 1024 / BLOCK : 1)
     PairIdx ix = {0, 0, 0, 0};
     if (p < np) ix = pair_idx(d, p);
     grid_dep_sync();
-    for (bool first = true; p < np; p += gridDim.x * blockDim.x, first = false)
-      pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p, first ? ix : pair_idx(d, p));
+    // The grid covers the list (it is sized for it), so a thread has one
+    // pair: a nearly parallel one is evaluated in FP64 after the FP32 work,
+    // out of any loop.  Pairs past the grid (a list that grew after the
+    // launch was sized) are handled by the loop below.
+    const int stride = gridDim.x * blockDim.x;
+    int flagged = -1;
+    if (p < np && !pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p, ix)) flagged = p;
+    for (p += stride; p < np; p += stride)
+      if (!pair_eval_one<ND, PREC, NPX>(k, d, R, rbuf, p, pair_idx(d, p)))
+        if (NPX) near_parallel_fp64<ND>(k, d, R, p);
+    if (NPX && flagged >= 0) near_parallel_fp64<ND>(k, d, R, flagged);
     return;
   }
   grid_dep_sync();
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < d.pcap_total;
        p += gridDim.x * blockDim.x) {
     int r;
-    if (pair_live(d, p, r)) pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p, pair_idx(d, p));
+    if (pair_live(d, p, r) && !pair_eval_one<ND, PREC, NPX>(k, d, d.rep[r], rbuf, p, pair_idx(d, p)))
+      if (NPX) near_parallel_fp64<ND>(k, d, d.rep[r], p);
   }
 }
 

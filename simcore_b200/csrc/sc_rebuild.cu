@@ -16,9 +16,10 @@
 //   (scan)         group offsets
 //   k_rb_scatter   bonds into their groups (counts back to zero)
 //   k_rb_rank      stable order inside each group; cell ranges and bits
-//   k_rb_count     pairs of every cell (head entry of the sorted order)
-//   (scan)         pair offsets
-//   k_rb_emit      pairs in the reference's order, per-bond degrees
+//   k_rb_pairs     one system: pairs of every cell (head entry of the
+//                  sorted order), their offsets by decoupled look-back, and
+//                  the pairs in the reference's order, per-bond degrees
+//   k_rb_count, (scan), k_rb_emit   the same in three steps, several systems
 //   (scan)         entry offsets
 //   k_rb_csr_fill  entries (pair << 1 | role) of every bond
 //   k_rb_csr_sort  entries in pair order, slots of both roles, ranges
@@ -47,6 +48,8 @@ __global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, Rebuild
     const int w0 = R.cell0 >> 5, w1 = (R.cell0 + R.n_cells + 31) >> 5;
     for (int w = w0 + tid; w < w1; w += nthreads) rb.occ[w] = 0u;
   }
+  for (int i = tid; i < rb.n_tiles; i += nthreads) rb.tile_status[i] = 0u;
+  if (tid == 0) *rb.ticket = 0;
   const int b = tid;
   bool in = false;
   int g = 0;
@@ -126,100 +129,80 @@ __device__ __forceinline__ int sys_hi(const RebuildBufs &rb, const ReplicaConst 
   return rb.gstart[(R.cell0 + R.n_cells + 31) >> 5];
 }
 
-// Pairs the cell whose head is sorted entry q contributes (zero for the
-// other entries): m (m - 1) / 2 inside it plus m * m_nbr with each kept
-// half-shell neighbour, less one for each bond whose filament neighbour
-// (b - 1 or b + 1) lies in the cell itself (counted once) or in a
-// neighbour -- the pairs pair_excluded drops.
-__global__ void k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
-  grid_dep_sync();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= d.nb) return;
-  int cnt_out = 0;
-  const int n_due = rb.gstart[rb.n_groups];
-  if (q < n_due && k.like_like) {
-    const int c = (int)rb.skey[q];
-    if (q == 0 || (int)rb.skey[q - 1] != c) {
-      const int m = rb.range[c].y - q;
-      const int *it = rb.sval + q;
-      const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, it[0]) : 0];
-      int x, y, z, nbr[13];
-      cell_coords(R, c - R.cell0, x, y, z);
-      const unsigned keep = half_shell_fixed(k, R, x, y, z, nbr);
-      long long cnt = (long long)m * (m - 1) / 2;
+// The cell whose head is sorted entry q: its m members, its half-shell
+// neighbours (context cell indices; -1 where the wrap gives the cell itself
+// or, in 2D, a third dimension) and their sorted ranges (empty where
+// unoccupied), and the mask of non-empty neighbours.
+struct CellHead {
+  int c, m;
+  const int *it;
+  int nbr[13], s0[13], s1[13];
+  unsigned busy;
+};
+
+__device__ __forceinline__ void cell_head(const SysConst &k, const RebuildBufs &rb,
+                                          const ReplicaConst &R, int q, int c, CellHead &h) {
+  h.c = c;
+  h.m = rb.range[c].y - q;
+  h.it = rb.sval + q;
+  int x, y, z;
+  cell_coords(R, c - R.cell0, x, y, z);
+  const unsigned keep = half_shell_fixed(k, R, x, y, z, h.nbr);
+  h.busy = 0;
 #pragma unroll
-      for (int kk = 0; kk < 13; ++kk) {
-        nbr[kk] += R.cell0;
-        if ((keep >> kk) & 1u) {
-          if (occupied(rb.occ, nbr[kk])) {
-            const int2 g = rb.range[nbr[kk]];
-            cnt += (long long)m * (g.y - g.x);
-          }
-        } else {
-          nbr[kk] = -1;  // matches no cell key
-        }
+  for (int kk = 0; kk < 13; ++kk) {  // all ranges loaded together
+    h.s0[kk] = h.s1[kk] = 0;
+    h.nbr[kk] += R.cell0;
+    if ((keep >> kk) & 1u) {
+      if (occupied(rb.occ, h.nbr[kk])) {
+        const int2 g = rb.range[h.nbr[kk]];
+        h.s0[kk] = g.x;
+        h.s1[kk] = g.y;
+        h.busy |= 1u << kk;
       }
-      for (int i = 0; i < m; ++i) {
-        const int a = it[i], fa = d.bond_fil[a];
-        if (a + 1 < d.nb && d.bond_fil[a + 1] == fa) {
-          const int ka = (int)rb.key[a + 1];
-          if (ka == c) --cnt;  // each adjacent pair inside the cell, once
-#pragma unroll
-          for (int kk = 0; kk < 13; ++kk) cnt -= ka == nbr[kk];
-        }
-        if (a > 0 && d.bond_fil[a - 1] == fa) {
-          const int ka = (int)rb.key[a - 1];
-#pragma unroll
-          for (int kk = 0; kk < 13; ++kk) cnt -= ka == nbr[kk];
-        }
-      }
-      cnt_out = cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
+    } else {
+      h.nbr[kk] = -1;  // matches no cell key
     }
   }
-  rb.pair_count[q] = cnt_out;
 }
 
-// Writes each cell's pairs at its offset in its system's pair segment, in the
+// Pairs of the cell: m (m - 1) / 2 inside it plus m * m_nbr with each kept
+// half-shell neighbour, less one for each bond whose filament neighbour
+// (b - 1 or b + 1) lies in the cell itself (counted once) or in a
+// neighbour -- the pairs pair_excluded drops.  Clamped to 2^30 - 1.
+__device__ __forceinline__ int cell_pair_count(const DevState &d, const RebuildBufs &rb,
+                                               const CellHead &h) {
+  const int m = h.m, c = h.c;
+  long long cnt = (long long)m * (m - 1) / 2;
+#pragma unroll
+  for (int kk = 0; kk < 13; ++kk) cnt += (long long)m * (h.s1[kk] - h.s0[kk]);
+  for (int i = 0; i < m; ++i) {
+    const int a = h.it[i], fa = d.bond_fil[a];
+    if (a + 1 < d.nb && d.bond_fil[a + 1] == fa) {
+      const int ka = (int)rb.key[a + 1];
+      if (ka == c) --cnt;  // each adjacent pair inside the cell, once
+#pragma unroll
+      for (int kk = 0; kk < 13; ++kk) cnt -= ka == h.nbr[kk];
+    }
+    if (a > 0 && d.bond_fil[a - 1] == fa) {
+      const int ka = (int)rb.key[a - 1];
+#pragma unroll
+      for (int kk = 0; kk < 13; ++kk) cnt -= ka == h.nbr[kk];
+    }
+  }
+  return cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
+}
+
+// Writes the cell's pairs from offset p of system R's pair segment, in the
 // reference's list order (Cell::MakePairs, src/cell.cpp:14-22): pairs inside
 // the cell, then with each half-shell neighbour in order; clears each new
 // pair's stored force and counts per-bond entries.  Only the non-empty
 // neighbours are visited (a warp steps through as many as its busiest lane
-// has, not all 13).  Threads q < nrep record their system's pair count (a
-// list longer than its segment sets the overflow bit; the count is kept so
-// the host can size the segment).
-__global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
-  grid_dep_sync();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < d.nrep && d.due[q]) {
-    const ReplicaConst &R = d.rep[q];
-    const int np = rb.pair_off[sys_hi(rb, R)] - rb.pair_off[sys_lo(rb, R)];
-    d.np_rep[q] = np;
-    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
-  }
-  if (q >= rb.gstart[rb.n_groups] || !k.like_like) return;
-  const int c = (int)rb.skey[q];
-  if (q > 0 && (int)rb.skey[q - 1] == c) return;
-  const int *it = rb.sval + q;
-  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, it[0]) : 0];
-  const int m = rb.range[c].y - q;
+// has, not all 13).
+__device__ __forceinline__ void cell_pair_emit(const SysConst &k, const DevState &d,
+                                               const RebuildBufs &rb, const ReplicaConst &R,
+                                               const CellHead &h, int p, int prec) {
   const int p0 = R.p0, pcap = R.pcap;
-  int p = rb.pair_off[q] - rb.pair_off[sys_lo(rb, R)];
-  int x, y, z, nbr[13];
-  cell_coords(R, c - R.cell0, x, y, z);
-  const unsigned keep = half_shell_fixed(k, R, x, y, z, nbr);
-  int s0[13], s1[13];
-  unsigned busy = 0;
-#pragma unroll
-  for (int kk = 0; kk < 13; ++kk) {  // all ranges loaded together
-    s0[kk] = s1[kk] = 0;
-    const int cn = R.cell0 + nbr[kk];
-    if (((keep >> kk) & 1u) && occupied(rb.occ, cn)) {
-      const int2 g = rb.range[cn];
-      s0[kk] = g.x;
-      s1[kk] = g.y;
-      busy |= 1u << kk;
-    }
-  }
   auto emit = [&](int a, int b) {
     if (pair_excluded(k, d, a, b)) return;
     if (p < pcap) {
@@ -244,8 +227,10 @@ __global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
     }
     ++p;
   };
+  const int m = h.m;
   for (int i = 0; i < m - 1; ++i)
-    for (int j = i + 1; j < m; ++j) emit(it[i], it[j]);
+    for (int j = i + 1; j < m; ++j) emit(h.it[i], h.it[j]);
+  unsigned busy = h.busy;
   while (busy) {
     const int kk = __ffs(busy) - 1;
     busy &= busy - 1;
@@ -253,12 +238,148 @@ __global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
 #pragma unroll
     for (int q2 = 0; q2 < 13; ++q2)
       if (q2 == kk) {
-        lo = s0[q2];
-        hi = s1[q2];
+        lo = h.s0[q2];
+        hi = h.s1[q2];
       }
     for (int i = 0; i < m; ++i)
-      for (int j = lo; j < hi; ++j) emit(it[i], rb.sval[j]);
+      for (int j = lo; j < hi; ++j) emit(h.it[i], rb.sval[j]);
   }
+}
+
+// Pairs each cell contributes, at its head entry (zero for the other
+// entries), for the offsets' scan (several systems).
+__global__ void k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
+  grid_dep_sync();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= d.nb) return;
+  int cnt = 0;
+  if (q < rb.gstart[rb.n_groups] && k.like_like) {
+    const int c = (int)rb.skey[q];
+    if (q == 0 || (int)rb.skey[q - 1] != c) {
+      CellHead h;
+      cell_head(k, rb, d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0], q, c, h);
+      cnt = cell_pair_count(d, rb, h);
+    }
+  }
+  rb.pair_count[q] = cnt;
+}
+
+// Each cell's pairs at its scanned offset in its system's pair segment
+// (several systems).  Threads q < nrep record their system's pair count (a
+// list longer than its segment sets the overflow bit; the count is kept so
+// the host can size the segment).
+__global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
+  grid_dep_sync();
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < d.nrep && d.due[q]) {
+    const ReplicaConst &R = d.rep[q];
+    const int np = rb.pair_off[sys_hi(rb, R)] - rb.pair_off[sys_lo(rb, R)];
+    d.np_rep[q] = np;
+    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+  }
+  if (q >= rb.gstart[rb.n_groups] || !k.like_like) return;
+  const int c = (int)rb.skey[q];
+  if (q > 0 && (int)rb.skey[q - 1] == c) return;
+  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0];
+  CellHead h;
+  cell_head(k, rb, R, q, c, h);
+  cell_pair_emit(k, d, rb, R, h, rb.pair_off[q] - rb.pair_off[sys_lo(rb, R)], prec);
+}
+
+// One system: counts, offsets and emission in one kernel.  Each block (a
+// tile of sorted entries, taken in ticket order) counts its cells' pairs,
+// scans them, and finds the pairs of all earlier tiles by decoupled
+// look-back (Merrill & Garland, "Single-pass parallel prefix scan with
+// decoupled look-back", NVIDIA tech. report NVR-2016-002): a tile publishes
+// its own total at once and its inclusive prefix when known, and one warp
+// reads 32 predecessors at a time back to the nearest inclusive prefix.
+// Tiles wait only on tiles with earlier tickets, which are running; a
+// look-back word that stays empty past the poll limit sets ST_TIMEOUT.  The
+// last tile records the system's pair count.
+constexpr int kPairTile = 128;
+constexpr uint32_t LB_AGG = 1u << 30;  // tile total published
+constexpr uint32_t LB_INC = 2u << 30;  // inclusive prefix published
+constexpr uint32_t LB_VAL = LB_AGG - 1u;
+constexpr int kLookbackPolls = 1 << 20;
+
+__global__ void __launch_bounds__(kPairTile) k_rb_pairs(SysConst k, DevState d, RebuildBufs rb,
+                                                          int prec) {
+  grid_dep_sync();
+  __shared__ int s_tile;
+  __shared__ uint32_t s_warp[kPairTile / 32];
+  __shared__ uint32_t s_excl;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_tile = atomicAdd(rb.ticket, 1);
+  __syncthreads();
+  const int tile = s_tile;
+  const int q = tile * kPairTile + threadIdx.x;
+  const ReplicaConst &R = d.rep[0];
+  CellHead h;
+  bool head = false;
+  int cnt = 0;
+  if (q < rb.gstart[rb.n_groups] && k.like_like) {
+    const int c = (int)rb.skey[q];
+    head = q == 0 || (int)rb.skey[q - 1] != c;
+    if (head) {
+      cell_head(k, rb, R, q, c, h);
+      cnt = cell_pair_count(d, rb, h);
+    }
+  }
+  // Exclusive scan of the counts over the tile.
+  uint32_t x = (uint32_t)cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[w] = x;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+#pragma unroll
+  for (int i = 0; i < kPairTile / 32; ++i) {
+    before += i < w ? s_warp[i] : 0u;
+    total += s_warp[i];
+  }
+  const uint32_t local = before + x - (uint32_t)cnt;
+  if (w == 0) {
+    uint32_t excl = 0;
+    volatile uint32_t *status = rb.tile_status;
+    if (tile == 0) {
+      if (lane == 0) status[0] = LB_INC | total;
+    } else {
+      if (lane == 0) status[tile] = LB_AGG | total;
+      for (int pt = tile - 1;; pt -= 32) {
+        const int i = pt - lane;
+        uint32_t sv = i >= 0 ? (uint32_t)status[i] : (uint32_t)LB_INC;  // before tile 0: 0
+        for (int polls = 0; __any_sync(0xffffffffu, (sv & ~LB_VAL) == 0u); ++polls) {
+          if (polls > kLookbackPolls) {
+            if ((sv & ~LB_VAL) == 0u) {
+              atomicOr(d.status, ST_TIMEOUT);
+              sv = LB_INC;
+            }
+          } else if ((sv & ~LB_VAL) == 0u) {
+            sv = status[i];
+          }
+        }
+        const unsigned inc = __ballot_sync(0xffffffffu, (sv & LB_INC) != 0u);
+        const int stop = inc ? __ffs(inc) - 1 : 31;
+        uint32_t v = lane <= stop ? (sv & LB_VAL) : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        excl += v;
+        if (inc) break;
+      }
+      if (lane == 0) status[tile] = LB_INC | (excl + total);
+    }
+    if (lane == 0) s_excl = excl;
+  }
+  __syncthreads();
+  if (tile == (int)gridDim.x - 1 && threadIdx.x == 0) {
+    const int np = (int)(s_excl + total);
+    d.np_rep[0] = np;
+    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+  }
+  if (head) cell_pair_emit(k, d, rb, R, h, (int)(s_excl + local), prec);
 }
 
 // First entry slot of bond b (rebuilt system R): its system's slots start at
@@ -358,6 +479,8 @@ __global__ void k_rb_finish(DevState d) {
   d.dt[i] = 0.0;
 }
 
+int rebuild_pair_tiles(int nb) { return nb > 0 ? (nb + kPairTile - 1) / kPairTile : 1; }
+
 int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, int prec,
                    cudaStream_t st, bool first_in_graph) {
   int launched = 0;
@@ -377,11 +500,16 @@ int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, 
   launched += launch_exclusive_scan(rb.gcount, rb.gstart, rb.n_groups, rb.scan_tmp, st);
   launch_pdl(k_rb_scatter, dim3(g256), dim3(256), 0, st, d, rb);
   launch_pdl(k_rb_rank, dim3(g256), dim3(256), 0, st, d, rb);
-  launch_pdl(k_rb_count, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb);
-  launched += 3;
-  launched += launch_exclusive_scan(rb.pair_count, rb.pair_off, d.nb, rb.scan_tmp, st);
-  launch_pdl(k_rb_emit, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb, prec);
-  ++launched;
+  launched += 2;
+  if (d.nrep == 1) {
+    launch_pdl(k_rb_pairs, dim3(rb.n_tiles), dim3(kPairTile), 0, st, k, d, rb, prec);
+    ++launched;
+  } else {
+    launch_pdl(k_rb_count, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb);
+    launched += 1 + launch_exclusive_scan(rb.pair_count, rb.pair_off, d.nb, rb.scan_tmp, st);
+    launch_pdl(k_rb_emit, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb, prec);
+    ++launched;
+  }
   launched += launch_exclusive_scan(rb.deg, rb.deg_off, d.nb, rb.scan_tmp, st);
   launch_pdl(k_rb_csr_fill, dim3((d.pcap_total > 0 ? d.pcap_total + 255 : 256) / 256), dim3(256),
              0, st, d, rb);
