@@ -63,8 +63,6 @@ sc_status check_status(sc_ctx *c) {
   unsigned s = c->hb->status;
   if (s & sc::ST_NAN) return fail(c, SC_ERR_NAN, "non-finite position or displacement");
   if (s & sc::ST_BAD_CELL) return fail(c, SC_ERR_NAN, "bond outside the cell grid (non-finite position)");
-  if (s & sc::ST_TIMEOUT)
-    return fail(c, SC_ERR_TIMEOUT, "the rebuild's pair pass gave up waiting on a tile");
   if (s & sc::ST_LIST_OVERFLOW) return fail(c, SC_ERR_LIST_OVERFLOW, "pair list overflow");
   if (s & sc::ST_TETHER)
     return fail(c, SC_ERR_UNPHYSICAL, "a crosslink anchor moved off the bonds around its site");
@@ -951,9 +949,6 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
     CKS(dzero(&rb.pair_off, (size_t)nbi + 1));
     CKS(dzero(&rb.deg, nbi));
     CKS(dzero(&rb.deg_off, (size_t)nbi + 1));
-    rb.n_tiles = sc::rebuild_pair_tiles((int)nbi);
-    CKS(dzero(&rb.tile_status, (size_t)rb.n_tiles));
-    CKS(dzero(&rb.ticket, 1));
     CKS(dalloc(c, &rb.scan_tmp,
                (size_t)std::max(sc::scan_temp_ints(rb.n_groups), sc::scan_temp_ints(nbi))));
   }

@@ -45,8 +45,7 @@ enum : unsigned {
   ST_UNPHYSICAL = 4u,     // accumulated displacement above 10000
   ST_BAD_CELL = 8u,       // cell index out of range (non-finite position)
   ST_BAD_INPUT = 16u,     // caller's device data out of range (site offsets)
-  ST_TETHER = 32u,        // a crosslink anchor left the bonds it can sit on
-  ST_TIMEOUT = 64u        // a bounded device wait gave up (the rebuild's pair pass)
+  ST_TETHER = 32u         // a crosslink anchor left the bonds it can sit on
 };
 
 // Bond geometry for the FP64 pair stage: the reference's Bond state after

@@ -63,8 +63,8 @@ int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st)
 // Scratch of a context's rebuild (sc_rebuild.cu).  Sizes: key, tmp, skey,
 // sval, pair_count, deg: nb; gcount: n_groups; gstart: n_groups + 1;
 // pair_off, deg_off: nb + 1; range: n_cells; occ: n_groups words;
-// scan_tmp: scan_temp_ints(max(n_groups, nb)); tile_status: n_tiles;
-// ticket: 1.  gcount, deg, range and occ start zeroed.
+// scan_tmp: scan_temp_ints(max(n_groups, nb)).  gcount, deg, range and occ
+// start zeroed.
 struct RebuildBufs {
   int n_groups;        // groups of 32 cells: n_cells / 32 (each system's cells
                        // start at a multiple of 32)
@@ -79,12 +79,7 @@ struct RebuildBufs {
   int *pair_count, *pair_off;
   int *deg, *deg_off;
   int *scan_tmp;
-  int n_tiles;             // tiles of 128 sorted entries (one system's fused pair pass)
-  uint32_t *tile_status;   // n_tiles look-back words
-  int *ticket;             // tile tickets
 };
-// Tiles of the one-system pair pass for nb bonds.
-int rebuild_pair_tiles(int nb);
 // The whole rebuild of the systems flagged in d.due; returns the kernels
 // launched.  first_in_graph: the first kernel opens a captured conditional
 // body (launched without the programmatic-dependence attribute).

@@ -16,10 +16,9 @@
 //   (scan)         group offsets
 //   k_rb_scatter   bonds into their groups (counts back to zero)
 //   k_rb_rank      stable order inside each group; cell ranges and bits
-//   k_rb_pairs     one system: pairs of every cell (head entry of the
-//                  sorted order), their offsets by decoupled look-back, and
-//                  the pairs in the reference's order, per-bond degrees
-//   k_rb_count, (scan), k_rb_emit   the same in three steps, several systems
+//   k_rb_count     pairs of every cell (head entry of the sorted order)
+//   (scan)         pair offsets
+//   k_rb_emit      pairs in the reference's order, per-bond degrees
 //   (scan)         entry offsets
 //   k_rb_csr_fill  entries (pair << 1 | role) of every bond
 //   k_rb_csr_sort  entries in pair order, slots of both roles, ranges
@@ -48,8 +47,6 @@ __global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, Rebuild
     const int w0 = R.cell0 >> 5, w1 = (R.cell0 + R.n_cells + 31) >> 5;
     for (int w = w0 + tid; w < w1; w += nthreads) rb.occ[w] = 0u;
   }
-  for (int i = tid; i < rb.n_tiles; i += nthreads) rb.tile_status[i] = 0u;
-  if (tid == 0) *rb.ticket = 0;
   const int b = tid;
   bool in = false;
   int g = 0;
@@ -247,7 +244,7 @@ __device__ __forceinline__ void cell_pair_emit(const SysConst &k, const DevState
 }
 
 // Pairs each cell contributes, at its head entry (zero for the other
-// entries), for the offsets' scan (several systems).
+// entries), for the offsets' scan.
 __global__ void k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
   grid_dep_sync();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -264,8 +261,8 @@ __global__ void k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
   rb.pair_count[q] = cnt;
 }
 
-// Each cell's pairs at its scanned offset in its system's pair segment
-// (several systems).  Threads q < nrep record their system's pair count (a
+// Each cell's pairs at its scanned offset in its system's pair segment.
+// Threads q < nrep record their system's pair count (a
 // list longer than its segment sets the overflow bit; the count is kept so
 // the host can size the segment).
 __global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
@@ -284,102 +281,6 @@ __global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
   CellHead h;
   cell_head(k, rb, R, q, c, h);
   cell_pair_emit(k, d, rb, R, h, rb.pair_off[q] - rb.pair_off[sys_lo(rb, R)], prec);
-}
-
-// One system: counts, offsets and emission in one kernel.  Each block (a
-// tile of sorted entries, taken in ticket order) counts its cells' pairs,
-// scans them, and finds the pairs of all earlier tiles by decoupled
-// look-back (Merrill & Garland, "Single-pass parallel prefix scan with
-// decoupled look-back", NVIDIA tech. report NVR-2016-002): a tile publishes
-// its own total at once and its inclusive prefix when known, and one warp
-// reads 32 predecessors at a time back to the nearest inclusive prefix.
-// Tiles wait only on tiles with earlier tickets, which are running; a
-// look-back word that stays empty past the poll limit sets ST_TIMEOUT.  The
-// last tile records the system's pair count.
-constexpr int kPairTile = 128;
-constexpr uint32_t LB_AGG = 1u << 30;  // tile total published
-constexpr uint32_t LB_INC = 2u << 30;  // inclusive prefix published
-constexpr uint32_t LB_VAL = LB_AGG - 1u;
-constexpr int kLookbackPolls = 1 << 20;
-
-__global__ void __launch_bounds__(kPairTile) k_rb_pairs(SysConst k, DevState d, RebuildBufs rb,
-                                                          int prec) {
-  grid_dep_sync();
-  __shared__ int s_tile;
-  __shared__ uint32_t s_warp[kPairTile / 32];
-  __shared__ uint32_t s_excl;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_tile = atomicAdd(rb.ticket, 1);
-  __syncthreads();
-  const int tile = s_tile;
-  const int q = tile * kPairTile + threadIdx.x;
-  const ReplicaConst &R = d.rep[0];
-  CellHead h;
-  bool head = false;
-  int cnt = 0;
-  if (q < rb.gstart[rb.n_groups] && k.like_like) {
-    const int c = (int)rb.skey[q];
-    head = q == 0 || (int)rb.skey[q - 1] != c;
-    if (head) {
-      cell_head(k, rb, R, q, c, h);
-      cnt = cell_pair_count(d, rb, h);
-    }
-  }
-  // Exclusive scan of the counts over the tile.
-  uint32_t x = (uint32_t)cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) s_warp[w] = x;
-  __syncthreads();
-  uint32_t before = 0, total = 0;
-#pragma unroll
-  for (int i = 0; i < kPairTile / 32; ++i) {
-    before += i < w ? s_warp[i] : 0u;
-    total += s_warp[i];
-  }
-  const uint32_t local = before + x - (uint32_t)cnt;
-  if (w == 0) {
-    uint32_t excl = 0;
-    volatile uint32_t *status = rb.tile_status;
-    if (tile == 0) {
-      if (lane == 0) status[0] = LB_INC | total;
-    } else {
-      if (lane == 0) status[tile] = LB_AGG | total;
-      for (int pt = tile - 1;; pt -= 32) {
-        const int i = pt - lane;
-        uint32_t sv = i >= 0 ? (uint32_t)status[i] : (uint32_t)LB_INC;  // before tile 0: 0
-        for (int polls = 0; __any_sync(0xffffffffu, (sv & ~LB_VAL) == 0u); ++polls) {
-          if (polls > kLookbackPolls) {
-            if ((sv & ~LB_VAL) == 0u) {
-              atomicOr(d.status, ST_TIMEOUT);
-              sv = LB_INC;
-            }
-          } else if ((sv & ~LB_VAL) == 0u) {
-            sv = status[i];
-          }
-        }
-        const unsigned inc = __ballot_sync(0xffffffffu, (sv & LB_INC) != 0u);
-        const int stop = inc ? __ffs(inc) - 1 : 31;
-        uint32_t v = lane <= stop ? (sv & LB_VAL) : 0u;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        excl += v;
-        if (inc) break;
-      }
-      if (lane == 0) status[tile] = LB_INC | (excl + total);
-    }
-    if (lane == 0) s_excl = excl;
-  }
-  __syncthreads();
-  if (tile == (int)gridDim.x - 1 && threadIdx.x == 0) {
-    const int np = (int)(s_excl + total);
-    d.np_rep[0] = np;
-    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
-  }
-  if (head) cell_pair_emit(k, d, rb, R, h, (int)(s_excl + local), prec);
 }
 
 // First entry slot of bond b (rebuilt system R): its system's slots start at
@@ -479,8 +380,6 @@ __global__ void k_rb_finish(DevState d) {
   d.dt[i] = 0.0;
 }
 
-int rebuild_pair_tiles(int nb) { return nb > 0 ? (nb + kPairTile - 1) / kPairTile : 1; }
-
 int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, int prec,
                    cudaStream_t st, bool first_in_graph) {
   int launched = 0;
@@ -500,16 +399,10 @@ int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, 
   launched += launch_exclusive_scan(rb.gcount, rb.gstart, rb.n_groups, rb.scan_tmp, st);
   launch_pdl(k_rb_scatter, dim3(g256), dim3(256), 0, st, d, rb);
   launch_pdl(k_rb_rank, dim3(g256), dim3(256), 0, st, d, rb);
-  launched += 2;
-  if (d.nrep == 1) {
-    launch_pdl(k_rb_pairs, dim3(rb.n_tiles), dim3(kPairTile), 0, st, k, d, rb, prec);
-    ++launched;
-  } else {
-    launch_pdl(k_rb_count, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb);
-    launched += 1 + launch_exclusive_scan(rb.pair_count, rb.pair_off, d.nb, rb.scan_tmp, st);
-    launch_pdl(k_rb_emit, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb, prec);
-    ++launched;
-  }
+  launch_pdl(k_rb_count, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb);
+  launched += 3 + launch_exclusive_scan(rb.pair_count, rb.pair_off, d.nb, rb.scan_tmp, st);
+  launch_pdl(k_rb_emit, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb, prec);
+  ++launched;
   launched += launch_exclusive_scan(rb.deg, rb.deg_off, d.nb, rb.scan_tmp, st);
   launch_pdl(k_rb_csr_fill, dim3((d.pcap_total > 0 ? d.pcap_total + 255 : 256) / 256), dim3(256),
              0, st, d, rb);
