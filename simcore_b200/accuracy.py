@@ -1,8 +1,9 @@
 """Accuracy of the mixed-precision path against the FP64 path, output by output.
 
 The FP64 path is bit-identical to the reference's CPU code.  The mixed path
-evaluates pair geometry and WCA forces in FP32 (nearly parallel pairs in
-FP64) and runs the fast FP64 integrator.  mixed_errors() loads one state into
+evaluates pair geometry and WCA forces in FP32 (nearly parallel pairs side by
+side in FP64) and runs the fast integrator: FP64 bending, tension solve and
+positions, the midstep noise drawn and projected in FP32.  mixed_errors() loads one state into
 a fresh context of each precision -- fresh pair lists and no stale pair
 forces, so both evaluate exactly the same pairs -- and compares, as
 max |mixed - fp64| / max |fp64| over all entries:

@@ -278,26 +278,38 @@ __device__ __forceinline__ double centered_uniform(uint32_t w) {
   return h * 2.3283064365386963e-10 - 0.5;
 }
 
-// FAST: one Newton reciprocal per row instead of two divisions.
-__device__ __forceinline__ void thomas_fast(double *a, const double *b, double *c,
-                                            double *d, int n) {
+// The same uniform in FP32 from the word's top 23 bits, (m + 1/2) 2^-23 -
+// 1/2 with m = w >> 9, exact (m from its bits, as above): the mixed step's
+// noise, within 2^-24 of the FP64 one.
+__device__ __forceinline__ float centered_uniform_f(uint32_t w) {
+  const float m = __uint_as_float(0x4B000000u | (w >> 9)) - 8388608.0f;
+  return fmaf(m + 0.5f, 1.1920928955078125e-7f, -0.5f);
+}
+
+__device__ __forceinline__ double recip_t(double x) { return recip_nr(x); }
+__device__ __forceinline__ float recip_t(float x) { return __frcp_rn(x); }
+
+// FAST: one reciprocal per row instead of two divisions (FP64: Newton from
+// the FP32 reciprocal; FP32: the rounded reciprocal).
+template <class T>
+__device__ __forceinline__ void thomas_fast(T *a, const T *b, T *c, T *d, int n) {
   n--;
-  double r = recip_nr(b[0]);
-  double cp = c[0] * r;
-  double dp = d[0] * r;
+  T r = recip_t(b[0]);
+  T cp = c[0] * r;
+  T dp = d[0] * r;
   c[0] = cp;
   d[0] = dp;
   for (int i = 1; i < n; ++i) {
-    const double am = a[i - 1];
-    r = recip_nr(b[i] - am * cp);
-    const double cn = c[i] * r;
-    const double dn = (d[i] - am * dp) * r;
+    const T am = a[i - 1];
+    r = recip_t(b[i] - am * cp);
+    const T cn = c[i] * r;
+    const T dn = (d[i] - am * dp) * r;
     c[i] = cn;
     d[i] = dn;
     cp = cn;
     dp = dn;
   }
-  dp = (d[n] - a[n - 1] * dp) * recip_nr(b[n] - a[n - 1] * cp);
+  dp = (d[n] - a[n - 1] * dp) * recip_t(b[n] - a[n - 1] * cp);
   d[n] = dp;
   for (int i = n; i-- > 0;) {
     dp = d[i] - c[i] * dp;
@@ -324,38 +336,38 @@ __device__ __forceinline__ void solve_tridiag(double *a, const double *b, double
 // one instruction stream: P[r] is the coupling to the row eliminated before
 // (a[r-1] going down, c[r] going up), Q[r] the one towards row m, which the
 // elimination overwrites with its reduced value.
-__device__ __forceinline__ void thomas_twisted(double *a, const double *b, double *c,
-                                               double *d, int n, bool top) {
+template <class T>
+__device__ __forceinline__ void thomas_twisted(T *a, const T *b, T *c, T *d, int n, bool top) {
   const unsigned pair = 3u << ((threadIdx.x & 31) & 30);
   const int m = n >> 1;
   const int steps = top ? m : n - 1 - m;
   const int dir = top ? 1 : -1;
   const int r0 = top ? 0 : n - 1;
-  const double *P = top ? a - 1 : c;
-  double *Q = top ? c : a - 1;
-  double u = 0.0, v = 0.0;  // reduced (Q, d) of the last row eliminated
+  const T *P = top ? a - 1 : c;
+  T *Q = top ? c : a - 1;
+  T u = 0, v = 0;  // reduced (Q, d) of the last row eliminated
   if (steps > 0) {
-    const double rr = recip_nr(b[r0]);
+    const T rr = recip_t(b[r0]);
     u = Q[r0] * rr;
     v = d[r0] * rr;
     Q[r0] = u;
     d[r0] = v;
     int r = r0 + dir;
     for (int st = 1; st < steps; ++st, r += dir) {
-      const double pc = P[r];
-      const double ri = recip_nr(b[r] - pc * u);
-      const double un = Q[r] * ri;
-      const double vn = (d[r] - pc * v) * ri;
+      const T pc = P[r];
+      const T ri = recip_t(b[r] - pc * u);
+      const T un = Q[r] * ri;
+      const T vn = (d[r] - pc * v) * ri;
       Q[r] = un;
       d[r] = vn;
       u = un;
       v = vn;
     }
   }
-  const double u2 = __shfl_xor_sync(pair, u, 1), v2 = __shfl_xor_sync(pair, v, 1);
-  const double tu = top ? u : u2, tv = top ? v : v2;  // row m-1: c', d'
-  const double bu = top ? u2 : u, bv = top ? v2 : v;  // row m+1: a', d'
-  double num = d[m], den = b[m];
+  const T u2 = __shfl_xor_sync(pair, u, 1), v2 = __shfl_xor_sync(pair, v, 1);
+  const T tu = top ? u : u2, tv = top ? v : v2;  // row m-1: c', d'
+  const T bu = top ? u2 : u, bv = top ? v2 : v;  // row m+1: a', d'
+  T num = d[m], den = b[m];
   if (m >= 1) {
     num -= a[m - 1] * tv;
     den -= a[m - 1] * tu;
@@ -364,7 +376,7 @@ __device__ __forceinline__ void thomas_twisted(double *a, const double *b, doubl
     num -= c[m] * bv;
     den -= c[m] * bu;
   }
-  double x = num * recip_nr(den);
+  T x = num * recip_t(den);
   __syncwarp(pair);  // both lanes have read row m
   if (top) d[m] = x;
   int r = m - dir;
@@ -758,7 +770,69 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
 
   // ---- P2: random forces, projection, previous positions -----------------
   double fr[3] = {0, 0, 0};
-  if (midstep) {
+  if (midstep && k.stoch && FAST && !pcr) {
+    // The mixed step draws, projects and applies its noise in FP32 (the
+    // north star keeps the tension solve, the bending forces that feed it
+    // and the positions in FP64): the same Philox words, the uniforms to
+    // 2^-24, the projection system solved from both ends in FP32 over the
+    // Thomas arrays' first halves, the projected force added in FP64.
+    float *ffn = reinterpret_cast<float *>(sfn);  // 3 x C floats
+    float *fT = reinterpret_cast<float *>(sT), *fa = reinterpret_cast<float *>(sa);
+    float *fb = reinterpret_cast<float *>(sb), *fcm = reinterpret_cast<float *>(sc);
+    float frf[3] = {0.f, 0.f, 0.f};
+    const float uf[3] = {(float)u[0], (float)u[1], (float)u[2]};
+    if (active) {  // ConstructUnprojectedRandomForces (:518-548)
+      uint32_t w[4];
+      sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
+                            s_seed, (uint32_t)fc.f_local, w);
+      float xi[3] = {0.f, 0.f, 0.f}, tnf[3] = {0.f, 0.f, 0.f}, txi = 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        xi[i] = centered_uniform_f(w[i]);
+        tnf[i] = (float)tn[i];
+        txi = fmaf(tnf[i], xi[i], txi);
+      }
+      const float sperp = (float)fc.sperp, dsp = (float)(fc.spar - fc.sperp);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) frf[i] = fmaf(sperp, xi[i], dsp * txi * tnf[i]);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) ffn[i * C + t] = frf[i];
+    }
+    __syncthreads();
+    if (has_bond) {  // GeometricallyProjectRandomForces (:550-599)
+      float rhs = 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) rhs = fmaf(ffn[i * C + t + 1] - frf[i], uf[i], rhs);
+      fT[t] = rhs;
+      fb[t] = 2.f;
+      if (j > 0) {
+        fcm[t - 1] = -(float)scos[t - 1];
+        fa[t - 1] = -(float)scos[t - 1];
+      }
+    }
+    __syncthreads();
+    if (t < 2 * nfb) {
+      const FilConst &f = sfil[t >> 1];
+      const int fb0 = f.site0 - s0;
+      thomas_twisted(fa + fb0, fb + fb0, fcm + fb0, fT + fb0, f.n - 1, (t & 1) == 0);
+    }
+    if (dets_early) {  // the determinants, on lanes of other warps meanwhile
+      if (t >= g_dt && t - g_dt < nfb) det_forward(sdt, scos, sfil[t - g_dt], s0, t - g_dt);
+      else if (t >= g_db && t - g_db < nfb) det_backward(sdb, scos, sfil[t - g_db], s0, t - g_db);
+    }
+    __syncthreads();
+    if (active) {
+      const float tt = j < n - 1 ? fT[t] : 0.f, tp = j > 0 ? fT[t - 1] : 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        const float up = j > 0 ? (float)V(su, t - 1, i) : 0.f;
+        fr[i] = (double)fmaf(tt, uf[i], fmaf(-tp, up, frf[i]));
+      }
+      d.fr[0][g] = fr[0];  // the projected noise, reused by the full step
+      d.fr[1][g] = fr[1];
+      d.fr[2][g] = fr[2];
+    }
+  } else if (midstep) {
     if (k.stoch) {
       if (active) {  // ConstructUnprojectedRandomForces (:518-548)
         uint32_t w[4];

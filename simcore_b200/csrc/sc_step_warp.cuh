@@ -108,12 +108,16 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
   }
   if (!has_bond) u[0] = u[1] = u[2] = 0.0;
   double xi[3] = {0, 0, 0};
+  float xif[3] = {0.f, 0.f, 0.f};  // fast: the mixed step's FP32 noise
   if (midstep && k.stoch) {  // uniforms of ConstructUnprojectedRandomForces
     uint32_t wv[4];
     sc_host_philox4x32_10((uint32_t)j, (uint32_t)mcount, (uint32_t)(mcount >> 32), 0u,
                           d.rep[fc.rep].seed, (uint32_t)fc.f_local, wv);
 #pragma unroll
-    for (int i = 0; i < ND; ++i) xi[i] = centered_uniform(wv[i]);
+    for (int i = 0; i < ND; ++i) {
+      if (FAST) xif[i] = centered_uniform_f(wv[i]);
+      else xi[i] = centered_uniform(wv[i]);
+    }
   }
   if (overflowed) return;  // the whole warp: the bit is uniform
   if (active && midstep) {  // Mesh::UpdatePrevPositions (src/mesh.cpp:175-182)
@@ -199,7 +203,53 @@ __global__ void __launch_bounds__(kIntWarps * 32, kIntMinBlocks)
   }
 
   // ---- random forces and their projection (midsteps, :518-599) ------------
-  if (midstep && k.stoch) {
+  if (FAST && midstep && k.stoch) {
+    // The mixed step: noise, projection and its solve in FP32 over the
+    // Thomas arrays' first halves (as in k_integrate), the result in FP64.
+    float *fa = reinterpret_cast<float *>(sa), *fb = reinterpret_cast<float *>(sb);
+    float *fcm = reinterpret_cast<float *>(sc), *fd = reinterpret_cast<float *>(sd);
+    float frf[3] = {0.f, 0.f, 0.f};
+    const float uf[3] = {(float)u[0], (float)u[1], (float)u[2]};
+    if (active) {
+      float tnf[3] = {0.f, 0.f, 0.f}, txi = 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        tnf[i] = (float)tn[i];
+        txi = fmaf(tnf[i], xif[i], txi);
+      }
+      const float sperp = (float)fc.sperp, dsp = (float)(fc.spar - fc.sperp);
+#pragma unroll
+      for (int i = 0; i < ND; ++i) frf[i] = fmaf(sperp, xif[i], dsp * txi * tnf[i]);
+    }
+    float frn[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) frn[i] = __shfl_down_sync(0xffffffffu, frf[i], 1);
+    if (has_bond) {
+      float rhs = 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) rhs = fmaf(frn[i] - frf[i], uf[i], rhs);
+      fd[t] = rhs;
+      fb[t] = 2.f;
+      if (j < n - 2) {
+        fcm[t] = -(float)cs;
+        fa[t] = -(float)cs;
+      }
+    }
+    __syncwarp();
+    if (active && j == 0) thomas_fast(fa + t, fb + t, fcm + t, fd + t, n - 1);
+    __syncwarp();
+    if (active) {
+      const float tt = j < n - 1 ? fd[t] : 0.f, tp = j > 0 ? fd[t - 1] : 0.f;
+#pragma unroll
+      for (int i = 0; i < ND; ++i) {
+        const float up = j > 0 ? (float)um[i] : 0.f;
+        fr[i] = (double)fmaf(tt, uf[i], fmaf(-tp, up, frf[i]));
+      }
+      d.fr[0][g] = fr[0];  // re-used by the full step
+      d.fr[1][g] = fr[1];
+      d.fr[2][g] = fr[2];
+    }
+  } else if (midstep && k.stoch) {
     if (active) {
       double xt[3] = {0, 0, 0};
       if (FAST) {

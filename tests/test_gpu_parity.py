@@ -228,22 +228,42 @@ def test_graph_matches_oracle():
         compare_state(ctx, o, 3, capture=False)
 
 
-def test_fast_integrator_long_filaments_close_to_exact():
-    """Workload C's length spread (5 to 200 bonds): the fast integrator solves
-    the 256-site blocks that hold a filament of more than 32 bonds by
-    parallel cyclic reduction.  Against the exact integrator (the
-    reference's sequential Thomas) on identical forces, positions agree to
-    1e-12 relative after one BD step; the captured run gives the host-driven
-    loop's bits."""
-    system, fils, sites = _workload("C", 0.002, seed=3, side=150.0)
-    assert max(f["length"] for f in fils) > 128
+def _fast_vs_exact(system, fils, sites):
+    """One BD step of the fast and the exact integrator on identical forces:
+    without noise, positions agree to 1e-12 relative (FMA contraction,
+    reciprocals, two-sided or parallel-cyclic solves: FP64 rounding only);
+    with noise, which the fast step draws and projects in FP32, the
+    displacements agree to 1e-6 of the largest one (the FP32 uniforms are
+    within 2^-24 of the FP64 ones)."""
+    quiet = dict(system, stoch_flag=0)
+    a = _ctx(quiet, fils, sites, "mixed")
+    b = _ctx(quiet, fils, sites, "mixed")
+    b.set_fast_integrator(False)
+    a.step(2)
+    b.step(2)
+    ra, rb = a.sites(), b.sites()
+    assert np.abs(ra - rb).max() <= 1e-12 * np.abs(rb).max()
     a = _ctx(system, fils, sites, "mixed")
     b = _ctx(system, fils, sites, "mixed")
     b.set_fast_integrator(False)
     a.step(2)
     b.step(2)
     ra, rb = a.sites(), b.sites()
-    assert np.abs(ra - rb).max() <= 1e-12 * np.abs(rb).max()
+    disp = np.abs(rb - sites).max()
+    assert disp > 0
+    assert np.abs(ra - rb).max() <= 1e-6 * disp
+    return a, b
+
+
+def test_fast_integrator_long_filaments_close_to_exact():
+    """Workload C's length spread (5 to 200 bonds): the fast integrator solves
+    the 256-site blocks that hold a filament of more than 32 bonds by
+    parallel cyclic reduction.  Against the exact integrator (the
+    reference's sequential Thomas) on identical forces: see _fast_vs_exact;
+    the captured run gives the host-driven loop's bits."""
+    system, fils, sites = _workload("C", 0.002, seed=3, side=150.0)
+    assert max(f["length"] for f in fils) > 128
+    _fast_vs_exact(system, fils, sites)
     c = _ctx(system, fils, sites, "mixed")
     d = _ctx(system, fils, sites, "mixed")
     c.step_graph(40)
@@ -252,19 +272,10 @@ def test_fast_integrator_long_filaments_close_to_exact():
 
 
 def test_fast_integrator_close_to_exact():
-    """The mixed path's contraction/reciprocal integrator against the exact
-    FP64 integrator on identical forces (both mixed precision): positions
-    agree to 1e-12 relative after one full BD step."""
+    """The mixed path's fast integrator against the exact FP64 integrator on
+    identical forces (both mixed precision): see _fast_vs_exact."""
     system, fils, sites = _workload("B", 0.05, seed=8)
-    a = _ctx(system, fils, sites, "mixed")
-    b = _ctx(system, fils, sites, "mixed")
-    b.set_fast_integrator(False)
-    a.step(2)
-    b.step(2)
-    ra, rb = a.sites(), b.sites()
-    scale = np.abs(rb).max()
-    assert np.abs(ra - rb).max() <= 1e-12 * scale
-    ta, tb = a.tensions(), b.tensions()
+    _fast_vs_exact(system, fils, sites)
 
 
 def _workload_E(scale, seed=0):
@@ -404,10 +415,12 @@ def test_fp64_uneven_lengths_bitwise():
 @pytest.mark.parametrize("precision,fast", [("fp64", False), ("mixed", False), ("mixed", True)])
 def test_warp_and_block_integrators_agree(precision, fast, block):
     """The warp-synchronous integrator (filaments of at most 32 sites) and the
-    block integrator give the same bits where both are exact, and agree to
-    1e-12 in the fast mixed variant (contraction choices differ); blocks of
-    64 sites run the kernel compiled for up to 128, blocks of 160 and 192 the
-    one compiled for up to 192."""
+    block integrator give the same bits where both are exact, and agree in
+    the fast mixed variant to 1e-5 of the largest displacement over the run's
+    46 steps (contraction choices and the FP32 noise projection's solve
+    order differ, by about 1e-7 of the noise each step);
+    blocks of 64 sites run the kernel compiled for up to 128, blocks of 160
+    and 192 the one compiled for up to 192."""
     system, fils, sites = _workload("B", 0.05, seed=9)
     a = _ctx(system, fils, sites, precision)
     b = _ctx(system, fils, sites, precision)
@@ -427,7 +440,7 @@ def test_warp_and_block_integrators_agree(precision, fast, block):
         assert_same(a.pairs(), b.pairs(), "pairs")
     else:
         ra, rb = a.sites(), b.sites()
-        assert np.abs(ra - rb).max() <= 1e-12 * np.abs(rb).max()
+        assert np.abs(ra - rb).max() <= 1e-5 * np.abs(rb - sites).max()
 
 
 def test_autotune_leaves_state_and_caches(tmp_path):
