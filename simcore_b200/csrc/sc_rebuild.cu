@@ -11,8 +11,9 @@
 // (n_cells / 32 of them), not the cell grid; cell ranges and occupancy bits
 // are written where cells start and end in the sorted order.
 //
-//   k_rb_keys      cell key of every bond, group counts; clears the
-//                  occupancy words of the rebuilt systems
+//   k_rb_keys      ZeroDrTot and the rebuild counters; cell key of every
+//                  bond, group counts; clears the occupancy words of the
+//                  rebuilt systems
 //   (scan)         group offsets
 //   k_rb_scatter   bonds into their groups (counts back to zero)
 //   k_rb_rank      stable order inside each group; cell ranges and bits
@@ -22,7 +23,6 @@
 //   (scan)         entry offsets
 //   k_rb_csr_fill  entries (pair << 1 | role) of every bond
 //   k_rb_csr_sort  entries in pair order, slots of both roles, ranges
-//   k_rb_finish    ZeroDrTot and the rebuild counters
 #include <cuda_runtime.h>
 
 #include "sc_cells.cuh"
@@ -41,6 +41,22 @@ __global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, Rebuild
   grid_dep_sync();
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int nthreads = gridDim.x * blockDim.x;
+  // InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321) for
+  // the rebuilt systems, and the rebuild counters (nothing in the rebuild
+  // reads or moves the sites).
+  if (tid == 0) *d.n_rebuilds += 1;
+  for (int r = tid; r < d.nrep; r += nthreads) {
+    if (!d.due[r]) continue;
+    d.dr_max_bits[r] = 0ull;
+    d.rep_rebuilds[r] += 1;
+  }
+  for (int i = tid; i < d.ns; i += nthreads) {
+    if (!d.due[d.fil[d.site_fil[i]].rep]) continue;
+    d.dz[0][i] = d.r[0][i];
+    d.dz[1][i] = d.r[1][i];
+    d.dz[2][i] = d.r[2][i];
+    d.dt[i] = 0.0;
+  }
   for (int r = 0; r < d.nrep; ++r) {
     if (!d.due[r]) continue;
     const ReplicaConst &R = d.rep[r];
@@ -362,23 +378,6 @@ __global__ void k_rb_csr_sort(DevState d, RebuildBufs rb) {
   }
 }
 
-// InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321) for
-// the rebuilt systems, and the rebuild counters.
-__global__ void k_rb_finish(DevState d) {
-  grid_dep_sync();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) *d.n_rebuilds += 1;
-  if (i < d.nrep && d.due[i]) {
-    d.dr_max_bits[i] = 0ull;
-    d.rep_rebuilds[i] += 1;
-  }
-  if (i >= d.ns) return;
-  if (!d.due[d.fil[d.site_fil[i]].rep]) return;
-  d.dz[0][i] = d.r[0][i];
-  d.dz[1][i] = d.r[1][i];
-  d.dz[2][i] = d.r[2][i];
-  d.dt[i] = 0.0;
-}
 
 int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, int prec,
                    cudaStream_t st, bool first_in_graph) {
@@ -407,9 +406,7 @@ int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, 
   launch_pdl(k_rb_csr_fill, dim3((d.pcap_total > 0 ? d.pcap_total + 255 : 256) / 256), dim3(256),
              0, st, d, rb);
   launch_pdl(k_rb_csr_sort, dim3(g256), dim3(256), 0, st, d, rb);
-  const int gfin = ((d.ns > d.nrep ? d.ns : d.nrep) + 255) / 256;
-  launch_pdl(k_rb_finish, dim3(gfin > 0 ? gfin : 1), dim3(256), 0, st, d);
-  return launched + 3;
+  return launched + 2;
 }
 
 }  // namespace sc

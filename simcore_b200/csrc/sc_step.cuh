@@ -439,7 +439,7 @@ __device__ __forceinline__ double dotn(const double *a, const double *b) {
 // Shared-memory words of one integrator block of C sites (the doubles; C/2
 // renormalisation flags and the block's filament constants follow).
 __host__ __device__ constexpr size_t integrate_smem_doubles(int C) {
-  return 24 * (size_t)C;
+  return 28 * (size_t)C;
 }
 
 // 8-byte asynchronous global -> shared copy (cp.async), completed by
@@ -561,7 +561,8 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // sc), free between the two solves' uses.
   double *sdt = midstep ? srp : sT;  // det_t     2C
   double *sdb = sdt + 2 * C;         // det_b     2C
-  int *sflag = (int *)(sfp + 3 * C);            // C/2 renormalisation flags
+  double *sdz = sfp + 3 * C;    // full step: prefetched rebuild origin (3C), tracker (C)
+  int *sflag = (int *)(sdz + 4 * C);            // C/2 renormalisation flags
   FilConst *sfil = (FilConst *)(sflag + C / 2); // the block's filaments
   __shared__ double s_drmax[32];
 
@@ -629,6 +630,10 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
       for (int i = 0; i < ND; ++i) cp_async8(&V(srp, t, i), &d.rp[i][g]);
       if (k.stoch)
         for (int i = 0; i < ND; ++i) cp_async8(&V(sfp, t, i), &d.fr[i][g]);
+      if (interaction) {  // the displacement tracker's inputs, read last
+        for (int i = 0; i < ND; ++i) cp_async8(&V(sdz, t, i), &d.dz[i][g]);
+        cp_async8(&V(sdz, t, 3), &d.dt[g]);
+      }
       cp_async_commit();
     }
   }
@@ -1232,11 +1237,11 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     // squared displacement twice, src/mesh.cpp:538-541, src/object.cpp:
     // 282-292).
     if (!midstep && interaction) {
-      double acc = d.dt[g];
+      double acc = V(sdz, t, 3);
       for (int twice = 0; twice < 2; ++twice)
 #pragma unroll
         for (int i = 0; i < ND; ++i) {
-          double dr = r[i] - d.dz[i][g];
+          double dr = r[i] - V(sdz, t, i);
           acc += dr * dr;
         }
       d.dt[g] = acc;
