@@ -255,16 +255,37 @@ __device__ __forceinline__ void thomas(double *a, const double *b, double *c,
   }
 }
 
-// 1/x for the fast integrator: Newton-Raphson iteration y <- y (2 - x y),
-// written as e = 1 - x y, y <- y + y e, twice from the FP32 reciprocal of x
-// (relative error 2^-23 -> 2^-46 -> FP64 rounding).  For |x| within the FP32
-// normal range, which the diagonals, determinants and lengths it serves are.
+// 1/x for the fast integrator: from the hardware's FP64 approximate
+// reciprocal y of x (PTX rcp.approx.ftz.f64), one step of the third-order
+// iteration y <- y (1 + e + e^2) with e = 1 - x y, the truncated series of
+// y / (1 - e) (Muller et al., Handbook of Floating-Point Arithmetic, 2nd
+// ed., sec. 4.7).  The seed's relative error is below 2^-19 (measured
+// 9.9e-7), so the step leaves e^3 < 2^-57 before the final rounding: within
+// an ulp of 1/x, from three dependent FMAs after one approximation and no
+// FP32 round trip (conversions are slow on this part).  For normal |x|,
+// which the diagonals, determinants and lengths it serves are.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ double recip_nr(double x) {
-  double y = (double)__frcp_rn((float)x);
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
+}
+
+// x^-1/2 for the fast integrator, the same way: the hardware's approximate
+// inverse square root y (PTX rsqrt.approx.ftz.f64), e = 1 - x y^2, and
+// y (1 - e)^-1/2 by its series to the second order, y (1 + e/2 + 3e^2/8):
+// relative error about 5e^3/16 before the final rounding (seed error below
+// 2^-19, measured 9.2e-7; the result within an ulp of 1/sqrt(x)).
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x, y * y, 1.0);
+  return fma(y, e * fma(e, 0.375, 0.5), y);
 }
 
 // ((double)w + 0.5) * 2^-32 - 0.5 for a 32-bit Philox word w, the noise's
@@ -287,10 +308,10 @@ __device__ __forceinline__ float centered_uniform_f(uint32_t w) {
 }
 
 __device__ __forceinline__ double recip_t(double x) { return recip_nr(x); }
-__device__ __forceinline__ float recip_t(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float recip_t(float x) { return rcp_approx(x); }
 
-// FAST: one reciprocal per row instead of two divisions (FP64: Newton from
-// the FP32 reciprocal; FP32: the rounded reciprocal).
+// FAST: one reciprocal per row instead of two divisions (FP64: recip_nr;
+// FP32: the approximate reciprocal, within an ulp).
 template <class T>
 __device__ __forceinline__ void thomas_fast(T *a, const T *b, T *c, T *d, int n) {
   n--;
@@ -346,23 +367,35 @@ __device__ __forceinline__ void thomas_twisted(T *a, const T *b, T *c, T *d, int
   const T *P = top ? a - 1 : c;
   T *Q = top ? c : a - 1;
   T u = 0, v = 0;  // reduced (Q, d) of the last row eliminated
+  // Each row's coefficients are loaded before the stores of the row before
+  // (they never overlap), so only the elimination's own chain is serial.
+  // The first row has no coupling (pc = 0 leaves b and d as they are).
+  int r = r0;
+  T pc = 0, bb = 0, qq = 0, dd = 0;
   if (steps > 0) {
-    const T rr = recip_t(b[r0]);
-    u = Q[r0] * rr;
-    v = d[r0] * rr;
-    Q[r0] = u;
-    d[r0] = v;
-    int r = r0 + dir;
-    for (int st = 1; st < steps; ++st, r += dir) {
-      const T pc = P[r];
-      const T ri = recip_t(b[r] - pc * u);
-      const T un = Q[r] * ri;
-      const T vn = (d[r] - pc * v) * ri;
-      Q[r] = un;
-      d[r] = vn;
-      u = un;
-      v = vn;
+    bb = b[r];
+    qq = Q[r];
+    dd = d[r];
+  }
+  for (int st = 0; st < steps; ++st) {
+    const int rn = r + dir;
+    T pcn = 0, bbn = 0, qqn = 0, ddn = 0;
+    if (st + 1 < steps) {
+      pcn = P[rn];
+      bbn = b[rn];
+      qqn = Q[rn];
+      ddn = d[rn];
     }
+    const T ri = recip_t(bb - pc * u);
+    u = qq * ri;
+    v = (dd - pc * v) * ri;
+    Q[r] = u;
+    d[r] = v;
+    r = rn;
+    pc = pcn;
+    bb = bbn;
+    qq = qqn;
+    dd = ddn;
   }
   const T u2 = __shfl_xor_sync(pair, u, 1), v2 = __shfl_xor_sync(pair, v, 1);
   const T tu = top ? u : u2, tv = top ? v : v2;  // row m-1: c', d'
@@ -379,10 +412,24 @@ __device__ __forceinline__ void thomas_twisted(T *a, const T *b, T *c, T *d, int
   T x = num * recip_t(den);
   __syncwarp(pair);  // both lanes have read row m
   if (top) d[m] = x;
-  int r = m - dir;
-  for (int st = 0; st < steps; ++st, r -= dir) {
-    x = d[r] - Q[r] * x;
+  r = m - dir;
+  T qb = 0, db = 0;
+  if (steps > 0) {
+    qb = Q[r];
+    db = d[r];
+  }
+  for (int st = 0; st < steps; ++st) {
+    const int rn = r - dir;
+    T qn = 0, dn = 0;
+    if (st + 1 < steps) {
+      qn = Q[rn];
+      dn = d[rn];
+    }
+    x = db - qb * x;
     d[r] = x;
+    r = rn;
+    qb = qn;
+    db = dn;
   }
 }
 
@@ -394,19 +441,38 @@ __device__ __forceinline__ void det_forward(double *sdt, const double *scos, con
   const int fb0 = f.site0 - s0, nn = f.n;
   double *dt = sdt + fb0 + q;
   const double *cs = scos + fb0;
-  dt[0] = 1;
-  dt[1] = 2;
-  for (int i = 2; i < nn; ++i) dt[i] = 2 * dt[i - 1] - (-cs[i - 2]) * (-cs[i - 2]) * dt[i - 2];
+  // The two previous values are carried in registers and each cosine is
+  // loaded a row ahead: the recurrence's chain holds no memory access.
+  double d2 = 1, d1 = 2;
+  dt[0] = d2;
+  dt[1] = d1;
+  double m = nn > 2 ? -cs[0] : 0.0;
+  for (int i = 2; i < nn; ++i) {
+    const double mn = i + 1 < nn ? -cs[i - 1] : 0.0;
+    const double dn = 2 * d1 - m * m * d2;
+    dt[i] = dn;
+    d2 = d1;
+    d1 = dn;
+    m = mn;
+  }
 }
 __device__ __forceinline__ void det_backward(double *sdb, const double *scos, const FilConst &f,
                                              int s0, int q) {
   const int fb0 = f.site0 - s0, nn = f.n;
   double *db = sdb + fb0 + q;
   const double *cs = scos + fb0;
-  db[nn] = 1;
-  db[nn - 1] = 2;
-  for (int i = 2; i < nn; ++i)
-    db[nn - i] = 2 * db[nn - i + 1] - (-cs[nn - i - 1]) * (-cs[nn - i - 1]) * db[nn - i + 2];
+  double d2 = 1, d1 = 2;
+  db[nn] = d2;
+  db[nn - 1] = d1;
+  double m = nn > 2 ? -cs[nn - 3] : 0.0;
+  for (int i = 2; i < nn; ++i) {
+    const double mn = i + 1 < nn ? -cs[nn - i - 2] : 0.0;
+    const double dn = 2 * d1 - m * m * d2;
+    db[nn - i] = dn;
+    d2 = d1;
+    d1 = dn;
+    m = mn;
+  }
 }
 
 // v /= |v| over ND components.  Exact: the reference's normalize_vector
@@ -417,7 +483,7 @@ __device__ __forceinline__ double normalize(double *v) {
 #pragma unroll
   for (int i = 0; i < ND; ++i) mag += v[i] * v[i];
   if (FAST) {
-    double inv = rsqrt(mag);
+    double inv = rsqrt_nr(mag);
 #pragma unroll
     for (int i = 0; i < ND; ++i) v[i] *= inv;
     return mag * inv;
