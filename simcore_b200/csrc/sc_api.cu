@@ -418,6 +418,23 @@ sc_status layout_integrator(sc_ctx *c) {
   c->nblocks = (int)blk_f0.size();
   d.blk_maxf = 0;
   for (int v : blk_nf) d.blk_maxf = std::max(d.blk_maxf, v);
+  // Equal filaments in equal blocks covering every filament: the kernel
+  // indexes them by arithmetic.
+  d.blk_uni_n = d.blk_uni_fpb = 0;
+  if (!blk_f0.empty() && n > 0) {
+    const int nn = off[1] - off[0], fpb = blk_nf[0];
+    bool uni = nn > 0 && fpb > 0 && (long long)blk_f0.size() == ((long long)n + fpb - 1) / fpb;
+    for (int q = 0; uni && q <= n; ++q) uni = off[q] == (long long)q * nn;
+    for (size_t i = 0; uni && i < blk_f0.size(); ++i) {
+      const long long f0 = (long long)i * fpb;
+      uni = blk_f0[i] == f0 && blk_nf[i] == std::min<long long>(fpb, n - f0) &&
+            blk_site0[i] == f0 * nn && blk_ns[i] == (long long)blk_nf[i] * nn;
+    }
+    if (uni) {
+      d.blk_uni_n = nn;
+      d.blk_uni_fpb = fpb;
+    }
+  }
   d.n_wg = (int)wg_f0.size();
   sc::prepare_integrate(c->C);
   drop_graph(c);

@@ -141,6 +141,10 @@ struct DevState {
   const int *blk_nf;       // per block: filament count
   const int *blk_ns;       // per block: site count
   int blk_maxf;            // most filaments in one block (shared-memory size)
+  // Equal filaments of blk_uni_n sites, blk_uni_fpb to a block, every block
+  // but the last full, sites numbered filament by filament from 0: blocks
+  // and sites then find their filaments by arithmetic (0: read the tables).
+  int blk_uni_n, blk_uni_fpb;
   // integrator warp groups (filaments of at most 32 sites): runs of whole
   // filaments, one lane per site
   int n_wg;

@@ -630,7 +630,6 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   double *sdz = sfp + 3 * C;    // full step: prefetched rebuild origin (3C), tracker (C)
   int *sflag = (int *)(sdz + 4 * C);            // C/2 renormalisation flags
   FilConst *sfil = (FilConst *)(sflag + C / 2); // the block's filaments
-  __shared__ double s_drmax[32];
 
 #define V(arr, slot, comp) arr[(comp) * C + (slot)]
 
@@ -645,10 +644,19 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // sets that bit), so the host can grow the list and redo the step.
   const bool overflowed = (*d.status & ST_LIST_OVERFLOW) != 0u;
   const unsigned long long mcount = *d.mcount;
-  const int s0 = d.blk_site0[blk];
-  const int count = d.blk_ns[blk];
-  const int f0 = d.blk_f0[blk];
-  const int nfb = d.blk_nf[blk];
+  const int un = d.blk_uni_n;
+  int s0, count, f0, nfb;
+  if (un > 0) {  // equal filaments: the block's range without a table load
+    f0 = blk * d.blk_uni_fpb;
+    nfb = min(d.blk_uni_fpb, d.nf - f0);
+    s0 = f0 * un;
+    count = nfb * un;
+  } else {
+    s0 = d.blk_site0[blk];
+    count = d.blk_ns[blk];
+    f0 = d.blk_f0[blk];
+    nfb = d.blk_nf[blk];
+  }
   __shared__ double s_hinv[9];  // the block's system (blocks never mix systems)
   __shared__ uint32_t s_seed;
   // Every global load the step needs is issued here, before the first
@@ -672,7 +680,11 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // P0 is issued here, alongside the staging of the filament constants,
   // rather than after the barrier.
   int f = 0, lf = 0, jn = 0;
-  if (active) {
+  if (active && un > 0) {
+    lf = t / un;
+    jn = (t - lf * un) | un << 16;
+    f = f0 + lf;
+  } else if (active) {
     f = d.site_fil[g];
     jn = d.site_jn[g];
     lf = f - f0;
@@ -686,7 +698,9 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // ---- P0: positions, orientations, bond forces --------------------------
   double r[3] = {0, 0, 0}, u[3] = {0, 0, 0};
   double bF[3] = {0, 0, 0}, bT[3] = {0, 0, 0};
+  int fsw = 0;  // the filament's renormalisation direction before this step
   if (active) {
+    fsw = d.f_switch[f];
     r[0] = d.r[0][g];
     r[1] = d.r[1][g];
     r[2] = d.r[2][g];
@@ -1220,43 +1234,66 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     if (stretched) sflag[lf] = 1;
   }
   // Positions change below only in a block with a filament to renormalise.
-  const int any_renorm = __syncthreads_or(stretched);
+  __syncthreads_or(stretched);
   if (t < nfb) {
-    const int fb0 = sfil[t].site0 - s0, nn = sfil[t].n;
-    const double l = sfil[t].l;
     const int fg = f0 + t;
     int sw = pre_sw, nnorm = pre_nn;
     if (sflag[t]) {
       sw = !sw;
       nnorm = 0;
-      if (sw) {
-        for (int jj = 1; jj < nn; ++jj)
-#pragma unroll
-          for (int i = 0; i < ND; ++i)
-            V(sr, fb0 + jj, i) = V(sr, fb0 + jj - 1, i) + l * V(su, fb0 + jj - 1, i);
-      } else {
-        for (int jj = nn - 1; jj > 0; --jj)
-#pragma unroll
-          for (int i = 0; i < ND; ++i)
-            V(sr, fb0 + jj - 1, i) = V(sr, fb0 + jj, i) - l * V(su, fb0 + jj - 1, i);
-      }
     }
     nnorm++;
     d.f_switch[fg] = sw;
     d.f_nnorm[fg] = nnorm;
   }
-  if (any_renorm) __syncthreads();
+  // The renormalised filament is rebuilt from one end along the bond
+  // orientations just computed: from its first site when the switch turns
+  // on, else from its last.  Every site runs the chain from that end itself
+  // (the same operations in the same order as one sweep over the filament),
+  // keeping its own position and its bond's far end, so no site waits for
+  // another's result.
+  const bool renorm = active && sflag[lf] != 0;
+  double rnext[3] = {0, 0, 0};
+  if (renorm) {
+    const double l = fc.l;
+    if (!fsw) {
+      double a[3] = {V(sr, base, 0), V(sr, base, 1), V(sr, base, 2)};
+      for (int jj = 1; jj <= j; ++jj)
+#pragma unroll
+        for (int i = 0; i < ND; ++i) a[i] = a[i] + l * V(su, base + jj - 1, i);
+      r[0] = a[0];
+      r[1] = a[1];
+      r[2] = a[2];
+      if (j < n - 1) {
+        rnext[0] = a[0];
+        rnext[1] = a[1];
+        rnext[2] = a[2];
+#pragma unroll
+        for (int i = 0; i < ND; ++i) rnext[i] = a[i] + l * V(su, t, i);
+      }
+    } else {
+      double a[3] = {V(sr, base + n - 1, 0), V(sr, base + n - 1, 1), V(sr, base + n - 1, 2)};
+      for (int jj = n - 1; jj > j; --jj) {
+        rnext[0] = a[0];
+        rnext[1] = a[1];
+        rnext[2] = a[2];
+#pragma unroll
+        for (int i = 0; i < ND; ++i) a[i] = a[i] - l * V(su, base + jj - 1, i);
+      }
+      r[0] = a[0];
+      r[1] = a[1];
+      r[2] = a[2];
+    }
+  }
 
   // ---- P6: bond geometry (Mesh::UpdateBondPositions), state write-back ----
   double my_dr = 0.0;
   if (active) {
-    const bool renorm = sflag[lf] != 0;
-    if (renorm)
-      for (int i = 0; i < 3; ++i) r[i] = V(sr, t, i);
     if (has_bond) {
       // Bond::ReInit on the final sites.  Without renormalisation it repeats
       // the orientation just computed (same operands, same operations).
-      double r2[3] = {V(sr, t + 1, 0), V(sr, t + 1, 1), V(sr, t + 1, 2)};
+      double r2[3];
+      for (int i = 0; i < 3; ++i) r2[i] = renorm ? rnext[i] : V(sr, t + 1, i);
       double s[3] = {0, 0, 0}, ub[3] = {0, 0, 0}, len, pos[3] = {0, 0, 0}, o[3] = {0, 0, 0};
       if (renorm) {
 #pragma unroll
@@ -1315,18 +1352,13 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
     }
   }
   if (!midstep && interaction) {
-    // Block max, then one atomic per block on the IEEE bits (non-negative).
+    // Warp max, then one atomic per warp on the IEEE bits (non-negative),
+    // with no barrier.
     double v = my_dr;
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    if ((t & 31) == 0) s_drmax[t >> 5] = v;
-    __syncthreads();
-    if (t < 32) {
-      v = (t < (C + 31) / 32) ? s_drmax[t] : 0.0;
-      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-      if (t == 0) {
-        if (!(v <= 1e300)) atomicOr(d.status, ST_NAN);
-        atomicMax(&d.dr_max_bits[sfil[0].rep], (unsigned long long)__double_as_longlong(v));
-      }
+    if ((t & 31) == 0 && v != 0.0) {
+      if (!(v <= 1e300)) atomicOr(d.status, ST_NAN);
+      atomicMax(&d.dr_max_bits[sfil[0].rep], (unsigned long long)__double_as_longlong(v));
     }
   }
 #undef V
