@@ -111,7 +111,7 @@ sc_status upload_reps(sc_ctx *c) {
 void free_store(sc_ctx *c, PairStore &q) {
   for (void *p : {(void *)q.pa, (void *)q.pb, (void *)q.pos1, (void *)q.pos2, (void *)q.pf64,
                   (void *)q.pf32, (void *)q.cf64, (void *)q.cf32, (void *)q.e_ent,
-                  (void *)q.pv64, (void *)q.pv32})
+                  (void *)q.pv64, (void *)q.pv32, (void *)q.cand})
     dfree(c, p);
   q = PairStore{};
 }
@@ -130,6 +130,8 @@ PairStore current_store(const sc_ctx *c) {
   q.pf32 = d.pf32;
   q.cf32 = d.cf32;
   q.pv32 = d.pv32;
+  q.cand = c->rb.cand;
+  q.cap = c->rb.cand_cap;
   return q;
 }
 
@@ -149,6 +151,8 @@ void install_store(sc_ctx *c, const PairStore &q) {
   d.pf32 = q.pf32;
   d.cf32 = q.cf32;
   d.pv32 = q.pv32;
+  c->rb.cand = q.cand;
+  c->rb.cand_cap = (int)q.cap;
 }
 
 // New pair arrays for `total` slots, with the context's precision and
@@ -165,6 +169,8 @@ sc_status alloc_store(sc_ctx *c, long long total, PairStore &q) {
     CKS(dalloc(c, &q.pos1, n));
     CKS(dalloc(c, &q.pos2, n));
     CKS(dalloc(c, &q.e_ent, 2 * n));
+    CKS(dalloc(c, &q.cand, n));
+    q.cap = (long long)n;
     CK(cudaMemsetAsync(q.pos1, 0, sizeof(int) * n, c->st));
     CK(cudaMemsetAsync(q.pos2, 0, sizeof(int) * n, c->st));
     if (c->prec == 0) {
@@ -962,12 +968,14 @@ static sc_status add_systems(sc_ctx *c, int nrep, const double *radius, const ui
     CKS(dalloc(c, &rb.sval, nbi));
     CKS(dzero(&rb.range, (size_t)k.n_cells));
     CKS(dzero(&rb.occ, (size_t)rb.n_groups));
-    CKS(dalloc(c, &rb.pair_count, nbi));
-    CKS(dzero(&rb.pair_off, (size_t)nbi + 1));
-    CKS(dzero(&rb.deg, nbi));
-    CKS(dzero(&rb.deg_off, (size_t)nbi + 1));
+    CKS(dzero(&rb.pair_count, 2 * (size_t)nbi));
+    rb.deg = rb.pair_count + nbi;
+    CKS(dzero(&rb.pair_off, 2 * (size_t)nbi + 1));
+    rb.deg_off = rb.pair_off + nbi;
     CKS(dalloc(c, &rb.scan_tmp,
-               (size_t)std::max(sc::scan_temp_ints(rb.n_groups), sc::scan_temp_ints(nbi))));
+               (size_t)std::max(sc::scan_temp_ints(rb.n_groups), sc::scan_temp_ints(2 * nbi))));
+    CKS(dzero(&rb.cand_n, 1));
+    CKS(dalloc(c, &rb.cand_start, nbi));
   }
   CKS(dzero(&d.e_off, nbi));
   CKS(dzero(&d.e_cnt, nbi));

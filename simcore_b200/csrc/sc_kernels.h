@@ -76,9 +76,20 @@ struct RebuildBufs {
   int *sval;           // sorted bond ids
   int2 *range;         // per cell: [start, end) in the sorted order
   unsigned *occ;       // per cell: occupied in the last rebuild of its system
+  // Per sorted entry: the pairs of the cell it heads (0 elsewhere), then per
+  // bond its pair entries; one array of 2 nb, scanned as one into 2 nb + 1
+  // offsets (pair_count = counts, deg = counts + nb; pair_off = offsets,
+  // deg_off = offsets + nb, shifted by the pair total, which cancels in
+  // every use).
   int *pair_count, *pair_off;
   int *deg, *deg_off;
   int *scan_tmp;
+  // Candidate pairs (a, b), each cell head's at cand_start[entry], in the
+  // reference's order; cand_cap = the pair slots of all segments.
+  int2 *cand;
+  int cand_cap;
+  int *cand_n;         // slots taken in the current rebuild
+  int *cand_start;     // per sorted entry
 };
 // The whole rebuild of the systems flagged in d.due; returns the kernels
 // launched.  first_in_graph: the first kernel opens a captured conditional

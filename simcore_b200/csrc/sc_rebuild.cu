@@ -12,16 +12,17 @@
 // are written where cells start and end in the sorted order.
 //
 //   k_rb_keys      ZeroDrTot and the rebuild counters; cell key of every
-//                  bond, group counts; clears the occupancy words of the
-//                  rebuilt systems
+//                  bond, group counts; clears the occupancy words and the
+//                  per-bond entry counts of the rebuilt systems
 //   (scan)         group offsets
 //   k_rb_scatter   bonds into their groups (counts back to zero)
 //   k_rb_rank      stable order inside each group; cell ranges and bits
-//   k_rb_count     pairs of every cell (head entry of the sorted order)
-//   (scan)         pair offsets
-//   k_rb_emit      pairs in the reference's order, per-bond degrees
-//   (scan)         entry offsets
-//   k_rb_csr_fill  entries (pair << 1 | role) of every bond
+//   k_rb_count     each cell's pairs in the reference's order, as candidates
+//                  (one reservation per block), their count at the cell's
+//                  head entry, per-bond entry counts
+//   (scan)         pair offsets and entry offsets, one scan of both
+//   k_rb_place     candidates to their list slots, stored forces zeroed,
+//                  per-bond entries (pair << 1 | role)
 //   k_rb_csr_sort  entries in pair order, slots of both roles, ranges
 #include <cuda_runtime.h>
 
@@ -44,7 +45,10 @@ __global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, Rebuild
   // InteractionManager::ZeroDrTot (src/interaction_manager.cpp:316-321) for
   // the rebuilt systems, and the rebuild counters (nothing in the rebuild
   // reads or moves the sites).
-  if (tid == 0) *d.n_rebuilds += 1;
+  if (tid == 0) {
+    *d.n_rebuilds += 1;
+    *rb.cand_n = 0;
+  }
   for (int r = tid; r < d.nrep; r += nthreads) {
     if (!d.due[r]) continue;
     d.dr_max_bits[r] = 0ull;
@@ -70,6 +74,7 @@ __global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, Rebuild
     uint32_t c = (uint32_t)k.n_cells;
     const int r = rep_of_bond(d, b);
     if (d.due[r]) {
+      rb.deg[b] = 0;
       const ReplicaConst &R = d.rep[r];
       int xyz[3];
       c = (uint32_t)(R.cell0 + bond_cell<ND>(d, R, b, xyz));
@@ -179,70 +184,21 @@ __device__ __forceinline__ void cell_head(const SysConst &k, const RebuildBufs &
   }
 }
 
-// Pairs of the cell: m (m - 1) / 2 inside it plus m * m_nbr with each kept
-// half-shell neighbour, less one for each bond whose filament neighbour
-// (b - 1 or b + 1) lies in the cell itself (counted once) or in a
-// neighbour -- the pairs pair_excluded drops.  Clamped to 2^30 - 1.
-__device__ __forceinline__ int cell_pair_count(const DevState &d, const RebuildBufs &rb,
-                                               const CellHead &h) {
-  const int m = h.m, c = h.c;
-  long long cnt = (long long)m * (m - 1) / 2;
-#pragma unroll
-  for (int kk = 0; kk < 13; ++kk) cnt += (long long)m * (h.s1[kk] - h.s0[kk]);
-  for (int i = 0; i < m; ++i) {
-    const int a = h.it[i], fa = d.bond_fil[a];
-    if (a + 1 < d.nb && d.bond_fil[a + 1] == fa) {
-      const int ka = (int)rb.key[a + 1];
-      if (ka == c) --cnt;  // each adjacent pair inside the cell, once
-#pragma unroll
-      for (int kk = 0; kk < 13; ++kk) cnt -= ka == h.nbr[kk];
-    }
-    if (a > 0 && d.bond_fil[a - 1] == fa) {
-      const int ka = (int)rb.key[a - 1];
-#pragma unroll
-      for (int kk = 0; kk < 13; ++kk) cnt -= ka == h.nbr[kk];
-    }
-  }
-  return cnt > 0x3fffffff ? 0x3fffffff : (int)cnt;
-}
-
-// Writes the cell's pairs from offset p of system R's pair segment, in the
-// reference's list order (Cell::MakePairs, src/cell.cpp:14-22): pairs inside
-// the cell, then with each half-shell neighbour in order; clears each new
-// pair's stored force and counts per-bond entries.  Only the non-empty
-// neighbours are visited (a warp steps through as many as its busiest lane
-// has, not all 13).
-__device__ __forceinline__ void cell_pair_emit(const SysConst &k, const DevState &d,
-                                               const RebuildBufs &rb, const ReplicaConst &R,
-                                               const CellHead &h, int p, int prec) {
-  const int p0 = R.p0, pcap = R.pcap;
-  auto emit = [&](int a, int b) {
-    if (pair_excluded(k, d, a, b)) return;
-    if (p < pcap) {
-      const int g = p0 + p;
-      d.pa[g] = a;
-      d.pb[g] = b;
-      if (prec == 0) {
-        double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)g;
-        st[0] = make_double2(0.0, 0.0);
-        st[1] = make_double2(0.0, 0.0);
-        if (d.pv64) {  // a new Interaction's stress and potential are 0
-          double2 *v = reinterpret_cast<double2 *>(d.pv64) + 2 * (size_t)g;
-          v[0] = make_double2(0.0, 0.0);
-          v[1] = make_double2(0.0, 0.0);
-        }
-      } else {
-        reinterpret_cast<float4 *>(d.pf32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (d.pv32) reinterpret_cast<float4 *>(d.pv32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-      atomicAdd(&rb.deg[a], 1);
-      atomicAdd(&rb.deg[b], 1);
-    }
-    ++p;
-  };
+// Calls f(a, b) for the cell's pairs in the reference's list order
+// (Cell::MakePairs, src/cell.cpp:14-22): pairs inside the cell, then with
+// each half-shell neighbour in order, less those pair_excluded drops.  Only
+// the non-empty neighbours are visited (a warp steps through as many as its
+// busiest lane has, not all 13).
+template <class F>
+__device__ __forceinline__ void cell_pairs_visit(const SysConst &k, const DevState &d,
+                                                 const RebuildBufs &rb, const CellHead &h,
+                                                 F &&f) {
   const int m = h.m;
   for (int i = 0; i < m - 1; ++i)
-    for (int j = i + 1; j < m; ++j) emit(h.it[i], h.it[j]);
+    for (int j = i + 1; j < m; ++j) {
+      const int a = h.it[i], b = h.it[j];
+      if (!pair_excluded(k, d, a, b)) f(a, b);
+    }
   unsigned busy = h.busy;
   while (busy) {
     const int kk = __ffs(busy) - 1;
@@ -255,48 +211,85 @@ __device__ __forceinline__ void cell_pair_emit(const SysConst &k, const DevState
         hi = h.s1[q2];
       }
     for (int i = 0; i < m; ++i)
-      for (int j = lo; j < hi; ++j) emit(h.it[i], rb.sval[j]);
+      for (int j = lo; j < hi; ++j) {
+        const int a = h.it[i], b = rb.sval[j];
+        if (!pair_excluded(k, d, a, b)) f(a, b);
+      }
   }
 }
 
-// Pairs each cell contributes, at its head entry (zero for the other
-// entries), for the offsets' scan.
-__global__ void k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
+// Each cell's pairs, found once: the head entry of a cell collects them (the
+// first kHeadBuf in shared memory, all again in the rare longer case), takes
+// a run of candidate slots from one reservation per block, and writes them
+// there in order; it records their count (0 at the other entries) and adds
+// each pair to both bonds' entry counts.  Candidates past cand_cap are
+// dropped: their system's list then outgrows its segment, which k_rb_place
+// reports.
+constexpr int kCountBlock = 128;
+constexpr int kHeadBuf = 8;
+
+__global__ void __launch_bounds__(kCountBlock) k_rb_count(SysConst k, DevState d, RebuildBufs rb) {
+  __shared__ int2 sbuf[kCountBlock][kHeadBuf];
+  __shared__ int swarp[kCountBlock / 32];
   grid_dep_sync();
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= d.nb) return;
+  const int t = threadIdx.x, lane = t & 31;
   int cnt = 0;
-  if (q < rb.gstart[rb.n_groups] && k.like_like) {
-    const int c = (int)rb.skey[q];
+  const ReplicaConst *R = nullptr;
+  int c = 0;
+  if (q < d.nb && q < rb.gstart[rb.n_groups] && k.like_like) {
+    c = (int)rb.skey[q];
     if (q == 0 || (int)rb.skey[q - 1] != c) {
+      R = &d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0];
       CellHead h;
-      cell_head(k, rb, d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0], q, c, h);
-      cnt = cell_pair_count(d, rb, h);
+      cell_head(k, rb, *R, q, c, h);
+      cell_pairs_visit(k, d, rb, h, [&](int a, int b) {
+        if (cnt < kHeadBuf) sbuf[t][cnt] = make_int2(a, b);
+        atomicAdd(&rb.deg[a], 1);
+        atomicAdd(&rb.deg[b], 1);
+        ++cnt;
+      });
     }
   }
-  rb.pair_count[q] = cnt;
-}
-
-// Each cell's pairs at its scanned offset in its system's pair segment.
-// Threads q < nrep record their system's pair count (a
-// list longer than its segment sets the overflow bit; the count is kept so
-// the host can size the segment).
-__global__ void k_rb_emit(SysConst k, DevState d, RebuildBufs rb, int prec) {
-  grid_dep_sync();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < d.nrep && d.due[q]) {
-    const ReplicaConst &R = d.rep[q];
-    const int np = rb.pair_off[sys_hi(rb, R)] - rb.pair_off[sys_lo(rb, R)];
-    d.np_rep[q] = np;
-    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+  // The block's candidate slots: a scan of the counts, one atomic.
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
   }
-  if (q >= rb.gstart[rb.n_groups] || !k.like_like) return;
-  const int c = (int)rb.skey[q];
-  if (q > 0 && (int)rb.skey[q - 1] == c) return;
-  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0];
-  CellHead h;
-  cell_head(k, rb, R, q, c, h);
-  cell_pair_emit(k, d, rb, R, h, rb.pair_off[q] - rb.pair_off[sys_lo(rb, R)], prec);
+  if (lane == 31) swarp[t >> 5] = incl;
+  __syncthreads();
+  if (t == 0) {
+    int run = 0;
+#pragma unroll
+    for (int w = 0; w < kCountBlock / 32; ++w) {
+      const int v = swarp[w];
+      swarp[w] = run;
+      run += v;
+    }
+    const int base = run > 0 ? atomicAdd(rb.cand_n, run) : 0;
+#pragma unroll
+    for (int w = 0; w < kCountBlock / 32; ++w) swarp[w] += base;
+  }
+  __syncthreads();
+  const int t0 = swarp[t >> 5] + incl - cnt;
+  if (cnt > 0 && cnt <= kHeadBuf) {
+    for (int i = 0; i < cnt; ++i)
+      if (t0 + i < rb.cand_cap) rb.cand[t0 + i] = sbuf[t][i];
+  } else if (cnt > kHeadBuf) {
+    CellHead h;
+    cell_head(k, rb, *R, q, c, h);
+    int i = 0;
+    cell_pairs_visit(k, d, rb, h, [&](int a, int b) {
+      if (t0 + i < rb.cand_cap) rb.cand[t0 + i] = make_int2(a, b);
+      ++i;
+    });
+  }
+  if (q < d.nb) {
+    rb.pair_count[q] = cnt;
+    rb.cand_start[q] = t0;
+  }
 }
 
 // First entry slot of bond b (rebuilt system R): its system's slots start at
@@ -305,20 +298,56 @@ __device__ __forceinline__ int entry_first(const RebuildBufs &rb, const ReplicaC
   return 2 * R.p0 + (rb.deg_off[b] - rb.deg_off[R.b0]);
 }
 
-// Entries (pair << 1 | role; role 0 = obj1, 1 = obj2) of every bond of the
-// rebuilt systems, in any order; the degrees are decremented back to zero.
-__global__ void k_rb_csr_fill(DevState d, RebuildBufs rb) {
+// Each cell's candidates at its scanned offset in its system's pair segment
+// (slots past the segment are not written), each new pair's stored force
+// (and virial record) zeroed, and both of its per-bond entries (pair << 1 |
+// role; role 0 = obj1, 1 = obj2) in any order, the entry counts going back
+// to zero.  A system whose list outgrew its segment gets no entries: its
+// step stops on the overflow bit and is redone.  Threads q < nrep record
+// their system's pair count (the count is kept so the host can size the
+// segment).
+__global__ void k_rb_place(DevState d, RebuildBufs rb, int prec) {
   grid_dep_sync();
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= d.pcap_total) return;
-  int r;
-  if (!pair_live(d, p, r) || !d.due[r]) return;
-  const ReplicaConst &R = d.rep[r];
-  const int a = d.pa[p], b = d.pb[p];
-  const int sa = atomicSub(&rb.deg[a], 1) - 1;
-  const int sb = atomicSub(&rb.deg[b], 1) - 1;
-  d.e_ent[entry_first(rb, R, a) + sa] = p << 1;
-  d.e_ent[entry_first(rb, R, b) + sb] = (p << 1) | 1;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < d.nrep && d.due[q]) {
+    const ReplicaConst &R = d.rep[q];
+    const int np = rb.pair_off[sys_hi(rb, R)] - rb.pair_off[sys_lo(rb, R)];
+    d.np_rep[q] = np;
+    if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
+  }
+  if (q >= d.nb) return;
+  const int cnt = rb.pair_count[q];
+  if (cnt == 0) return;
+  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0];
+  const int lo = rb.pair_off[sys_lo(rb, R)];
+  const bool fits = rb.pair_off[sys_hi(rb, R)] - lo <= R.pcap;
+  const int t0 = rb.cand_start[q];
+  int p = rb.pair_off[q] - lo;
+  for (int i = 0; i < cnt && p < R.pcap && t0 + i < rb.cand_cap; ++i, ++p) {
+    const int2 e = rb.cand[t0 + i];
+    const int g = R.p0 + p;
+    d.pa[g] = e.x;
+    d.pb[g] = e.y;
+    if (prec == 0) {
+      double2 *st = reinterpret_cast<double2 *>(d.pf64) + 2 * (size_t)g;
+      st[0] = make_double2(0.0, 0.0);
+      st[1] = make_double2(0.0, 0.0);
+      if (d.pv64) {  // a new Interaction's stress and potential are 0
+        double2 *v = reinterpret_cast<double2 *>(d.pv64) + 2 * (size_t)g;
+        v[0] = make_double2(0.0, 0.0);
+        v[1] = make_double2(0.0, 0.0);
+      }
+    } else {
+      reinterpret_cast<float4 *>(d.pf32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (d.pv32) reinterpret_cast<float4 *>(d.pv32)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (fits) {
+      const int sa = atomicSub(&rb.deg[e.x], 1) - 1;
+      const int sb = atomicSub(&rb.deg[e.y], 1) - 1;
+      d.e_ent[entry_first(rb, R, e.x) + sa] = g << 1;
+      d.e_ent[entry_first(rb, R, e.y) + sb] = (g << 1) | 1;
+    }
+  }
 }
 
 // Each bond's entries sorted by pair index -- the order in which the
@@ -334,6 +363,7 @@ __global__ void k_rb_csr_sort(DevState d, RebuildBufs rb) {
   const int r = rep_of_bond(d, b);
   if (!d.due[r]) return;
   const ReplicaConst &R = d.rep[r];
+  if (d.np_rep[r] > R.pcap) return;  // outgrew its segment: no entries
   const int e0 = entry_first(rb, R, b), n = rb.deg_off[b + 1] - rb.deg_off[b];
   d.e_off[b] = e0;
   d.e_cnt[b] = n;
@@ -398,13 +428,11 @@ int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, 
   launched += launch_exclusive_scan(rb.gcount, rb.gstart, rb.n_groups, rb.scan_tmp, st);
   launch_pdl(k_rb_scatter, dim3(g256), dim3(256), 0, st, d, rb);
   launch_pdl(k_rb_rank, dim3(g256), dim3(256), 0, st, d, rb);
-  launch_pdl(k_rb_count, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb);
-  launched += 3 + launch_exclusive_scan(rb.pair_count, rb.pair_off, d.nb, rb.scan_tmp, st);
-  launch_pdl(k_rb_emit, dim3((nb + 127) / 128), dim3(128), 0, st, k, d, rb, prec);
-  ++launched;
-  launched += launch_exclusive_scan(rb.deg, rb.deg_off, d.nb, rb.scan_tmp, st);
-  launch_pdl(k_rb_csr_fill, dim3((d.pcap_total > 0 ? d.pcap_total + 255 : 256) / 256), dim3(256),
-             0, st, d, rb);
+  const int gc = (nb + kCountBlock - 1) / kCountBlock;
+  launch_pdl(k_rb_count, dim3(gc), dim3(kCountBlock), 0, st, k, d, rb);
+  // pair_count and deg are one array of 2 nb (pair_off and deg_off alike).
+  launched += 3 + launch_exclusive_scan(rb.pair_count, rb.pair_off, 2LL * d.nb, rb.scan_tmp, st);
+  launch_pdl(k_rb_place, dim3(gc), dim3(kCountBlock), 0, st, d, rb, prec);
   launch_pdl(k_rb_csr_sort, dim3(g256), dim3(256), 0, st, d, rb);
   return launched + 2;
 }
