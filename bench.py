@@ -285,9 +285,9 @@ def new_context(sc, wl, prec, device):
 
 def cpu_runs(wl, cores):
     """CPU simulations of a workload for the baseline: the reference's own
-    code (oracle/_ref, OpenMP on `cores` threads) where it covers the
-    workload; tethered networks run on the C oracle, the reference's tether
-    code being unbuildable here.  Independent systems run one after another
+    code (oracle/_ref, OpenMP on `cores` threads, its own Crosslink and
+    Anchor code for tethered networks), or the C oracle on one thread where
+    oracle/_ref was not built.  Independent systems run one after another
     (the reference keeps static state: one simulation per process at a time),
     a leading subset of them.  Returns (kind, cores, [(make, bonds)], note),
     make() creating one simulation.  Uses the CPU checkers only (bond counts
@@ -296,16 +296,17 @@ def cpu_runs(wl, cores):
     from checkers import Oracle, Reference, oracle_n_bonds, workloads_module
     system, fils, sites, reps, xl = wl
     bonds = lambda fs: sum(oracle_n_bonds(f) for f in fs)
-    if xl is not None:
-        def make_tethered():
-            sim = Oracle(system, fils, sites)
-            sim.add_crosslinks(xl[0], xl[1], k_spring=xl[2], rest_length=xl[3])
-            return sim
-        return "port", 1, [(make_tethered, bonds(fils))], \
-            "C oracle with the restated tethers (1 thread)"
     use_ref = Reference.available()
     kind, cores = ("reference", cores) if use_ref else ("port", 1)
     make = (lambda *a: Reference(*a, n_threads=cores)) if use_ref else Oracle
+    if xl is not None:
+        def make_tethered():
+            sim = make(system, fils, sites)
+            sim.add_crosslinks(xl[0], xl[1], k_spring=xl[2], rest_length=xl[3])
+            return sim
+        return kind, cores, [(make_tethered, bonds(fils))], \
+            "with the crosslinks attached by the reference's own code" if use_ref else \
+            "C oracle with the restated tethers (1 thread)"
     if reps is None:
         if bonds(fils) <= 1000000:
             return kind, cores, [(lambda: make(system, fils, sites), bonds(fils))], ""

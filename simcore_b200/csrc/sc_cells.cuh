@@ -51,11 +51,10 @@ __device__ __forceinline__ int bond_cell(const DevState &d, const ReplicaConst &
 __device__ __forceinline__ bool pair_excluded(const SysConst &k,
                                               const DevState &d, int a, int b) {
   if (!k.like_like) return true;
-  if (d.bond_fil[a] == d.bond_fil[b]) {
-    int diff = a - b;
-    if (diff <= 1 && diff >= -1) return true;
-  }
-  return false;
+  // Adjacent indices first: the filaments are read only for those.
+  const int diff = a - b;
+  if (diff > 1 || diff < -1) return false;
+  return d.bond_fil[a] == d.bond_fil[b];
 }
 
 // Half-shell neighbour cells of (x, y, z) in the order of

@@ -185,7 +185,7 @@ struct PairStore {
   int *pa = nullptr, *pb = nullptr, *pos1 = nullptr, *pos2 = nullptr, *e_ent = nullptr;
   double *pf64 = nullptr, *cf64 = nullptr, *pv64 = nullptr;
   float *pf32 = nullptr, *cf32 = nullptr, *pv32 = nullptr;
-  int2 *cand = nullptr;  // the rebuild's candidate pairs, one per slot
+  int4 *cand = nullptr;  // the rebuild's candidate pairs, one per slot
   long long cap = 0;     // slots
 };
 

@@ -84,9 +84,10 @@ struct RebuildBufs {
   int *pair_count, *pair_off;
   int *deg, *deg_off;
   int *scan_tmp;
-  // Candidate pairs (a, b), each cell head's at cand_start[entry], in the
-  // reference's order; cand_cap = the pair slots of all segments.
-  int2 *cand;
+  // Candidate pairs (a, b, head entry, -), each cell head's at
+  // cand_start[entry], in the reference's order; cand_cap = the pair slots of
+  // all segments.
+  int4 *cand;
   int cand_cap;
   int *cand_n;         // slots taken in the current rebuild
   int *cand_start;     // per sorted entry

@@ -276,13 +276,13 @@ __global__ void __launch_bounds__(kCountBlock) k_rb_count(SysConst k, DevState d
   const int t0 = swarp[t >> 5] + incl - cnt;
   if (cnt > 0 && cnt <= kHeadBuf) {
     for (int i = 0; i < cnt; ++i)
-      if (t0 + i < rb.cand_cap) rb.cand[t0 + i] = sbuf[t][i];
+      if (t0 + i < rb.cand_cap) rb.cand[t0 + i] = make_int4(sbuf[t][i].x, sbuf[t][i].y, q, 0);
   } else if (cnt > kHeadBuf) {
     CellHead h;
     cell_head(k, rb, *R, q, c, h);
     int i = 0;
     cell_pairs_visit(k, d, rb, h, [&](int a, int b) {
-      if (t0 + i < rb.cand_cap) rb.cand[t0 + i] = make_int2(a, b);
+      if (t0 + i < rb.cand_cap) rb.cand[t0 + i] = make_int4(a, b, q, 0);
       ++i;
     });
   }
@@ -298,33 +298,31 @@ __device__ __forceinline__ int entry_first(const RebuildBufs &rb, const ReplicaC
   return 2 * R.p0 + (rb.deg_off[b] - rb.deg_off[R.b0]);
 }
 
-// Each cell's candidates at its scanned offset in its system's pair segment
-// (slots past the segment are not written), each new pair's stored force
-// (and virial record) zeroed, and both of its per-bond entries (pair << 1 |
-// role; role 0 = obj1, 1 = obj2) in any order, the entry counts going back
-// to zero.  A system whose list outgrew its segment gets no entries: its
-// step stops on the overflow bit and is redone.  Threads q < nrep record
-// their system's pair count (the count is kept so the host can size the
-// segment).
+// Every candidate to its slot -- its cell's scanned offset in its system's
+// pair segment plus its place among the cell's candidates (slots past the
+// segment are not written) -- with the new pair's stored force (and virial
+// record) zeroed and both of its per-bond entries (pair << 1 | role; role 0
+// = obj1, 1 = obj2) in any order, the entry counts going back to zero.  A
+// system whose list outgrew its segment gets no entries: its step stops on
+// the overflow bit and is redone.  Threads u < nrep record their system's
+// pair count (the count is kept so the host can size the segment).
 __global__ void k_rb_place(DevState d, RebuildBufs rb, int prec) {
   grid_dep_sync();
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q < d.nrep && d.due[q]) {
-    const ReplicaConst &R = d.rep[q];
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < d.nrep && d.due[u]) {
+    const ReplicaConst &R = d.rep[u];
     const int np = rb.pair_off[sys_hi(rb, R)] - rb.pair_off[sys_lo(rb, R)];
-    d.np_rep[q] = np;
+    d.np_rep[u] = np;
     if (np > R.pcap) atomicOr(d.status, ST_LIST_OVERFLOW);
   }
-  if (q >= d.nb) return;
-  const int cnt = rb.pair_count[q];
-  if (cnt == 0) return;
-  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, rb.sval[q]) : 0];
+  if (u >= min(*rb.cand_n, rb.cand_cap)) return;
+  const int4 e = rb.cand[u];
+  const int q = e.z;
+  const ReplicaConst &R = d.rep[d.nrep > 1 ? rep_of_bond(d, e.x) : 0];
   const int lo = rb.pair_off[sys_lo(rb, R)];
   const bool fits = rb.pair_off[sys_hi(rb, R)] - lo <= R.pcap;
-  const int t0 = rb.cand_start[q];
-  int p = rb.pair_off[q] - lo;
-  for (int i = 0; i < cnt && p < R.pcap && t0 + i < rb.cand_cap; ++i, ++p) {
-    const int2 e = rb.cand[t0 + i];
+  const int p = rb.pair_off[q] - lo + (u - rb.cand_start[q]);
+  if (p < R.pcap) {
     const int g = R.p0 + p;
     d.pa[g] = e.x;
     d.pb[g] = e.y;
@@ -432,7 +430,8 @@ int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, 
   launch_pdl(k_rb_count, dim3(gc), dim3(kCountBlock), 0, st, k, d, rb);
   // pair_count and deg are one array of 2 nb (pair_off and deg_off alike).
   launched += 3 + launch_exclusive_scan(rb.pair_count, rb.pair_off, 2LL * d.nb, rb.scan_tmp, st);
-  launch_pdl(k_rb_place, dim3(gc), dim3(kCountBlock), 0, st, d, rb, prec);
+  const int cap = rb.cand_cap > d.nrep ? rb.cand_cap : d.nrep;
+  launch_pdl(k_rb_place, dim3((cap + 255) / 256), dim3(256), 0, st, d, rb, prec);
   launch_pdl(k_rb_csr_sort, dim3(g256), dim3(256), 0, st, d, rb);
   return launched + 2;
 }
