@@ -44,10 +44,10 @@ I_STEPS_PER_STEP = 20
 N_SNAPSHOTS = 4
 # DRAM bytes (read + write) of one k_integrate launch, mixed precision, from
 # ncu (cold cache), per workload captured, with the block layout the timed
-# runs use: for B (192-site blocks) the mean of a midstep launch (24.41 MB)
-# and a full-step launch (41.94 MB), which alternate.  Workloads without a
+# runs use: for B (192-site blocks) the mean of a midstep launch (22.11 MB)
+# and a full-step launch (39.73 MB), which alternate.  Workloads without a
 # capture report null.
-TRAFFIC_K_INTEGRATE_MIXED = {"B": 33.18e6}
+TRAFFIC_K_INTEGRATE_MIXED = {"B": 30.92e6}
 TRAFFIC_LAYOUT = {"B": "0,192"}
 WORKLOAD_DESCS = {
     "A": "A: 100 filaments x 20 bonds (2,000 segments, 2,100 sites), 3D periodic cube side 50, "
