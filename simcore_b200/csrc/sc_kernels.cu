@@ -484,6 +484,14 @@ template <int ND>
 __device__ __forceinline__ bool near_parallel(const SysConst &k, const float *hf,
                                               const BondGeomF32 &A, const BondGeomF32 &B,
                                               const float4 &st) {
+  // Cheap rejection first, with the operations sphero_f32 repeats (so they
+  // are shared): for unit vectors 1 - (u1 . u2)^2 = |u1 x u2|^2, and the two
+  // FP32 evaluations differ by less than 2e-6 here, so no pair the exact
+  // test below flags is rejected.
+  float c = 0.f;
+#pragma unroll
+  for (int i = 0; i < ND; ++i) c = __fmaf_rn(A.u[i], B.u[i], c);
+  if (!(__fmaf_rn(-c, c, 1.0f) < k.npx_s2 + 2e-6f)) return false;
   float s2;
   const float cz = __fmaf_rn(A.u[0], B.u[1], -A.u[1] * B.u[0]);
   if (ND == 3) {
