@@ -6,18 +6,23 @@ using namespace scapi;
 
 extern "C" {
 
-// Captures one graph: WHILE (loop_count > 0) { decide -> IF(rebuild) ->
-// midstep -> full step -> tail }.  Built for the current geometry-buffer
-// parity; every BD step returns the parity to where it started.
+// Captures one graph: head (loop condition, first rebuild decision) ->
+// WHILE (loop_count > 0) { IF(rebuild) -> midstep -> full step -> tail (next
+// rebuild decision) }.  Built for the current geometry-buffer parity; every
+// BD step returns the parity to where it started.
 static sc_status build_graph(sc_ctx *c) {
   drop_graph(c);
   cudaGraph_t g = nullptr;
   CK(cudaGraphCreate(&g, 0));
-  cudaGraphConditionalHandle h_loop;
+  const int interaction = c->desc.interaction_flag ? 1 : 0;
+  cudaGraphConditionalHandle h_loop, h_if = 0;
   CK(cudaGraphConditionalHandleCreate(&h_loop, g, 0, 0));
-  // head kernel: sets the loop condition
+  // The rebuild condition is set by the head and by every tail (the decision
+  // for the step after), so it belongs to the outer graph, like the loop's.
+  if (interaction) CK(cudaGraphConditionalHandleCreate(&h_if, g, 0, 0));
+  // head kernel: sets the loop condition and decides the first rebuild
   CK(cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  sc::launch_loop_head(c->d, h_loop, c->st);
+  sc::launch_loop_head(c->d, h_loop, h_if, interaction, c->st);
   cudaStreamCaptureStatus cs;
   const cudaGraphNode_t *deps = nullptr;
   size_t ndeps = 0;
@@ -33,23 +38,15 @@ static sc_status build_graph(sc_ctx *c) {
   cudaGraphNode_t wnode;
   CK(cudaGraphAddNode(&wnode, g, head.data(), head.size(), &wp));
   cudaGraph_t body = wp.conditional.phGraph_out[0];
-  const int interaction = c->desc.interaction_flag ? 1 : 0;
   std::vector<cudaGraphNode_t> tail;
   if (interaction) {
-    cudaGraphConditionalHandle h_if;
-    CK(cudaGraphConditionalHandleCreate(&h_if, body, 0, 0));
-    CK(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    sc::launch_decide(c->k, c->d, h_if, c->st);
-    CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, nullptr, &deps, &ndeps));
-    std::vector<cudaGraphNode_t> dec(deps, deps + ndeps);
-    CK(cudaStreamEndCapture(c->st, &body));
     cudaGraphNodeParams ip = {};
     ip.type = cudaGraphNodeTypeConditional;
     ip.conditional.handle = h_if;
     ip.conditional.type = cudaGraphCondTypeIf;
     ip.conditional.size = 1;
     cudaGraphNode_t inode;
-    CK(cudaGraphAddNode(&inode, body, dec.data(), dec.size(), &ip));
+    CK(cudaGraphAddNode(&inode, body, nullptr, 0, &ip));
     cudaGraph_t rb = ip.conditional.phGraph_out[0];
     CK(cudaStreamBeginCaptureToGraph(c->st, rb, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     long long launches = c->launches;
@@ -89,7 +86,7 @@ static sc_status build_graph(sc_ctx *c) {
                            c->capture, c->prec, c->fast, c->st, fuse);
     }
   }
-  sc::launch_loop_tail(c->d, c->desc.stoch_flag ? 1 : 0, h_loop, c->st);
+  sc::launch_loop_tail(c->d, c->desc.stoch_flag ? 1 : 0, h_loop, h_if, interaction, c->st);
   CK(cudaStreamEndCapture(c->st, &body));
   CK(cudaGetLastError());
   cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);

@@ -1308,11 +1308,14 @@ int launch_csr(const DevState &d, int *deg, const int *deg_off, cudaStream_t st)
 // ---------------------------------------------------------------------------
 // Device-side control of captured step graphs.
 
-// Interact's rebuild check on the device (CheckUpdateInteractions + GetDrMax,
-// src/interaction_manager.cpp:284-312, include/simcore/species.hpp:114-118):
-// sets the IF condition of the rebuild body; above 10000 the reference
-// throws, here the status word records it and no rebuild runs.
-__global__ void k_decide(SysConst k, DevState d, cudaGraphConditionalHandle h) {
+// Interact's rebuild check on the device for the next BD step of a graph
+// loop (CheckUpdateInteractions + GetDrMax, src/interaction_manager.cpp:
+// 284-312, include/simcore/species.hpp:114-118), one block: each system is
+// due when its displacement maximum (reduced on the device by the last full
+// step) is above its threshold; above 10000 the reference throws, here the
+// status word records it and no rebuild runs.  Sets the rebuild node's
+// condition h_if.
+__device__ void decide_systems(const DevState &d, cudaGraphConditionalHandle h_if) {
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
@@ -1325,29 +1328,38 @@ __global__ void k_decide(SysConst k, DevState d, cudaGraphConditionalHandle h) {
     if (due) any = 1;
   }
   __syncthreads();
-  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h_if, any ? 1u : 0u);
 }
 
-__global__ void k_loop_head(DevState d, cudaGraphConditionalHandle h) {
-  cudaGraphSetConditional(h, *d.loop_count > 0 ? 1u : 0u);
+// Start of a graph loop: the loop condition and the first step's rebuild
+// decision.
+__global__ void k_loop_head(DevState d, cudaGraphConditionalHandle h,
+                            cudaGraphConditionalHandle h_if, int decide) {
+  if (decide) decide_systems(d, h_if);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, *d.loop_count > 0 ? 1u : 0u);
 }
 
 // End of one BD step (midstep + full step) of a graph loop: advances the
-// noise counter and decrements the remaining count.  A recorded error stops
-// the loop.  A step whose rebuild overflowed its list did nothing past the
-// rebuild: it stays counted as remaining, so the host can grow the list,
-// redo the rebuild and resume with it.
-__global__ void k_loop_tail(DevState d, int stoch, cudaGraphConditionalHandle h) {
-  const unsigned status = *d.status;
+// noise counter, decrements the remaining count and decides the next step's
+// rebuild.  A recorded error stops the loop.  A step whose rebuild
+// overflowed its list did nothing past the rebuild: it stays counted as
+// remaining, so the host can grow the list, redo the rebuild and resume
+// with it.
+__global__ void k_loop_tail(DevState d, int stoch, cudaGraphConditionalHandle h,
+                            cudaGraphConditionalHandle h_if, int decide) {
+  const unsigned status = *d.status;  // the same word for every thread
   if (status & ST_LIST_OVERFLOW) {
-    cudaGraphSetConditional(h, 0u);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
     return;
   }
-  if (stoch) *d.mcount += 1ull;
-  int left = *d.loop_count - 1;
-  if (status != 0u) left = 0;
-  *d.loop_count = left;
-  cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
+  if (threadIdx.x == 0) {
+    if (stoch) *d.mcount += 1ull;
+    int left = *d.loop_count - 1;
+    if (status != 0u) left = 0;
+    *d.loop_count = left;
+    cudaGraphSetConditional(h, left > 0 ? 1u : 0u);
+  }
+  if (decide) decide_systems(d, h_if);
 }
 
 __global__ void k_advance_mcount(DevState d) {
@@ -1355,21 +1367,15 @@ __global__ void k_advance_mcount(DevState d) {
   *d.mcount += 1ull;
 }
 
-int launch_decide(const SysConst &k, const DevState &d,
-                  cudaGraphConditionalHandle h, cudaStream_t st) {
-  k_decide<<<1, 256, 0, st>>>(k, d, h);
-  return 1;
-}
-
 int launch_loop_head(const DevState &d, cudaGraphConditionalHandle h,
-                     cudaStream_t st) {
-  k_loop_head<<<1, 1, 0, st>>>(d, h);
+                     cudaGraphConditionalHandle h_if, int decide, cudaStream_t st) {
+  k_loop_head<<<1, 256, 0, st>>>(d, h, h_if, decide);
   return 1;
 }
 
 int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
-                     cudaStream_t st) {
-  k_loop_tail<<<1, 1, 0, st>>>(d, stoch, h);
+                     cudaGraphConditionalHandle h_if, int decide, cudaStream_t st) {
+  k_loop_tail<<<1, 256, 0, st>>>(d, stoch, h, h_if, decide);
   return 1;
 }
 

@@ -97,12 +97,13 @@ struct RebuildBufs {
 // body (launched without the programmatic-dependence attribute).
 int launch_rebuild(const SysConst &k, const DevState &d, const RebuildBufs &rb, int prec,
                    cudaStream_t st, bool first_in_graph);
-int launch_decide(const SysConst &k, const DevState &d,
-                  cudaGraphConditionalHandle h, cudaStream_t st);
+// Graph loop control: the head sets the WHILE condition h and, with
+// `decide`, the first step's rebuild decision (IF condition h_if); the tail
+// ends a BD step and decides the next step's rebuild.
 int launch_loop_head(const DevState &d, cudaGraphConditionalHandle h,
-                     cudaStream_t st);
+                     cudaGraphConditionalHandle h_if, int decide, cudaStream_t st);
 int launch_loop_tail(const DevState &d, int stoch, cudaGraphConditionalHandle h,
-                     cudaStream_t st);
+                     cudaGraphConditionalHandle h_if, int decide, cudaStream_t st);
 int launch_advance_mcount(const DevState &d, cudaStream_t st);
 int launch_zero_dr(const DevState &d, cudaStream_t st);
 // Grid sized for `expected` pairs (one system) or every slot (several); the
