@@ -150,15 +150,15 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
         CK(cudaEventElapsedTime(&ms, c->gev0, c->gev1));
         c->graph_ms += ms;
       }
-      // Kernels the graph ran: loop head, per BD step decide + the two
-      // tether kernels (mesh lambdas, anchor forces) + 2 steps + tail (the
-      // stopped step's too), per rebuild the captured sequence.  A step is
-      // its pair kernel (unless fused; near-parallel pairs are evaluated in
-      // place), thermo and one or two integrator kernels.
+      // Kernels the graph ran: loop head, per BD step the two tether
+      // kernels (mesh lambdas, anchor forces) + 2 steps + tail (the stopped
+      // step's too), per rebuild the captured sequence.  A step is its pair
+      // kernel (unless fused; near-parallel pairs are evaluated in place),
+      // thermo and one or two integrator kernels.
       const int int_l = (c->d.n_wg > 0 ? 1 : 0) + (c->nblocks > 0 ? 1 : 0);
       const long long per_bd =
           c->desc.interaction_flag
-              ? 2 + (c->d.nx ? 2 : 0) +
+              ? 1 + (c->d.nx ? 2 : 0) +
                     2 * ((c->graph_fused ? 0 : 1) + int_l + (c->k.thermo ? 1 : 0))
               : 1 + 2 * int_l;
       c->launches += 1 + (long long)(done + (overflow ? 1 : 0)) * per_bd +
