@@ -856,11 +856,12 @@ __global__ void __launch_bounds__(MAXC, IntegrateBounds<MAXC, FAST>::min_blocks)
   // ---- P2: random forces, projection, previous positions -----------------
   double fr[3] = {0, 0, 0};
   if (midstep && k.stoch && FAST && !pcr) {
-    // The mixed step draws, projects and applies its noise in FP32 (the
-    // north star keeps the tension solve, the bending forces that feed it
-    // and the positions in FP64): the same Philox words, the uniforms to
-    // 2^-24, the projection system solved from both ends in FP32 over the
-    // Thomas arrays' first halves, the projected force added in FP64.
+    // The mixed step draws, projects and applies its noise in FP32 (its
+    // precision contract keeps only the tension solve, the bending forces
+    // that feed it and the positions in FP64): the same Philox words, the
+    // uniforms to 2^-24, the projection system solved from both ends in FP32
+    // over the Thomas arrays' first halves, the projected force added in
+    // FP64.
     float *ffn = reinterpret_cast<float *>(sfn);  // 3 x C floats
     float *fT = reinterpret_cast<float *>(sT), *fa = reinterpret_cast<float *>(sa);
     float *fb = reinterpret_cast<float *>(sb), *fcm = reinterpret_cast<float *>(sc);
