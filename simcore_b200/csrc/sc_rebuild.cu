@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(256) k_rb_keys(SysConst k, DevState d, Rebuild
     d.rep_rebuilds[r] += 1;
   }
   for (int i = tid; i < d.ns; i += nthreads) {
-    if (!d.due[d.fil[d.site_fil[i]].rep]) continue;
+    // (One system is always due when its rebuild runs: no lookup.)
+    if (d.nrep > 1 && !d.due[d.fil[d.site_fil[i]].rep]) continue;
     d.dz[0][i] = d.r[0][i];
     d.dz[1][i] = d.r[1][i];
     d.dz[2][i] = d.r[2][i];
