@@ -110,6 +110,7 @@ struct sc_ctx {
     unsigned long long dr_bits;
     unsigned status;
     int total;
+    long long rebuilds[2];  // rebuild counter before and after a graph launch
   } *hb = nullptr;
   unsigned long long *h_dr = nullptr;  // per system displacement maxima
   int *h_np = nullptr;                 // per system pair counts

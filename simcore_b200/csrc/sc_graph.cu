@@ -127,18 +127,21 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       if (!c->graph_exec || c->graph_rbuf != c->rbuf) CKS(build_graph(c));
       *c->h_loop = bd;
       CK(cudaMemcpyAsync(c->d.loop_count, c->h_loop, sizeof(int), cudaMemcpyHostToDevice, c->st));
-      long long nr0 = 0, nr1 = 0;
-      CK(cudaMemcpyAsync(&nr0, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+      // Every readback goes to pinned memory: one synchronisation per launch.
+      CK(cudaMemcpyAsync(&c->hb->rebuilds[0], c->d.n_rebuilds, sizeof(long long),
+                         cudaMemcpyDeviceToHost, c->st));
       CK(cudaEventRecord(c->gev0, c->st));
       CK(cudaGraphLaunch(c->graph_exec, c->st));
       CK(cudaEventRecord(c->gev1, c->st));
-      CK(cudaMemcpyAsync(&nr1, c->d.n_rebuilds, sizeof(long long), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaMemcpyAsync(&c->hb->rebuilds[1], c->d.n_rebuilds, sizeof(long long),
+                         cudaMemcpyDeviceToHost, c->st));
       CK(cudaMemcpyAsync(c->h_loop, c->d.loop_count, sizeof(int), cudaMemcpyDeviceToHost, c->st));
       c->pairs_ready = false;
       CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost,
                          c->st));
       CK(cudaStreamSynchronize(c->st));
       const unsigned st = c->hb->status;
+      const long long nr0 = c->hb->rebuilds[0], nr1 = c->hb->rebuilds[1];
       const bool overflow = (st & sc::ST_LIST_OVERFLOW) != 0u;
       // BD steps completed: all of them, or those before the stopped one.
       const int done = overflow ? bd - *c->h_loop : bd;
