@@ -139,6 +139,9 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
       c->pairs_ready = false;
       CK(cudaMemcpyAsync(&c->hb->status, c->d.status, sizeof(unsigned), cudaMemcpyDeviceToHost,
                          c->st));
+      if (c->d.nrep > 0)  // the displacement maxima too (readback's copies)
+        CK(cudaMemcpyAsync(c->h_dr, c->d.dr_max_bits, sizeof(unsigned long long) * c->d.nrep,
+                           cudaMemcpyDeviceToHost, c->st));
       CK(cudaStreamSynchronize(c->st));
       const unsigned st = c->hb->status;
       const long long nr0 = c->hb->rebuilds[0], nr1 = c->hb->rebuilds[1];
@@ -168,7 +171,7 @@ sc_status sc_step_graph(sc_ctx *c, int n) {
                      (nr1 - nr0) * c->rebuild_kernels;
       bd -= done;
       if (!overflow) {
-        CKS(readback(c));
+        CKS(check_status(c));  // status and maxima were read with the counters
         break;
       }
       if (st & ~sc::ST_LIST_OVERFLOW) {
