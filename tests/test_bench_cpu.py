@@ -6,6 +6,7 @@ import os
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 from checkers import Reference
@@ -64,3 +65,26 @@ def test_algorithmic_bytes():
     b_int, b_pair = bench.algorithmic_bytes(ns, nb, npairs, "fp64")
     assert b_int == 96 * ns + 104 * nb
     assert bench.fused_bytes(ns, nb, npairs) == 96 * ns + 64 * nb + 8 * npairs
+
+
+@pytest.mark.skipif(not Reference.available(), reason="reference build not present")
+def test_tethered_cpu_baseline_runs_the_reference_crosslinks():
+    """The CPU baseline of a crosslinked network is the reference's own code,
+    its tethers attached by its own Crosslink and Anchor classes, and it
+    steps."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from checkers import oracle_workload
+    wl = oracle_workload("E", seed=0, scale=0.002)
+    assert wl[4] is not None and len(wl[4][0]) > 0
+    kind, cores, runs, note = bench.cpu_runs(wl, 2)
+    assert kind == "reference" and cores == 2 and len(runs) == 1
+    assert "reference" in note
+    make, n_bonds = runs[0]
+    sim = make()
+    try:
+        assert sim.n_links == len(wl[4][0])
+        assert sim.step(2) >= 0.0
+        assert np.isfinite(sim.sites()).all()
+    finally:
+        sim.close()
